@@ -1,0 +1,326 @@
+"""CPU oracle for the SReD block-correlation path (numpy/ctypes front end).
+
+TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()``
+and the CPU-baseline leg of ``bench.py`` as the checker. The product
+(``sred_b200``) never imports it.
+
+Layers:
+  * ``liboracle.so``  (``oracle/sred_oracle.c``): FP32 restatement of the
+    reference kernels and Java host code (bit-exact target) and the FP64 judge.
+  * ``_ref/librefshim.so``: the reference's own OpenCL kernels compiled as C++
+    by ``oracle/refshim/build.py`` (present only where a reference checkout
+    was available at build time; it travels with the built tree).
+  * Pure-Python helpers below: the Java-side orchestration of
+    ``java/GlobalRepetition2D_.java:97-145`` and
+    ``java/CLUtils.java:486-981`` expressed over those primitives.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+EPSILON = np.float32(1e-7)
+
+# Metric names exactly as the reference's dialogs spell them
+# (java/GlobalRepetition2D_.java:20-25, java/BlockRepetition2D_.java:18-23).
+GLOBAL_METRICS = {"Pearson's R": 0, "SSIM": 1, "NRMSE": 2, "Abs. diff. of StdDevs": 3}
+BLOCK_METRICS = {"Pearson's R": 0, "SSIM": 1, "NRMSE (inverted)": 2, "Abs. Diff. of StdDevs.": 3}
+COSINE = 4
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_fp = C.POINTER(C.c_float)
+
+_lib = None
+_ref = None
+
+
+def _build() -> None:
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_oracle_build", HERE / "refshim" / "build.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    mod.build_oracle()
+    mod.build_refshim(Path("/root/reference"))
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        so = HERE / "liboracle.so"
+        if not so.exists():
+            _build()
+        L = C.CDLL(str(so))
+        L.orc_block_size.restype = C.c_int
+        L.orc_local_stats_f32.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, _f32p, _f32p]
+        L.orc_mean_noise_var.argtypes = [_f32p, C.c_int, C.c_int, _fp]
+        L.orc_relevance_mask.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, _f32p, C.c_float,
+                                         _f32p, _fp, _fp]
+        L.orc_normalize_image.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        L.orc_n_pixels.restype = C.c_float
+        L.orc_n_pixels.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.orc_global_f32.argtypes = [C.c_int, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, _f32p, _f32p,
+                                     C.c_float, C.c_float, _i32p, C.c_int, _f32p, _f32p]
+        L.orc_global_f64.argtypes = [C.c_int, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, _f32p,
+                                     C.c_float, C.c_float, _i32p, C.c_int, _f64p, _f64p]
+        L.orc_global_finalize_f32.argtypes = [C.c_int, _f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                              _f32p, C.c_float, C.c_float, C.c_int, _f32p]
+        L.orc_global_finalize_f64.argtypes = [C.c_int, _f64p, _f64p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                              _f32p, C.c_float, C.c_double, C.c_int, _f64p]
+        L.orc_reference_block.argtypes = [_f32p, C.c_int, C.c_int, _f32p, _fp, _fp]
+        L.orc_block_kernel_f32.argtypes = [C.c_int, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, _f32p,
+                                           _f32p, _f32p, C.c_int, C.c_float, C.c_float, _f32p]
+        L.orc_block_postprocess_f32.argtypes = [C.c_int, _f32p, _f32p, C.c_int, C.c_int, C.c_int,
+                                                C.c_int, _f32p, C.c_float, C.c_int]
+        L.orc_block_kernel_f64.argtypes = [C.c_int, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, _f32p,
+                                           _f32p, C.c_int, C.c_float, C.c_float, _f64p]
+        L.orc_java_random_floats.argtypes = [C.c_int64, C.c_int, _f32p]
+        _lib = L
+    return _lib
+
+
+def refshim() -> C.CDLL | None:
+    """The reference's own kernels compiled for the CPU, or None if not built here."""
+    global _ref
+    if _ref is None:
+        so = HERE / "_ref" / "librefshim.so"
+        if not so.exists():
+            return None
+        _ref = C.CDLL(str(so))
+    return _ref
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+# --------------------------------------------------------------------------
+# Host numerics (java/Utils.java)
+# --------------------------------------------------------------------------
+
+def block_size(bw: int, bh: int) -> int:
+    """Ellipse block size K (java/GlobalRepetition2D_.java:102-111)."""
+    return lib().orc_block_size(bw, bh)
+
+
+def normalize_input(img: np.ndarray) -> np.ndarray:
+    """Min-max to [0,1] with epsilon (java/Utils.java:707-722)."""
+    a = _f32(img).copy()
+    lib().orc_normalize_input(a.ctypes.data_as(_fp), C.c_int(a.size))
+    return a
+
+
+def local_stats(img: np.ndarray, bw: int, bh: int):
+    """(means, stds) per pixel, FP32 reference order (cl/kernelGetLocalStatistics2D.cl)."""
+    img = _f32(img)
+    H, W = img.shape
+    m = np.zeros_like(img)
+    s = np.zeros_like(img)
+    lib().orc_local_stats_f32(img, W, H, bw, bh, m, s)
+    return m, s
+
+
+def mean_noise_var(img: np.ndarray) -> float:
+    img = _f32(img)
+    H, W = img.shape
+    out = C.c_float()
+    if lib().orc_mean_noise_var(img, W, H, C.byref(out)) != 0:
+        raise IndexError("image smaller than one noise tile")
+    return np.float32(out.value)
+
+
+def relevance_mask(img: np.ndarray, bw: int, bh: int, stds: np.ndarray, c: float):
+    """(mask, threshold, noise_var) as java/Utils.java:944-968."""
+    img = _f32(img)
+    H, W = img.shape
+    mask = np.zeros_like(img)
+    thr, nv = C.c_float(), C.c_float()
+    if lib().orc_relevance_mask(img, W, H, bw // 2, bh // 2, _f32(stds), C.c_float(c), mask,
+                                C.byref(thr), C.byref(nv)) != 0:
+        raise IndexError("image smaller than one noise tile")
+    return mask, np.float32(thr.value), np.float32(nv.value)
+
+
+def normalize_image(a: np.ndarray, rw: int, rh: int, mask: np.ndarray | None) -> np.ndarray:
+    a = _f32(a).copy()
+    H, W = a.shape
+    mp = None if mask is None else _f32(mask)
+    rc = lib().orc_normalize_image(a, W, H, rw, rh, None if mp is None else mp.ctypes.data)
+    if rc != 0:
+        raise ValueError("Relevance mask must be binary (0.0f or 1.0f)")
+    return a
+
+
+def n_pixels(mask: np.ndarray, rw: int, rh: int) -> np.float32:
+    H, W = mask.shape
+    return np.float32(lib().orc_n_pixels(_f32(mask), W, H, rw, rh))
+
+
+def reference_block(block_img: np.ndarray):
+    """(pixels[K], mean, std) as java/Utils.java:557-639."""
+    b = _f32(block_img)
+    bh, bw = b.shape
+    px = np.zeros(bw * bh, np.float32)
+    m, s = C.c_float(), C.c_float()
+    K = lib().orc_reference_block(b, bw, bh, px, C.byref(m), C.byref(s))
+    return px[:K].copy(), np.float32(m.value), np.float32(s.value)
+
+
+def java_random_floats(seed: int, n: int) -> np.ndarray:
+    out = np.zeros(n, np.float32)
+    lib().orc_java_random_floats(seed, n, out)
+    return out
+
+
+# --------------------------------------------------------------------------
+# Global repetition map
+# --------------------------------------------------------------------------
+
+def _pix(W, H, rw, rh, pix):
+    if pix is None:
+        ys, xs = np.mgrid[rh:H - rh, rw:W - rw]
+        pix = (ys * W + xs).ravel()
+    return np.ascontiguousarray(pix, dtype=np.int32)
+
+
+def global_sums_f32(metric: str, img, bw, bh, means, stds, filter_param, threshold, pix=None,
+                    use_refshim: bool = False):
+    """(num, den) per listed reference pixel, FP32 reference semantics.
+
+    With ``use_refshim`` the reference's own kernel (compiled for the CPU) runs
+    instead of the restatement."""
+    img = _f32(img)
+    H, W = img.shape
+    pix = _pix(W, H, bw // 2, bh // 2, pix)
+    m = GLOBAL_METRICS[metric]
+    if use_refshim:
+        R = refshim()
+        if R is None:
+            raise RuntimeError("refshim not built (no reference checkout at build time)")
+        K = block_size(bw, bh)
+        num = np.zeros(W * H, np.float32)
+        den = np.zeros(W * H, np.float32)
+        name = ["kernelGetGlobalPearson2D", "kernelGetGlobalSsim2D", "kernelGetGlobalNrmse2D",
+                "kernelGetGlobalAbsDiffStds2D"][m]
+        fn = getattr(R, f"rs_{name}")
+        args = [C.c_int(K), C.c_int(W), C.c_int(H), C.c_int(bw), C.c_int(bh), C.c_float(filter_param),
+                C.c_float(threshold), C.c_float(EPSILON), C.c_float(0), C.c_float(0),
+                pix.ctypes.data_as(C.c_void_p), C.c_int(pix.size), img.ctypes.data_as(C.c_void_p)]
+        if m != 3:
+            args.append(_f32(means).ctypes.data_as(C.c_void_p))
+        args += [_f32(stds).ctypes.data_as(C.c_void_p), den.ctypes.data_as(C.c_void_p),
+                 num.ctypes.data_as(C.c_void_p)]
+        if fn(*args) != 0:
+            raise ValueError(f"refshim has no instantiation for K={K}")
+        return num[pix], den[pix]
+    num = np.zeros(pix.size, np.float32)
+    den = np.zeros(pix.size, np.float32)
+    lib().orc_global_f32(m, img, W, H, bw, bh, _f32(means), _f32(stds), C.c_float(filter_param),
+                         C.c_float(threshold), pix, pix.size, num, den)
+    return num, den
+
+
+def global_sums_f64(metric: str, img, bw, bh, stds, filter_param, threshold, pix=None):
+    """(num, den) per listed reference pixel, FP64 judge."""
+    img = _f32(img)
+    H, W = img.shape
+    pix = _pix(W, H, bw // 2, bh // 2, pix)
+    num = np.zeros(pix.size, np.float64)
+    den = np.zeros(pix.size, np.float64)
+    lib().orc_global_f64(GLOBAL_METRICS[metric], img, W, H, bw, bh, _f32(stds),
+                         C.c_float(filter_param), C.c_float(threshold), pix, pix.size, num, den)
+    return num, den
+
+
+def global_map(metric: str, img, bw: int, bh: int, relevance_constant: float, normalize=True,
+               precision: str = "f32", use_refshim: bool = False):
+    """Full global repetition map as GlobalRepetition2D_ computes it after
+    preprocessing (java/GlobalRepetition2D_.java:97-145, java/CLUtils.java:2174).
+
+    Returns a dict with the map and every intermediate."""
+    img = _f32(img)
+    H, W = img.shape
+    rw, rh = bw // 2, bh // 2
+    means, stds = local_stats(img, bw, bh)
+    mask, thr, nv = relevance_mask(img, bw, bh, stds, relevance_constant)
+    npx = n_pixels(mask, rw, rh)
+    pix = _pix(W, H, rw, rh, None)
+    m = GLOBAL_METRICS[metric]
+    if precision == "f32":
+        num, den = global_sums_f32(metric, img, bw, bh, means, stds, nv, thr, pix, use_refshim)
+        nf = np.zeros(W * H, np.float32); df = np.zeros(W * H, np.float32)
+        nf[pix] = num; df[pix] = den
+        out = np.zeros(W * H, np.float32)
+        rc = lib().orc_global_finalize_f32(m, nf, df, W, H, rw, rh, mask.ravel().copy(),
+                                           C.c_float(relevance_constant), C.c_float(npx),
+                                           int(normalize), out)
+        if rc != 0:
+            raise ValueError("non-binary mask")
+    else:
+        num, den = global_sums_f64(metric, img, bw, bh, stds, nv, thr, pix)
+        nf = np.zeros(W * H, np.float64); df = np.zeros(W * H, np.float64)
+        nf[pix] = num; df[pix] = den
+        out = np.zeros(W * H, np.float64)
+        lib().orc_global_finalize_f64(m, nf, df, W, H, rw, rh, mask.ravel().copy(),
+                                      C.c_float(relevance_constant), C.c_double(float(npx)),
+                                      int(normalize), out)
+    return {"map": out.reshape(H, W), "num": nf.reshape(H, W), "den": df.reshape(H, W),
+            "means": means, "stds": stds, "mask": mask, "threshold": thr, "noise_var": nv,
+            "n_pixels": npx}
+
+
+# --------------------------------------------------------------------------
+# Block (local) repetition map
+# --------------------------------------------------------------------------
+
+def block_map(metric: str, img, ref_pixels, bw: int, bh: int, ref_mean: float, ref_std: float,
+              relevance_constant: float = 0.0, normalize: bool = True, use_refshim: bool = False):
+    """Block repetition map as java/CLUtils.java:995-1010 computes it, FP32."""
+    img = _f32(img)
+    H, W = img.shape
+    means, stds = local_stats(img, bw, bh)
+    ref = _f32(ref_pixels)
+    K = ref.size
+    m = BLOCK_METRICS[metric]
+    out = np.zeros(W * H, np.float32)
+    if use_refshim:
+        R = refshim()
+        if R is None:
+            raise RuntimeError("refshim not built")
+        name = ["kernelGetBlockPearson2D", "kernelGetBlockSsim2D", "kernelGetBlockNrmse2D",
+                "kernelGetBlockAbsDiffStds2D"][m]
+        pix = np.arange(W * H, dtype=np.int32)
+        bufs = {"ref": ref, "img": img, "means": means, "stds": stds, "map": out}
+        args = [C.c_int(K), C.c_int(W), C.c_int(H), C.c_int(bw), C.c_int(bh), C.c_float(0),
+                C.c_float(0), C.c_float(EPSILON), C.c_float(ref_std), C.c_float(ref_mean),
+                pix.ctypes.data_as(C.c_void_p), C.c_int(pix.size)]
+        kind_args = {0: ["ref", "img", "means", "stds", "map"], 1: ["ref", "img", "means", "stds", "map"],
+                     2: ["ref", "img", "means", "map"], 3: ["stds", "map"]}[m]
+        args += [bufs[a].ctypes.data_as(C.c_void_p) for a in kind_args]
+        if getattr(R, f"rs_{name}")(*args) != 0:
+            raise ValueError(f"refshim has no instantiation for K={K}")
+    else:
+        lib().orc_block_kernel_f32(m, img, W, H, bw, bh, means, stds, ref, K, C.c_float(ref_mean),
+                                   C.c_float(ref_std), out)
+    raw = out.copy()
+    rc = lib().orc_block_postprocess_f32(m, out, img, W, H, bw // 2, bh // 2, stds,
+                                         C.c_float(relevance_constant), int(normalize))
+    if rc != 0:
+        raise IndexError("image smaller than one noise tile")
+    return {"map": out.reshape(H, W), "raw": raw.reshape(H, W), "means": means, "stds": stds}
+
+
+def block_raw_f64(metric: int, img, ref_pixels, bw, bh, ref_mean, ref_std, stds32):
+    """FP64 judge of the block-map kernel output (before host post-processing).
+    ``metric`` is 0..3 as BLOCK_METRICS, or COSINE."""
+    img = _f32(img)
+    H, W = img.shape
+    out = np.zeros(W * H, np.float64)
+    ref = _f32(ref_pixels)
+    lib().orc_block_kernel_f64(metric, img, W, H, bw, bh, _f32(stds32), ref, ref.size,
+                               C.c_float(ref_mean), C.c_float(ref_std), out)
+    return out.reshape(H, W)

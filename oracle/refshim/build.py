@@ -1,0 +1,180 @@
+"""Build recipe for the oracle: the C restatement and the reference's own kernels.
+
+TEST INFRASTRUCTURE ONLY.
+
+1. ``oracle/liboracle.so`` from ``oracle/sred_oracle.c`` (committed source).
+2. ``oracle/_ref/librefshim.so``: the reference's OpenCL C kernels, read from a
+   SReD checkout (default ``/root/reference``), with their ``$PLACEHOLDER$``
+   tokens substituted the way the reference's host code substitutes them
+   (``java/CLUtils.java:325-339``, first occurrence only) and compiled as C++
+   against ``oracle/refshim/shim.h``. The substituted kernel text is written
+   only under ``oracle/_ref/`` (git-ignored); nothing of the reference's source
+   is committed. Step 2 is skipped when the checkout is absent.
+
+Usage: ``python oracle/refshim/build.py [--reference PATH] [--force]``
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import hashlib
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE = HERE.parent
+REF_OUT = ORACLE / "_ref"
+CFLAGS = ["-O2", "-fPIC", "-fopenmp", "-ffp-contract=off", "-fno-fast-math"]
+
+# Kernels the hot path uses (cl/ = src/main/resources/), with the argument
+# lists of their entry points: g = global-map kernel, b = block-map kernel,
+# s = local statistics.
+KERNELS = {
+    "kernelGetLocalStatistics2D": ("s", ["img", "means", "stds"]),
+    "kernelGetGlobalPearson2D": ("g", ["img", "means", "stds", "den", "num"]),
+    "kernelGetGlobalSsim2D": ("g", ["img", "means", "stds", "den", "num"]),
+    "kernelGetGlobalNrmse2D": ("g", ["img", "means", "stds", "den", "num"]),
+    "kernelGetGlobalAbsDiffStds2D": ("g", ["img", "stds", "den", "num"]),
+    "kernelGetBlockPearson2D": ("b", ["ref", "img", "means", "stds", "map"]),
+    "kernelGetBlockSsim2D": ("b", ["ref", "img", "means", "stds", "map"]),
+    "kernelGetBlockNrmse2D": ("b", ["ref", "img", "means", "map"]),
+    "kernelGetBlockAbsDiffStds2D": ("b", ["stds", "map"]),
+}
+
+PLACEHOLDERS = {
+    "$WIDTH$": "RS_W", "$HEIGHT$": "RS_H", "$BLOCK_SIZE$": "RS_KT",
+    "$BW$": "RS_BW", "$BH$": "RS_BH", "$BRW$": "RS_BRW", "$BRH$": "RS_BRH",
+    "$FILTER_PARAM$": "RS_FILTER", "$THRESHOLD$": "RS_THRESHOLD",
+    "$EPSILON$": "RS_EPSILON", "$BLOCK_STD$": "RS_BLOCK_STD",
+    "$BLOCK_MEAN$": "RS_BLOCK_MEAN",
+}
+MACROS = ["image_width", "image_height", "block_size", "bW", "bH", "bRW", "bRH",
+          "filter_param", "threshold", "EPSILON", "w", "h", "ref_std", "ref_mean", "kernel"]
+
+MAX_BLOCK = 15  # every odd block width/height 3..15 is instantiated
+
+
+def ellipse_k(bw: int, bh: int) -> int:
+    f = np.float32
+    rw, rh = bw // 2, bh // 2
+    k = 0
+    for y in range(bh):
+        for x in range(bw):
+            dx, dy = f(x - rw), f(y - rh)
+            if (dx * dx) / f(rw * rw) + (dy * dy) / f(rh * rh) <= f(1):
+                k += 1
+    return k
+
+
+def k_list() -> list[int]:
+    return sorted({ellipse_k(a, b) for a in range(3, MAX_BLOCK + 1, 2)
+                   for b in range(3, MAX_BLOCK + 1, 2)})
+
+
+def replace_first(src: str, target: str, repl: str) -> str:
+    i = src.find(target)
+    return src if i < 0 else src[:i] + repl + src[i + len(target):]
+
+
+def entry_code(name: str, kind: str, args: list[str], ks: list[int]) -> str:
+    call = ", ".join(f"(float*){a}" for a in args)
+    cases = "\n".join(f"    case {k}: rs_loop<{k}>(pix, npix, {', '.join(args)}); break;" for k in ks)
+    params = ", ".join(f"const float* {a}" if a in ("img", "means", "stds", "ref") else f"float* {a}"
+                       for a in args)
+    return f"""
+{''.join(f'#undef {m}' + chr(10) for m in MACROS)}
+template <int KT>
+static void rs_loop(const int* pix, int npix, {params}) {{
+  #pragma omp parallel for schedule(dynamic, 1)
+  for (int i = 0; i < npix; i++) {{
+    rs_gid[0] = pix[i] % RS_W;
+    rs_gid[1] = pix[i] / RS_W;
+    {name}<KT>({call});
+  }}
+}}
+
+extern "C" int rs_{name}(int K, int W, int H, int bw, int bh, float filter, float threshold,
+                       float eps, float block_std, float block_mean, const int* pix, int npix,
+                       {params}) {{
+  RS_W = W; RS_H = H; RS_BW = bw; RS_BH = bh; RS_BRW = bw / 2; RS_BRH = bh / 2;
+  RS_FILTER = filter; RS_THRESHOLD = threshold; RS_EPSILON = eps;
+  RS_BLOCK_STD = block_std; RS_BLOCK_MEAN = block_mean;
+  switch (K) {{
+{cases}
+    default: return -1;
+  }}
+  return 0;
+}}
+"""
+
+
+def gen_unit(ref: Path, name: str, ks: list[int]) -> str:
+    kind, args = KERNELS[name]
+    src = (ref / "src/main/resources" / f"{name}.cl").read_text()
+    for tok, repl in PLACEHOLDERS.items():
+        src = replace_first(src, tok, repl)
+    head = ('#include "shim.h"\n'
+            "#define kernel template <int RS_KT> static inline\n")
+    return head + src + "\n" + entry_code(name, kind, args, ks)
+
+
+def run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+
+
+def build_oracle(force: bool = False) -> Path:
+    out = ORACLE / "liboracle.so"
+    src = ORACLE / "sred_oracle.c"
+    if force or not out.exists() or out.stat().st_mtime < src.stat().st_mtime:
+        run(["gcc", *CFLAGS, "-shared", str(src), "-o", str(out), "-lm"])
+    return out
+
+
+def build_refshim(ref: Path, force: bool = False) -> Path | None:
+    if not (ref / "src/main/resources/kernelGetGlobalPearson2D.cl").exists():
+        return None
+    out = REF_OUT / "librefshim.so"
+    ks = k_list()
+    units = {n: gen_unit(ref, n, ks) for n in KERNELS}
+    digest = hashlib.sha256(("".join(units.values()) + (HERE / "shim.h").read_text()).encode()).hexdigest()
+    stamp = REF_OUT / "build.sha256"
+    if not force and out.exists() and stamp.exists() and stamp.read_text() == digest:
+        return out
+    gen = REF_OUT / "gen"
+    gen.mkdir(parents=True, exist_ok=True)
+    objs = []
+    jobs = []
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        for n, text in units.items():
+            cpp = gen / f"{n}.cpp"
+            cpp.write_text(text)
+            obj = gen / f"{n}.o"
+            objs.append(str(obj))
+            jobs.append(ex.submit(run, ["g++", "-std=c++17", *CFLAGS, "-w", f"-I{HERE}", "-c",
+                                        str(cpp), "-o", str(obj)]))
+        for j in jobs:
+            j.result()
+    run(["g++", "-shared", "-fopenmp", *objs, "-o", str(out)])
+    stamp.write_text(digest)
+    return out
+
+
+def main(argv: list[str] | None = None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("SRED_REFERENCE", "/root/reference"))
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args(argv)
+    print("oracle:", build_oracle(a.force))
+    r = build_refshim(Path(a.reference), a.force)
+    print("refshim:", r if r else "skipped (no reference checkout)")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

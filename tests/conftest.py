@@ -1,0 +1,24 @@
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+
+
+@pytest.fixture(scope="session")
+def junit():
+    import json
+    return json.loads((ROOT / "tests" / "golden" / "reference_junit.json").read_text())
+
+
+@pytest.fixture(scope="session")
+def refshim_fx():
+    import numpy as np
+    return dict(np.load(ROOT / "tests" / "golden" / "global_refshim.npz"))

@@ -1,0 +1,193 @@
+"""Regenerate the golden fixtures in this folder.
+
+Two kinds of fixtures are written:
+
+1. ``reference_junit.json``: the known-answer vectors of the reference's own
+   JUnit tests, read as text from a SReD checkout
+   (``src/test/java/CLUtilsTest.java`` and ``src/test/java/UtilsTest.java``):
+   inputs, parameters and expected outputs of the local-statistics,
+   block-map, relevance-mask, normalisation and mask tests.
+
+2. ``global_refshim.npz``: outputs of the reference's own global-map and
+   block-map kernels (compiled for the CPU by ``oracle/refshim/build.py``) on
+   small seeded synthetic images, with the Java host steps applied by the
+   oracle. No reference test pins the global map; these frozen outputs do.
+
+Usage: ``python tests/golden/make_golden.py [--reference /root/reference]``
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import re
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parent.parent))
+
+import oracle  # noqa: E402
+from sred_b200 import synth  # noqa: E402
+
+FLOAT = r"[-+]?\d+(?:\.\d*)?(?:[eE][-+]?\d+)?f?"
+
+
+def _method(src: str, name: str) -> str:
+    i = src.index(f"void {name}(")
+    depth, j, started = 0, src.index("{", i), False
+    for k in range(j, len(src)):
+        if src[k] == "{":
+            depth += 1
+            started = True
+        elif src[k] == "}":
+            depth -= 1
+            if started and depth == 0:
+                return src[j:k + 1]
+    raise ValueError(name)
+
+
+def _array(body: str, var: str) -> list[float]:
+    m = re.search(r"\b" + re.escape(var) + r"\s*=\s*(?:new\s+float\s*\[\s*\]\s*)?\{([^}]*)\}", body)
+    if not m:
+        raise ValueError(var)
+    return [float(t.rstrip("f")) for t in re.findall(FLOAT, m.group(1))]
+
+
+def _scalar(body: str, pattern: str) -> float:
+    m = re.search(pattern, body)
+    if not m:
+        raise ValueError(pattern)
+    return float(m.group(1).rstrip("f"))
+
+
+def junit_vectors(ref: Path) -> dict:
+    cl = (ref / "src/test/java/CLUtilsTest.java").read_text()
+    ut = (ref / "src/test/java/UtilsTest.java").read_text()
+    out: dict = {"source": "SReD src/test/java (JUnit 5)"}
+
+    b = _method(cl, "testGetLocalStatistics2D")
+    out["local_statistics_2d"] = {
+        "cite": "src/test/java/CLUtilsTest.java testGetLocalStatistics2D",
+        "width": 5, "height": 5, "block_width": 3, "block_height": 3,
+        "image": _array(b, "inputImageData"),
+        "expected_means": _array(b, "expectedLocalMeans"),
+        "expected_stds": _array(b, "expectedLocalStds"),
+        "tolerance": 1e-7,
+    }
+    tol = {"testGetBlockPearson2D": 1e-6, "testGetBlockSsim2D": 1e-7,
+           "testGetBlockNrmse2D": 1e-5, "testGetBlockAbsDiffStds2D": 1e-7}
+    metric = {"testGetBlockPearson2D": "Pearson's R", "testGetBlockSsim2D": "SSIM",
+              "testGetBlockNrmse2D": "NRMSE (inverted)",
+              "testGetBlockAbsDiffStds2D": "Abs. Diff. of StdDevs."}
+    out["block_maps_2d"] = []
+    for name in tol:
+        b = _method(cl, name)
+        out["block_maps_2d"].append({
+            "cite": f"src/test/java/CLUtilsTest.java {name}",
+            "metric": metric[name], "width": 10, "height": 10, "block_width": 3,
+            "block_height": 3, "relevance_constant": 0.0, "normalize": True,
+            "image": _array(b, "imageArray"), "block": _array(b, "block"),
+            "expected": _array(b, "expectedResult"), "tolerance": tol[name],
+        })
+    b = _method(ut, "GetRelevanceMaskTest")
+    out["relevance_mask"] = {
+        "cite": "src/test/java/UtilsTest.java GetRelevanceMaskTest",
+        "width": 50, "height": 50, "java_random_seed": 42,
+        "block_radius_width": 2, "block_radius_height": 2,
+        "relevance_constant": _scalar(b, r"float relevanceConstant\s*=\s*(" + FLOAT + ")"),
+        "expected_threshold": _scalar(b, r"assertEquals\((" + FLOAT + r"),\s*relevanceMask\.getRelevanceThreshold"),
+        "expected_noise_var": _scalar(b, r"assertEquals\((" + FLOAT + r"),\s*relevanceMask\.getNoiseMeanVariance"),
+    }
+    b = _method(ut, "testNormalizeImageWithBinaryMask")
+    out["normalize_image_2d"] = {
+        "cite": "src/test/java/UtilsTest.java testNormalizeImageWithBinaryMask",
+        "width": 4, "height": 4, "border_width": 1, "border_height": 1,
+        "image": _array(b, "imageArray"), "mask": _array(b, "mask"),
+        "expected": _array(b, "expectedArray"), "tolerance": 1e-4,
+    }
+    b = _method(ut, "testNormalizeImageWithInvalidMask")
+    out["normalize_image_2d_invalid"] = {
+        "cite": "src/test/java/UtilsTest.java testNormalizeImageWithInvalidMask",
+        "width": 4, "height": 4, "image": _array(b, "imageArray"), "mask": _array(b, "invalidMask"),
+    }
+    b = _method(ut, "testApplyMask2D")
+    out["apply_mask_2d"] = {
+        "cite": "src/test/java/UtilsTest.java testApplyMask2D",
+        "image": _array(b, "imageArray"), "mask": _array(b, "mask"),
+        "expected": _array(b, "expectedResult"),
+    }
+    return out
+
+
+GLOBAL_CASES = [
+    # (name, W, H, lattice, seed, bw, bh, relevance constants)
+    ("spots48x40_3x3", 48, 40, 4, 11, 3, 3, (0.0, 1.0)),
+    ("spots40x44_5x5", 40, 44, 4, 12, 5, 5, (0.0, 1.0)),
+    ("spots52x36_5x3", 52, 36, 5, 13, 5, 3, (0.0, 2.0)),
+    ("spots36x36_9x9", 36, 36, 3, 14, 9, 9, (0.0,)),
+]
+
+
+def flat_image() -> np.ndarray:
+    """Image with exactly flat regions (exercises the sigma == 0 special cases)."""
+    img = np.zeros((32, 40), np.float32)
+    img[8:20, 10:30] = 0.5
+    img[22:28, 4:12] = 1.0
+    rng = np.random.default_rng(5)
+    img[0:6, :] = rng.uniform(0, 1, (6, 40)).astype(np.float32)
+    return img
+
+
+def refshim_fixtures() -> dict:
+    if oracle.refshim() is None:
+        raise SystemExit("refshim not built; run oracle/refshim/build.py with a reference checkout")
+    fx: dict = {}
+    images = {name: synth.normalize_input(synth.spot_image(W, H, lat, seed=seed))
+              for name, W, H, lat, seed, *_ in GLOBAL_CASES}
+    images["flat32x40_3x3"] = flat_image()
+    cases = [(n, bw, bh, cs) for n, _, _, _, _, bw, bh, cs in GLOBAL_CASES]
+    cases.append(("flat32x40_3x3", 3, 3, (0.0,)))
+    for name, bw, bh, cs in cases:
+        img = images[name]
+        fx[f"{name}/image"] = img
+        for c in cs:
+            for metric in oracle.GLOBAL_METRICS:
+                r = oracle.global_map(metric, img, bw, bh, c, normalize=True, use_refshim=True)
+                tag = f"{name}/c{c:g}/{metric}"
+                fx[f"{tag}/num"] = r["num"]
+                fx[f"{tag}/den"] = r["den"]
+                fx[f"{tag}/map"] = r["map"]
+            fx[f"{name}/c{c:g}/threshold"] = np.float32(r["threshold"])
+            fx[f"{name}/c{c:g}/noise_var"] = np.float32(r["noise_var"])
+        # block map against a block cut from the image itself
+        K = oracle.block_size(bw, bh)
+        y0, x0 = img.shape[0] // 2 - bh // 2, img.shape[1] // 3 - bw // 2
+        px, bm, bs = oracle.reference_block(img[y0:y0 + bh, x0:x0 + bw])
+        assert px.size == K
+        fx[f"{name}/block/pixels"] = px
+        fx[f"{name}/block/mean_std"] = np.array([bm, bs], np.float32)
+        for metric in oracle.BLOCK_METRICS:
+            for c in (0.0, 1.0):
+                r = oracle.block_map(metric, img, px, bw, bh, bm, bs, c, True, use_refshim=True)
+                fx[f"{name}/block/c{c:g}/{metric}/raw"] = r["raw"]
+                fx[f"{name}/block/c{c:g}/{metric}/map"] = r["map"]
+    return fx
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    a = ap.parse_args(argv)
+    ref = Path(a.reference)
+    vec = junit_vectors(ref)
+    (HERE / "reference_junit.json").write_text(json.dumps(vec, indent=1))
+    fx = refshim_fixtures()
+    np.savez_compressed(HERE / "global_refshim.npz", **fx)
+    print("wrote", HERE / "reference_junit.json", "and", HERE / "global_refshim.npz", len(fx), "arrays")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,158 @@
+"""Pin the CPU oracle before trusting it.
+
+The FP32 restatement must reproduce (a) the reference's JUnit known-answer
+vectors and (b) the reference's own kernels compiled for the CPU (frozen in
+tests/golden/global_refshim.npz, and live when oracle/_ref is built), bit for
+bit. The FP64 judge must agree with the FP32 path to FP32 accuracy.
+"""
+import numpy as np
+import pytest
+
+import oracle
+
+
+def _ref_block_as_junit(block, bw, bh):
+    """ReferenceBlock2D as the JUnit tests build it: raw ellipse pixels, FP32
+    mean and (K-1) standard deviation (src/test/java/CLUtilsTest.java:560-600)."""
+    f = np.float32
+    rw, rh = bw // 2, bh // 2
+    px = []
+    for y in range(bh):
+        for x in range(bw):
+            dx, dy = f(x - rw), f(y - rh)
+            if (dx * dx) / f(rw * rw) + (dy * dy) / f(rh * rh) <= f(1):
+                px.append(f(block[y * bw + x]))
+    px = np.array(px, np.float32)
+    mean = f(0)
+    for v in px:
+        mean = f(mean + v)
+    mean = f(mean / f(px.size))
+    sd = f(0)
+    for v in px:
+        sd = f(sd + f(f(v - mean) * f(v - mean)))
+    sd = f(sd / f(f(px.size) - f(1)))
+    sd = f(np.sqrt(np.float64(sd)))
+    return px, mean, sd
+
+
+def test_block_size_ellipse():
+    assert [oracle.block_size(b, b) for b in (3, 5, 7, 9, 11, 13, 15)] == [5, 13, 29, 49, 81, 113, 149]
+
+
+def test_local_statistics_golden(junit):
+    g = junit["local_statistics_2d"]
+    img = np.array(g["image"], np.float32).reshape(g["height"], g["width"])
+    m, s = oracle.local_stats(img, g["block_width"], g["block_height"])
+    np.testing.assert_allclose(m.ravel(), g["expected_means"], atol=g["tolerance"], rtol=0)
+    np.testing.assert_allclose(s.ravel(), g["expected_stds"], atol=g["tolerance"], rtol=0)
+
+
+@pytest.mark.parametrize("idx", range(4))
+@pytest.mark.parametrize("shim", [False, True])
+def test_block_map_golden(junit, idx, shim):
+    g = junit["block_maps_2d"][idx]
+    if shim and oracle.refshim() is None:
+        pytest.skip("refshim not built")
+    img = np.array(g["image"], np.float32).reshape(g["height"], g["width"])
+    px, mean, sd = _ref_block_as_junit(g["block"], g["block_width"], g["block_height"])
+    r = oracle.block_map(g["metric"], img, px, g["block_width"], g["block_height"], mean, sd,
+                         g["relevance_constant"], g["normalize"], use_refshim=shim)
+    out = r["map"].ravel()
+    assert np.all((out >= 0) & (out <= 1))
+    np.testing.assert_allclose(out, g["expected"], atol=g["tolerance"], rtol=0)
+
+
+def test_relevance_mask_golden(junit):
+    g = junit["relevance_mask"]
+    W, H = g["width"], g["height"]
+    # Rebuild the test's inputs: java.util.Random(42), draws interleaved per pixel.
+    stream = oracle.java_random_floats(g["java_random_seed"], 2 * W * H)
+    img = np.zeros(W * H, np.float32)
+    stds = np.zeros(W * H, np.float32)
+    k = 0
+    for i in range(W * H):
+        if i % 50 == 0:
+            img[i], stds[i] = 1.0, 0.0
+        else:
+            img[i] = np.float32(1.0) + stream[k] * np.float32(2.0)
+            stds[i] = stream[k + 1]
+            k += 2
+    img, stds = img.reshape(H, W), stds.reshape(H, W)
+    bw, bh = 2 * g["block_radius_width"] + 1, 2 * g["block_radius_height"] + 1
+    mask, thr, nv = oracle.relevance_mask(img, bw, bh, stds, g["relevance_constant"])
+    assert thr == np.float32(g["expected_threshold"])
+    assert float(nv) == g["expected_noise_var"]
+    assert set(np.unique(mask)) <= {0.0, 1.0}
+
+
+def test_normalize_golden(junit):
+    g = junit["normalize_image_2d"]
+    img = np.array(g["image"], np.float32).reshape(4, 4)
+    mask = np.array(g["mask"], np.float32).reshape(4, 4)
+    out = oracle.normalize_image(img, g["border_width"], g["border_height"], mask)
+    np.testing.assert_allclose(out.ravel(), g["expected"], atol=g["tolerance"])
+    g = junit["normalize_image_2d_invalid"]
+    with pytest.raises(ValueError):
+        oracle.normalize_image(np.array(g["image"], np.float32).reshape(4, 4), 0, 0,
+                               np.array(g["mask"], np.float32).reshape(4, 4))
+
+
+def _fixture_cases(fx):
+    names = sorted({k.split("/")[0] for k in fx})
+    for n in names:
+        bw, bh = (int(v) for v in n.rsplit("_", 1)[1].split("x"))
+        cs = sorted({k.split("/")[1] for k in fx if k.startswith(n + "/c")})
+        for c in cs:
+            yield n, bw, bh, float(c[1:])
+
+
+def test_global_f32_matches_refshim_fixtures(refshim_fx):
+    """Oracle port == the reference's own kernels (frozen), bit for bit."""
+    fx = refshim_fx
+    n_cases = 0
+    for name, bw, bh, c in _fixture_cases(fx):
+        img = fx[f"{name}/image"]
+        for metric in oracle.GLOBAL_METRICS:
+            r = oracle.global_map(metric, img, bw, bh, c, normalize=True)
+            tag = f"{name}/c{c:g}/{metric}"
+            assert np.array_equal(r["num"], fx[f"{tag}/num"]), tag
+            assert np.array_equal(r["den"], fx[f"{tag}/den"]), tag
+            assert np.array_equal(r["map"], fx[f"{tag}/map"], equal_nan=True), tag
+            n_cases += 1
+    assert n_cases >= 30
+
+
+def test_block_f32_matches_refshim_fixtures(refshim_fx):
+    fx = refshim_fx
+    for name in sorted({k.split("/")[0] for k in fx}):
+        bw, bh = (int(v) for v in name.rsplit("_", 1)[1].split("x"))
+        img = fx[f"{name}/image"]
+        px = fx[f"{name}/block/pixels"]
+        bm, bs = fx[f"{name}/block/mean_std"]
+        for metric in oracle.BLOCK_METRICS:
+            for c in (0.0, 1.0):
+                r = oracle.block_map(metric, img, px, bw, bh, bm, bs, c, True)
+                tag = f"{name}/block/c{c:g}/{metric}"
+                assert np.array_equal(r["raw"], fx[f"{tag}/raw"]), tag
+                assert np.array_equal(r["map"], fx[f"{tag}/map"]), tag
+
+
+@pytest.mark.skipif(oracle.refshim() is None, reason="refshim not built")
+@pytest.mark.parametrize("metric", list(oracle.GLOBAL_METRICS))
+def test_global_f32_matches_refshim_live(metric):
+    from sred_b200 import synth
+    img = synth.normalize_input(synth.spot_image(46, 38, 4, seed=99))
+    for bw, bh in ((3, 5), (7, 7)):
+        a = oracle.global_map(metric, img, bw, bh, 1.0)
+        b = oracle.global_map(metric, img, bw, bh, 1.0, use_refshim=True)
+        assert np.array_equal(a["num"], b["num"]) and np.array_equal(a["den"], b["den"])
+        assert np.array_equal(a["map"], b["map"])
+
+
+@pytest.mark.parametrize("metric", list(oracle.GLOBAL_METRICS))
+def test_f64_judge_close_to_f32(refshim_fx, metric):
+    img = refshim_fx["spots40x44_5x5/image"]
+    a = oracle.global_map(metric, img, 5, 5, 1.0, precision="f32")
+    b = oracle.global_map(metric, img, 5, 5, 1.0, precision="f64")
+    m = a["mask"] > 0
+    np.testing.assert_allclose(a["map"][m], b["map"][m], atol=2e-5, rtol=0)
