@@ -1,0 +1,350 @@
+"""Benchmark of the global repetition map (SReD's block-correlation hot path).
+
+Workload: global repetition map of a 1024x1024 float32 synthetic spot image
+(80x80 jittered lattice plus 30% random spots, Poisson + Gaussian noise,
+seed 0), 9x9 block (ellipse K = 49), Pearson's R, relevance constant 1.0.
+
+A step is one complete map: moments, relevance mask, compaction, the
+all-pairs contraction with its fused epilogue, finalisation and
+normalisation. ``value`` is block-pairs/s with the image resident in HBM
+(pairs = relevant blocks squared, the pairs the map is defined over); ``e2e``
+is the same through the C ABI with host buffers (H2D of the image and D2H of
+the map inside the timed region). L2 is flushed (256 MiB write) between
+steps, outside the timed region.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs an independent replica (the map of its own
+image); value = total pairs of all ranks / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "global-map block-pairs/s at 1024²/9×9; split-BF16 vs FP32 speedup @≤1e-5 err"
+W_IMG = H_IMG = 1024
+BW = BH = 9
+SIM = "Pearson's R"
+RELC = 1.0
+WORKLOAD = ("global repetition map, 1024x1024 float32 spot image (80x80 lattice + 30% random spots), "
+            "9x9 block (ellipse K=49), Pearson's R, relevance constant 1.0")
+
+
+def peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"],
+                "bf16_tflops_sustained": d["bf16_tflops_sustained"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "fallback"}
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p:
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                self.out, _ = self.p.communicate()
+
+    def summary(self) -> dict:
+        rows = [r.split(", ") for r in (self.out or "").strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return rank, local, world
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def image(seed: int) -> np.ndarray:
+    from sred_b200 import synth
+    return synth.normalize_input(synth.image_1024_spots_random(seed=seed))
+
+
+def time_engine(ctx, engine, d_img, d_out, flush, steps, warmup, stream):
+    """Device-resident steps; returns (per-step ms list, last run info, launches)."""
+    import torch
+    from sred_b200 import clutils
+    ctx.set_engine(engine)
+    for _ in range(warmup):
+        clutils.global_map_device(SIM, d_img.data_ptr(), W_IMG, H_IMG, BW, BH, RELC, True, d_out.data_ptr(),
+                                  stream.cuda_stream, ctx=ctx)
+    ms, gram_ms, launches, info = [], [], 0, None
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        info = clutils.global_map_device(SIM, d_img.data_ptr(), W_IMG, H_IMG, BW, BH, RELC, True,
+                                         d_out.data_ptr(), stream.cuda_stream, ctx=ctx)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        gram_ms.append(info["ms_gram"])
+        launches += info["launches"]
+    return ms, gram_ms, info, launches
+
+
+def cpu_baseline(img: np.ndarray, gpu_map: np.ndarray | None, budget_s: float = 12.0) -> dict:
+    """The reference's own kernel (oracle/_ref, compiled for the CPU) on a
+    bounded sample of reference pixels against all test blocks, on all host
+    cores; falls back to the oracle's FP32 port if _ref was not built."""
+    import oracle
+    kind = "reference" if oracle.refshim() is not None else "port"
+    means, stds = oracle.local_stats(img, BW, BH)
+    mask, thr, nv = oracle.relevance_mask(img, BW, BH, stds, RELC)
+    H, W = img.shape
+    rel = np.flatnonzero((stds.ravel() * stds.ravel() >= thr) & (np.arange(W * H) % W >= BW // 2) &
+                         (np.arange(W * H) % W < W - BW // 2) & (np.arange(W * H) // W >= BH // 2) &
+                         (np.arange(W * H) // W < H - BH // 2))
+    n_rel = rel.size
+    rng = np.random.default_rng(123)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    rows = rng.choice(rel, size=min(n_rel, 2 * cores), replace=False).astype(np.int32)
+    t0 = time.perf_counter()
+    oracle.global_sums_f32(SIM, img, BW, BH, means, stds, nv, thr, rows, use_refshim=(kind == "reference"))
+    t_probe = time.perf_counter() - t0
+    n_rows = int(max(cores, min(n_rel, budget_s / max(t_probe, 1e-6) * rows.size)))
+    rows = rng.choice(rel, size=n_rows, replace=False).astype(np.int32)
+    t0 = time.perf_counter()
+    num, den = oracle.global_sums_f32(SIM, img, BW, BH, means, stds, nv, thr, rows,
+                                      use_refshim=(kind == "reference"))
+    dt = time.perf_counter() - t0
+    pairs = float(rows.size) * n_rel
+    res = {"value": pairs / dt, "unit": "block-pairs/s", "cores": cores, "kind": kind,
+           "sample": f"{rows.size} relevant reference pixels x all {n_rel} relevant test blocks "
+                     f"({pairs:.3g} pairs, {dt:.1f} s); rate extrapolates per pair"}
+    if gpu_map is not None:
+        npx = float(oracle.n_pixels(mask, BW // 2, BH // 2))
+        raw = num / (den * np.float32(npx) + np.float32(1e-7))
+        res["gpu_raw_rel_err_vs_reference_sample"] = None if gpu_map is None else float(
+            np.max(np.abs(gpu_map.ravel()[rows] - raw) / np.maximum(np.abs(raw), 1e-30)))
+    return res
+
+
+def run_ours(args, rank, local, world):
+    import torch
+    from sred_b200 import _lib, clutils
+    torch.cuda.set_device(local)
+    ctx = _lib.Context(local, "tc")
+    stream = torch.cuda.Stream()
+    img = image(seed=rank)
+    d_img = torch.from_numpy(img).cuda()
+    d_out = torch.empty_like(d_img)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    engines = [args.engine] + (["fp32"] if args.engine == "tc" and not args.no_compare else [])
+    results = {}
+    for eng in engines:
+        steps = args.steps if eng == args.engine else max(2, min(args.steps, 3))
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+        with Clocks(local) as clk:
+            ms, gram_ms, info, launches = time_engine(ctx, eng, d_img, d_out, flush, steps, args.warmup, stream)
+        torch.cuda.synchronize()
+        total_ms = max_over_ranks(sum(ms), world)
+        pairs = sum_over_ranks(info["pairs"] * steps, world)
+        results[eng] = {"ms": ms, "gram_ms": gram_ms, "info": info, "launches": launches, "total_ms": total_ms,
+                        "pairs": pairs, "clocks": clk.summary(), "steps": steps}
+
+    # End to end through the C ABI with host buffers (pinned).
+    ctx.set_engine(args.engine)
+    h_img = torch.from_numpy(img).pin_memory()
+    h_out = torch.empty_like(h_img).pin_memory()
+    for _ in range(args.warmup):
+        clutils.global_map_host(SIM, h_img.numpy(), BW, BH, RELC, True, out=h_out.numpy(), ctx=ctx)
+    e2e_s = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, info_e = clutils.global_map_host(SIM, h_img.numpy(), BW, BH, RELC, True, out=h_out.numpy(), ctx=ctx)
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_total = max_over_ranks(sum(e2e_s), world)
+    e2e_pairs = sum_over_ranks(info_e["pairs"] * args.steps, world)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+    if rank != 0:
+        return
+    r = results[args.engine]
+    pk = peaks()
+    K = r["info"]["k"]
+    gram_s = statistics.mean(r["gram_ms"]) / 1e3
+    per_launch_pairs = r["info"]["pairs"]
+    line = {
+        "metric": METRIC,
+        "value": r["pairs"] / (r["total_ms"] / 1e3),
+        "unit": "block-pairs/s",
+        "n_gpus": world,
+        "steps": r["steps"],
+        "warmup": args.warmup,
+        "ms_per_step": r["total_ms"] / r["steps"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "bf16x3 split (hi/lo) tensor-core Gram, f32 accumulate, f64 moments" if args.engine == "tc"
+                 else "f32 CUDA-core Gram, f64 moments",
+        "data": "synthetic (seeded spot image, numpy default_rng; no dataset)",
+        "config": {"workload": WORKLOAD, "image": f"{W_IMG}x{H_IMG}", "block": f"{BW}x{BH}", "K": K,
+                   "metric": SIM, "relevance_constant": RELC, "engine": args.engine,
+                   "relevant_blocks": r["info"]["n_relevant"], "pairs_per_step": per_launch_pairs,
+                   "l2": "flushed between steps (256 MiB write, outside the timed region)",
+                   "parallelism": f"{world} independent replica(s)"},
+        "gpu_launches": r["launches"],
+        "clocks": r["clocks"],
+    }
+    if args.engine == "tc":
+        eff_peak = pk["bf16_tflops_sustained"] / 3.0
+        achieved = per_launch_pairs * 2 * K / gram_s / 1e12
+        line["roofline"] = {
+            "bound": "tensor", "achieved": achieved, "peak": eff_peak, "unit": "TFLOP/s",
+            "frac": achieved / eff_peak, "traffic": traffic_from_profile(),
+            "note": f"all-pairs Gram kernel; algorithmic FLOPs = pairs x 2K (K={K}); peak = {pk['source']} "
+                    f"sustained BF16 / 3 (three hi/lo products per FP32-accurate product)"}
+    if "fp32" in results and args.engine != "fp32":
+        f = results["fp32"]
+        fv = f["pairs"] / (f["total_ms"] / 1e3)
+        line["fp32_engine"] = {"value": fv, "ms_per_step": f["total_ms"] / f["steps"], "steps": f["steps"],
+                               "gram_ms": statistics.mean(f["gram_ms"])}
+        line["speedup_tc_vs_fp32"] = line["value"] / fv
+        line["gram_speedup_tc_vs_fp32"] = statistics.mean(f["gram_ms"]) / (gram_s * 1e3)
+    line["e2e"] = {"value": e2e_pairs / e2e_total, "unit": "block-pairs/s",
+                   "h2d_bytes_per_step": 4 * W_IMG * H_IMG, "d2h_bytes_per_step": 4 * W_IMG * H_IMG,
+                   "ms_per_step": 1e3 * e2e_total / args.steps}
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(img, None)
+    print(json.dumps(line), flush=True)
+
+
+def traffic_from_profile():
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get("gram_tc_bytes_per_launch")
+        except Exception:
+            return None
+    return None
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    img = image(seed=0)
+    vals, secs = [], []
+    base = None
+    for i in range(args.warmup + args.steps):
+        b = cpu_baseline(img, None, budget_s=4.0 if i < args.warmup else 8.0)
+        if i >= args.warmup:
+            vals.append(b["value"])
+            base = b
+    v = statistics.mean(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "block-pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (reference kernels on host cores)",
+            "data": "synthetic (seeded spot image, numpy default_rng; no dataset)",
+            "config": {"workload": WORKLOAD, "image": f"{W_IMG}x{H_IMG}", "block": f"{BW}x{BH}",
+                       "metric": SIM, "relevance_constant": RELC, "engine": "reference CPU kernels"},
+            "cpu_baseline": {"value": v, "unit": "block-pairs/s", "cores": base["cores"], "kind": base["kind"],
+                             "sample": base["sample"]},
+            "e2e": {"value": v, "unit": "block-pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--engine", choices=["tc", "fp32"], default="tc")
+    ap.add_argument("--no-compare", action="store_true", help="skip the FP32-engine comparison")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, rank, int(os.environ.get("WORLD_SIZE", "1")))
+        return
+    rank, local, world = dist_init()
+    try:
+        run_ours(args, rank, local, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,147 @@
+/*
+ * libsred: B200 (sm_100a) implementation of SReD's block-correlation path.
+ *
+ * C ABI only: plain pointers and sizes, no C++ or torch types. Every entry
+ * point returns an sred_status and never aborts the process. Host pointers
+ * ("const float* img", "float* out") are caller-owned host memory; functions
+ * with the _device suffix take device pointers on the given CUDA stream.
+ *
+ * Reference interfaces replaced (paths relative to the SReD repository root):
+ *   java/  = src/main/java/
+ * Metric arguments are the reference's dialog strings, matched exactly.
+ */
+#ifndef SRED_H
+#define SRED_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    SRED_OK = 0,
+    SRED_ERR_ARG = 1,            /* bad size/argument; the reference throws or IJ.error()s */
+    SRED_ERR_UNKNOWN_METRIC = 2, /* the reference returns null (java/CLUtils.java:2193-2195) */
+    SRED_ERR_NODEV = 3,
+    SRED_ERR_OOM = 4,
+    SRED_ERR_LAUNCH = 5,
+    SRED_ERR_TIMEOUT = 6,
+    SRED_ERR_INTERNAL = 7,
+    SRED_ERR_INVALID_INPUT = 8   /* NaN/Inf pixel in a noise tile (java/Utils.java:886-889) */
+} sred_status;
+
+/* Contraction engine of the global map. SRED_ENGINE_TC: split-BF16 (hi/lo)
+ * tcgen05 tensor-core Gram with FP32 accumulation; SRED_ENGINE_FP32: plain
+ * FP32 CUDA-core Gram. Both share moments, tiling and the fused epilogue. */
+typedef enum { SRED_ENGINE_TC = 0, SRED_ENGINE_FP32 = 1 } sred_engine;
+
+typedef struct sred_ctx sred_ctx;
+
+/* Timing and counts of the last global-map call. */
+typedef struct {
+    int64_t n_blocks;          /* interior blocks (W-2rw)*(H-2rh) */
+    int64_t n_relevant;        /* blocks with sigma^2 >= threshold (enter the sums) */
+    int64_t n_flat;            /* relevant blocks with sigma == 0 */
+    double pairs;              /* n_relevant^2: block pairs the map is defined over */
+    float noise_var;           /* FILTER_PARAM (java/Utils.java:790-837) */
+    float threshold;           /* noise_var * relevance constant */
+    float n_pixels;            /* java/GlobalRepetition2D_.java:133-140 */
+    int k;                     /* ellipse block size */
+    int engine;                /* sred_engine used */
+    double ms_moments, ms_gram, ms_finalize, ms_total; /* CUDA-event times */
+    int launches;              /* kernels this call launched */
+} sred_run_info;
+
+/* Context: owns the device, a stream and reusable workspaces.
+ * One context per host thread; calls on one context are serialised. */
+sred_status sred_create(int device_ordinal, sred_ctx **out);
+sred_status sred_destroy(sred_ctx *ctx);
+sred_status sred_set_engine(sred_ctx *ctx, int engine);
+const char *sred_status_string(sred_status s);
+const char *sred_last_error(sred_ctx *ctx);
+
+/* Ellipse block size K for a bw x bh block (java/GlobalRepetition2D_.java:102-111). */
+int sred_block_size(int bw, int bh);
+
+/* Replaces CLUtils.getLocalStatistics2D (java/CLUtils.java:376-467) and
+ * cl/kernelGetLocalStatistics2D.cl: per-pixel ellipse-block mean and (K-1)
+ * standard deviation in FP32, reference evaluation order; border pixels 0. */
+sred_status sred_local_statistics_2d(sred_ctx *ctx, const float *img, int w, int h, int bw, int bh,
+                                     float *local_means, float *local_stds);
+
+/* Replaces Utils.getMeanNoiseVar2D (java/Utils.java:790-837). */
+sred_status sred_mean_noise_var_2d(sred_ctx *ctx, const float *img, int w, int h, float *noise_var);
+
+/* Replaces Utils.getRelevanceMask (java/Utils.java:944-968): mask[w*h] in {0,1},
+ * threshold = noise_var * relevance_constant. */
+sred_status sred_relevance_mask_2d(sred_ctx *ctx, const float *img, int w, int h, int bw, int bh,
+                                   const float *local_stds, float relevance_constant, float *mask,
+                                   float *threshold, float *noise_var);
+
+/* Replaces CLUtils.calculateGlobalRepetitionMap2D (java/CLUtils.java:2174-2196)
+ * and the four getGlobal*2D methods it dispatches to (:1680-2156), with the
+ * same inputs: the preprocessed image, block size, the FP32 local statistics
+ * of CLLocalStatistics (relevance and flat-block decisions are taken on
+ * local_stds, as the reference kernels take them), the RelevanceMask fields
+ * (mask, relevance constant, threshold, noise variance) and nPixels.
+ * metric: "Pearson's R", "SSIM", "NRMSE" or "Abs. diff. of StdDevs".
+ * out receives the finished map (w*h), including the host post-processing. */
+sred_status sred_calculate_global_repetition_map_2d(
+    sred_ctx *ctx, const char *metric, const float *img, int w, int h, int bw, int bh, int block_size,
+    const float *local_means, const float *local_stds, const float *mask, float relevance_constant,
+    float threshold, float noise_var, float n_pixels, int normalize_output, float *out,
+    sred_run_info *info);
+
+/* The whole command after preprocessing, as GlobalRepetition2D_.run does it
+ * (java/GlobalRepetition2D_.java:97-145): K, local statistics, relevance
+ * mask, nPixels and the map, all on the device. */
+sred_status sred_global_map_2d(sred_ctx *ctx, const char *metric, const float *img, int w, int h,
+                               int bw, int bh, float relevance_constant, int normalize_output,
+                               float *out, sred_run_info *info);
+
+/* Same as sred_global_map_2d with device-resident input and output on
+ * `stream` (a cudaStream_t; NULL = the context's stream). The call returns
+ * when the map is complete. */
+sred_status sred_global_map_2d_device(sred_ctx *ctx, const char *metric, const float *d_img, int w,
+                                      int h, int bw, int bh, float relevance_constant,
+                                      int normalize_output, float *d_out, void *stream,
+                                      sred_run_info *info);
+
+/* Replaces CLUtils.calculateBlockRepetitionMap2D (java/CLUtils.java:995-1010)
+ * and getBlock{Pearson,Ssim,Nrmse,AbsDiffStds}2D (:486-981). ref_pixels,
+ * block_size, bw, bh, ref_mean and ref_std are the ReferenceBlock2D fields
+ * (java/Utils.java:108-216), passed through unchanged. metric:
+ * "Pearson's R", "SSIM", "NRMSE (inverted)", "Abs. Diff. of StdDevs." (the
+ * reference's four), or "Cosine" (raw-vector cosine similarity; no reference
+ * counterpart, same post-processing as Pearson). */
+sred_status sred_calculate_block_repetition_map_2d(sred_ctx *ctx, const char *metric, const float *img,
+                                                   int w, int h, const float *ref_pixels, int block_size,
+                                                   int bw, int bh, float ref_mean, float ref_std,
+                                                   float relevance_constant, int normalize_output,
+                                                   float *out);
+
+/* Device-resident variant over a stack of `frames` images (the time-lapse
+ * loop of java/BlockRepetition2D_.java:95-130): d_img is frames*w*h, d_out the
+ * same. */
+sred_status sred_block_map_2d_device(sred_ctx *ctx, const char *metric, const float *d_img, int w,
+                                     int h, int frames, const float *ref_pixels, int block_size, int bw,
+                                     int bh, float ref_mean, float ref_std, float relevance_constant,
+                                     int normalize_output, float *d_out, void *stream);
+
+/* Replaces Utils.getReferenceBlock2D (java/Utils.java:557-639) for a block
+ * image already converted to float: ellipse-flatten, min-max, mean-subtract,
+ * std. pixels must hold sred_block_size(bw, bh) floats. */
+sred_status sred_reference_block_2d(const float *block_img, int bw, int bh, float *pixels,
+                                    int *block_size, float *mean, float *std);
+
+/* Replaces Utils.normalizeImage2D (java/Utils.java:985-1031) on host memory.
+ * mask may be NULL. SRED_ERR_ARG for a non-binary mask. */
+sred_status sred_normalize_image_2d(float *img, int w, int h, int border_w, int border_h,
+                                    const float *mask);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SRED_H */

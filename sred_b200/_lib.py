@@ -1,0 +1,139 @@
+"""ctypes binding of libsred.so (the C ABI declared in include/sred.h).
+
+The library is the only compute path: if it is missing or no CUDA device is
+present, calls raise instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libsred.so"
+
+OK, ERR_ARG, ERR_UNKNOWN_METRIC, ERR_NODEV, ERR_OOM, ERR_LAUNCH, ERR_TIMEOUT, ERR_INTERNAL, ERR_INVALID_INPUT = range(9)
+ENGINE_TC, ENGINE_FP32 = 0, 1
+
+# Every symbol include/sred.h declares.
+EXPORTS = [
+    "sred_create", "sred_destroy", "sred_set_engine", "sred_status_string", "sred_last_error",
+    "sred_block_size", "sred_local_statistics_2d", "sred_mean_noise_var_2d", "sred_relevance_mask_2d",
+    "sred_calculate_global_repetition_map_2d", "sred_global_map_2d", "sred_global_map_2d_device",
+    "sred_calculate_block_repetition_map_2d", "sred_block_map_2d_device", "sred_reference_block_2d",
+    "sred_normalize_image_2d",
+]
+
+
+class RunInfo(C.Structure):
+    _fields_ = [("n_blocks", C.c_int64), ("n_relevant", C.c_int64), ("n_flat", C.c_int64),
+                ("pairs", C.c_double), ("noise_var", C.c_float), ("threshold", C.c_float),
+                ("n_pixels", C.c_float), ("k", C.c_int), ("engine", C.c_int),
+                ("ms_moments", C.c_double), ("ms_gram", C.c_double), ("ms_finalize", C.c_double),
+                ("ms_total", C.c_double), ("launches", C.c_int)]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class SredError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_fp = C.POINTER(C.c_float)
+_vp = C.c_void_p
+_lib = None
+_lock = threading.Lock()
+
+
+def load() -> C.CDLL:
+    """Load libsred.so, declaring every exported signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not LIB_PATH.exists():
+            raise SredError(ERR_INTERNAL, f"{LIB_PATH} is not built; run `python -m sred_b200.build`")
+        L = C.CDLL(str(LIB_PATH))
+        s = C.c_int
+        L.sred_status_string.restype = C.c_char_p
+        L.sred_status_string.argtypes = [s]
+        L.sred_last_error.restype = C.c_char_p
+        L.sred_last_error.argtypes = [_vp]
+        L.sred_create.argtypes = [s, C.POINTER(_vp)]
+        L.sred_destroy.argtypes = [_vp]
+        L.sred_set_engine.argtypes = [_vp, s]
+        L.sred_block_size.argtypes = [s, s]
+        L.sred_local_statistics_2d.argtypes = [_vp, _f32p, s, s, s, s, _f32p, _f32p]
+        L.sred_mean_noise_var_2d.argtypes = [_vp, _f32p, s, s, _fp]
+        L.sred_relevance_mask_2d.argtypes = [_vp, _f32p, s, s, s, s, _f32p, C.c_float, _f32p, _fp, _fp]
+        L.sred_calculate_global_repetition_map_2d.argtypes = [
+            _vp, C.c_char_p, _f32p, s, s, s, s, s, _f32p, _f32p, _f32p, C.c_float, C.c_float, C.c_float,
+            C.c_float, s, _f32p, C.POINTER(RunInfo)]
+        L.sred_global_map_2d.argtypes = [_vp, C.c_char_p, _vp, s, s, s, s, C.c_float, s, _vp,
+                                         C.POINTER(RunInfo)]
+        L.sred_global_map_2d_device.argtypes = [_vp, C.c_char_p, _vp, s, s, s, s, C.c_float, s, _vp, _vp,
+                                                C.POINTER(RunInfo)]
+        L.sred_calculate_block_repetition_map_2d.argtypes = [
+            _vp, C.c_char_p, _f32p, s, s, _f32p, s, s, s, C.c_float, C.c_float, C.c_float, s, _f32p]
+        L.sred_block_map_2d_device.argtypes = [_vp, C.c_char_p, _vp, s, s, s, _f32p, s, s, s, C.c_float,
+                                               C.c_float, C.c_float, s, _vp, _vp]
+        L.sred_reference_block_2d.argtypes = [_f32p, s, s, _f32p, C.POINTER(C.c_int), _fp, _fp]
+        L.sred_normalize_image_2d.argtypes = [_f32p, s, s, s, s, _vp]
+        _lib = L
+    return _lib
+
+
+def status_string(st: int) -> str:
+    return load().sred_status_string(st).decode()
+
+
+class Context:
+    """Owns a libsred context (device, stream, workspaces)."""
+
+    def __init__(self, device: int = 0, engine: str = "fp32"):
+        self._L = load()
+        h = _vp()
+        st = self._L.sred_create(device, C.byref(h))
+        if st != OK:
+            raise SredError(st, f"sred_create({device}): {status_string(st)}")
+        self.h = h
+        self.set_engine(engine)
+
+    def set_engine(self, engine: str) -> None:
+        e = {"tc": ENGINE_TC, "fp32": ENGINE_FP32}[engine]
+        self.check(self._L.sred_set_engine(self.h, e), "sred_set_engine")
+        self.engine = engine
+
+    def check(self, st: int, what: str) -> None:
+        if st != OK:
+            msg = self._L.sred_last_error(self.h).decode() if self.h else ""
+            raise SredError(st, f"{what}: {status_string(st)} ({msg})")
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self._L.sred_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default: Context | None = None
+
+
+def default_context() -> Context:
+    global _default
+    if _default is None:
+        _default = Context(0)
+    return _default

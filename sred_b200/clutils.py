@@ -1,0 +1,173 @@
+"""Host-side mirror of the reference's ``CLUtils`` (java/CLUtils.java), 2D parts.
+
+The OpenCL orchestration of the reference is replaced by libsred (CUDA,
+sm_100a); the method names, arguments and results stay. ``OpenCLResources``
+becomes a libsred ``Context``; ``CLLocalStatistics`` holds the FP32 local
+means and stds.
+
+Errors follow the reference: an unknown metric returns None
+(java/CLUtils.java:2193-2195, :1007-1009); bad arguments raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .utils import InputImage2D, ReferenceBlock2D, RelevanceMask
+
+GLOBAL_METRICS = ["Pearson's R", "SSIM", "NRMSE", "Abs. diff. of StdDevs"]  # java/GlobalRepetition2D_.java:20-25
+BLOCK_METRICS = ["Pearson's R", "SSIM", "NRMSE (inverted)", "Abs. Diff. of StdDevs."]  # java/BlockRepetition2D_.java:18-23
+COSINE = "Cosine"  # raw-vector cosine similarity; no reference counterpart
+
+
+@dataclass
+class CLLocalStatistics:
+    """java/CLUtils.java:84-158 (the device buffers live in libsred)."""
+    local_means: np.ndarray
+    local_stds: np.ndarray
+
+
+def get_open_cl_resources(use_device: bool = False, device: int = 0, engine: str = "tc") -> _lib.Context:
+    """java/CLUtils.java:169-238 counterpart: a libsred context on a CUDA device."""
+    return _lib.Context(device, engine)
+
+
+def _ctx(ctx):
+    return ctx if ctx is not None else _lib.default_context()
+
+
+def get_local_statistics_2d(input_image: InputImage2D, block_width: int, block_height: int,
+                            ctx=None) -> CLLocalStatistics:
+    """java/CLUtils.java:376-467."""
+    c = _ctx(ctx)
+    n = input_image.size
+    m = np.zeros(n, np.float32)
+    s = np.zeros(n, np.float32)
+    c.check(c._L.sred_local_statistics_2d(c.h, np.ascontiguousarray(input_image.image_array, np.float32).ravel(),
+                                          input_image.width, input_image.height, block_width, block_height, m, s),
+            "sred_local_statistics_2d")
+    return CLLocalStatistics(m, s)
+
+
+def calculate_global_repetition_map_2d(metric: str, input_image: InputImage2D, block_width: int,
+                                       block_height: int, block_size: int, local_statistics: CLLocalStatistics,
+                                       relevance_mask: RelevanceMask, n_pixels: float, normalize_output: bool,
+                                       ctx=None, run_info: dict | None = None):
+    """java/CLUtils.java:2174-2196: dispatch on the metric string to the global map."""
+    if metric not in GLOBAL_METRICS:
+        return None
+    c = _ctx(ctx)
+    n = input_image.size
+    out = np.zeros(n, np.float32)
+    info = _lib.RunInfo()
+    c.check(c._L.sred_calculate_global_repetition_map_2d(
+        c.h, metric.encode(), np.ascontiguousarray(input_image.image_array, np.float32).ravel(),
+        input_image.width, input_image.height, block_width, block_height, block_size,
+        np.ascontiguousarray(local_statistics.local_means, np.float32).ravel(),
+        np.ascontiguousarray(local_statistics.local_stds, np.float32).ravel(),
+        np.ascontiguousarray(relevance_mask.relevance_mask, np.float32).ravel(),
+        float(relevance_mask.relevance_constant), float(relevance_mask.relevance_threshold),
+        float(relevance_mask.noise_mean_variance), float(n_pixels), int(bool(normalize_output)), out,
+        C.byref(info)), "sred_calculate_global_repetition_map_2d")
+    if run_info is not None:
+        run_info.update(info.as_dict())
+    return out
+
+
+def _global_getter(metric):
+    def f(input_image, local_statistics, block_width, block_height, block_size, relevance_mask, n_pixels,
+          normalize_output, ctx=None):
+        return calculate_global_repetition_map_2d(metric, input_image, block_width, block_height, block_size,
+                                                  local_statistics, relevance_mask, n_pixels, normalize_output, ctx)
+    f.__doc__ = f"getGlobal*2D for {metric!r} (java/CLUtils.java:1680-2156)."
+    return f
+
+
+get_global_pearson_2d = _global_getter("Pearson's R")
+get_global_ssim_2d = _global_getter("SSIM")
+get_global_nrmse_2d = _global_getter("NRMSE")
+
+
+def get_global_abs_diff_stds_2d(input_image, local_statistics, block_width, block_height, relevance_mask, n_pixels,
+                                normalize_output, ctx=None):
+    """java/CLUtils.java:2049-2156 (no block size argument, as the reference)."""
+    from .utils import block_size
+    return calculate_global_repetition_map_2d("Abs. diff. of StdDevs", input_image, block_width, block_height,
+                                              block_size(block_width, block_height), local_statistics,
+                                              relevance_mask, n_pixels, normalize_output, ctx)
+
+
+def calculate_block_repetition_map_2d(metric: str, input_image: InputImage2D, reference_block: ReferenceBlock2D,
+                                      relevance_constant: float, normalize_output: bool, use_device: bool = False,
+                                      ctx=None):
+    """java/CLUtils.java:995-1010."""
+    if metric not in BLOCK_METRICS and metric != COSINE:
+        return None
+    c = _ctx(ctx)
+    out = np.zeros(input_image.size, np.float32)
+    c.check(c._L.sred_calculate_block_repetition_map_2d(
+        c.h, metric.encode(), np.ascontiguousarray(input_image.image_array, np.float32).ravel(),
+        input_image.width, input_image.height, np.ascontiguousarray(reference_block.pixels, np.float32).ravel(),
+        int(reference_block.size), reference_block.width, reference_block.height, float(reference_block.mean),
+        float(reference_block.std), float(relevance_constant), int(bool(normalize_output)), out),
+        "sred_calculate_block_repetition_map_2d")
+    return out
+
+
+def _block_getter(metric):
+    def f(input_image, reference_block, relevance_constant, normalize_output, use_device=False, ctx=None):
+        return calculate_block_repetition_map_2d(metric, input_image, reference_block, relevance_constant,
+                                                 normalize_output, use_device, ctx)
+    f.__doc__ = f"getBlock*2D for {metric!r} (java/CLUtils.java:486-981)."
+    return f
+
+
+get_block_pearson_2d = _block_getter("Pearson's R")
+get_block_ssim_2d = _block_getter("SSIM")
+get_block_nrmse_2d = _block_getter("NRMSE (inverted)")
+get_block_abs_diff_stds_2d = _block_getter("Abs. Diff. of StdDevs.")
+
+
+def global_map_device(metric: str, d_img_ptr: int, width: int, height: int, block_width: int, block_height: int,
+                      relevance_constant: float, normalize_output: bool, d_out_ptr: int, stream_ptr: int = 0,
+                      ctx=None) -> dict:
+    """Global map on device-resident buffers (raw CUDA pointers); returns run info."""
+    c = _ctx(ctx)
+    info = _lib.RunInfo()
+    c.check(c._L.sred_global_map_2d_device(c.h, metric.encode(), C.c_void_p(d_img_ptr), width, height, block_width,
+                                           block_height, float(relevance_constant), int(bool(normalize_output)),
+                                           C.c_void_p(d_out_ptr), C.c_void_p(stream_ptr or None), C.byref(info)),
+            "sred_global_map_2d_device")
+    return info.as_dict()
+
+
+def global_map_host(metric: str, img: np.ndarray, block_width: int, block_height: int, relevance_constant: float,
+                    normalize_output: bool = True, out: np.ndarray | None = None, ctx=None) -> tuple:
+    """The whole global-map command on host buffers (sred_global_map_2d):
+    returns (map, run info). ``img`` may be pinned memory."""
+    c = _ctx(ctx)
+    a = np.ascontiguousarray(img, np.float32)
+    h, w = a.shape
+    if out is None:
+        out = np.empty((h, w), np.float32)
+    info = _lib.RunInfo()
+    c.check(c._L.sred_global_map_2d(c.h, metric.encode(), C.c_void_p(a.ctypes.data), w, h, block_width,
+                                    block_height, float(relevance_constant), int(bool(normalize_output)),
+                                    C.c_void_p(out.ctypes.data), C.byref(info)), "sred_global_map_2d")
+    return out, info.as_dict()
+
+
+def block_map_device(metric: str, d_img_ptr: int, width: int, height: int, frames: int,
+                     reference_block: ReferenceBlock2D, relevance_constant: float, normalize_output: bool,
+                     d_out_ptr: int, stream_ptr: int = 0, ctx=None) -> None:
+    """Block map over a device-resident stack of frames (raw CUDA pointers)."""
+    c = _ctx(ctx)
+    c.check(c._L.sred_block_map_2d_device(
+        c.h, metric.encode(), C.c_void_p(d_img_ptr), width, height, frames,
+        np.ascontiguousarray(reference_block.pixels, np.float32).ravel(), int(reference_block.size),
+        reference_block.width, reference_block.height, float(reference_block.mean), float(reference_block.std),
+        float(relevance_constant), int(bool(normalize_output)), C.c_void_p(d_out_ptr),
+        C.c_void_p(stream_ptr or None)), "sred_block_map_2d_device")

@@ -1,0 +1,80 @@
+// Fused per-pair epilogue of the global repetition map, shared by the FP32
+// CUDA-core engine and the split-BF16 tensor-core engine.
+//
+// Input per pair (p, q): G = <u_p, u_q>, the dot product of the two blocks'
+// zero-mean unit vectors (the contraction engine's output), and the blocks'
+// FP64-derived parameters. The reference's per-pair quantities
+// (cl/kernelGetGlobal*2D.cl) are rewritten in terms of G:
+//   cov_pq            = sigma_p sigma_q G                  (K-1 normalisation)
+//   weight            = exp(-(sigma_p - sigma_q)^2 / (v + eps)) = 2^-(a_p - a_q)^2
+//   Pearson           = max(0, G sigma_p sigma_q / (sigma_p sigma_q + eps)) * weight
+//                     = max(0, G / (1 + t)) * weight,  t = (eps / sigma_p)(1 / sigma_q)
+//   SSIM (global)     = max(0, (2 mu_p mu_q + c1)(2 cov + c2) /
+//                              ((mu_p^2 mu_q^2 + c1)(sigma_p^2 + sigma_q^2 + c2)) * weight)
+//   NRMSE (unweighted)= sqrt(((K-1)/K) ((sigma_p - sigma_q)^2 + 2 sigma_p sigma_q (1 - G)))
+//   Abs-diff          = |sigma_p - sigma_q| * weight
+// The NRMSE form uses the normalised vectors, so the large common part of
+// |x_p|^2 + |x_q|^2 - 2<x_p, x_q> never cancels in FP32.
+// 1/(1+t) is evaluated as 1 - t + t^2 when the tile's largest t is below
+// 2^-8 (relative error < t^3 < 6e-8), exactly otherwise.
+#pragma once
+#include "common.cuh"
+
+namespace sred {
+
+constexpr float kTFast = 1.0f / 256.0f;
+
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+struct RowState {
+  float a, e, sigma, mu;
+  float mu2x2;   // 2 mu_p
+  float mumu;    // mu_p^2
+  float s2;      // sigma_p^2 + c2
+  float sig2x;   // 2 sigma_p
+};
+
+__device__ __forceinline__ RowState make_row(const BlockParams& bp, const EpiConsts& ec) {
+  RowState r;
+  r.a = bp.a;
+  r.e = bp.e;
+  r.sigma = bp.sigma;
+  r.mu = bp.mu;
+  r.mu2x2 = 2.0f * bp.mu;
+  r.mumu = bp.mu * bp.mu;
+  r.s2 = bp.sigma * bp.sigma + ec.c2;
+  r.sig2x = 2.0f * bp.sigma;
+  return r;
+}
+
+// One pair. EXACT selects the exact 1/(1+t) (Pearson only).
+template <int METRIC, bool EXACT>
+__device__ __forceinline__ void epi_pair(float G, const RowState& rp, const BlockParams& cq,
+                                         const EpiConsts& ec, float& sn, float& sd) {
+  const float d = rp.a - cq.a;
+  const float w = ex2_approx(-d * d);
+  sd += w;
+  if (METRIC == kPearson) {
+    const float t = rp.e * cq.r;
+    float c;
+    if (EXACT) c = __frcp_rn(1.0f + t);
+    else c = fmaf(t, t - 1.0f, 1.0f);
+    sn = fmaf(fmaxf(G * c, 0.0f), w, sn);
+  } else if (METRIC == kSsim) {
+    const float num = fmaf(rp.mu2x2, cq.mu, ec.c1) * fmaf(rp.sig2x * cq.sigma, G, ec.c2);
+    const float den = fmaf(rp.mumu, cq.mu * cq.mu, ec.c1) * fmaf(cq.sigma, cq.sigma, rp.s2);
+    sn += fmaxf(__fdividef(num, den) * w, 0.0f);
+  } else if (METRIC == kNrmse) {
+    const float ds = rp.sigma - cq.sigma;
+    const float m = ec.nrmse_scale * fmaf(ds, ds, rp.sig2x * cq.sigma * (1.0f - G));
+    sn += sqrtf(fmaxf(m, 0.0f));
+  } else {  // Abs-diff of stds
+    sn = fmaf(fabsf(rp.sigma - cq.sigma), w, sn);
+  }
+}
+
+}  // namespace sred

@@ -1,0 +1,44 @@
+// Kernel declarations shared between the device translation units and the
+// host orchestration (sred_api.cu).
+#pragma once
+#include "common.cuh"
+
+namespace sred {
+
+constexpr int kCompactSeg = 2048;
+
+struct RefBlock {
+  int k;
+  float mean, std;
+  float px[kMaxK];
+};
+
+// moments.cu
+__global__ void k_local_stats(const float* img, int W, int H, Ellipse e, float* means, float* stds);
+__global__ void k_noise_tiles(const float* img, int W, int t, int nbx, int nb, float* vars, int* bad);
+__global__ void k_flags(const float* stds, const float* mask_in, int W, int H, int rw, int rh, float thr,
+                        float* mask, uint8_t* flags, unsigned long long* n_mask);
+__global__ void k_count(const uint8_t* flags, size_t n, int2* counts);
+__global__ void k_scan(int2* counts, int nseg);
+__global__ void k_scatter(const uint8_t* flags, size_t n, const int2* offs, int* gram_pix, int* flat_pix,
+                          int* slot);
+__global__ void k_pack(const float* img, int W, Ellipse e, const int* gram_pix, int n, float wscale, int mode,
+                       float* U, int kp, __nv_bfloat16* A, __nv_bfloat16* B, int kq, BlockParams* params,
+                       float* tile_rmax, double* sums);
+__global__ void k_finalize(const int* slot, int W, int H, int rw, int rh, const double* num, const double* den,
+                           const BlockParams* params, const double* sums, int n_flat, int metric, double sk,
+                           double n_pixels, const float* mask, int apply_mask, float* out);
+__global__ void k_minmax(const float* a, const float* mask, int W, int H, int bw_, int bh_, size_t plane,
+                         unsigned* mm);
+__global__ void k_remap(float* a, const float* mask, int W, int H, int bw_, int bh_, size_t plane,
+                        const unsigned* mm);
+
+// block_map.cu
+__global__ void k_block_map(const float* img, int W, int H, int frames, Ellipse e, RefBlock rb, int metric,
+                            float* out, float* stds_out);
+__global__ void k_block_absdiff_post(float* a, int W, int H, int rw, int rh, size_t plane, const unsigned* mm);
+__global__ void k_interior_mask(float* mask, int W, int H, int rw, int rh, size_t plane);
+__global__ void k_apply_mask(float* a, const float* mask, size_t n);
+__global__ void k_invert_masked(float* a, const float* mask, int W, int H, int rw, int rh, size_t plane);
+
+}  // namespace sred

@@ -1,0 +1,690 @@
+// libsred C ABI: context, workspaces and the orchestration of the global and
+// block repetition maps (the part of java/CLUtils.java and java/Utils.java
+// that runs between the plugin commands and the kernels).
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+using namespace sred;
+
+namespace {
+
+enum BufId {
+  B_IMG, B_MEANS, B_STDS, B_MASK, B_MASKIN, B_FLAGS, B_SLOT, B_GPIX, B_FPIX, B_COUNTS, B_U, B_A, B_B,
+  B_PARAMS, B_RMAX, B_NUM, B_DEN, B_SUMS, B_OUT, B_VARS, B_MM, B_NMASK, B_BAD, B_STATUS, B_STDS2, B_NBUF
+};
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+}  // namespace
+
+struct sred_ctx {
+  int device = 0;
+  int num_sms = 148;
+  int engine = SRED_ENGINE_FP32;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[6] = {};
+  DevBuf buf[B_NBUF];
+  std::vector<float> hvars;
+  std::string err;
+  std::recursive_mutex mu;
+};
+
+namespace {
+
+// Host-side fault injection for tests: SRED_FAULT=alloc|launch makes the
+// library report that failure without touching the GPU.
+bool fault(const char* what) {
+  const char* f = std::getenv("SRED_FAULT");
+  return f && std::strcmp(f, what) == 0;
+}
+
+sred_status fail(sred_ctx* c, sred_status s, const std::string& msg) {
+  if (c) c->err = msg;
+  return s;
+}
+
+sred_status cuda_fail(sred_ctx* c, cudaError_t e, const char* where) {
+  std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+  return fail(c, e == cudaErrorMemoryAllocation ? SRED_ERR_OOM : SRED_ERR_LAUNCH, m);
+}
+
+#define CK(call)                                              \
+  do {                                                        \
+    cudaError_t _e = (call);                                  \
+    if (_e != cudaSuccess) return cuda_fail(c, _e, #call);    \
+  } while (0)
+
+#define CKS(expr)                      \
+  do {                                 \
+    sred_status _s = (expr);           \
+    if (_s != SRED_OK) return _s;      \
+  } while (0)
+
+template <class T>
+sred_status ensure(sred_ctx* c, int id, size_t count, T** out) {
+  size_t bytes = std::max<size_t>(count * sizeof(T), 256);
+  DevBuf& b = c->buf[id];
+  if (fault("alloc")) return fail(c, SRED_ERR_OOM, "injected allocation failure");
+  if (b.cap < bytes) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    size_t cap = bytes + bytes / 8;
+    cudaError_t e = cudaMalloc(&b.p, cap);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc");
+    b.cap = cap;
+  }
+  *out = static_cast<T*>(b.p);
+  return SRED_OK;
+}
+
+int global_metric(const char* m) {
+  if (!m) return -1;
+  if (!std::strcmp(m, "Pearson's R")) return kPearson;
+  if (!std::strcmp(m, "SSIM")) return kSsim;
+  if (!std::strcmp(m, "NRMSE")) return kNrmse;
+  if (!std::strcmp(m, "Abs. diff. of StdDevs")) return kAbsDiff;
+  return -1;
+}
+
+int block_metric(const char* m) {
+  if (!m) return -1;
+  if (!std::strcmp(m, "Pearson's R")) return kPearson;
+  if (!std::strcmp(m, "SSIM")) return kSsim;
+  if (!std::strcmp(m, "NRMSE (inverted)")) return kNrmse;
+  if (!std::strcmp(m, "Abs. Diff. of StdDevs.")) return kAbsDiff;
+  if (!std::strcmp(m, "Cosine")) return kCosine;
+  return -1;
+}
+
+// nPixels accumulates 1.0f per masked pixel in FP32
+// (java/GlobalRepetition2D_.java:133-140), which saturates at 2^24.
+float java_float_count(unsigned long long n) { return n <= 16777216ull ? (float)n : 16777216.0f; }
+
+size_t round_up(size_t a, size_t b) { return (a + b - 1) / b * b; }
+
+int grid_for(size_t n, int threads, int cap) {
+  size_t g = (n + threads - 1) / threads;
+  return (int)std::max<size_t>(1, std::min<size_t>(g, (size_t)cap));
+}
+
+sred_status check_block(sred_ctx* c, int w, int h, int bw, int bh, Ellipse* e) {
+  if (w <= 0 || h <= 0) return fail(c, SRED_ERR_ARG, "image dimensions must be positive");
+  if (bw % 2 == 0 || bh % 2 == 0 || bw < 3 || bh < 3)
+    return fail(c, SRED_ERR_ARG, "block dimensions must be odd and at least 3");
+  int k = build_ellipse(bw, bh, e);
+  if (k < 2 || k > kMaxK) return fail(c, SRED_ERR_ARG, "ellipse block size out of range");
+  return SRED_OK;
+}
+
+// Noise variance, java/Utils.java:790-837: tile variances on the device in
+// the reference's FP32 order, then the sort and the mean of the lowest 3% on
+// the host in FP32, exactly as the reference does them.
+sred_status noise_var_dev(sred_ctx* c, const float* d_img, int w, int h, cudaStream_t st, float* out) {
+  const int wh = w * h;
+  const int t = (wh <= 352 * 288) ? 8 : 16;
+  const int nbx = w / t, nby = h / t, nb = nbx * nby;
+  const int nv = (int)(0.03f * (float)nb + 1.0f);
+  if (nv > nb) return fail(c, SRED_ERR_ARG, "image smaller than one noise-variance tile");
+  float* d_vars;
+  int* d_bad;
+  CKS(ensure(c, B_VARS, nb, &d_vars));
+  CKS(ensure(c, B_BAD, 1, &d_bad));
+  CK(cudaMemsetAsync(d_bad, 0, sizeof(int), st));
+  k_noise_tiles<<<grid_for(nb, 128, 1 << 30), 128, 0, st>>>(d_img, w, t, nbx, nb, d_vars, d_bad);
+  CK(cudaGetLastError());
+  c->hvars.resize(nb);
+  int bad = 0;
+  CK(cudaMemcpyAsync(c->hvars.data(), d_vars, sizeof(float) * nb, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (bad) return fail(c, SRED_ERR_INVALID_INPUT, "Input contains invalid (NaN or Infinite) values.");
+  std::sort(c->hvars.begin(), c->hvars.end());
+  float v = 0.0f;
+  for (int i = 0; i < nv; i++) v += c->hvars[i];
+  v = std::fabs(v / (float)nv);
+  v = (1.0f + 0.001f * (v - 40.0f)) * v;
+  *out = v;
+  return SRED_OK;
+}
+
+sred_status normalize_dev(sred_ctx* c, float* d_a, const float* d_mask, int w, int h, int rw, int rh, int planes,
+                          cudaStream_t st) {
+  unsigned* mm;
+  CKS(ensure(c, B_MM, 2 * planes, &mm));
+  std::vector<unsigned> init(2 * planes);
+  for (int i = 0; i < planes; i++) { init[2 * i] = 0xffffffffu; init[2 * i + 1] = 0u; }
+  CK(cudaMemcpyAsync(mm, init.data(), sizeof(unsigned) * 2 * planes, cudaMemcpyHostToDevice, st));
+  dim3 g(grid_for((size_t)w * h, 256, 4 * c->num_sms), planes);
+  k_minmax<<<g, 256, 0, st>>>(d_a, d_mask, w, h, rw, rh, (size_t)w * h, mm);
+  k_remap<<<g, 256, 0, st>>>(d_a, d_mask, w, h, rw, rh, (size_t)w * h, mm);
+  CK(cudaGetLastError());
+  return SRED_OK;
+}
+
+struct GivenStats {
+  const float* means;  // host
+  const float* stds;
+  const float* mask;
+  float threshold, noise_var, n_pixels;
+};
+
+// The global repetition map on device-resident data.
+sred_status global_core(sred_ctx* c, int metric, const float* d_img, int w, int h, int bw, int bh, float relc,
+                        int normalize, float* d_out, cudaStream_t st, sred_run_info* info,
+                        const GivenStats* given) {
+  Ellipse e;
+  CKS(check_block(c, w, h, bw, bh, &e));
+  const int K = e.k, rw = e.rw, rh = e.rh;
+  const size_t n = (size_t)w * h;
+  if (n > (size_t)INT32_MAX / 2) return fail(c, SRED_ERR_ARG, "image too large");
+  if (fault("launch")) return fail(c, SRED_ERR_LAUNCH, "injected launch failure");
+  CK(cudaEventRecord(c->ev[0], st));
+
+  float *d_means, *d_stds, *d_mask;
+  CKS(ensure(c, B_MEANS, n, &d_means));
+  CKS(ensure(c, B_STDS, n, &d_stds));
+  CKS(ensure(c, B_MASK, n, &d_mask));
+  float nv, thr;
+  const float* d_mask_in = nullptr;
+  if (!given) {
+    k_local_stats<<<dim3((w + 127) / 128, h), 128, 0, st>>>(d_img, w, h, e, d_means, d_stds);
+    CK(cudaGetLastError());
+    CKS(noise_var_dev(c, d_img, w, h, st, &nv));
+    thr = nv * relc;
+  } else {
+    float* d_mi;
+    CKS(ensure(c, B_MASKIN, n, &d_mi));
+    CK(cudaMemcpyAsync(d_means, given->means, n * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_stds, given->stds, n * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_mi, given->mask, n * sizeof(float), cudaMemcpyHostToDevice, st));
+    d_mask_in = d_mi;
+    nv = given->noise_var;
+    thr = given->threshold;
+  }
+
+  uint8_t* d_flags;
+  int *d_slot, *d_gpix, *d_fpix;
+  int2* d_counts;
+  unsigned long long* d_nmask;
+  const int nseg = (int)((n + kCompactSeg - 1) / kCompactSeg);
+  CKS(ensure(c, B_FLAGS, n, &d_flags));
+  CKS(ensure(c, B_SLOT, n, &d_slot));
+  CKS(ensure(c, B_GPIX, n, &d_gpix));
+  CKS(ensure(c, B_FPIX, n, &d_fpix));
+  CKS(ensure(c, B_COUNTS, nseg + 1, &d_counts));
+  CKS(ensure(c, B_NMASK, 1, &d_nmask));
+  CK(cudaMemsetAsync(d_nmask, 0, sizeof(unsigned long long), st));
+  k_flags<<<grid_for(n, 256, 1 << 30), 256, 0, st>>>(d_stds, d_mask_in, w, h, rw, rh, thr, d_mask, d_flags,
+                                                      d_nmask);
+  k_count<<<nseg, 256, 0, st>>>(d_flags, n, d_counts);
+  k_scan<<<1, 1024, 0, st>>>(d_counts, nseg);
+  k_scatter<<<nseg, 256, 0, st>>>(d_flags, n, d_counts, d_gpix, d_fpix, d_slot);
+  CK(cudaGetLastError());
+  int2 tot;
+  unsigned long long nmask = 0;
+  CK(cudaMemcpyAsync(&tot, d_counts + nseg, sizeof(int2), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&nmask, d_nmask, sizeof(nmask), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  const int n_g = tot.x, n_flat = tot.y;
+  const float npx = given ? given->n_pixels : java_float_count(nmask);
+
+  // Operands and per-block parameters of the all-pairs contraction.
+  const int engine = (metric == kAbsDiff) ? SRED_ENGINE_FP32 : c->engine;
+  const size_t n_pad = round_up((size_t)std::max(n_g, 1), 256);
+  const int kp = (int)round_up(K, 4);
+  const int kq = (int)round_up(3 * K, 16);
+  float* d_U = nullptr;
+  __nv_bfloat16 *d_A = nullptr, *d_B = nullptr;
+  BlockParams* d_params;
+  float* d_rmax;
+  double *d_num, *d_den, *d_sums;
+  CKS(ensure(c, B_PARAMS, n_pad, &d_params));
+  CKS(ensure(c, B_RMAX, n_pad / 128, &d_rmax));
+  CKS(ensure(c, B_NUM, n_pad, &d_num));
+  CKS(ensure(c, B_DEN, n_pad, &d_den));
+  CKS(ensure(c, B_SUMS, 4, &d_sums));
+  if (engine == SRED_ENGINE_FP32) {
+    CKS(ensure(c, B_U, n_pad * kp, &d_U));
+    CK(cudaMemsetAsync(d_U + (size_t)n_g * kp, 0, (n_pad - n_g) * kp * sizeof(float), st));
+  } else {
+    CKS(ensure(c, B_A, n_pad * kq, &d_A));
+    CKS(ensure(c, B_B, n_pad * kq, &d_B));
+    CK(cudaMemsetAsync(d_A + (size_t)n_g * kq, 0, (n_pad - n_g) * kq * sizeof(__nv_bfloat16), st));
+    CK(cudaMemsetAsync(d_B + (size_t)n_g * kq, 0, (n_pad - n_g) * kq * sizeof(__nv_bfloat16), st));
+  }
+  CK(cudaMemsetAsync(d_params + n_g, 0, (n_pad - n_g) * sizeof(BlockParams), st));
+  CK(cudaMemsetAsync(d_rmax, 0, (n_pad / 128) * sizeof(float), st));
+  CK(cudaMemsetAsync(d_num, 0, n_pad * sizeof(double), st));
+  CK(cudaMemsetAsync(d_den, 0, n_pad * sizeof(double), st));
+  CK(cudaMemsetAsync(d_sums, 0, 4 * sizeof(double), st));
+  // weight = exp(-(s_p - s_q)^2 / (FILTER_PARAM + EPSILON)) = 2^-(a_p - a_q)^2,
+  // FILTER_PARAM + EPSILON summed in FP32 as the reference kernel does.
+  const float hden = nv + kEps;
+  const float wscale = (float)std::sqrt(1.4426950408889634 / (double)hden);
+  if (n_g > 0) {
+    const int pgrid = grid_for((size_t)n_g * 32, 256, 8 * c->num_sms);
+    k_pack<<<pgrid, 256, 0, st>>>(d_img, w, e, d_gpix, n_g, wscale, engine == SRED_ENGINE_FP32 ? 0 : 1, d_U,
+                                  kp, d_A, d_B, kq, d_params, d_rmax, d_sums);
+    CK(cudaGetLastError());
+  }
+  CK(cudaEventRecord(c->ev[1], st));
+  EpiConsts ec;
+  ec.metric = metric;
+  ec.n = n_g;
+  ec.nrmse_scale = (float)((double)(K - 1) / (double)K);
+  ec.c1 = kC1;
+  ec.c2 = kC2;
+  if (n_g > 0) {
+    if (engine == SRED_ENGINE_FP32) {
+      CK(launch_gram_fp32(d_U, kp, d_params, d_rmax, ec, d_num, d_den, c->num_sms, st));
+    } else {
+      int* d_status;
+      CKS(ensure(c, B_STATUS, 4, &d_status));
+      CK(cudaMemsetAsync(d_status, 0, 4 * sizeof(int), st));
+      CK(launch_gram_tc(d_A, d_B, kq, (int)n_pad, d_params, d_rmax, ec, d_num, d_den, c->num_sms, d_status, st));
+      int status = 0;
+      CK(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      if (status) return fail(c, SRED_ERR_TIMEOUT, "tensor-core pipeline wait exceeded its bound");
+    }
+  }
+  CK(cudaEventRecord(c->ev[2], st));
+  const double sk = std::sqrt((double)(K - 1) / (double)K);
+  k_finalize<<<grid_for(n, 256, 1 << 30), 256, 0, st>>>(d_slot, w, h, rw, rh, d_num, d_den, d_params, d_sums,
+                                                          n_flat, metric, sk, (double)npx, d_mask,
+                                                          relc > 0.0f ? 1 : 0, d_out);
+  CK(cudaGetLastError());
+  if (normalize) CKS(normalize_dev(c, d_out, d_mask, w, h, rw, rh, 1, st));
+  CK(cudaEventRecord(c->ev[3], st));
+  CK(cudaEventSynchronize(c->ev[3]));
+  if (info) {
+    info->n_blocks = (int64_t)std::max(0, w - 2 * rw) * std::max(0, h - 2 * rh);
+    info->n_relevant = (int64_t)n_g + n_flat;
+    info->n_flat = n_flat;
+    info->pairs = (double)info->n_relevant * (double)info->n_relevant;
+    info->noise_var = nv;
+    info->threshold = thr;
+    info->n_pixels = npx;
+    info->k = K;
+    info->engine = engine;
+    float t01 = 0, t12 = 0, t23 = 0, t03 = 0;
+    cudaEventElapsedTime(&t01, c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&t12, c->ev[1], c->ev[2]);
+    cudaEventElapsedTime(&t23, c->ev[2], c->ev[3]);
+    cudaEventElapsedTime(&t03, c->ev[0], c->ev[3]);
+    info->ms_moments = t01;
+    info->ms_gram = t12;
+    info->ms_finalize = t23;
+    info->ms_total = t03;
+    info->launches = (given ? 0 : 2) + 4 + (n_g > 0 ? 2 : 0) + 1 + (normalize ? 2 : 0);
+  }
+  return SRED_OK;
+}
+
+sred_status block_core(sred_ctx* c, int metric, const float* d_img, int w, int h, int frames,
+                       const float* ref_pixels, int block_size, int bw, int bh, float ref_mean, float ref_std,
+                       float relc, int normalize, float* d_out, cudaStream_t st) {
+  Ellipse e;
+  CKS(check_block(c, w, h, bw, bh, &e));
+  if (block_size != e.k) return fail(c, SRED_ERR_ARG, "block_size does not match the ellipse of bw x bh");
+  if (frames < 1) return fail(c, SRED_ERR_ARG, "frames must be >= 1");
+  if (fault("launch")) return fail(c, SRED_ERR_LAUNCH, "injected launch failure");
+  const int rw = e.rw, rh = e.rh;
+  const size_t plane = (size_t)w * h, n = plane * frames;
+  RefBlock rb;
+  rb.k = e.k;
+  rb.mean = ref_mean;
+  rb.std = ref_std;
+  std::memcpy(rb.px, ref_pixels, sizeof(float) * e.k);
+  const bool need_mask = (metric == kNrmse) || relc > 0.0f;
+  float* d_stds = nullptr;
+  if (need_mask) CKS(ensure(c, B_STDS2, n, &d_stds));
+  dim3 grid((w + 31) / 32, (h + 7) / 8, frames), blk(32, 8);
+  size_t smem = sizeof(float) * (32 + 2 * rw) * (8 + 2 * rh);
+  if (smem > 200 * 1024) return fail(c, SRED_ERR_ARG, "block too large for the streaming tile");
+  if (smem > 48 * 1024)
+    CK(cudaFuncSetAttribute(k_block_map, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_block_map<<<grid, blk, smem, st>>>(d_img, w, h, frames, e, rb, metric, d_out, d_stds);
+  CK(cudaGetLastError());
+
+  float* d_mask = nullptr;
+  const dim3 pg(grid_for(plane, 256, 4 * c->num_sms), frames);
+  auto relevance_masks = [&]() -> sred_status {
+    float* d_m;
+    uint8_t* d_flags;
+    unsigned long long* d_cnt;
+    CKS(ensure(c, B_MASK, n, &d_m));
+    CKS(ensure(c, B_FLAGS, plane, &d_flags));
+    CKS(ensure(c, B_NMASK, 1, &d_cnt));
+    for (int f = 0; f < frames; f++) {
+      float nv;
+      CKS(noise_var_dev(c, d_img + f * plane, w, h, st, &nv));
+      k_flags<<<grid_for(plane, 256, 1 << 30), 256, 0, st>>>(d_stds + f * plane, nullptr, w, h, rw, rh,
+                                                             nv * relc, d_m + f * plane, d_flags, d_cnt);
+    }
+    CK(cudaGetLastError());
+    d_mask = d_m;
+    return SRED_OK;
+  };
+
+  if (metric == kNrmse) {
+    if (relc == 0.0f) {
+      CKS(ensure(c, B_MASK, n, &d_mask));
+      k_interior_mask<<<pg, 256, 0, st>>>(d_mask, w, h, rw, rh, plane);
+    } else {
+      CKS(relevance_masks());
+    }
+    k_apply_mask<<<grid_for(n, 256, 8 * c->num_sms), 256, 0, st>>>(d_out, d_mask, n);
+    CKS(normalize_dev(c, d_out, d_mask, w, h, rw, rh, frames, st));
+    k_invert_masked<<<pg, 256, 0, st>>>(d_out, d_mask, w, h, rw, rh, plane);
+    if (normalize) CKS(normalize_dev(c, d_out, d_mask, w, h, rw, rh, frames, st));
+  } else {
+    if (metric == kAbsDiff) {
+      unsigned* mm;
+      CKS(ensure(c, B_MM, 2 * frames, &mm));
+      std::vector<unsigned> init(2 * frames);
+      for (int i = 0; i < frames; i++) { init[2 * i] = 0xffffffffu; init[2 * i + 1] = 0u; }
+      CK(cudaMemcpyAsync(mm, init.data(), sizeof(unsigned) * 2 * frames, cudaMemcpyHostToDevice, st));
+      k_minmax<<<pg, 256, 0, st>>>(d_out, nullptr, w, h, rw, rh, plane, mm);
+      k_block_absdiff_post<<<pg, 256, 0, st>>>(d_out, w, h, rw, rh, plane, mm);
+    }
+    if (relc > 0.0f) {
+      CKS(relevance_masks());
+      k_apply_mask<<<grid_for(n, 256, 8 * c->num_sms), 256, 0, st>>>(d_out, d_mask, n);
+    }
+    if (normalize) CKS(normalize_dev(c, d_out, d_mask, w, h, rw, rh, frames, st));
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+  return SRED_OK;
+}
+
+cudaStream_t pick(sred_ctx* c, void* s) { return s ? (cudaStream_t)s : c->stream; }
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* sred_status_string(sred_status s) {
+  switch (s) {
+    case SRED_OK: return "ok";
+    case SRED_ERR_ARG: return "invalid argument";
+    case SRED_ERR_UNKNOWN_METRIC: return "unknown metric";
+    case SRED_ERR_NODEV: return "no CUDA device";
+    case SRED_ERR_OOM: return "out of device memory";
+    case SRED_ERR_LAUNCH: return "kernel launch or CUDA call failed";
+    case SRED_ERR_TIMEOUT: return "device wait timed out";
+    case SRED_ERR_INTERNAL: return "internal error";
+    case SRED_ERR_INVALID_INPUT: return "input contains NaN or Inf";
+  }
+  return "unknown status";
+}
+
+const char* sred_last_error(sred_ctx* c) { return c ? c->err.c_str() : ""; }
+
+int sred_block_size(int bw, int bh) {
+  if (bw < 3 || bh < 3) return 0;
+  Ellipse e;
+  int k = build_ellipse(bw, bh, &e);
+  return k;
+}
+
+sred_status sred_create(int device, sred_ctx** out) {
+  if (!out) return SRED_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return SRED_ERR_NODEV;
+  }
+  if (device < 0 || device >= ndev) return SRED_ERR_NODEV;
+  sred_ctx* c = new sred_ctx();
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) { delete c; return SRED_ERR_NODEV; }
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return SRED_ERR_LAUNCH; }
+  for (auto& e : c->ev) cudaEventCreate(&e);
+  *out = c;
+  return SRED_OK;
+}
+
+sred_status sred_destroy(sred_ctx* c) {
+  if (!c) return SRED_ERR_ARG;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (auto& b : c->buf)
+    if (b.p) cudaFree(b.p);
+  for (auto& e : c->ev) cudaEventDestroy(e);
+  cudaStreamDestroy(c->stream);
+  delete c;
+  return SRED_OK;
+}
+
+sred_status sred_set_engine(sred_ctx* c, int engine) {
+  if (!c || (engine != SRED_ENGINE_TC && engine != SRED_ENGINE_FP32)) return SRED_ERR_ARG;
+  c->engine = engine;
+  return SRED_OK;
+}
+
+sred_status sred_local_statistics_2d(sred_ctx* c, const float* img, int w, int h, int bw, int bh,
+                                     float* means, float* stds) {
+  if (!c || !img || !means || !stds) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  Ellipse e;
+  CKS(check_block(c, w, h, bw, bh, &e));
+  const size_t n = (size_t)w * h;
+  float *d_img, *d_m, *d_s;
+  CKS(ensure(c, B_IMG, n, &d_img));
+  CKS(ensure(c, B_MEANS, n, &d_m));
+  CKS(ensure(c, B_STDS, n, &d_s));
+  cudaStream_t st = c->stream;
+  CK(cudaMemcpyAsync(d_img, img, n * sizeof(float), cudaMemcpyHostToDevice, st));
+  k_local_stats<<<dim3((w + 127) / 128, h), 128, 0, st>>>(d_img, w, h, e, d_m, d_s);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(means, d_m, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(stds, d_s, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return SRED_OK;
+}
+
+sred_status sred_mean_noise_var_2d(sred_ctx* c, const float* img, int w, int h, float* noise_var) {
+  if (!c || !img || !noise_var || w <= 0 || h <= 0) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  const size_t n = (size_t)w * h;
+  float* d_img;
+  CKS(ensure(c, B_IMG, n, &d_img));
+  CK(cudaMemcpyAsync(d_img, img, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  return noise_var_dev(c, d_img, w, h, c->stream, noise_var);
+}
+
+sred_status sred_relevance_mask_2d(sred_ctx* c, const float* img, int w, int h, int bw, int bh,
+                                   const float* stds, float relc, float* mask, float* threshold, float* noise_var) {
+  if (!c || !img || !stds || !mask || !threshold || !noise_var) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (w <= 0 || h <= 0 || bw < 1 || bh < 1) return fail(c, SRED_ERR_ARG, "bad dimensions");
+  const size_t n = (size_t)w * h;
+  float *d_img, *d_s, *d_m;
+  uint8_t* d_f;
+  unsigned long long* d_cnt;
+  CKS(ensure(c, B_IMG, n, &d_img));
+  CKS(ensure(c, B_STDS, n, &d_s));
+  CKS(ensure(c, B_MASK, n, &d_m));
+  CKS(ensure(c, B_FLAGS, n, &d_f));
+  CKS(ensure(c, B_NMASK, 1, &d_cnt));
+  cudaStream_t st = c->stream;
+  CK(cudaMemcpyAsync(d_img, img, n * sizeof(float), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_s, stds, n * sizeof(float), cudaMemcpyHostToDevice, st));
+  float nv;
+  CKS(noise_var_dev(c, d_img, w, h, st, &nv));
+  const float thr = nv * relc;
+  k_flags<<<grid_for(n, 256, 1 << 30), 256, 0, st>>>(d_s, nullptr, w, h, bw / 2, bh / 2, thr, d_m, d_f, d_cnt);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(mask, d_m, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  *threshold = thr;
+  *noise_var = nv;
+  return SRED_OK;
+}
+
+sred_status sred_calculate_global_repetition_map_2d(sred_ctx* c, const char* metric, const float* img, int w,
+                                                    int h, int bw, int bh, int block_size,
+                                                    const float* local_means, const float* local_stds,
+                                                    const float* mask, float relc, float threshold,
+                                                    float noise_var, float n_pixels, int normalize, float* out,
+                                                    sred_run_info* info) {
+  if (!c || !img || !local_means || !local_stds || !mask || !out) return SRED_ERR_ARG;
+  const int m = global_metric(metric);
+  if (m < 0) return fail(c, SRED_ERR_UNKNOWN_METRIC, "unknown global metric");
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (block_size != sred_block_size(bw, bh))
+    return fail(c, SRED_ERR_ARG, "block_size does not match the ellipse of bw x bh");
+  const size_t n = (size_t)w * h;
+  if (w <= 0 || h <= 0) return fail(c, SRED_ERR_ARG, "bad dimensions");
+  float *d_img, *d_out;
+  CKS(ensure(c, B_IMG, n, &d_img));
+  CKS(ensure(c, B_OUT, n, &d_out));
+  CK(cudaMemcpyAsync(d_img, img, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  GivenStats g{local_means, local_stds, mask, threshold, noise_var, n_pixels};
+  CKS(global_core(c, m, d_img, w, h, bw, bh, relc, normalize, d_out, c->stream, info, &g));
+  CK(cudaMemcpyAsync(out, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SRED_OK;
+}
+
+sred_status sred_global_map_2d(sred_ctx* c, const char* metric, const float* img, int w, int h, int bw, int bh,
+                               float relc, int normalize, float* out, sred_run_info* info) {
+  if (!c || !img || !out) return SRED_ERR_ARG;
+  const int m = global_metric(metric);
+  if (m < 0) return fail(c, SRED_ERR_UNKNOWN_METRIC, "unknown global metric");
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (w <= 0 || h <= 0) return fail(c, SRED_ERR_ARG, "bad dimensions");
+  const size_t n = (size_t)w * h;
+  float *d_img, *d_out;
+  CKS(ensure(c, B_IMG, n, &d_img));
+  CKS(ensure(c, B_OUT, n, &d_out));
+  CK(cudaMemcpyAsync(d_img, img, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  CKS(global_core(c, m, d_img, w, h, bw, bh, relc, normalize, d_out, c->stream, info, nullptr));
+  CK(cudaMemcpyAsync(out, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SRED_OK;
+}
+
+sred_status sred_global_map_2d_device(sred_ctx* c, const char* metric, const float* d_img, int w, int h, int bw,
+                                      int bh, float relc, int normalize, float* d_out, void* stream,
+                                      sred_run_info* info) {
+  if (!c || !d_img || !d_out) return SRED_ERR_ARG;
+  const int m = global_metric(metric);
+  if (m < 0) return fail(c, SRED_ERR_UNKNOWN_METRIC, "unknown global metric");
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  return global_core(c, m, d_img, w, h, bw, bh, relc, normalize, d_out, pick(c, stream), info, nullptr);
+}
+
+sred_status sred_calculate_block_repetition_map_2d(sred_ctx* c, const char* metric, const float* img, int w,
+                                                   int h, const float* ref_pixels, int block_size, int bw, int bh,
+                                                   float ref_mean, float ref_std, float relc, int normalize,
+                                                   float* out) {
+  if (!c || !img || !ref_pixels || !out) return SRED_ERR_ARG;
+  const int m = block_metric(metric);
+  if (m < 0) return fail(c, SRED_ERR_UNKNOWN_METRIC, "unknown block metric");
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (w <= 0 || h <= 0) return fail(c, SRED_ERR_ARG, "bad dimensions");
+  const size_t n = (size_t)w * h;
+  float *d_img, *d_out;
+  CKS(ensure(c, B_IMG, n, &d_img));
+  CKS(ensure(c, B_OUT, n, &d_out));
+  CK(cudaMemcpyAsync(d_img, img, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  CKS(block_core(c, m, d_img, w, h, 1, ref_pixels, block_size, bw, bh, ref_mean, ref_std, relc, normalize, d_out,
+                 c->stream));
+  CK(cudaMemcpyAsync(out, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SRED_OK;
+}
+
+sred_status sred_block_map_2d_device(sred_ctx* c, const char* metric, const float* d_img, int w, int h,
+                                     int frames, const float* ref_pixels, int block_size, int bw, int bh,
+                                     float ref_mean, float ref_std, float relc, int normalize, float* d_out,
+                                     void* stream) {
+  if (!c || !d_img || !ref_pixels || !d_out) return SRED_ERR_ARG;
+  const int m = block_metric(metric);
+  if (m < 0) return fail(c, SRED_ERR_UNKNOWN_METRIC, "unknown block metric");
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  return block_core(c, m, d_img, w, h, frames, ref_pixels, block_size, bw, bh, ref_mean, ref_std, relc, normalize,
+                    d_out, pick(c, stream));
+}
+
+// java/Utils.java:557-639 on host memory (ImageJ's float conversion is the caller's).
+sred_status sred_reference_block_2d(const float* blk, int bw, int bh, float* pixels, int* block_size, float* mean,
+                                    float* std_out) {
+  if (!blk || !pixels || !block_size || !mean || !std_out) return SRED_ERR_ARG;
+  if (bw % 2 == 0 || bh % 2 == 0 || bw < 3 || bh < 3) return SRED_ERR_ARG;
+  Ellipse e;
+  const int K = build_ellipse(bw, bh, &e);
+  if (K < 2 || K > kMaxK) return SRED_ERR_ARG;
+  for (int i = 0; i < K; i++) pixels[i] = blk[(e.dy[i] + e.rh) * bw + (e.dx[i] + e.rw)];
+  float mn = 3.40282347e38f, mx = -3.40282347e38f;
+  for (int i = 0; i < K; i++) {
+    mn = std::min(mn, pixels[i]);
+    mx = std::max(mx, pixels[i]);
+  }
+  float m = 0.0f;
+  for (int i = 0; i < K; i++) {
+    pixels[i] = (pixels[i] - mn) / (mx - mn + kEps);
+    m += pixels[i];
+  }
+  m /= (float)K;
+  for (int i = 0; i < K; i++) pixels[i] = pixels[i] - m;
+  float sd = 0.0f;
+  for (int i = 0; i < K; i++) sd += (pixels[i] - m) * (pixels[i] - m);
+  sd = (float)std::sqrt((double)(sd / ((float)(K - 1))));
+  *block_size = K;
+  *mean = m;
+  *std_out = sd;
+  return SRED_OK;
+}
+
+sred_status sred_normalize_image_2d(float* a, int w, int h, int bw_, int bh_, const float* mask) {
+  if (!a || w <= 0 || h <= 0) return SRED_ERR_ARG;
+  float mn = 3.40282347e38f, mx = -3.40282347e38f;
+  for (int y = bh_; y < h - bh_; y++)
+    for (int x = bw_; x < w - bw_; x++) {
+      const int i = y * w + x;
+      if (mask) {
+        if (mask[i] != 0.0f && mask[i] != 1.0f) return SRED_ERR_ARG;
+        if (!(mask[i] > 0.0f)) continue;
+      }
+      mn = std::min(a[i], mn);
+      mx = std::max(a[i], mx);
+    }
+  for (int y = bh_; y < h - bh_; y++)
+    for (int x = bw_; x < w - bw_; x++) {
+      const int i = y * w + x;
+      if (mask && !(mask[i] > 0.0f)) continue;
+      a[i] = (a[i] - mn) / (mx - mn + kEps);
+    }
+  return SRED_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,138 @@
+"""Host-side mirror of the reference's ``Utils`` (java/Utils.java), 2D parts.
+
+Same names (snake_case), argument meaning and error behaviour: the data types
+``InputImage2D``, ``ReferenceBlock2D`` and ``RelevanceMask``, and the host
+numerics that run between the plugin commands and the maps. The numerics run
+in libsred (``include/sred.h``); this module only marshals arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+
+EPSILON = np.float32(1e-7)  # java/Utils.java:20
+
+
+@dataclass
+class InputImage2D:
+    """java/Utils.java InputImage2D: a float32 image and its dimensions."""
+    image_array: np.ndarray  # float32 [height * width] or [height, width]
+    width: int
+    height: int
+
+    @property
+    def size(self) -> int:
+        return self.width * self.height
+
+    def array2d(self) -> np.ndarray:
+        return np.ascontiguousarray(self.image_array, np.float32).reshape(self.height, self.width)
+
+
+@dataclass
+class ReferenceBlock2D:
+    """java/Utils.java:108-216 ReferenceBlock2D: ellipse pixels and their stats."""
+    pixels: np.ndarray
+    width: int
+    height: int
+    radius_width: int
+    radius_height: int
+    size: int
+    mean: float
+    std: float
+
+
+@dataclass
+class RelevanceMask:
+    """java/Utils.java:35-96 RelevanceMask."""
+    relevance_mask: np.ndarray
+    relevance_constant: float
+    relevance_threshold: float
+    noise_mean_variance: float
+
+
+def _ctx(ctx):
+    return ctx if ctx is not None else _lib.default_context()
+
+
+def get_input_image_2d(image: np.ndarray, normalize_output: bool = True) -> InputImage2D:
+    """java/Utils.java:653-725 for an image given as an array (variance
+    stabilisation is outside this path): float conversion and min-max to
+    [0, 1] with epsilon, in FP32."""
+    a = np.ascontiguousarray(image, dtype=np.float32)
+    h, w = a.shape
+    if normalize_output:
+        mn, mx = np.float32(a.min()), np.float32(a.max())
+        a = ((a - mn) / (mx - mn + EPSILON)).astype(np.float32)
+    return InputImage2D(a.ravel(), w, h)
+
+
+def get_reference_block_2d(block: np.ndarray) -> ReferenceBlock2D:
+    """java/Utils.java:557-639: ellipse-flatten, min-max, mean-subtract and std
+    of a block image (odd dimensions; otherwise None, as the reference)."""
+    b = np.ascontiguousarray(block, dtype=np.float32)
+    bh, bw = b.shape
+    if bw % 2 == 0 or bh % 2 == 0:
+        return None
+    L = _lib.load()
+    px = np.zeros(bw * bh, np.float32)
+    k, m, s = C.c_int(), C.c_float(), C.c_float()
+    st = L.sred_reference_block_2d(b, bw, bh, px, C.byref(k), C.byref(m), C.byref(s))
+    if st != _lib.OK:
+        raise ValueError(_lib.status_string(st))
+    return ReferenceBlock2D(px[:k.value].copy(), bw, bh, bw // 2, bh // 2, k.value, np.float32(m.value),
+                            np.float32(s.value))
+
+
+def get_mean_noise_var_2d(ref_pixels: np.ndarray, w: int, h: int, ctx=None) -> np.float32:
+    """java/Utils.java:790-837."""
+    c = _ctx(ctx)
+    out = C.c_float()
+    c.check(c._L.sred_mean_noise_var_2d(c.h, np.ascontiguousarray(ref_pixels, np.float32).ravel(), w, h,
+                                        C.byref(out)), "sred_mean_noise_var_2d")
+    return np.float32(out.value)
+
+
+def get_relevance_mask(image_array: np.ndarray, image_width: int, image_height: int, block_radius_width: int,
+                       block_radius_height: int, local_stds: np.ndarray, relevance_constant: float,
+                       ctx=None) -> RelevanceMask:
+    """java/Utils.java:944-968."""
+    c = _ctx(ctx)
+    n = image_width * image_height
+    mask = np.zeros(n, np.float32)
+    thr, nv = C.c_float(), C.c_float()
+    c.check(c._L.sred_relevance_mask_2d(
+        c.h, np.ascontiguousarray(image_array, np.float32).ravel(), image_width, image_height,
+        2 * block_radius_width + 1, 2 * block_radius_height + 1,
+        np.ascontiguousarray(local_stds, np.float32).ravel(), relevance_constant, mask, C.byref(thr),
+        C.byref(nv)), "sred_relevance_mask_2d")
+    return RelevanceMask(mask, np.float32(relevance_constant), np.float32(thr.value), np.float32(nv.value))
+
+
+def apply_mask_2d(image_array: np.ndarray, image_width: int, image_height: int, mask: np.ndarray) -> np.ndarray:
+    """java/Utils.java:919-930 (in place; returns the array)."""
+    image_array *= np.asarray(mask, np.float32).reshape(image_array.shape)
+    return image_array
+
+
+def normalize_image_2d(image_array: np.ndarray, image_width: int, image_height: int, border_width: int,
+                       border_height: int, mask: np.ndarray | None) -> np.ndarray:
+    """java/Utils.java:985-1031. Raises ValueError for a non-binary mask, as the
+    reference throws IllegalArgumentException."""
+    a = np.ascontiguousarray(image_array, np.float32).ravel().copy()
+    mp = None
+    if mask is not None:
+        mp = np.ascontiguousarray(mask, np.float32).ravel()
+    st = _lib.load().sred_normalize_image_2d(a, image_width, image_height, border_width, border_height,
+                                             None if mp is None else mp.ctypes.data)
+    if st != _lib.OK:
+        raise ValueError("Relevance mask must be binary (0.0f or 1.0f)")
+    return a.reshape(np.shape(image_array))
+
+
+def block_size(block_width: int, block_height: int) -> int:
+    """Ellipse block size (java/GlobalRepetition2D_.java:102-111)."""
+    return _lib.load().sred_block_size(block_width, block_height)
