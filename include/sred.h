@@ -141,6 +141,14 @@ sred_status sred_reference_block_2d(const float *block_img, int bw, int bh, floa
 sred_status sred_normalize_image_2d(float *img, int w, int h, int border_w, int border_h,
                                     const float *mask);
 
+/* Diagnostics of the contraction engines (no counterpart in the reference):
+ * for caller-given vectors u (n x k, row-major) and column weights w1, w2,
+ * num[p] = sum_q <u_p, u_q> w1[q] and den[p] = sum_q w2[q], computed by the
+ * chosen engine's all-pairs kernel (the tensor-core engine splits u into
+ * bf16 hi/lo without normalising it). */
+sred_status sred_debug_gram_rowdot(sred_ctx *ctx, int engine, const float *u, const float *w1,
+                                   const float *w2, int n, int k, double *num, double *den);
+
 #ifdef __cplusplus
 }
 #endif

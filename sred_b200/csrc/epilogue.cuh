@@ -55,6 +55,11 @@ __device__ __forceinline__ RowState make_row(const BlockParams& bp, const EpiCon
 template <int METRIC, bool EXACT>
 __device__ __forceinline__ void epi_pair(float G, const RowState& rp, const BlockParams& cq,
                                          const EpiConsts& ec, float& sn, float& sd) {
+  if (METRIC == kDebugDot) {
+    sn = fmaf(G, cq.a, sn);
+    sd += cq.r;
+    return;
+  }
   const float d = rp.a - cq.a;
   const float w = ex2_approx(-d * d);
   sd += w;

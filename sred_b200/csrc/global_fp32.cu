@@ -185,6 +185,7 @@ cudaError_t launch_gram_fp32(const float* U, int kp, const BlockParams* params, 
     case kPearson: SRED_LAUNCH(kPearson); break;
     case kSsim: SRED_LAUNCH(kSsim); break;
     case kNrmse: SRED_LAUNCH(kNrmse); break;
+    case kDebugDot: SRED_LAUNCH(kDebugDot); break;
     default: SRED_LAUNCH(kAbsDiff); break;
   }
 #undef SRED_LAUNCH

@@ -1,11 +1,451 @@
-// Split-BF16 tcgen05 engine of the global repetition map (under construction).
+// Split-BF16 tcgen05 engine of the global repetition map (sm_100a).
+//
+// G = A' B'^T on the 5th-generation tensor cores, where each block's FP64 unit
+// vector u is split into bf16 hi = bf16(u), lo = bf16(u - hi), and
+//   A' = [hi | lo | hi],  B' = [hi | hi | lo]   (K' = round_up(3K, 16))
+// so one BF16 MMA chain with FP32 accumulation yields hi.hi + lo.hi + hi.lo,
+// an FP32-accurate <u_p, u_q> (the dropped lo.lo term is below 2^-16).
+//
+// CTA = 1 per SM, persistent over work items (128-row block, range of
+// 256-column tiles). Warp roles:
+//   warp 8      TMA producer: the item's A tile (resident, all K' chunks) and
+//               a ring of B stages (one 256 x 64 bf16 chunk each, SWIZZLE_128B)
+//   warp 9      MMA issuer (one thread): tcgen05.mma M=128 N=256 K=16 into one
+//               of two TMEM accumulators (2 x 256 columns), tcgen05.commit to
+//               release B stages and to publish finished accumulators
+//   warps 0-7   epilogue: tcgen05.ld of the accumulator (warp w reads TMEM
+//               lanes 32(w%4).. and columns 128(w/4)..), the fused per-pair
+//               metric (epilogue.cuh), row sums in registers; FP64 atomics
+//               per row per item. The N x N matrix is never stored.
+// Every mbarrier wait is bounded by wall time; on expiry the kernel records a
+// status code, stops issuing work, waits (bounded) for its own copies in
+// flight, frees TMEM and returns. No TMA multicast is used.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "common.cuh"
+#include "epilogue.cuh"
 
 namespace sred {
 
-cudaError_t launch_gram_tc(const __nv_bfloat16*, const __nv_bfloat16*, int, int, const BlockParams*, const float*,
-                           EpiConsts, double*, double*, int, int*, cudaStream_t) {
-  return cudaErrorNotSupported;
+namespace {
+
+constexpr int kBM = 128;          // rows per tile (TMEM lanes)
+constexpr int kBN = 256;          // columns per tile
+constexpr int kChunk = 64;        // bf16 elements per K chunk (128 B, one swizzle atom row)
+constexpr int kAChunkBytes = kBM * kChunk * 2;   // 16 KB
+constexpr int kBStageBytes = kBN * kChunk * 2;   // 32 KB
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = (kEpiWarps + 2) * 32;
+constexpr unsigned long long kTimeoutNs = 4000000000ull;  // 4 s per wait
+
+enum { ST_OK = 0, ST_TIMEOUT_PRODUCER = 1, ST_TIMEOUT_MMA = 2, ST_TIMEOUT_EPI = 3, ST_TIMEOUT_DRAIN = 4 };
+
+struct TcArgs {
+  int kq, nkc, stages;
+  int n_rb, n_ct, ct_per_item, n_items;
+  const BlockParams* params;
+  const float* tile_rmax;
+  EpiConsts ec;
+  double* num;
+  double* den;
+  int* status;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for the phase with the given parity. Returns false (and
+// records `code`) if the wait exceeded kTimeoutNs or another role of any CTA
+// already gave up.
+// Drain waits (for copies or MMAs this CTA issued) pass abort = false: they
+// keep waiting, within the same bound, after another role has given up.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* status, int code,
+                                          bool abort = true) {
+  if (mbar_test(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer();
+  for (uint32_t i = 1;; i++) {
+    if (mbar_test(bar, parity)) return true;
+    if ((i & 255u) == 0) {
+      if (abort && *reinterpret_cast<volatile int*>(status) != ST_OK) return false;
+      if (globaltimer() - t0 > kTimeoutNs) {
+        atomicCAS(status, ST_OK, code);
+        return false;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::
+          "r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
+      : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, SWIZZLE_128B, 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr & 0x3FFFFu) >> 4);
+  d |= static_cast<uint64_t>(1) << 16;           // leading byte offset (unused for swizzled K-major)
+  d |= static_cast<uint64_t>(1024 >> 4) << 32;   // stride byte offset
+  d |= static_cast<uint64_t>(1) << 46;           // descriptor version (sm_100)
+  d |= static_cast<uint64_t>(2) << 61;           // SWIZZLE_128B
+  return d;
+}
+
+// Instruction descriptor, kind::f16: D = F32, A = B = BF16, both K-major, M = 128, N = 256.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(kBN >> 3) << 17) |
+                            (static_cast<uint32_t>(kBM >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 32 lanes x 32 columns of 32-bit accumulator; the wait is fused with a
+// register dependency so no use of v can be scheduled before it.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+        "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
+                 "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]),
+                 "+r"(v[15]), "+r"(v[16]), "+r"(v[17]), "+r"(v[18]), "+r"(v[19]), "+r"(v[20]), "+r"(v[21]),
+                 "+r"(v[22]), "+r"(v[23]), "+r"(v[24]), "+r"(v[25]), "+r"(v[26]), "+r"(v[27]), "+r"(v[28]),
+                 "+r"(v[29]), "+r"(v[30]), "+r"(v[31])
+               :
+               : "memory");
+}
+
+// Column parameters of one tile, structure-of-arrays in shared memory.
+struct ColTile {
+  float a[kBN];
+  float r[kBN];
+  float sigma[kBN];
+  float mu[kBN];
+};
+
+template <int METRIC, bool EXACT, bool FULL>
+__device__ __forceinline__ void epi_tile(uint32_t taddr, const ColTile& ct, int cbase, int col0,
+                                         const RowState& rs, const EpiConsts& ec, float& sn, float& sd) {
+#pragma unroll 1
+  for (int c = 0; c < kBN / 2; c += 32) {
+    uint32_t v[32];
+    tmem_ld32(taddr + c, v);
+#pragma unroll
+    for (int j = 0; j < 32; j += 4) {
+      const int q = cbase + c + j;
+      const float4 a4 = *reinterpret_cast<const float4*>(&ct.a[q]);
+      const float4 r4 = *reinterpret_cast<const float4*>(&ct.r[q]);
+      float4 s4 = make_float4(0.f, 0.f, 0.f, 0.f), m4 = s4;
+      if (METRIC != kPearson) s4 = *reinterpret_cast<const float4*>(&ct.sigma[q]);
+      if (METRIC == kSsim) m4 = *reinterpret_cast<const float4*>(&ct.mu[q]);
+      const float av[4] = {a4.x, a4.y, a4.z, a4.w};
+      const float rv[4] = {r4.x, r4.y, r4.z, r4.w};
+      const float sv[4] = {s4.x, s4.y, s4.z, s4.w};
+      const float mv[4] = {m4.x, m4.y, m4.z, m4.w};
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        BlockParams cq;
+        cq.a = av[u];
+        cq.r = rv[u];
+        cq.sigma = sv[u];
+        cq.mu = mv[u];
+        if (FULL || col0 + q + u < ec.n) epi_pair<METRIC, EXACT>(__uint_as_float(v[j + u]), rs, cq, ec, sn, sd);
+      }
+    }
+  }
+}
+
+template <int METRIC>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_gram_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcArgs g) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t* sbase = smem_raw + (base - raw);
+  const int S = g.stages, nkc = g.nkc;
+  const uint32_t sA = base;                                     // nkc x 16 KB
+  const uint32_t sB = sA + nkc * kAChunkBytes;                  // S x 32 KB
+  ColTile* cols = reinterpret_cast<ColTile*>(sbase + (nkc * kAChunkBytes + S * kBStageBytes));  // [2]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(cols) + 2 * sizeof(ColTile));
+  // barrier layout: full[S], empty[S], acc_full[2], acc_empty[2], a_full, a_empty, done
+  const uint32_t b_full = smem_u32(bars), b_empty = b_full + 8 * S, b_accf = b_empty + 8 * S,
+                 b_acce = b_accf + 16, b_afull = b_acce + 16, b_aempty = b_afull + 8, b_done = b_aempty + 8;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 7);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; s++) {
+      mbar_init(b_full + 8 * s, 1);
+      mbar_init(b_empty + 8 * s, 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(b_accf + 8 * b, 1);
+      mbar_init(b_acce + 8 * b, kEpiWarps);
+    }
+    mbar_init(b_afull, 1);
+    mbar_init(b_aempty, 1);
+    mbar_init(b_done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == kEpiWarps + 1) {  // MMA warp owns the TMEM allocation
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(2 * kBN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == kEpiWarps) {
+    // ---------------------------------------------------------------- TMA
+    if (lane == 0) {
+      uint32_t it = 0, item_i = 0;
+      bool ok = true;
+      for (int item = blockIdx.x; ok && item < g.n_items; item += gridDim.x, item_i++) {
+        const int rb = item % g.n_rb, seg = item / g.n_rb;
+        const int ct0 = seg * g.ct_per_item, ct1 = min(ct0 + g.ct_per_item, g.n_ct);
+        if (!mbar_wait(b_aempty, (item_i & 1) ^ 1, g.status, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
+        mbar_expect_tx(b_afull, nkc * kAChunkBytes);
+        for (int kc = 0; kc < nkc; kc++) tma_load_2d(sA + kc * kAChunkBytes, &tmA, b_afull, kc * kChunk, rb * kBM);
+        for (int ct = ct0; ok && ct < ct1; ct++) {
+          for (int kc = 0; kc < nkc; kc++, it++) {
+            const int s = it % S;
+            if (!mbar_wait(b_empty + 8 * s, ((it / S) & 1) ^ 1, g.status, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
+            mbar_expect_tx(b_full + 8 * s, kBStageBytes);
+            tma_load_2d(sB + s * kBStageBytes, &tmB, b_full + 8 * s, kc * kChunk, ct * kBN);
+          }
+        }
+      }
+      // Drain: every issued B load has landed before the CTA may exit.
+      for (uint32_t k = (it > (uint32_t)S ? it - S : 0); k < it; k++)
+        mbar_wait(b_full + 8 * (k % S), (k / S) & 1, g.status, ST_TIMEOUT_DRAIN, false);
+    }
+    __syncwarp();
+  } else if (warp == kEpiWarps + 1) {
+    // ---------------------------------------------------------------- MMA
+    if (lane == 0) {
+      uint32_t it = 0, tile = 0, item_i = 0;
+      bool ok = true;
+      for (int item = blockIdx.x; ok && item < g.n_items; item += gridDim.x, item_i++) {
+        const int seg = item / g.n_rb;
+        const int ct0 = seg * g.ct_per_item, ct1 = min(ct0 + g.ct_per_item, g.n_ct);
+        if (!mbar_wait(b_afull, item_i & 1, g.status, ST_TIMEOUT_MMA)) { ok = false; break; }
+        tc_fence_after();
+        for (int ct = ct0; ok && ct < ct1; ct++, tile++) {
+          const uint32_t b = tile & 1;
+          if (!mbar_wait(b_acce + 8 * b, ((tile >> 1) & 1) ^ 1, g.status, ST_TIMEOUT_MMA)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t d = tmem + b * kBN;
+          for (int kc = 0; kc < nkc; kc++, it++) {
+            const int s = it % S;
+            if (!mbar_wait(b_full + 8 * s, (it / S) & 1, g.status, ST_TIMEOUT_MMA)) { ok = false; break; }
+            tc_fence_after();
+            const int nks = min(kChunk, g.kq - kc * kChunk) / 16;
+            for (int ks = 0; ks < nks; ks++) {
+              const uint64_t da = desc_sw128(sA + kc * kAChunkBytes + ks * 32);
+              const uint64_t db = desc_sw128(sB + s * kBStageBytes + ks * 32);
+              mma_bf16(d, da, db, (kc | ks) != 0);
+            }
+            mma_commit(b_empty + 8 * s);
+          }
+          if (ok) mma_commit(b_accf + 8 * b);
+        }
+        if (ok) mma_commit(b_aempty);
+      }
+      // All MMAs this thread issued are complete before TMEM is released.
+      mma_commit(b_done);
+      mbar_wait(b_done, 0, g.status, ST_TIMEOUT_DRAIN, false);
+    }
+    __syncwarp();
+  } else {
+    // ---------------------------------------------------------------- epilogue
+    const int quarter = warp & 3, half = warp >> 2;
+    const int et = threadIdx.x;  // 0..255: column this thread stages
+    uint32_t tile = 0;
+    bool ok = true;
+    for (int item = blockIdx.x; ok && item < g.n_items; item += gridDim.x) {
+      const int rb = item % g.n_rb, seg = item / g.n_rb;
+      const int ct0 = seg * g.ct_per_item, ct1 = min(ct0 + g.ct_per_item, g.n_ct);
+      const int row = rb * kBM + quarter * 32 + lane;
+      const RowState rs = make_row(g.params[row], g.ec);
+      const float rmax_r = g.tile_rmax[rb];
+      double acc_n = 0.0, acc_d = 0.0;
+      for (int ct = ct0; ok && ct < ct1; ct++, tile++) {
+        const uint32_t b = tile & 1;
+        const int col0 = ct * kBN;
+        {
+          const BlockParams cp = g.params[col0 + et];
+          ColTile& t = cols[b];
+          t.a[et] = cp.a;
+          t.r[et] = cp.r;
+          t.sigma[et] = cp.sigma;
+          t.mu[et] = cp.mu;
+        }
+        asm volatile("bar.sync 1, %0;" ::"r"(kEpiWarps * 32) : "memory");
+        if (!mbar_wait(b_accf + 8 * b, (tile >> 1) & 1, g.status, ST_TIMEOUT_EPI)) { ok = false; break; }
+        tc_fence_after();
+        const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + b * kBN + half * (kBN / 2);
+        const float cmax = fmaxf(g.tile_rmax[2 * ct], g.tile_rmax[2 * ct + 1]);
+        const bool exact = METRIC == kPearson && (kEps * rmax_r * cmax > kTFast);
+        const bool full = col0 + kBN <= g.ec.n;
+        float sn = 0.0f, sd = 0.0f;
+        const int cbase = half * (kBN / 2);
+        if (exact) {
+          if (full) epi_tile<METRIC, true, true>(taddr, cols[b], cbase, col0, rs, g.ec, sn, sd);
+          else epi_tile<METRIC, true, false>(taddr, cols[b], cbase, col0, rs, g.ec, sn, sd);
+        } else {
+          if (full) epi_tile<METRIC, false, true>(taddr, cols[b], cbase, col0, rs, g.ec, sn, sd);
+          else epi_tile<METRIC, false, false>(taddr, cols[b], cbase, col0, rs, g.ec, sn, sd);
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(b_acce + 8 * b);
+        acc_n += (double)sn;
+        acc_d += (double)sd;
+      }
+      if (ok && row < g.ec.n) {
+        atomicAdd(g.num + row, acc_n);
+        atomicAdd(g.den + row, acc_d);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == kEpiWarps + 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kBN) : "memory");
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+bool make_map(CUtensorMap* m, const __nv_bfloat16* ptr, int kq, int rows, int box_rows) {
+  auto enc = get_encode();
+  if (!enc) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)kq, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)kq * 2};
+  cuuint32_t box[2] = {(cuuint32_t)kChunk, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(ptr), dims, strides, box,
+                   estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int kq, int n_pad,
+                           const BlockParams* params, const float* tile_rmax, EpiConsts ec, double* num,
+                           double* den, int num_sms, int* status, cudaStream_t st) {
+  if (kq % 16 != 0 || n_pad % kBN != 0) return cudaErrorInvalidValue;
+  TcArgs g;
+  g.kq = kq;
+  g.nkc = (kq + kChunk - 1) / kChunk;
+  g.n_rb = n_pad / kBM;
+  g.n_ct = (ec.n + kBN - 1) / kBN;
+  const size_t fixed = 1024 + (size_t)g.nkc * kAChunkBytes + 2 * sizeof(ColTile) + 8 * 64;
+  const size_t budget = 227 * 1024;
+  if (fixed + 2 * kBStageBytes > budget) return cudaErrorInvalidValue;
+  g.stages = (int)std::min<size_t>(6, (budget - fixed) / kBStageBytes);
+  const size_t smem = fixed + (size_t)g.stages * kBStageBytes;
+  // Only row blocks that hold valid rows are work; split the column range so
+  // that every SM gets several items.
+  const int n_rb_valid = (ec.n + kBM - 1) / kBM;
+  int segs = (4 * num_sms + n_rb_valid - 1) / n_rb_valid;
+  segs = std::max(1, std::min(segs, g.n_ct));
+  g.ct_per_item = (g.n_ct + segs - 1) / segs;
+  segs = (g.n_ct + g.ct_per_item - 1) / g.ct_per_item;
+  g.n_rb = n_rb_valid;
+  g.n_items = g.n_rb * segs;
+  g.params = params;
+  g.tile_rmax = tile_rmax;
+  g.ec = ec;
+  g.num = num;
+  g.den = den;
+  g.status = status;
+  CUtensorMap mA, mB;
+  if (!make_map(&mA, A, kq, n_pad, kBM) || !make_map(&mB, B, kq, n_pad, kBN)) return cudaErrorInvalidValue;
+  const int grid = std::min(g.n_items, num_sms);
+  cudaError_t e;
+#define SRED_TC(M)                                                                                   \
+  e = cudaFuncSetAttribute(k_gram_tc<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);      \
+  if (e != cudaSuccess) return e;                                                                    \
+  k_gram_tc<M><<<grid, kThreads, smem, st>>>(mA, mB, g);
+  switch (ec.metric) {
+    case kPearson: SRED_TC(kPearson); break;
+    case kSsim: SRED_TC(kSsim); break;
+    case kNrmse: SRED_TC(kNrmse); break;
+    case kDebugDot: SRED_TC(kDebugDot); break;
+    default: return cudaErrorInvalidValue;
+  }
+#undef SRED_TC
+  return cudaGetLastError();
 }
 
 }  // namespace sred

@@ -312,6 +312,35 @@ __global__ void k_pack(const float* __restrict__ img, int W, Ellipse e, const in
   }
 }
 
+// Diagnostics: pack caller-given vectors (n x K, FP32) as operands without
+// normalising them (one warp per row).
+__global__ void k_pack_vectors(const float* __restrict__ u, int n, int K, int mode, float* __restrict__ U, int kp,
+                               __nv_bfloat16* __restrict__ A, __nv_bfloat16* __restrict__ B, int kq) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int j = gw; j < n; j += nw) {
+    if (mode == 0) {
+      for (int i = lane; i < kp; i += 32) U[(size_t)j * kp + i] = i < K ? u[(size_t)j * K + i] : 0.0f;
+    } else {
+      for (int i = lane; i < kq; i += 32) {
+        A[(size_t)j * kq + i] = __float2bfloat16_rn(0.0f);
+        B[(size_t)j * kq + i] = __float2bfloat16_rn(0.0f);
+      }
+      __syncwarp();
+      for (int i = lane; i < K; i += 32) {
+        const float x = u[(size_t)j * K + i];
+        const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+        __nv_bfloat16* a = A + (size_t)j * kq;
+        __nv_bfloat16* b = B + (size_t)j * kq;
+        a[i] = hi; a[K + i] = lo; a[2 * K + i] = hi;
+        b[i] = hi; b[K + i] = hi; b[2 * K + i] = lo;
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Finalisation, java/CLUtils.java:1747-1770, :1998-2027, :2127-2156:
 // out = num / (den * nPixels + eps) (FP64 here), the NRMSE / Abs-diff
@@ -344,9 +373,10 @@ __global__ void k_finalize(const int* __restrict__ slot, int W, int H, int rw, i
       else if (metric == kNrmse) nu = sums[1];
       else nu = sums[2];
     }
-    double r = nu / (de * n_pixels + (double)kEps);
-    o = (float)r;
-    if ((metric == kNrmse || metric == kAbsDiff) && mask[p] > 0.0f) o = (r == 0.0) ? 1.0f : (float)(1.0 / r);
+    o = (float)(nu / (de * n_pixels + (double)kEps));
+    // Inversion of the FP32 value, as java/CLUtils.java:1998-2010 does it
+    // (a value that rounds to 0 becomes 1, a denormal becomes inf).
+    if ((metric == kNrmse || metric == kAbsDiff) && mask[p] > 0.0f) o = (o == 0.0f) ? 1.0f : __fdiv_rn(1.0f, o);
     if (apply_mask) o = __fmul_rn(o, mask[p]);
   }
   out[p] = o;

@@ -635,6 +635,63 @@ sred_status sred_block_map_2d_device(sred_ctx* c, const char* metric, const floa
                     d_out, pick(c, stream));
 }
 
+sred_status sred_debug_gram_rowdot(sred_ctx* c, int engine, const float* u, const float* w1, const float* w2, int n,
+                                   int k, double* num, double* den) {
+  if (!c || !u || !w1 || !w2 || !num || !den || n <= 0 || k <= 0 || k > kMaxK) return SRED_ERR_ARG;
+  if (engine != SRED_ENGINE_TC && engine != SRED_ENGINE_FP32) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  cudaStream_t st = c->stream;
+  const size_t n_pad = round_up((size_t)n, 256);
+  const int kp = (int)round_up(k, 4), kq = (int)round_up(3 * k, 16);
+  float *d_u, *d_U = nullptr, *d_rmax;
+  __nv_bfloat16 *d_A = nullptr, *d_B = nullptr;
+  BlockParams* d_params;
+  double *d_num, *d_den;
+  CKS(ensure(c, B_IMG, (size_t)n * k, &d_u));
+  CKS(ensure(c, B_PARAMS, n_pad, &d_params));
+  CKS(ensure(c, B_RMAX, n_pad / 128, &d_rmax));
+  CKS(ensure(c, B_NUM, n_pad, &d_num));
+  CKS(ensure(c, B_DEN, n_pad, &d_den));
+  if (engine == SRED_ENGINE_FP32) {
+    CKS(ensure(c, B_U, n_pad * kp, &d_U));
+    CK(cudaMemsetAsync(d_U, 0, n_pad * kp * sizeof(float), st));
+  } else {
+    CKS(ensure(c, B_A, n_pad * kq, &d_A));
+    CKS(ensure(c, B_B, n_pad * kq, &d_B));
+    CK(cudaMemsetAsync(d_A, 0, n_pad * kq * sizeof(__nv_bfloat16), st));
+    CK(cudaMemsetAsync(d_B, 0, n_pad * kq * sizeof(__nv_bfloat16), st));
+  }
+  std::vector<BlockParams> hp(n_pad);
+  std::memset(hp.data(), 0, n_pad * sizeof(BlockParams));
+  for (int i = 0; i < n; i++) { hp[i].a = w1[i]; hp[i].r = w2[i]; }
+  CK(cudaMemcpyAsync(d_u, u, (size_t)n * k * sizeof(float), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_params, hp.data(), n_pad * sizeof(BlockParams), cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(d_rmax, 0, (n_pad / 128) * sizeof(float), st));
+  CK(cudaMemsetAsync(d_num, 0, n_pad * sizeof(double), st));
+  CK(cudaMemsetAsync(d_den, 0, n_pad * sizeof(double), st));
+  k_pack_vectors<<<grid_for((size_t)n * 32, 256, 8 * c->num_sms), 256, 0, st>>>(
+      d_u, n, k, engine == SRED_ENGINE_FP32 ? 0 : 1, d_U, kp, d_A, d_B, kq);
+  CK(cudaGetLastError());
+  EpiConsts ec{kDebugDot, n, 1.0f, kC1, kC2};
+  if (engine == SRED_ENGINE_FP32) {
+    CK(launch_gram_fp32(d_U, kp, d_params, d_rmax, ec, d_num, d_den, c->num_sms, st));
+  } else {
+    int* d_status;
+    CKS(ensure(c, B_STATUS, 4, &d_status));
+    CK(cudaMemsetAsync(d_status, 0, 4 * sizeof(int), st));
+    CK(launch_gram_tc(d_A, d_B, kq, (int)n_pad, d_params, d_rmax, ec, d_num, d_den, c->num_sms, d_status, st));
+    int status = 0;
+    CK(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (status) return fail(c, SRED_ERR_TIMEOUT, "tensor-core pipeline wait exceeded its bound");
+  }
+  CK(cudaMemcpyAsync(num, d_num, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(den, d_den, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return SRED_OK;
+}
+
 // java/Utils.java:557-639 on host memory (ImageJ's float conversion is the caller's).
 sred_status sred_reference_block_2d(const float* blk, int bw, int bh, float* pixels, int* block_size, float* mean,
                                     float* std_out) {

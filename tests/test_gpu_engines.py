@@ -1,0 +1,66 @@
+"""The two contraction engines on caller-given vectors, through the C ABI.
+
+num[p] = sum_q <u_p, u_q> w1[q] and den[p] = sum_q w2[q] are checked
+against an FP64 evaluation for every K' chunk count the tensor-core engine
+uses (K' = round_up(3K, 16) from 16 to 448) and for ragged N (partial row
+blocks and column tiles). Bound: |err| <= tol * sum_q |G_pq w1_q| with
+tol = 2e-6 for the FP32 engine and 4e-5 for split-BF16 (the omitted lo*lo
+term and bf16 rounding of lo are below 2^-15 of |u_p||u_q|).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from sred_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+TOL = {"fp32": 2e-6, "tc": 4e-5}
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return _lib.Context(0, "fp32")
+
+
+def rowdot(ctx, engine, u, w1, w2):
+    n, k = u.shape
+    num = np.zeros(n, np.float64)
+    den = np.zeros(n, np.float64)
+    e = {"tc": _lib.ENGINE_TC, "fp32": _lib.ENGINE_FP32}[engine]
+    ctx.check(ctx._L.sred_debug_gram_rowdot(ctx.h, e, np.ascontiguousarray(u, np.float32),
+                                            np.ascontiguousarray(w1, np.float32),
+                                            np.ascontiguousarray(w2, np.float32), n, k, num, den),
+              "sred_debug_gram_rowdot")
+    return num, den
+
+
+@pytest.mark.parametrize("engine", ["fp32", "tc"])
+@pytest.mark.parametrize("n,k", [(1, 5), (100, 5), (300, 13), (1000, 49), (777, 81), (513, 113), (260, 149)])
+def test_rowdot_matches_fp64(ctx, engine, n, k):
+    rng = np.random.default_rng(n * 1000 + k)
+    u = rng.normal(size=(n, k)).astype(np.float32)
+    u /= np.linalg.norm(u, axis=1, keepdims=True).astype(np.float32)
+    w1 = rng.uniform(-1, 1, n).astype(np.float32)
+    w2 = rng.uniform(0, 1, n).astype(np.float32)
+    num, den = rowdot(ctx, engine, u, w1, w2)
+    U = u.astype(np.float64)
+    G = U @ U.T
+    exp = G @ w1.astype(np.float64)
+    scale = np.abs(G) @ np.abs(w1.astype(np.float64))
+    err = np.abs(num - exp) / np.maximum(scale, 1e-30)
+    assert float(err.max()) <= TOL[engine], float(err.max())
+    np.testing.assert_allclose(den, np.full(n, w2.astype(np.float64).sum()), rtol=1e-6)
+
+
+def test_tc_matches_fp32_unnormalised(ctx):
+    """Vectors of mixed magnitude (the engine must not assume unit norm)."""
+    rng = np.random.default_rng(5)
+    n, k = 700, 49
+    u = (rng.normal(size=(n, k)) * rng.uniform(0.01, 10, (n, 1))).astype(np.float32)
+    w1 = rng.uniform(0, 1, n).astype(np.float32)
+    a, _ = rowdot(ctx, "fp32", u, w1, w1)
+    b, _ = rowdot(ctx, "tc", u, w1, w1)
+    U = u.astype(np.float64)
+    scale = np.abs(U @ U.T) @ w1.astype(np.float64)
+    assert float(np.max(np.abs(a - b) / scale)) <= TOL["tc"]
