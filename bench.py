@@ -126,7 +126,11 @@ def sum_over_ranks(x: float, world: int) -> float:
 
 def image(seed: int) -> np.ndarray:
     from sred_b200 import synth
-    return synth.normalize_input(synth.image_1024_spots_random(seed=seed))
+    if W_IMG == 1024 and H_IMG == 1024:
+        return synth.normalize_input(synth.image_1024_spots_random(seed=seed))
+    # Same spot density and layout at another side (used for profiling captures).
+    return synth.normalize_input(synth.spot_image(W_IMG, H_IMG, max(2, W_IMG * 80 // 1024), seed=seed,
+                                                  random_fraction=0.3))
 
 
 def time_engine(ctx, engine, d_img, d_out, flush, steps, warmup, stream):
@@ -331,7 +335,14 @@ def main():
     ap.add_argument("--engine", choices=["tc", "fp32"], default="tc")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP32-engine comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", type=int, default=1024,
+                    help="image side (default 1024, the benchmark workload; smaller sides for profiling)")
     args = ap.parse_args()
+    global W_IMG, H_IMG, WORKLOAD
+    if args.size != 1024:
+        W_IMG = H_IMG = args.size
+        WORKLOAD = WORKLOAD.replace("1024x1024", f"{args.size}x{args.size}").replace(
+            "80x80 lattice", f"{max(2, args.size * 80 // 1024)}x{max(2, args.size * 80 // 1024)} lattice")
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))

@@ -17,6 +17,8 @@
 // |x_p|^2 + |x_q|^2 - 2<x_p, x_q> never cancels in FP32.
 // 1/(1+t) is evaluated as 1 - t + t^2 when the tile's largest t is below
 // 2^-8 (relative error < t^3 < 6e-8), exactly otherwise.
+// The self pair (q == p) uses G = 1 exactly, as the reference's direct
+// evaluation gives; only tiles that contain the diagonal check for it.
 #pragma once
 #include "common.cuh"
 
@@ -31,7 +33,7 @@ __device__ __forceinline__ float ex2_approx(float x) {
 }
 
 struct RowState {
-  float a, e, sigma, mu;
+  float a, e, r, sigma, mu;
   float mu2x2;   // 2 mu_p
   float mumu;    // mu_p^2
   float s2;      // sigma_p^2 + c2
@@ -42,6 +44,7 @@ __device__ __forceinline__ RowState make_row(const BlockParams& bp, const EpiCon
   RowState r;
   r.a = bp.a;
   r.e = bp.e;
+  r.r = bp.r;
   r.sigma = bp.sigma;
   r.mu = bp.mu;
   r.mu2x2 = 2.0f * bp.mu;

@@ -48,7 +48,7 @@ __device__ __forceinline__ void load_tile_t(float* S, const float* __restrict__ 
   }
 }
 
-template <int METRIC, bool EXACT, bool FULL>
+template <int METRIC, bool EXACT, bool FULL, bool DIAG>
 __device__ __forceinline__ void tile_epilogue(const float (&acc)[TM][TM], const BlockParams* __restrict__ rowp,
                                               const BlockParams* __restrict__ colp, int row0, int col0,
                                               const EpiConsts& ec, float (&rn)[TM], float (&rd)[TM]) {
@@ -60,12 +60,13 @@ __device__ __forceinline__ void tile_epilogue(const float (&acc)[TM][TM], const 
 #pragma unroll
     for (int j = 0; j < TM; j++) {
       const int c = tx * TM + j;
-      if (FULL || col0 + c < ec.n) epi_pair<METRIC, EXACT>(acc[i][j], rs, colp[c], ec, sn, sd);
+      float G = acc[i][j];
+      if (DIAG && col0 + c == row0 + ty * TM + i && rs.r > 0.0f) G = 1.0f;
+      if (FULL || col0 + c < ec.n) epi_pair<METRIC, EXACT>(G, rs, colp[c], ec, sn, sd);
     }
     rn[i] += sn;
     rd[i] += sd;
   }
-  (void)row0;
 }
 
 template <int METRIC>
@@ -122,13 +123,10 @@ __global__ void __launch_bounds__(NT, 2) k_gram_fp32(Fp32Args g) {
       }
       const bool full = col0 + BM <= g.ec.n;
       const bool exact = METRIC == kPearson && (kEps * rmax_r * g.tile_rmax[ct] > kTFast);
-      if (exact) {
-        if (full) tile_epilogue<METRIC, true, true>(acc, Ap, Bp, row0, col0, g.ec, rn, rd);
-        else tile_epilogue<METRIC, true, false>(acc, Ap, Bp, row0, col0, g.ec, rn, rd);
-      } else {
-        if (full) tile_epilogue<METRIC, false, true>(acc, Ap, Bp, row0, col0, g.ec, rn, rd);
-        else tile_epilogue<METRIC, false, false>(acc, Ap, Bp, row0, col0, g.ec, rn, rd);
-      }
+      const bool diag = (ct == rb);
+      if (full && !exact && !diag) tile_epilogue<METRIC, false, true, false>(acc, Ap, Bp, row0, col0, g.ec, rn, rd);
+      else if (exact) tile_epilogue<METRIC, true, false, true>(acc, Ap, Bp, row0, col0, g.ec, rn, rd);
+      else tile_epilogue<METRIC, false, false, true>(acc, Ap, Bp, row0, col0, g.ec, rn, rd);
     }
     // Reduce row partials over the 16 column-threads of each row group
     // (lanes tx = 0..15 of a half-warp), then one FP64 atomic per row.

@@ -177,8 +177,8 @@ struct ColTile {
   float mu[kBN];
 };
 
-template <int METRIC, bool EXACT, bool FULL>
-__device__ __forceinline__ void epi_tile(uint32_t taddr, const ColTile& ct, int cbase, int col0,
+template <int METRIC, bool EXACT, bool FULL, bool DIAG>
+__device__ __forceinline__ void epi_tile(uint32_t taddr, const ColTile& ct, int cbase, int col0, int row,
                                          const RowState& rs, const EpiConsts& ec, float& sn, float& sd) {
 #pragma unroll 1
   for (int c = 0; c < kBN / 2; c += 32) {
@@ -203,7 +203,9 @@ __device__ __forceinline__ void epi_tile(uint32_t taddr, const ColTile& ct, int 
         cq.r = rv[u];
         cq.sigma = sv[u];
         cq.mu = mv[u];
-        if (FULL || col0 + q + u < ec.n) epi_pair<METRIC, EXACT>(__uint_as_float(v[j + u]), rs, cq, ec, sn, sd);
+        float G = __uint_as_float(v[j + u]);
+        if (DIAG && col0 + q + u == row && rs.r > 0.0f) G = 1.0f;
+        if (FULL || col0 + q + u < ec.n) epi_pair<METRIC, EXACT>(G, rs, cq, ec, sn, sd);
       }
     }
   }
@@ -346,12 +348,13 @@ __global__ void __launch_bounds__(kThreads, 1)
         const bool full = col0 + kBN <= g.ec.n;
         float sn = 0.0f, sd = 0.0f;
         const int cbase = half * (kBN / 2);
-        if (exact) {
-          if (full) epi_tile<METRIC, true, true>(taddr, cols[b], cbase, col0, rs, g.ec, sn, sd);
-          else epi_tile<METRIC, true, false>(taddr, cols[b], cbase, col0, rs, g.ec, sn, sd);
+        const bool diag = (ct == (rb >> 1));
+        if (full && !exact && !diag) {
+          epi_tile<METRIC, false, true, false>(taddr, cols[b], cbase, col0, row, rs, g.ec, sn, sd);
+        } else if (exact) {
+          epi_tile<METRIC, true, false, true>(taddr, cols[b], cbase, col0, row, rs, g.ec, sn, sd);
         } else {
-          if (full) epi_tile<METRIC, false, true>(taddr, cols[b], cbase, col0, rs, g.ec, sn, sd);
-          else epi_tile<METRIC, false, false>(taddr, cols[b], cbase, col0, rs, g.ec, sn, sd);
+          epi_tile<METRIC, false, false, true>(taddr, cols[b], cbase, col0, row, rs, g.ec, sn, sd);
         }
         tc_fence_before();
         __syncwarp();
