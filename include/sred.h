@@ -141,6 +141,23 @@ sred_status sred_reference_block_2d(const float *block_img, int bw, int bh, floa
 sred_status sred_normalize_image_2d(float *img, int w, int h, int border_w, int border_h,
                                     const float *mask);
 
+/* Block map that allocates nothing (no counterpart in the reference): for
+ * callers that cannot call cudaMalloc, such as code inside a CUDA graph being
+ * captured, hosts whose runtime owns the device allocator, or loops that must
+ * not touch the allocator once started. Same result as
+ * sred_block_map_2d_device with relevance_constant 0; needs no context.
+ * Runs on the current device and on `stream` (NULL = the default stream) and
+ * returns when the map is complete. Scratch is a fixed device array of about
+ * 4 MiB that every GPU loading this library holds until exit; the limits are
+ * frames <= 4096 and, for NRMSE, frames * w * h <= 1,048,576
+ * (SRED_ERR_ARG beyond them). The first call on a device looks the array's
+ * device address up (make that first call before any stream capture). Every
+ * call shares the array, so calls that overlap on the GPU race. */
+sred_status sred_block_map_2d_device_noalloc(const char *metric, const float *d_img, int w, int h,
+                                             int frames, const float *ref_pixels, int block_size, int bw,
+                                             int bh, float ref_mean, float ref_std, int normalize_output,
+                                             float *d_out, void *stream);
+
 /* Diagnostics of the contraction engines (no counterpart in the reference):
  * for caller-given vectors u (n x k, row-major) and column weights w1, w2,
  * num[p] = sum_q <u_p, u_q> w1[q] and den[p] = sum_q w2[q], computed by the

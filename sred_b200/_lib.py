@@ -23,7 +23,7 @@ EXPORTS = [
     "sred_block_size", "sred_local_statistics_2d", "sred_mean_noise_var_2d", "sred_relevance_mask_2d",
     "sred_calculate_global_repetition_map_2d", "sred_global_map_2d", "sred_global_map_2d_device",
     "sred_calculate_block_repetition_map_2d", "sred_block_map_2d_device", "sred_reference_block_2d",
-    "sred_normalize_image_2d", "sred_debug_gram_rowdot",
+    "sred_normalize_image_2d", "sred_debug_gram_rowdot", "sred_block_map_2d_device_noalloc",
 ]
 
 
@@ -89,6 +89,8 @@ def load() -> C.CDLL:
         L.sred_normalize_image_2d.argtypes = [_f32p, s, s, s, s, _vp]
         _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
         L.sred_debug_gram_rowdot.argtypes = [_vp, s, _f32p, _f32p, _f32p, s, s, _f64p, _f64p]
+        L.sred_block_map_2d_device_noalloc.argtypes = [C.c_char_p, _vp, s, s, s, _f32p, s, s, s, C.c_float,
+                                                       C.c_float, s, _vp, _vp]
         _lib = L
     return _lib
 
