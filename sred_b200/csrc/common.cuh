@@ -54,10 +54,16 @@ struct EpiConsts {
 cudaError_t launch_gram_fp32(const float* U, int kp, const BlockParams* params, const float* tile_rmax,
                              EpiConsts ec, double* num, double* den, int num_sms, cudaStream_t st);
 
+// Column parameters of one 256-column tile, structure of arrays, as the
+// tensor-core engine copies them into shared memory:
+//   [a x256 | r x256 | sigma x256 | mu x256 | max r of the tile | 3 x pad]
+constexpr int kColSoaFloats = 4 * 256 + 4;
+
 // Launch the split-BF16 tcgen05 all-pairs kernel (global_tc.cu).
-// A, B: n_pad x kq bf16 ([hi|lo|hi] and [hi|hi|lo]).
+// A, B: n_pad x kq bf16 ([hi|lo|hi] and [hi|hi|lo]); colsoa: n_pad/256 tiles
+// of kColSoaFloats (k_col_soa).
 cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int kq, int n_pad,
-                           const BlockParams* params, const float* tile_rmax, EpiConsts ec,
+                           const BlockParams* params, const float* colsoa, const float* tile_rmax, EpiConsts ec,
                            double* num, double* den, int num_sms, int* status, cudaStream_t st);
 
 }  // namespace sred

@@ -15,8 +15,8 @@
 //   Abs-diff          = |sigma_p - sigma_q| * weight
 // The NRMSE form uses the normalised vectors, so the large common part of
 // |x_p|^2 + |x_q|^2 - 2<x_p, x_q> never cancels in FP32.
-// 1/(1+t) is evaluated as 1 - t + t^2 when the tile's largest t is below
-// 2^-8 (relative error < t^3 < 6e-8), exactly otherwise.
+// 1/(1+t) is evaluated to first or second order, or exactly, according to the
+// tile's largest t (c_mode below), with relative error below 6e-8.
 // The self pair (q == p) uses G = 1 exactly, as the reference's direct
 // evaluation gives; only tiles that contain the diagonal check for it.
 #pragma once
@@ -54,8 +54,20 @@ __device__ __forceinline__ RowState make_row(const BlockParams& bp, const EpiCon
   return r;
 }
 
-// One pair. EXACT selects the exact 1/(1+t) (Pearson only).
-template <int METRIC, bool EXACT>
+// Evaluation of the Pearson factor 1/(1+t), chosen per tile from the tile's
+// largest t = eps / (sigma_p sigma_q):
+//   kCFirst  t < 2^-13: G (1 - t)          (relative error t^2 < 1.5e-8)
+//   kCSecond t < 2^-8:  G (1 - t + t^2)    (relative error t^3 < 6e-8)
+//   kCExact  otherwise: G / (1 + t)
+enum { kCFirst = 0, kCSecond = 1, kCExact = 2 };
+constexpr float kTFirst = 1.0f / 8192.0f;
+
+__device__ __forceinline__ int c_mode(float tmax) {
+  return tmax < kTFirst ? kCFirst : (tmax < kTFast ? kCSecond : kCExact);
+}
+
+// One pair; CMODE is used by Pearson only.
+template <int METRIC, int CMODE>
 __device__ __forceinline__ void epi_pair(float G, const RowState& rp, const BlockParams& cq,
                                          const EpiConsts& ec, float& sn, float& sd) {
   if (METRIC == kDebugDot) {
@@ -67,11 +79,16 @@ __device__ __forceinline__ void epi_pair(float G, const RowState& rp, const Bloc
   const float w = ex2_approx(-d * d);
   sd += w;
   if (METRIC == kPearson) {
-    const float t = rp.e * cq.r;
-    float c;
-    if (EXACT) c = __frcp_rn(1.0f + t);
-    else c = fmaf(t, t - 1.0f, 1.0f);
-    sn = fmaf(fmaxf(G * c, 0.0f), w, sn);
+    float gc;
+    if (CMODE == kCFirst) {
+      gc = fmaf(-G * rp.e, cq.r, G);
+    } else if (CMODE == kCSecond) {
+      const float t = rp.e * cq.r;
+      gc = G * fmaf(t, t - 1.0f, 1.0f);
+    } else {
+      gc = G * __frcp_rn(1.0f + rp.e * cq.r);
+    }
+    sn = fmaf(fmaxf(gc, 0.0f), w, sn);
   } else if (METRIC == kSsim) {
     const float num = fmaf(rp.mu2x2, cq.mu, ec.c1) * fmaf(rp.sig2x * cq.sigma, G, ec.c2);
     const float den = fmaf(rp.mumu, cq.mu * cq.mu, ec.c1) * fmaf(cq.sigma, cq.sigma, rp.s2);

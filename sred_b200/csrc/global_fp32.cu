@@ -48,7 +48,7 @@ __device__ __forceinline__ void load_tile_t(float* S, const float* __restrict__ 
   }
 }
 
-template <int METRIC, bool EXACT, bool FULL, bool DIAG>
+template <int METRIC, int CMODE, bool FULL, bool DIAG>
 __device__ __forceinline__ void tile_epilogue(const float (&acc)[TM][TM], const BlockParams* __restrict__ rowp,
                                               const BlockParams* __restrict__ colp, int row0, int col0,
                                               const EpiConsts& ec, float (&rn)[TM], float (&rd)[TM]) {
@@ -62,7 +62,7 @@ __device__ __forceinline__ void tile_epilogue(const float (&acc)[TM][TM], const 
       const int c = tx * TM + j;
       float G = acc[i][j];
       if (DIAG && col0 + c == row0 + ty * TM + i && rs.r > 0.0f) G = 1.0f;
-      if (FULL || col0 + c < ec.n) epi_pair<METRIC, EXACT>(G, rs, colp[c], ec, sn, sd);
+      if (FULL || col0 + c < ec.n) epi_pair<METRIC, CMODE>(G, rs, colp[c], ec, sn, sd);
     }
     rn[i] += sn;
     rd[i] += sd;
@@ -122,11 +122,18 @@ __global__ void __launch_bounds__(NT, 2) k_gram_fp32(Fp32Args g) {
         }
       }
       const bool full = col0 + BM <= g.ec.n;
-      const bool exact = METRIC == kPearson && (kEps * rmax_r * g.tile_rmax[ct] > kTFast);
+      const int cm = METRIC == kPearson ? c_mode(kEps * rmax_r * g.tile_rmax[ct]) : kCFirst;
       const bool diag = (ct == rb);
-      if (full && !exact && !diag) tile_epilogue<METRIC, false, true, false>(acc, Ap, Bp, row0, col0, g.ec, rn, rd);
-      else if (exact) tile_epilogue<METRIC, true, false, true>(acc, Ap, Bp, row0, col0, g.ec, rn, rd);
-      else tile_epilogue<METRIC, false, false, true>(acc, Ap, Bp, row0, col0, g.ec, rn, rd);
+      if (full && !diag && cm == kCFirst)
+        tile_epilogue<METRIC, kCFirst, true, false>(acc, Ap, Bp, row0, col0, g.ec, rn, rd);
+      else if (full && !diag && cm == kCSecond)
+        tile_epilogue<METRIC, kCSecond, true, false>(acc, Ap, Bp, row0, col0, g.ec, rn, rd);
+      else if (cm == kCFirst)
+        tile_epilogue<METRIC, kCFirst, false, true>(acc, Ap, Bp, row0, col0, g.ec, rn, rd);
+      else if (cm == kCSecond)
+        tile_epilogue<METRIC, kCSecond, false, true>(acc, Ap, Bp, row0, col0, g.ec, rn, rd);
+      else
+        tile_epilogue<METRIC, kCExact, false, true>(acc, Ap, Bp, row0, col0, g.ec, rn, rd);
     }
     // Reduce row partials over the 16 column-threads of each row group
     // (lanes tx = 0..15 of a half-warp), then one FP64 atomic per row.

@@ -8,15 +8,19 @@
 //
 // CTA = 1 per SM, persistent over work items (128-row block, range of
 // 256-column tiles). Warp roles:
-//   warp 8      TMA producer: the item's A tile (resident, all K' chunks) and
+//   warp 16     TMA producer: the item's A tile (resident, all K' chunks) and
 //               a ring of B stages (one 256 x 64 bf16 chunk each, SWIZZLE_128B)
-//   warp 9      MMA issuer (one thread): tcgen05.mma M=128 N=256 K=16 into one
-//               of two TMEM accumulators (2 x 256 columns), tcgen05.commit to
-//               release B stages and to publish finished accumulators
-//   warps 0-7   epilogue: tcgen05.ld of the accumulator (warp w reads TMEM
-//               lanes 32(w%4).. and columns 128(w/4)..), the fused per-pair
+//   warp 17     MMA issuer (one thread): on claiming one of two TMEM
+//               accumulators (2 x 256 columns) it bulk-copies the tile's
+//               column parameters (4 KB) into the matching shared slot, then
+//               issues tcgen05.mma M=128 N=256 K=16 and tcgen05.commit to
+//               release B stages and to publish the finished accumulator
+//   warps 0-15  epilogue: tcgen05.ld of the accumulator (warp w reads TMEM
+//               lanes 32(w%4).. and columns 64(w/4)..), the fused per-pair
 //               metric (epilogue.cuh), row sums in registers; FP64 atomics
-//               per row per item. The N x N matrix is never stored.
+//               per row per item. The N x N matrix is never stored. Epilogue
+//               warps synchronise only through mbarriers, so they drift and
+//               overlap each other's TMEM-load latency.
 // Every mbarrier wait is bounded by wall time; on expiry the kernel records a
 // status code, stops issuing work, waits (bounded) for its own copies in
 // flight, frees TMEM and returns. No TMA multicast is used.
@@ -32,11 +36,14 @@ namespace {
 
 constexpr int kBM = 128;          // rows per tile (TMEM lanes)
 constexpr int kBN = 256;          // columns per tile
-constexpr int kChunk = 64;        // bf16 elements per K chunk (128 B, one swizzle atom row)
+constexpr int kChunk = 64;        // bf16 elements per K chunk (128 B, one SWIZZLE_128B atom row)
 constexpr int kAChunkBytes = kBM * kChunk * 2;   // 16 KB
 constexpr int kBStageBytes = kBN * kChunk * 2;   // 32 KB
-constexpr int kEpiWarps = 8;
+constexpr int kMaxStages = 16;
+constexpr int kEpiWarps = 16;                       // 4 per SM sub-partition
+constexpr int kColsPerWarp = kBN / (kEpiWarps / 4);  // 64: each warp reads 32 lanes x 64 columns
 constexpr int kThreads = (kEpiWarps + 2) * 32;
+constexpr int kSoaBytes = kColSoaFloats * 4;         // one tile's column parameters
 constexpr unsigned long long kTimeoutNs = 4000000000ull;  // 4 s per wait
 
 enum { ST_OK = 0, ST_TIMEOUT_PRODUCER = 1, ST_TIMEOUT_MMA = 2, ST_TIMEOUT_EPI = 3, ST_TIMEOUT_DRAIN = 4 };
@@ -45,6 +52,7 @@ struct TcArgs {
   int kq, nkc, stages;
   int n_rb, n_ct, ct_per_item, n_items;
   const BlockParams* params;
+  const float* colsoa;
   const float* tile_rmax;
   EpiConsts ec;
   double* num;
@@ -88,9 +96,9 @@ __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
 
 // Bounded wait for the phase with the given parity. Returns false (and
 // records `code`) if the wait exceeded kTimeoutNs or another role of any CTA
-// already gave up.
-// Drain waits (for copies or MMAs this CTA issued) pass abort = false: they
-// keep waiting, within the same bound, after another role has given up.
+// already gave up. Drain waits (for copies or MMAs this CTA issued) pass
+// abort = false: they keep waiting, within the same bound, after another
+// role has given up.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* status, int code,
                                           bool abort = true) {
   if (mbar_test(bar, parity)) return true;
@@ -115,7 +123,15 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
       : "memory");
 }
 
-// Shared-memory matrix descriptor: K-major, SWIZZLE_128B, 8-row groups 1024 B apart.
+// Plain bulk copy (no tensor map): 16-byte aligned addresses, size a multiple of 16.
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, SWIZZLE_128B (128-byte rows),
+// 8-row groups 1024 B apart.
 __device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
   uint64_t d = 0;
   d |= static_cast<uint64_t>((saddr & 0x3FFFFu) >> 4);
@@ -147,68 +163,77 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// 32 lanes x 32 columns of 32-bit accumulator; the wait is fused with a
-// register dependency so no use of v can be scheduled before it.
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+// Issue a load of 32 lanes x 16 columns of 32-bit accumulator (no wait).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
       : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
-        "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
       : "r"(taddr)
       : "memory");
+}
+
+// Wait for every TMEM load this thread issued; the register operands tie
+// later uses of v to the wait, so none is scheduled before it.
+__device__ __forceinline__ void tmem_wait(uint32_t (&v)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;"
                : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
                  "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]),
-                 "+r"(v[15]), "+r"(v[16]), "+r"(v[17]), "+r"(v[18]), "+r"(v[19]), "+r"(v[20]), "+r"(v[21]),
-                 "+r"(v[22]), "+r"(v[23]), "+r"(v[24]), "+r"(v[25]), "+r"(v[26]), "+r"(v[27]), "+r"(v[28]),
-                 "+r"(v[29]), "+r"(v[30]), "+r"(v[31])
+                 "+r"(v[15])
                :
                : "memory");
 }
 
-// Column parameters of one tile, structure-of-arrays in shared memory.
-struct ColTile {
-  float a[kBN];
-  float r[kBN];
-  float sigma[kBN];
-  float mu[kBN];
-};
-
-template <int METRIC, bool EXACT, bool FULL, bool DIAG>
-__device__ __forceinline__ void epi_tile(uint32_t taddr, const ColTile& ct, int cbase, int col0, int row,
-                                         const RowState& rs, const EpiConsts& ec, float& sn, float& sd) {
-#pragma unroll 1
-  for (int c = 0; c < kBN / 2; c += 32) {
-    uint32_t v[32];
-    tmem_ld32(taddr + c, v);
+// 16 pairs: accumulator columns c0..c0+15 of this thread's row against the
+// columns' parameters in the shared-memory slot (structure of arrays).
+template <int METRIC, int CMODE, bool FULL, bool DIAG>
+__device__ __forceinline__ void epi_chunk(const uint32_t (&v)[16], const float* __restrict__ soa, int c0, int col0,
+                                          int row, const RowState& rs, const EpiConsts& ec, float& sn, float& sd) {
 #pragma unroll
-    for (int j = 0; j < 32; j += 4) {
-      const int q = cbase + c + j;
-      const float4 a4 = *reinterpret_cast<const float4*>(&ct.a[q]);
-      const float4 r4 = *reinterpret_cast<const float4*>(&ct.r[q]);
-      float4 s4 = make_float4(0.f, 0.f, 0.f, 0.f), m4 = s4;
-      if (METRIC != kPearson) s4 = *reinterpret_cast<const float4*>(&ct.sigma[q]);
-      if (METRIC == kSsim) m4 = *reinterpret_cast<const float4*>(&ct.mu[q]);
-      const float av[4] = {a4.x, a4.y, a4.z, a4.w};
-      const float rv[4] = {r4.x, r4.y, r4.z, r4.w};
-      const float sv[4] = {s4.x, s4.y, s4.z, s4.w};
-      const float mv[4] = {m4.x, m4.y, m4.z, m4.w};
+  for (int j = 0; j < 16; j += 4) {
+    const int q = c0 + j;
+    const float4 a4 = *reinterpret_cast<const float4*>(soa + q);
+    const float4 r4 = *reinterpret_cast<const float4*>(soa + kBN + q);
+    float4 s4 = make_float4(0.f, 0.f, 0.f, 0.f), m4 = s4;
+    if (METRIC != kPearson && METRIC != kDebugDot) s4 = *reinterpret_cast<const float4*>(soa + 2 * kBN + q);
+    if (METRIC == kSsim) m4 = *reinterpret_cast<const float4*>(soa + 3 * kBN + q);
+    const float av[4] = {a4.x, a4.y, a4.z, a4.w};
+    const float rv[4] = {r4.x, r4.y, r4.z, r4.w};
+    const float sv[4] = {s4.x, s4.y, s4.z, s4.w};
+    const float mv[4] = {m4.x, m4.y, m4.z, m4.w};
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        BlockParams cq;
-        cq.a = av[u];
-        cq.r = rv[u];
-        cq.sigma = sv[u];
-        cq.mu = mv[u];
-        float G = __uint_as_float(v[j + u]);
-        if (DIAG && col0 + q + u == row && rs.r > 0.0f) G = 1.0f;
-        if (FULL || col0 + q + u < ec.n) epi_pair<METRIC, EXACT>(G, rs, cq, ec, sn, sd);
-      }
+    for (int u = 0; u < 4; u++) {
+      BlockParams cq;
+      cq.a = av[u];
+      cq.r = rv[u];
+      cq.sigma = sv[u];
+      cq.mu = mv[u];
+      float G = __uint_as_float(v[j + u]);
+      if (DIAG && col0 + q + u == row && rs.r > 0.0f) G = 1.0f;
+      if (FULL || col0 + q + u < ec.n) epi_pair<METRIC, CMODE>(G, rs, cq, ec, sn, sd);
     }
   }
+}
+
+// One warp's 64 columns of a tile in four 16-column chunks: each chunk's TMEM
+// load is in flight while the previous chunk is evaluated.
+template <int METRIC, int CMODE, bool FULL, bool DIAG>
+__device__ __forceinline__ void epi_tile(uint32_t taddr, const float* __restrict__ soa, int cbase, int col0, int row,
+                                         const RowState& rs, const EpiConsts& ec, float& sn, float& sd) {
+  uint32_t v0[16], v1[16];
+  tmem_ld16(taddr, v0);
+  tmem_wait(v0);
+  tmem_ld16(taddr + 16, v1);
+  epi_chunk<METRIC, CMODE, FULL, DIAG>(v0, soa, cbase, col0, row, rs, ec, sn, sd);
+  tmem_wait(v1);
+  tmem_ld16(taddr + 32, v0);
+  epi_chunk<METRIC, CMODE, FULL, DIAG>(v1, soa, cbase + 16, col0, row, rs, ec, sn, sd);
+  tmem_wait(v0);
+  tmem_ld16(taddr + 48, v1);
+  epi_chunk<METRIC, CMODE, FULL, DIAG>(v0, soa, cbase + 32, col0, row, rs, ec, sn, sd);
+  tmem_wait(v1);
+  epi_chunk<METRIC, CMODE, FULL, DIAG>(v1, soa, cbase + 48, col0, row, rs, ec, sn, sd);
 }
 
 template <int METRIC>
@@ -221,12 +246,14 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int S = g.stages, nkc = g.nkc;
   const uint32_t sA = base;                                     // nkc x 16 KB
   const uint32_t sB = sA + nkc * kAChunkBytes;                  // S x 32 KB
-  ColTile* cols = reinterpret_cast<ColTile*>(sbase + (nkc * kAChunkBytes + S * kBStageBytes));  // [2]
-  uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(cols) + 2 * sizeof(ColTile));
-  // barrier layout: full[S], empty[S], acc_full[2], acc_empty[2], a_full, a_empty, done
+  const uint32_t sP = sB + S * kBStageBytes;                    // 2 x column-parameter slots
+  const float* slots = reinterpret_cast<const float*>(sbase + (sP - base));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + (sP - base) + 2 * kSoaBytes);
+  // barrier layout: full[S], empty[S], acc_full[2], acc_empty[2], par_full[2], a_full, a_empty, done
   const uint32_t b_full = smem_u32(bars), b_empty = b_full + 8 * S, b_accf = b_empty + 8 * S,
-                 b_acce = b_accf + 16, b_afull = b_acce + 16, b_aempty = b_afull + 8, b_done = b_aempty + 8;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 7);
+                 b_acce = b_accf + 16, b_parf = b_acce + 16, b_afull = b_parf + 16, b_aempty = b_afull + 8,
+                 b_done = b_aempty + 8;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 9);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -237,6 +264,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int b = 0; b < 2; b++) {
       mbar_init(b_accf + 8 * b, 1);
       mbar_init(b_acce + 8 * b, kEpiWarps);
+      mbar_init(b_parf + 8 * b, 1);
     }
     mbar_init(b_afull, 1);
     mbar_init(b_aempty, 1);
@@ -274,7 +302,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
         }
       }
-      // Drain: every issued B load has landed before the CTA may exit.
+      // Drain: every issued copy has landed before the CTA may exit.
       for (uint32_t k = (it > (uint32_t)S ? it - S : 0); k < it; k++)
         mbar_wait(b_full + 8 * (k % S), (k / S) & 1, g.status, ST_TIMEOUT_DRAIN, false);
     }
@@ -283,6 +311,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     // ---------------------------------------------------------------- MMA
     if (lane == 0) {
       uint32_t it = 0, tile = 0, item_i = 0;
+      uint32_t par_issued = 0;  // parameter copies issued (for the drain)
       bool ok = true;
       for (int item = blockIdx.x; ok && item < g.n_items; item += gridDim.x, item_i++) {
         const int seg = item / g.n_rb;
@@ -293,6 +322,10 @@ __global__ void __launch_bounds__(kThreads, 1)
           const uint32_t b = tile & 1;
           if (!mbar_wait(b_acce + 8 * b, ((tile >> 1) & 1) ^ 1, g.status, ST_TIMEOUT_MMA)) { ok = false; break; }
           tc_fence_after();
+          // The epilogue released this buffer, so its parameter slot is free too.
+          mbar_expect_tx(b_parf + 8 * b, kSoaBytes);
+          bulk_load(sP + b * kSoaBytes, g.colsoa + (size_t)ct * kColSoaFloats, kSoaBytes, b_parf + 8 * b);
+          par_issued = tile + 1;
           const uint32_t d = tmem + b * kBN;
           for (int kc = 0; kc < nkc; kc++, it++) {
             const int s = it % S;
@@ -310,15 +343,18 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         if (ok) mma_commit(b_aempty);
       }
-      // All MMAs this thread issued are complete before TMEM is released.
+      // All MMAs and parameter copies this thread issued are complete before
+      // TMEM is released and the CTA exits.
       mma_commit(b_done);
       mbar_wait(b_done, 0, g.status, ST_TIMEOUT_DRAIN, false);
+      for (uint32_t k = (par_issued > 2 ? par_issued - 2 : 0); k < par_issued; k++)
+        mbar_wait(b_parf + 8 * (k & 1), (k >> 1) & 1, g.status, ST_TIMEOUT_DRAIN, false);
     }
     __syncwarp();
   } else {
     // ---------------------------------------------------------------- epilogue
-    const int quarter = warp & 3, half = warp >> 2;
-    const int et = threadIdx.x;  // 0..255: column this thread stages
+    const int quarter = warp & 3, group = warp >> 2;
+    const int cbase = group * kColsPerWarp;
     uint32_t tile = 0;
     bool ok = true;
     for (int item = blockIdx.x; ok && item < g.n_items; item += gridDim.x) {
@@ -329,33 +365,30 @@ __global__ void __launch_bounds__(kThreads, 1)
       const float rmax_r = g.tile_rmax[rb];
       double acc_n = 0.0, acc_d = 0.0;
       for (int ct = ct0; ok && ct < ct1; ct++, tile++) {
-        const uint32_t b = tile & 1;
-        const int col0 = ct * kBN;
-        {
-          const BlockParams cp = g.params[col0 + et];
-          ColTile& t = cols[b];
-          t.a[et] = cp.a;
-          t.r[et] = cp.r;
-          t.sigma[et] = cp.sigma;
-          t.mu[et] = cp.mu;
+        const uint32_t b = tile & 1, par = (tile >> 1) & 1;
+        if (!mbar_wait(b_parf + 8 * b, par, g.status, ST_TIMEOUT_EPI) ||
+            !mbar_wait(b_accf + 8 * b, par, g.status, ST_TIMEOUT_EPI)) {
+          ok = false;
+          break;
         }
-        asm volatile("bar.sync 1, %0;" ::"r"(kEpiWarps * 32) : "memory");
-        if (!mbar_wait(b_accf + 8 * b, (tile >> 1) & 1, g.status, ST_TIMEOUT_EPI)) { ok = false; break; }
         tc_fence_after();
-        const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + b * kBN + half * (kBN / 2);
-        const float cmax = fmaxf(g.tile_rmax[2 * ct], g.tile_rmax[2 * ct + 1]);
-        const bool exact = METRIC == kPearson && (kEps * rmax_r * cmax > kTFast);
+        const float* soa = slots + b * kColSoaFloats;
+        const int col0 = ct * kBN;
+        const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + b * kBN + cbase;
+        const int cm = METRIC == kPearson ? c_mode(kEps * rmax_r * soa[4 * kBN]) : kCFirst;
         const bool full = col0 + kBN <= g.ec.n;
-        float sn = 0.0f, sd = 0.0f;
-        const int cbase = half * (kBN / 2);
         const bool diag = (ct == (rb >> 1));
-        if (full && !exact && !diag) {
-          epi_tile<METRIC, false, true, false>(taddr, cols[b], cbase, col0, row, rs, g.ec, sn, sd);
-        } else if (exact) {
-          epi_tile<METRIC, true, false, true>(taddr, cols[b], cbase, col0, row, rs, g.ec, sn, sd);
-        } else {
-          epi_tile<METRIC, false, false, true>(taddr, cols[b], cbase, col0, row, rs, g.ec, sn, sd);
-        }
+        float sn = 0.0f, sd = 0.0f;
+        if (full && !diag && cm == kCFirst)
+          epi_tile<METRIC, kCFirst, true, false>(taddr, soa, cbase, col0, row, rs, g.ec, sn, sd);
+        else if (full && !diag && cm == kCSecond)
+          epi_tile<METRIC, kCSecond, true, false>(taddr, soa, cbase, col0, row, rs, g.ec, sn, sd);
+        else if (cm == kCFirst)
+          epi_tile<METRIC, kCFirst, false, true>(taddr, soa, cbase, col0, row, rs, g.ec, sn, sd);
+        else if (cm == kCSecond)
+          epi_tile<METRIC, kCSecond, false, true>(taddr, soa, cbase, col0, row, rs, g.ec, sn, sd);
+        else
+          epi_tile<METRIC, kCExact, false, true>(taddr, soa, cbase, col0, row, rs, g.ec, sn, sd);
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(b_acce + 8 * b);
@@ -404,18 +437,17 @@ bool make_map(CUtensorMap* m, const __nv_bfloat16* ptr, int kq, int rows, int bo
 }  // namespace
 
 cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int kq, int n_pad,
-                           const BlockParams* params, const float* tile_rmax, EpiConsts ec, double* num,
-                           double* den, int num_sms, int* status, cudaStream_t st) {
+                           const BlockParams* params, const float* colsoa, const float* tile_rmax, EpiConsts ec,
+                           double* num, double* den, int num_sms, int* status, cudaStream_t st) {
   if (kq % 16 != 0 || n_pad % kBN != 0) return cudaErrorInvalidValue;
   TcArgs g;
   g.kq = kq;
   g.nkc = (kq + kChunk - 1) / kChunk;
-  g.n_rb = n_pad / kBM;
   g.n_ct = (ec.n + kBN - 1) / kBN;
-  const size_t fixed = 1024 + (size_t)g.nkc * kAChunkBytes + 2 * sizeof(ColTile) + 8 * 64;
+  const size_t fixed = 1024 + (size_t)g.nkc * kAChunkBytes + 2 * kSoaBytes + 8 * 64;
   const size_t budget = 227 * 1024;
   if (fixed + 2 * kBStageBytes > budget) return cudaErrorInvalidValue;
-  g.stages = (int)std::min<size_t>(6, (budget - fixed) / kBStageBytes);
+  g.stages = (int)std::min<size_t>(kMaxStages, (budget - fixed) / kBStageBytes);
   const size_t smem = fixed + (size_t)g.stages * kBStageBytes;
   // Only row blocks that hold valid rows are work; split the column range so
   // that every SM gets several items.
@@ -427,6 +459,7 @@ cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int k
   g.n_rb = n_rb_valid;
   g.n_items = g.n_rb * segs;
   g.params = params;
+  g.colsoa = colsoa;
   g.tile_rmax = tile_rmax;
   g.ec = ec;
   g.num = num;

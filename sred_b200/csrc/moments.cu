@@ -312,6 +312,30 @@ __global__ void k_pack(const float* __restrict__ img, int W, Ellipse e, const in
   }
 }
 
+// Tile-major structure-of-arrays copy of the column parameters (one CTA of
+// 256 threads per 256-column tile), with each tile's largest 1/sigma.
+__global__ void k_col_soa(const BlockParams* __restrict__ params, float* __restrict__ colsoa) {
+  const int t = blockIdx.x, i = threadIdx.x;
+  const BlockParams p = params[(size_t)t * 256 + i];
+  float* o = colsoa + (size_t)t * kColSoaFloats;
+  o[i] = p.a;
+  o[256 + i] = p.r;
+  o[512 + i] = p.sigma;
+  o[768 + i] = p.mu;
+  float m = p.r;
+  for (int s = 16; s; s >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, s));
+  __shared__ float wm[8];
+  if ((i & 31) == 0) wm[i >> 5] = m;
+  __syncthreads();
+  if (i < 4) o[1024 + i] = 0.0f;
+  __syncthreads();
+  if (i == 0) {
+    float mm = wm[0];
+    for (int w = 1; w < 8; w++) mm = fmaxf(mm, wm[w]);
+    o[1024] = mm;
+  }
+}
+
 // Diagnostics: pack caller-given vectors (n x K, FP32) as operands without
 // normalising them (one warp per row).
 __global__ void k_pack_vectors(const float* __restrict__ u, int n, int K, int mode, float* __restrict__ U, int kp,

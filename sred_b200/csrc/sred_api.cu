@@ -18,7 +18,7 @@ namespace {
 
 enum BufId {
   B_IMG, B_MEANS, B_STDS, B_MASK, B_MASKIN, B_FLAGS, B_SLOT, B_GPIX, B_FPIX, B_COUNTS, B_U, B_A, B_B,
-  B_PARAMS, B_RMAX, B_NUM, B_DEN, B_SUMS, B_OUT, B_VARS, B_MM, B_NMASK, B_BAD, B_STATUS, B_STDS2, B_NBUF
+  B_PARAMS, B_RMAX, B_NUM, B_DEN, B_SUMS, B_OUT, B_VARS, B_MM, B_NMASK, B_BAD, B_STATUS, B_STDS2, B_COLSOA, B_NBUF
 };
 
 struct DevBuf {
@@ -279,6 +279,12 @@ sred_status global_core(sred_ctx* c, int metric, const float* d_img, int w, int 
                                   kp, d_A, d_B, kq, d_params, d_rmax, d_sums);
     CK(cudaGetLastError());
   }
+  float* d_colsoa = nullptr;
+  if (engine == SRED_ENGINE_TC) {
+    CKS(ensure(c, B_COLSOA, (n_pad / 256) * kColSoaFloats, &d_colsoa));
+    k_col_soa<<<(int)(n_pad / 256), 256, 0, st>>>(d_params, d_colsoa);
+    CK(cudaGetLastError());
+  }
   CK(cudaEventRecord(c->ev[1], st));
   EpiConsts ec;
   ec.metric = metric;
@@ -293,7 +299,8 @@ sred_status global_core(sred_ctx* c, int metric, const float* d_img, int w, int 
       int* d_status;
       CKS(ensure(c, B_STATUS, 4, &d_status));
       CK(cudaMemsetAsync(d_status, 0, 4 * sizeof(int), st));
-      CK(launch_gram_tc(d_A, d_B, kq, (int)n_pad, d_params, d_rmax, ec, d_num, d_den, c->num_sms, d_status, st));
+      CK(launch_gram_tc(d_A, d_B, kq, (int)n_pad, d_params, d_colsoa, d_rmax, ec, d_num, d_den, c->num_sms,
+                        d_status, st));
       int status = 0;
       CK(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
@@ -328,7 +335,7 @@ sred_status global_core(sred_ctx* c, int metric, const float* d_img, int w, int 
     info->ms_gram = t12;
     info->ms_finalize = t23;
     info->ms_total = t03;
-    info->launches = (given ? 0 : 2) + 4 + (n_g > 0 ? 2 : 0) + 1 + (normalize ? 2 : 0);
+    info->launches = (given ? 0 : 2) + 4 + (n_g > 0 ? (engine == SRED_ENGINE_TC ? 3 : 2) : 0) + 1 + (normalize ? 2 : 0);
   }
   return SRED_OK;
 }
@@ -680,7 +687,11 @@ sred_status sred_debug_gram_rowdot(sred_ctx* c, int engine, const float* u, cons
     int* d_status;
     CKS(ensure(c, B_STATUS, 4, &d_status));
     CK(cudaMemsetAsync(d_status, 0, 4 * sizeof(int), st));
-    CK(launch_gram_tc(d_A, d_B, kq, (int)n_pad, d_params, d_rmax, ec, d_num, d_den, c->num_sms, d_status, st));
+    float* d_colsoa;
+    CKS(ensure(c, B_COLSOA, (n_pad / 256) * kColSoaFloats, &d_colsoa));
+    k_col_soa<<<(int)(n_pad / 256), 256, 0, st>>>(d_params, d_colsoa);
+    CK(launch_gram_tc(d_A, d_B, kq, (int)n_pad, d_params, d_colsoa, d_rmax, ec, d_num, d_den, c->num_sms, d_status,
+                      st));
     int status = 0;
     CK(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
