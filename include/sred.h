@@ -159,8 +159,9 @@ sred_status sred_block_map_2d_device_noalloc(const char *metric, const float *d_
                                              float *d_out, void *stream);
 
 /* Diagnostics of the contraction engines (no counterpart in the reference):
- * for caller-given vectors u (n x k, row-major) and column weights w1, w2,
- * num[p] = sum_q <u_p, u_q> w1[q] and den[p] = sum_q w2[q], computed by the
+ * for caller-given vectors u (n x k, row-major) and weights w1, w2,
+ * num[p] = sum_q <u_p, u_q> w1[p] w1[q] and den[p] = sum_q (w2[p] + w2[q]),
+ * symmetric pair terms like the maps' own, computed by the
  * chosen engine's all-pairs kernel (the tensor-core engine splits u into
  * bf16 hi/lo without normalising it). */
 sred_status sred_debug_gram_rowdot(sred_ctx *ctx, int engine, const float *u, const float *w1,

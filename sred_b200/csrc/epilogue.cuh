@@ -66,18 +66,19 @@ __device__ __forceinline__ int c_mode(float tmax) {
   return tmax < kTFirst ? kCFirst : (tmax < kTFast ? kCSecond : kCExact);
 }
 
-// One pair; CMODE is used by Pearson only.
+// The two per-pair terms (numerator tn, denominator td); symmetric in p, q.
+// CMODE is used by Pearson only.
 template <int METRIC, int CMODE>
-__device__ __forceinline__ void epi_pair(float G, const RowState& rp, const BlockParams& cq,
-                                         const EpiConsts& ec, float& sn, float& sd) {
-  if (METRIC == kDebugDot) {
-    sn = fmaf(G, cq.a, sn);
-    sd += cq.r;
+__device__ __forceinline__ void pair_terms(float G, const RowState& rp, const BlockParams& cq,
+                                           const EpiConsts& ec, float& tn, float& td) {
+  if (METRIC == kDebugDot) {  // symmetric diagnostic terms
+    tn = G * rp.a * cq.a;
+    td = rp.r + cq.r;
     return;
   }
   const float d = rp.a - cq.a;
   const float w = ex2_approx(-d * d);
-  sd += w;
+  td = w;
   if (METRIC == kPearson) {
     float gc;
     if (CMODE == kCFirst) {
@@ -88,18 +89,57 @@ __device__ __forceinline__ void epi_pair(float G, const RowState& rp, const Bloc
     } else {
       gc = G * __frcp_rn(1.0f + rp.e * cq.r);
     }
-    sn = fmaf(fmaxf(gc, 0.0f), w, sn);
+    tn = fmaxf(gc, 0.0f) * w;
   } else if (METRIC == kSsim) {
     const float num = fmaf(rp.mu2x2, cq.mu, ec.c1) * fmaf(rp.sig2x * cq.sigma, G, ec.c2);
     const float den = fmaf(rp.mumu, cq.mu * cq.mu, ec.c1) * fmaf(cq.sigma, cq.sigma, rp.s2);
-    sn += fmaxf(__fdividef(num, den) * w, 0.0f);
+    tn = fmaxf(__fdividef(num, den) * w, 0.0f);
   } else if (METRIC == kNrmse) {
     const float ds = rp.sigma - cq.sigma;
     const float m = ec.nrmse_scale * fmaf(ds, ds, rp.sig2x * cq.sigma * (1.0f - G));
-    sn += sqrtf(fmaxf(m, 0.0f));
+    tn = sqrtf(fmaxf(m, 0.0f));
   } else {  // Abs-diff of stds
-    sn = fmaf(fabsf(rp.sigma - cq.sigma), w, sn);
+    tn = fabsf(rp.sigma - cq.sigma) * w;
   }
+}
+
+// One pair accumulated into the row sums.
+template <int METRIC, int CMODE>
+__device__ __forceinline__ void epi_pair(float G, const RowState& rp, const BlockParams& cq,
+                                         const EpiConsts& ec, float& sn, float& sd) {
+  float tn, td;
+  pair_terms<METRIC, CMODE>(G, rp, cq, ec, tn, td);
+  sn += tn;
+  sd += td;
+}
+
+// Column sums of 16 columns over the 32 lanes of a warp (lane l holds row l's
+// terms x[0..15]): four butterfly exchanges halve the columns each lane keeps,
+// a fifth adds the lane pairs. Afterwards lanes 2c and 2c+1 both hold the sum
+// of column c over all 32 rows.
+__device__ __forceinline__ float lane_column_sums16(const float (&x)[16]) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  float y8[8], y4[4], y2[2];
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const float send = b4 ? x[i] : x[i + 8], keep = b4 ? x[i + 8] : x[i];
+    y8[i] = keep + __shfl_xor_sync(full, send, 16);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const float send = b3 ? y8[i] : y8[i + 4], keep = b3 ? y8[i + 4] : y8[i];
+    y4[i] = keep + __shfl_xor_sync(full, send, 8);
+  }
+#pragma unroll
+  for (int i = 0; i < 2; i++) {
+    const float send = b2 ? y4[i] : y4[i + 2], keep = b2 ? y4[i + 2] : y4[i];
+    y2[i] = keep + __shfl_xor_sync(full, send, 4);
+  }
+  const float send = b1 ? y2[0] : y2[1], keep = b1 ? y2[1] : y2[0];
+  float y = keep + __shfl_xor_sync(full, send, 2);
+  return y + __shfl_xor_sync(full, y, 1);
 }
 
 }  // namespace sred

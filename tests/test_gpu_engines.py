@@ -1,9 +1,10 @@
 """The two contraction engines on caller-given vectors, through the C ABI.
 
-num[p] = sum_q <u_p, u_q> w1[q] and den[p] = sum_q w2[q] are checked
+num[p] = sum_q <u_p, u_q> w1[p] w1[q] and den[p] = sum_q (w2[p] + w2[q])
+(symmetric pair terms, as the engines evaluate the upper triangle) are checked
 against an FP64 evaluation for every K' chunk count the tensor-core engine
 uses (K' = round_up(3K, 16) from 16 to 448) and for ragged N (partial row
-blocks and column tiles). Bound: |err| <= tol * sum_q |G_pq w1_q| with
+blocks and column tiles). Bound: |err| <= tol * sum_q |G_pq w1_p w1_q| with
 tol = 2e-6 for the FP32 engine and 4e-5 for split-BF16 (the omitted lo*lo
 term and bf16 rounding of lo are below 2^-15 of |u_p||u_q|).
 """
@@ -46,11 +47,13 @@ def test_rowdot_matches_fp64(ctx, engine, n, k):
     num, den = rowdot(ctx, engine, u, w1, w2)
     U = u.astype(np.float64)
     G = U @ U.T
-    exp = G @ w1.astype(np.float64)
-    scale = np.abs(G) @ np.abs(w1.astype(np.float64))
+    w = w1.astype(np.float64)
+    exp = w * (G @ w)
+    scale = np.abs(w) * (np.abs(G) @ np.abs(w))
     err = np.abs(num - exp) / np.maximum(scale, 1e-30)
     assert float(err.max()) <= TOL[engine], float(err.max())
-    np.testing.assert_allclose(den, np.full(n, w2.astype(np.float64).sum()), rtol=1e-6)
+    w2d = w2.astype(np.float64)
+    np.testing.assert_allclose(den, n * w2d + w2d.sum(), rtol=1e-6)
 
 
 def test_tc_matches_fp32_unnormalised(ctx):
@@ -62,5 +65,6 @@ def test_tc_matches_fp32_unnormalised(ctx):
     a, _ = rowdot(ctx, "fp32", u, w1, w1)
     b, _ = rowdot(ctx, "tc", u, w1, w1)
     U = u.astype(np.float64)
-    scale = np.abs(U @ U.T) @ w1.astype(np.float64)
+    w = w1.astype(np.float64)
+    scale = w * (np.abs(U @ U.T) @ w)
     assert float(np.max(np.abs(a - b) / scale)) <= TOL["tc"]
