@@ -79,6 +79,16 @@ def lib() -> C.CDLL:
         L.orc_block_kernel_f64.argtypes = [C.c_int, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, _f32p,
                                            _f32p, C.c_int, C.c_float, C.c_float, _f64p]
         L.orc_java_random_floats.argtypes = [C.c_int64, C.c_int, _f32p]
+        L.orc_patch_hu1_ref.restype = C.c_double
+        L.orc_patch_hu1_ref.argtypes = [_f32p, C.c_int, C.c_int]
+        L.orc_patch_hu.argtypes = [_f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f32p]
+        L.orc_hu_prepare_patch.argtypes = [_f32p, C.c_int, C.c_int, _f32p]
+        L.orc_hu_feature.restype = C.c_float
+        L.orc_hu_feature.argtypes = [_f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.orc_hu_map.argtypes = [_f32p, _f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f64p]
+        L.orc_phase_map.argtypes = [_f32p, _f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f64p]
+        L.orc_block_phase.argtypes = [_f32p, _f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, _f32p,
+                                      C.c_float, _f64p]
         _lib = L
     return _lib
 
@@ -323,4 +333,96 @@ def block_raw_f64(metric: int, img, ref_pixels, bw, bh, ref_mean, ref_std, stds3
     ref = _f32(ref_pixels)
     lib().orc_block_kernel_f64(metric, img, W, H, bw, bh, _f32(stds32), ref, ref.size,
                                C.c_float(ref_mean), C.c_float(ref_std), out)
+    return out.reshape(H, W)
+
+
+# --------------------------------------------------------------------------
+# Shape metrics: the reference's Hu and phase-correlation kernels
+# (cl/kernelGetPatchHu2D.cl, cl/kernelGetHuMap.cl,
+# cl/kernelGetPhaseCorrelationMap.cl; shipped, never loaded by its Java code)
+# --------------------------------------------------------------------------
+
+def _shape_refshim(name, W, H, bw, bh, patch_size, bufs):
+    R = refshim()
+    if R is None:
+        raise RuntimeError("refshim not built")
+    pix = np.arange(W * H, dtype=np.int32)
+    fn = getattr(R, f"rs_{name}")
+    args = [C.c_int(W), C.c_int(H), C.c_int(bw), C.c_int(bh), C.c_int(patch_size), C.c_float(EPSILON),
+            pix.ctypes.data_as(C.c_void_p), C.c_int(pix.size)]
+    args += [None if b is None else b.ctypes.data_as(C.c_void_p) for b in bufs]
+    if fn(*args) != 0:
+        raise ValueError(f"refshim has no {name} instantiation for {bw}x{bh}")
+
+
+def patch_hu_map(patch, img, bw, bh, patch_size=None, use_refshim=False):
+    """cl/kernelGetPatchHu2D.cl over every pixel: interior pixels get
+    sqrt(hu1(patch) * hu1(comparison patch)); border pixels stay 0.
+    ``patch`` is the bw x bh grid the kernel reads (at the ellipse positions)."""
+    img = _f32(img)
+    H, W = img.shape
+    patch = _f32(patch).ravel()
+    ps = block_size(bw, bh) if patch_size is None else patch_size
+    out = np.zeros(W * H, np.float32)
+    if use_refshim:
+        _shape_refshim("kernelGetPatchHu2D", W, H, bw, bh, ps, [patch, img, np.zeros_like(img), out])
+    else:
+        lib().orc_patch_hu(patch, img, W, H, bw, bh, ps, out)
+    return out.reshape(H, W)
+
+
+def patch_hu1(patch, bw, bh) -> float:
+    return float(lib().orc_patch_hu1_ref(_f32(patch).ravel(), bw, bh))
+
+
+def hu_prepare_patch(ref_pixels, bw, bh) -> np.ndarray:
+    """bw x bh reference patch of the block-map Hu metric (see orc_hu_prepare_patch)."""
+    g = np.zeros(bw * bh, np.float32)
+    lib().orc_hu_prepare_patch(_f32(ref_pixels), bw, bh, g)
+    return g.reshape(bh, bw)
+
+
+def hu_map(img, bw, bh, means=None, stds=None, precision="f32", use_refshim=False):
+    """cl/kernelGetHuMap.cl over every interior pixel (raw sums)."""
+    img = _f32(img)
+    H, W = img.shape
+    if means is None:
+        means, stds = local_stats(img, bw, bh)
+    if use_refshim:
+        out = np.zeros(W * H, np.float32)
+        _shape_refshim("kernelGetHuMap", W, H, bw, bh, bw * bh, [img, _f32(means), _f32(stds), None, out])
+        return out.reshape(H, W).astype(np.float64)
+    out = np.zeros(W * H, np.float64)
+    lib().orc_hu_map(img, _f32(means), _f32(stds), W, H, bw, bh, int(precision == "f64"), out)
+    return out.reshape(H, W)
+
+
+def phase_map(img, bw, bh, means=None, stds=None, precision="f32", use_refshim=False):
+    """cl/kernelGetPhaseCorrelationMap.cl (three repairs, see orc_phase_map)
+    over every interior pixel (raw sums)."""
+    img = _f32(img)
+    H, W = img.shape
+    if means is None:
+        means, stds = local_stats(img, bw, bh)
+    if use_refshim:
+        out = np.zeros(W * H, np.float32)
+        _shape_refshim("kernelGetPhaseCorrelationMap", W, H, bw, bh, bw * bh,
+                       [img, _f32(means), _f32(stds), None, out])
+        return out.reshape(H, W).astype(np.float64)
+    out = np.zeros(W * H, np.float64)
+    if lib().orc_phase_map(img, _f32(means), _f32(stds), W, H, bw, bh, int(precision == "f64"), out):
+        raise ValueError("phase correlation supports blocks up to 15x15")
+    return out.reshape(H, W)
+
+
+def block_phase_raw(img, ref_pixels, bw, bh, ref_std, means=None, stds=None):
+    """Block-map phase correlation before post-processing (FP64)."""
+    img = _f32(img)
+    H, W = img.shape
+    if means is None:
+        means, stds = local_stats(img, bw, bh)
+    out = np.zeros(W * H, np.float64)
+    if lib().orc_block_phase(img, _f32(means), _f32(stds), W, H, bw, bh, _f32(ref_pixels),
+                             C.c_float(ref_std), out):
+        raise ValueError("phase correlation supports blocks up to 15x15")
     return out.reshape(H, W)

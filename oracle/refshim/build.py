@@ -57,6 +57,25 @@ MACROS = ["image_width", "image_height", "block_size", "bW", "bH", "bRW", "bRH",
 
 MAX_BLOCK = 15  # every odd block width/height 3..15 is instantiated
 
+# Shape-metric kernels (shipped by the reference, never loaded by its Java
+# code). Their block width and height are template parameters; $PATCH_SIZE$
+# is the ellipse count K for the Hu patch kernel (the Java convention of
+# java/RelevanceMask2D_.java:161-167) and bw*bh for the two all-pairs kernels,
+# whose private arrays hold the whole square block.
+SHAPE_KERNELS = {
+    "kernelGetPatchHu2D": (["patch", "img", "means", "map"], "RS_PS"),
+    "kernelGetHuMap": (["img", "means", "stds", "uniq", "map"], "(RS_TBW*RS_TBH)"),
+    "kernelGetPhaseCorrelationMap": (["img", "means", "stds", "uniq", "map"], "(RS_TBW*RS_TBH)"),
+}
+# The phase kernel does not compile as shipped; these text repairs make it
+# the intended computation (each is documented in oracle/sred_oracle.c):
+#   nUnique is never defined (:27) -> the unique-coordinate pre-filter is off;
+#   (1*i*ii/bW) divides integers (:66, :101, :138) -> real-valued phases;
+#   cross_corr_real[j*w+i] reads past the block (:150) -> block width.
+PHASE_REPAIRS = [("(1*i*ii/bW)", "(1.0*i*ii/bW)"), ("(1*j*jj/bH)", "(1.0*j*jj/bH)"),
+                 ("cross_corr_real[j*w+i]", "cross_corr_real[j*bW+i]")]
+SHAPE_SIZES = sorted({(a, b) for a in (3, 5, 7, 9) for b in (3, 5, 7, 9)} | {(11, 11), (13, 13), (15, 15)})
+
 
 def ellipse_k(bw: int, bh: int) -> int:
     f = np.float32
@@ -122,6 +141,58 @@ def gen_unit(ref: Path, name: str, ks: list[int]) -> str:
     return head + src + "\n" + entry_code(name, kind, args, ks)
 
 
+def gen_shape_unit(ref: Path, name: str) -> str:
+    args, psize = SHAPE_KERNELS[name]
+    src = (ref / "src/main/resources" / f"{name}.cl").read_text()
+    reps = {"$WIDTH$": "RS_W", "$HEIGHT$": "RS_H", "$PATCH_SIZE$": psize, "$BW$": "RS_TBW",
+            "$BH$": "RS_TBH", "$BRW$": "(RS_TBW/2)", "$BRH$": "(RS_TBH/2)", "$EPSILON$": "RS_EPSILON",
+            "$NUNIQUE$": "0", "$SPEEDUP$": "0"}
+    for tok, repl in reps.items():
+        src = replace_first(src, tok, repl)
+    if name == "kernelGetPhaseCorrelationMap":
+        src = "#define nUnique 0\n" + src
+        for a, b in PHASE_REPAIRS:
+            if a not in src:
+                raise RuntimeError(f"repair target {a!r} not found in {name}.cl")
+            src = src.replace(a, b)
+    ptypes = {"patch": "const float*", "img": "const float*", "means": "const float*",
+              "stds": "const float*", "uniq": "void*", "map": "float*"}
+    params = ", ".join(f"{ptypes[a]} {a}" for a in args)
+    call = ", ".join(f"(int*){a}" if (a == "uniq" and name == "kernelGetHuMap") else
+                     f"(float*){a}" for a in args)
+    cases = "\n".join(f"    case {a * 100 + b}: rs_loop<{a}, {b}>(pix, npix, {', '.join(args)}); break;"
+                      for a, b in SHAPE_SIZES)
+    undef = "".join(f"#undef {m}\n" for m in MACROS + ["patch_size", "nUnique", "speedUp"])
+    return f"""#include "shim_shape.h"
+namespace rsns_{name} {{
+#define kernel template <int RS_TBW, int RS_TBH> static inline
+{src}
+{undef}
+template <int TBW, int TBH>
+static void rs_loop(const int* pix, int npix, {params}) {{
+  #pragma omp parallel for schedule(dynamic, 1)
+  for (int i = 0; i < npix; i++) {{
+    rs_gid[0] = pix[i] % RS_W;
+    rs_gid[1] = pix[i] / RS_W;
+    {name}<TBW, TBH>({call});
+  }}
+}}
+}}  // namespace rsns_{name}
+
+extern "C" int rs_{name}(int W, int H, int bw, int bh, int patch_size, float eps, const int* pix,
+                       int npix, {params}) {{
+  using namespace rsns_{name};
+  RS_W = W; RS_H = H; RS_BW = bw; RS_BH = bh; RS_BRW = bw / 2; RS_BRH = bh / 2;
+  RS_PS = patch_size; RS_EPSILON = eps;
+  switch (bw * 100 + bh) {{
+{cases}
+    default: return -1;
+  }}
+  return 0;
+}}
+"""
+
+
 def run(cmd: list[str]) -> None:
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
@@ -142,7 +213,9 @@ def build_refshim(ref: Path, force: bool = False) -> Path | None:
     out = REF_OUT / "librefshim.so"
     ks = k_list()
     units = {n: gen_unit(ref, n, ks) for n in KERNELS}
-    digest = hashlib.sha256(("".join(units.values()) + (HERE / "shim.h").read_text()).encode()).hexdigest()
+    units.update({n: gen_shape_unit(ref, n) for n in SHAPE_KERNELS})
+    digest = hashlib.sha256(("".join(units.values()) + (HERE / "shim.h").read_text()
+                             + (HERE / "shim_shape.h").read_text()).encode()).hexdigest()
     stamp = REF_OUT / "build.sha256"
     if not force and out.exists() and stamp.exists() and stamp.read_text() == digest:
         return out

@@ -617,3 +617,375 @@ void orc_java_random_floats(int64_t seed, int n, float *out) {
         out[i] = (float)bits / (float)(1 << 24);
     }
 }
+
+/* ------------------------------------------------------------------ */
+/* Shape metrics: Hu moments and phase correlation                     */
+/*                                                                     */
+/* The reference ships three OpenCL kernels for these that its Java    */
+/* code never loads: cl/kernelGetPatchHu2D.cl (one patch against every */
+/* block, FP64), cl/kernelGetHuMap.cl (all pairs, FP32) and            */
+/* cl/kernelGetPhaseCorrelationMap.cl (all pairs, FP64; it does not    */
+/* compile as shipped). The functions below restate them statement for */
+/* statement. $PATCH_SIZE$ is the ellipse count K for the Hu patch     */
+/* kernel (the Java convention, java/RelevanceMask2D_.java:161-167)    */
+/* and bw*bh for the two all-pairs kernels, whose private arrays hold  */
+/* the whole square block. The phase kernel is restated with three     */
+/* repairs: no unique-coordinate pre-filter (its nUnique is never      */
+/* defined, :27), real-valued DFT phases (the shipped (1*i*ii/bW) is   */
+/* an integer division, :66/:101/:138) and the peak search indexed     */
+/* with the block width (the shipped j*w+i reads past the block,       */
+/* :150).                                                              */
+/* ------------------------------------------------------------------ */
+
+/* cl/kernelGetPatchHu2D.cl:38-40 (float test) and :58-60 (double test);
+ * both select the same positions as in_ellipse() for every odd size 3..15. */
+static int hu_in_ellipse_f(int i, int j, int rw, int rh) {
+    float dx = (float)(i - rw) / rw, dy = (float)(j - rh) / rh;
+    return dx * dx + dy * dy <= 1.0f;
+}
+
+/* Hu invariant 1 of a bw x bh patch read at the ellipse positions:
+ * cl/kernelGetPatchHu2D.cl:51-101 (reference patch) = :189-239 (comparison
+ * patch). Raw moments use 1-based coordinates, central moments 0-based
+ * ones, as the kernel does. */
+static double orc_hu1_patch(const double *v, int bw, int bh) {
+    const int rw = bw / 2, rh = bh / 2;
+    double M00 = 0.0, M10 = 0.0, M01 = 0.0;
+    for (int j = 0; j < bh; j++)
+        for (int i = 0; i < bw; i++)
+            if (hu_in_ellipse_f(i, j, rw, rh)) {
+                double p = v[j * bw + i];
+                M00 += p;
+                M10 += (double)(i + 1) * p;
+                M01 += (double)(j + 1) * p;
+            }
+    double cx = M10 / (M00 + (double)ORC_EPS);
+    double cy = M01 / (M00 + (double)ORC_EPS);
+    double mu20 = 0.0, mu02 = 0.0;
+    for (int j = 0; j < bh; j++)
+        for (int i = 0; i < bw; i++)
+            if (hu_in_ellipse_f(i, j, rw, rh)) {
+                double p = v[j * bw + i];
+                mu20 += pow(((double)i - cx), 2.0) * p;
+                mu02 += pow(((double)j - cy), 2.0) * p;
+            }
+    double nu20 = mu20 / (pow(M00, 2.0) + (double)ORC_EPS);
+    double nu02 = mu02 / (pow(M00, 2.0) + (double)ORC_EPS);
+    return nu20 + nu02;
+}
+
+/* Hu invariant 1 of the reference patch as the kernel reads it
+ * (cl/kernelGetPatchHu2D.cl:34-44: float patch values widened to double). */
+double orc_patch_hu1_ref(const float *patch, int bw, int bh) {
+    double v[32 * 32];
+    if (bw > 31 || bh > 31) return NAN;
+    for (int k = 0; k < bw * bh; k++) v[k] = (double)patch[k];
+    return orc_hu1_patch(v, bw, bh);
+}
+
+/* cl/kernelGetPatchHu2D.cl:18-267 for every pixel: interior pixels get
+ * (float)sqrt(hu1_ref * hu1_comp), border pixels are left untouched. */
+void orc_patch_hu(const float *patch, const float *img, int W, int H, int bw, int bh, int patch_size,
+                  float *out) {
+    const int rw = bw / 2, rh = bh / 2;
+    const double ref_hu1 = orc_patch_hu1_ref(patch, bw, bh);
+    double comp[32 * 32];
+    for (int gy = rh; gy < H - rh; gy++)
+        for (int gx = rw; gx < W - rw; gx++) {
+            double mean = 0.0;
+            /* :129-140, the gather's ellipse test divides integers, so it keeps
+             * every position of the square except its four corners */
+            for (int j = gy - rh; j <= gy + rh; j++)
+                for (int i = gx - rw; i <= gx + rw; i++) {
+                    float dx = (float)((i - gx) / rw);
+                    float dy = (float)((j - gy) / rh);
+                    if (dx * dx + dy * dy <= 1.0f) {
+                        double p = (double)img[j * W + i];
+                        comp[(j - (gy - rh)) * bw + (i - (gx - rw))] = p;
+                        mean += p;
+                    }
+                }
+            mean /= (double)patch_size;
+            for (int j = 0; j < bh; j++) /* :143-151 */
+                for (int i = 0; i < bw; i++)
+                    if (hu_in_ellipse_f(i, j, rw, rh)) comp[j * bw + i] -= mean;
+            double mn = DBL_MAX, mx = -DBL_MAX; /* :158-171 */
+            for (int j = 0; j < bh; j++)
+                for (int i = 0; i < bw; i++)
+                    if (hu_in_ellipse_f(i, j, rw, rh)) {
+                        double p = comp[j * bw + i];
+                        mn = p < mn ? p : mn;
+                        mx = p > mx ? p : mx;
+                    }
+            for (int j = 0; j < bh; j++) /* :174-182 */
+                for (int i = 0; i < bw; i++)
+                    if (hu_in_ellipse_f(i, j, rw, rh))
+                        comp[j * bw + i] = (comp[j * bw + i] - mn) / (mx - mn + (double)ORC_EPS);
+            out[gy * W + gx] = (float)sqrt(ref_hu1 * orc_hu1_patch(comp, bw, bh));
+        }
+}
+
+/* Reference patch of the block-map form of the Hu metric (a definition of
+ * this library; the reference never wires the kernel): the ReferenceBlock2D
+ * pixels (ellipse order) scattered onto the bw x bh grid and normalised the
+ * way cl/kernelGetPatchHu2D.cl:126-182 normalises every comparison patch
+ * (mean-subtract over the ellipse, then min-max to [0, 1]), in FP64, stored
+ * as float like the kernel's patch buffer. Off-ellipse grid cells are 0. */
+void orc_hu_prepare_patch(const float *ref_pixels, int bw, int bh, float *grid) {
+    const int rw = bw / 2, rh = bh / 2;
+    double v[32 * 32];
+    int k = 0, K = 0;
+    double mean = 0.0;
+    for (int j = 0; j < bh; j++)
+        for (int i = 0; i < bw; i++)
+            if (hu_in_ellipse_f(i, j, rw, rh)) K++;
+    for (int j = 0; j < bh; j++)
+        for (int i = 0; i < bw; i++) {
+            v[j * bw + i] = 0.0;
+            if (hu_in_ellipse_f(i, j, rw, rh)) {
+                v[j * bw + i] = (double)ref_pixels[k++];
+                mean += v[j * bw + i];
+            }
+        }
+    mean /= (double)K;
+    double mn = DBL_MAX, mx = -DBL_MAX;
+    for (int j = 0; j < bh; j++)
+        for (int i = 0; i < bw; i++)
+            if (hu_in_ellipse_f(i, j, rw, rh)) {
+                v[j * bw + i] -= mean;
+                mn = v[j * bw + i] < mn ? v[j * bw + i] : mn;
+                mx = v[j * bw + i] > mx ? v[j * bw + i] : mx;
+            }
+    for (int j = 0; j < bh; j++)
+        for (int i = 0; i < bw; i++)
+            grid[j * bw + i] = hu_in_ellipse_f(i, j, rw, rh)
+                                   ? (float)((v[j * bw + i] - mn) / (mx - mn + (double)ORC_EPS))
+                                   : 0.0f;
+}
+
+/* getInvariant (cl/kernelGetHuMap.cl:146-172), FP32. */
+static float orc_hu_invariant(const float *patch, int pw, int ph, int p, int q) {
+    float x_avg = 0.0f;
+    for (int i = 1; i <= pw; i++) x_avg += (float)i;
+    x_avg /= (float)pw;
+    float y_avg = 0.0f;
+    for (int i = 1; i <= ph; i++) y_avg += (float)i;
+    y_avg /= (float)ph;
+    float mu_pq = 0.0f, mu_00 = 0.0f;
+    for (int j = 0; j < ph; j++)
+        for (int i = 0; i < pw; i++) {
+            mu_pq += (float)powf((float)i + 1.0f - x_avg, (float)p) *
+                     ((float)powf((float)j + 1.0f - y_avg, (float)q)) * patch[j * pw + i];
+            mu_00 += patch[j * pw + i];
+        }
+    mu_00 = (float)powf(mu_00, 1.0f + (p + q) / 2.0f);
+    return mu_pq / (mu_00 + ORC_EPS);
+}
+
+/* Per-block Hu feature of cl/kernelGetHuMap.cl:62-80 (= :109-124): the whole
+ * square block minus the block's local mean, invariant(2,0) + invariant(0,2). */
+float orc_hu_feature(const float *img, const float *means, int W, int bw, int bh, int x0, int y0) {
+    float patch[32 * 32];
+    const int rw = bw / 2, rh = bh / 2;
+    const float m = means[y0 * W + x0];
+    int c = 0;
+    for (int j = y0 - rh; j <= y0 + rh; j++)
+        for (int i = x0 - rw; i <= x0 + rw; i++) patch[c++] = img[j * W + i] - m;
+    return orc_hu_invariant(patch, bw, bh, 2, 0) + orc_hu_invariant(patch, bw, bh, 0, 2);
+}
+
+/* getExpDecayWeight of cl/kernelGetHuMap.cl:136-144. */
+static float orc_hu_weight(float ref, float comp) {
+    float similarity = 1.0f - (fabsf(ref - comp) / (fabsf(ref) + fabsf(comp) + ORC_EPS));
+    return ((float)powf(100.0f, similarity) - 1) / 99;
+}
+
+/* cl/kernelGetHuMap.cl:23-133 for every interior reference pixel:
+ * sum over every interior q of |hu_q - hu_p| * weight(sigma_p, sigma_q).
+ * f64acc = 0: the reference's FP32 accumulation in raster order;
+ * f64acc = 1: the same FP32 terms summed in FP64 (the judge). */
+void orc_hu_map(const float *img, const float *means, const float *stds, int W, int H, int bw, int bh,
+                int f64acc, double *out) {
+    const int rw = bw / 2, rh = bh / 2;
+    float *feat = (float *)calloc((size_t)W * H, sizeof(float));
+    for (int y = rh; y < H - rh; y++)
+        for (int x = rw; x < W - rw; x++) feat[y * W + x] = orc_hu_feature(img, means, W, bw, bh, x, y);
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int y0 = rh; y0 < H - rh; y0++)
+        for (int x0 = rw; x0 < W - rw; x0++) {
+            const float ref_hu = feat[y0 * W + x0];
+            float acc32 = 0.0f;
+            double acc64 = 0.0;
+            for (int y1 = rh; y1 < H - rh; y1++)
+                for (int x1 = rw; x1 < W - rw; x1++) {
+                    float weight = orc_hu_weight(stds[y0 * W + x0], stds[y1 * W + x1]);
+                    float t = fabsf((float)feat[y1 * W + x1] - (float)ref_hu) * weight;
+                    acc32 += t;
+                    acc64 += (double)t;
+                }
+            out[y0 * W + x0] = f64acc ? acc64 : (double)acc32;
+        }
+    free(feat);
+}
+
+/* The kernel's pi is a float literal widened to double
+ * (cl/kernelGetPhaseCorrelationMap.cl:44). */
+static const double ORC_PHASE_PI = (double)3.14159265358979323846f;
+
+/* Forward DFT of a bw x bh real patch, as :59-71 / :93-106 compute it (with
+ * real-valued phases). tc/ts: cos/sin tables of the n x n phase matrix. */
+static void orc_phase_dft(const double *x, int n, const double *tc, const double *ts, double *re, double *im) {
+    const double sn = sqrt((double)n);
+    for (int a = 0; a < n; a++) {
+        re[a] = 0.0;
+        im[a] = 0.0;
+        for (int b = 0; b < n; b++) {
+            re[a] += (x[b] * tc[a * n + b]) / sn;
+            im[a] -= (x[b] * ts[a * n + b]) / sn;
+        }
+    }
+}
+
+/* Phase tables: angle(a = j*bw+i, b = jj*bw+ii) = 2*PI*((1.0*i*ii/bw) + (1.0*j*jj/bh)). */
+static void orc_phase_tables(int bw, int bh, double *tc, double *ts) {
+    const int n = bw * bh;
+    for (int j = 0; j < bh; j++)
+        for (int i = 0; i < bw; i++)
+            for (int jj = 0; jj < bh; jj++)
+                for (int ii = 0; ii < bw; ii++) {
+                    double ang = 2 * ORC_PHASE_PI * ((1.0 * i * ii / bw) + (1.0 * j * jj / bh));
+                    tc[(j * bw + i) * n + jj * bw + ii] = cos(ang);
+                    ts[(j * bw + i) * n + jj * bw + ii] = sin(ang);
+                }
+}
+
+/* Normalised cross-power spectrum (:108-130), inverse DFT (:132-142) and
+ * peak search (:144-157, first strict maximum above 0 in raster order,
+ * 1-based coordinates). Returns sqrt(x^2 + y^2) of the peak as float, 0 when
+ * no value is positive. */
+static float orc_phase_peak(const double *rr, const double *ri, const double *cr, const double *ci, int bw,
+                            int bh, const double *tc, const double *ts, double *xr, double *xi) {
+    const int n = bw * bh;
+    const double sn = sqrt((double)n);
+    for (int i = 0; i < n; i++) {
+        double conj = (-1) * ci[i];
+        double multReal = rr[i] * cr[i] - ri[i] * conj;
+        double multImag = rr[i] * conj + ri[i] * cr[i];
+        double ar = fabs(multReal), ai = fabs(multImag);
+        xr[i] = ((multReal * ar) + (multImag * ai)) / ((ar * ar) + (ai * ai) + ORC_EPS);
+        xi[i] = ((multImag * ar) - (multReal * ai)) / ((ar * ar) + (ai * ai) + ORC_EPS);
+    }
+    double max_value = 0.0;
+    int xc = 0, yc = 0;
+    for (int j = 0; j < bh; j++)
+        for (int i = 0; i < bw; i++) {
+            const int a = j * bw + i;
+            double v = 0.0;
+            for (int b = 0; b < n; b++) v += (xr[b] * tc[a * n + b] - xi[b] * ts[a * n + b]) / sn;
+            if (v > max_value) {
+                max_value = v;
+                xc = i + 1;
+                yc = j + 1;
+            }
+        }
+    return (float)sqrt(((double)xc * (double)xc) + ((double)yc * (double)yc));
+}
+
+/* getExpDecayWeight of cl/kernelGetPhaseCorrelationMap.cl:167-179. */
+static float orc_phase_weight(float ref, float comp) {
+    float weight = 0;
+    if (ref == comp) weight = 1;
+    else weight = 1 - (2 * (fabsf(ref - comp) / (fabsf(ref) + fabsf(comp))));
+    return weight;
+}
+
+/* Normalised whole-square patch of :46-57 / :80-91. */
+static void orc_phase_patch(const float *img, const float *means, const float *stds, int W, int bw, int bh,
+                            int x0, int y0, double *x) {
+    const int rw = bw / 2, rh = bh / 2;
+    int c = 0;
+    for (int j = y0 - rh; j <= y0 + rh; j++)
+        for (int i = x0 - rw; i <= x0 + rw; i++)
+            x[c++] = ((double)img[j * W + i] - (double)means[y0 * W + x0]) /
+                     ((double)stds[y0 * W + x0] + ORC_EPS);
+}
+
+/* cl/kernelGetPhaseCorrelationMap.cl:21-164 (repaired as stated above) for
+ * every interior reference pixel. f64acc as in orc_hu_map. Returns -1 for a
+ * block larger than 15 x 15. */
+int orc_phase_map(const float *img, const float *means, const float *stds, int W, int H, int bw, int bh,
+                  int f64acc, double *out) {
+    const int rw = bw / 2, rh = bh / 2, n = bw * bh;
+    if (n > 225) return -1;
+    const int nx = W - 2 * rw, ny = H - 2 * rh;
+    double *tc = (double *)malloc(sizeof(double) * n * n), *ts = (double *)malloc(sizeof(double) * n * n);
+    double *fr = (double *)malloc(sizeof(double) * n * (size_t)nx * ny);
+    double *fi = (double *)malloc(sizeof(double) * n * (size_t)nx * ny);
+    orc_phase_tables(bw, bh, tc, ts);
+    #pragma omp parallel for schedule(static)
+    for (int y = rh; y < H - rh; y++)
+        for (int xq = rw; xq < W - rw; xq++) {
+            double x[225];
+            const size_t b = (size_t)(y - rh) * nx + (xq - rw);
+            orc_phase_patch(img, means, stds, W, bw, bh, xq, y, x);
+            orc_phase_dft(x, n, tc, ts, fr + b * n, fi + b * n);
+        }
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int y0 = rh; y0 < H - rh; y0++)
+        for (int x0 = rw; x0 < W - rw; x0++) {
+            double xr[225], xi[225];
+            const size_t p = (size_t)(y0 - rh) * nx + (x0 - rw);
+            float acc32 = 0.0f;
+            double acc64 = 0.0;
+            for (int y1 = rh; y1 < H - rh; y1++)
+                for (int x1 = rw; x1 < W - rw; x1++) {
+                    const size_t q = (size_t)(y1 - rh) * nx + (x1 - rw);
+                    float d = orc_phase_peak(fr + p * n, fi + p * n, fr + q * n, fi + q * n, bw, bh, tc, ts, xr, xi);
+                    double weight = (double)orc_phase_weight(stds[y0 * W + x0], stds[y1 * W + x1]);
+                    acc32 = (float)((double)acc32 + (double)d * weight);
+                    acc64 += (double)d * weight;
+                }
+            out[y0 * W + x0] = f64acc ? acc64 : (double)acc32;
+        }
+    free(tc); free(ts); free(fr); free(fi);
+    return 0;
+}
+
+/* Block-map form of the phase correlation (a definition of this library, the
+ * reference has only the all-pairs kernel): the reference block
+ * (ReferenceBlock2D pixels / (std + eps)) and each interior block
+ * ((x - mean) / (std + eps) with the block's FP32 local statistics), both on
+ * the ellipse and 0 elsewhere on the bw x bh grid, go through the kernel's
+ * DFT, cross-power, inverse DFT and peak search; out = peak distance. */
+int orc_block_phase(const float *img, const float *means, const float *stds, int W, int H, int bw, int bh,
+                    const float *ref_pixels, float ref_std, double *out) {
+    const int rw = bw / 2, rh = bh / 2, n = bw * bh;
+    if (n > 225) return -1;
+    double *tc = (double *)malloc(sizeof(double) * n * n), *ts = (double *)malloc(sizeof(double) * n * n);
+    orc_phase_tables(bw, bh, tc, ts);
+    double x[225], rr[225], ri[225];
+    int k = 0;
+    for (int j = 0; j < bh; j++)
+        for (int i = 0; i < bw; i++)
+            x[j * bw + i] = in_ellipse(i - rw, j - rh, rw, rh)
+                                ? (double)ref_pixels[k++] / ((double)ref_std + ORC_EPS) : 0.0;
+    orc_phase_dft(x, n, tc, ts, rr, ri);
+    #pragma omp parallel for schedule(dynamic, 4)
+    for (int y = 0; y < H; y++)
+        for (int xq = 0; xq < W; xq++) {
+            double x[225], cr[225], ci[225], xr[225], xi[225];
+            if (xq < rw || xq >= W - rw || y < rh || y >= H - rh) {
+                out[y * W + xq] = 0.0;
+                continue;
+            }
+            const double m = (double)means[y * W + xq], s = (double)stds[y * W + xq] + ORC_EPS;
+            for (int j = 0; j < bh; j++)
+                for (int i = 0; i < bw; i++)
+                    x[j * bw + i] = in_ellipse(i - rw, j - rh, rw, rh)
+                                        ? ((double)img[(y + j - rh) * W + xq + i - rw] - m) / s : 0.0;
+            orc_phase_dft(x, n, tc, ts, cr, ci);
+            out[y * W + xq] = (double)orc_phase_peak(rr, ri, cr, ci, bw, bh, tc, ts, xr, xi);
+        }
+    free(tc); free(ts);
+    return 0;
+}

@@ -22,3 +22,9 @@ def junit():
 def refshim_fx():
     import numpy as np
     return dict(np.load(ROOT / "tests" / "golden" / "global_refshim.npz"))
+
+
+@pytest.fixture(scope="session")
+def shape_fx():
+    import numpy as np
+    return dict(np.load(ROOT / "tests" / "golden" / "shape_refshim.npz"))

@@ -13,6 +13,12 @@ Two kinds of fixtures are written:
    small seeded synthetic images, with the Java host steps applied by the
    oracle. No reference test pins the global map; these frozen outputs do.
 
+3. ``shape_refshim.npz``: outputs of the reference's shape-metric kernels
+   (``cl/kernelGetPatchHu2D.cl``, ``cl/kernelGetHuMap.cl`` and, with the
+   repairs listed in ``oracle/refshim/build.py``,
+   ``cl/kernelGetPhaseCorrelationMap.cl``), compiled the same way, on small
+   seeded images. No reference test covers these kernels.
+
 Usage: ``python tests/golden/make_golden.py [--reference /root/reference]``
 """
 from __future__ import annotations
@@ -176,6 +182,38 @@ def refshim_fixtures() -> dict:
     return fx
 
 
+SHAPE_CASES = [
+    # (name, W, H, lattice, seed, bw, bh, phase): the phase kernel's CPU cost
+    # grows with (W H)^2 (bw bh)^2, so it runs on the smaller cases only
+    ("spots32x28_3x3", 32, 28, 4, 21, 3, 3, True),
+    ("spots30x26_5x3", 30, 26, 5, 22, 5, 3, True),
+    ("spots40x36_5x5", 40, 36, 4, 23, 5, 5, False),
+    ("spots44x40_9x9", 44, 40, 3, 24, 9, 9, False),
+]
+
+
+def shape_fixtures() -> dict:
+    fx: dict = {}
+    cases = [(n, synth.normalize_input(synth.spot_image(W, H, lat, seed=seed)), bw, bh, ph)
+             for n, W, H, lat, seed, bw, bh, ph in SHAPE_CASES]
+    cases.append(("flat32x40_3x3", flat_image(), 3, 3, True))
+    for name, img, bw, bh, phase in cases:
+        fx[f"{name}/image"] = img
+        means, stds = oracle.local_stats(img, bw, bh)
+        y0, x0 = img.shape[0] // 2 - bh // 2, img.shape[1] // 3 - bw // 2
+        px, bm, bs = oracle.reference_block(img[y0:y0 + bh, x0:x0 + bw])
+        patch = oracle.hu_prepare_patch(px, bw, bh)
+        fx[f"{name}/block/pixels"] = px
+        fx[f"{name}/block/mean_std"] = np.array([bm, bs], np.float32)
+        fx[f"{name}/patch_hu/patch"] = patch
+        fx[f"{name}/patch_hu/map"] = oracle.patch_hu_map(patch, img, bw, bh, use_refshim=True)
+        fx[f"{name}/hu_map"] = oracle.hu_map(img, bw, bh, means, stds, use_refshim=True).astype(np.float32)
+        if phase:
+            fx[f"{name}/phase_map"] = oracle.phase_map(img, bw, bh, means, stds,
+                                                       use_refshim=True).astype(np.float32)
+    return fx
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -185,7 +223,10 @@ def main(argv=None) -> int:
     (HERE / "reference_junit.json").write_text(json.dumps(vec, indent=1))
     fx = refshim_fixtures()
     np.savez_compressed(HERE / "global_refshim.npz", **fx)
-    print("wrote", HERE / "reference_junit.json", "and", HERE / "global_refshim.npz", len(fx), "arrays")
+    sx = shape_fixtures()
+    np.savez_compressed(HERE / "shape_refshim.npz", **sx)
+    print("wrote", HERE / "reference_junit.json", HERE / "global_refshim.npz", len(fx), "arrays,",
+          HERE / "shape_refshim.npz", len(sx), "arrays")
     return 0
 
 

@@ -156,3 +156,85 @@ def test_f64_judge_close_to_f32(refshim_fx, metric):
     b = oracle.global_map(metric, img, 5, 5, 1.0, precision="f64")
     m = a["mask"] > 0
     np.testing.assert_allclose(a["map"][m], b["map"][m], atol=2e-5, rtol=0)
+
+
+# ---------------------------------------------------------------------------
+# Shape metrics (cl/kernelGetPatchHu2D.cl, cl/kernelGetHuMap.cl,
+# cl/kernelGetPhaseCorrelationMap.cl): the restatement against the
+# reference's kernels, frozen in tests/golden/shape_refshim.npz
+# ---------------------------------------------------------------------------
+
+def _shape_cases(fx):
+    for n in sorted({k.split("/")[0] for k in fx}):
+        bw, bh = (int(v) for v in n.rsplit("_", 1)[1].split("x"))
+        yield n, bw, bh
+
+
+def test_patch_hu_matches_refshim_fixtures(shape_fx):
+    fx = shape_fx
+    for name, bw, bh in _shape_cases(fx):
+        img = fx[f"{name}/image"]
+        patch = oracle.hu_prepare_patch(fx[f"{name}/block/pixels"], bw, bh)
+        assert np.array_equal(patch, fx[f"{name}/patch_hu/patch"]), name
+        got = oracle.patch_hu_map(patch, img, bw, bh)
+        assert np.array_equal(got, fx[f"{name}/patch_hu/map"], equal_nan=True), name
+
+
+def test_hu_map_matches_refshim_fixtures(shape_fx):
+    fx = shape_fx
+    for name, bw, bh in _shape_cases(fx):
+        got = oracle.hu_map(fx[f"{name}/image"], bw, bh).astype(np.float32)
+        assert np.array_equal(got, fx[f"{name}/hu_map"]), name
+
+
+def test_phase_map_matches_refshim_fixtures(shape_fx):
+    fx = shape_fx
+    n = 0
+    for name, bw, bh in _shape_cases(fx):
+        if f"{name}/phase_map" not in fx:
+            continue
+        got = oracle.phase_map(fx[f"{name}/image"], bw, bh).astype(np.float32)
+        assert np.array_equal(got, fx[f"{name}/phase_map"]), name
+        n += 1
+    assert n >= 3
+
+
+def test_shape_f64_judges_close_to_f32(shape_fx):
+    """The FP64-accumulated judges agree with the FP32 reference order."""
+    img = shape_fx["spots32x28_3x3/image"]
+    for fn in (oracle.hu_map, oracle.phase_map):
+        a = fn(img, 3, 3)
+        b = fn(img, 3, 3, precision="f64")
+        assert float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-30))) < 2e-5
+
+
+@pytest.mark.skipif(oracle.refshim() is None, reason="refshim not built")
+def test_shape_matches_refshim_live():
+    from sred_b200 import synth
+    img = synth.normalize_input(synth.spot_image(26, 22, 4, seed=98))
+    for bw, bh in ((3, 5), (7, 7)):
+        patch = oracle.hu_prepare_patch(oracle.reference_block(img[5:5 + bh, 6:6 + bw])[0], bw, bh)
+        assert np.array_equal(oracle.patch_hu_map(patch, img, bw, bh),
+                              oracle.patch_hu_map(patch, img, bw, bh, use_refshim=True))
+        assert np.array_equal(oracle.hu_map(img, bw, bh), oracle.hu_map(img, bw, bh, use_refshim=True))
+    assert np.array_equal(oracle.phase_map(img, 3, 5), oracle.phase_map(img, 3, 5, use_refshim=True))
+
+
+def test_block_phase_self_peak():
+    """A block compared with itself peaks at displacement (0, 0): the
+    1-based coordinates (1, 1) give sqrt(2)."""
+    from sred_b200 import synth
+    img = synth.normalize_input(synth.spot_image(30, 24, 4, seed=97))
+    bw = bh = 5
+    means, stds = oracle.local_stats(img, bw, bh)
+    y, x = 11, 13
+    # the block's own normalised ellipse pixels as the reference block
+    K = oracle.block_size(bw, bh)
+    blk = img[y - 2:y + 3, x - 2:x + 3]
+    f = np.float32
+    px = [blk[j, i] for j in range(5) for i in range(5)
+          if (f(i - 2) ** 2) / f(4) + (f(j - 2) ** 2) / f(4) <= f(1)]
+    px = np.array(px, np.float32) - means[y, x]
+    assert px.size == K
+    out = oracle.block_phase_raw(img, px, bw, bh, stds[y, x], means, stds)
+    assert abs(out[y, x] - np.sqrt(2.0)) < 1e-6
