@@ -114,8 +114,20 @@ sred_status sred_global_map_2d_device(sred_ctx *ctx, const char *metric, const f
  * block_size, bw, bh, ref_mean and ref_std are the ReferenceBlock2D fields
  * (java/Utils.java:108-216), passed through unchanged. metric:
  * "Pearson's R", "SSIM", "NRMSE (inverted)", "Abs. Diff. of StdDevs." (the
- * reference's four), or "Cosine" (raw-vector cosine similarity; no reference
- * counterpart, same post-processing as Pearson). */
+ * reference's four), or one of three without a dialog entry in the
+ * reference, all post-processed like Pearson:
+ *   "Cosine"            raw-vector cosine similarity;
+ *   "Hu moments"        cl/kernelGetPatchHu2D.cl (sqrt(hu1_ref * hu1_block))
+ *                       with the reference block's ellipse pixels normalised
+ *                       the way that kernel normalises each block
+ *                       (mean-subtract, min-max to [0, 1], FP64);
+ *   "Phase correlation" the peak distance of
+ *                       cl/kernelGetPhaseCorrelationMap.cl's normalised
+ *                       cross-power spectrum (repaired as for
+ *                       sred_phase_correlation_map_2d) between the reference
+ *                       block / (ref_std + eps) and each block, normalised
+ *                       with its FP32 local mean and std, both restricted to
+ *                       the ellipse; bw, bh <= 15. */
 sred_status sred_calculate_block_repetition_map_2d(sred_ctx *ctx, const char *metric, const float *img,
                                                    int w, int h, const float *ref_pixels, int block_size,
                                                    int bw, int bh, float ref_mean, float ref_std,
@@ -140,6 +152,42 @@ sred_status sred_reference_block_2d(const float *block_img, int bw, int bh, floa
  * mask may be NULL. SRED_ERR_ARG for a non-binary mask. */
 sred_status sred_normalize_image_2d(float *img, int w, int h, int border_w, int border_h,
                                     const float *mask);
+
+/* The reference's shape-metric kernels, which it ships in
+ * src/main/resources/ but never loads from its Java code. Host memory in and
+ * out; border pixels of `out` are 0.
+ *
+ * Replaces cl/kernelGetPatchHu2D.cl:11-282: for every interior pixel
+ * (float)sqrt(hu1(patch) * hu1(block)), FP64, with the kernel's own
+ * arithmetic (raw moments at 1-based and central moments at 0-based
+ * coordinates; the block mean summed over the square minus its four corners
+ * and divided by patch_size; min-max remap over the ellipse). patch: the
+ * bw x bh grid the kernel reads at the ellipse positions; patch_size: its
+ * $PATCH_SIZE$ (the reference's Java convention is the ellipse count K). */
+sred_status sred_patch_hu_map_2d(sred_ctx *ctx, const float *patch, const float *img, int w, int h, int bw,
+                                 int bh, int patch_size, float *out);
+
+/* Replaces cl/kernelGetHuMap.cl:15-172 (speedUp off): for every interior
+ * pixel p, the sum over every interior pixel q of |hu_q - hu_p| *
+ * (100^s - 1) / 99 with s = 1 - |std_p - std_q| / (|std_p| + |std_q| + eps),
+ * where hu is the FP32 invariant(2,0) + invariant(0,2) of the whole square
+ * block minus the local mean. FP32 terms, FP64 sums. local_means/local_stds
+ * are CLLocalStatistics' buffers (sred_local_statistics_2d). */
+sred_status sred_hu_map_2d(sred_ctx *ctx, const float *img, const float *local_means, const float *local_stds,
+                           int w, int h, int bw, int bh, float *out);
+
+/* Replaces cl/kernelGetPhaseCorrelationMap.cl:13-179 (speedUp off), which does
+ * not compile as shipped, with its three defects repaired: no unique-pixel
+ * pre-filter (nUnique is never defined, :27), real-valued DFT phases (the
+ * shipped (1*i*ii/bW) divides integers, :66/:101/:138) and the peak search
+ * indexed by the block width (:150 uses the image width). For every interior
+ * pixel p, the sum over every interior q of |peak_pq| * weight(std_p, std_q),
+ * peak_pq the 1-based position of the first maximum above 0 of the inverse
+ * DFT of the normalised cross-power spectrum of the two whole square blocks,
+ * each normalised as (x - mean) / (std + eps). FP64, FP64 sums. bw, bh <= 15;
+ * the cost grows as (interior pixels)^2 * bw * bh * (bw + bh). */
+sred_status sred_phase_correlation_map_2d(sred_ctx *ctx, const float *img, const float *local_means,
+                                          const float *local_stds, int w, int h, int bw, int bh, float *out);
 
 /* Block map that allocates nothing (no counterpart in the reference): for
  * callers that cannot call cudaMalloc, such as code inside a CUDA graph being

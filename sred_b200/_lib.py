@@ -24,6 +24,7 @@ EXPORTS = [
     "sred_calculate_global_repetition_map_2d", "sred_global_map_2d", "sred_global_map_2d_device",
     "sred_calculate_block_repetition_map_2d", "sred_block_map_2d_device", "sred_reference_block_2d",
     "sred_normalize_image_2d", "sred_debug_gram_rowdot", "sred_block_map_2d_device_noalloc",
+    "sred_patch_hu_map_2d", "sred_hu_map_2d", "sred_phase_correlation_map_2d",
 ]
 
 
@@ -91,6 +92,9 @@ def load() -> C.CDLL:
         L.sred_debug_gram_rowdot.argtypes = [_vp, s, _f32p, _f32p, _f32p, s, s, _f64p, _f64p]
         L.sred_block_map_2d_device_noalloc.argtypes = [C.c_char_p, _vp, s, s, s, _f32p, s, s, s, C.c_float,
                                                        C.c_float, s, _vp, _vp]
+        L.sred_patch_hu_map_2d.argtypes = [_vp, _f32p, _f32p, s, s, s, s, s, _f32p]
+        L.sred_hu_map_2d.argtypes = [_vp, _f32p, _f32p, _f32p, s, s, s, s, _f32p]
+        L.sred_phase_correlation_map_2d.argtypes = [_vp, _f32p, _f32p, _f32p, s, s, s, s, _f32p]
         _lib = L
     return _lib
 

@@ -21,6 +21,10 @@ from .utils import InputImage2D, ReferenceBlock2D, RelevanceMask
 GLOBAL_METRICS = ["Pearson's R", "SSIM", "NRMSE", "Abs. diff. of StdDevs"]  # java/GlobalRepetition2D_.java:20-25
 BLOCK_METRICS = ["Pearson's R", "SSIM", "NRMSE (inverted)", "Abs. Diff. of StdDevs."]  # java/BlockRepetition2D_.java:18-23
 COSINE = "Cosine"  # raw-vector cosine similarity; no reference counterpart
+# Block-map forms of the reference's shape-metric kernels (no dialog entry in the reference).
+HU = "Hu moments"  # cl/kernelGetPatchHu2D.cl
+PHASE = "Phase correlation"  # cl/kernelGetPhaseCorrelationMap.cl (repaired)
+EXTRA_BLOCK_METRICS = [COSINE, HU, PHASE]
 
 
 @dataclass
@@ -104,7 +108,7 @@ def calculate_block_repetition_map_2d(metric: str, input_image: InputImage2D, re
                                       relevance_constant: float, normalize_output: bool, use_device: bool = False,
                                       ctx=None):
     """java/CLUtils.java:995-1010."""
-    if metric not in BLOCK_METRICS and metric != COSINE:
+    if metric not in BLOCK_METRICS and metric not in EXTRA_BLOCK_METRICS:
         return None
     c = _ctx(ctx)
     out = np.zeros(input_image.size, np.float32)
@@ -129,6 +133,58 @@ get_block_pearson_2d = _block_getter("Pearson's R")
 get_block_ssim_2d = _block_getter("SSIM")
 get_block_nrmse_2d = _block_getter("NRMSE (inverted)")
 get_block_abs_diff_stds_2d = _block_getter("Abs. Diff. of StdDevs.")
+
+
+# ---------------------------------------------------------------------------
+# The reference's shape-metric kernels (src/main/resources/, never loaded by
+# its Java code): Hu moments and phase correlation.
+# ---------------------------------------------------------------------------
+
+def get_patch_hu_map_2d(input_image: InputImage2D, patch: np.ndarray, block_width: int, block_height: int,
+                        patch_size: int | None = None, ctx=None) -> np.ndarray:
+    """cl/kernelGetPatchHu2D.cl: sqrt(hu1(patch) * hu1(block)) per interior pixel.
+    ``patch`` is the bw x bh grid the kernel reads at the ellipse positions;
+    ``patch_size`` defaults to the ellipse count K."""
+    from .utils import block_size
+    c = _ctx(ctx)
+    out = np.zeros(input_image.size, np.float32)
+    ps = block_size(block_width, block_height) if patch_size is None else int(patch_size)
+    c.check(c._L.sred_patch_hu_map_2d(c.h, np.ascontiguousarray(patch, np.float32).ravel(),
+                                      np.ascontiguousarray(input_image.image_array, np.float32).ravel(),
+                                      input_image.width, input_image.height, block_width, block_height, ps, out),
+            "sred_patch_hu_map_2d")
+    return out
+
+
+def _stats_args(input_image, local_statistics):
+    return (np.ascontiguousarray(input_image.image_array, np.float32).ravel(),
+            np.ascontiguousarray(local_statistics.local_means, np.float32).ravel(),
+            np.ascontiguousarray(local_statistics.local_stds, np.float32).ravel())
+
+
+def get_hu_map_2d(input_image: InputImage2D, local_statistics: CLLocalStatistics, block_width: int,
+                  block_height: int, ctx=None) -> np.ndarray:
+    """cl/kernelGetHuMap.cl over all interior pairs (raw sums)."""
+    c = _ctx(ctx)
+    out = np.zeros(input_image.size, np.float32)
+    c.check(c._L.sred_hu_map_2d(c.h, *_stats_args(input_image, local_statistics), input_image.width,
+                                input_image.height, block_width, block_height, out), "sred_hu_map_2d")
+    return out
+
+
+def get_phase_correlation_map_2d(input_image: InputImage2D, local_statistics: CLLocalStatistics, block_width: int,
+                                 block_height: int, ctx=None) -> np.ndarray:
+    """cl/kernelGetPhaseCorrelationMap.cl (defects repaired) over all interior pairs (raw sums)."""
+    c = _ctx(ctx)
+    out = np.zeros(input_image.size, np.float32)
+    c.check(c._L.sred_phase_correlation_map_2d(c.h, *_stats_args(input_image, local_statistics),
+                                               input_image.width, input_image.height, block_width, block_height,
+                                               out), "sred_phase_correlation_map_2d")
+    return out
+
+
+get_block_hu_2d = _block_getter(HU)
+get_block_phase_correlation_2d = _block_getter(PHASE)
 
 
 def global_map_device(metric: str, d_img_ptr: int, width: int, height: int, block_width: int, block_height: int,

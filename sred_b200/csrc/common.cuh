@@ -14,7 +14,8 @@ constexpr float kC2 = 0.0009f;      // cl/kernelGetGlobalSsim2D.cl:104
 constexpr int kMaxK = 512;          // largest ellipse block size accepted
 
 enum Metric { kPearson = 0, kSsim = 1, kNrmse = 2, kAbsDiff = 3, kCosine = 4,
-              kDebugDot = 5 /* diagnostics: num += G a_p a_q, den += r_p + r_q */ };
+              kDebugDot = 5 /* diagnostics: num += G a_p a_q, den += r_p + r_q */,
+              kHu = 6, kPhase = 7 /* block-map shape metrics */ };
 
 // Ellipse pixel offsets (dx, dy), row-major ellipse order, as the kernels gather them.
 struct Ellipse {

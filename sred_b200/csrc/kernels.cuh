@@ -44,4 +44,16 @@ __global__ void k_interior_mask(float* mask, int W, int H, int rw, int rh, size_
 __global__ void k_apply_mask(float* a, const float* mask, size_t n);
 __global__ void k_invert_masked(float* a, const float* mask, int W, int H, int rw, int rh, size_t plane);
 
+// shape.cu (k_block_phase is declared in shape.cuh, next to PhaseRef)
+__global__ void k_patch_hu(const float* img, int W, int H, Ellipse e, int patch_size, double ref_hu1, float* out,
+                           float* stds_out);
+__global__ void k_hu_features(const float* img, const float* means, const float* stds, int W, int bw, int bh,
+                              int nx, int n, float* feat, float* sig);
+__global__ void k_hu_pairs(const float* feat, const float* sig, int n, int W, int rw, int rh, int nx, float* out);
+__global__ void k_phase_dft(const float* img, const float* means, const float* stds, int W, int bw, int bh, int nx,
+                            int n, double* fr, double* fi);
+__global__ void k_gather_interior(const float* a, int W, int rw, int rh, int nx, int n, float* out);
+__global__ void k_phase_pairs(const double* fr, const double* fi, const float* sig, int n, int bw, int bh, int W,
+                              int nx, float* out);
+
 }  // namespace sred

@@ -17,6 +17,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "shape.cuh"
 
 namespace {
 
@@ -68,6 +69,8 @@ int block_metric_id(const char* m) {
   if (!std::strcmp(m, "NRMSE (inverted)")) return sred::kNrmse;
   if (!std::strcmp(m, "Abs. Diff. of StdDevs.")) return sred::kAbsDiff;
   if (!std::strcmp(m, "Cosine")) return sred::kCosine;
+  if (!std::strcmp(m, "Hu moments")) return sred::kHu;
+  if (!std::strcmp(m, "Phase correlation")) return sred::kPhase;
   return -1;
 }
 
@@ -108,8 +111,22 @@ extern "C" sred_status sred_block_map_2d_device_noalloc(const char* metric, cons
   rb.std = ref_std;
   std::memcpy(rb.px, ref_pixels, sizeof(float) * block_size);
   const int rw = e.rw, rh = e.rh;
-  dim3 grid((w + 31) / 32, (h + 7) / 8, frames), blk(32, 8);
-  k_block_map<<<grid, blk, tile_smem, s>>>(d_img, w, h, frames, e, rb, m, d_out, nullptr);
+  if (m == kHu) {
+    float patch[kMaxK * 4];  // bw * bh < 4 K for every ellipse of K <= kMaxK
+    if (bw * bh > kMaxK * 4) return SRED_ERR_ARG;
+    hu_prepare_patch(ref_pixels, bw, bh, patch);
+    k_patch_hu<<<dim3((unsigned)((plane + 127) / 128), frames), 128, 0, s>>>(
+        d_img, w, h, e, block_size, patch_hu1(patch, bw, bh), d_out, nullptr);
+  } else if (m == kPhase) {
+    if (bw > kPhaseMaxDim || bh > kPhaseMaxDim) return SRED_ERR_ARG;
+    PhaseRef pr;
+    phase_reference_dft(ref_pixels, ref_std, bw, bh, &pr);
+    k_block_phase<<<dim3((unsigned)((plane + 127) / 128), frames), 128, 0, s>>>(d_img, w, h, e, bw, bh, pr,
+                                                                                  d_out, nullptr);
+  } else {
+    dim3 grid((w + 31) / 32, (h + 7) / 8, frames), blk(32, 8);
+    k_block_map<<<grid, blk, tile_smem, s>>>(d_img, w, h, frames, e, rb, m, d_out, nullptr);
+  }
   const dim3 pg(grid_of(plane, 256, 4 * sms), frames);
   const int ig = grid_of((size_t)frames, 256, 64);
   // The relevance constant is 0 here: the mask is the interior for NRMSE

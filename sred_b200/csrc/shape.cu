@@ -1,0 +1,344 @@
+// Shape metrics: Hu moments and phase correlation (kernels and host helpers).
+//
+// This file is compiled with -fmad=false: the Hu kernels restate the
+// reference's FP32/FP64 evaluation order statement for statement, and a fused
+// multiply-add would round differently.
+#include <float.h>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "shape.cuh"
+
+namespace sred {
+
+// ---------------------------------------------------------------------------
+// Hu patch map: kernelGetPatchHu2D.cl:18-267 (FP64), one thread per pixel.
+// stds_out (optional): the pixel's FP32 local standard deviation, which the
+// relevance mask of the block-map form needs.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128)
+    k_patch_hu(const float* __restrict__ img_all, int W, int H, Ellipse e, int patch_size, double ref_hu1,
+               float* __restrict__ out_all, float* __restrict__ stds_out) {
+  const size_t plane = (size_t)W * H;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= plane) return;
+  const size_t off = (size_t)blockIdx.y * plane;
+  const float* img = img_all + off;
+  float* out = out_all + off;
+  const int x = (int)(idx % W), y = (int)(idx / W), rw = e.rw, rh = e.rh;
+  if (x < rw || x >= W - rw || y < rh || y >= H - rh) {
+    out[idx] = 0.0f;
+    if (stds_out) stds_out[off + idx] = 0.0f;
+    return;
+  }
+  if (stds_out) {
+    float m, sd;
+    block_stats_f32(img + idx, W, e, &m, &sd);
+    stds_out[off + idx] = sd;
+  }
+  // :129-140: the gather's ellipse test divides integers, which keeps every
+  // position of the square except its four corners; the sum is divided by
+  // patch_size all the same.
+  double mean = 0.0;
+  for (int j = -rh; j <= rh; j++)
+    for (int i = -rw; i <= rw; i++) {
+      const float dx = (float)(i / rw), dy = (float)(j / rh);
+      if (dx * dx + dy * dy <= 1.0f) mean += (double)img[(size_t)(y + j) * W + x + i];
+    }
+  mean /= (double)patch_size;
+  // :143-171: mean-subtract and min/max over the ellipse (raster order).
+  double mn = DBL_MAX, mx = -DBL_MAX;
+  for (int k = 0; k < e.k; k++) {
+    const double p = (double)img[(size_t)(y + e.dy[k]) * W + x + e.dx[k]] - mean;
+    mn = p < mn ? p : mn;
+    mx = mx < p ? p : mx;
+  }
+  const double den = mx - mn + (double)kEps;
+  // :174-205: remap to [0, 1] and raw moments (1-based coordinates).
+  double m00 = 0.0, m10 = 0.0, m01 = 0.0;
+  for (int k = 0; k < e.k; k++) {
+    const double r = (((double)img[(size_t)(y + e.dy[k]) * W + x + e.dx[k]] - mean) - mn) / den;
+    m00 += r;
+    m10 += (double)(e.dx[k] + rw + 1) * r;
+    m01 += (double)(e.dy[k] + rh + 1) * r;
+  }
+  // :207-239: central moments around that centroid with 0-based coordinates.
+  const double cx = m10 / (m00 + (double)kEps), cy = m01 / (m00 + (double)kEps);
+  double mu20 = 0.0, mu02 = 0.0;
+  for (int k = 0; k < e.k; k++) {
+    const double r = (((double)img[(size_t)(y + e.dy[k]) * W + x + e.dx[k]] - mean) - mn) / den;
+    const double ax = (double)(e.dx[k] + rw) - cx, ay = (double)(e.dy[k] + rh) - cy;
+    mu20 += (ax * ax) * r;
+    mu02 += (ay * ay) * r;
+  }
+  const double m2 = m00 * m00 + (double)kEps;
+  const double hu1 = mu20 / m2 + mu02 / m2;
+  out[idx] = (float)sqrt(ref_hu1 * hu1);  // :267
+}
+
+// ---------------------------------------------------------------------------
+// Hu map, kernelGetHuMap.cl (FP32): per-block feature, then all pairs.
+// ---------------------------------------------------------------------------
+
+// :62-80 / :109-124 with getInvariant (:146-172): the whole square block minus
+// the block's local mean; invariant(2,0) + invariant(0,2). Both invariants
+// accumulate mu_00 in the same order, so it is summed once.
+__global__ void k_hu_features(const float* __restrict__ img, const float* __restrict__ means,
+                              const float* __restrict__ stds, int W, int bw, int bh, int nx, int n,
+                              float* __restrict__ feat, float* __restrict__ sig) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int rw = bw / 2, rh = bh / 2;
+  const int x = rw + t % nx, y = rh + t / nx;
+  float x_avg = 0.0f;
+  for (int i = 1; i <= bw; i++) x_avg += (float)i;
+  x_avg /= (float)bw;
+  float y_avg = 0.0f;
+  for (int i = 1; i <= bh; i++) y_avg += (float)i;
+  y_avg /= (float)bh;
+  const float m = means[(size_t)y * W + x];
+  float s20 = 0.0f, s02 = 0.0f, m00 = 0.0f;
+  for (int j = 0; j < bh; j++) {
+    const float b = (float)j + 1.0f - y_avg;
+    for (int i = 0; i < bw; i++) {
+      const float a = (float)i + 1.0f - x_avg;
+      const float p = img[(size_t)(y - rh + j) * W + x - rw + i] - m;
+      s20 += (a * a) * p;  // pow(a, 2) * pow(b, 0) * p
+      s02 += (b * b) * p;  // pow(a, 0) * pow(b, 2) * p
+      m00 += p;
+    }
+  }
+  const float mu00 = m00 * m00;  // pow(mu_00, 1 + (p + q) / 2) with p + q = 2
+  feat[t] = s20 / (mu00 + kEps) + s02 / (mu00 + kEps);
+  sig[t] = stds[(size_t)y * W + x];
+}
+
+constexpr int kHuChunk = 2048;
+
+// :82-132: hu_map[p] = sum_q |hu_q - hu_p| * weight(sigma_p, sigma_q), with
+// weight = (100^similarity - 1) / 99 (getExpDecayWeight, :136-144). One
+// thread per reference block; FP32 terms, FP32 runs of 32 added into FP64.
+__global__ void __launch_bounds__(256)
+    k_hu_pairs(const float* __restrict__ feat, const float* __restrict__ sig, int n, int W, int rw, int rh,
+               int nx, float* __restrict__ out) {
+  __shared__ float sf[kHuChunk], ss[kHuChunk];
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const float hp = p < n ? feat[p] : 0.0f, sp = p < n ? sig[p] : 0.0f;
+  const float asp = fabsf(sp);
+  double acc = 0.0;
+  for (int q0 = 0; q0 < n; q0 += kHuChunk) {
+    const int m = min(kHuChunk, n - q0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+      sf[i] = feat[q0 + i];
+      ss[i] = sig[q0 + i];
+    }
+    __syncthreads();
+    for (int t0 = 0; t0 < m; t0 += 32) {
+      const int t1 = min(m, t0 + 32);
+      float part = 0.0f;
+      for (int t = t0; t < t1; t++) {
+        const float sq = ss[t];
+        const float sim = 1.0f - __fdiv_rn(fabsf(sp - sq), asp + fabsf(sq) + kEps);
+        const float w = __fdiv_rn(exp2f(sim * kLog2Hundred) - 1.0f, 99.0f);
+        part += fabsf(sf[t] - hp) * w;
+      }
+      acc += (double)part;
+    }
+  }
+  if (p < n) out[(size_t)(rh + p / nx) * W + rw + p % nx] = (float)acc;
+}
+
+// ---------------------------------------------------------------------------
+// Phase correlation (kernelGetPhaseCorrelationMap.cl with its three defects
+// repaired), FP64.
+// ---------------------------------------------------------------------------
+
+// Twiddles of both axes into shared memory, all threads of the block.
+__device__ __forceinline__ void phase_twiddles_smem(int bw, int bh, double* cw, double* sw, double* ch,
+                                                    double* sh) {
+  for (int t = threadIdx.x; t < bw * bw; t += blockDim.x) {
+    const double ang = 2 * kPhasePi * (1.0 * (t / bw) * (t % bw) / bw);
+    cw[t] = cos(ang);
+    sw[t] = sin(ang);
+  }
+  for (int t = threadIdx.x; t < bh * bh; t += blockDim.x) {
+    const double ang = 2 * kPhasePi * (1.0 * (t / bh) * (t % bh) / bh);
+    ch[t] = cos(ang);
+    sh[t] = sin(ang);
+  }
+}
+
+// :46-71 / :80-106: DFT of every interior block's whole square patch,
+// normalised as (x - mean) / (std + eps). F[q * bw*bh + k].
+__global__ void __launch_bounds__(128)
+    k_phase_dft(const float* __restrict__ img, const float* __restrict__ means, const float* __restrict__ stds,
+                int W, int bw, int bh, int nx, int n, double* __restrict__ fr, double* __restrict__ fi) {
+  __shared__ double tw[4 * kPhaseMaxN];
+  double *cw = tw, *sw = tw + bw * bw, *ch = sw + bw * bw, *sh = ch + bh * bh;
+  phase_twiddles_smem(bw, bh, cw, sw, ch, sh);
+  __syncthreads();
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int rw = bw / 2, rh = bh / 2, nn = bw * bh;
+  const int x = rw + q % nx, y = rh + q / nx;
+  const double m = (double)means[(size_t)y * W + x], s = (double)stds[(size_t)y * W + x] + (double)kEps;
+  double work[kPhaseMaxN + kPhaseTmp];  // [patch | temporaries]
+  double* xg = work;
+  for (int j = 0; j < bh; j++)
+    for (int i = 0; i < bw; i++) xg[j * bw + i] = ((double)img[(size_t)(y - rh + j) * W + x - rw + i] - m) / s;
+  phase_dft(xg, bw, bh, cw, sw, ch, sh, fr + (size_t)q * nn, fi + (size_t)q * nn, work + kPhaseMaxN);
+}
+
+// :73-163: one CTA per reference block p, threads over comparison blocks q;
+// phase_map[p] = sum_q |peak_pq| * weight(sigma_p, sigma_q), summed in FP64 in
+// a fixed order.
+__global__ void __launch_bounds__(128)
+    k_phase_pairs(const double* __restrict__ fr, const double* __restrict__ fi, const float* __restrict__ sig,
+                  int n, int bw, int bh, int W, int nx, float* __restrict__ out) {
+  __shared__ double tw[4 * kPhaseMaxN];
+  __shared__ double pr[kPhaseMaxN], pi[kPhaseMaxN];
+  __shared__ double red[128];
+  double *cw = tw, *sw = tw + bw * bw, *ch = sw + bw * bw, *sh = ch + bh * bh;
+  const int p = blockIdx.x, nn = bw * bh;
+  phase_twiddles_smem(bw, bh, cw, sw, ch, sh);
+  for (int k = threadIdx.x; k < nn; k += blockDim.x) {
+    pr[k] = fr[(size_t)p * nn + k];
+    pi[k] = fi[(size_t)p * nn + k];
+  }
+  __syncthreads();
+  const float sp = sig[p];
+  double acc = 0.0;
+  double work[2 * kPhaseMaxN + kPhaseTmp];  // [cross re | cross im | temporaries]
+  double *cr = work, *ci = work + kPhaseMaxN;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    const double* qr = fr + (size_t)q * nn;
+    const double* qi = fi + (size_t)q * nn;
+    for (int k = 0; k < nn; k++) phase_cross(pr[k], pi[k], qr[k], qi[k], &cr[k], &ci[k]);
+    const float d = phase_peak(cr, ci, bw, bh, cw, sw, ch, sh, work + 2 * kPhaseMaxN);
+    acc += (double)d * (double)phase_weight(sp, sig[q]);
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = 64; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const int rw = bw / 2, rh = bh / 2;
+    out[(size_t)(rh + p / nx) * W + rw + p % nx] = (float)red[0];
+  }
+}
+
+// Block-map form: the reference block's DFT against each block's, one thread
+// per pixel. Blocks are normalised with their FP32 local statistics (computed
+// here, and written to stds_out when it is given) and restricted to the
+// ellipse (0 elsewhere on the bw x bh grid).
+__global__ void __launch_bounds__(128)
+    k_block_phase(const float* __restrict__ img_all, int W, int H, Ellipse e, int bw, int bh, PhaseRef ref,
+                  float* __restrict__ out_all, float* __restrict__ stds_out) {
+  __shared__ double tw[4 * kPhaseMaxN];
+  double *cw = tw, *sw = tw + bw * bw, *ch = sw + bw * bw, *sh = ch + bh * bh;
+  phase_twiddles_smem(bw, bh, cw, sw, ch, sh);
+  __syncthreads();
+  const size_t plane = (size_t)W * H;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= plane) return;
+  const size_t off = (size_t)blockIdx.y * plane;
+  const float* img = img_all + off;
+  float* out = out_all + off;
+  const int x = (int)(idx % W), y = (int)(idx / W), rw = e.rw, rh = e.rh, nn = bw * bh;
+  if (x < rw || x >= W - rw || y < rh || y >= H - rh) {
+    out[idx] = 0.0f;
+    if (stds_out) stds_out[off + idx] = 0.0f;
+    return;
+  }
+  float mf, sf;
+  block_stats_f32(img + idx, W, e, &mf, &sf);
+  if (stds_out) stds_out[off + idx] = sf;
+  const double m = (double)mf, s = (double)sf + (double)kEps;
+  double work[3 * kPhaseMaxN + kPhaseTmp];  // [patch | spectrum re | spectrum im | temporaries]
+  double *xg = work, *cr = work + kPhaseMaxN, *ci = work + 2 * kPhaseMaxN, *tmp = work + 3 * kPhaseMaxN;
+  for (int k = 0; k < nn; k++) xg[k] = 0.0;
+  for (int k = 0; k < e.k; k++)
+    xg[(e.dy[k] + rh) * bw + e.dx[k] + rw] = ((double)img[(size_t)(y + e.dy[k]) * W + x + e.dx[k]] - m) / s;
+  phase_dft(xg, bw, bh, cw, sw, ch, sh, cr, ci, tmp);
+  for (int k = 0; k < nn; k++) phase_cross(ref.re[k], ref.im[k], cr[k], ci[k], &cr[k], &ci[k]);
+  out[idx] = phase_peak(cr, ci, bw, bh, cw, sw, ch, sh, tmp);
+}
+
+// Values of `a` at the interior pixels, in interior raster order.
+__global__ void k_gather_interior(const float* __restrict__ a, int W, int rw, int rh, int nx, int n,
+                                  float* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) out[t] = a[(size_t)(rh + t / nx) * W + rw + t % nx];
+}
+
+// ---------------------------------------------------------------------------
+// Host helpers
+// ---------------------------------------------------------------------------
+
+// The reference block of the block-map Hu metric: ReferenceBlock2D pixels
+// (ellipse order) on the bw x bh grid, mean-subtracted over the ellipse and
+// min-max remapped to [0, 1] in FP64 as kernelGetPatchHu2D.cl:126-182 does to
+// every comparison patch; stored as float like the kernel's patch buffer.
+void hu_prepare_patch(const float* ref_pixels, int bw, int bh, float* grid) {
+  Ellipse e;
+  const int K = build_ellipse(bw, bh, &e);
+  double v[kMaxK];
+  double mean = 0.0;
+  for (int k = 0; k < K; k++) {
+    v[k] = (double)ref_pixels[k];
+    mean += v[k];
+  }
+  mean /= (double)K;
+  double mn = DBL_MAX, mx = -DBL_MAX;
+  for (int k = 0; k < K; k++) {
+    v[k] -= mean;
+    mn = v[k] < mn ? v[k] : mn;
+    mx = mx < v[k] ? v[k] : mx;
+  }
+  for (int i = 0; i < bw * bh; i++) grid[i] = 0.0f;
+  for (int k = 0; k < K; k++)
+    grid[(e.dy[k] + e.rh) * bw + e.dx[k] + e.rw] = (float)((v[k] - mn) / (mx - mn + (double)kEps));
+}
+
+// Hu invariant 1 of the patch as kernelGetPatchHu2D.cl:51-101 computes it for
+// its reference patch.
+double patch_hu1(const float* patch, int bw, int bh) {
+  Ellipse e;
+  const int K = build_ellipse(bw, bh, &e);
+  double m00 = 0.0, m10 = 0.0, m01 = 0.0;
+  for (int k = 0; k < K; k++) {
+    const int i = e.dx[k] + e.rw, j = e.dy[k] + e.rh;
+    const double p = (double)patch[j * bw + i];
+    m00 += p;
+    m10 += (double)(i + 1) * p;
+    m01 += (double)(j + 1) * p;
+  }
+  const double cx = m10 / (m00 + (double)kEps), cy = m01 / (m00 + (double)kEps);
+  double mu20 = 0.0, mu02 = 0.0;
+  for (int k = 0; k < K; k++) {
+    const int i = e.dx[k] + e.rw, j = e.dy[k] + e.rh;
+    const double p = (double)patch[j * bw + i];
+    mu20 += pow(((double)i - cx), 2.0) * p;
+    mu02 += pow(((double)j - cy), 2.0) * p;
+  }
+  const double nu20 = mu20 / (pow(m00, 2.0) + (double)kEps);
+  const double nu02 = mu02 / (pow(m00, 2.0) + (double)kEps);
+  return nu20 + nu02;
+}
+
+void phase_reference_dft(const float* ref_pixels, float ref_std, int bw, int bh, PhaseRef* out) {
+  Ellipse e;
+  const int K = build_ellipse(bw, bh, &e);
+  double xg[kPhaseMaxN], tmp[kPhaseTmp], cw[kPhaseMaxN], sw[kPhaseMaxN], ch[kPhaseMaxN], sh[kPhaseMaxN];
+  for (int k = 0; k < bw * bh; k++) xg[k] = 0.0;
+  for (int k = 0; k < K; k++)
+    xg[(e.dy[k] + e.rh) * bw + e.dx[k] + e.rw] = (double)ref_pixels[k] / ((double)ref_std + (double)kEps);
+  phase_twiddles(bw, cw, sw);
+  phase_twiddles(bh, ch, sh);
+  phase_dft(xg, bw, bh, cw, sw, ch, sh, out->re, out->im, tmp);
+}
+
+}  // namespace sred

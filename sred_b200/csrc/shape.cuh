@@ -1,0 +1,176 @@
+// Shape metrics: Hu moments and phase correlation (device and host helpers).
+//
+// The reference ships three OpenCL kernels for these that its Java code never
+// loads (paths relative to src/main/resources/):
+//   kernelGetPatchHu2D.cl            one patch against every block, FP64
+//   kernelGetHuMap.cl                all pairs of blocks, FP32
+//   kernelGetPhaseCorrelationMap.cl  all pairs of blocks, FP64; it does not
+//                                    compile as shipped (nUnique undefined,
+//                                    :27), its DFT phases divide integers
+//                                    (:66, :101, :138) and its peak search
+//                                    indexes with the image width (:150).
+// libsred evaluates the first two with the kernels' own arithmetic and the
+// third with those three defects repaired (no unique-coordinate pre-filter,
+// real-valued phases, block-width indexing).
+//
+// Per-thread work arrays of the phase kernels live in ONE local array per
+// thread, carved into sections by offset (kPhaseWork*): with separate
+// local arrays, nvcc 12.9 for sm_100a gave the column temporaries of
+// phase_dft the same stack slots as the caller's input patch, and the DFT
+// read overwritten inputs.
+#pragma once
+#include <math.h>
+
+#include "common.cuh"
+
+namespace sred {
+
+constexpr int kPhaseMaxDim = 15;                    // phase correlation: bw, bh <= 15
+constexpr int kPhaseMaxN = kPhaseMaxDim * kPhaseMaxDim;
+constexpr int kPhaseTmp = 2 * kPhaseMaxDim;         // temporaries of phase_dft / phase_peak
+// The kernel's pi is a float literal widened to double (:44).
+constexpr double kPhasePi = (double)3.14159265358979323846f;
+constexpr float kLog2Hundred = 6.64385618977472469574f;  // log2(100)
+
+// DFT of the reference block of the block-map form, computed on the host.
+struct PhaseRef {
+  double re[kPhaseMaxN];
+  double im[kPhaseMaxN];
+};
+
+// Twiddle tables of one axis: c[a*len+b] = cos(2*PI*(1.0*a*b/len)), s = sin.
+// The product a*b is not reduced modulo len: PI is not pi, so the reduction
+// would change the angles.
+__host__ __device__ inline void phase_twiddles(int len, double* c, double* s) {
+  for (int a = 0; a < len; a++)
+    for (int b = 0; b < len; b++) {
+      const double ang = 2 * kPhasePi * (1.0 * a * b / len);
+      c[a * len + b] = cos(ang);
+      s[a * len + b] = sin(ang);
+    }
+}
+
+// F = DFT(x) / sqrt(bw bh) of a real bw x bh patch (x row-major), the
+// reference's sum over exp(-i 2 PI (i ii / bw + j jj / bh)) evaluated
+// separably one output column at a time:
+//   T[jj] = sum_ii x[jj][ii] e^{-i a(i, ii)},  F[j][i] = sum_jj T[jj] e^{-i b(j, jj)}.
+// tmp: kPhaseTmp doubles, disjoint from x, fr and fi.
+__host__ __device__ inline void phase_dft(const double* x, int bw, int bh, const double* cw, const double* sw,
+                                          const double* ch, const double* sh, double* fr, double* fi,
+                                          double* tmp) {
+  const double sn = sqrt((double)(bw * bh));
+  double* tr = tmp;
+  double* ti = tmp + kPhaseMaxDim;
+  for (int i = 0; i < bw; i++) {
+    for (int jj = 0; jj < bh; jj++) {
+      double ar = 0.0, ai = 0.0;
+      for (int ii = 0; ii < bw; ii++) {
+        const double v = x[jj * bw + ii];
+        ar += v * cw[i * bw + ii];
+        ai -= v * sw[i * bw + ii];
+      }
+      tr[jj] = ar;
+      ti[jj] = ai;
+    }
+    for (int j = 0; j < bh; j++) {
+      double br = 0.0, bi = 0.0;
+      for (int jj = 0; jj < bh; jj++) {
+        const double c = ch[j * bh + jj], s = sh[j * bh + jj];
+        br += tr[jj] * c + ti[jj] * s;
+        bi += ti[jj] * c - tr[jj] * s;
+      }
+      fr[j * bw + i] = br / sn;
+      fi[j * bw + i] = bi / sn;
+    }
+  }
+}
+
+// Normalised cross-power of one frequency (:108-130): m = ref * conj(comp),
+// out = (m_r|m_r| + m_i|m_i|, m_i|m_r| - m_r|m_i|) / (m_r^2 + m_i^2 + eps).
+__host__ __device__ inline void phase_cross(double rr, double ri, double qr, double qi, double* xr, double* xi) {
+  const double conj = (-1) * qi;
+  const double mr = rr * qr - ri * conj;
+  const double mi = rr * conj + ri * qr;
+  const double ar = fabs(mr), ai = fabs(mi);
+  *xr = ((mr * ar) + (mi * ai)) / ((ar * ar) + (ai * ai) + (double)kEps);
+  *xi = ((mi * ar) - (mr * ai)) / ((ar * ar) + (ai * ai) + (double)kEps);
+}
+
+// Inverse DFT (real part, :132-142) of the cross-power spectrum and peak
+// search (:144-157): the first strict maximum above 0 in raster order, at
+// 1-based coordinates (x, y); returns (float)sqrt(x^2 + y^2), 0 when no value
+// is positive. Evaluated separably one output column at a time; ties keep
+// the lowest raster index, which is what the raster scan keeps.
+// tmp: kPhaseTmp doubles, disjoint from cr and ci.
+__host__ __device__ inline float phase_peak(const double* cr, const double* ci, int bw, int bh, const double* cw,
+                                            const double* sw, const double* ch, const double* sh, double* tmp) {
+  const double sn = sqrt((double)(bw * bh));
+  double* sr = tmp;
+  double* si = tmp + kPhaseMaxDim;
+  double best = 0.0;
+  int bidx = -1;
+  for (int i = 0; i < bw; i++) {
+    for (int jj = 0; jj < bh; jj++) {
+      double ar = 0.0, ai = 0.0;
+      for (int ii = 0; ii < bw; ii++) {
+        const double c = cw[i * bw + ii], s = sw[i * bw + ii];
+        const double xr = cr[jj * bw + ii], xi = ci[jj * bw + ii];
+        ar += xr * c - xi * s;
+        ai += xr * s + xi * c;
+      }
+      sr[jj] = ar;
+      si[jj] = ai;
+    }
+    for (int j = 0; j < bh; j++) {
+      double v = 0.0;
+      for (int jj = 0; jj < bh; jj++) v += sr[jj] * ch[j * bh + jj] - si[jj] * sh[j * bh + jj];
+      v /= sn;
+      const int idx = j * bw + i;
+      if (v > best || (bidx >= 0 && v == best && idx < bidx)) {
+        best = v;
+        bidx = idx;
+      }
+    }
+  }
+  if (bidx < 0) return 0.0f;
+  const double x = (double)(bidx % bw + 1), y = (double)(bidx / bw + 1);
+  return (float)sqrt((x * x) + (y * y));
+}
+
+// getExpDecayWeight of kernelGetPhaseCorrelationMap.cl:167-179.
+__host__ __device__ inline float phase_weight(float ref, float comp) {
+  if (ref == comp) return 1.0f;
+  return 1 - (2 * (fabsf(ref - comp) / (fabsf(ref) + fabsf(comp))));
+}
+
+// Ellipse-block mean and (K-1) standard deviation of the pixel at `c`
+// (row stride W) in the FP32 order of cl/kernelGetLocalStatistics2D.cl:15-56,
+// the same sequence as k_local_stats.
+__device__ __forceinline__ void block_stats_f32(const float* c, int W, const Ellipse& e, float* mean_out,
+                                                float* std_out) {
+  float s = 0.0f;
+  for (int i = 0; i < e.k; i++) s = __fadd_rn(s, c[e.dy[i] * W + e.dx[i]]);
+  const float mean = __fdiv_rn(s, (float)e.k);
+  float v = 0.0f;
+  for (int i = 0; i < e.k; i++) {
+    const float d = __fsub_rn(c[e.dy[i] * W + e.dx[i]], mean);
+    v = __fadd_rn(v, __fmul_rn(d, d));
+  }
+  *mean_out = mean;
+  *std_out = __fsqrt_rn(__fdiv_rn(v, (float)(e.k - 1)));
+}
+
+// Block-map phase correlation against the reference block's DFT (shape.cu).
+__global__ void k_block_phase(const float* img, int W, int H, Ellipse e, int bw, int bh, PhaseRef ref, float* out,
+                              float* stds_out);
+
+// Host side (shape.cu).
+// Block-map Hu metric: the bw x bh reference patch (ellipse pixels of the
+// ReferenceBlock2D normalised like the kernel's comparison patches) and its
+// Hu invariant 1.
+void hu_prepare_patch(const float* ref_pixels, int bw, int bh, float* grid);
+double patch_hu1(const float* patch, int bw, int bh);
+// Block-map phase metric: DFT of the reference block.
+void phase_reference_dft(const float* ref_pixels, float ref_std, int bw, int bh, PhaseRef* out);
+
+}  // namespace sred

@@ -11,6 +11,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "shape.cuh"
 
 using namespace sred;
 
@@ -18,7 +19,8 @@ namespace {
 
 enum BufId {
   B_IMG, B_MEANS, B_STDS, B_MASK, B_MASKIN, B_FLAGS, B_SLOT, B_GPIX, B_FPIX, B_COUNTS, B_U, B_A, B_B,
-  B_PARAMS, B_RMAX, B_NUM, B_DEN, B_SUMS, B_OUT, B_VARS, B_MM, B_NMASK, B_BAD, B_STATUS, B_STDS2, B_COLSOA, B_NBUF
+  B_PARAMS, B_RMAX, B_NUM, B_DEN, B_SUMS, B_OUT, B_VARS, B_MM, B_NMASK, B_BAD, B_STATUS, B_STDS2, B_COLSOA,
+  B_FEAT, B_SIG, B_FR, B_FI, B_NBUF
 };
 
 struct DevBuf {
@@ -105,6 +107,8 @@ int block_metric(const char* m) {
   if (!std::strcmp(m, "NRMSE (inverted)")) return kNrmse;
   if (!std::strcmp(m, "Abs. Diff. of StdDevs.")) return kAbsDiff;
   if (!std::strcmp(m, "Cosine")) return kCosine;
+  if (!std::strcmp(m, "Hu moments")) return kHu;
+  if (!std::strcmp(m, "Phase correlation")) return kPhase;
   return -1;
 }
 
@@ -340,13 +344,37 @@ sred_status global_core(sred_ctx* c, int metric, const float* d_img, int w, int 
   return SRED_OK;
 }
 
+// Raw block map of the shape metrics (stds_out: FP32 local stds, or NULL).
+// Hu moments: cl/kernelGetPatchHu2D.cl with the reference block prepared by
+// hu_prepare_patch; phase correlation: the block-map form of
+// cl/kernelGetPhaseCorrelationMap.cl (k_block_phase).
+sred_status block_shape_launch(sred_ctx* c, int metric, const float* d_img, int w, int h, int frames,
+                               const Ellipse& e, const float* ref_pixels, int bw, int bh, float ref_std, float* d_out,
+                               float* d_stds, cudaStream_t st) {
+  const size_t plane = (size_t)w * h;
+  const dim3 grid((unsigned)((plane + 127) / 128), (unsigned)frames);
+  if (metric == kHu) {
+    std::vector<float> patch((size_t)bw * bh);
+    hu_prepare_patch(ref_pixels, bw, bh, patch.data());
+    k_patch_hu<<<grid, 128, 0, st>>>(d_img, w, h, e, e.k, patch_hu1(patch.data(), bw, bh), d_out, d_stds);
+  } else {
+    if (bw > kPhaseMaxDim || bh > kPhaseMaxDim)
+      return fail(c, SRED_ERR_ARG, "phase correlation supports blocks up to 15x15");
+    PhaseRef pr;
+    phase_reference_dft(ref_pixels, ref_std, bw, bh, &pr);
+    k_block_phase<<<grid, 128, 0, st>>>(d_img, w, h, e, bw, bh, pr, d_out, d_stds);
+  }
+  CK(cudaGetLastError());
+  return SRED_OK;
+}
+
 sred_status block_core(sred_ctx* c, int metric, const float* d_img, int w, int h, int frames,
                        const float* ref_pixels, int block_size, int bw, int bh, float ref_mean, float ref_std,
                        float relc, int normalize, float* d_out, cudaStream_t st) {
   Ellipse e;
   CKS(check_block(c, w, h, bw, bh, &e));
   if (block_size != e.k) return fail(c, SRED_ERR_ARG, "block_size does not match the ellipse of bw x bh");
-  if (frames < 1) return fail(c, SRED_ERR_ARG, "frames must be >= 1");
+  if (frames < 1 || frames > 65535) return fail(c, SRED_ERR_ARG, "frames must be in 1..65535");
   if (fault("launch")) return fail(c, SRED_ERR_LAUNCH, "injected launch failure");
   const int rw = e.rw, rh = e.rh;
   const size_t plane = (size_t)w * h, n = plane * frames;
@@ -358,12 +386,16 @@ sred_status block_core(sred_ctx* c, int metric, const float* d_img, int w, int h
   const bool need_mask = (metric == kNrmse) || relc > 0.0f;
   float* d_stds = nullptr;
   if (need_mask) CKS(ensure(c, B_STDS2, n, &d_stds));
-  dim3 grid((w + 31) / 32, (h + 7) / 8, frames), blk(32, 8);
-  size_t smem = sizeof(float) * (32 + 2 * rw) * (8 + 2 * rh);
-  if (smem > 200 * 1024) return fail(c, SRED_ERR_ARG, "block too large for the streaming tile");
-  if (smem > 48 * 1024)
-    CK(cudaFuncSetAttribute(k_block_map, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_block_map<<<grid, blk, smem, st>>>(d_img, w, h, frames, e, rb, metric, d_out, d_stds);
+  if (metric == kHu || metric == kPhase) {
+    CKS(block_shape_launch(c, metric, d_img, w, h, frames, e, ref_pixels, bw, bh, ref_std, d_out, d_stds, st));
+  } else {
+    dim3 grid((w + 31) / 32, (h + 7) / 8, frames), blk(32, 8);
+    size_t smem = sizeof(float) * (32 + 2 * rw) * (8 + 2 * rh);
+    if (smem > 200 * 1024) return fail(c, SRED_ERR_ARG, "block too large for the streaming tile");
+    if (smem > 48 * 1024)
+      CK(cudaFuncSetAttribute(k_block_map, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_block_map<<<grid, blk, smem, st>>>(d_img, w, h, frames, e, rb, metric, d_out, d_stds);
+  }
   CK(cudaGetLastError());
 
   float* d_mask = nullptr;
@@ -699,6 +731,115 @@ sred_status sred_debug_gram_rowdot(sred_ctx* c, int engine, const float* u, cons
   }
   CK(cudaMemcpyAsync(num, d_num, n * sizeof(double), cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(den, d_den, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return SRED_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Shape metrics on host memory: the reference's Hu and phase-correlation
+// kernels (shipped in src/main/resources/, never loaded by its Java code).
+// ---------------------------------------------------------------------------
+
+namespace {
+
+// Interior extent of the all-pairs shape maps.
+sred_status shape_interior(sred_ctx* c, int w, int h, const Ellipse& e, int* nx, int* ny) {
+  *nx = w - 2 * e.rw;
+  *ny = h - 2 * e.rh;
+  if (*nx <= 0 || *ny <= 0) return fail(c, SRED_ERR_ARG, "image has no interior block");
+  return SRED_OK;
+}
+
+// Uploads img, local means and stds; zeroes the output map.
+sred_status shape_inputs(sred_ctx* c, const float* img, const float* means, const float* stds, size_t n,
+                         float** d_img, float** d_m, float** d_s, float** d_out) {
+  cudaStream_t st = c->stream;
+  CKS(ensure(c, B_IMG, n, d_img));
+  CKS(ensure(c, B_MEANS, n, d_m));
+  CKS(ensure(c, B_STDS, n, d_s));
+  CKS(ensure(c, B_OUT, n, d_out));
+  CK(cudaMemcpyAsync(*d_img, img, n * sizeof(float), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(*d_m, means, n * sizeof(float), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(*d_s, stds, n * sizeof(float), cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(*d_out, 0, n * sizeof(float), st));
+  return SRED_OK;
+}
+
+}  // namespace
+
+sred_status sred_patch_hu_map_2d(sred_ctx* c, const float* patch, const float* img, int w, int h, int bw, int bh,
+                                 int patch_size, float* out) {
+  if (!c || !patch || !img || !out || patch_size <= 0) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  Ellipse e;
+  CKS(check_block(c, w, h, bw, bh, &e));
+  if (fault("launch")) return fail(c, SRED_ERR_LAUNCH, "injected launch failure");
+  const size_t n = (size_t)w * h;
+  cudaStream_t st = c->stream;
+  float *d_img, *d_out;
+  CKS(ensure(c, B_IMG, n, &d_img));
+  CKS(ensure(c, B_OUT, n, &d_out));
+  CK(cudaMemcpyAsync(d_img, img, n * sizeof(float), cudaMemcpyHostToDevice, st));
+  k_patch_hu<<<dim3((unsigned)((n + 127) / 128), 1), 128, 0, st>>>(d_img, w, h, e, patch_size,
+                                                                    patch_hu1(patch, bw, bh), d_out, nullptr);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return SRED_OK;
+}
+
+sred_status sred_hu_map_2d(sred_ctx* c, const float* img, const float* local_means, const float* local_stds, int w,
+                           int h, int bw, int bh, float* out) {
+  if (!c || !img || !local_means || !local_stds || !out) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  Ellipse e;
+  int nx, ny;
+  CKS(check_block(c, w, h, bw, bh, &e));
+  CKS(shape_interior(c, w, h, e, &nx, &ny));
+  if (fault("launch")) return fail(c, SRED_ERR_LAUNCH, "injected launch failure");
+  const size_t n = (size_t)w * h;
+  const int ni = nx * ny;
+  cudaStream_t st = c->stream;
+  float *d_img, *d_m, *d_s, *d_out, *d_feat, *d_sig;
+  CKS(shape_inputs(c, img, local_means, local_stds, n, &d_img, &d_m, &d_s, &d_out));
+  CKS(ensure(c, B_FEAT, ni, &d_feat));
+  CKS(ensure(c, B_SIG, ni, &d_sig));
+  k_hu_features<<<(ni + 127) / 128, 128, 0, st>>>(d_img, d_m, d_s, w, bw, bh, nx, ni, d_feat, d_sig);
+  k_hu_pairs<<<(ni + 255) / 256, 256, 0, st>>>(d_feat, d_sig, ni, w, e.rw, e.rh, nx, d_out);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return SRED_OK;
+}
+
+sred_status sred_phase_correlation_map_2d(sred_ctx* c, const float* img, const float* local_means,
+                                          const float* local_stds, int w, int h, int bw, int bh, float* out) {
+  if (!c || !img || !local_means || !local_stds || !out) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  Ellipse e;
+  int nx, ny;
+  CKS(check_block(c, w, h, bw, bh, &e));
+  if (bw > kPhaseMaxDim || bh > kPhaseMaxDim)
+    return fail(c, SRED_ERR_ARG, "phase correlation supports blocks up to 15x15");
+  CKS(shape_interior(c, w, h, e, &nx, &ny));
+  if (fault("launch")) return fail(c, SRED_ERR_LAUNCH, "injected launch failure");
+  const size_t n = (size_t)w * h;
+  const int ni = nx * ny, nn = bw * bh;
+  cudaStream_t st = c->stream;
+  float *d_img, *d_m, *d_s, *d_out, *d_sig;
+  double *d_fr, *d_fi;
+  CKS(shape_inputs(c, img, local_means, local_stds, n, &d_img, &d_m, &d_s, &d_out));
+  CKS(ensure(c, B_SIG, ni, &d_sig));
+  CKS(ensure(c, B_FR, (size_t)ni * nn, &d_fr));
+  CKS(ensure(c, B_FI, (size_t)ni * nn, &d_fi));
+  k_phase_dft<<<(ni + 127) / 128, 128, 0, st>>>(d_img, d_m, d_s, w, bw, bh, nx, ni, d_fr, d_fi);
+  k_gather_interior<<<(ni + 255) / 256, 256, 0, st>>>(d_s, w, e.rw, e.rh, nx, ni, d_sig);
+  k_phase_pairs<<<ni, 128, 0, st>>>(d_fr, d_fi, d_sig, ni, bw, bh, w, nx, d_out);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   return SRED_OK;
 }

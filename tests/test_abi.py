@@ -80,7 +80,8 @@ def test_header_cites_reference_for_each_entry_point():
     text = (ROOT / "include" / "sred.h").read_text()
     for fn in ["sred_local_statistics_2d", "sred_mean_noise_var_2d", "sred_relevance_mask_2d",
                "sred_calculate_global_repetition_map_2d", "sred_calculate_block_repetition_map_2d",
-               "sred_reference_block_2d", "sred_normalize_image_2d"]:
+               "sred_reference_block_2d", "sred_normalize_image_2d", "sred_patch_hu_map_2d",
+               "sred_hu_map_2d", "sred_phase_correlation_map_2d"]:
         i = text.index(fn + "(")
-        before = text[max(0, i - 900):i]
-        assert "java/" in before, fn
+        comment = text[text.rindex("/*", 0, i):i]
+        assert "java/" in comment or "cl/" in comment, fn
