@@ -14,10 +14,10 @@
 // real-valued phases, block-width indexing).
 //
 // Per-thread work arrays of the phase kernels live in ONE local array per
-// thread, carved into sections by offset (kPhaseWork*): with separate
-// local arrays, nvcc 12.9 for sm_100a gave the column temporaries of
-// phase_dft the same stack slots as the caller's input patch, and the DFT
-// read overwritten inputs.
+// thread, carved into sections by offset. With separate local arrays,
+// k_block_phase built by nvcc 12.9 for sm_100a computed DFTs whose first row
+// read overwritten inputs, as if phase_dft's column temporaries shared the
+// input patch's stack slots; with one array per thread the results are exact.
 #pragma once
 #include <math.h>
 
