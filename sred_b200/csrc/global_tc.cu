@@ -8,13 +8,16 @@
 //
 // CTA = 1 per SM, persistent over work items (128-row block, range of
 // 256-column tiles). Warp roles:
-//   warp 16     TMA producer: the item's A tile (resident, all K' chunks) and
-//               a ring of B stages (one 256 x 64 bf16 chunk each, SWIZZLE_128B)
+//   warp 16     TMA producer: the item's A tile (resident, all K' chunks), a
+//               ring of B stages (one 256 x 64 bf16 chunk each, SWIZZLE_128B)
+//               and a ring of four column-parameter slots (4 KB per tile)
 //   warp 17     MMA issuer (one thread): on claiming one of two TMEM
-//               accumulators (2 x 256 columns) it bulk-copies the tile's
-//               column parameters (4 KB) into the matching shared slot, then
-//               issues tcgen05.mma M=128 N=256 K=16 and tcgen05.commit to
-//               release B stages and to publish the finished accumulator
+//               accumulators (2 x 256 columns) it issues tcgen05.mma
+//               M=128 N=256 K=16 and tcgen05.commit to release B stages and
+//               to publish the finished accumulator. It shares an SM
+//               sub-partition with four busy epilogue warps, so its loop is
+//               kept to a few instructions per MMA: no divisions, operand
+//               descriptors advanced by adds, K steps unrolled.
 //   warps 0-15  epilogue: tcgen05.ld of the accumulator (warp w reads TMEM
 //               lanes 32(w%4).. and columns 64(w/4)..), the fused per-pair
 //               metric (epilogue.cuh), row sums in registers; FP64 atomics
@@ -44,6 +47,7 @@ constexpr int kEpiWarps = 16;                       // 4 per SM sub-partition
 constexpr int kColsPerWarp = kBN / (kEpiWarps / 4);  // 64: each warp reads 32 lanes x 64 columns
 constexpr int kThreads = (kEpiWarps + 2) * 32;
 constexpr int kSoaBytes = kColSoaFloats * 4;         // one tile's column parameters
+constexpr int kParSlots = 4;                         // column-parameter ring depth
 constexpr unsigned long long kTimeoutNs = 4000000000ull;  // 4 s per wait
 
 enum { ST_OK = 0, ST_TIMEOUT_PRODUCER = 1, ST_TIMEOUT_MMA = 2, ST_TIMEOUT_EPI = 3, ST_TIMEOUT_DRAIN = 4 };
@@ -246,14 +250,15 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int S = g.stages, nkc = g.nkc;
   const uint32_t sA = base;                                     // nkc x 16 KB
   const uint32_t sB = sA + nkc * kAChunkBytes;                  // S x 32 KB
-  const uint32_t sP = sB + S * kBStageBytes;                    // 2 x column-parameter slots
+  const uint32_t sP = sB + S * kBStageBytes;                    // kParSlots column-parameter slots
   const float* slots = reinterpret_cast<const float*>(sbase + (sP - base));
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + (sP - base) + 2 * kSoaBytes);
-  // barrier layout: full[S], empty[S], acc_full[2], acc_empty[2], par_full[2], a_full, a_empty, done
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + (sP - base) + kParSlots * kSoaBytes);
+  // barrier layout: full[S], empty[S], acc_full[2], acc_empty[2], par_full[4], par_empty[4],
+  //                 a_full, a_empty, done
   const uint32_t b_full = smem_u32(bars), b_empty = b_full + 8 * S, b_accf = b_empty + 8 * S,
-                 b_acce = b_accf + 16, b_parf = b_acce + 16, b_afull = b_parf + 16, b_aempty = b_afull + 8,
-                 b_done = b_aempty + 8;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 9);
+                 b_acce = b_accf + 16, b_parf = b_acce + 16, b_pare = b_parf + 8 * kParSlots,
+                 b_afull = b_pare + 8 * kParSlots, b_aempty = b_afull + 8, b_done = b_aempty + 8;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 4 + 2 * kParSlots + 3);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -264,7 +269,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int b = 0; b < 2; b++) {
       mbar_init(b_accf + 8 * b, 1);
       mbar_init(b_acce + 8 * b, kEpiWarps);
-      mbar_init(b_parf + 8 * b, 1);
+    }
+    for (int p = 0; p < kParSlots; p++) {
+      mbar_init(b_parf + 8 * p, 1);
+      mbar_init(b_pare + 8 * p, kEpiWarps);
     }
     mbar_init(b_afull, 1);
     mbar_init(b_aempty, 1);
@@ -285,33 +293,55 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == kEpiWarps) {
     // ---------------------------------------------------------------- TMA
     if (lane == 0) {
-      uint32_t it = 0, item_i = 0;
-      bool ok = true;
+      uint32_t it = 0, item_i = 0, ptile = 0;
+      uint32_t s = 0, eph = 0;  // B ring: stage, parity of the round being refilled
+      bool ok = true, a_issued = false;
       for (int item = blockIdx.x; ok && item < g.n_items; item += gridDim.x, item_i++) {
         const int rb = item % g.n_rb, seg = item / g.n_rb;
         const int ct0 = seg * g.ct_per_item, ct1 = min(ct0 + g.ct_per_item, g.n_ct);
         if (!mbar_wait(b_aempty, (item_i & 1) ^ 1, g.status, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
         mbar_expect_tx(b_afull, nkc * kAChunkBytes);
         for (int kc = 0; kc < nkc; kc++) tma_load_2d(sA + kc * kAChunkBytes, &tmA, b_afull, kc * kChunk, rb * kBM);
-        for (int ct = ct0; ok && ct < ct1; ct++) {
+        a_issued = true;
+        for (int ct = ct0; ok && ct < ct1; ct++, ptile++) {
+          // the tile's column parameters, into the slot the epilogue released four tiles ago
+          const uint32_t ps = ptile & (kParSlots - 1);
+          if (!mbar_wait(b_pare + 8 * ps, ((ptile / kParSlots) & 1) ^ 1, g.status, ST_TIMEOUT_PRODUCER)) {
+            ok = false;
+            break;
+          }
+          mbar_expect_tx(b_parf + 8 * ps, kSoaBytes);
+          bulk_load(sP + ps * kSoaBytes, g.colsoa + (size_t)ct * kColSoaFloats, kSoaBytes, b_parf + 8 * ps);
           for (int kc = 0; kc < nkc; kc++, it++) {
-            const int s = it % S;
-            if (!mbar_wait(b_empty + 8 * s, ((it / S) & 1) ^ 1, g.status, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
+            if (!mbar_wait(b_empty + 8 * s, eph ^ 1, g.status, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
             mbar_expect_tx(b_full + 8 * s, kBStageBytes);
             tma_load_2d(sB + s * kBStageBytes, &tmB, b_full + 8 * s, kc * kChunk, ct * kBN);
+            if (++s == (uint32_t)S) {
+              s = 0;
+              eph ^= 1;
+            }
           }
         }
       }
       // Drain: every issued copy has landed before the CTA may exit.
       for (uint32_t k = (it > (uint32_t)S ? it - S : 0); k < it; k++)
         mbar_wait(b_full + 8 * (k % S), (k / S) & 1, g.status, ST_TIMEOUT_DRAIN, false);
+      for (uint32_t k = (ptile > (uint32_t)kParSlots ? ptile - kParSlots : 0); k < ptile; k++)
+        mbar_wait(b_parf + 8 * (k % kParSlots), (k / kParSlots) & 1, g.status, ST_TIMEOUT_DRAIN, false);
+      // item_i - 1 is the last item whose A tile was issued (a failed wait
+      // leaves item_i at the item it was waiting for)
+      if (a_issued) mbar_wait(b_afull, (item_i - 1) & 1, g.status, ST_TIMEOUT_DRAIN, false);
     }
     __syncwarp();
   } else if (warp == kEpiWarps + 1) {
     // ---------------------------------------------------------------- MMA
     if (lane == 0) {
-      uint32_t it = 0, tile = 0, item_i = 0;
-      uint32_t par_issued = 0;  // parameter copies issued (for the drain)
+      uint32_t tile = 0, item_i = 0;
+      uint32_t s = 0, fph = 0;  // B ring: stage, parity of the round being consumed
+      // Operand descriptors: the start-address field counts 16-byte units, so
+      // a K step of 16 bf16 (32 B) adds 2 and a chunk or stage adds its size / 16.
+      const uint64_t a_desc0 = desc_sw128(sA), b_desc0 = desc_sw128(sB);
+      const int last_nks = (g.kq - (nkc - 1) * kChunk) / 16;
       bool ok = true;
       for (int item = blockIdx.x; ok && item < g.n_items; item += gridDim.x, item_i++) {
         const int seg = item / g.n_rb;
@@ -322,33 +352,35 @@ __global__ void __launch_bounds__(kThreads, 1)
           const uint32_t b = tile & 1;
           if (!mbar_wait(b_acce + 8 * b, ((tile >> 1) & 1) ^ 1, g.status, ST_TIMEOUT_MMA)) { ok = false; break; }
           tc_fence_after();
-          // The epilogue released this buffer, so its parameter slot is free too.
-          mbar_expect_tx(b_parf + 8 * b, kSoaBytes);
-          bulk_load(sP + b * kSoaBytes, g.colsoa + (size_t)ct * kColSoaFloats, kSoaBytes, b_parf + 8 * b);
-          par_issued = tile + 1;
           const uint32_t d = tmem + b * kBN;
-          for (int kc = 0; kc < nkc; kc++, it++) {
-            const int s = it % S;
-            if (!mbar_wait(b_full + 8 * s, (it / S) & 1, g.status, ST_TIMEOUT_MMA)) { ok = false; break; }
+          uint64_t da = a_desc0;
+          for (int kc = 0; kc < nkc; kc++) {
+            if (!mbar_wait(b_full + 8 * s, fph, g.status, ST_TIMEOUT_MMA)) { ok = false; break; }
             tc_fence_after();
-            const int nks = min(kChunk, g.kq - kc * kChunk) / 16;
-            for (int ks = 0; ks < nks; ks++) {
-              const uint64_t da = desc_sw128(sA + kc * kAChunkBytes + ks * 32);
-              const uint64_t db = desc_sw128(sB + s * kBStageBytes + ks * 32);
-              mma_bf16(d, da, db, (kc | ks) != 0);
+            const uint64_t db = b_desc0 + (uint64_t)(s * (kBStageBytes >> 4));
+            if (kc + 1 < nkc) {
+#pragma unroll
+              for (int ks = 0; ks < kChunk / 16; ks++) mma_bf16(d, da + 2 * ks, db + 2 * ks, (kc | ks) != 0);
+            } else {
+#pragma unroll
+              for (int ks = 0; ks < kChunk / 16; ks++)
+                if (ks < last_nks) mma_bf16(d, da + 2 * ks, db + 2 * ks, (kc | ks) != 0);
             }
             mma_commit(b_empty + 8 * s);
+            da += kAChunkBytes >> 4;
+            if (++s == (uint32_t)S) {
+              s = 0;
+              fph ^= 1;
+            }
           }
           if (ok) mma_commit(b_accf + 8 * b);
         }
         if (ok) mma_commit(b_aempty);
       }
-      // All MMAs and parameter copies this thread issued are complete before
-      // TMEM is released and the CTA exits.
+      // All MMAs this thread issued are complete before TMEM is released and
+      // the CTA exits.
       mma_commit(b_done);
       mbar_wait(b_done, 0, g.status, ST_TIMEOUT_DRAIN, false);
-      for (uint32_t k = (par_issued > 2 ? par_issued - 2 : 0); k < par_issued; k++)
-        mbar_wait(b_parf + 8 * (k & 1), (k >> 1) & 1, g.status, ST_TIMEOUT_DRAIN, false);
     }
     __syncwarp();
   } else {
@@ -366,13 +398,14 @@ __global__ void __launch_bounds__(kThreads, 1)
       double acc_n = 0.0, acc_d = 0.0;
       for (int ct = ct0; ok && ct < ct1; ct++, tile++) {
         const uint32_t b = tile & 1, par = (tile >> 1) & 1;
-        if (!mbar_wait(b_parf + 8 * b, par, g.status, ST_TIMEOUT_EPI) ||
+        const uint32_t ps = tile & (kParSlots - 1), pph = (tile / kParSlots) & 1;
+        if (!mbar_wait(b_parf + 8 * ps, pph, g.status, ST_TIMEOUT_EPI) ||
             !mbar_wait(b_accf + 8 * b, par, g.status, ST_TIMEOUT_EPI)) {
           ok = false;
           break;
         }
         tc_fence_after();
-        const float* soa = slots + b * kColSoaFloats;
+        const float* soa = slots + ps * kColSoaFloats;
         const int col0 = ct * kBN;
         const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + b * kBN + cbase;
         const int cm = METRIC == kPearson ? c_mode(kEps * rmax_r * soa[4 * kBN]) : kCFirst;
@@ -391,7 +424,10 @@ __global__ void __launch_bounds__(kThreads, 1)
           epi_tile<METRIC, kCExact, false, true>(taddr, soa, cbase, col0, row, rs, g.ec, sn, sd);
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(b_acce + 8 * b);
+        if (lane == 0) {
+          mbar_arrive(b_acce + 8 * b);
+          mbar_arrive(b_pare + 8 * ps);
+        }
         acc_n += (double)sn;
         acc_d += (double)sd;
       }
@@ -444,7 +480,7 @@ cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int k
   g.kq = kq;
   g.nkc = (kq + kChunk - 1) / kChunk;
   g.n_ct = (ec.n + kBN - 1) / kBN;
-  const size_t fixed = 1024 + (size_t)g.nkc * kAChunkBytes + 2 * kSoaBytes + 8 * 64;
+  const size_t fixed = 1024 + (size_t)g.nkc * kAChunkBytes + kParSlots * kSoaBytes + 8 * 64;
   const size_t budget = 227 * 1024;
   if (fixed + 2 * kBStageBytes > budget) return cudaErrorInvalidValue;
   g.stages = (int)std::min<size_t>(kMaxStages, (budget - fixed) / kBStageBytes);
