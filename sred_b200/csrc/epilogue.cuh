@@ -113,6 +113,80 @@ __device__ __forceinline__ void epi_pair(float G, const RowState& rp, const Bloc
   sd += td;
 }
 
+// ---------------------------------------------------------------------------
+// Packed FP32 pairs (sm_100 f32x2 arithmetic): two columns' terms per
+// instruction. Used by the tensor-core engine's Pearson fast path.
+// ---------------------------------------------------------------------------
+struct F2 {
+  unsigned long long v;
+};
+
+__device__ __forceinline__ F2 f2(float lo, float hi) {
+  F2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2_split(F2 a, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a.v));
+}
+__device__ __forceinline__ F2 add2(F2 a, F2 b) {
+  F2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 sub2(F2 a, F2 b) {
+  F2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 mul2(F2 a, F2 b) {
+  F2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {  // a * b + c
+  F2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+  return r;
+}
+
+// Row constants of the packed Pearson path, both halves equal.
+struct PearsonRow2 {
+  F2 a, e, ne, m1, one;
+};
+
+__device__ __forceinline__ PearsonRow2 make_pearson_row2(const RowState& rs) {
+  PearsonRow2 r;
+  r.a = f2(rs.a, rs.a);
+  r.e = f2(rs.e, rs.e);
+  r.ne = f2(-rs.e, -rs.e);
+  r.m1 = f2(-1.0f, -1.0f);
+  r.one = f2(1.0f, 1.0f);
+  return r;
+}
+
+// Two Pearson pairs (columns q0, q1 of one row), the terms of pair_terms for
+// CMODE kCFirst / kCSecond, accumulated into packed sums (numerator with one
+// fused multiply-add).
+template <int CMODE>
+__device__ __forceinline__ void pearson_pair2(F2 G, F2 aq, F2 rq, const PearsonRow2& r, F2& sn, F2& sd) {
+  const F2 d = sub2(r.a, aq);
+  float m0, m1;
+  f2_split(mul2(d, d), m0, m1);
+  const F2 w = f2(ex2_approx(-m0), ex2_approx(-m1));
+  F2 gc;
+  if (CMODE == kCFirst) {
+    gc = fma2(mul2(G, r.ne), rq, G);  // G - G e_p r_q
+  } else {
+    const F2 t = mul2(r.e, rq);
+    gc = mul2(G, fma2(t, add2(t, r.m1), r.one));  // G (1 - t + t^2)
+  }
+  float g0, g1;
+  f2_split(gc, g0, g1);
+  sn = fma2(f2(fmaxf(g0, 0.0f), fmaxf(g1, 0.0f)), w, sn);
+  sd = add2(sd, w);
+}
+
 // Column sums of 16 columns over the 32 lanes of a warp (lane l holds row l's
 // terms x[0..15]): four butterfly exchanges halve the columns each lane keeps,
 // a fifth adds the lane pairs. Afterwards lanes 2c and 2c+1 both hold the sum

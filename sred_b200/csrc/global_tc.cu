@@ -220,6 +220,46 @@ __device__ __forceinline__ void epi_chunk(const uint32_t (&v)[16], const float* 
   }
 }
 
+// Packed Pearson fast path (full, off-diagonal tiles, CMODE kCFirst or
+// kCSecond): 16 pairs as eight f32x2 pairs.
+template <int CMODE>
+__device__ __forceinline__ void epi_chunk_pearson2(const uint32_t (&v)[16], const float* __restrict__ soa, int c0,
+                                                   const PearsonRow2& r2, F2& sn, F2& sd) {
+#pragma unroll
+  for (int j = 0; j < 16; j += 4) {
+    const float4 a4 = *reinterpret_cast<const float4*>(soa + c0 + j);
+    const float4 r4 = *reinterpret_cast<const float4*>(soa + kBN + c0 + j);
+    pearson_pair2<CMODE>(f2(__uint_as_float(v[j]), __uint_as_float(v[j + 1])), f2(a4.x, a4.y), f2(r4.x, r4.y), r2,
+                         sn, sd);
+    pearson_pair2<CMODE>(f2(__uint_as_float(v[j + 2]), __uint_as_float(v[j + 3])), f2(a4.z, a4.w),
+                         f2(r4.z, r4.w), r2, sn, sd);
+  }
+}
+
+template <int CMODE>
+__device__ __forceinline__ void epi_tile_pearson2(uint32_t taddr, const float* __restrict__ soa, int cbase,
+                                                  const PearsonRow2& r2, float& sn_out, float& sd_out) {
+  uint32_t v0[16], v1[16];
+  F2 sn = f2(0.0f, 0.0f), sd = sn;
+  tmem_ld16(taddr, v0);
+  tmem_wait(v0);
+  tmem_ld16(taddr + 16, v1);
+  epi_chunk_pearson2<CMODE>(v0, soa, cbase, r2, sn, sd);
+  tmem_wait(v1);
+  tmem_ld16(taddr + 32, v0);
+  epi_chunk_pearson2<CMODE>(v1, soa, cbase + 16, r2, sn, sd);
+  tmem_wait(v0);
+  tmem_ld16(taddr + 48, v1);
+  epi_chunk_pearson2<CMODE>(v0, soa, cbase + 32, r2, sn, sd);
+  tmem_wait(v1);
+  epi_chunk_pearson2<CMODE>(v1, soa, cbase + 48, r2, sn, sd);
+  float a, b;
+  f2_split(sn, a, b);
+  sn_out += a + b;
+  f2_split(sd, a, b);
+  sd_out += a + b;
+}
+
 // One warp's 64 columns of a tile in four 16-column chunks: each chunk's TMEM
 // load is in flight while the previous chunk is evaluated.
 template <int METRIC, int CMODE, bool FULL, bool DIAG>
@@ -394,6 +434,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int ct0 = seg * g.ct_per_item, ct1 = min(ct0 + g.ct_per_item, g.n_ct);
       const int row = rb * kBM + quarter * 32 + lane;
       const RowState rs = make_row(g.params[row], g.ec);
+      const PearsonRow2 r2 = make_pearson_row2(rs);
       const float rmax_r = g.tile_rmax[rb];
       double acc_n = 0.0, acc_d = 0.0;
       for (int ct = ct0; ok && ct < ct1; ct++, tile++) {
@@ -412,7 +453,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         const bool full = col0 + kBN <= g.ec.n;
         const bool diag = (ct == (rb >> 1));
         float sn = 0.0f, sd = 0.0f;
-        if (full && !diag && cm == kCFirst)
+        if (METRIC == kPearson && full && !diag && cm == kCFirst)
+          epi_tile_pearson2<kCFirst>(taddr, soa, cbase, r2, sn, sd);
+        else if (METRIC == kPearson && full && !diag && cm == kCSecond)
+          epi_tile_pearson2<kCSecond>(taddr, soa, cbase, r2, sn, sd);
+        else if (full && !diag && cm == kCFirst)
           epi_tile<METRIC, kCFirst, true, false>(taddr, soa, cbase, col0, row, rs, g.ec, sn, sd);
         else if (full && !diag && cm == kCSecond)
           epi_tile<METRIC, kCSecond, true, false>(taddr, soa, cbase, col0, row, rs, g.ec, sn, sd);
