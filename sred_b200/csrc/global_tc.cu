@@ -54,6 +54,8 @@ enum { ST_OK = 0, ST_TIMEOUT_PRODUCER = 1, ST_TIMEOUT_MMA = 2, ST_TIMEOUT_EPI = 
 
 struct TcArgs {
   int kq, nkc, stages;
+  int nfull, tail;              // tile-ring mode: 64-column chunks and a 32-column tail (0 or 1)
+  uint32_t a_bytes, b_bytes;    // tile-ring mode: A tile and one B tile in shared memory
   int n_rb, n_ct, ct_per_item, n_items;
   const BlockParams* params;
   const float* colsoa;
@@ -143,6 +145,18 @@ __device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
   d |= static_cast<uint64_t>(1024 >> 4) << 32;   // stride byte offset
   d |= static_cast<uint64_t>(1) << 46;           // descriptor version (sm_100)
   d |= static_cast<uint64_t>(2) << 61;           // SWIZZLE_128B
+  return d;
+}
+
+// Same for SWIZZLE_64B (64-byte rows, 8-row groups 512 B apart): the 32-column
+// tail of K' in the tile-ring mode.
+__device__ __forceinline__ uint64_t desc_sw64(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr & 0x3FFFFu) >> 4);
+  d |= static_cast<uint64_t>(1) << 16;
+  d |= static_cast<uint64_t>(512 >> 4) << 32;
+  d |= static_cast<uint64_t>(1) << 46;
+  d |= static_cast<uint64_t>(4) << 61;  // SWIZZLE_64B
   return d;
 }
 
@@ -280,17 +294,27 @@ __device__ __forceinline__ void epi_tile(uint32_t taddr, const float* __restrict
   epi_chunk<METRIC, CMODE, FULL, DIAG>(v1, soa, cbase + 48, col0, row, rs, ec, sn, sd);
 }
 
-template <int METRIC>
+// TR (tile ring, K' <= 160): the B operand moves one whole 256-column tile at
+// a time through two buffers, and the single tcgen05.commit per tile both
+// publishes the accumulator and frees the tile's B buffer (the producer waits
+// on the accumulator barrier). Each mbarrier operation that follows a commit
+// stalls the MMA stream for ~100 cycles, so one commit-then-wait per tile
+// instead of one per K chunk is worth ~30% of MMA throughput. K' = 64 c + 32 t:
+// c SWIZZLE_128B chunks and an optional SWIZZLE_64B tail.
+// !TR (chunk ring): B moves in 64-column chunks through S stages, one commit
+// per chunk; used when two whole tiles do not fit in shared memory.
+template <int METRIC, bool TR>
 __global__ void __launch_bounds__(kThreads, 1)
-    k_gram_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcArgs g) {
+    k_gram_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+              const __grid_constant__ CUtensorMap tmA64, const __grid_constant__ CUtensorMap tmB64, TcArgs g) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   uint8_t* sbase = smem_raw + (base - raw);
   const int S = g.stages, nkc = g.nkc;
-  const uint32_t sA = base;                                     // nkc x 16 KB
-  const uint32_t sB = sA + nkc * kAChunkBytes;                  // S x 32 KB
-  const uint32_t sP = sB + S * kBStageBytes;                    // kParSlots column-parameter slots
+  const uint32_t sA = base;  // TR: a_bytes; else nkc x 16 KB
+  const uint32_t sB = sA + (TR ? g.a_bytes : nkc * kAChunkBytes);   // TR: 2 x b_bytes; else S x 32 KB
+  const uint32_t sP = sB + (TR ? 2 * g.b_bytes : S * kBStageBytes);  // kParSlots column-parameter slots
   const float* slots = reinterpret_cast<const float*>(sbase + (sP - base));
   uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + (sP - base) + kParSlots * kSoaBytes);
   // barrier layout: full[S], empty[S], acc_full[2], acc_empty[2], par_full[4], par_empty[4],
@@ -340,8 +364,14 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int rb = item % g.n_rb, seg = item / g.n_rb;
         const int ct0 = seg * g.ct_per_item, ct1 = min(ct0 + g.ct_per_item, g.n_ct);
         if (!mbar_wait(b_aempty, (item_i & 1) ^ 1, g.status, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
-        mbar_expect_tx(b_afull, nkc * kAChunkBytes);
-        for (int kc = 0; kc < nkc; kc++) tma_load_2d(sA + kc * kAChunkBytes, &tmA, b_afull, kc * kChunk, rb * kBM);
+        if (TR) {
+          mbar_expect_tx(b_afull, g.a_bytes);
+          for (int c = 0; c < g.nfull; c++) tma_load_2d(sA + c * kAChunkBytes, &tmA, b_afull, c * kChunk, rb * kBM);
+          if (g.tail) tma_load_2d(sA + g.nfull * kAChunkBytes, &tmA64, b_afull, g.nfull * kChunk, rb * kBM);
+        } else {
+          mbar_expect_tx(b_afull, nkc * kAChunkBytes);
+          for (int kc = 0; kc < nkc; kc++) tma_load_2d(sA + kc * kAChunkBytes, &tmA, b_afull, kc * kChunk, rb * kBM);
+        }
         a_issued = true;
         for (int ct = ct0; ok && ct < ct1; ct++, ptile++) {
           // the tile's column parameters, into the slot the epilogue released four tiles ago
@@ -350,8 +380,24 @@ __global__ void __launch_bounds__(kThreads, 1)
             ok = false;
             break;
           }
+          // TR: B buffer ptile & 1 is free once the accumulator of tile ptile - 2
+          // is published. Both waits come before any copy of this tile is issued.
+          if (TR && !mbar_wait(b_accf + 8 * (ptile & 1), ((ptile >> 1) & 1) ^ 1, g.status, ST_TIMEOUT_PRODUCER)) {
+            ok = false;
+            break;
+          }
           mbar_expect_tx(b_parf + 8 * ps, kSoaBytes);
           bulk_load(sP + ps * kSoaBytes, g.colsoa + (size_t)ct * kColSoaFloats, kSoaBytes, b_parf + 8 * ps);
+          if (TR) {
+            const uint32_t b = ptile & 1;
+            const uint32_t dst = sB + b * g.b_bytes;
+            mbar_expect_tx(b_full + 8 * b, g.b_bytes);
+            for (int c = 0; c < g.nfull; c++)
+              tma_load_2d(dst + c * kBStageBytes, &tmB, b_full + 8 * b, c * kChunk, ct * kBN);
+            if (g.tail) tma_load_2d(dst + g.nfull * kBStageBytes, &tmB64, b_full + 8 * b, g.nfull * kChunk, ct * kBN);
+            it++;
+            continue;
+          }
           for (int kc = 0; kc < nkc; kc++, it++) {
             if (!mbar_wait(b_empty + 8 * s, eph ^ 1, g.status, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
             mbar_expect_tx(b_full + 8 * s, kBStageBytes);
@@ -363,7 +409,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
         }
       }
-      // Drain: every issued copy has landed before the CTA may exit.
+      // Drain: every issued copy has landed before the CTA may exit (TR: `it`
+      // counts whole-tile loads through S = 2 buffers).
       for (uint32_t k = (it > (uint32_t)S ? it - S : 0); k < it; k++)
         mbar_wait(b_full + 8 * (k % S), (k / S) & 1, g.status, ST_TIMEOUT_DRAIN, false);
       for (uint32_t k = (ptile > (uint32_t)kParSlots ? ptile - kParSlots : 0); k < ptile; k++)
@@ -393,6 +440,25 @@ __global__ void __launch_bounds__(kThreads, 1)
           if (!mbar_wait(b_acce + 8 * b, ((tile >> 1) & 1) ^ 1, g.status, ST_TIMEOUT_MMA)) { ok = false; break; }
           tc_fence_after();
           const uint32_t d = tmem + b * kBN;
+          if (TR) {
+            if (!mbar_wait(b_full + 8 * b, (tile >> 1) & 1, g.status, ST_TIMEOUT_MMA)) { ok = false; break; }
+            tc_fence_after();
+            const uint64_t db0 = b_desc0 + (uint64_t)((b * g.b_bytes) >> 4);
+            for (int c = 0; c < g.nfull; c++) {
+#pragma unroll
+              for (int ks = 0; ks < kChunk / 16; ks++)
+                mma_bf16(d, a_desc0 + (uint64_t)(c * (kAChunkBytes >> 4) + 2 * ks),
+                         db0 + (uint64_t)(c * (kBStageBytes >> 4) + 2 * ks), (c | ks) != 0);
+            }
+            if (g.tail) {
+              const uint64_t da = desc_sw64(sA + g.nfull * kAChunkBytes);
+              const uint64_t db = desc_sw64(sB + b * g.b_bytes + g.nfull * kBStageBytes);
+              mma_bf16(d, da, db, g.nfull != 0);
+              mma_bf16(d, da + 2, db + 2, 1);
+            }
+            mma_commit(b_accf + 8 * b);
+            continue;
+          }
           uint64_t da = a_desc0;
           for (int kc = 0; kc < nkc; kc++) {
             if (!mbar_wait(b_full + 8 * s, fph, g.status, ST_TIMEOUT_MMA)) { ok = false; break; }
@@ -502,15 +568,17 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
   return fn;
 }
 
-bool make_map(CUtensorMap* m, const __nv_bfloat16* ptr, int kq, int rows, int box_rows) {
+// box_cols 64 (128-byte rows, SWIZZLE_128B) or 32 (64-byte rows, SWIZZLE_64B).
+bool make_map(CUtensorMap* m, const __nv_bfloat16* ptr, int kq, int rows, int box_rows, int box_cols = kChunk) {
   auto enc = get_encode();
   if (!enc) return false;
   cuuint64_t dims[2] = {(cuuint64_t)kq, (cuuint64_t)rows};
   cuuint64_t strides[1] = {(cuuint64_t)kq * 2};
-  cuuint32_t box[2] = {(cuuint32_t)kChunk, (cuuint32_t)box_rows};
+  cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(ptr), dims, strides, box,
-                   estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   box_cols == kChunk ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
@@ -525,11 +593,23 @@ cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int k
   g.kq = kq;
   g.nkc = (kq + kChunk - 1) / kChunk;
   g.n_ct = (ec.n + kBN - 1) / kBN;
-  const size_t fixed = 1024 + (size_t)g.nkc * kAChunkBytes + kParSlots * kSoaBytes + 8 * 64;
   const size_t budget = 227 * 1024;
-  if (fixed + 2 * kBStageBytes > budget) return cudaErrorInvalidValue;
-  g.stages = (int)std::min<size_t>(kMaxStages, (budget - fixed) / kBStageBytes);
-  const size_t smem = fixed + (size_t)g.stages * kBStageBytes;
+  g.nfull = kq / kChunk;
+  g.tail = (kq % kChunk) ? 1 : 0;
+  g.a_bytes = (uint32_t)kBM * kq * 2;
+  g.b_bytes = (uint32_t)kBN * kq * 2;
+  const size_t tr_smem = 1024 + (size_t)g.a_bytes + 2 * (size_t)g.b_bytes + kParSlots * kSoaBytes + 8 * 64;
+  const bool tr = (kq % (kChunk / 2) == 0) && tr_smem <= budget;
+  size_t smem;
+  if (tr) {
+    g.stages = 2;
+    smem = tr_smem;
+  } else {
+    const size_t fixed = 1024 + (size_t)g.nkc * kAChunkBytes + kParSlots * kSoaBytes + 8 * 64;
+    if (fixed + 2 * kBStageBytes > budget) return cudaErrorInvalidValue;
+    g.stages = (int)std::min<size_t>(kMaxStages, (budget - fixed) / kBStageBytes);
+    smem = fixed + (size_t)g.stages * kBStageBytes;
+  }
   // Only row blocks that hold valid rows are work; split the column range so
   // that every SM gets several items.
   const int n_rb_valid = (ec.n + kBM - 1) / kBM;
@@ -546,14 +626,24 @@ cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int k
   g.num = num;
   g.den = den;
   g.status = status;
-  CUtensorMap mA, mB;
+  CUtensorMap mA, mB, mA64, mB64;
   if (!make_map(&mA, A, kq, n_pad, kBM) || !make_map(&mB, B, kq, n_pad, kBN)) return cudaErrorInvalidValue;
+  mA64 = mA;
+  mB64 = mB;
+  if (tr && g.tail && (!make_map(&mA64, A, kq, n_pad, kBM, kChunk / 2) || !make_map(&mB64, B, kq, n_pad, kBN, kChunk / 2)))
+    return cudaErrorInvalidValue;
   const int grid = std::min(g.n_items, num_sms);
   cudaError_t e;
-#define SRED_TC(M)                                                                                   \
-  e = cudaFuncSetAttribute(k_gram_tc<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);      \
-  if (e != cudaSuccess) return e;                                                                    \
-  k_gram_tc<M><<<grid, kThreads, smem, st>>>(mA, mB, g);
+#define SRED_TC(M)                                                                                         \
+  if (tr) {                                                                                                \
+    e = cudaFuncSetAttribute(k_gram_tc<M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
+    if (e != cudaSuccess) return e;                                                                        \
+    k_gram_tc<M, true><<<grid, kThreads, smem, st>>>(mA, mB, mA64, mB64, g);                               \
+  } else {                                                                                                 \
+    e = cudaFuncSetAttribute(k_gram_tc<M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
+    if (e != cudaSuccess) return e;                                                                        \
+    k_gram_tc<M, false><<<grid, kThreads, smem, st>>>(mA, mB, mA64, mB64, g);                              \
+  }
   switch (ec.metric) {
     case kPearson: SRED_TC(kPearson); break;
     case kSsim: SRED_TC(kSsim); break;

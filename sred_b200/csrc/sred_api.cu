@@ -248,7 +248,7 @@ sred_status global_core(sred_ctx* c, int metric, const float* d_img, int w, int 
   const int engine = (metric == kAbsDiff) ? SRED_ENGINE_FP32 : c->engine;
   const size_t n_pad = round_up((size_t)std::max(n_g, 1), 256);
   const int kp = (int)round_up(K, 4);
-  const int kq = (int)round_up(3 * K, 16);
+  const int kq = (int)round_up(3 * K, 32);  // K' of the split-BF16 operands (tail of 0 or 32 columns)
   float* d_U = nullptr;
   __nv_bfloat16 *d_A = nullptr, *d_B = nullptr;
   BlockParams* d_params;
@@ -682,7 +682,7 @@ sred_status sred_debug_gram_rowdot(sred_ctx* c, int engine, const float* u, cons
   cudaSetDevice(c->device);
   cudaStream_t st = c->stream;
   const size_t n_pad = round_up((size_t)n, 256);
-  const int kp = (int)round_up(k, 4), kq = (int)round_up(3 * k, 16);
+  const int kp = (int)round_up(k, 4), kq = (int)round_up(3 * k, 32);
   float *d_u, *d_U = nullptr, *d_rmax;
   __nv_bfloat16 *d_A = nullptr, *d_B = nullptr;
   BlockParams* d_params;
