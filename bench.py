@@ -366,6 +366,55 @@ def run_block(args, rank, local, world):
     print(json.dumps(line), flush=True)
 
 
+BATCH_SIDES = [256, 384, 512, 768, 1024]
+BATCH_BLOCKS = [3, 5, 9, 13, 15]
+
+
+def run_batch(args, rank, local, world):
+    """Batched global maps (the multi-scale set): `--images` seeded spot
+    images with sides from {256, 384, 512, 768, 1024} (width and height drawn
+    independently, so most are not square), each mapped with 3x3, 5x5, 9x9,
+    13x13 and 15x15 blocks (K = 5, 13, 49, 113, 149) and with Pearson's R and
+    SSIM at relevance 1.0: 10 maps per image through sred_global_map_2d_batch
+    with host buffers. Reports the sum over maps of relevant^2 block pairs per
+    second of wall time (transfers included) and maps per second."""
+    import torch
+    from sred_b200 import _lib, clutils, synth
+    torch.cuda.set_device(local)
+    ctx = _lib.Context(local, "tc")
+    rng = np.random.default_rng(11 + rank)
+    jobs = []
+    for i in range(args.images):
+        w, h = (int(v) for v in rng.choice(BATCH_SIDES, 2))
+        img = synth.normalize_input(synth.spot_image(w, h, max(4, min(w, h) // 13), seed=1000 * rank + i))
+        for b in BATCH_BLOCKS:
+            for metric in ("Pearson's R", "SSIM"):
+                jobs.append({"metric": metric, "img": img, "block_width": b, "block_height": b,
+                             "relevance_constant": 1.0})
+    # warm-up: the largest image's maps, which also sizes every worker's workspaces
+    big = max(range(args.images), key=lambda i: jobs[10 * i]["img"].size)
+    clutils.global_map_batch(jobs[10 * big:10 * big + 10], n_workers=args.workers, ctx=ctx)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    res = clutils.global_map_batch(jobs, n_workers=args.workers, ctx=ctx)
+    torch.cuda.synchronize()
+    dt = max_over_ranks(time.perf_counter() - t0, world)
+    pairs = sum_over_ranks(float(sum(info["pairs"] for _, info in res)), world)
+    if rank != 0:
+        return
+    line = {"metric": "batched global maps: block-pairs/s summed over maps (wall time, host buffers)",
+            "value": pairs / dt, "unit": "block-pairs/s", "n_gpus": world, "steps": 1, "warmup": 1,
+            "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16x3 split (hi/lo) tensor-core Gram, f32 accumulate, f64 moments", "data": "synthetic",
+            "config": {"workload": f"{args.images} images x 5 block sizes x 2 metrics = {len(jobs)} global maps, "
+                                   "sides 256-1024, relevance 1.0", "images": args.images, "maps": len(jobs),
+                       "workers": args.workers, "pairs": pairs},
+            "maps_per_s": len(jobs) * world / dt}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -399,8 +448,11 @@ def main():
     ap.add_argument("--engine", choices=["tc", "fp32"], default="tc")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP32-engine comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["global", "block"], default="global",
-                    help="global repetition map (default, the headline) or the block (local) map")
+    ap.add_argument("--workload", choices=["global", "block", "batch"], default="global",
+                    help="global repetition map (default, the headline), the block (local) map, or batched "
+                         "global maps of many images")
+    ap.add_argument("--images", type=int, default=8, help="images of the batch workload (10 maps each)")
+    ap.add_argument("--workers", type=int, default=4, help="host workers of the batch workload")
     ap.add_argument("--frames", type=int, default=64, help="frames of the block-map workload")
     ap.add_argument("--size", type=int, default=1024,
                     help="image side (default 1024, the benchmark workload; smaller sides for profiling)")
@@ -419,6 +471,8 @@ def main():
     try:
         if args.workload == "block":
             run_block(args, rank, local, world)
+        elif args.workload == "batch":
+            run_batch(args, rank, local, world)
         else:
             run_ours(args, rank, local, world)
     finally:

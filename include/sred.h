@@ -101,6 +101,27 @@ sred_status sred_global_map_2d(sred_ctx *ctx, const char *metric, const float *i
                                int bw, int bh, float relevance_constant, int normalize_output,
                                float *out, sred_run_info *info);
 
+/* One map of a batch (sred_global_map_2d_batch): the arguments of
+ * sred_global_map_2d, and the job's own status on return. */
+typedef struct {
+    const char *metric;
+    const float *img;          /* host, w*h */
+    int w, h, bw, bh;
+    float relevance_constant;
+    int normalize_output;
+    float *out;                /* host, w*h */
+    sred_run_info *info;       /* nullable */
+    int status;                /* written: sred_status of this job */
+} sred_job;
+
+/* Many global maps in one call (no counterpart in the reference, whose
+ * command computes one map per invocation): jobs run on `n_workers` (1..8)
+ * host threads, each with its own CUDA stream and workspaces, so that one
+ * map's host steps and transfers overlap another map's kernels. Each map is
+ * identical to what sred_global_map_2d returns for it. Returns SRED_OK if
+ * every job succeeded, else the first failing job's status. */
+sred_status sred_global_map_2d_batch(sred_ctx *ctx, sred_job *jobs, int n_jobs, int n_workers);
+
 /* Same as sred_global_map_2d with device-resident input and output on
  * `stream` (a cudaStream_t; NULL = the context's stream). The call returns
  * when the map is complete. */

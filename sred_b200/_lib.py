@@ -24,7 +24,7 @@ EXPORTS = [
     "sred_calculate_global_repetition_map_2d", "sred_global_map_2d", "sred_global_map_2d_device",
     "sred_calculate_block_repetition_map_2d", "sred_block_map_2d_device", "sred_reference_block_2d",
     "sred_normalize_image_2d", "sred_debug_gram_rowdot", "sred_block_map_2d_device_noalloc",
-    "sred_patch_hu_map_2d", "sred_hu_map_2d", "sred_phase_correlation_map_2d",
+    "sred_patch_hu_map_2d", "sred_hu_map_2d", "sred_phase_correlation_map_2d", "sred_global_map_2d_batch",
 ]
 
 
@@ -37,6 +37,13 @@ class RunInfo(C.Structure):
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class SredJob(C.Structure):
+    """sred_job: one map of sred_global_map_2d_batch."""
+    _fields_ = [("metric", C.c_char_p), ("img", C.c_void_p), ("w", C.c_int), ("h", C.c_int), ("bw", C.c_int),
+                ("bh", C.c_int), ("relevance_constant", C.c_float), ("normalize_output", C.c_int),
+                ("out", C.c_void_p), ("info", C.POINTER(RunInfo)), ("status", C.c_int)]
 
 
 class SredError(RuntimeError):
@@ -92,6 +99,7 @@ def load() -> C.CDLL:
         L.sred_debug_gram_rowdot.argtypes = [_vp, s, _f32p, _f32p, _f32p, s, s, _f64p, _f64p]
         L.sred_block_map_2d_device_noalloc.argtypes = [C.c_char_p, _vp, s, s, s, _f32p, s, s, s, C.c_float,
                                                        C.c_float, s, _vp, _vp]
+        L.sred_global_map_2d_batch.argtypes = [_vp, C.POINTER(SredJob), s, s]
         L.sred_patch_hu_map_2d.argtypes = [_vp, _f32p, _f32p, s, s, s, s, s, _f32p]
         L.sred_hu_map_2d.argtypes = [_vp, _f32p, _f32p, _f32p, s, s, s, s, _f32p]
         L.sred_phase_correlation_map_2d.argtypes = [_vp, _f32p, _f32p, _f32p, s, s, s, s, _f32p]

@@ -216,6 +216,28 @@ def global_map_host(metric: str, img: np.ndarray, block_width: int, block_height
     return out, info.as_dict()
 
 
+def global_map_batch(jobs: list[dict], n_workers: int = 4, ctx=None) -> list[tuple]:
+    """Many global maps in one call (sred_global_map_2d_batch). Each job is a
+    dict with metric, img (float32 [h, w]), block_width, block_height,
+    relevance_constant and optionally normalize_output; returns one
+    (map, run info) per job, in order."""
+    c = _ctx(ctx)
+    arr = (_lib.SredJob * len(jobs))()
+    keep = []
+    for i, j in enumerate(jobs):
+        img = np.ascontiguousarray(j["img"], np.float32)
+        h, w = img.shape
+        out = np.empty((h, w), np.float32)
+        info = _lib.RunInfo()
+        m = j["metric"].encode()
+        keep.append((img, out, info, m))
+        arr[i] = _lib.SredJob(m, img.ctypes.data, w, h, int(j["block_width"]), int(j["block_height"]),
+                              float(j["relevance_constant"]), int(bool(j.get("normalize_output", True))),
+                              out.ctypes.data, C.pointer(info), -1)
+    c.check(c._L.sred_global_map_2d_batch(c.h, arr, len(jobs), int(n_workers)), "sred_global_map_2d_batch")
+    return [(out, info.as_dict()) for _, out, info, _ in keep]
+
+
 def block_map_device(metric: str, d_img_ptr: int, width: int, height: int, frames: int,
                      reference_block: ReferenceBlock2D, relevance_constant: float, normalize_output: bool,
                      d_out_ptr: int, stream_ptr: int = 0, ctx=None) -> None:

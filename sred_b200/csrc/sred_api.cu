@@ -2,11 +2,13 @@
 // block repetition maps (the part of java/CLUtils.java and java/Utils.java
 // that runs between the plugin commands and the kernels).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -40,6 +42,7 @@ struct sred_ctx {
   std::vector<float> hvars;
   std::string err;
   std::recursive_mutex mu;
+  std::vector<sred_ctx*> workers;  // extra contexts of sred_global_map_2d_batch (own streams and workspaces)
 };
 
 namespace {
@@ -504,6 +507,7 @@ sred_status sred_create(int device, sred_ctx** out) {
 
 sred_status sred_destroy(sred_ctx* c) {
   if (!c) return SRED_ERR_ARG;
+  for (sred_ctx* w : c->workers) sred_destroy(w);
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   for (auto& b : c->buf)
@@ -625,6 +629,92 @@ sred_status sred_global_map_2d(sred_ctx* c, const char* metric, const float* img
   CKS(global_core(c, m, d_img, w, h, bw, bh, relc, normalize, d_out, c->stream, info, nullptr));
   CK(cudaMemcpyAsync(out, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return SRED_OK;
+}
+
+// Grows a context's global-map workspaces to the largest of `jobs` (upper
+// bounds: every interior block relevant), so that no job reallocates, and
+// thereby synchronises the device, while other workers' kernels run.
+sred_status reserve_global(sred_ctx* c, const sred_job* jobs, int n_jobs) {
+  size_t n = 1, n_pad = 256, a = 1, u = 1, cols = 1;
+  bool fp32 = c->engine == SRED_ENGINE_FP32, tc = c->engine == SRED_ENGINE_TC;
+  for (int i = 0; i < n_jobs; i++) {
+    const sred_job& j = jobs[i];
+    Ellipse e;
+    if (j.w <= 0 || j.h <= 0 || j.bw < 3 || j.bh < 3 || j.bw % 2 == 0 || j.bh % 2 == 0) continue;
+    const int K = build_ellipse(j.bw, j.bh, &e);
+    if (K < 2 || K > kMaxK) continue;
+    const size_t inter = (size_t)std::max(0, j.w - 2 * e.rw) * std::max(0, j.h - 2 * e.rh);
+    const size_t np = round_up(std::max<size_t>(inter, 1), 256);
+    n = std::max(n, (size_t)j.w * j.h);
+    n_pad = std::max(n_pad, np);
+    a = std::max(a, np * round_up(3 * K, 32));
+    u = std::max(u, np * round_up(K, 4));
+    cols = std::max(cols, (np / 256) * kColSoaFloats);
+    if (global_metric(j.metric) == kAbsDiff) fp32 = true;
+  }
+  float* f;
+  uint8_t* u8;
+  int* i32;
+  int2* i2;
+  BlockParams* bp;
+  double* d;
+  __nv_bfloat16* bf;
+  for (int id : {B_IMG, B_OUT, B_MEANS, B_STDS, B_MASK, B_MASKIN}) CKS(ensure(c, id, n, &f));
+  CKS(ensure(c, B_FLAGS, n, &u8));
+  for (int id : {B_SLOT, B_GPIX, B_FPIX}) CKS(ensure(c, id, n, &i32));
+  CKS(ensure(c, B_COUNTS, n / kCompactSeg + 2, &i2));
+  CKS(ensure(c, B_PARAMS, n_pad, &bp));
+  CKS(ensure(c, B_RMAX, n_pad / 128, &f));
+  CKS(ensure(c, B_NUM, n_pad, &d));
+  CKS(ensure(c, B_DEN, n_pad, &d));
+  if (tc) {
+    CKS(ensure(c, B_A, a, &bf));
+    CKS(ensure(c, B_B, a, &bf));
+    CKS(ensure(c, B_COLSOA, cols, &f));
+  }
+  if (fp32) CKS(ensure(c, B_U, u, &f));
+  return SRED_OK;
+}
+
+// Jobs are taken in order from a shared counter by `n_workers` host threads,
+// each driving its own context (the caller's and up to seven extra ones kept
+// in the caller's context), so one map's host steps and transfers overlap
+// another map's kernels. Every map is computed exactly as by
+// sred_global_map_2d.
+sred_status sred_global_map_2d_batch(sred_ctx* c, sred_job* jobs, int n_jobs, int n_workers) {
+  if (!c || n_jobs < 0 || (n_jobs > 0 && !jobs)) return SRED_ERR_ARG;
+  if (n_jobs == 0) return SRED_OK;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  n_workers = std::max(1, std::min(n_workers, std::min(8, n_jobs)));
+  while ((int)c->workers.size() < n_workers - 1) {
+    sred_ctx* w = nullptr;
+    const sred_status s = sred_create(c->device, &w);
+    if (s != SRED_OK) return fail(c, s, "could not create a batch worker context");
+    c->workers.push_back(w);
+  }
+  for (sred_ctx* w : c->workers) w->engine = c->engine;
+  CKS(reserve_global(c, jobs, n_jobs));
+  for (int k = 0; k < n_workers - 1; k++) {
+    const sred_status s = reserve_global(c->workers[k], jobs, n_jobs);
+    if (s != SRED_OK) return fail(c, s, "batch workspace: " + c->workers[k]->err);
+  }
+  std::atomic<int> next(0);
+  auto run = [&](sred_ctx* w) {
+    for (;;) {
+      const int i = next.fetch_add(1);
+      if (i >= n_jobs) break;
+      sred_job& j = jobs[i];
+      j.status = sred_global_map_2d(w, j.metric, j.img, j.w, j.h, j.bw, j.bh, j.relevance_constant,
+                                    j.normalize_output, j.out, j.info);
+    }
+  };
+  std::vector<std::thread> threads;
+  for (int k = 1; k < n_workers; k++) threads.emplace_back(run, c->workers[k - 1]);
+  run(c);
+  for (auto& t : threads) t.join();
+  for (int i = 0; i < n_jobs; i++)
+    if (jobs[i].status != SRED_OK) return fail(c, (sred_status)jobs[i].status, "batch job " + std::to_string(i) + " failed");
   return SRED_OK;
 }
 

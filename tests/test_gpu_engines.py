@@ -68,3 +68,24 @@ def test_tc_matches_fp32_unnormalised(ctx):
     w = w1.astype(np.float64)
     scale = w * (np.abs(U @ U.T) @ w)
     assert float(np.max(np.abs(a - b) / scale)) <= TOL["tc"]
+
+
+def test_global_map_batch_equals_single_maps(ctx):
+    """A batch of maps of mixed sizes, blocks and metrics on several workers
+    returns each map exactly as a single call does."""
+    from sred_b200 import clutils, synth
+    jobs = []
+    for i, (w, h, b, metric) in enumerate([(96, 80, 3, "Pearson's R"), (64, 64, 5, "SSIM"), (120, 72, 9, "NRMSE"),
+                                          (80, 96, 5, "Pearson's R"), (72, 72, 11, "SSIM"),
+                                          (64, 96, 3, "Abs. diff. of StdDevs")]):
+        img = synth.normalize_input(synth.spot_image(w, h, 4, seed=40 + i))
+        jobs.append({"metric": metric, "img": img, "block_width": b, "block_height": b, "relevance_constant": 1.0})
+    for engine in ("tc", "fp32"):
+        ctx.set_engine(engine)
+        res = clutils.global_map_batch(jobs, n_workers=3, ctx=ctx)
+        for j, (out, info) in zip(jobs, res):
+            single, _ = clutils.global_map_host(j["metric"], j["img"], j["block_width"], j["block_height"], 1.0,
+                                                ctx=ctx)
+            np.testing.assert_array_equal(out, single)
+            assert info["n_relevant"] > 0
+    ctx.set_engine("fp32")
