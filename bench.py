@@ -128,6 +128,8 @@ def image(seed: int) -> np.ndarray:
     from sred_b200 import synth
     if W_IMG == 1024 and H_IMG == 1024:
         return synth.normalize_input(synth.image_1024_spots_random(seed=seed))
+    if W_IMG == 2048 and H_IMG == 2048:
+        return synth.normalize_input(synth.image_2048_elongated(seed=seed))
     # Same spot density and layout at another side (used for profiling captures).
     return synth.normalize_input(synth.spot_image(W_IMG, H_IMG, max(2, W_IMG * 80 // 1024), seed=seed,
                                                   random_fraction=0.3))
@@ -293,6 +295,9 @@ def run_ours(args, rank, local, world):
 
 
 def traffic_from_profile():
+    """ncu DRAM bytes per Gram launch, recorded for the default workload only."""
+    if (W_IMG, H_IMG, BW, BH) != (1024, 1024, 9, 9):
+        return None
     p = ROOT / "profiles" / "traffic.json"
     if p.exists():
         try:
@@ -456,12 +461,24 @@ def main():
     ap.add_argument("--frames", type=int, default=64, help="frames of the block-map workload")
     ap.add_argument("--size", type=int, default=1024,
                     help="image side (default 1024, the benchmark workload; smaller sides for profiling)")
+    ap.add_argument("--block", type=int, default=9, help="block side of the global workload (default 9)")
     args = ap.parse_args()
-    global W_IMG, H_IMG, WORKLOAD
-    if args.size != 1024:
+    global W_IMG, H_IMG, WORKLOAD, BW, BH, METRIC
+    if args.size == 2048:
+        W_IMG = H_IMG = 2048
+        WORKLOAD = ("global repetition map, 2048x2048 float32 spot image (160x160 lattice, 10% elongated "
+                    "spots), 9x9 block (ellipse K=49), Pearson's R, relevance constant 1.0")
+    elif args.size != 1024:
         W_IMG = H_IMG = args.size
         WORKLOAD = WORKLOAD.replace("1024x1024", f"{args.size}x{args.size}").replace(
             "80x80 lattice", f"{max(2, args.size * 80 // 1024)}x{max(2, args.size * 80 // 1024)} lattice")
+    if args.block != 9:
+        from sred_b200 import utils
+        BW = BH = args.block
+        WORKLOAD = WORKLOAD.replace("9x9 block (ellipse K=49)",
+                                    f"{BW}x{BH} block (ellipse K={utils.block_size(BW, BH)})")
+    if args.size != 1024 or args.block != 9:
+        METRIC = METRIC.replace("1024²/9×9", f"{W_IMG}²/{BW}×{BH}")
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))

@@ -356,3 +356,19 @@ def test_global_1024_sampled(ctx, engine, metric):
     e_n, e_rel = _sampled_errors(ctx, out, info, img, metric, 9, 9, 1.0, rows)
     _note(test="global_1024_sampled", engine=engine, metric=metric, err_norm=e_n, err_rel_raw=e_rel, info=info)
     assert e_n <= GLOBAL_TOL[engine]
+
+
+def test_global_2048_11x11_sampled(ctx):
+    """2048x2048 elongated-spot image, 11x11 (K=81, K'=256: the tensor-core
+    engine's chunk-ring path), Pearson with the relevance mask: sampled rows
+    against FP64."""
+    img = synth.normalize_input(synth.image_2048_elongated(seed=0))
+    ctx.set_engine("tc")
+    out, info = clutils.global_map_host("Pearson's R", img, 11, 11, 1.0, True, ctx=ctx)
+    rng = np.random.default_rng(3)
+    ys, xs = rng.integers(5, 2043, 24), rng.integers(5, 2043, 24)
+    rows = (ys * 2048 + xs).astype(np.int32)
+    e_n, e_rel = _sampled_errors(ctx, out, info, img, "Pearson's R", 11, 11, 1.0, rows)
+    _note(test="global_2048_11x11_sampled", engine="tc", err_norm=e_n, err_rel_raw=e_rel, info=info)
+    assert info["k"] == 81 and info["n_relevant"] > 1_000_000
+    assert e_n <= GLOBAL_TOL["tc"]
