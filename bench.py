@@ -371,6 +371,59 @@ def run_block(args, rank, local, world):
     print(json.dumps(line), flush=True)
 
 
+def run_shard(args, rank, local, world):
+    """One global map of the default workload split by rows across the ranks
+    (strong scaling): every rank prepares the same image, computes the sums
+    of its row blocks, the ranks sum them with one NCCL all-reduce, and every
+    rank finishes the map. Timed on the device, max over ranks."""
+    import torch
+    from sred_b200 import _lib, clutils
+    torch.cuda.set_device(local)
+    ctx = _lib.Context(local, "tc")
+    img = image(0)
+    d_img = torch.from_numpy(img).cuda()
+    d_out = torch.empty_like(d_img)
+    stream = torch.cuda.current_stream()
+    if world > 1:
+        import torch.distributed as dist
+        allreduce = dist.all_reduce
+    else:
+        def allreduce(t):
+            return None
+    info = {}
+
+    def step():
+        nonlocal info
+        info = clutils.global_map_device_sharded(SIM, d_img.data_ptr(), W_IMG, H_IMG, BW, BH, RELC, True,
+                                                 d_out.data_ptr(), rank, world, allreduce, stream.cuda_stream,
+                                                 ctx=ctx)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+    if rank != 0:
+        return
+    pairs = float(info["pairs"])
+    line = {"metric": METRIC.replace("split-BF16 vs FP32 speedup @≤1e-5 err", "one map row-sharded across GPUs"),
+            "value": pairs / (ms / 1e3), "unit": "block-pairs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "bf16x3 split (hi/lo) tensor-core Gram, f32 accumulate, f64 moments",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "image": f"{W_IMG}x{H_IMG}", "block": f"{BW}x{BH}",
+                       "pairs_per_step": pairs, "parallelism": f"rows sharded over {world} GPU(s), one all-reduce "
+                                                               "of per-row sums"}}
+    print(json.dumps(line), flush=True)
+
+
 BATCH_SIDES = [256, 384, 512, 768, 1024]
 BATCH_BLOCKS = [3, 5, 9, 13, 15]
 
@@ -456,6 +509,9 @@ def main():
     ap.add_argument("--workload", choices=["global", "block", "batch"], default="global",
                     help="global repetition map (default, the headline), the block (local) map, or batched "
                          "global maps of many images")
+    ap.add_argument("--mode", choices=["replicas", "shard"], default="replicas",
+                    help="global workload on N GPUs: independent replicas (default, weak scaling) or one map "
+                         "row-sharded across the GPUs (strong scaling)")
     ap.add_argument("--images", type=int, default=8, help="images of the batch workload (10 maps each)")
     ap.add_argument("--workers", type=int, default=4, help="host workers of the batch workload")
     ap.add_argument("--frames", type=int, default=64, help="frames of the block-map workload")
@@ -490,6 +546,8 @@ def main():
             run_block(args, rank, local, world)
         elif args.workload == "batch":
             run_batch(args, rank, local, world)
+        elif args.mode == "shard":
+            run_shard(args, rank, local, world)
         else:
             run_ours(args, rank, local, world)
     finally:

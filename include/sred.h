@@ -101,6 +101,26 @@ sred_status sred_global_map_2d(sred_ctx *ctx, const char *metric, const float *i
                                int bw, int bh, float relevance_constant, int normalize_output,
                                float *out, sred_run_info *info);
 
+/* Row-sharded global map (no counterpart in the reference): the map of
+ * sred_global_map_2d_device split across n_shards processes, usually one
+ * per GPU. Phase 1, on every shard: the moment pass, relevance mask and
+ * compaction (all of them, on every shard), then the all-pairs sums of this
+ * shard's rows only; they are written to d_sums (device memory, capacity in
+ * doubles >= 2 x relevant blocks; the interior pixel count always suffices)
+ * as [num | den] over the relevant non-flat blocks, zero for other shards'
+ * rows, and info->n_relevant - info->n_flat is their count. The caller then
+ * sums d_sums over the shards (one all-reduce, e.g. NCCL) and calls phase 2
+ * on every shard that needs the map, with the summed buffer: finalisation and
+ * normalisation into d_out. Rows are split in 128-row blocks of the compacted
+ * block list, shard s taking blocks [n s / S, n (s + 1) / S). No other call
+ * may use the context between the two phases (phase 2 then fails with
+ * SRED_ERR_ARG). */
+sred_status sred_global_map_2d_shard_sums(sred_ctx *ctx, const char *metric, const float *d_img, int w, int h,
+                                          int bw, int bh, float relevance_constant, int shard, int n_shards,
+                                          double *d_sums, size_t capacity, void *stream, sred_run_info *info);
+sred_status sred_global_map_2d_shard_finish(sred_ctx *ctx, const double *d_sums, int normalize_output,
+                                            float *d_out, void *stream, sred_run_info *info);
+
 /* One map of a batch (sred_global_map_2d_batch): the arguments of
  * sred_global_map_2d, and the job's own status on return. */
 typedef struct {

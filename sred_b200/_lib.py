@@ -25,6 +25,7 @@ EXPORTS = [
     "sred_calculate_block_repetition_map_2d", "sred_block_map_2d_device", "sred_reference_block_2d",
     "sred_normalize_image_2d", "sred_debug_gram_rowdot", "sred_block_map_2d_device_noalloc",
     "sred_patch_hu_map_2d", "sred_hu_map_2d", "sred_phase_correlation_map_2d", "sred_global_map_2d_batch",
+    "sred_global_map_2d_shard_sums", "sred_global_map_2d_shard_finish",
 ]
 
 
@@ -100,6 +101,9 @@ def load() -> C.CDLL:
         L.sred_block_map_2d_device_noalloc.argtypes = [C.c_char_p, _vp, s, s, s, _f32p, s, s, s, C.c_float,
                                                        C.c_float, s, _vp, _vp]
         L.sred_global_map_2d_batch.argtypes = [_vp, C.POINTER(SredJob), s, s]
+        L.sred_global_map_2d_shard_sums.argtypes = [_vp, C.c_char_p, _vp, s, s, s, s, C.c_float, s, s, _vp,
+                                                    C.c_size_t, _vp, C.POINTER(RunInfo)]
+        L.sred_global_map_2d_shard_finish.argtypes = [_vp, _vp, s, _vp, _vp, C.POINTER(RunInfo)]
         L.sred_patch_hu_map_2d.argtypes = [_vp, _f32p, _f32p, s, s, s, s, s, _f32p]
         L.sred_hu_map_2d.argtypes = [_vp, _f32p, _f32p, _f32p, s, s, s, s, _f32p]
         L.sred_phase_correlation_map_2d.argtypes = [_vp, _f32p, _f32p, _f32p, s, s, s, s, _f32p]

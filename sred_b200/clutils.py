@@ -238,6 +238,59 @@ def global_map_batch(jobs: list[dict], n_workers: int = 4, ctx=None) -> list[tup
     return [(out, info.as_dict()) for _, out, info, _ in keep]
 
 
+# ---------------------------------------------------------------------------
+# Row-sharded global map (one map across several processes / GPUs)
+# ---------------------------------------------------------------------------
+
+def shard_row_blocks(n_gram: int, shard: int, n_shards: int) -> tuple[int, int]:
+    """Row blocks [rb0, rb1) (128 rows of the compacted block list each) that
+    shard `shard` of `n_shards` computes; the rule libsred applies."""
+    n_rb = (n_gram + 127) // 128
+    return n_rb * shard // n_shards, n_rb * (shard + 1) // n_shards
+
+
+def sharded_exchange(compute_sums, finish, allreduce):
+    """The row-sharded global map's one exchange step: this rank's per-row
+    sums (zero outside its rows) -> summed over all ranks in place (the only
+    collective) -> the map finished from the summed sums."""
+    sums, n_gram = compute_sums()
+    allreduce(sums[:2 * n_gram])
+    return finish(sums)
+
+
+def global_map_device_sharded(metric: str, d_img_ptr: int, width: int, height: int, block_width: int,
+                              block_height: int, relevance_constant: float, normalize_output: bool, d_out_ptr: int,
+                              rank: int, world: int, allreduce=None, stream_ptr: int = 0, ctx=None) -> dict:
+    """One global map computed by `world` ranks (each its own GPU and
+    context), every rank finishing the full map into d_out. `allreduce`
+    (default torch.distributed.all_reduce) sums a float64 CUDA tensor across
+    the ranks in place."""
+    import torch
+    c = _ctx(ctx)
+    cap = 2 * max(1, width * height)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    sums = torch.zeros(cap, dtype=torch.float64, device=dev)
+    info1, info2 = _lib.RunInfo(), _lib.RunInfo()
+    if allreduce is None:
+        import torch.distributed as dist
+        allreduce = dist.all_reduce
+
+    def compute():
+        c.check(c._L.sred_global_map_2d_shard_sums(
+            c.h, metric.encode(), C.c_void_p(d_img_ptr), width, height, block_width, block_height,
+            float(relevance_constant), int(rank), int(world), C.c_void_p(sums.data_ptr()), cap,
+            C.c_void_p(stream_ptr or None), C.byref(info1)), "sred_global_map_2d_shard_sums")
+        return sums, int(info1.n_relevant - info1.n_flat)
+
+    def fin(summed):
+        c.check(c._L.sred_global_map_2d_shard_finish(c.h, C.c_void_p(summed.data_ptr()), int(bool(normalize_output)),
+                                                     C.c_void_p(d_out_ptr), C.c_void_p(stream_ptr or None),
+                                                     C.byref(info2)), "sred_global_map_2d_shard_finish")
+        return info2.as_dict()
+
+    return sharded_exchange(compute, fin, allreduce)
+
+
 def block_map_device(metric: str, d_img_ptr: int, width: int, height: int, frames: int,
                      reference_block: ReferenceBlock2D, relevance_constant: float, normalize_output: bool,
                      d_out_ptr: int, stream_ptr: int = 0, ctx=None) -> None:

@@ -52,8 +52,11 @@ struct EpiConsts {
 
 // Launch the FP32 CUDA-core all-pairs kernel (global_fp32.cu).
 // U: n_pad x kp floats (unit vectors), params: n_pad entries, num/den: n doubles (zeroed).
+// Rows are processed in 128-row blocks; [rb_begin, rb_end) restricts the launch
+// to those row blocks (rb_end < 0: all), the unit of row sharding.
 cudaError_t launch_gram_fp32(const float* U, int kp, const BlockParams* params, const float* tile_rmax,
-                             EpiConsts ec, double* num, double* den, int num_sms, cudaStream_t st);
+                             EpiConsts ec, double* num, double* den, int num_sms, cudaStream_t st,
+                             int rb_begin = 0, int rb_end = -1);
 
 // Column parameters of one 256-column tile, structure of arrays, as the
 // tensor-core engine copies them into shared memory:
@@ -65,6 +68,7 @@ constexpr int kColSoaFloats = 4 * 256 + 4;
 // of kColSoaFloats (k_col_soa).
 cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int kq, int n_pad,
                            const BlockParams* params, const float* colsoa, const float* tile_rmax, EpiConsts ec,
-                           double* num, double* den, int num_sms, int* status, cudaStream_t st);
+                           double* num, double* den, int num_sms, int* status, cudaStream_t st,
+                           int rb_begin = 0, int rb_end = -1);
 
 }  // namespace sred

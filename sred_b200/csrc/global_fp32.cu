@@ -10,6 +10,8 @@
 //
 // This is the comparison form for the tensor-core engine: the same moments,
 // compaction, work split and epilogue, with FFMA contraction.
+#include <algorithm>
+
 #include "common.cuh"
 #include "epilogue.cuh"
 
@@ -29,7 +31,8 @@ struct Fp32Args {
   EpiConsts ec;
   double* num;
   double* den;
-  int n_rb;          // 128-row blocks
+  int rb0;           // first 128-row block of this launch
+  int n_rb;          // 128-row blocks of this launch
   int n_ct;          // 128-column tiles
   int ct_per_item;   // column tiles per work item
   int n_items;
@@ -80,7 +83,7 @@ __global__ void __launch_bounds__(NT, 2) k_gram_fp32(Fp32Args g) {
   const bool gram = METRIC != kAbsDiff;
 
   for (int item = blockIdx.x; item < g.n_items; item += gridDim.x) {
-    const int rb = item % g.n_rb;
+    const int rb = g.rb0 + item % g.n_rb;
     const int seg = item / g.n_rb;
     const int ct0 = seg * g.ct_per_item;
     const int ct1 = min(ct0 + g.ct_per_item, g.n_ct);
@@ -161,7 +164,8 @@ __global__ void __launch_bounds__(NT, 2) k_gram_fp32(Fp32Args g) {
 }  // namespace
 
 cudaError_t launch_gram_fp32(const float* U, int kp, const BlockParams* params, const float* tile_rmax,
-                             EpiConsts ec, double* num, double* den, int num_sms, cudaStream_t st) {
+                             EpiConsts ec, double* num, double* den, int num_sms, cudaStream_t st, int rb_begin,
+                             int rb_end) {
   Fp32Args g;
   g.U = U;
   g.kp = kp;
@@ -170,8 +174,12 @@ cudaError_t launch_gram_fp32(const float* U, int kp, const BlockParams* params, 
   g.ec = ec;
   g.num = num;
   g.den = den;
-  g.n_rb = (ec.n + BM - 1) / BM;
-  g.n_ct = g.n_rb;
+  g.n_ct = (ec.n + BM - 1) / BM;
+  if (rb_end < 0) rb_end = g.n_ct;
+  rb_end = std::min(rb_end, g.n_ct);
+  if (rb_begin < 0 || rb_begin >= rb_end) return cudaSuccess;  // no rows in this range
+  g.rb0 = rb_begin;
+  g.n_rb = rb_end - rb_begin;
   // Split the column range so that there are at least ~4 items per SM.
   int segs = (4 * num_sms + g.n_rb - 1) / g.n_rb;
   if (segs > g.n_ct) segs = g.n_ct;

@@ -56,6 +56,7 @@ struct TcArgs {
   int kq, nkc, stages;
   int nfull, tail;              // tile-ring mode: 64-column chunks and a 32-column tail (0 or 1)
   uint32_t a_bytes, b_bytes;    // tile-ring mode: A tile and one B tile in shared memory
+  int rb0;                      // first 128-row block of this launch
   int n_rb, n_ct, ct_per_item, n_items;
   const BlockParams* params;
   const float* colsoa;
@@ -361,7 +362,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint32_t s = 0, eph = 0;  // B ring: stage, parity of the round being refilled
       bool ok = true, a_issued = false;
       for (int item = blockIdx.x; ok && item < g.n_items; item += gridDim.x, item_i++) {
-        const int rb = item % g.n_rb, seg = item / g.n_rb;
+        const int rb = g.rb0 + item % g.n_rb, seg = item / g.n_rb;
         const int ct0 = seg * g.ct_per_item, ct1 = min(ct0 + g.ct_per_item, g.n_ct);
         if (!mbar_wait(b_aempty, (item_i & 1) ^ 1, g.status, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
         if (TR) {
@@ -496,7 +497,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint32_t tile = 0;
     bool ok = true;
     for (int item = blockIdx.x; ok && item < g.n_items; item += gridDim.x) {
-      const int rb = item % g.n_rb, seg = item / g.n_rb;
+      const int rb = g.rb0 + item % g.n_rb, seg = item / g.n_rb;
       const int ct0 = seg * g.ct_per_item, ct1 = min(ct0 + g.ct_per_item, g.n_ct);
       const int row = rb * kBM + quarter * 32 + lane;
       const RowState rs = make_row(g.params[row], g.ec);
@@ -587,7 +588,8 @@ bool make_map(CUtensorMap* m, const __nv_bfloat16* ptr, int kq, int rows, int bo
 
 cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int kq, int n_pad,
                            const BlockParams* params, const float* colsoa, const float* tile_rmax, EpiConsts ec,
-                           double* num, double* den, int num_sms, int* status, cudaStream_t st) {
+                           double* num, double* den, int num_sms, int* status, cudaStream_t st, int rb_begin,
+                           int rb_end) {
   if (kq % 16 != 0 || n_pad % kBN != 0) return cudaErrorInvalidValue;
   TcArgs g;
   g.kq = kq;
@@ -612,7 +614,12 @@ cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int k
   }
   // Only row blocks that hold valid rows are work; split the column range so
   // that every SM gets several items.
-  const int n_rb_valid = (ec.n + kBM - 1) / kBM;
+  int n_rb_valid = (ec.n + kBM - 1) / kBM;
+  if (rb_end < 0) rb_end = n_rb_valid;
+  rb_end = std::min(rb_end, n_rb_valid);
+  if (rb_begin < 0 || rb_begin >= rb_end) return cudaSuccess;  // no rows in this range
+  g.rb0 = rb_begin;
+  n_rb_valid = rb_end - rb_begin;
   int segs = (4 * num_sms + n_rb_valid - 1) / n_rb_valid;
   segs = std::max(1, std::min(segs, g.n_ct));
   g.ct_per_item = (g.n_ct + segs - 1) / segs;

@@ -30,6 +30,17 @@ struct DevBuf {
   size_t cap = 0;
 };
 
+// A prepared global map: moments, relevance mask, compaction and the
+// contraction operands are in the context's workspaces. Kept in the context
+// between the two phases of the row-sharded entry points.
+struct GState {
+  bool valid = false;
+  int metric = 0, w = 0, h = 0, rw = 0, rh = 0, K = 0, n_g = 0, n_flat = 0, engine = 0, kp = 0, kq = 0;
+  size_t n = 0, n_pad = 0;
+  float nv = 0, thr = 0, npx = 0, relc = 0;
+  bool given = false;
+};
+
 }  // namespace
 
 struct sred_ctx {
@@ -43,6 +54,7 @@ struct sred_ctx {
   std::string err;
   std::recursive_mutex mu;
   std::vector<sred_ctx*> workers;  // extra contexts of sred_global_map_2d_batch (own streams and workspaces)
+  GState shard;                    // the map prepared by sred_global_map_2d_shard_sums
 };
 
 namespace {
@@ -187,10 +199,12 @@ struct GivenStats {
   float threshold, noise_var, n_pixels;
 };
 
-// The global repetition map on device-resident data.
-sred_status global_core(sred_ctx* c, int metric, const float* d_img, int w, int h, int bw, int bh, float relc,
-                        int normalize, float* d_out, cudaStream_t st, sred_run_info* info,
-                        const GivenStats* given) {
+
+// Phase 1: everything before the all-pairs contraction.
+sred_status global_prepare(sred_ctx* c, int metric, const float* d_img, int w, int h, int bw, int bh, float relc,
+                           cudaStream_t st, const GivenStats* given, GState* gs) {
+  gs->valid = false;
+  c->shard.valid = false;  // the workspaces are about to be overwritten
   Ellipse e;
   CKS(check_block(c, w, h, bw, bh, &e));
   const int K = e.k, rw = e.rw, rh = e.rh;
@@ -286,28 +300,60 @@ sred_status global_core(sred_ctx* c, int metric, const float* d_img, int w, int 
                                   kp, d_A, d_B, kq, d_params, d_rmax, d_sums);
     CK(cudaGetLastError());
   }
-  float* d_colsoa = nullptr;
   if (engine == SRED_ENGINE_TC) {
+    float* d_colsoa;
     CKS(ensure(c, B_COLSOA, (n_pad / 256) * kColSoaFloats, &d_colsoa));
     k_col_soa<<<(int)(n_pad / 256), 256, 0, st>>>(d_params, d_colsoa);
     CK(cudaGetLastError());
   }
   CK(cudaEventRecord(c->ev[1], st));
-  EpiConsts ec;
-  ec.metric = metric;
-  ec.n = n_g;
-  ec.nrmse_scale = (float)((double)(K - 1) / (double)K);
-  ec.c1 = kC1;
-  ec.c2 = kC2;
-  if (n_g > 0) {
-    if (engine == SRED_ENGINE_FP32) {
-      CK(launch_gram_fp32(d_U, kp, d_params, d_rmax, ec, d_num, d_den, c->num_sms, st));
+  gs->metric = metric;
+  gs->w = w;
+  gs->h = h;
+  gs->rw = rw;
+  gs->rh = rh;
+  gs->K = K;
+  gs->n_g = n_g;
+  gs->n_flat = n_flat;
+  gs->engine = engine;
+  gs->kp = kp;
+  gs->kq = kq;
+  gs->n = n;
+  gs->n_pad = n_pad;
+  gs->nv = nv;
+  gs->thr = thr;
+  gs->npx = npx;
+  gs->relc = relc;
+  gs->given = given != nullptr;
+  gs->valid = true;
+  return SRED_OK;
+}
+
+// Phase 2: the all-pairs contraction for the row blocks [rb_begin, rb_end)
+// (128 rows each; rb_end < 0: all rows) into the num/den workspaces.
+sred_status global_gram(sred_ctx* c, const GState& gs, cudaStream_t st, int rb_begin, int rb_end) {
+  if (gs.n_g > 0) {
+    EpiConsts ec;
+    ec.metric = gs.metric;
+    ec.n = gs.n_g;
+    ec.nrmse_scale = (float)((double)(gs.K - 1) / (double)gs.K);
+    ec.c1 = kC1;
+    ec.c2 = kC2;
+    double* d_num = static_cast<double*>(c->buf[B_NUM].p);
+    double* d_den = static_cast<double*>(c->buf[B_DEN].p);
+    const BlockParams* d_params = static_cast<const BlockParams*>(c->buf[B_PARAMS].p);
+    const float* d_rmax = static_cast<const float*>(c->buf[B_RMAX].p);
+    if (gs.engine == SRED_ENGINE_FP32) {
+      CK(launch_gram_fp32(static_cast<const float*>(c->buf[B_U].p), gs.kp, d_params, d_rmax, ec, d_num, d_den,
+                          c->num_sms, st, rb_begin, rb_end));
     } else {
       int* d_status;
       CKS(ensure(c, B_STATUS, 4, &d_status));
       CK(cudaMemsetAsync(d_status, 0, 4 * sizeof(int), st));
-      CK(launch_gram_tc(d_A, d_B, kq, (int)n_pad, d_params, d_colsoa, d_rmax, ec, d_num, d_den, c->num_sms,
-                        d_status, st));
+      CK(launch_gram_tc(static_cast<const __nv_bfloat16*>(c->buf[B_A].p),
+                        static_cast<const __nv_bfloat16*>(c->buf[B_B].p), gs.kq, (int)gs.n_pad, d_params,
+                        static_cast<const float*>(c->buf[B_COLSOA].p), d_rmax, ec, d_num, d_den, c->num_sms,
+                        d_status, st, rb_begin, rb_end));
       int status = 0;
       CK(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
@@ -315,24 +361,34 @@ sred_status global_core(sred_ctx* c, int metric, const float* d_img, int w, int 
     }
   }
   CK(cudaEventRecord(c->ev[2], st));
-  const double sk = std::sqrt((double)(K - 1) / (double)K);
-  k_finalize<<<grid_for(n, 256, 1 << 30), 256, 0, st>>>(d_slot, w, h, rw, rh, d_num, d_den, d_params, d_sums,
-                                                          n_flat, metric, sk, (double)npx, d_mask,
-                                                          relc > 0.0f ? 1 : 0, d_out);
+  return SRED_OK;
+}
+
+// Phase 3: per-pixel finalisation (num / (den nPixels + eps), inversion,
+// mask), normalisation, run info.
+sred_status global_finish(sred_ctx* c, const GState& gs, cudaStream_t st, int normalize, float* d_out,
+                          sred_run_info* info) {
+  const double sk = std::sqrt((double)(gs.K - 1) / (double)gs.K);
+  const float* d_mask = static_cast<const float*>(c->buf[B_MASK].p);
+  k_finalize<<<grid_for(gs.n, 256, 1 << 30), 256, 0, st>>>(
+      static_cast<const int*>(c->buf[B_SLOT].p), gs.w, gs.h, gs.rw, gs.rh,
+      static_cast<const double*>(c->buf[B_NUM].p), static_cast<const double*>(c->buf[B_DEN].p),
+      static_cast<const BlockParams*>(c->buf[B_PARAMS].p), static_cast<const double*>(c->buf[B_SUMS].p),
+      gs.n_flat, gs.metric, sk, (double)gs.npx, d_mask, gs.relc > 0.0f ? 1 : 0, d_out);
   CK(cudaGetLastError());
-  if (normalize) CKS(normalize_dev(c, d_out, d_mask, w, h, rw, rh, 1, st));
+  if (normalize) CKS(normalize_dev(c, d_out, d_mask, gs.w, gs.h, gs.rw, gs.rh, 1, st));
   CK(cudaEventRecord(c->ev[3], st));
   CK(cudaEventSynchronize(c->ev[3]));
   if (info) {
-    info->n_blocks = (int64_t)std::max(0, w - 2 * rw) * std::max(0, h - 2 * rh);
-    info->n_relevant = (int64_t)n_g + n_flat;
-    info->n_flat = n_flat;
+    info->n_blocks = (int64_t)std::max(0, gs.w - 2 * gs.rw) * std::max(0, gs.h - 2 * gs.rh);
+    info->n_relevant = (int64_t)gs.n_g + gs.n_flat;
+    info->n_flat = gs.n_flat;
     info->pairs = (double)info->n_relevant * (double)info->n_relevant;
-    info->noise_var = nv;
-    info->threshold = thr;
-    info->n_pixels = npx;
-    info->k = K;
-    info->engine = engine;
+    info->noise_var = gs.nv;
+    info->threshold = gs.thr;
+    info->n_pixels = gs.npx;
+    info->k = gs.K;
+    info->engine = gs.engine;
     float t01 = 0, t12 = 0, t23 = 0, t03 = 0;
     cudaEventElapsedTime(&t01, c->ev[0], c->ev[1]);
     cudaEventElapsedTime(&t12, c->ev[1], c->ev[2]);
@@ -342,9 +398,20 @@ sred_status global_core(sred_ctx* c, int metric, const float* d_img, int w, int 
     info->ms_gram = t12;
     info->ms_finalize = t23;
     info->ms_total = t03;
-    info->launches = (given ? 0 : 2) + 4 + (n_g > 0 ? (engine == SRED_ENGINE_TC ? 3 : 2) : 0) + 1 + (normalize ? 2 : 0);
+    info->launches = (gs.given ? 0 : 2) + 4 + (gs.n_g > 0 ? (gs.engine == SRED_ENGINE_TC ? 3 : 2) : 0) + 1 +
+                     (normalize ? 2 : 0);
   }
   return SRED_OK;
+}
+
+// The global repetition map on device-resident data.
+sred_status global_core(sred_ctx* c, int metric, const float* d_img, int w, int h, int bw, int bh, float relc,
+                        int normalize, float* d_out, cudaStream_t st, sred_run_info* info,
+                        const GivenStats* given) {
+  GState gs;
+  CKS(global_prepare(c, metric, d_img, w, h, bw, bh, relc, st, given, &gs));
+  CKS(global_gram(c, gs, st, 0, -1));
+  return global_finish(c, gs, st, normalize, d_out, info);
 }
 
 // Raw block map of the shape metrics (stds_out: FP32 local stds, or NULL).
@@ -374,6 +441,7 @@ sred_status block_shape_launch(sred_ctx* c, int metric, const float* d_img, int 
 sred_status block_core(sred_ctx* c, int metric, const float* d_img, int w, int h, int frames,
                        const float* ref_pixels, int block_size, int bw, int bh, float ref_mean, float ref_std,
                        float relc, int normalize, float* d_out, cudaStream_t st) {
+  c->shard.valid = false;  // shares workspaces with the global map
   Ellipse e;
   CKS(check_block(c, w, h, bw, bh, &e));
   if (block_size != e.k) return fail(c, SRED_ERR_ARG, "block_size does not match the ellipse of bw x bh");
@@ -561,6 +629,7 @@ sred_status sred_relevance_mask_2d(sred_ctx* c, const float* img, int w, int h, 
                                    const float* stds, float relc, float* mask, float* threshold, float* noise_var) {
   if (!c || !img || !stds || !mask || !threshold || !noise_var) return SRED_ERR_ARG;
   std::lock_guard<std::recursive_mutex> lk(c->mu);
+  c->shard.valid = false;  // overwrites workspaces of a prepared shard
   cudaSetDevice(c->device);
   if (w <= 0 || h <= 0 || bw < 1 || bh < 1) return fail(c, SRED_ERR_ARG, "bad dimensions");
   const size_t n = (size_t)w * h;
@@ -718,6 +787,68 @@ sred_status sred_global_map_2d_batch(sred_ctx* c, sred_job* jobs, int n_jobs, in
   return SRED_OK;
 }
 
+// Row blocks (128 rows of the compacted block list) of shard `shard`.
+void shard_row_blocks(int n_g, int shard, int n_shards, int* rb0, int* rb1) {
+  const int64_t n_rb = (n_g + 127) / 128;
+  *rb0 = (int)(n_rb * shard / n_shards);
+  *rb1 = (int)(n_rb * (shard + 1) / n_shards);
+}
+
+sred_status sred_global_map_2d_shard_sums(sred_ctx* c, const char* metric, const float* d_img, int w, int h,
+                                          int bw, int bh, float relc, int shard, int n_shards, double* d_sums,
+                                          size_t capacity, void* stream, sred_run_info* info) {
+  if (!c || !d_img || !d_sums || n_shards < 1 || shard < 0 || shard >= n_shards) return SRED_ERR_ARG;
+  const int m = global_metric(metric);
+  if (m < 0) return fail(c, SRED_ERR_UNKNOWN_METRIC, "unknown global metric");
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  cudaStream_t st = pick(c, stream);
+  GState gs;
+  CKS(global_prepare(c, m, d_img, w, h, bw, bh, relc, st, nullptr, &gs));
+  if (capacity < 2 * (size_t)gs.n_g) return fail(c, SRED_ERR_ARG, "sums buffer smaller than 2 x relevant blocks");
+  int rb0, rb1;
+  shard_row_blocks(gs.n_g, shard, n_shards, &rb0, &rb1);
+  if (rb0 < rb1) CKS(global_gram(c, gs, st, rb0, rb1));
+  if (gs.n_g > 0) {
+    CK(cudaMemcpyAsync(d_sums, c->buf[B_NUM].p, gs.n_g * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(d_sums + gs.n_g, c->buf[B_DEN].p, gs.n_g * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  if (info) {
+    std::memset(info, 0, sizeof(*info));
+    info->n_blocks = (int64_t)std::max(0, w - 2 * gs.rw) * std::max(0, h - 2 * gs.rh);
+    info->n_relevant = (int64_t)gs.n_g + gs.n_flat;
+    info->n_flat = gs.n_flat;
+    info->pairs = (double)info->n_relevant * (double)info->n_relevant;
+    info->noise_var = gs.nv;
+    info->threshold = gs.thr;
+    info->n_pixels = gs.npx;
+    info->k = gs.K;
+    info->engine = gs.engine;
+  }
+  c->shard = gs;
+  return SRED_OK;
+}
+
+sred_status sred_global_map_2d_shard_finish(sred_ctx* c, const double* d_sums, int normalize, float* d_out,
+                                            void* stream, sred_run_info* info) {
+  if (!c || !d_sums || !d_out) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (!c->shard.valid) return fail(c, SRED_ERR_ARG, "no map prepared by sred_global_map_2d_shard_sums on this context");
+  cudaStream_t st = pick(c, stream);
+  const GState gs = c->shard;
+  c->shard.valid = false;
+  if (gs.n_g > 0) {
+    CK(cudaMemcpyAsync(c->buf[B_NUM].p, d_sums, gs.n_g * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(c->buf[B_DEN].p, d_sums + gs.n_g, gs.n_g * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  }
+  CK(cudaEventRecord(c->ev[0], st));
+  CK(cudaEventRecord(c->ev[1], st));
+  CK(cudaEventRecord(c->ev[2], st));
+  return global_finish(c, gs, st, normalize, d_out, info);
+}
+
 sred_status sred_global_map_2d_device(sred_ctx* c, const char* metric, const float* d_img, int w, int h, int bw,
                                       int bh, float relc, int normalize, float* d_out, void* stream,
                                       sred_run_info* info) {
@@ -769,6 +900,7 @@ sred_status sred_debug_gram_rowdot(sred_ctx* c, int engine, const float* u, cons
   if (!c || !u || !w1 || !w2 || !num || !den || n <= 0 || k <= 0 || k > kMaxK) return SRED_ERR_ARG;
   if (engine != SRED_ENGINE_TC && engine != SRED_ENGINE_FP32) return SRED_ERR_ARG;
   std::lock_guard<std::recursive_mutex> lk(c->mu);
+  c->shard.valid = false;  // overwrites workspaces of a prepared shard
   cudaSetDevice(c->device);
   cudaStream_t st = c->stream;
   const size_t n_pad = round_up((size_t)n, 256);

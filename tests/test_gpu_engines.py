@@ -89,3 +89,43 @@ def test_global_map_batch_equals_single_maps(ctx):
             np.testing.assert_array_equal(out, single)
             assert info["n_relevant"] > 0
     ctx.set_engine("fp32")
+
+
+def test_sharded_map_equals_full_map(ctx):
+    """The row-sharded entry points, every shard run in turn on one GPU and
+    their sums added (what the all-reduce does across GPUs), give the map of
+    sred_global_map_2d_device."""
+    import ctypes as C
+
+    import torch
+    from sred_b200 import clutils, synth
+    img = synth.normalize_input(synth.spot_image(176, 144, 8, seed=7))
+    H, W = img.shape
+    d_in = torch.from_numpy(img).cuda()
+    for engine in ("tc", "fp32"):
+        ctx.set_engine(engine)
+        for metric in ("Pearson's R", "SSIM", "NRMSE"):
+            full = torch.empty_like(d_in)
+            clutils.global_map_device(metric, d_in.data_ptr(), W, H, 5, 5, 1.0, True, full.data_ptr(), ctx=ctx)
+            torch.cuda.synchronize()
+            for world in (2, 3):
+                cap = 2 * W * H
+                acc = torch.zeros(cap, dtype=torch.float64, device="cuda")
+                for s in range(world):
+                    part = torch.zeros(cap, dtype=torch.float64, device="cuda")
+                    info = _lib.RunInfo()
+                    ctx.check(ctx._L.sred_global_map_2d_shard_sums(
+                        ctx.h, metric.encode(), C.c_void_p(d_in.data_ptr()), W, H, 5, 5, 1.0, s, world,
+                        C.c_void_p(part.data_ptr()), cap, None, C.byref(info)), "shard_sums")
+                    acc += part
+                out = torch.empty_like(d_in)
+                ctx.check(ctx._L.sred_global_map_2d_shard_finish(ctx.h, C.c_void_p(acc.data_ptr()), 1,
+                                                                 C.c_void_p(out.data_ptr()), None, None),
+                          "shard_finish")
+                torch.cuda.synchronize()
+                np.testing.assert_allclose(out.cpu().numpy(), full.cpu().numpy(), rtol=0, atol=1e-6)
+    # phase 2 without phase 1 is refused
+    st = ctx._L.sred_global_map_2d_shard_finish(ctx.h, C.c_void_p(d_in.data_ptr()), 1, C.c_void_p(d_in.data_ptr()),
+                                                None, None)
+    assert st == _lib.ERR_ARG
+    ctx.set_engine("fp32")
