@@ -130,6 +130,8 @@ def image(seed: int) -> np.ndarray:
         return synth.normalize_input(synth.image_1024_spots_random(seed=seed))
     if W_IMG == 2048 and H_IMG == 2048:
         return synth.normalize_input(synth.image_2048_elongated(seed=seed))
+    if W_IMG == 256 and H_IMG == 256:
+        return synth.normalize_input(synth.image_256_spots(seed=seed))
     # Same spot density and layout at another side (used for profiling captures).
     return synth.normalize_input(synth.spot_image(W_IMG, H_IMG, max(2, W_IMG * 80 // 1024), seed=seed,
                                                   random_fraction=0.3))
@@ -296,7 +298,7 @@ def run_ours(args, rank, local, world):
 
 def traffic_from_profile():
     """ncu DRAM bytes per Gram launch, recorded for the default workload only."""
-    if (W_IMG, H_IMG, BW, BH) != (1024, 1024, 9, 9):
+    if (W_IMG, H_IMG, BW, BH, RELC) != (1024, 1024, 9, 9, 1.0):
         return None
     p = ROOT / "profiles" / "traffic.json"
     if p.exists():
@@ -518,9 +520,14 @@ def main():
     ap.add_argument("--size", type=int, default=1024,
                     help="image side (default 1024, the benchmark workload; smaller sides for profiling)")
     ap.add_argument("--block", type=int, default=9, help="block side of the global workload (default 9)")
+    ap.add_argument("--relevance", type=float, default=1.0, help="relevance constant of the global workload")
     args = ap.parse_args()
-    global W_IMG, H_IMG, WORKLOAD, BW, BH, METRIC
-    if args.size == 2048:
+    global W_IMG, H_IMG, WORKLOAD, BW, BH, METRIC, RELC
+    if args.size == 256:
+        W_IMG = H_IMG = 256
+        WORKLOAD = ("global repetition map, 256x256 float32 spot image (20x20 lattice, 400 spots), "
+                    "9x9 block (ellipse K=49), Pearson's R, relevance constant 1.0")
+    elif args.size == 2048:
         W_IMG = H_IMG = 2048
         WORKLOAD = ("global repetition map, 2048x2048 float32 spot image (160x160 lattice, 10% elongated "
                     "spots), 9x9 block (ellipse K=49), Pearson's R, relevance constant 1.0")
@@ -533,6 +540,9 @@ def main():
         BW = BH = args.block
         WORKLOAD = WORKLOAD.replace("9x9 block (ellipse K=49)",
                                     f"{BW}x{BH} block (ellipse K={utils.block_size(BW, BH)})")
+    if args.relevance != 1.0:
+        RELC = args.relevance
+        WORKLOAD = WORKLOAD.replace("relevance constant 1.0", f"relevance constant {RELC:g}")
     if args.size != 1024 or args.block != 9:
         METRIC = METRIC.replace("1024²/9×9", f"{W_IMG}²/{BW}×{BH}")
     args.warmup = max(args.warmup, 3)

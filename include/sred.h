@@ -59,6 +59,12 @@ typedef struct {
 sred_status sred_create(int device_ordinal, sred_ctx **out);
 sred_status sred_destroy(sred_ctx *ctx);
 sred_status sred_set_engine(sred_ctx *ctx, int engine);
+/* Messages of the context (errors, and one line per global map with its
+ * size, relevant blocks, engine and time) are passed to cb on the calling
+ * thread; NULL turns logging off. The reference reports through IJ.log /
+ * IJ.error (java/GlobalRepetition2D_.java, java/CLUtils.java); a host binds
+ * this callback to its own log. */
+sred_status sred_set_log_callback(sred_ctx *ctx, void (*cb)(const char *message, void *user), void *user);
 const char *sred_status_string(sred_status s);
 const char *sred_last_error(sred_ctx *ctx);
 

@@ -25,7 +25,7 @@ EXPORTS = [
     "sred_calculate_block_repetition_map_2d", "sred_block_map_2d_device", "sred_reference_block_2d",
     "sred_normalize_image_2d", "sred_debug_gram_rowdot", "sred_block_map_2d_device_noalloc",
     "sred_patch_hu_map_2d", "sred_hu_map_2d", "sred_phase_correlation_map_2d", "sred_global_map_2d_batch",
-    "sred_global_map_2d_shard_sums", "sred_global_map_2d_shard_finish",
+    "sred_global_map_2d_shard_sums", "sred_global_map_2d_shard_finish", "sred_set_log_callback",
 ]
 
 
@@ -54,6 +54,7 @@ class SredError(RuntimeError):
 
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+LOG_CB = C.CFUNCTYPE(None, C.c_char_p, C.c_void_p)
 _fp = C.POINTER(C.c_float)
 _vp = C.c_void_p
 _lib = None
@@ -79,6 +80,7 @@ def load() -> C.CDLL:
         L.sred_create.argtypes = [s, C.POINTER(_vp)]
         L.sred_destroy.argtypes = [_vp]
         L.sred_set_engine.argtypes = [_vp, s]
+        L.sred_set_log_callback.argtypes = [_vp, LOG_CB, _vp]
         L.sred_block_size.argtypes = [s, s]
         L.sred_local_statistics_2d.argtypes = [_vp, _f32p, s, s, s, s, _f32p, _f32p]
         L.sred_mean_noise_var_2d.argtypes = [_vp, _f32p, s, s, _fp]
@@ -131,6 +133,11 @@ class Context:
         e = {"tc": ENGINE_TC, "fp32": ENGINE_FP32}[engine]
         self.check(self._L.sred_set_engine(self.h, e), "sred_set_engine")
         self.engine = engine
+
+    def set_log_callback(self, fn) -> None:
+        """fn(message: str) receives the context's messages; None turns logging off."""
+        self._log_cb = LOG_CB(lambda msg, user: fn(msg.decode())) if fn else LOG_CB()
+        self.check(self._L.sred_set_log_callback(self.h, self._log_cb, None), "sred_set_log_callback")
 
     def check(self, st: int, what: str) -> None:
         if st != OK:

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -55,6 +56,8 @@ struct sred_ctx {
   std::recursive_mutex mu;
   std::vector<sred_ctx*> workers;  // extra contexts of sred_global_map_2d_batch (own streams and workspaces)
   GState shard;                    // the map prepared by sred_global_map_2d_shard_sums
+  void (*log_cb)(const char*, void*) = nullptr;
+  void* log_user = nullptr;
 };
 
 namespace {
@@ -66,8 +69,15 @@ bool fault(const char* what) {
   return f && std::strcmp(f, what) == 0;
 }
 
+void log_msg(sred_ctx* c, const std::string& msg) {
+  if (c && c->log_cb) c->log_cb(msg.c_str(), c->log_user);
+}
+
 sred_status fail(sred_ctx* c, sred_status s, const std::string& msg) {
-  if (c) c->err = msg;
+  if (c) {
+    c->err = msg;
+    log_msg(c, std::string("error: ") + msg);
+  }
   return s;
 }
 
@@ -401,6 +411,15 @@ sred_status global_finish(sred_ctx* c, const GState& gs, cudaStream_t st, int no
     info->launches = (gs.given ? 0 : 2) + 4 + (gs.n_g > 0 ? (gs.engine == SRED_ENGINE_TC ? 3 : 2) : 0) + 1 +
                      (normalize ? 2 : 0);
   }
+  if (c->log_cb) {
+    float t03 = 0;
+    cudaEventElapsedTime(&t03, c->ev[0], c->ev[3]);
+    char line[256];
+    std::snprintf(line, sizeof(line), "global map %dx%d K=%d: %d relevant blocks (%d flat), %s engine, %.3f ms",
+                  gs.w, gs.h, gs.K, gs.n_g + gs.n_flat, gs.n_flat,
+                  gs.engine == SRED_ENGINE_TC ? "tensor-core" : "fp32", t03);
+    log_msg(c, line);
+  }
   return SRED_OK;
 }
 
@@ -583,6 +602,14 @@ sred_status sred_destroy(sred_ctx* c) {
   for (auto& e : c->ev) cudaEventDestroy(e);
   cudaStreamDestroy(c->stream);
   delete c;
+  return SRED_OK;
+}
+
+sred_status sred_set_log_callback(sred_ctx* c, void (*cb)(const char* message, void* user), void* user) {
+  if (!c) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  c->log_cb = cb;
+  c->log_user = user;
   return SRED_OK;
 }
 

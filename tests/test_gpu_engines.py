@@ -129,3 +129,20 @@ def test_sharded_map_equals_full_map(ctx):
                                                 None, None)
     assert st == _lib.ERR_ARG
     ctx.set_engine("fp32")
+
+
+def test_log_callback(ctx):
+    """Messages reach the callback: one line per global map, and errors."""
+    from sred_b200 import clutils, synth
+    got = []
+    ctx.set_log_callback(got.append)
+    img = synth.normalize_input(synth.spot_image(64, 48, 4, seed=3))
+    clutils.global_map_host("Pearson's R", img, 5, 5, 1.0, ctx=ctx)
+    assert any(m.startswith("global map 64x48 K=13") for m in got), got
+    with pytest.raises(_lib.SredError):
+        clutils.global_map_host("no such metric", img, 5, 5, 1.0, ctx=ctx)
+    assert any(m.startswith("error: unknown global metric") for m in got), got
+    ctx.set_log_callback(None)
+    n = len(got)
+    clutils.global_map_host("Pearson's R", img, 5, 5, 1.0, ctx=ctx)
+    assert len(got) == n
