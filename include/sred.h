@@ -195,6 +195,31 @@ sred_status sred_block_map_2d_device(sred_ctx *ctx, const char *metric, const fl
 sred_status sred_reference_block_2d(const float *block_img, int bw, int bh, float *pixels,
                                     int *block_size, float *mean, float *std);
 
+/* Variance stabilisation of the input image (the default "stabiliseNoiseVariance"
+ * step of java/Utils.java:674-684, Simplex method).
+ *
+ * Replaces VarianceStabilisingTransform2D_.getGAT
+ * (java/VarianceStabilisingTransform2D_.java:136-151), in place on host memory:
+ * v = (2 / gain) sqrt(gain v + c), c = 3/8 gain^2 + sigma^2 - gain offset, 0
+ * where gain v + c < 0; double arithmetic, float result. */
+sred_status sred_gat_2d(sred_ctx *ctx, float *img, int w, int h, double gain, double sigma, double offset);
+
+/* The objective of GATMinimizer2D.userFunction (java/GATMinimizer2D.java): the
+ * image transformed as its applyGAT does, cut into width/6 x height/6-pixel
+ * blocks, sum over blocks of (block variance - 1)^2 / blocks. w, h >= 12. */
+sred_status sred_gat_objective_2d(sred_ctx *ctx, const float *img, int w, int h, double gain, double sigma,
+                                  double offset, double *error);
+
+/* Replaces GATMinimizer2D.run: minimises that objective over (gain, sigma,
+ * offset) from the values passed in (the reference starts at 1, 10, 100 with
+ * steps 1, 10, 100 and 5000 iterations), with a Nelder-Mead simplex of this
+ * library (the reference uses ImageJ's Minimizer, which is not part of SReD,
+ * so the fitted values agree with the reference's only as minimisers of the
+ * same objective). On return the three values are the fit; error (nullable)
+ * receives its objective. */
+sred_status sred_gat_fit_2d(sred_ctx *ctx, const float *img, int w, int h, int max_iter, double *gain,
+                            double *sigma, double *offset, double *error);
+
 /* Replaces Utils.normalizeImage2D (java/Utils.java:985-1031) on host memory.
  * mask may be NULL. SRED_ERR_ARG for a non-binary mask. */
 sred_status sred_normalize_image_2d(float *img, int w, int h, int border_w, int border_h,

@@ -79,6 +79,9 @@ def lib() -> C.CDLL:
         L.orc_block_kernel_f64.argtypes = [C.c_int, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, _f32p,
                                            _f32p, C.c_int, C.c_float, C.c_float, _f64p]
         L.orc_java_random_floats.argtypes = [C.c_int64, C.c_int, _f32p]
+        L.orc_gat.argtypes = [_f32p, C.c_int, C.c_double, C.c_double, C.c_double]
+        L.orc_gat_objective.restype = C.c_double
+        L.orc_gat_objective.argtypes = [_f32p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
         L.orc_patch_hu1_ref.restype = C.c_double
         L.orc_patch_hu1_ref.argtypes = [_f32p, C.c_int, C.c_int]
         L.orc_patch_hu.argtypes = [_f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f32p]
@@ -426,3 +429,20 @@ def block_phase_raw(img, ref_pixels, bw, bh, ref_std, means=None, stds=None):
                              C.c_float(ref_std), out):
         raise ValueError("phase correlation supports blocks up to 15x15")
     return out.reshape(H, W)
+
+
+# --------------------------------------------------------------------------
+# Variance stabilisation (java/VarianceStabilisingTransform2D_.java,
+# java/GATMinimizer2D.java)
+# --------------------------------------------------------------------------
+
+def gat(img, gain, sigma, offset) -> np.ndarray:
+    a = _f32(img).copy()
+    lib().orc_gat(a.ravel(), a.size, float(gain), float(sigma), float(offset))
+    return a
+
+
+def gat_objective(img, gain, sigma, offset) -> float:
+    a = _f32(img)
+    H, W = a.shape
+    return float(lib().orc_gat_objective(a.ravel(), W, H, float(gain), float(sigma), float(offset)))

@@ -989,3 +989,55 @@ int orc_block_phase(const float *img, const float *means, const float *stds, int
     free(tc); free(ts);
     return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* Variance stabilisation (generalised Anscombe transform)             */
+/* ------------------------------------------------------------------ */
+
+/* java/VarianceStabilisingTransform2D_.java:136-151 (getGAT), in place. */
+void orc_gat(float *img, int n, double gain, double sigma, double offset) {
+    double refConstant = (3.0 / 8.0) * gain * gain + sigma * sigma - gain * offset;
+    for (int i = 0; i < n; i++) {
+        double v = (double)img[i];
+        if ((gain * v + refConstant) < 0.0) v = 0.0;
+        else v = (2.0 / gain) * sqrt(gain * v + refConstant);
+        img[i] = (float)v;
+    }
+}
+
+/* java/GATMinimizer2D.java userFunction with applyGAT and getMeanAndVarBlock:
+ * width/6 x height/6 blocks, sum of (variance - 1)^2 / blocks. Returns -1 when
+ * the grid has fewer than 2 blocks a side. */
+double orc_gat_objective(const float *pixels, int width, int height, double gain, double sigma, double offset) {
+    double refConstant = (3.0 / 8.0) * gain * gain + sigma * sigma - gain * offset;
+    int blockWidth = width / 6, blockHeight = height / 6;
+    if (blockWidth < 1 || blockHeight < 1) return -1.0;
+    int nBlocksX = width / blockWidth, nBlocksY = height / blockHeight;
+    if (nBlocksX < 2 || nBlocksY < 2) return -1.0;
+    float *g = (float *)malloc(sizeof(float) * (size_t)width * height);
+    for (int n = 0; n < width * height; n++) {
+        double v = pixels[n];
+        if (v <= -refConstant / gain) v = 0;
+        else v = (2 / gain) * sqrt(gain * v + refConstant);
+        g[n] = (float)v;
+    }
+    int nBlocks = nBlocksX * nBlocksY;
+    double error = 0;
+    for (int bY = 0; bY < nBlocksY; bY++)
+        for (int bX = 0; bX < nBlocksX; bX++) {
+            double mean = 0, sq_sum = 0;
+            int bWH = blockWidth * blockHeight;
+            for (int j = bY * blockHeight; j < (bY + 1) * blockHeight; j++)
+                for (int i = bX * blockWidth; i < (bX + 1) * blockWidth; i++) {
+                    float v = g[j * width + i];
+                    mean += v;
+                    sq_sum += v * v;
+                }
+            mean = mean / bWH;
+            double var = sq_sum / bWH - mean * mean;
+            double delta = var - 1;
+            error += (delta * delta) / (double)nBlocks;
+        }
+    free(g);
+    return error;
+}

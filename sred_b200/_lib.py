@@ -26,6 +26,7 @@ EXPORTS = [
     "sred_normalize_image_2d", "sred_debug_gram_rowdot", "sred_block_map_2d_device_noalloc",
     "sred_patch_hu_map_2d", "sred_hu_map_2d", "sred_phase_correlation_map_2d", "sred_global_map_2d_batch",
     "sred_global_map_2d_shard_sums", "sred_global_map_2d_shard_finish", "sred_set_log_callback",
+    "sred_gat_2d", "sred_gat_objective_2d", "sred_gat_fit_2d",
 ]
 
 
@@ -81,6 +82,10 @@ def load() -> C.CDLL:
         L.sred_destroy.argtypes = [_vp]
         L.sred_set_engine.argtypes = [_vp, s]
         L.sred_set_log_callback.argtypes = [_vp, LOG_CB, _vp]
+        _dp = C.POINTER(C.c_double)
+        L.sred_gat_2d.argtypes = [_vp, _f32p, s, s, C.c_double, C.c_double, C.c_double]
+        L.sred_gat_objective_2d.argtypes = [_vp, _f32p, s, s, C.c_double, C.c_double, C.c_double, _dp]
+        L.sred_gat_fit_2d.argtypes = [_vp, _f32p, s, s, s, _dp, _dp, _dp, _dp]
         L.sred_block_size.argtypes = [s, s]
         L.sred_local_statistics_2d.argtypes = [_vp, _f32p, s, s, s, s, _f32p, _f32p]
         L.sred_mean_noise_var_2d.argtypes = [_vp, _f32p, s, s, _fp]

@@ -1,0 +1,94 @@
+// Generalised Anscombe transform (variance stabilisation of the input image)
+// and the fit of its parameters.
+//
+// java/VarianceStabilisingTransform2D_.java:136-151 (getGAT) transforms the
+// image; java/GATMinimizer2D.java (userFunction, applyGAT, getMeanAndVarBlock)
+// defines the objective its Simplex option minimises: the transformed image
+// cut into a 6 x 6 grid of blocks, sum over blocks of (variance - 1)^2 /
+// blocks. Both are double-precision code in the reference; this file is
+// compiled with -fmad=false so that no multiply-add is fused where Java
+// rounds twice.
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace sred {
+
+// getGAT: v < 0 under the root -> 0, else (2 / gain) sqrt(gain v + c), in
+// double, stored as float; c = (3/8) gain^2 + sigma^2 - gain offset.
+__global__ void k_gat(float* __restrict__ img, size_t n, double gain, double c) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double v = (double)img[i];
+    if ((gain * v + c) < 0.0) {
+      v = 0.0;
+    } else {
+      v = (2.0 / gain) * sqrt(gain * v + c);
+    }
+    img[i] = (float)v;
+  }
+}
+
+// One block of the objective (GATMinimizer2D.userFunction): the pixels
+// transformed as applyGAT does (v <= -c / gain -> 0), stored as float, then
+// sum v and sum v*v (the product in float, as Java multiplies two floats) in
+// double. One CTA per block; out[2 b] = sum, out[2 b + 1] = sum of squares.
+__global__ void __launch_bounds__(256)
+    k_gat_block_moments(const float* __restrict__ img, int W, int bw, int bh, int nbx, double gain, double c,
+                        double* __restrict__ out) {
+  __shared__ double s1[256], s2[256];
+  const int b = blockIdx.x, bx = b % nbx, by = b / nbx;
+  const int x0 = bx * bw, y0 = by * bh;
+  const double lim = -c / gain, scale = 2.0 / gain;
+  double a1 = 0.0, a2 = 0.0;
+  for (int t = threadIdx.x; t < bw * bh; t += blockDim.x) {
+    const int x = x0 + t % bw, y = y0 + t / bw;
+    double v = (double)img[(size_t)y * W + x];
+    v = (v <= lim) ? 0.0 : scale * sqrt(gain * v + c);
+    const float f = (float)v;
+    a1 += (double)f;
+    a2 += (double)(f * f);
+  }
+  s1[threadIdx.x] = a1;
+  s2[threadIdx.x] = a2;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      s1[threadIdx.x] += s1[threadIdx.x + s];
+      s2[threadIdx.x] += s2[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[2 * b] = s1[0];
+    out[2 * b + 1] = s2[0];
+  }
+}
+
+// Block grid of the objective: width / 6 by height / 6 pixels
+// (java/GATMinimizer2D.java userFunction). Returns false when the grid has
+// fewer than 2 blocks a side (the reference then loops forever).
+bool gat_grid(int w, int h, int* bw, int* bh, int* nbx, int* nby) {
+  *bw = w / 6;
+  *bh = h / 6;
+  if (*bw < 1 || *bh < 1) return false;
+  *nbx = w / *bw;
+  *nby = h / *bh;
+  return *nbx >= 2 && *nby >= 2;
+}
+
+// The objective from the per-block sums, in the reference's order.
+double gat_error(const double* sums, int nblocks, int bw, int bh) {
+  double error = 0.0;
+  const int bwh = bw * bh;
+  for (int b = 0; b < nblocks; b++) {
+    double mean = sums[2 * b] / bwh;
+    const double var = sums[2 * b + 1] / bwh - mean * mean;
+    const double delta = var - 1;
+    error += (delta * delta) / (double)nblocks;
+  }
+  return error;
+}
+
+}  // namespace sred

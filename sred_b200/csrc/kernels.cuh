@@ -44,6 +44,13 @@ __global__ void k_interior_mask(float* mask, int W, int H, int rw, int rh, size_
 __global__ void k_apply_mask(float* a, const float* mask, size_t n);
 __global__ void k_invert_masked(float* a, const float* mask, int W, int H, int rw, int rh, size_t plane);
 
+// gat.cu
+__global__ void k_gat(float* img, size_t n, double gain, double c);
+__global__ void k_gat_block_moments(const float* img, int W, int bw, int bh, int nbx, double gain, double c,
+                                    double* out);
+bool gat_grid(int w, int h, int* bw, int* bh, int* nbx, int* nby);
+double gat_error(const double* sums, int nblocks, int bw, int bh);
+
 // shape.cu (k_block_phase is declared in shape.cuh, next to PhaseRef)
 __global__ void k_patch_hu(const float* img, int W, int H, Ellipse e, int patch_size, double ref_hu1, float* out,
                            float* stds_out);

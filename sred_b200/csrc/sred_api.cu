@@ -23,7 +23,7 @@ namespace {
 enum BufId {
   B_IMG, B_MEANS, B_STDS, B_MASK, B_MASKIN, B_FLAGS, B_SLOT, B_GPIX, B_FPIX, B_COUNTS, B_U, B_A, B_B,
   B_PARAMS, B_RMAX, B_NUM, B_DEN, B_SUMS, B_OUT, B_VARS, B_MM, B_NMASK, B_BAD, B_STATUS, B_STDS2, B_COLSOA,
-  B_FEAT, B_SIG, B_FR, B_FI, B_NBUF
+  B_FEAT, B_SIG, B_FR, B_FI, B_GAT, B_NBUF
 };
 
 struct DevBuf {
@@ -1090,6 +1090,148 @@ sred_status sred_phase_correlation_map_2d(sred_ctx* c, const float* img, const f
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  return SRED_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Variance stabilisation (generalised Anscombe transform)
+// ---------------------------------------------------------------------------
+
+namespace {
+
+// The objective of GATMinimizer2D for one parameter set, the image already on
+// the device.
+sred_status gat_objective_dev(sred_ctx* c, const float* d_img, int w, int h, double gain, double sigma,
+                              double offset, double* error) {
+  int bw, bh, nbx, nby;
+  if (!gat_grid(w, h, &bw, &bh, &nbx, &nby)) return fail(c, SRED_ERR_ARG, "image too small for the GAT fit (width and height >= 12)");
+  const int nb = nbx * nby;
+  double* d_sums;
+  CKS(ensure(c, B_GAT, 2 * (size_t)nb, &d_sums));
+  const double cst = (3.0 / 8.0) * gain * gain + sigma * sigma - gain * offset;
+  k_gat_block_moments<<<nb, 256, 0, c->stream>>>(d_img, w, bw, bh, nbx, gain, cst, d_sums);
+  CK(cudaGetLastError());
+  std::vector<double> sums(2 * (size_t)nb);
+  CK(cudaMemcpyAsync(sums.data(), d_sums, sums.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *error = gat_error(sums.data(), nb, bw, bh);
+  return SRED_OK;
+}
+
+}  // namespace
+
+sred_status sred_gat_2d(sred_ctx* c, float* img, int w, int h, double gain, double sigma, double offset) {
+  if (!c || !img || w <= 0 || h <= 0 || !(gain != 0.0)) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->shard.valid = false;
+  const size_t n = (size_t)w * h;
+  float* d;
+  CKS(ensure(c, B_IMG, n, &d));
+  CK(cudaMemcpyAsync(d, img, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  const double cst = (3.0 / 8.0) * gain * gain + sigma * sigma - gain * offset;
+  k_gat<<<grid_for(n, 256, 8 * c->num_sms), 256, 0, c->stream>>>(d, n, gain, cst);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(img, d, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SRED_OK;
+}
+
+sred_status sred_gat_objective_2d(sred_ctx* c, const float* img, int w, int h, double gain, double sigma,
+                                  double offset, double* error) {
+  if (!c || !img || !error || w <= 0 || h <= 0) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->shard.valid = false;
+  const size_t n = (size_t)w * h;
+  float* d;
+  CKS(ensure(c, B_IMG, n, &d));
+  CK(cudaMemcpyAsync(d, img, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  return gat_objective_dev(c, d, w, h, gain, sigma, offset, error);
+}
+
+// Nelder-Mead downhill simplex (Nelder & Mead, Computer Journal 7:308, 1965;
+// reflection 1, expansion 2, contraction 1/2, shrink 1/2) over (gain, sigma,
+// offset), started from the given values with the initial steps of
+// GATMinimizer2D.run (1, 10, 100). The objective is evaluated on the GPU with
+// the image resident. Stops after max_iter evaluations or when the simplex's
+// objective values agree to 1e-15 of the best.
+sred_status sred_gat_fit_2d(sred_ctx* c, const float* img, int w, int h, int max_iter, double* gain, double* sigma,
+                            double* offset, double* error_out) {
+  if (!c || !img || !gain || !sigma || !offset || w <= 0 || h <= 0 || max_iter < 1) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->shard.valid = false;
+  const size_t n = (size_t)w * h;
+  float* d;
+  CKS(ensure(c, B_IMG, n, &d));
+  CK(cudaMemcpyAsync(d, img, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  double x[4][3];
+  double f[4];
+  const double step[3] = {1.0, 10.0, 100.0};
+  int evals = 0;
+  auto eval = [&](const double* p, double* out) -> sred_status {
+    evals++;
+    return gat_objective_dev(c, d, w, h, p[0], p[1], p[2], out);
+  };
+  for (int v = 0; v < 4; v++) {
+    x[v][0] = *gain;
+    x[v][1] = *sigma;
+    x[v][2] = *offset;
+    if (v > 0) x[v][v - 1] += step[v - 1];
+    CKS(eval(x[v], &f[v]));
+  }
+  while (evals < max_iter) {
+    int order[4] = {0, 1, 2, 3};
+    std::sort(order, order + 4, [&](int a, int b) { return f[a] < f[b]; });
+    const int best = order[0], worst = order[3], second = order[2];
+    if (std::fabs(f[worst] - f[best]) <= 1e-15 * std::fabs(f[best])) break;
+    double cen[3] = {0, 0, 0};
+    for (int v = 0; v < 4; v++)
+      if (v != worst)
+        for (int k = 0; k < 3; k++) cen[k] += x[v][k] / 3.0;
+    double xr[3], fr;
+    for (int k = 0; k < 3; k++) xr[k] = cen[k] + (cen[k] - x[worst][k]);
+    CKS(eval(xr, &fr));
+    if (fr < f[best]) {
+      double xe[3], fe;
+      for (int k = 0; k < 3; k++) xe[k] = cen[k] + 2.0 * (cen[k] - x[worst][k]);
+      CKS(eval(xe, &fe));
+      if (fe < fr) {
+        std::copy(xe, xe + 3, x[worst]);
+        f[worst] = fe;
+      } else {
+        std::copy(xr, xr + 3, x[worst]);
+        f[worst] = fr;
+      }
+    } else if (fr < f[second]) {
+      std::copy(xr, xr + 3, x[worst]);
+      f[worst] = fr;
+    } else {
+      double xc[3], fc;
+      const bool outside = fr < f[worst];
+      for (int k = 0; k < 3; k++)
+        xc[k] = outside ? cen[k] + 0.5 * (xr[k] - cen[k]) : cen[k] + 0.5 * (x[worst][k] - cen[k]);
+      CKS(eval(xc, &fc));
+      if (fc < (outside ? fr : f[worst])) {
+        std::copy(xc, xc + 3, x[worst]);
+        f[worst] = fc;
+      } else {
+        for (int v = 0; v < 4; v++)
+          if (v != best) {
+            for (int k = 0; k < 3; k++) x[v][k] = x[best][k] + 0.5 * (x[v][k] - x[best][k]);
+            CKS(eval(x[v], &f[v]));
+          }
+      }
+    }
+  }
+  int best = 0;
+  for (int v = 1; v < 4; v++)
+    if (f[v] < f[best]) best = v;
+  *gain = x[best][0];
+  *sigma = x[best][1];
+  *offset = x[best][2];
+  if (error_out) *error_out = f[best];
   return SRED_OK;
 }
 

@@ -58,12 +58,54 @@ def _ctx(ctx):
     return ctx if ctx is not None else _lib.default_context()
 
 
-def get_input_image_2d(image: np.ndarray, normalize_output: bool = True) -> InputImage2D:
-    """java/Utils.java:653-725 for an image given as an array (variance
-    stabilisation is outside this path): float conversion and min-max to
-    [0, 1] with epsilon, in FP32."""
+def get_gat_2d(image: np.ndarray, gain: float, sigma: float, offset: float, ctx=None) -> np.ndarray:
+    """VarianceStabilisingTransform2D_.getGAT
+    (java/VarianceStabilisingTransform2D_.java:136-151) on the GPU."""
+    c = _ctx(ctx)
+    a = np.ascontiguousarray(image, dtype=np.float32).copy()
+    h, w = a.shape
+    c.check(c._L.sred_gat_2d(c.h, a, w, h, float(gain), float(sigma), float(offset)), "sred_gat_2d")
+    return a
+
+
+def gat_objective_2d(image: np.ndarray, gain: float, sigma: float, offset: float, ctx=None) -> float:
+    """GATMinimizer2D.userFunction (java/GATMinimizer2D.java) on the GPU."""
+    c = _ctx(ctx)
     a = np.ascontiguousarray(image, dtype=np.float32)
     h, w = a.shape
+    e = C.c_double()
+    c.check(c._L.sred_gat_objective_2d(c.h, a, w, h, float(gain), float(sigma), float(offset), C.byref(e)),
+            "sred_gat_objective_2d")
+    return e.value
+
+
+def fit_gat_2d(image: np.ndarray, max_iter: int = 5000, gain: float = 1.0, sigma: float = 10.0,
+               offset: float = 100.0, ctx=None) -> tuple:
+    """GATMinimizer2D.run: (gain, sigma, offset, objective) minimising the
+    objective from the reference's starting point (java/Utils.java:676)."""
+    c = _ctx(ctx)
+    a = np.ascontiguousarray(image, dtype=np.float32)
+    h, w = a.shape
+    g, s, o, e = C.c_double(gain), C.c_double(sigma), C.c_double(offset), C.c_double()
+    c.check(c._L.sred_gat_fit_2d(c.h, a, w, h, int(max_iter), C.byref(g), C.byref(s), C.byref(o), C.byref(e)),
+            "sred_gat_fit_2d")
+    return g.value, s.value, o.value, e.value
+
+
+def get_input_image_2d(image: np.ndarray, normalize_output: bool = True, stabilise_noise_variance: bool = False,
+                       gat_method: str = "Simplex", max_iter: int = 5000, ctx=None) -> InputImage2D:
+    """java/Utils.java:653-725 for an image given as an array: float
+    conversion, optional variance stabilisation (the Simplex method: the GAT
+    parameters fitted on the GPU, then the transform), and min-max to [0, 1]
+    with epsilon, in FP32. The reference's other method ("Quad/Octree") is
+    not provided."""
+    a = np.ascontiguousarray(image, dtype=np.float32)
+    h, w = a.shape
+    if stabilise_noise_variance:
+        if gat_method != "Simplex":
+            raise ValueError(f"unsupported GAT method {gat_method!r} (only 'Simplex')")
+        gain, sigma, offset, _ = fit_gat_2d(a, max_iter, ctx=ctx)
+        a = get_gat_2d(a, np.float32(gain), np.float32(sigma), np.float32(offset), ctx=ctx)
     if normalize_output:
         mn, mx = np.float32(a.min()), np.float32(a.max())
         a = ((a - mn) / (mx - mn + EPSILON)).astype(np.float32)

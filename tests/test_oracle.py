@@ -238,3 +238,48 @@ def test_block_phase_self_peak():
     assert px.size == K
     out = oracle.block_phase_raw(img, px, bw, bh, stds[y, x], means, stds)
     assert abs(out[y, x] - np.sqrt(2.0)) < 1e-6
+
+
+# ---------------------------------------------------------------------------
+# Variance stabilisation: the restatement against an independent numpy
+# evaluation of java/VarianceStabilisingTransform2D_.java:136-151 and
+# java/GATMinimizer2D.java (no reference test pins either)
+# ---------------------------------------------------------------------------
+
+def _poisson_gaussian(w, h, gain, sigma, offset, seed):
+    """Poisson-Gaussian noise on an intensity that is constant over each cell
+    of the objective's 6 x 6 block grid (20 to 500 photons per cell)."""
+    rng = np.random.default_rng(seed)
+    cells = rng.uniform(20, 500, (6, 6))
+    lam = np.kron(cells, np.ones((h // 6, w // 6)))
+    lam = np.pad(lam, ((0, h - lam.shape[0]), (0, w - lam.shape[1])), mode="edge")
+    return (gain * rng.poisson(lam) + offset + rng.normal(0, sigma, (h, w))).astype(np.float32)
+
+
+def test_gat_matches_numpy():
+    img = _poisson_gaussian(60, 48, 2.0, 5.0, 100.0, 1)
+    img[0, :5] = [-1e6, -50.0, 0.0, 1.0, 3.0]
+    for g, s, o in [(2.0, 5.0, 100.0), (1.0, 10.0, 100.0), (0.5, 30.0, -20.0)]:
+        c = 3.0 / 8.0 * g * g + s * s - g * o
+        v = img.astype(np.float64)
+        exp = np.where(g * v + c < 0, 0.0, (2.0 / g) * np.sqrt(np.maximum(g * v + c, 0))).astype(np.float32)
+        assert np.array_equal(oracle.gat(img, g, s, o), exp)
+
+
+def test_gat_objective_matches_numpy():
+    img = _poisson_gaussian(66, 54, 2.0, 5.0, 100.0, 2)
+    for g, s, o in [(2.0, 5.0, 100.0), (1.0, 10.0, 100.0)]:
+        c = 3.0 / 8.0 * g * g + s * s - g * o
+        v = img.astype(np.float64)
+        t = np.where(v <= -c / g, 0.0, (2 / g) * np.sqrt(np.maximum(g * v + c, 0))).astype(np.float32)
+        bw, bh = 66 // 6, 54 // 6
+        err = 0.0
+        for by in range(54 // bh):
+            for bx in range(66 // bw):
+                blk = t[by * bh:(by + 1) * bh, bx * bw:(bx + 1) * bw].astype(np.float64)
+                sq = (t[by * bh:(by + 1) * bh, bx * bw:(bx + 1) * bw] ** 2).astype(np.float64)
+                var = sq.sum() / blk.size - (blk.sum() / blk.size) ** 2
+                err += (var - 1) ** 2 / 36
+        assert abs(oracle.gat_objective(img, g, s, o) - err) <= 1e-9 * max(err, 1e-12)
+    # the true parameters stabilise the variance much better than the reference's starting point
+    assert oracle.gat_objective(img, 2.0, 5.0, 100.0) < 0.1 * oracle.gat_objective(img, 1.0, 10.0, 100.0)
