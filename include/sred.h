@@ -287,6 +287,61 @@ sred_status sred_block_map_2d_device_noalloc(const char *metric, const float *d_
 sred_status sred_debug_gram_rowdot(sred_ctx *ctx, int engine, const float *u, const float *w1,
                                    const float *w2, int n, int k, double *num, double *den);
 
+/* ---------------------------------------------------------------------
+ * 3D block repetition maps. Volumes are w x h x d floats, x fastest then y
+ * then z (the reference's flattened ImageStack, index w*h*z + y*w + x); the
+ * block is the ellipsoid inscribed in an odd bw x bh x bd box (each >= 3).
+ * --------------------------------------------------------------------- */
+
+/* Ellipsoid block size K (java/Utils.java:1075-1085, float arithmetic). */
+int sred_block_size_3d(int bw, int bh, int bd);
+
+/* Replaces Utils.getReferenceBlock3D (java/Utils.java:1047-1160) for a block
+ * already converted to float (bd slices of bh x bw): ellipsoid-flatten,
+ * normalizeArray, minus the mean, normalizeArray again; mean and (K-1) std of
+ * the result. pixels must hold sred_block_size_3d(bw, bh, bd) floats. */
+sred_status sred_reference_block_3d(const float *block_vol, int bw, int bh, int bd, float *pixels,
+                                    int *block_size, float *mean, float *std_dev);
+
+/* Replaces CLUtils.getLocalStatistics3D (java/CLUtils.java:1030-1131) and
+ * cl/kernelGetLocalStatistics3D.cl: per-voxel ellipsoid-block mean and (K-1)
+ * standard deviation in FP32, reference evaluation order; border voxels 0. */
+sred_status sred_local_statistics_3d(sred_ctx *ctx, const float *vol, int w, int h, int d, int bw, int bh,
+                                     int bd, float *means, float *stds);
+
+/* Replaces Utils.getRelevanceMask3D (java/Utils.java:1501-1525) with
+ * getMeanNoiseVar3D (java/Utils.java:1463-1498): the noise variance is the
+ * mean local variance over the interior (FP32 raster-order sum, float count);
+ * mask = 1 where the interior voxel's local variance exceeds
+ * noise_var * relevance_constant, else 0. */
+sred_status sred_relevance_mask_3d(sred_ctx *ctx, int w, int h, int d, int bw, int bh, int bd,
+                                   const float *local_stds, float relevance_constant, float *mask,
+                                   float *noise_var);
+
+/* Replaces CLUtils.calculateBlockRepetitionMap3D (java/CLUtils.java:1639-1653)
+ * and the four getBlock*3D methods it dispatches to (:1133-1637) with their
+ * kernels (cl/kernelGetBlock{Pearson,Ssim,Nrmse,AbsDiffStds}3D.cl), for a
+ * volume already prepared by getInputImage3D. metric: "Pearson's R",
+ * "SSIM", "NRMSE (inverted)" or "Abs. Diff. of StdDevs."
+ * (java/BlockRepetition3D_.java:19-24). FP32 in the kernels' order; then, over
+ * the interior, NRMSE inverted (0 -> 1) and Abs-diff as 1 - x, the relevance
+ * mask applied when relevance_constant > 0, and normalizeImage3D over the
+ * interior (over the mask when one is applied). The Pearson command of the
+ * reference passes the block depth as the z radius (java/CLUtils.java:1149,
+ * gathering from a box twice as deep); here every metric uses the block's own
+ * radius, as the other three do. */
+sred_status sred_calculate_block_repetition_map_3d(sred_ctx *ctx, const char *metric, const float *vol, int w,
+                                                   int h, int d, const float *ref_pixels, int block_size, int bw,
+                                                   int bh, int bd, float ref_mean, float ref_std,
+                                                   float relevance_constant, int normalize_output, float *out);
+
+/* Device-resident variant: d_vol and d_out are w*h*d floats on the context's
+ * device; runs on `stream` (NULL = the context's stream). */
+sred_status sred_block_map_3d_device(sred_ctx *ctx, const char *metric, const float *d_vol, int w, int h, int d,
+                                     const float *ref_pixels, int block_size, int bw, int bh, int bd,
+                                     float ref_mean, float ref_std, float relevance_constant,
+                                     int normalize_output, float *d_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

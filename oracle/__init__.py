@@ -80,6 +80,21 @@ def lib() -> C.CDLL:
                                            _f32p, C.c_int, C.c_float, C.c_float, _f64p]
         L.orc_java_random_floats.argtypes = [C.c_int64, C.c_int, _f32p]
         L.orc_gat.argtypes = [_f32p, C.c_int, C.c_double, C.c_double, C.c_double]
+        L.orc_block_size3d.restype = C.c_int
+        L.orc_block_size3d.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.orc_local_stats3d_f32.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f32p,
+                                            _f32p]
+        L.orc_reference_block3d.restype = C.c_int
+        L.orc_reference_block3d.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _f32p, _fp, _fp]
+        L.orc_block3d_kernel_f32.argtypes = [C.c_int, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                             _f32p, _f32p, _f32p, C.c_int, C.c_float, C.c_float, _f32p]
+        L.orc_noise_var3d.restype = C.c_float
+        L.orc_noise_var3d.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f32p]
+        L.orc_relevance_mask3d.restype = C.c_float
+        L.orc_relevance_mask3d.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f32p, C.c_float,
+                                           _f32p]
+        L.orc_block3d_postprocess_f32.argtypes = [C.c_int, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                  C.c_int, _f32p, C.c_float, C.c_int]
         L.orc_gat_objective.restype = C.c_double
         L.orc_gat_objective.argtypes = [_f32p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
         L.orc_patch_hu1_ref.restype = C.c_double
@@ -446,3 +461,84 @@ def gat_objective(img, gain, sigma, offset) -> float:
     a = _f32(img)
     H, W = a.shape
     return float(lib().orc_gat_objective(a.ravel(), W, H, float(gain), float(sigma), float(offset)))
+
+
+# --------------------------------------------------------------------------
+# 3D block repetition maps (cl/kernelGet*3D.cl, java/CLUtils.java:1030-1653)
+# Volumes are float32 [D, H, W].
+# --------------------------------------------------------------------------
+
+BLOCK_METRICS_3D = {"Pearson's R": 0, "SSIM": 1, "NRMSE (inverted)": 2, "Abs. Diff. of StdDevs.": 3}
+
+
+def block_size3d(bw, bh, bd) -> int:
+    return lib().orc_block_size3d(bw, bh, bd)
+
+
+def local_stats3d(vol, bw, bh, bd, use_refshim=False):
+    v = _f32(vol)
+    D, H, W = v.shape
+    m = np.zeros_like(v)
+    s = np.zeros_like(v)
+    if use_refshim:
+        R = refshim()
+        pix = np.arange(v.size, dtype=np.int32)
+        rc = R.rs_kernelGetLocalStatistics3D(C.c_int(block_size3d(bw, bh, bd)), W, H, D, bw, bh, bd,
+                                             C.c_float(EPSILON), C.c_float(0), C.c_float(0),
+                                             pix.ctypes.data_as(C.c_void_p), C.c_int(pix.size),
+                                             v.ctypes.data_as(C.c_void_p), m.ctypes.data_as(C.c_void_p),
+                                             s.ctypes.data_as(C.c_void_p))
+        if rc != 0:
+            raise ValueError("refshim has no instantiation for this block")
+    else:
+        lib().orc_local_stats3d_f32(v.ravel(), W, H, D, bw, bh, bd, m.ravel(), s.ravel())
+    return m, s
+
+
+def reference_block3d(block):
+    b = _f32(block)
+    bd, bh, bw = b.shape
+    px = np.zeros(b.size, np.float32)
+    m, s = C.c_float(), C.c_float()
+    K = lib().orc_reference_block3d(b.ravel(), bw, bh, bd, px, C.byref(m), C.byref(s))
+    return px[:K].copy(), np.float32(m.value), np.float32(s.value)
+
+
+def block_map3d(metric, vol, ref_pixels, bw, bh, bd, ref_mean, ref_std, relevance_constant=0.0, normalize=True,
+                use_refshim=False):
+    """3D block map: the kernel (reference FP32 order) and the host steps."""
+    v = _f32(vol)
+    D, H, W = v.shape
+    means, stds = local_stats3d(v, bw, bh, bd, use_refshim)
+    ref = _f32(ref_pixels)
+    K = ref.size
+    m = BLOCK_METRICS_3D[metric]
+    out = np.zeros(v.size, np.float32)
+    if use_refshim:
+        name = ["kernelGetBlockPearson3D", "kernelGetBlockSsim3D", "kernelGetBlockNrmse3D",
+                "kernelGetBlockAbsDiffStds3D"][m]
+        bufs = {"ref": ref, "img": v, "means": means, "stds": stds, "map": out}
+        args = {0: ["ref", "img", "means", "stds", "map"], 1: ["ref", "img", "means", "stds", "map"],
+                2: ["ref", "img", "means", "map"], 3: ["stds", "map"]}[m]
+        pix = np.arange(v.size, dtype=np.int32)
+        rc = getattr(refshim(), f"rs_{name}")(C.c_int(K), W, H, D, bw, bh, bd, C.c_float(EPSILON),
+                                              C.c_float(ref_std), C.c_float(ref_mean),
+                                              pix.ctypes.data_as(C.c_void_p), C.c_int(pix.size),
+                                              *[bufs[a].ctypes.data_as(C.c_void_p) for a in args])
+        if rc != 0:
+            raise ValueError("refshim has no instantiation for this block")
+    else:
+        lib().orc_block3d_kernel_f32(m, v.ravel(), W, H, D, bw, bh, bd, means.ravel(), stds.ravel(), ref, K,
+                                     C.c_float(ref_mean), C.c_float(ref_std), out)
+    raw = out.copy()
+    lib().orc_block3d_postprocess_f32(m, out, W, H, D, bw // 2, bh // 2, bd // 2, stds.ravel(),
+                                      C.c_float(relevance_constant), int(normalize))
+    return {"map": out.reshape(D, H, W), "raw": raw.reshape(D, H, W), "means": means, "stds": stds}
+
+
+def relevance_mask3d(stds, bw, bh, bd, c):
+    s = _f32(stds)
+    D, H, W = s.shape
+    mask = np.zeros(s.size, np.float32)
+    nv = lib().orc_relevance_mask3d(W, H, D, bw // 2, bh // 2, bd // 2, s.ravel(), C.c_float(c), mask)
+    return mask.reshape(D, H, W), np.float32(nv)

@@ -74,6 +74,79 @@ SHAPE_KERNELS = {
 #   cross_corr_real[j*w+i] reads past the block (:150) -> block width.
 PHASE_REPAIRS = [("(1*i*ii/bW)", "(1.0*i*ii/bW)"), ("(1*j*jj/bH)", "(1.0*j*jj/bH)"),
                  ("cross_corr_real[j*w+i]", "cross_corr_real[j*bW+i]")]
+# 3D kernels (block maps and local statistics): same scheme with a depth.
+KERNELS_3D = {
+    "kernelGetLocalStatistics3D": ["img", "means", "stds"],
+    "kernelGetBlockPearson3D": ["ref", "img", "means", "stds", "map"],
+    "kernelGetBlockSsim3D": ["ref", "img", "means", "stds", "map"],
+    "kernelGetBlockNrmse3D": ["ref", "img", "means", "map"],
+    "kernelGetBlockAbsDiffStds3D": ["stds", "map"],
+}
+PLACEHOLDERS_3D = {"$DEPTH$": "RS_D", "$BZ$": "RS_BZ", "$BRZ$": "RS_BRZ"}
+MACROS_3D = ["image_depth", "bZ", "bRZ", "imageWidth", "imageHeight", "imageDepth"]
+SIZES_3D = [(a, b, c) for a in (3, 5, 7) for b in (3, 5, 7) for c in (3, 5)]
+
+
+def ellipsoid_k(bw: int, bh: int, bd: int) -> int:
+    f = np.float32
+    rw, rh, rd = bw // 2, bh // 2, bd // 2
+    k = 0
+    for z in range(bd):
+        for y in range(bh):
+            for x in range(bw):
+                dx, dy, dz = f(x - rw), f(y - rh), f(z - rd)
+                if (dx * dx) / f(rw * rw) + (dy * dy) / f(rh * rh) + (dz * dz) / f(rd * rd) <= f(1):
+                    k += 1
+    return k
+
+
+def gen_unit_3d(ref: Path, name: str) -> str:
+    args = KERNELS_3D[name]
+    src = (ref / "src/main/resources" / f"{name}.cl").read_text()
+    for tok, repl in {**PLACEHOLDERS, **PLACEHOLDERS_3D}.items():
+        src = replace_first(src, tok, repl)
+    ks = sorted({ellipsoid_k(*s) for s in SIZES_3D})
+    call = ", ".join(f"(float*){a}" for a in args)
+    params = ", ".join(f"const float* {a}" if a in ("img", "means", "stds", "ref") else f"float* {a}"
+                       for a in args)
+    cases = "\n".join(f"    case {k}: rs_loop<{k}>(pix, npix, {', '.join(args)}); break;" for k in ks)
+    undef = "".join(f"#undef {m}\n" for m in MACROS + MACROS_3D)
+    return f"""#include "shim.h"
+#include <cfloat>
+using std::fmax;
+using std::max;
+using std::min;
+namespace rsns_{name} {{
+#define kernel template <int RS_KT> static inline
+{src}
+{undef}
+template <int KT>
+static void rs_loop(const int* pix, int npix, {params}) {{
+  #pragma omp parallel for schedule(dynamic, 16)
+  for (int i = 0; i < npix; i++) {{
+    rs_gid[0] = pix[i] % RS_W;
+    rs_gid[1] = (pix[i] / RS_W) % RS_H;
+    rs_gid[2] = pix[i] / (RS_W * RS_H);
+    {name}<KT>({call});
+  }}
+}}
+}}  // namespace rsns_{name}
+
+extern "C" int rs_{name}(int K, int W, int H, int D, int bw, int bh, int bd, float eps, float block_std,
+                       float block_mean, const int* pix, int npix, {params}) {{
+  using namespace rsns_{name};
+  RS_W = W; RS_H = H; RS_D = D; RS_BW = bw; RS_BH = bh; RS_BZ = bd;
+  RS_BRW = bw / 2; RS_BRH = bh / 2; RS_BRZ = bd / 2;
+  RS_EPSILON = eps; RS_BLOCK_STD = block_std; RS_BLOCK_MEAN = block_mean;
+  switch (K) {{
+{cases}
+    default: return -1;
+  }}
+  return 0;
+}}
+"""
+
+
 SHAPE_SIZES = sorted({(a, b) for a in (3, 5, 7, 9) for b in (3, 5, 7, 9)} | {(11, 11), (13, 13), (15, 15)})
 
 
@@ -214,6 +287,7 @@ def build_refshim(ref: Path, force: bool = False) -> Path | None:
     ks = k_list()
     units = {n: gen_unit(ref, n, ks) for n in KERNELS}
     units.update({n: gen_shape_unit(ref, n) for n in SHAPE_KERNELS})
+    units.update({n: gen_unit_3d(ref, n) for n in KERNELS_3D})
     digest = hashlib.sha256(("".join(units.values()) + (HERE / "shim.h").read_text()
                              + (HERE / "shim_shape.h").read_text()).encode()).hexdigest()
     stamp = REF_OUT / "build.sha256"

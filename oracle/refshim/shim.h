@@ -33,8 +33,8 @@ using std::sqrt;
 #define __local
 #define local
 
-static int RS_W, RS_H, RS_BW, RS_BH, RS_BRW, RS_BRH;
+static int RS_W, RS_H, RS_BW, RS_BH, RS_BRW, RS_BRH, RS_D, RS_BZ, RS_BRZ;
 static float RS_FILTER, RS_THRESHOLD, RS_EPSILON, RS_BLOCK_STD, RS_BLOCK_MEAN;
-static thread_local int rs_gid[2];
+static thread_local int rs_gid[3];
 
 static inline int get_global_id(int d) { return rs_gid[d]; }

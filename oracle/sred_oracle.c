@@ -1041,3 +1041,240 @@ double orc_gat_objective(const float *pixels, int width, int height, double gain
     free(g);
     return error;
 }
+
+/* ------------------------------------------------------------------ */
+/* 3D block repetition maps                                            */
+/* ------------------------------------------------------------------ */
+
+/* Inscribed-ellipsoid test of the 3D code (java/Utils.java:1075-1085,
+ * cl/kernelGetLocalStatistics3D.cl:35-38), float arithmetic, same order. */
+static int in_ellipsoid(int dx, int dy, int dz, int rw, int rh, int rd) {
+    float fx = (float)dx, fy = (float)dy, fz = (float)dz;
+    return ((fx * fx) / (float)(rw * rw)) + ((fy * fy) / (float)(rh * rh)) + ((fz * fz) / (float)(rd * rd)) <= 1.0f;
+}
+
+int orc_block_size3d(int bw, int bh, int bd) {
+    int rw = bw / 2, rh = bh / 2, rd = bd / 2, k = 0;
+    for (int z = -rd; z <= rd; z++)
+        for (int y = -rh; y <= rh; y++)
+            for (int x = -rw; x <= rw; x++) k += in_ellipsoid(x, y, z, rw, rh, rd);
+    return k;
+}
+
+/* Linear offsets of the ellipsoid in raster order (z, y, x). */
+static int ellipsoid_offsets(int bw, int bh, int bd, int W, int H, long *off) {
+    int rw = bw / 2, rh = bh / 2, rd = bd / 2, k = 0;
+    for (int z = -rd; z <= rd; z++)
+        for (int y = -rh; y <= rh; y++)
+            for (int x = -rw; x <= rw; x++)
+                if (in_ellipsoid(x, y, z, rw, rh, rd)) off[k++] = (long)z * W * H + (long)y * W + x;
+    return k;
+}
+
+static int interior3d(int x, int y, int z, int W, int H, int D, int rw, int rh, int rd) {
+    return x >= rw && x < W - rw && y >= rh && y < H - rh && z >= rd && z < D - rd;
+}
+
+/* cl/kernelGetLocalStatistics3D.cl:11-61 for every voxel. */
+void orc_local_stats3d_f32(const float *img, int W, int H, int D, int bw, int bh, int bd, float *means,
+                           float *stds) {
+    const int rw = bw / 2, rh = bh / 2, rd = bd / 2;
+    long off[4096];
+    const int K = ellipsoid_offsets(bw, bh, bd, W, H, off);
+    #pragma omp parallel for schedule(static)
+    for (int z = 0; z < D; z++)
+        for (int y = 0; y < H; y++)
+            for (int x = 0; x < W; x++) {
+                const long p = (long)z * W * H + (long)y * W + x;
+                if (!interior3d(x, y, z, W, H, D, rw, rh, rd)) {
+                    means[p] = 0.0f;
+                    stds[p] = 0.0f;
+                    continue;
+                }
+                float mean = 0.0f;
+                for (int i = 0; i < K; i++) mean += img[p + off[i]];
+                mean /= (float)K;
+                float var = 0.0f;
+                for (int i = 0; i < K; i++) var += (img[p + off[i]] - mean) * (img[p + off[i]] - mean);
+                means[p] = mean;
+                stds[p] = sqrtf(var / (float)(K - 1));
+            }
+}
+
+/* java/Utils.java:1642-1662 (normalizeArray). */
+static void orc_normalize_array(float *a, int n) {
+    float mn = 3.40282347e38f, mx = -3.40282347e38f;
+    for (int i = 0; i < n; i++) {
+        mn = jmin(a[i], mn);
+        mx = jmax(a[i], mx);
+    }
+    for (int i = 0; i < n; i++) a[i] = (a[i] - mn) / (mx - mn + ORC_EPS);
+}
+
+/* java/Utils.java:1047-1160 (getReferenceBlock3D) for a block given as
+ * bd slices of bh x bw floats: ellipsoid-flatten, normalise, subtract the
+ * mean, normalise again; mean and (K-1) std of the result. Returns K. */
+int orc_reference_block3d(const float *blk, int bw, int bh, int bd, float *pixels, float *mean_out,
+                          float *std_out) {
+    const int rw = bw / 2, rh = bh / 2, rd = bd / 2;
+    int K = 0;
+    for (int z = 0; z < bd; z++)
+        for (int y = 0; y < bh; y++)
+            for (int x = 0; x < bw; x++)
+                if (in_ellipsoid(x - rw, y - rh, z - rd, rw, rh, rd)) pixels[K++] = blk[(z * bh + y) * bw + x];
+    orc_normalize_array(pixels, K);
+    float m = 0.0f;
+    for (int i = 0; i < K; i++) m += pixels[i];
+    m /= (float)K;
+    for (int i = 0; i < K; i++) pixels[i] = pixels[i] - m;
+    orc_normalize_array(pixels, K);
+    m = 0.0f;
+    for (int i = 0; i < K; i++) m += pixels[i];
+    m /= (float)K;
+    float s = 0.0f;
+    for (int i = 0; i < K; i++) s += (pixels[i] - m) * (pixels[i] - m);
+    *mean_out = m;
+    *std_out = (float)sqrt((double)(s / ((float)(K - 1))));
+    return K;
+}
+
+/* cl/kernelGetBlock{Pearson,Ssim,Nrmse,AbsDiffStds}3D.cl for every voxel,
+ * with the block radii of the block itself (the reference's Pearson command
+ * passes the block depth as the z radius, java/CLUtils.java:1149; repaired). */
+void orc_block3d_kernel_f32(int metric, const float *img, int W, int H, int D, int bw, int bh, int bd,
+                            const float *means, const float *stds, const float *ref, int K, float ref_mean,
+                            float ref_std, float *out) {
+    const int rw = bw / 2, rh = bh / 2, rd = bd / 2;
+    long off[4096];
+    ellipsoid_offsets(bw, bh, bd, W, H, off);
+    #pragma omp parallel for schedule(static)
+    for (int z = 0; z < D; z++)
+        for (int y = 0; y < H; y++)
+            for (int x = 0; x < W; x++) {
+                const long p = (long)z * W * H + (long)y * W + x;
+                if (!interior3d(x, y, z, W, H, D, rw, rh, rd)) {
+                    out[p] = 0.0f;
+                    continue;
+                }
+                float t[4096];
+                const float tstd = stds[p], tmean = means[p];
+                if (metric == ORC_ABSDIFF) {
+                    out[p] = fabsf((float)ref_std - (float)tstd);
+                    continue;
+                }
+                for (int i = 0; i < K; i++) t[i] = img[p + off[i]];
+                if (metric == ORC_PEARSON) {
+                    float mn = FLT_MAX, mx = -FLT_MAX;
+                    for (int i = 0; i < K; i++) {
+                        mn = fminf(mn, t[i]);
+                        mx = fmaxf(mx, t[i]);
+                    }
+                    for (int i = 0; i < K; i++) t[i] = (t[i] - mn) / (mx - mn + ORC_EPS);
+                    for (int i = 0; i < K; i++) t[i] = t[i] - tmean;
+                    mn = FLT_MAX;
+                    mx = -FLT_MAX;
+                    for (int i = 0; i < K; i++) {
+                        mn = fminf(mn, t[i]);
+                        mx = fmaxf(mx, t[i]);
+                    }
+                    for (int i = 0; i < K; i++) t[i] = (t[i] - mn) / (mx - mn + ORC_EPS);
+                    float cov = 0.0f;
+                    for (int i = 0; i < K; i++) cov += ref[i] * t[i];
+                    cov /= (float)(K - 1);
+                    if (ref_std == 0.0 && tstd == 0.0) out[p] = 1.0f;
+                    else if (ref_std == 0.0 || tstd == 0.0) out[p] = 0.0f;
+                    else out[p] = fmaxf(0.0f, (float)(cov / ((ref_std * tstd) + ORC_EPS)));
+                } else if (metric == ORC_SSIM) {
+                    for (int i = 0; i < K; i++) t[i] = t[i] - tmean;
+                    float cov = 0.0f;
+                    for (int i = 0; i < K; i++) cov += ref[i] * t[i];
+                    cov /= (float)(K - 1);
+                    const float c1 = 0.0001f, c2 = 0.0009f;
+                    if (ref_std == 0.0 && tstd == 0.0) out[p] = 1.0f;
+                    else if (ref_std == 0.0 || tstd == 0.0) out[p] = 0.0f;
+                    else {
+                        float ssim = (float)((2.0f * ref_mean * tmean + c1) * (2.0f * cov + c2)) /
+                                     (((ref_mean * ref_mean) + (tmean * tmean) + c1) *
+                                      ((ref_std * ref_std) + (tstd * tstd) + c2));
+                        out[p] = fmaxf(0.0f, ssim);
+                    }
+                } else { /* NRMSE */
+                    for (int i = 0; i < K; i++) t[i] = t[i] - tmean;
+                    float mse = 0.0f;
+                    for (int i = 0; i < K; i++) mse += (ref[i] - t[i]) * (ref[i] - t[i]);
+                    mse /= (float)K;
+                    out[p] = sqrtf(mse);
+                }
+            }
+}
+
+/* java/Utils.java:1463-1498 (getMeanNoiseVar3D from local stds): the mean
+ * local variance over the interior, FP32, raster order; the element count is
+ * a float (it stops growing at 2^24). */
+float orc_noise_var3d(int W, int H, int D, int rw, int rh, int rd, const float *stds) {
+    float s = 0.0f, n = 0.0f;
+    for (int z = rd; z < D - rd; z++)
+        for (int y = rh; y < H - rh; y++)
+            for (int x = rw; x < W - rw; x++) {
+                long i = (long)W * H * z + (long)y * W + x;
+                s += stds[i] * stds[i];
+                n += 1.0f;
+            }
+    return s / n;
+}
+
+/* java/Utils.java:1501-1525 (getRelevanceMask3D). Returns the noise variance. */
+float orc_relevance_mask3d(int W, int H, int D, int rw, int rh, int rd, const float *stds, float c, float *mask) {
+    const float nv = orc_noise_var3d(W, H, D, rw, rh, rd, stds);
+    memset(mask, 0, sizeof(float) * (size_t)W * H * D);
+    for (int z = rd; z < D - rd; z++)
+        for (int y = rh; y < H - rh; y++)
+            for (int x = rw; x < W - rw; x++) {
+                long i = (long)W * H * z + (long)y * W + x;
+                mask[i] = (stds[i] * stds[i]) <= nv * c ? 0.0f : 1.0f;
+            }
+    return nv;
+}
+
+/* java/Utils.java:1572-1630 (normalizeImage3D), in place; mask may be NULL. */
+void orc_normalize_image3d(float *a, int W, int H, int D, int rw, int rh, int rd, const float *mask) {
+    float mn = 3.40282347e38f, mx = -3.40282347e38f;
+    for (int z = rd; z < D - rd; z++)
+        for (int y = rh; y < H - rh; y++)
+            for (int x = rw; x < W - rw; x++) {
+                long i = (long)W * H * z + (long)y * W + x;
+                if (!mask || mask[i] > 0.0f) {
+                    mn = jmin(a[i], mn);
+                    mx = jmax(a[i], mx);
+                }
+            }
+    for (int z = rd; z < D - rd; z++)
+        for (int y = rh; y < H - rh; y++)
+            for (int x = rw; x < W - rw; x++) {
+                long i = (long)W * H * z + (long)y * W + x;
+                if (!mask || mask[i] > 0.0f) a[i] = (a[i] - mn) / (mx - mn + ORC_EPS);
+            }
+}
+
+/* Host steps after the 3D block kernels (java/CLUtils.java:1133-1637): NRMSE
+ * inverted (0 -> 1) and Abs-diff turned into 1 - x over the interior, the
+ * relevance mask applied when c > 0, normalisation over the interior (over
+ * the mask when c > 0). */
+void orc_block3d_postprocess_f32(int metric, float *map, int W, int H, int D, int rw, int rh, int rd,
+                                 const float *stds, float c, int normalize) {
+    for (int z = rd; z < D - rd; z++)
+        for (int y = rh; y < H - rh; y++)
+            for (int x = rw; x < W - rw; x++) {
+                long i = (long)W * H * z + (long)y * W + x;
+                if (metric == ORC_NRMSE) map[i] = map[i] == 0.0f ? 1.0f : 1.0f / map[i];
+                else if (metric == ORC_ABSDIFF) map[i] = 1.0f - map[i];
+            }
+    float *mask = NULL;
+    if (c > 0.0f) {
+        mask = (float *)malloc(sizeof(float) * (size_t)W * H * D);
+        orc_relevance_mask3d(W, H, D, rw, rh, rd, stds, c, mask);
+        for (long i = 0; i < (long)W * H * D; i++) map[i] *= mask[i];
+    }
+    if (normalize) orc_normalize_image3d(map, W, H, D, rw, rh, rd, mask);
+    free(mask);
+}

@@ -26,7 +26,9 @@ EXPORTS = [
     "sred_normalize_image_2d", "sred_debug_gram_rowdot", "sred_block_map_2d_device_noalloc",
     "sred_patch_hu_map_2d", "sred_hu_map_2d", "sred_phase_correlation_map_2d", "sred_global_map_2d_batch",
     "sred_global_map_2d_shard_sums", "sred_global_map_2d_shard_finish", "sred_set_log_callback",
-    "sred_gat_2d", "sred_gat_objective_2d", "sred_gat_fit_2d",
+    "sred_gat_2d", "sred_gat_objective_2d", "sred_gat_fit_2d", "sred_block_size_3d", "sred_reference_block_3d",
+    "sred_local_statistics_3d", "sred_relevance_mask_3d", "sred_calculate_block_repetition_map_3d",
+    "sred_block_map_3d_device",
 ]
 
 
@@ -103,6 +105,15 @@ def load() -> C.CDLL:
                                                C.c_float, C.c_float, s, _vp, _vp]
         L.sred_reference_block_2d.argtypes = [_f32p, s, s, _f32p, C.POINTER(C.c_int), _fp, _fp]
         L.sred_normalize_image_2d.argtypes = [_f32p, s, s, s, s, _vp]
+        f = C.c_float
+        L.sred_block_size_3d.argtypes = [s, s, s]
+        L.sred_reference_block_3d.argtypes = [_f32p, s, s, s, _f32p, C.POINTER(C.c_int), _fp, _fp]
+        L.sred_local_statistics_3d.argtypes = [_vp, _f32p, s, s, s, s, s, s, _f32p, _f32p]
+        L.sred_relevance_mask_3d.argtypes = [_vp, s, s, s, s, s, s, _f32p, f, _f32p, _fp]
+        L.sred_calculate_block_repetition_map_3d.argtypes = [_vp, C.c_char_p, _f32p, s, s, s, _f32p, s, s, s, s,
+                                                             f, f, f, s, _f32p]
+        L.sred_block_map_3d_device.argtypes = [_vp, C.c_char_p, _vp, s, s, s, _f32p, s, s, s, s, f, f, f, s, _vp,
+                                               _vp]
         _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
         L.sred_debug_gram_rowdot.argtypes = [_vp, s, _f32p, _f32p, _f32p, s, s, _f64p, _f64p]
         L.sred_block_map_2d_device_noalloc.argtypes = [C.c_char_p, _vp, s, s, s, _f32p, s, s, s, C.c_float,

@@ -1,4 +1,4 @@
-"""Host-side mirror of the reference's ``CLUtils`` (java/CLUtils.java), 2D parts.
+"""Host-side mirror of the reference's ``CLUtils`` (java/CLUtils.java).
 
 The OpenCL orchestration of the reference is replaced by libsred (CUDA,
 sm_100a); the method names, arguments and results stay. ``OpenCLResources``
@@ -16,7 +16,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from .utils import InputImage2D, ReferenceBlock2D, RelevanceMask
+from .utils import InputImage2D, InputImage3D, ReferenceBlock2D, ReferenceBlock3D, RelevanceMask
 
 GLOBAL_METRICS = ["Pearson's R", "SSIM", "NRMSE", "Abs. diff. of StdDevs"]  # java/GlobalRepetition2D_.java:20-25
 BLOCK_METRICS = ["Pearson's R", "SSIM", "NRMSE (inverted)", "Abs. Diff. of StdDevs."]  # java/BlockRepetition2D_.java:18-23
@@ -25,6 +25,7 @@ COSINE = "Cosine"  # raw-vector cosine similarity; no reference counterpart
 HU = "Hu moments"  # cl/kernelGetPatchHu2D.cl
 PHASE = "Phase correlation"  # cl/kernelGetPhaseCorrelationMap.cl (repaired)
 EXTRA_BLOCK_METRICS = [COSINE, HU, PHASE]
+BLOCK_METRICS_3D = ["Pearson's R", "SSIM", "NRMSE (inverted)", "Abs. Diff. of StdDevs."]  # java/BlockRepetition3D_.java:19-24
 
 
 @dataclass
@@ -302,3 +303,64 @@ def block_map_device(metric: str, d_img_ptr: int, width: int, height: int, frame
         reference_block.width, reference_block.height, float(reference_block.mean), float(reference_block.std),
         float(relevance_constant), int(bool(normalize_output)), C.c_void_p(d_out_ptr),
         C.c_void_p(stream_ptr or None)), "sred_block_map_2d_device")
+
+
+# ---------------------------------------------------------------------------
+# Volumes (java/CLUtils.java:1030-1653)
+# ---------------------------------------------------------------------------
+
+def get_local_statistics_3d(input_image: InputImage3D, block_width: int, block_height: int, block_depth: int,
+                            ctx=None) -> CLLocalStatistics:
+    """java/CLUtils.java:1030-1131."""
+    c = _ctx(ctx)
+    n = input_image.size
+    m = np.zeros(n, np.float32)
+    s = np.zeros(n, np.float32)
+    c.check(c._L.sred_local_statistics_3d(c.h, np.ascontiguousarray(input_image.image_array, np.float32).ravel(),
+                                          input_image.width, input_image.height, input_image.depth, block_width,
+                                          block_height, block_depth, m, s), "sred_local_statistics_3d")
+    return CLLocalStatistics(m, s)
+
+
+def calculate_block_repetition_map_3d(metric: str, input_image: InputImage3D, reference_block: ReferenceBlock3D,
+                                      relevance_constant: float, normalize_output: bool, use_device: bool = False,
+                                      ctx=None):
+    """java/CLUtils.java:1639-1653 (None for an unknown metric)."""
+    if metric not in BLOCK_METRICS_3D:
+        return None
+    c = _ctx(ctx)
+    out = np.zeros(input_image.size, np.float32)
+    rb = reference_block
+    c.check(c._L.sred_calculate_block_repetition_map_3d(
+        c.h, metric.encode(), np.ascontiguousarray(input_image.image_array, np.float32).ravel(), input_image.width,
+        input_image.height, input_image.depth, np.ascontiguousarray(rb.pixels, np.float32).ravel(), int(rb.size),
+        rb.width, rb.height, rb.depth, float(rb.mean), float(rb.std), float(relevance_constant),
+        int(bool(normalize_output)), out), "sred_calculate_block_repetition_map_3d")
+    return out
+
+
+def _block3d_getter(metric):
+    def f(input_image, reference_block, relevance_constant, normalize_output, use_device=False, ctx=None):
+        return calculate_block_repetition_map_3d(metric, input_image, reference_block, relevance_constant,
+                                                 normalize_output, use_device, ctx)
+    f.__doc__ = f"getBlock*3D for {metric!r} (java/CLUtils.java:1133-1637)."
+    return f
+
+
+get_block_pearson_3d = _block3d_getter("Pearson's R")
+get_block_ssim_3d = _block3d_getter("SSIM")
+get_block_nrmse_3d = _block3d_getter("NRMSE (inverted)")
+get_block_abs_diff_stds_3d = _block3d_getter("Abs. Diff. of StdDevs.")
+
+
+def block_map_3d_device(metric: str, d_vol_ptr: int, width: int, height: int, depth: int,
+                        reference_block: ReferenceBlock3D, relevance_constant: float, normalize_output: bool,
+                        d_out_ptr: int, stream_ptr: int = 0, ctx=None) -> None:
+    """3D block map over a device-resident volume (raw CUDA pointers)."""
+    c = _ctx(ctx)
+    rb = reference_block
+    c.check(c._L.sred_block_map_3d_device(
+        c.h, metric.encode(), C.c_void_p(d_vol_ptr), width, height, depth,
+        np.ascontiguousarray(rb.pixels, np.float32).ravel(), int(rb.size), rb.width, rb.height, rb.depth,
+        float(rb.mean), float(rb.std), float(relevance_constant), int(bool(normalize_output)),
+        C.c_void_p(d_out_ptr), C.c_void_p(stream_ptr or None)), "sred_block_map_3d_device")

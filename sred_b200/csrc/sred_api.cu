@@ -15,6 +15,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "shape.cuh"
+#include "volume.cuh"
 
 using namespace sred;
 
@@ -23,7 +24,7 @@ namespace {
 enum BufId {
   B_IMG, B_MEANS, B_STDS, B_MASK, B_MASKIN, B_FLAGS, B_SLOT, B_GPIX, B_FPIX, B_COUNTS, B_U, B_A, B_B,
   B_PARAMS, B_RMAX, B_NUM, B_DEN, B_SUMS, B_OUT, B_VARS, B_MM, B_NMASK, B_BAD, B_STATUS, B_STDS2, B_COLSOA,
-  B_FEAT, B_SIG, B_FR, B_FI, B_GAT, B_NBUF
+  B_FEAT, B_SIG, B_FR, B_FI, B_GAT, B_OFF3, B_REF3, B_NBUF
 };
 
 struct DevBuf {
@@ -536,6 +537,100 @@ sred_status block_core(sred_ctx* c, int metric, const float* d_img, int w, int h
     if (normalize) CKS(normalize_dev(c, d_out, d_mask, w, h, rw, rh, frames, st));
   }
   CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+  return SRED_OK;
+}
+
+// ---------------------------------------------------------------------------
+// 3D block repetition maps (java/CLUtils.java:1030-1653)
+// ---------------------------------------------------------------------------
+
+// Validates a volume and an ellipsoid block and uploads the block offsets.
+sred_status prepare_volume(sred_ctx* c, int w, int h, int d, int bw, int bh, int bd, cudaStream_t st, Vol3* v,
+                           int** d_off) {
+  if (w <= 0 || h <= 0 || d <= 0) return fail(c, SRED_ERR_ARG, "volume dimensions must be positive");
+  if (bw % 2 == 0 || bh % 2 == 0 || bd % 2 == 0 || bw < 3 || bh < 3 || bd < 3)
+    return fail(c, SRED_ERR_ARG, "block dimensions must be odd and at least 3");
+  if ((h + 3) / 4 > 65535 || d > 65535) return fail(c, SRED_ERR_ARG, "volume height or depth too large");
+  if ((long long)(bd / 2) * w * h + (long long)(bh / 2) * w + bw / 2 > 0x7fffffffll)
+    return fail(c, SRED_ERR_ARG, "block offsets exceed 32 bits");
+  std::vector<int> off(kMaxK3);
+  const int k = build_ellipsoid(bw, bh, bd, w, h, off.data());
+  if (k < 2 || k > kMaxK3) return fail(c, SRED_ERR_ARG, "ellipsoid block size out of range");
+  CKS(ensure(c, B_OFF3, k, d_off));
+  CK(cudaMemcpyAsync(*d_off, off.data(), sizeof(int) * k, cudaMemcpyHostToDevice, st));
+  *v = Vol3{w, h, d, bw / 2, bh / 2, bd / 2, k};
+  return SRED_OK;
+}
+
+dim3 vol_grid(const Vol3& v) { return dim3((v.W + 31) / 32, (v.H + 3) / 4, v.D); }
+
+// java/Utils.java:1463-1498 (getMeanNoiseVar3D): the mean of the local
+// variances over the interior, summed in FP32 in raster order with a float
+// count, as the reference does on the host.
+float noise_var_3d(const Vol3& v, const float* stds) {
+  float s = 0.0f, n = 0.0f;
+  for (int z = v.rd; z < v.D - v.rd; z++)
+    for (int y = v.rh; y < v.H - v.rh; y++)
+      for (int x = v.rw; x < v.W - v.rw; x++) {
+        const float sd = stds[((size_t)z * v.H + y) * v.W + x];
+        s += sd * sd;
+        n += 1.0f;
+      }
+  return s / n;
+}
+
+// Relevance mask of a volume from device local stds (the noise variance on
+// the host from a copy of them); map, if not null, is multiplied by the mask.
+sred_status mask_3d(sred_ctx* c, const Vol3& v, const float* d_stds, float relc, float* d_mask, float* d_map,
+                    cudaStream_t st, float* noise_var) {
+  const size_t n = (size_t)v.W * v.H * v.D;
+  std::vector<float> h_stds(n);
+  CK(cudaMemcpyAsync(h_stds.data(), d_stds, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  const float nv = noise_var_3d(v, h_stds.data());
+  k_mask3d<<<vol_grid(v), dim3(32, 4), 0, st>>>(d_stds, v, nv * relc, d_mask, d_map);
+  CK(cudaGetLastError());
+  if (noise_var) *noise_var = nv;
+  return SRED_OK;
+}
+
+sred_status block3d_core(sred_ctx* c, int metric, const float* d_vol, int w, int h, int d, const float* ref_pixels,
+                         int block_size, int bw, int bh, int bd, float ref_mean, float ref_std, float relc,
+                         int normalize, float* d_out, cudaStream_t st) {
+  c->shard.valid = false;  // shares workspaces with the global map
+  if (metric < kPearson || metric > kAbsDiff) return fail(c, SRED_ERR_UNKNOWN_METRIC, "unknown 3D block metric");
+  if (fault("launch")) return fail(c, SRED_ERR_LAUNCH, "injected launch failure");
+  Vol3 v;
+  int* d_off;
+  CKS(prepare_volume(c, w, h, d, bw, bh, bd, st, &v, &d_off));
+  if (block_size != v.k) return fail(c, SRED_ERR_ARG, "block_size does not match the ellipsoid of bw x bh x bd");
+  const size_t n = (size_t)w * h * d;
+  float *d_ref, *d_means, *d_stds;
+  CKS(ensure(c, B_REF3, v.k, &d_ref));
+  CKS(ensure(c, B_MEANS, n, &d_means));
+  CKS(ensure(c, B_STDS, n, &d_stds));
+  CK(cudaMemcpyAsync(d_ref, ref_pixels, sizeof(float) * v.k, cudaMemcpyHostToDevice, st));
+  const dim3 grid = vol_grid(v), blk(32, 4);
+  k_local_stats3d<<<grid, blk, sizeof(int) * v.k, st>>>(d_vol, v, d_off, d_means, d_stds);
+  k_block_map3d<<<grid, blk, 2 * sizeof(int) * v.k, st>>>(d_vol, v, d_off, d_ref, ref_mean, ref_std, metric,
+                                                          d_means, d_stds, d_out);
+  if (metric == kNrmse || metric == kAbsDiff) k_block3d_post<<<grid, blk, 0, st>>>(d_out, v, metric);
+  CK(cudaGetLastError());
+  float* d_mask = nullptr;
+  if (relc > 0.0f) {
+    CKS(ensure(c, B_MASK, n, &d_mask));
+    CKS(mask_3d(c, v, d_stds, relc, d_mask, d_out, st, nullptr));
+  }
+  if (normalize) {
+    unsigned* mm;
+    CKS(ensure(c, B_MM, 2, &mm));
+    const unsigned init[2] = {0xffffffffu, 0u};
+    CK(cudaMemcpyAsync(mm, init, sizeof(init), cudaMemcpyHostToDevice, st));
+    k_minmax3d<<<grid, blk, 0, st>>>(d_out, d_mask, v, mm);
+    k_remap3d<<<grid, blk, 0, st>>>(d_out, d_mask, v, mm);
+    CK(cudaGetLastError());
+  }
   CK(cudaStreamSynchronize(st));
   return SRED_OK;
 }
@@ -1285,6 +1380,137 @@ sred_status sred_normalize_image_2d(float* a, int w, int h, int bw_, int bh_, co
       a[i] = (a[i] - mn) / (mx - mn + kEps);
     }
   return SRED_OK;
+}
+
+// ---------------------------------------------------------------------------
+// 3D block repetition maps
+// ---------------------------------------------------------------------------
+
+int sred_block_size_3d(int bw, int bh, int bd) {
+  if (bw < 3 || bh < 3 || bd < 3) return 0;
+  return build_ellipsoid(bw, bh, bd, 1, 1, nullptr);
+}
+
+sred_status sred_reference_block_3d(const float* blk, int bw, int bh, int bd, float* pixels, int* block_size,
+                                    float* mean, float* std_out) {
+  if (!blk || !pixels || !block_size || !mean || !std_out) return SRED_ERR_ARG;
+  if (bw % 2 == 0 || bh % 2 == 0 || bd % 2 == 0 || bw < 3 || bh < 3 || bd < 3) return SRED_ERR_ARG;
+  const int rw = bw / 2, rh = bh / 2, rd = bd / 2;
+  const int K = build_ellipsoid(bw, bh, bd, 1, 1, nullptr);
+  if (K < 2 || K > kMaxK3) return SRED_ERR_ARG;
+  int k = 0;
+  for (int z = 0; z < bd; z++)
+    for (int y = 0; y < bh; y++)
+      for (int x = 0; x < bw; x++) {
+        const float fx = (float)(x - rw), fy = (float)(y - rh), fz = (float)(z - rd);
+        if (((fx * fx) / (float)(rw * rw)) + ((fy * fy) / (float)(rh * rh)) + ((fz * fz) / (float)(rd * rd)) <=
+            1.0f)
+          pixels[k++] = blk[((size_t)z * bh + y) * bw + x];
+      }
+  // normalizeArray, minus the mean, normalizeArray again (java/Utils.java:1100-1140)
+  auto minmax = [&]() {
+    float mn = 3.40282347e38f, mx = -3.40282347e38f;
+    for (int i = 0; i < K; i++) {
+      mn = std::min(pixels[i], mn);
+      mx = std::max(pixels[i], mx);
+    }
+    for (int i = 0; i < K; i++) pixels[i] = (pixels[i] - mn) / (mx - mn + kEps);
+  };
+  auto mean_of = [&]() {
+    float m = 0.0f;
+    for (int i = 0; i < K; i++) m += pixels[i];
+    return m / (float)K;
+  };
+  minmax();
+  float m = mean_of();
+  for (int i = 0; i < K; i++) pixels[i] = pixels[i] - m;
+  minmax();
+  m = mean_of();
+  float sd = 0.0f;
+  for (int i = 0; i < K; i++) sd += (pixels[i] - m) * (pixels[i] - m);
+  *block_size = K;
+  *mean = m;
+  *std_out = (float)std::sqrt((double)(sd / ((float)(K - 1))));
+  return SRED_OK;
+}
+
+sred_status sred_local_statistics_3d(sred_ctx* c, const float* vol, int w, int h, int d, int bw, int bh, int bd,
+                                     float* means, float* stds) {
+  if (!c || !vol || !means || !stds) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->shard.valid = false;
+  cudaStream_t st = c->stream;
+  Vol3 v;
+  int* d_off;
+  CKS(prepare_volume(c, w, h, d, bw, bh, bd, st, &v, &d_off));
+  const size_t n = (size_t)w * h * d;
+  float *d_vol, *d_m, *d_s;
+  CKS(ensure(c, B_IMG, n, &d_vol));
+  CKS(ensure(c, B_MEANS, n, &d_m));
+  CKS(ensure(c, B_STDS, n, &d_s));
+  CK(cudaMemcpyAsync(d_vol, vol, n * sizeof(float), cudaMemcpyHostToDevice, st));
+  k_local_stats3d<<<vol_grid(v), dim3(32, 4), sizeof(int) * v.k, st>>>(d_vol, v, d_off, d_m, d_s);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(means, d_m, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(stds, d_s, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return SRED_OK;
+}
+
+sred_status sred_relevance_mask_3d(sred_ctx* c, int w, int h, int d, int bw, int bh, int bd, const float* stds,
+                                   float relc, float* mask, float* noise_var) {
+  if (!c || !stds || !mask || !noise_var) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->shard.valid = false;
+  cudaStream_t st = c->stream;
+  Vol3 v;
+  int* d_off;
+  CKS(prepare_volume(c, w, h, d, bw, bh, bd, st, &v, &d_off));
+  const size_t n = (size_t)w * h * d;
+  float *d_s, *d_m;
+  CKS(ensure(c, B_STDS, n, &d_s));
+  CKS(ensure(c, B_MASK, n, &d_m));
+  CK(cudaMemcpyAsync(d_s, stds, n * sizeof(float), cudaMemcpyHostToDevice, st));
+  CKS(mask_3d(c, v, d_s, relc, d_m, nullptr, st, noise_var));
+  CK(cudaMemcpyAsync(mask, d_m, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return SRED_OK;
+}
+
+sred_status sred_calculate_block_repetition_map_3d(sred_ctx* c, const char* metric, const float* vol, int w,
+                                                   int h, int d, const float* ref_pixels, int block_size, int bw,
+                                                   int bh, int bd, float ref_mean, float ref_std, float relc,
+                                                   int normalize, float* out) {
+  if (!c || !vol || !ref_pixels || !out) return SRED_ERR_ARG;
+  const int m = block_metric(metric);
+  if (m < kPearson || m > kAbsDiff) return fail(c, SRED_ERR_UNKNOWN_METRIC, "unknown 3D block metric");
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (w <= 0 || h <= 0 || d <= 0) return fail(c, SRED_ERR_ARG, "bad dimensions");
+  const size_t n = (size_t)w * h * d;
+  float *d_vol, *d_out;
+  CKS(ensure(c, B_IMG, n, &d_vol));
+  CKS(ensure(c, B_OUT, n, &d_out));
+  CK(cudaMemcpyAsync(d_vol, vol, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  CKS(block3d_core(c, m, d_vol, w, h, d, ref_pixels, block_size, bw, bh, bd, ref_mean, ref_std, relc, normalize,
+                   d_out, c->stream));
+  CK(cudaMemcpyAsync(out, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SRED_OK;
+}
+
+sred_status sred_block_map_3d_device(sred_ctx* c, const char* metric, const float* d_vol, int w, int h, int d,
+                                     const float* ref_pixels, int block_size, int bw, int bh, int bd, float ref_mean,
+                                     float ref_std, float relc, int normalize, float* d_out, void* stream) {
+  if (!c || !d_vol || !ref_pixels || !d_out) return SRED_ERR_ARG;
+  const int m = block_metric(metric);
+  if (m < kPearson || m > kAbsDiff) return fail(c, SRED_ERR_UNKNOWN_METRIC, "unknown 3D block metric");
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  return block3d_core(c, m, d_vol, w, h, d, ref_pixels, block_size, bw, bh, bd, ref_mean, ref_std, relc, normalize,
+                      d_out, pick(c, stream));
 }
 
 }  // extern "C"

@@ -1,0 +1,223 @@
+// 3D (volume) block repetition maps: local statistics and one reference
+// block against every interior block of a volume, with the host steps of
+// java/CLUtils.java:1133-1637 (metric transform, relevance mask,
+// normalisation) on the device.
+//
+// FP32 in the reference kernels' evaluation order (cl/kernelGetLocalStatistics3D.cl,
+// cl/kernelGetBlock{Pearson,Ssim,Nrmse,AbsDiffStds}3D.cl); compiled with
+// -fmad=false so that no multiply-add is fused. One thread per voxel, threads
+// of a warp on consecutive x so that every gather of the block is coalesced;
+// the block offsets (and reference voxels) sit in shared memory and the
+// Pearson chain re-reads the block through L1 instead of holding it in a
+// local array.
+#include <float.h>
+
+#include "volume.cuh"
+
+namespace sred {
+
+namespace {
+
+__device__ __forceinline__ bool interior3(int x, int y, int z, const Vol3& v) {
+  return x >= v.rw && x < v.W - v.rw && y >= v.rh && y < v.H - v.rh && z >= v.rd && z < v.D - v.rd;
+}
+
+// Voxel of this thread for the (32, 4) block and ((W+31)/32, (H+3)/4, D) grid.
+__device__ __forceinline__ bool voxel(const Vol3& v, int* x, int* y, int* z, size_t* p) {
+  *x = blockIdx.x * blockDim.x + threadIdx.x;
+  *y = blockIdx.y * blockDim.y + threadIdx.y;
+  *z = blockIdx.z;
+  if (*x >= v.W || *y >= v.H) return false;
+  *p = ((size_t)*z * v.H + *y) * v.W + *x;
+  return true;
+}
+
+// Order-preserving key of a float for atomicMin/atomicMax on unsigned ints
+// (-0 orders below +0, as Math.min / Math.max do).
+__device__ __forceinline__ unsigned f2key(float f) {
+  const unsigned u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float key2f(unsigned k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(128)
+    k_local_stats3d(const float* __restrict__ img, Vol3 v, const int* __restrict__ off, float* __restrict__ means,
+                    float* __restrict__ stds) {
+  extern __shared__ int s_off[];
+  for (int i = threadIdx.y * blockDim.x + threadIdx.x; i < v.k; i += blockDim.x * blockDim.y) s_off[i] = off[i];
+  __syncthreads();
+  int x, y, z;
+  size_t p;
+  if (!voxel(v, &x, &y, &z, &p)) return;
+  if (!interior3(x, y, z, v)) {
+    means[p] = 0.0f;
+    stds[p] = 0.0f;
+    return;
+  }
+  const float* c = img + p;
+  const int K = v.k;
+  float mean = 0.0f;
+  for (int i = 0; i < K; i++) mean += c[s_off[i]];
+  mean /= (float)K;
+  float var = 0.0f;
+  for (int i = 0; i < K; i++) {
+    const float d = c[s_off[i]] - mean;
+    var += d * d;
+  }
+  means[p] = mean;
+  stds[p] = sqrtf(var / (float)(K - 1));
+}
+
+__global__ void __launch_bounds__(128)
+    k_block_map3d(const float* __restrict__ img, Vol3 v, const int* __restrict__ off, const float* __restrict__ ref,
+                  float ref_mean, float ref_std, int metric, const float* __restrict__ means,
+                  const float* __restrict__ stds, float* __restrict__ out) {
+  extern __shared__ int s_off[];
+  float* s_ref = reinterpret_cast<float*>(s_off + v.k);
+  for (int i = threadIdx.y * blockDim.x + threadIdx.x; i < v.k; i += blockDim.x * blockDim.y) {
+    s_off[i] = off[i];
+    s_ref[i] = ref[i];
+  }
+  __syncthreads();
+  int x, y, z;
+  size_t p;
+  if (!voxel(v, &x, &y, &z, &p)) return;
+  if (!interior3(x, y, z, v)) {
+    out[p] = 0.0f;
+    return;
+  }
+  const float tstd = stds[p];
+  const float* c = img + p;
+  const int K = v.k;
+  if (metric == kAbsDiff) {  // cl/kernelGetBlockAbsDiffStds3D.cl
+    out[p] = fabsf(ref_std - tstd);
+    return;
+  }
+  const float tmean = means[p];
+  if (metric == kPearson) {
+    // cl/kernelGetBlockPearson3D.cl: min-max of the block, minus its mean,
+    // min-max again, then the covariance with the reference.
+    float mn = FLT_MAX, mx = -FLT_MAX;
+    for (int i = 0; i < K; i++) {
+      const float t = c[s_off[i]];
+      mn = fminf(mn, t);
+      mx = fmaxf(mx, t);
+    }
+    const float d1 = mx - mn + kEps;
+    float mn2 = FLT_MAX, mx2 = -FLT_MAX;
+    for (int i = 0; i < K; i++) {
+      const float t = (c[s_off[i]] - mn) / d1 - tmean;
+      mn2 = fminf(mn2, t);
+      mx2 = fmaxf(mx2, t);
+    }
+    const float d2 = mx2 - mn2 + kEps;
+    float cov = 0.0f;
+    for (int i = 0; i < K; i++) {
+      const float t = (((c[s_off[i]] - mn) / d1 - tmean) - mn2) / d2;
+      cov += s_ref[i] * t;
+    }
+    cov /= (float)(K - 1);
+    if (ref_std == 0.0f && tstd == 0.0f) out[p] = 1.0f;
+    else if (ref_std == 0.0f || tstd == 0.0f) out[p] = 0.0f;
+    else out[p] = fmaxf(0.0f, cov / ((ref_std * tstd) + kEps));
+    return;
+  }
+  if (metric == kSsim) {  // cl/kernelGetBlockSsim3D.cl
+    float cov = 0.0f;
+    for (int i = 0; i < K; i++) cov += s_ref[i] * (c[s_off[i]] - tmean);
+    cov /= (float)(K - 1);
+    if (ref_std == 0.0f && tstd == 0.0f) {
+      out[p] = 1.0f;
+    } else if (ref_std == 0.0f || tstd == 0.0f) {
+      out[p] = 0.0f;
+    } else {
+      const float ssim = ((2.0f * ref_mean * tmean + kC1) * (2.0f * cov + kC2)) /
+                         (((ref_mean * ref_mean) + (tmean * tmean) + kC1) * ((ref_std * ref_std) + (tstd * tstd) + kC2));
+      out[p] = fmaxf(0.0f, ssim);
+    }
+    return;
+  }
+  // NRMSE, cl/kernelGetBlockNrmse3D.cl
+  float mse = 0.0f;
+  for (int i = 0; i < K; i++) {
+    const float d = s_ref[i] - (c[s_off[i]] - tmean);
+    mse += d * d;
+  }
+  mse /= (float)K;
+  out[p] = sqrtf(mse);
+}
+
+// Host steps on the interior (java/CLUtils.java:1459-1471, 1590-1600): NRMSE
+// inverted (0 -> 1), Abs-diff turned into 1 - x.
+__global__ void k_block3d_post(float* __restrict__ a, Vol3 v, int metric) {
+  int x, y, z;
+  size_t p;
+  if (!voxel(v, &x, &y, &z, &p) || !interior3(x, y, z, v)) return;
+  if (metric == kNrmse) a[p] = a[p] == 0.0f ? 1.0f : 1.0f / a[p];
+  else if (metric == kAbsDiff) a[p] = 1.0f - a[p];
+}
+
+// java/Utils.java:1501-1525 (getRelevanceMask3D) for the threshold
+// noise_var * c; map (if not null) is multiplied by the mask (applyMask3D).
+__global__ void k_mask3d(const float* __restrict__ stds, Vol3 v, float thr, float* __restrict__ mask,
+                         float* __restrict__ map) {
+  int x, y, z;
+  size_t p;
+  if (!voxel(v, &x, &y, &z, &p)) return;
+  float m = 0.0f;
+  if (interior3(x, y, z, v)) m = (stds[p] * stds[p]) <= thr ? 0.0f : 1.0f;
+  mask[p] = m;
+  if (map) map[p] *= m;
+}
+
+// java/Utils.java:1572-1630 (normalizeImage3D): min and max over the interior
+// (where mask > 0 when a mask is given); mm = {min key, max key}.
+__global__ void k_minmax3d(const float* __restrict__ a, const float* __restrict__ mask, Vol3 v,
+                           unsigned* __restrict__ mm) {
+  int x, y, z;
+  size_t p;
+  unsigned lo = 0xffffffffu, hi = 0u;
+  if (voxel(v, &x, &y, &z, &p) && interior3(x, y, z, v) && (!mask || mask[p] > 0.0f)) {
+    lo = hi = f2key(a[p]);
+  }
+  for (int o = 16; o; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0 && lo != 0xffffffffu) {
+    atomicMin(mm, lo);
+    atomicMax(mm + 1, hi);
+  }
+}
+
+__global__ void k_remap3d(float* __restrict__ a, const float* __restrict__ mask, Vol3 v,
+                          const unsigned* __restrict__ mm) {
+  if (mm[0] == 0xffffffffu) return;  // no voxel selected: the reference changes nothing
+  int x, y, z;
+  size_t p;
+  if (!voxel(v, &x, &y, &z, &p) || !interior3(x, y, z, v) || (mask && !(mask[p] > 0.0f))) return;
+  const float mn = key2f(mm[0]), mx = key2f(mm[1]);
+  a[p] = (a[p] - mn) / (mx - mn + kEps);
+}
+
+int build_ellipsoid(int bw, int bh, int bd, int W, int H, int* off) {
+  const int rw = bw / 2, rh = bh / 2, rd = bd / 2;
+  int k = 0;
+  for (int z = -rd; z <= rd; z++)
+    for (int y = -rh; y <= rh; y++)
+      for (int x = -rw; x <= rw; x++) {
+        const float fx = (float)x, fy = (float)y, fz = (float)z;
+        if (((fx * fx) / (float)(rw * rw)) + ((fy * fy) / (float)(rh * rh)) + ((fz * fz) / (float)(rd * rd)) <=
+            1.0f) {
+          if (off && k < kMaxK3) off[k] = z * W * H + y * W + x;
+          k++;
+        }
+      }
+  return k;
+}
+
+}  // namespace sred

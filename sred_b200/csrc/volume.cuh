@@ -1,0 +1,32 @@
+// 3D (volume) block repetition maps: device kernels and host helpers.
+#pragma once
+#include "common.cuh"
+
+namespace sred {
+
+constexpr int kMaxK3 = 4096;  // largest ellipsoid block size accepted
+
+// A W x H x D volume ([D][H][W] floats) and the ellipsoid block radii; k is
+// the number of voxels of the ellipsoid.
+struct Vol3 {
+  int W, H, D;
+  int rw, rh, rd;
+  int k;
+};
+
+// Host: linear offsets (z W H + y W + x) of the voxels of the ellipsoid
+// inscribed in a bw x bh x bd block, z-y-x order (java/Utils.java:1075-1085,
+// float arithmetic). Writes at most kMaxK3 offsets; returns the voxel count.
+int build_ellipsoid(int bw, int bh, int bd, int W, int H, int* off);
+
+// One thread per voxel; dynamic shared memory: k ints (stats), k ints + k
+// floats (block map).
+__global__ void k_local_stats3d(const float* img, Vol3 v, const int* off, float* means, float* stds);
+__global__ void k_block_map3d(const float* img, Vol3 v, const int* off, const float* ref, float ref_mean,
+                              float ref_std, int metric, const float* means, const float* stds, float* out);
+__global__ void k_block3d_post(float* a, Vol3 v, int metric);
+__global__ void k_mask3d(const float* stds, Vol3 v, float thr, float* mask, float* map);
+__global__ void k_minmax3d(const float* a, const float* mask, Vol3 v, unsigned* mm);
+__global__ void k_remap3d(float* a, const float* mask, Vol3 v, const unsigned* mm);
+
+}  // namespace sred

@@ -53,6 +53,36 @@ def spot_image(width: int, height: int, lattice: int, *, seed: int = 0, backgrou
     return img.astype(np.float32)
 
 
+def spot_volume(width: int, height: int, depth: int, lattice: int, lattice_z: int, *, seed: int = 0,
+                background: float = 100.0, sigma: float = 2.0, sigma_z: float = 1.5, amp_range=(50.0, 200.0),
+                jitter: float = 1.5, read_noise: float = 10.0) -> np.ndarray:
+    """float32 [depth, height, width] volume: isotropic-in-xy Gaussian spots
+    (width ``sigma``, ``sigma_z`` along z) on a jittered lattice of
+    ``lattice`` x ``lattice`` x ``lattice_z`` sites, Poisson shot noise and
+    Gaussian read noise."""
+    rng = np.random.default_rng(seed)
+    vol = np.full((depth, height, width), background, np.float64)
+    sx, sy, sz = width / lattice, height / lattice, depth / lattice_z
+    gz, gy, gx = np.mgrid[0:lattice_z, 0:lattice, 0:lattice]
+    n = gx.size
+    cx = (gx.ravel() + 0.5) * sx + rng.uniform(-jitter, jitter, n)
+    cy = (gy.ravel() + 0.5) * sy + rng.uniform(-jitter, jitter, n)
+    cz = (gz.ravel() + 0.5) * sz + rng.uniform(-jitter / 2, jitter / 2, n)
+    amp = rng.uniform(amp_range[0], amp_range[1], n)
+    r, rz = int(np.ceil(4 * sigma)), int(np.ceil(4 * sigma_z))
+    for i in range(n):
+        x0, x1 = max(int(cx[i]) - r, 0), min(int(cx[i]) + r + 1, width)
+        y0, y1 = max(int(cy[i]) - r, 0), min(int(cy[i]) + r + 1, height)
+        z0, z1 = max(int(cz[i]) - rz, 0), min(int(cz[i]) + rz + 1, depth)
+        if x0 >= x1 or y0 >= y1 or z0 >= z1:
+            continue
+        zz, yy, xx = np.mgrid[z0:z1, y0:y1, x0:x1]
+        d2 = ((xx - cx[i]) ** 2 + (yy - cy[i]) ** 2) / sigma ** 2 + (zz - cz[i]) ** 2 / sigma_z ** 2
+        vol[z0:z1, y0:y1, x0:x1] += amp[i] * np.exp(-0.5 * d2)
+    vol = rng.poisson(vol).astype(np.float64) + rng.normal(0.0, read_noise, vol.shape)
+    return vol.astype(np.float32)
+
+
 def normalize_input(img: np.ndarray) -> np.ndarray:
     """Min-max to [0, 1] with the reference's epsilon, in FP32 (java/Utils.java:707-722)."""
     a = np.ascontiguousarray(img, dtype=np.float32)
@@ -79,3 +109,9 @@ def image_1024_spots_random(seed: int = 0) -> np.ndarray:
 def image_2048_elongated(seed: int = 0) -> np.ndarray:
     """2048x2048, 25,600 spots on a 160x160 lattice, 10% elongated."""
     return spot_image(2048, 2048, 160, seed=seed, elongated_fraction=0.1)
+
+
+def volume_512_spots(seed: int = 0) -> np.ndarray:
+    """512x512x128 volume (134 MB as float32), 25,600 spots on a jittered
+    40x40x16 lattice."""
+    return spot_volume(512, 512, 128, 40, 16, seed=seed)

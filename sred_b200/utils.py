@@ -1,7 +1,8 @@
-"""Host-side mirror of the reference's ``Utils`` (java/Utils.java), 2D parts.
+"""Host-side mirror of the reference's ``Utils`` (java/Utils.java).
 
 Same names (snake_case), argument meaning and error behaviour: the data types
-``InputImage2D``, ``ReferenceBlock2D`` and ``RelevanceMask``, and the host
+``InputImage2D``, ``ReferenceBlock2D``, ``RelevanceMask`` and their 3D
+counterparts, and the host
 numerics that run between the plugin commands and the maps. The numerics run
 in libsred (``include/sred.h``); this module only marshals arrays.
 """
@@ -178,3 +179,91 @@ def normalize_image_2d(image_array: np.ndarray, image_width: int, image_height: 
 def block_size(block_width: int, block_height: int) -> int:
     """Ellipse block size (java/GlobalRepetition2D_.java:102-111)."""
     return _lib.load().sred_block_size(block_width, block_height)
+
+
+# ---------------------------------------------------------------------------
+# Volumes (java/Utils.java:291-470, 1047-1660). A volume is float32 [depth,
+# height, width], flattened as the reference's w*h*z + y*w + x.
+# ---------------------------------------------------------------------------
+
+@dataclass
+class InputImage3D:
+    """java/Utils.java:427-470 InputImage3D."""
+    image_array: np.ndarray
+    width: int
+    height: int
+    depth: int
+
+    @property
+    def size(self) -> int:
+        return self.width * self.height * self.depth
+
+
+@dataclass
+class ReferenceBlock3D:
+    """java/Utils.java:291-425 ReferenceBlock3D: ellipsoid voxels and their stats."""
+    pixels: np.ndarray
+    width: int
+    height: int
+    depth: int
+    radius_width: int
+    radius_height: int
+    radius_depth: int
+    size: int
+    mean: float
+    std: float
+
+
+def get_input_image_3d(volume: np.ndarray, stabilise_noise_variance: bool = False,
+                       normalize_output: bool = True) -> InputImage3D:
+    """java/Utils.java:1279-1354 for a volume given as an array: float
+    conversion and normalizeArray (min-max over the whole volume with epsilon,
+    FP32). Variance stabilisation of volumes is not provided (ValueError)."""
+    if stabilise_noise_variance:
+        raise ValueError("variance stabilisation of volumes is not provided")
+    a = np.ascontiguousarray(volume, dtype=np.float32)
+    d, h, w = a.shape
+    if normalize_output:
+        mn, mx = np.float32(a.min()), np.float32(a.max())
+        a = ((a - mn) / (mx - mn + EPSILON)).astype(np.float32)
+    return InputImage3D(a.ravel(), w, h, d)
+
+
+def block_size_3d(block_width: int, block_height: int, block_depth: int) -> int:
+    """Ellipsoid block size (java/Utils.java:1075-1085)."""
+    return _lib.load().sred_block_size_3d(block_width, block_height, block_depth)
+
+
+def get_reference_block_3d(block: np.ndarray) -> ReferenceBlock3D:
+    """java/Utils.java:1047-1160 for a block given as an array [bd, bh, bw].
+    Raises ValueError for even dimensions or fewer than 3 slices, as the
+    reference throws IllegalArgumentException."""
+    b = np.ascontiguousarray(block, dtype=np.float32)
+    bd, bh, bw = b.shape
+    if bw % 2 == 0 or bh % 2 == 0 or bd % 2 == 0:
+        raise ValueError("Block dimensions must be odd.")
+    if bd < 3:
+        raise ValueError("Reference block must have at least 3 slices.")
+    px = np.zeros(b.size, np.float32)
+    k, m, s = C.c_int(), C.c_float(), C.c_float()
+    st = _lib.load().sred_reference_block_3d(b.ravel(), bw, bh, bd, px, C.byref(k), C.byref(m), C.byref(s))
+    if st != _lib.OK:
+        raise ValueError(_lib.status_string(st))
+    return ReferenceBlock3D(px[:k.value].copy(), bw, bh, bd, bw // 2, bh // 2, bd // 2, k.value,
+                            np.float32(m.value), np.float32(s.value))
+
+
+def get_relevance_mask_3d(image_width: int, image_height: int, image_depth: int, block_radius_width: int,
+                          block_radius_height: int, block_radius_depth: int, local_stds: np.ndarray,
+                          relevance_constant: float, ctx=None) -> RelevanceMask:
+    """java/Utils.java:1501-1525 (the reference returns the mask alone; here
+    with its threshold and noise variance, as RelevanceMask)."""
+    c = _ctx(ctx)
+    mask = np.zeros(image_width * image_height * image_depth, np.float32)
+    nv = C.c_float()
+    c.check(c._L.sred_relevance_mask_3d(
+        c.h, image_width, image_height, image_depth, 2 * block_radius_width + 1, 2 * block_radius_height + 1,
+        2 * block_radius_depth + 1, np.ascontiguousarray(local_stds, np.float32).ravel(),
+        float(relevance_constant), mask, C.byref(nv)), "sred_relevance_mask_3d")
+    nvf = np.float32(nv.value)
+    return RelevanceMask(mask, np.float32(relevance_constant), np.float32(nvf * np.float32(relevance_constant)), nvf)

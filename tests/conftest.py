@@ -28,3 +28,16 @@ def refshim_fx():
 def shape_fx():
     import numpy as np
     return dict(np.load(ROOT / "tests" / "golden" / "shape_refshim.npz"))
+
+
+@pytest.fixture(scope="session")
+def volume_fx():
+    import numpy as np
+    return dict(np.load(ROOT / "tests" / "golden" / "volume_refshim.npz"))
+
+
+def volume_cases(fx):
+    """(name, bw, bh, bd) of the cases in volume_refshim.npz."""
+    for n in sorted({k.split("/")[0] for k in fx}):
+        bw, bh, bd = (int(v) for v in n.rsplit("_", 1)[1].split("x"))
+        yield n, bw, bh, bd

@@ -19,7 +19,13 @@ Two kinds of fixtures are written:
    ``cl/kernelGetPhaseCorrelationMap.cl``), compiled the same way, on small
    seeded images. No reference test covers these kernels.
 
-Usage: ``python tests/golden/make_golden.py [--reference /root/reference]``
+4. ``volume_refshim.npz``: outputs of the reference's 3D local-statistics and
+   3D block-map kernels (``cl/kernelGetLocalStatistics3D.cl``,
+   ``cl/kernelGetBlock{Pearson,Ssim,Nrmse,AbsDiffStds}3D.cl``), compiled the
+   same way, on small seeded volumes, with the Java host steps of
+   ``getBlock*3D`` applied by the oracle. No reference test covers 3D.
+
+Usage: ``python tests/golden/make_golden.py [--reference /root/reference] [--only volume ...]``
 """
 from __future__ import annotations
 
@@ -214,19 +220,70 @@ def shape_fixtures() -> dict:
     return fx
 
 
+VOLUME_CASES = [
+    # (name, W, H, D, lattice, lattice_z, seed, bw, bh, bd)
+    ("spots28x24x12_3x3x3", 28, 24, 12, 4, 2, 31, 3, 3, 3),
+    ("spots30x26x14_5x3x3", 30, 26, 14, 4, 2, 32, 5, 3, 3),
+    ("spots24x24x16_5x5x5", 24, 24, 16, 3, 2, 33, 5, 5, 5),
+    ("spots26x22x12_7x5x3", 26, 22, 12, 3, 2, 34, 7, 5, 3),
+]
+
+
+def flat_volume() -> np.ndarray:
+    """Volume with exactly flat regions (the std == 0 special cases)."""
+    v = np.zeros((10, 20, 24), np.float32)
+    v[2:8, 4:14, 5:20] = 0.5
+    v[:, 15:19, 2:8] = 1.0
+    rng = np.random.default_rng(7)
+    v[:, 0:3, :] = rng.uniform(0, 1, (10, 3, 24)).astype(np.float32)
+    return v
+
+
+def volume_fixtures() -> dict:
+    fx: dict = {}
+    cases = [(n, synth.normalize_input(synth.spot_volume(W, H, D, lat, latz, seed=seed)), bw, bh, bd)
+             for n, W, H, D, lat, latz, seed, bw, bh, bd in VOLUME_CASES]
+    cases.append(("flat24x20x10_3x3x3", flat_volume(), 3, 3, 3))
+    for name, vol, bw, bh, bd in cases:
+        fx[f"{name}/volume"] = vol
+        means, stds = oracle.local_stats3d(vol, bw, bh, bd, use_refshim=True)
+        fx[f"{name}/means"] = means
+        fx[f"{name}/stds"] = stds
+        D, H, W = vol.shape
+        z0, y0, x0 = D // 2 - bd // 2, H // 2 - bh // 2, W // 3 - bw // 2
+        px, bm, bs = oracle.reference_block3d(vol[z0:z0 + bd, y0:y0 + bh, x0:x0 + bw])
+        assert px.size == oracle.block_size3d(bw, bh, bd)
+        fx[f"{name}/block/pixels"] = px
+        fx[f"{name}/block/mean_std"] = np.array([bm, bs], np.float32)
+        for c in (0.0, 1.0):
+            mask, nv = oracle.relevance_mask3d(stds, bw, bh, bd, c)
+            fx[f"{name}/c{c:g}/mask"] = mask
+            fx[f"{name}/c{c:g}/noise_var"] = nv
+            for metric in oracle.BLOCK_METRICS_3D:
+                r = oracle.block_map3d(metric, vol, px, bw, bh, bd, bm, bs, c, True, use_refshim=True)
+                fx[f"{name}/{metric}/raw"] = r["raw"]  # the kernel's output does not depend on c
+                fx[f"{name}/c{c:g}/{metric}/map"] = r["map"]
+    return fx
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", choices=["junit", "global", "shape", "volume"], action="append",
+                    help="regenerate only these fixture files (default: all)")
     a = ap.parse_args(argv)
-    ref = Path(a.reference)
-    vec = junit_vectors(ref)
-    (HERE / "reference_junit.json").write_text(json.dumps(vec, indent=1))
-    fx = refshim_fixtures()
-    np.savez_compressed(HERE / "global_refshim.npz", **fx)
-    sx = shape_fixtures()
-    np.savez_compressed(HERE / "shape_refshim.npz", **sx)
-    print("wrote", HERE / "reference_junit.json", HERE / "global_refshim.npz", len(fx), "arrays,",
-          HERE / "shape_refshim.npz", len(sx), "arrays")
+    only = set(a.only or ["junit", "global", "shape", "volume"])
+    if "junit" in only:
+        vec = junit_vectors(Path(a.reference))
+        (HERE / "reference_junit.json").write_text(json.dumps(vec, indent=1))
+        print("wrote", HERE / "reference_junit.json")
+    for kind, fname, make in (("global", "global_refshim.npz", refshim_fixtures),
+                              ("shape", "shape_refshim.npz", shape_fixtures),
+                              ("volume", "volume_refshim.npz", volume_fixtures)):
+        if kind in only:
+            fx = make()
+            np.savez_compressed(HERE / fname, **fx)
+            print("wrote", HERE / fname, len(fx), "arrays")
     return 0
 
 

@@ -1,0 +1,130 @@
+"""Parity of the 3D block repetition maps through the C ABI.
+
+References: the reference's 3D kernels compiled for the CPU
+(cl/kernelGetLocalStatistics3D.cl, cl/kernelGetBlock{Pearson,Ssim,Nrmse,
+AbsDiffStds}3D.cl) with the Java host steps of getBlock*3D applied, frozen in
+tests/golden/volume_refshim.npz, and the oracle's restatement of both at
+sizes beyond the fixtures.
+
+Bar: bit-exact. The device code runs the kernels' FP32 operations in their
+order without fused multiply-adds, and the host steps (noise variance as an
+FP32 raster-order sum, relevance mask, normalisation) exactly as the
+reference's Java does.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import volume_cases
+from sred_b200 import _lib, clutils, synth, utils
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return _lib.Context(0, "fp32")
+
+
+def _inp(vol):
+    d, h, w = vol.shape
+    return utils.InputImage3D(np.ascontiguousarray(vol, np.float32).ravel(), w, h, d)
+
+
+def _block(vol, bw, bh, bd):
+    D, H, W = vol.shape
+    z0, y0, x0 = D // 2 - bd // 2, H // 2 - bh // 2, W // 3 - bw // 2
+    return vol[z0:z0 + bd, y0:y0 + bh, x0:x0 + bw]
+
+
+def test_local_statistics_3d_bit_exact(ctx, volume_fx):
+    for name, bw, bh, bd in volume_cases(volume_fx):
+        vol = volume_fx[f"{name}/volume"]
+        st = clutils.get_local_statistics_3d(_inp(vol), bw, bh, bd, ctx=ctx)
+        assert np.array_equal(st.local_means, volume_fx[f"{name}/means"].ravel()), name
+        assert np.array_equal(st.local_stds, volume_fx[f"{name}/stds"].ravel()), name
+
+
+def test_reference_block_3d_bit_exact(volume_fx):
+    for name, bw, bh, bd in volume_cases(volume_fx):
+        rb = utils.get_reference_block_3d(_block(volume_fx[f"{name}/volume"], bw, bh, bd))
+        assert np.array_equal(rb.pixels, volume_fx[f"{name}/block/pixels"]), name
+        assert [rb.mean, rb.std] == list(volume_fx[f"{name}/block/mean_std"]), name
+        assert rb.size == utils.block_size_3d(bw, bh, bd)
+
+
+def test_relevance_mask_3d_bit_exact(ctx, volume_fx):
+    for name, bw, bh, bd in volume_cases(volume_fx):
+        d, h, w = volume_fx[f"{name}/volume"].shape
+        for c in (0.0, 1.0):
+            rm = utils.get_relevance_mask_3d(w, h, d, bw // 2, bh // 2, bd // 2, volume_fx[f"{name}/stds"], c,
+                                             ctx=ctx)
+            assert np.array_equal(rm.relevance_mask, volume_fx[f"{name}/c{c:g}/mask"].ravel()), (name, c)
+            assert rm.noise_mean_variance == volume_fx[f"{name}/c{c:g}/noise_var"], (name, c)
+
+
+@pytest.mark.parametrize("metric", clutils.BLOCK_METRICS_3D)
+def test_block_map_3d_bit_exact(ctx, volume_fx, metric):
+    for name, bw, bh, bd in volume_cases(volume_fx):
+        vol = volume_fx[f"{name}/volume"]
+        rb = utils.get_reference_block_3d(_block(vol, bw, bh, bd))
+        for c in (0.0, 1.0):
+            got = clutils.calculate_block_repetition_map_3d(metric, _inp(vol), rb, c, True, ctx=ctx)
+            assert np.array_equal(got, volume_fx[f"{name}/c{c:g}/{metric}/map"].ravel()), (name, c)
+        # without normalisation: the kernel output with the metric transform
+        px, (bm, bs) = volume_fx[f"{name}/block/pixels"], volume_fx[f"{name}/block/mean_std"]
+        exp = oracle.block_map3d(metric, vol, px, bw, bh, bd, bm, bs, 0.0, False)["map"]
+        got = clutils.calculate_block_repetition_map_3d(metric, _inp(vol), rb, 0.0, False, ctx=ctx)
+        assert np.array_equal(got, exp.ravel()), name
+
+
+@pytest.mark.parametrize("shape,block", [((64, 96, 80), (5, 5, 5)), ((40, 128, 120), (9, 7, 3)),
+                                         ((33, 61, 47), (11, 11, 11))])
+def test_block_map_3d_larger_volumes(ctx, shape, block):
+    """Volumes beyond the fixtures (ragged sides, K up to 515) against the oracle."""
+    d, h, w = shape
+    bw, bh, bd = block
+    vol = synth.normalize_input(synth.spot_volume(w, h, d, 6, 3, seed=d + h + w))
+    rb = utils.get_reference_block_3d(vol[d // 3:d // 3 + bd, h // 2:h // 2 + bh, w // 4:w // 4 + bw])
+    for metric in clutils.BLOCK_METRICS_3D:
+        for c in (0.0, 0.7):
+            exp = oracle.block_map3d(metric, vol, rb.pixels, bw, bh, bd, rb.mean, rb.std, c, True)["map"]
+            got = clutils.calculate_block_repetition_map_3d(metric, _inp(vol), rb, c, True, ctx=ctx)
+            assert np.array_equal(got, exp.ravel()), (metric, c)
+
+
+def test_block_map_3d_device_matches_host(ctx, volume_fx):
+    import torch
+    name, bw, bh, bd = next(volume_cases(volume_fx))
+    vol = volume_fx[f"{name}/volume"]
+    d, h, w = vol.shape
+    rb = utils.get_reference_block_3d(_block(vol, bw, bh, bd))
+    dv = torch.from_numpy(np.ascontiguousarray(vol)).cuda()
+    out = torch.empty_like(dv)
+    for metric in clutils.BLOCK_METRICS_3D:
+        clutils.block_map_3d_device(metric, dv.data_ptr(), w, h, d, rb, 1.0, True, out.data_ptr(),
+                                    torch.cuda.current_stream().cuda_stream, ctx=ctx)
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy().ravel(), volume_fx[f"{name}/c1/{metric}/map"].ravel()), metric
+
+
+def test_block_map_3d_edges(ctx):
+    """No interior (depth below the block), the smallest interior, and argument errors."""
+    rng = np.random.default_rng(3)
+    rb = utils.get_reference_block_3d(rng.random((3, 3, 3), dtype=np.float32))
+    for d in (2, 3):
+        vol = rng.random((d, 9, 8), dtype=np.float32)
+        for metric in clutils.BLOCK_METRICS_3D:
+            for c in (0.0, 1.0):
+                exp = oracle.block_map3d(metric, vol, rb.pixels, 3, 3, 3, rb.mean, rb.std, c, True)["map"]
+                got = clutils.calculate_block_repetition_map_3d(metric, _inp(vol), rb, c, True, ctx=ctx)
+                assert np.array_equal(got, exp.ravel(), equal_nan=True), (d, metric, c)
+    vol = _inp(rng.random((6, 7, 8), dtype=np.float32))
+    assert clutils.calculate_block_repetition_map_3d("Cosine", vol, rb, 0.0, True, ctx=ctx) is None
+    with pytest.raises(ValueError):
+        utils.get_reference_block_3d(np.zeros((3, 4, 3), np.float32))
+    with pytest.raises(ValueError):
+        utils.get_reference_block_3d(np.zeros((1, 3, 3), np.float32))
+    bad = utils.ReferenceBlock3D(rb.pixels, 3, 3, 3, 1, 1, 1, rb.size + 1, rb.mean, rb.std)
+    with pytest.raises(_lib.SredError):
+        clutils.calculate_block_repetition_map_3d("SSIM", vol, bad, 0.0, True, ctx=ctx)

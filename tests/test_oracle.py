@@ -283,3 +283,85 @@ def test_gat_objective_matches_numpy():
         assert abs(oracle.gat_objective(img, g, s, o) - err) <= 1e-9 * max(err, 1e-12)
     # the true parameters stabilise the variance much better than the reference's starting point
     assert oracle.gat_objective(img, 2.0, 5.0, 100.0) < 0.1 * oracle.gat_objective(img, 1.0, 10.0, 100.0)
+
+
+# ---------------------------------------------------------------------------
+# 3D block maps (cl/kernelGetLocalStatistics3D.cl,
+# cl/kernelGetBlock*3D.cl and the host steps of java/CLUtils.java:1133-1637):
+# the restatement against the reference's kernels, frozen in
+# tests/golden/volume_refshim.npz
+# ---------------------------------------------------------------------------
+
+from conftest import volume_cases  # noqa: E402
+
+
+def test_block_size_ellipsoid():
+    f = np.float32
+    for bw, bh, bd in [(3, 3, 3), (5, 3, 7), (9, 9, 9), (11, 11, 11)]:
+        rw, rh, rd = bw // 2, bh // 2, bd // 2
+        k = 0
+        for z in range(-rd, rd + 1):
+            for y in range(-rh, rh + 1):
+                for x in range(-rw, rw + 1):
+                    k += (f(x * x) / f(rw * rw)) + (f(y * y) / f(rh * rh)) + (f(z * z) / f(rd * rd)) <= f(1)
+        assert oracle.block_size3d(bw, bh, bd) == k
+
+
+def test_volume_stats_match_refshim_fixtures(volume_fx):
+    fx = volume_fx
+    for name, bw, bh, bd in volume_cases(fx):
+        m, s = oracle.local_stats3d(fx[f"{name}/volume"], bw, bh, bd)
+        assert np.array_equal(m, fx[f"{name}/means"]) and np.array_equal(s, fx[f"{name}/stds"]), name
+
+
+def test_volume_block_maps_match_refshim_fixtures(volume_fx):
+    fx = volume_fx
+    n = 0
+    for name, bw, bh, bd in volume_cases(fx):
+        vol = fx[f"{name}/volume"]
+        px = fx[f"{name}/block/pixels"]
+        bm, bs = fx[f"{name}/block/mean_std"]
+        D, H, W = vol.shape
+        z0, y0, x0 = D // 2 - bd // 2, H // 2 - bh // 2, W // 3 - bw // 2
+        q = oracle.reference_block3d(vol[z0:z0 + bd, y0:y0 + bh, x0:x0 + bw])
+        assert np.array_equal(q[0], px) and q[1] == bm and q[2] == bs, name
+        for c in (0.0, 1.0):
+            mask, nv = oracle.relevance_mask3d(fx[f"{name}/stds"], bw, bh, bd, c)
+            assert np.array_equal(mask, fx[f"{name}/c{c:g}/mask"]) and nv == fx[f"{name}/c{c:g}/noise_var"]
+            for metric in oracle.BLOCK_METRICS_3D:
+                r = oracle.block_map3d(metric, vol, px, bw, bh, bd, bm, bs, c, True)
+                assert np.array_equal(r["raw"], fx[f"{name}/{metric}/raw"]), (name, metric)
+                assert np.array_equal(r["map"], fx[f"{name}/c{c:g}/{metric}/map"]), (name, c, metric)
+                n += 1
+    assert n == 40
+
+
+def test_volume_flat_special_cases(volume_fx):
+    """Flat blocks: Pearson and SSIM 1 where both stds are 0, 0 where one is."""
+    fx = volume_fx
+    name = "flat24x20x10_3x3x3"
+    stds = fx[f"{name}/stds"]
+    px, (bm, bs) = fx[f"{name}/block/pixels"], fx[f"{name}/block/mean_std"]
+    flat = (stds == 0)
+    flat[:1] = flat[-1:] = False
+    flat[:, :1] = flat[:, -1:] = False
+    flat[:, :, :1] = flat[:, :, -1:] = False
+    assert flat.sum() > 100
+    for metric in ("Pearson's R", "SSIM"):
+        raw = fx[f"{name}/{metric}/raw"]
+        assert np.all(raw[flat] == (1.0 if bs == 0 else 0.0))
+
+
+@pytest.mark.skipif(oracle.refshim() is None, reason="refshim not built")
+def test_volume_matches_refshim_live():
+    from sred_b200 import synth
+    vol = synth.normalize_input(synth.spot_volume(22, 20, 11, 3, 2, seed=77))
+    for bw, bh, bd in ((3, 3, 5), (7, 3, 3), (5, 7, 5)):
+        a = oracle.local_stats3d(vol, bw, bh, bd)
+        b = oracle.local_stats3d(vol, bw, bh, bd, use_refshim=True)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+        px, bm, bs = oracle.reference_block3d(vol[3:3 + bd, 5:5 + bh, 6:6 + bw])
+        for metric in oracle.BLOCK_METRICS_3D:
+            x = oracle.block_map3d(metric, vol, px, bw, bh, bd, bm, bs, 1.0)
+            y = oracle.block_map3d(metric, vol, px, bw, bh, bd, bm, bs, 1.0, use_refshim=True)
+            assert np.array_equal(x["raw"], y["raw"]) and np.array_equal(x["map"], y["map"]), metric
