@@ -342,6 +342,39 @@ sred_status sred_block_map_3d_device(sred_ctx *ctx, const char *metric, const fl
                                      float ref_mean, float ref_std, float relevance_constant,
                                      int normalize_output, float *d_out, void *stream);
 
+/* Replaces CLUtils.calculateGlobalRepetitionMap3D (java/CLUtils.java:2793-2816)
+ * and the four getGlobal*3D methods (:2225-2790) with their kernels
+ * (cl/kernelGetGlobal{Pearson,Ssim,Nrmse,AbsDiffStds}3D.cl), after the
+ * preprocessing of java/GlobalRepetition3D_.java:97-143 (local statistics,
+ * relevance mask, nPixels). metric: "Pearson's R", "SSIM", "NRMSE" or
+ * "Abs. diff. of StdDevs". For every interior voxel p of non-zero local
+ * variance with sigma_p^2 >= threshold: num_p = sum over the test voxels q
+ * (interior, sigma_q^2 >= threshold; Abs-diff also sigma_q^2 != 0) of
+ * term(p, q) w(p, q), den_p = sum of w(p, q), w = exp(-(sigma_p - sigma_q)^2 /
+ * (noise_var + eps)); term: Pearson max(0, r), SSIM the kernel's SSIM (the
+ * product mu_p^2 mu_q^2 in its denominator), NRMSE the root mean squared
+ * difference of the centred blocks, Abs-diff |sigma_p - sigma_q|; a flat test
+ * block gives Pearson and SSIM 0. The map is num / (den nPixels + eps), NRMSE
+ * and Abs-diff inverted where the mask is 1, the mask applied when
+ * relevance_constant > 0, normalizeImage3D over the mask. Sums in FP64 from
+ * FP32 terms (the tensor-core engine computes the block dot products in split
+ * BF16, as the 2D global map). Repairs of the reference, which does not run as
+ * shipped: the relevance mask is getRelevanceMask3D's (noise variance = mean
+ * local variance over the interior; the command passes the 2D mask,
+ * java/GlobalRepetition3D_.java:126-128, whose indexing fails on the first
+ * interior slice), the reference block spans all bd slices (the kernels gather
+ * one slice short, e.g. cl/kernelGetGlobalPearson3D.cl:46), and SSIM compiles
+ * (cl/kernelGetGlobalSsim3D.cl:76). K <= 512. */
+sred_status sred_calculate_global_repetition_map_3d(sred_ctx *ctx, const char *metric, const float *vol, int w,
+                                                    int h, int d, int bw, int bh, int bd,
+                                                    float relevance_constant, int normalize_output, float *out,
+                                                    sred_run_info *info);
+
+/* Device-resident variant of sred_calculate_global_repetition_map_3d. */
+sred_status sred_global_map_3d_device(sred_ctx *ctx, const char *metric, const float *d_vol, int w, int h, int d,
+                                      int bw, int bh, int bd, float relevance_constant, int normalize_output,
+                                      float *d_out, void *stream, sred_run_info *info);
+
 #ifdef __cplusplus
 }
 #endif

@@ -95,6 +95,17 @@ def lib() -> C.CDLL:
                                            _f32p]
         L.orc_block3d_postprocess_f32.argtypes = [C.c_int, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                                   C.c_int, _f32p, C.c_float, C.c_int]
+        i32 = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+        L.orc_global3d_f32.argtypes = [C.c_int, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       _f32p, _f32p, C.c_float, C.c_float, i32, C.c_int, _f32p, _f32p]
+        L.orc_global3d_f64.argtypes = [C.c_int, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       _f32p, C.c_float, C.c_float, i32, C.c_int, _f64p, _f64p]
+        L.orc_n_pixels3d.restype = C.c_float
+        L.orc_n_pixels3d.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.orc_global3d_finalize_f32.argtypes = [C.c_int, _f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                C.c_int, C.c_int, _f32p, C.c_float, C.c_float, C.c_int, _f32p]
+        L.orc_global3d_finalize_f64.argtypes = [C.c_int, _f64p, _f64p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                C.c_int, C.c_int, _f32p, C.c_float, C.c_double, C.c_int, _f64p]
         L.orc_gat_objective.restype = C.c_double
         L.orc_gat_objective.argtypes = [_f32p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
         L.orc_patch_hu1_ref.restype = C.c_double
@@ -542,3 +553,96 @@ def relevance_mask3d(stds, bw, bh, bd, c):
     mask = np.zeros(s.size, np.float32)
     nv = lib().orc_relevance_mask3d(W, H, D, bw // 2, bh // 2, bd // 2, s.ravel(), C.c_float(c), mask)
     return mask.reshape(D, H, W), np.float32(nv)
+
+
+# --------------------------------------------------------------------------
+# 3D global repetition maps (cl/kernelGetGlobal*3D.cl, java/CLUtils.java:2225-2816,
+# java/GlobalRepetition3D_.java:97-158), with the relevance mask of the 3D
+# block command (getRelevanceMask3D) in place of the 2D mask the 3D global
+# command passes (java/GlobalRepetition3D_.java:126-128, which makes the
+# command fail on its first interior slice).
+# --------------------------------------------------------------------------
+
+def _pix3(W, H, D, rw, rh, rd):
+    zs, ys, xs = np.mgrid[rd:D - rd, rh:H - rh, rw:W - rw]
+    return np.ascontiguousarray((zs * (W * H) + ys * W + xs).ravel(), dtype=np.int32)
+
+
+def global3d_sums_f32(metric, vol, bw, bh, bd, means, stds, filter_param, threshold, pix=None,
+                      use_refshim=False):
+    """(num, den) per listed reference voxel, FP32 reference semantics."""
+    v = _f32(vol)
+    D, H, W = v.shape
+    pix = _pix3(W, H, D, bw // 2, bh // 2, bd // 2) if pix is None else np.ascontiguousarray(pix, np.int32)
+    m = GLOBAL_METRICS[metric]
+    if use_refshim:
+        R = refshim()
+        if R is None:
+            raise RuntimeError("refshim not built (no reference checkout at build time)")
+        K = block_size3d(bw, bh, bd)
+        num = np.zeros(v.size, np.float32)
+        den = np.zeros(v.size, np.float32)
+        name = ["kernelGetGlobalPearson3D", "kernelGetGlobalSsim3D", "kernelGetGlobalNrmse3D",
+                "kernelGetGlobalAbsDiffStds3D"][m]
+        args = [C.c_int(K), W, H, D, bw, bh, bd, C.c_float(filter_param), C.c_float(threshold),
+                C.c_float(EPSILON), pix.ctypes.data_as(C.c_void_p), C.c_int(pix.size),
+                v.ctypes.data_as(C.c_void_p)]
+        if m != 3:
+            args.append(_f32(means).ctypes.data_as(C.c_void_p))
+        args += [_f32(stds).ctypes.data_as(C.c_void_p), den.ctypes.data_as(C.c_void_p),
+                 num.ctypes.data_as(C.c_void_p)]
+        if getattr(R, f"rs_{name}")(*args) != 0:
+            raise ValueError(f"refshim has no instantiation for K={K}")
+        return num[pix], den[pix]
+    num = np.zeros(pix.size, np.float32)
+    den = np.zeros(pix.size, np.float32)
+    lib().orc_global3d_f32(m, v.ravel(), W, H, D, bw, bh, bd, _f32(means).ravel(), _f32(stds).ravel(),
+                           C.c_float(filter_param), C.c_float(threshold), pix, pix.size, num, den)
+    return num, den
+
+
+def global3d_sums_f64(metric, vol, bw, bh, bd, stds, filter_param, threshold, pix=None):
+    """(num, den) per listed reference voxel, FP64 judge."""
+    v = _f32(vol)
+    D, H, W = v.shape
+    pix = _pix3(W, H, D, bw // 2, bh // 2, bd // 2) if pix is None else np.ascontiguousarray(pix, np.int32)
+    num = np.zeros(pix.size, np.float64)
+    den = np.zeros(pix.size, np.float64)
+    lib().orc_global3d_f64(GLOBAL_METRICS[metric], v.ravel(), W, H, D, bw, bh, bd, _f32(stds).ravel(),
+                           C.c_float(filter_param), C.c_float(threshold), pix, pix.size, num, den)
+    return num, den
+
+
+def global_map3d(metric, vol, bw, bh, bd, relevance_constant, normalize=True, precision="f32",
+                 use_refshim=False):
+    """Full 3D global repetition map; a dict with the map and every intermediate."""
+    v = _f32(vol)
+    D, H, W = v.shape
+    rw, rh, rd = bw // 2, bh // 2, bd // 2
+    means, stds = local_stats3d(v, bw, bh, bd, use_refshim)
+    mask, nv = relevance_mask3d(stds, bw, bh, bd, relevance_constant)
+    thr = np.float32(nv * np.float32(relevance_constant))
+    npx = np.float32(lib().orc_n_pixels3d(mask.ravel(), W, H, D, rw, rh, rd))
+    pix = _pix3(W, H, D, rw, rh, rd)
+    m = GLOBAL_METRICS[metric]
+    if precision == "f32":
+        num, den = global3d_sums_f32(metric, v, bw, bh, bd, means, stds, nv, thr, pix, use_refshim)
+        nf = np.zeros(v.size, np.float32)
+        df = np.zeros(v.size, np.float32)
+        nf[pix] = num
+        df[pix] = den
+        out = np.zeros(v.size, np.float32)
+        lib().orc_global3d_finalize_f32(m, nf, df, W, H, D, rw, rh, rd, mask.ravel().copy(),
+                                        C.c_float(relevance_constant), C.c_float(npx), int(normalize), out)
+    else:
+        num, den = global3d_sums_f64(metric, v, bw, bh, bd, stds, nv, thr, pix)
+        nf = np.zeros(v.size, np.float64)
+        df = np.zeros(v.size, np.float64)
+        nf[pix] = num
+        df[pix] = den
+        out = np.zeros(v.size, np.float64)
+        lib().orc_global3d_finalize_f64(m, nf, df, W, H, D, rw, rh, rd, mask.ravel().copy(),
+                                        C.c_float(relevance_constant), C.c_double(float(npx)), int(normalize), out)
+    sh = (D, H, W)
+    return {"map": out.reshape(sh), "num": nf.reshape(sh), "den": df.reshape(sh), "means": means,
+            "stds": stds, "mask": mask, "threshold": thr, "noise_var": nv, "n_pixels": npx}

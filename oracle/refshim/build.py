@@ -87,6 +87,25 @@ MACROS_3D = ["image_depth", "bZ", "bRZ", "imageWidth", "imageHeight", "imageDept
 SIZES_3D = [(a, b, c) for a in (3, 5, 7) for b in (3, 5, 7) for c in (3, 5)]
 
 
+# 3D global-map kernels. Two repairs (documented in oracle/sred_oracle.c,
+# orc_global3d_f32): the reference block is gathered over all bd slices
+# (the kernels stop one slice short), and SSIM's below-threshold branch names
+# its own map (the shipped kernel names an undeclared pearson_map).
+KERNELS_3D_GLOBAL = {
+    "kernelGetGlobalPearson3D": ["img", "means", "stds", "den", "num"],
+    "kernelGetGlobalSsim3D": ["img", "means", "stds", "den", "num"],
+    "kernelGetGlobalNrmse3D": ["img", "means", "stds", "den", "num"],
+    "kernelGetGlobalAbsDiffStds3D": ["img", "stds", "den", "num"],
+}
+GLOBAL_3D_REPAIRS = {
+    "kernelGetGlobalPearson3D": [("z<gz+bRZ", "z<=gz+bRZ")],
+    "kernelGetGlobalSsim3D": [("z<gz+bRZ", "z<=gz+bRZ"), ("pearson_map[ref_index] += 0.0f;",
+                                                          "ssim_map[ref_index] += 0.0f;")],
+    "kernelGetGlobalNrmse3D": [("z<gz+bRZ", "z<=gz+bRZ")],
+    "kernelGetGlobalAbsDiffStds3D": [],
+}
+
+
 def ellipsoid_k(bw: int, bh: int, bd: int) -> int:
     f = np.float32
     rw, rh, rd = bw // 2, bh // 2, bd // 2
@@ -138,6 +157,54 @@ extern "C" int rs_{name}(int K, int W, int H, int D, int bw, int bh, int bd, flo
   RS_W = W; RS_H = H; RS_D = D; RS_BW = bw; RS_BH = bh; RS_BZ = bd;
   RS_BRW = bw / 2; RS_BRH = bh / 2; RS_BRZ = bd / 2;
   RS_EPSILON = eps; RS_BLOCK_STD = block_std; RS_BLOCK_MEAN = block_mean;
+  switch (K) {{
+{cases}
+    default: return -1;
+  }}
+  return 0;
+}}
+"""
+
+
+def gen_unit_3d_global(ref: Path, name: str) -> str:
+    args = KERNELS_3D_GLOBAL[name]
+    src = (ref / "src/main/resources" / f"{name}.cl").read_text()
+    for tok, repl in {**PLACEHOLDERS, **PLACEHOLDERS_3D}.items():
+        src = replace_first(src, tok, repl)
+    for a, b in GLOBAL_3D_REPAIRS[name]:
+        if a not in src:
+            raise RuntimeError(f"repair target {a!r} not found in {name}.cl")
+        src = src.replace(a, b)
+    ks = sorted({ellipsoid_k(*s) for s in SIZES_3D})
+    call = ", ".join(f"(float*){a}" for a in args)
+    params = ", ".join(f"const float* {a}" if a in ("img", "means", "stds") else f"float* {a}" for a in args)
+    cases = "\n".join(f"    case {k}: rs_loop<{k}>(pix, npix, {', '.join(args)}); break;" for k in ks)
+    undef = "".join(f"#undef {m}\n" for m in MACROS + MACROS_3D)
+    return f"""#include "shim.h"
+#include <cfloat>
+using std::fmax;
+namespace rsns_{name} {{
+#define kernel template <int RS_KT> static inline
+{src}
+{undef}
+template <int KT>
+static void rs_loop(const int* pix, int npix, {params}) {{
+  #pragma omp parallel for schedule(dynamic, 1)
+  for (int i = 0; i < npix; i++) {{
+    rs_gid[0] = pix[i] % RS_W;
+    rs_gid[1] = (pix[i] / RS_W) % RS_H;
+    rs_gid[2] = pix[i] / (RS_W * RS_H);
+    {name}<KT>({call});
+  }}
+}}
+}}  // namespace rsns_{name}
+
+extern "C" int rs_{name}(int K, int W, int H, int D, int bw, int bh, int bd, float filter, float threshold,
+                       float eps, const int* pix, int npix, {params}) {{
+  using namespace rsns_{name};
+  RS_W = W; RS_H = H; RS_D = D; RS_BW = bw; RS_BH = bh; RS_BZ = bd;
+  RS_BRW = bw / 2; RS_BRH = bh / 2; RS_BRZ = bd / 2;
+  RS_FILTER = filter; RS_THRESHOLD = threshold; RS_EPSILON = eps;
   switch (K) {{
 {cases}
     default: return -1;
@@ -288,6 +355,7 @@ def build_refshim(ref: Path, force: bool = False) -> Path | None:
     units = {n: gen_unit(ref, n, ks) for n in KERNELS}
     units.update({n: gen_shape_unit(ref, n) for n in SHAPE_KERNELS})
     units.update({n: gen_unit_3d(ref, n) for n in KERNELS_3D})
+    units.update({n: gen_unit_3d_global(ref, n) for n in KERNELS_3D_GLOBAL})
     digest = hashlib.sha256(("".join(units.values()) + (HERE / "shim.h").read_text()
                              + (HERE / "shim_shape.h").read_text()).encode()).hexdigest()
     stamp = REF_OUT / "build.sha256"

@@ -1278,3 +1278,255 @@ void orc_block3d_postprocess_f32(int metric, float *map, int W, int H, int D, in
     if (normalize) orc_normalize_image3d(map, W, H, D, rw, rh, rd, mask);
     free(mask);
 }
+
+/* ------------------------------------------------------------------ */
+/* 3D global repetition maps                                           */
+/* ------------------------------------------------------------------ */
+
+/* cl/kernelGetGlobal{Pearson,Ssim,Nrmse,AbsDiffStds}3D.cl, FP32 in the kernels'
+ * order, for the reference voxels listed in pix (num/den indexed like pix).
+ * Differences from the 2D kernels that these kernels carry: a reference voxel
+ * with zero local variance is skipped (:37), NRMSE accumulates sqrt(mse) times
+ * the weight, Abs-diff skips test voxels of zero variance. Two defects are
+ * repaired: the reference block is gathered over z <= gz + bRZ (the kernels
+ * stop at z < gz + bRZ, :46, leaving the last slice's ellipsoid voxels at 0
+ * before the mean subtraction), and SSIM's below-threshold branch adds to its
+ * own map (kernelGetGlobalSsim3D.cl:76 names an undeclared pearson_map and
+ * does not compile). */
+void orc_global3d_f32(int metric, const float *img, int W, int H, int D, int bw, int bh, int bd,
+                      const float *means, const float *stds, float filter_param, float threshold,
+                      const int *pix, int n_pix, float *num, float *den) {
+    const int rw = bw / 2, rh = bh / 2, rd = bd / 2;
+    long *off = (long *)malloc(sizeof(long) * bw * bh * bd);
+    const int K = ellipsoid_offsets(bw, bh, bd, W, H, off);
+    const float c1 = 0.0001f, c2 = 0.0009f;
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int ii = 0; ii < n_pix; ii++) {
+        const long p = pix[ii];
+        const int gx = (int)(p % W), gy = (int)((p / W) % H), gz = (int)(p / ((long)W * H));
+        float S = 0.0f, Wsum = 0.0f;
+        float rb[4096], tb[4096];
+        num[ii] = 0.0f;
+        den[ii] = 0.0f;
+        if (!interior3d(gx, gy, gz, W, H, D, rw, rh, rd)) continue;
+        const float rs = stds[p];
+        const float rv = rs * rs;
+        if (rv < threshold || rv == 0.0f) continue;
+        const float rm = means[p];
+        if (metric != ORC_ABSDIFF)
+            for (int i = 0; i < K; i++) rb[i] = img[p + off[i]] - rm;
+        for (int z = rd; z < D - rd; z++)
+            for (int y = rh; y < H - rh; y++)
+                for (int x = rw; x < W - rw; x++) {
+                    const long q = (long)W * H * z + (long)y * W + x;
+                    const float ts = stds[q];
+                    const float tv = ts * ts;
+                    if (tv < threshold) continue;
+                    if (metric == ORC_ABSDIFF) {
+                        if (tv == 0.0f) continue;
+                        const float wgt = expf((-1.0f) * (((rs - ts) * (rs - ts)) / (filter_param + ORC_EPS)));
+                        Wsum += wgt;
+                        S += fmaxf(0.0f, fabsf(rs - ts)) * wgt;
+                        continue;
+                    }
+                    const float tm = means[q];
+                    for (int i = 0; i < K; i++) tb[i] = img[q + off[i]] - tm;
+                    const float wgt = expf((-1.0f) * (((rs - ts) * (rs - ts)) / (filter_param + ORC_EPS)));
+                    if (metric == ORC_NRMSE) {
+                        Wsum += wgt;
+                        float mse = 0.0f;
+                        for (int i = 0; i < K; i++) mse += (rb[i] - tb[i]) * (rb[i] - tb[i]);
+                        mse /= (float)K;
+                        S += sqrtf(mse) * wgt;
+                        continue;
+                    }
+                    float cov = 0.0f;
+                    for (int i = 0; i < K; i++) cov += rb[i] * tb[i];
+                    cov /= (float)(K - 1);
+                    Wsum += wgt;
+                    if (ts == 0.0f) {
+                        S += 0.0f;
+                    } else if (metric == ORC_PEARSON) {
+                        S += fmaxf(0.0f, cov / ((rs * ts) + ORC_EPS)) * wgt;
+                    } else {
+                        float ssim = ((2.0f * rm * tm + c1) * (2.0f * cov + c2)) /
+                                     (((rm * rm) * (tm * tm) + c1) * ((rs * rs) + (ts * ts) + c2)) * wgt;
+                        S += fmaxf(0.0f, ssim);
+                    }
+                }
+        num[ii] = S;
+        den[ii] = Wsum;
+    }
+    free(off);
+}
+
+/* The same sums in FP64 (the judge): block moments and vectors in FP64 from
+ * the FP32 voxels; relevance and flatness decisions on the FP32 stds. */
+void orc_global3d_f64(int metric, const float *img, int W, int H, int D, int bw, int bh, int bd,
+                      const float *stds32, float filter_param, float threshold, const int *pix, int n_pix,
+                      double *num, double *den) {
+    const int rw = bw / 2, rh = bh / 2, rd = bd / 2;
+    long *off = (long *)malloc(sizeof(long) * bw * bh * bd);
+    const int K = ellipsoid_offsets(bw, bh, bd, W, H, off);
+    long nint = (long)(W - 2 * rw > 0 ? W - 2 * rw : 0) * (H - 2 * rh > 0 ? H - 2 * rh : 0) *
+                (D - 2 * rd > 0 ? D - 2 * rd : 0);
+    long nq = 0;
+    long *qi = (long *)malloc(sizeof(long) * (size_t)(nint > 0 ? nint : 1));
+    for (int z = rd; z < D - rd; z++)
+        for (int y = rh; y < H - rh; y++)
+            for (int x = rw; x < W - rw; x++) {
+                const long q = (long)W * H * z + (long)y * W + x;
+                const float s = stds32[q];
+                if (s * s < threshold) continue;
+                if (metric == ORC_ABSDIFF && s * s == 0.0f) continue;
+                qi[nq++] = q;
+            }
+    double *qv = (double *)malloc(sizeof(double) * (size_t)(nq > 0 ? nq : 1) * K);
+    double *qm = (double *)malloc(sizeof(double) * (size_t)(nq > 0 ? nq : 1));
+    double *qs = (double *)malloc(sizeof(double) * (size_t)(nq > 0 ? nq : 1));
+    #pragma omp parallel for schedule(static)
+    for (long j = 0; j < nq; j++) {
+        const long q = qi[j];
+        double m = 0.0, v = 0.0;
+        for (int i = 0; i < K; i++) m += (double)img[q + off[i]];
+        m /= K;
+        for (int i = 0; i < K; i++) {
+            const double d = (double)img[q + off[i]] - m;
+            qv[(size_t)j * K + i] = d;
+            v += d * d;
+        }
+        qm[j] = m;
+        qs[j] = sqrt(v / (K - 1));
+    }
+    const double c1 = (double)0.0001f, c2 = (double)0.0009f;
+    const double h = (double)filter_param + (double)ORC_EPS;
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int ii = 0; ii < n_pix; ii++) {
+        const long p = pix[ii];
+        const int gx = (int)(p % W), gy = (int)((p / W) % H), gz = (int)(p / ((long)W * H));
+        num[ii] = 0;
+        den[ii] = 0;
+        if (!interior3d(gx, gy, gz, W, H, D, rw, rh, rd)) continue;
+        const float rs32 = stds32[p];
+        if (rs32 * rs32 < threshold || rs32 * rs32 == 0.0f) continue;
+        double rb[4096], rm = 0.0, rv = 0.0;
+        for (int i = 0; i < K; i++) rm += (double)img[p + off[i]];
+        rm /= K;
+        for (int i = 0; i < K; i++) {
+            rb[i] = (double)img[p + off[i]] - rm;
+            rv += rb[i] * rb[i];
+        }
+        const double rs = sqrt(rv / (K - 1));
+        double S = 0.0, Ws = 0.0;
+        for (long j = 0; j < nq; j++) {
+            const double *tb = qv + (size_t)j * K;
+            const double ts = qs[j], tm = qm[j];
+            const double wgt = exp(-((rs - ts) * (rs - ts)) / h);
+            Ws += wgt;
+            if (metric == ORC_ABSDIFF) {
+                S += fabs(rs - ts) * wgt;
+                continue;
+            }
+            if (metric == ORC_NRMSE) {
+                double mse = 0.0;
+                for (int i = 0; i < K; i++) {
+                    const double d = rb[i] - tb[i];
+                    mse += d * d;
+                }
+                S += sqrt(mse / K) * wgt;
+                continue;
+            }
+            if (stds32[qi[j]] == 0.0f) continue;
+            double cov = 0.0;
+            for (int i = 0; i < K; i++) cov += rb[i] * tb[i];
+            cov /= (K - 1);
+            if (metric == ORC_PEARSON) {
+                const double r = cov / (rs * ts + (double)ORC_EPS);
+                S += (r > 0.0 ? r : 0.0) * wgt;
+            } else {
+                const double s = ((2.0 * rm * tm + c1) * (2.0 * cov + c2)) /
+                                 ((rm * rm * tm * tm + c1) * (rs * rs + ts * ts + c2)) * wgt;
+                S += s > 0.0 ? s : 0.0;
+            }
+        }
+        num[ii] = S;
+        den[ii] = Ws;
+    }
+    free(off);
+    free(qi);
+    free(qv);
+    free(qm);
+    free(qs);
+}
+
+/* nPixels of the 3D command (java/GlobalRepetition3D_.java:132-143): 1.0f per
+ * interior voxel with mask > 0, summed in FP32. */
+float orc_n_pixels3d(const float *mask, int W, int H, int D, int rw, int rh, int rd) {
+    float n = 0.0f;
+    for (int z = rd; z < D - rd; z++)
+        for (int y = rh; y < H - rh; y++)
+            for (int x = rw; x < W - rw; x++)
+                if (mask[(long)W * H * z + (long)y * W + x] > 0.0f) n += 1.0f;
+    return n;
+}
+
+/* Host steps of getGlobal*3D (java/CLUtils.java:2225-2790) on a full W*H*D
+ * map of num/den: num / (den * nPixels + eps) over the interior; NRMSE and
+ * Abs-diff inverted where mask > 0 (0 -> 1); the mask applied when the
+ * relevance constant is > 0; normalizeImage3D over the mask (always given). */
+void orc_global3d_finalize_f32(int metric, const float *num, const float *den, int W, int H, int D, int rw,
+                               int rh, int rd, const float *mask, float relevance_constant, float n_pixels,
+                               int normalize, float *out) {
+    const long n = (long)W * H * D;
+    memset(out, 0, sizeof(float) * (size_t)n);
+    for (int z = rd; z < D - rd; z++)
+        for (int y = rh; y < H - rh; y++)
+            for (int x = rw; x < W - rw; x++) {
+                const long i = (long)W * H * z + (long)y * W + x;
+                out[i] = num[i] / (den[i] * n_pixels + ORC_EPS);
+            }
+    if (metric == ORC_NRMSE || metric == ORC_ABSDIFF)
+        for (int z = rd; z < D - rd; z++)
+            for (int y = rh; y < H - rh; y++)
+                for (int x = rw; x < W - rw; x++) {
+                    const long i = (long)W * H * z + (long)y * W + x;
+                    if (mask[i] > 0.0f) out[i] = (out[i] == 0.0f) ? 1.0f : 1.0f / out[i];
+                }
+    if (relevance_constant > 0.0f)
+        for (long i = 0; i < n; i++) out[i] *= mask[i];
+    if (normalize) orc_normalize_image3d(out, W, H, D, rw, rh, rd, mask);
+}
+
+/* The same steps in FP64 on FP64 sums (the judge's map). */
+void orc_global3d_finalize_f64(int metric, const double *num, const double *den, int W, int H, int D, int rw,
+                               int rh, int rd, const float *mask, float relevance_constant, double n_pixels,
+                               int normalize, double *out) {
+    const long n = (long)W * H * D;
+    memset(out, 0, sizeof(double) * (size_t)n);
+    for (int z = rd; z < D - rd; z++)
+        for (int y = rh; y < H - rh; y++)
+            for (int x = rw; x < W - rw; x++) {
+                const long i = (long)W * H * z + (long)y * W + x;
+                out[i] = num[i] / (den[i] * n_pixels + (double)ORC_EPS);
+                if ((metric == ORC_NRMSE || metric == ORC_ABSDIFF) && mask[i] > 0.0f)
+                    out[i] = (out[i] == 0.0) ? 1.0 : 1.0 / out[i];
+            }
+    if (relevance_constant > 0.0f)
+        for (long i = 0; i < n; i++) out[i] *= (double)mask[i];
+    if (!normalize) return;
+    double mn = DBL_MAX, mx = -DBL_MAX;
+    for (int z = rd; z < D - rd; z++)
+        for (int y = rh; y < H - rh; y++)
+            for (int x = rw; x < W - rw; x++) {
+                const long i = (long)W * H * z + (long)y * W + x;
+                if (!(mask[i] > 0.0f)) continue;
+                if (out[i] < mn) mn = out[i];
+                if (out[i] > mx) mx = out[i];
+            }
+    for (int z = rd; z < D - rd; z++)
+        for (int y = rh; y < H - rh; y++)
+            for (int x = rw; x < W - rw; x++) {
+                const long i = (long)W * H * z + (long)y * W + x;
+                if (mask[i] > 0.0f) out[i] = (out[i] - mn) / (mx - mn + (double)ORC_EPS);
+            }
+}

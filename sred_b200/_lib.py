@@ -28,7 +28,7 @@ EXPORTS = [
     "sred_global_map_2d_shard_sums", "sred_global_map_2d_shard_finish", "sred_set_log_callback",
     "sred_gat_2d", "sred_gat_objective_2d", "sred_gat_fit_2d", "sred_block_size_3d", "sred_reference_block_3d",
     "sred_local_statistics_3d", "sred_relevance_mask_3d", "sred_calculate_block_repetition_map_3d",
-    "sred_block_map_3d_device",
+    "sred_block_map_3d_device", "sred_calculate_global_repetition_map_3d", "sred_global_map_3d_device",
 ]
 
 
@@ -114,6 +114,10 @@ def load() -> C.CDLL:
                                                              f, f, f, s, _f32p]
         L.sred_block_map_3d_device.argtypes = [_vp, C.c_char_p, _vp, s, s, s, _f32p, s, s, s, s, f, f, f, s, _vp,
                                                _vp]
+        L.sred_calculate_global_repetition_map_3d.argtypes = [_vp, C.c_char_p, _f32p, s, s, s, s, s, s, f, s, _f32p,
+                                                              C.POINTER(RunInfo)]
+        L.sred_global_map_3d_device.argtypes = [_vp, C.c_char_p, _vp, s, s, s, s, s, s, f, s, _vp, _vp,
+                                                C.POINTER(RunInfo)]
         _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
         L.sred_debug_gram_rowdot.argtypes = [_vp, s, _f32p, _f32p, _f32p, s, s, _f64p, _f64p]
         L.sred_block_map_2d_device_noalloc.argtypes = [C.c_char_p, _vp, s, s, s, _f32p, s, s, s, C.c_float,

@@ -364,3 +364,35 @@ def block_map_3d_device(metric: str, d_vol_ptr: int, width: int, height: int, de
         np.ascontiguousarray(rb.pixels, np.float32).ravel(), int(rb.size), rb.width, rb.height, rb.depth,
         float(rb.mean), float(rb.std), float(relevance_constant), int(bool(normalize_output)),
         C.c_void_p(d_out_ptr), C.c_void_p(stream_ptr or None)), "sred_block_map_3d_device")
+
+
+def calculate_global_repetition_map_3d(metric: str, input_image: InputImage3D, block_width: int, block_height: int,
+                                       block_depth: int, relevance_constant: float, normalize_output: bool = True,
+                                       ctx=None, return_info: bool = False):
+    """java/CLUtils.java:2793-2816 with the preprocessing of
+    java/GlobalRepetition3D_.java:97-143 (local statistics, the 3D relevance
+    mask, nPixels) done inside libsred. None for an unknown metric; with
+    ``return_info`` a (map, run info) pair."""
+    if metric not in GLOBAL_METRICS:
+        return None
+    c = _ctx(ctx)
+    out = np.zeros(input_image.size, np.float32)
+    info = _lib.RunInfo()
+    c.check(c._L.sred_calculate_global_repetition_map_3d(
+        c.h, metric.encode(), np.ascontiguousarray(input_image.image_array, np.float32).ravel(), input_image.width,
+        input_image.height, input_image.depth, block_width, block_height, block_depth, float(relevance_constant),
+        int(bool(normalize_output)), out, C.byref(info)), "sred_calculate_global_repetition_map_3d")
+    return (out, info.as_dict()) if return_info else out
+
+
+def global_map_3d_device(metric: str, d_vol_ptr: int, width: int, height: int, depth: int, block_width: int,
+                         block_height: int, block_depth: int, relevance_constant: float, normalize_output: bool,
+                         d_out_ptr: int, stream_ptr: int = 0, ctx=None) -> dict:
+    """3D global map on device-resident buffers (raw CUDA pointers); returns run info."""
+    c = _ctx(ctx)
+    info = _lib.RunInfo()
+    c.check(c._L.sred_global_map_3d_device(c.h, metric.encode(), C.c_void_p(d_vol_ptr), width, height, depth,
+                                           block_width, block_height, block_depth, float(relevance_constant),
+                                           int(bool(normalize_output)), C.c_void_p(d_out_ptr),
+                                           C.c_void_p(stream_ptr or None), C.byref(info)), "sred_global_map_3d_device")
+    return info.as_dict()

@@ -15,7 +15,15 @@ constexpr int kMaxK = 512;          // largest ellipse block size accepted
 
 enum Metric { kPearson = 0, kSsim = 1, kNrmse = 2, kAbsDiff = 3, kCosine = 4,
               kDebugDot = 5 /* diagnostics: num += G a_p a_q, den += r_p + r_q */,
-              kHu = 6, kPhase = 7 /* block-map shape metrics */ };
+              kHu = 6, kPhase = 7 /* block-map shape metrics */,
+              kNrmseW = 8 /* NRMSE with each term weighted (the 3D global kernel) */,
+              // NRMSE from the accumulated squared difference of the unit
+              // vectors (FP32 engine): unweighted (2D) and weighted (3D)
+              kNrmseD = 9, kNrmseDW = 10 };
+
+// The FP32 engine's accumulator holds sum_i (u_p,i - u_q,i)^2 instead of the
+// dot product for these metrics.
+__host__ __device__ constexpr bool diff_metric(int m) { return m == kNrmseD || m == kNrmseDW; }
 
 // Ellipse pixel offsets (dx, dy), row-major ellipse order, as the kernels gather them.
 struct Ellipse {
@@ -41,6 +49,33 @@ struct BlockParams {
   float mu;     // mu64
   float pad0, pad1, pad2;
 };
+
+// Split-BF16 operands of the tensor-core engine, u = hi + mid (+ lo), each
+// part the BF16 rounding of what the previous parts leave of u:
+//   two levels:   A = [hi|mid|hi], B = [hi|hi|mid] (3K columns); the products
+//                 carry about 16 significand bits (dot-product error up to
+//                 ~1e-5 for unit vectors);
+//   three levels: A = [hi|mid|lo|hi|mid|hi], B = [hi|hi|hi|mid|mid|lo] (6K
+//                 columns); every product down to 2^-18 relative, an FP32-level
+//                 dot product. Used while 6K fits in 128 columns, where the
+//                 tiles are bound by the epilogue and the deeper MMA is free.
+inline int split_levels(int K) { return 6 * K <= 128 ? 3 : 2; }
+inline int split_cols(int K) { return split_levels(K) == 3 ? (6 * K + 31) / 32 * 32 : (3 * K + 31) / 32 * 32; }
+
+__device__ __forceinline__ void store_split(__nv_bfloat16* a, __nv_bfloat16* b, int K, int i, double u,
+                                            int levels) {
+  const __nv_bfloat16 hi = __float2bfloat16_rn((float)u);
+  const double r = u - (double)__bfloat162float(hi);
+  const __nv_bfloat16 mid = __float2bfloat16_rn((float)r);
+  if (levels == 2) {
+    a[i] = hi; a[K + i] = mid; a[2 * K + i] = hi;
+    b[i] = hi; b[K + i] = hi; b[2 * K + i] = mid;
+    return;
+  }
+  const __nv_bfloat16 lo = __float2bfloat16_rn((float)(r - (double)__bfloat162float(mid)));
+  a[i] = hi; a[K + i] = mid; a[2 * K + i] = lo; a[3 * K + i] = hi; a[4 * K + i] = mid; a[5 * K + i] = hi;
+  b[i] = hi; b[K + i] = hi; b[2 * K + i] = hi; b[3 * K + i] = mid; b[4 * K + i] = mid; b[5 * K + i] = lo;
+}
 
 // Epilogue constants shared by all tiles of one map.
 struct EpiConsts {

@@ -94,10 +94,17 @@ __device__ __forceinline__ void pair_terms(float G, const RowState& rp, const Bl
     const float num = fmaf(rp.mu2x2, cq.mu, ec.c1) * fmaf(rp.sig2x * cq.sigma, G, ec.c2);
     const float den = fmaf(rp.mumu, cq.mu * cq.mu, ec.c1) * fmaf(cq.sigma, cq.sigma, rp.s2);
     tn = fmaxf(__fdividef(num, den) * w, 0.0f);
-  } else if (METRIC == kNrmse) {
+  } else if (METRIC == kNrmse || METRIC == kNrmseW) {
     const float ds = rp.sigma - cq.sigma;
     const float m = ec.nrmse_scale * fmaf(ds, ds, rp.sig2x * cq.sigma * (1.0f - G));
     tn = sqrtf(fmaxf(m, 0.0f));
+    if (METRIC == kNrmseW) tn *= w;
+  } else if (METRIC == kNrmseD || METRIC == kNrmseDW) {
+    // G holds |u_p - u_q|^2 = 2 (1 - <u_p, u_q>): both terms are >= 0, so
+    // near-identical blocks lose nothing to cancellation.
+    const float ds = rp.sigma - cq.sigma;
+    tn = sqrtf(ec.nrmse_scale * fmaf(ds, ds, rp.sigma * cq.sigma * G));
+    if (METRIC == kNrmseDW) tn *= w;
   } else {  // Abs-diff of stds
     tn = fabsf(rp.sigma - cq.sigma) * w;
   }

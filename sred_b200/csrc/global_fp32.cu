@@ -9,7 +9,9 @@
 // accumulators with one atomic per row per item.
 //
 // This is the comparison form for the tensor-core engine: the same moments,
-// compaction, work split and epilogue, with FFMA contraction.
+// compaction, work split and epilogue, with FFMA contraction. For NRMSE it
+// accumulates |u_p - u_q|^2 instead (diff_metric), the form without
+// cancellation for near-identical blocks; NRMSE always runs here.
 #include <algorithm>
 
 #include "common.cuh"
@@ -64,7 +66,7 @@ __device__ __forceinline__ void tile_epilogue(const float (&acc)[TM][TM], const 
     for (int j = 0; j < TM; j++) {
       const int c = tx * TM + j;
       float G = acc[i][j];
-      if (DIAG && col0 + c == row0 + ty * TM + i && rs.r > 0.0f) G = 1.0f;
+      if (!diff_metric(METRIC) && DIAG && col0 + c == row0 + ty * TM + i && rs.r > 0.0f) G = 1.0f;
       if (FULL || col0 + c < ec.n) epi_pair<METRIC, CMODE>(G, rs, colp[c], ec, sn, sd);
     }
     rn[i] += sn;
@@ -121,7 +123,14 @@ __global__ void __launch_bounds__(NT, 2) k_gram_fp32(Fp32Args g) {
 #pragma unroll
           for (int i = 0; i < TM; i++)
 #pragma unroll
-            for (int j = 0; j < TM; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+            for (int j = 0; j < TM; j++) {
+              if (diff_metric(METRIC)) {
+                const float d = a[i] - b[j];
+                acc[i][j] = fmaf(d, d, acc[i][j]);
+              } else {
+                acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+              }
+            }
         }
       }
       const bool full = col0 + BM <= g.ec.n;
@@ -198,6 +207,9 @@ cudaError_t launch_gram_fp32(const float* U, int kp, const BlockParams* params, 
     case kPearson: SRED_LAUNCH(kPearson); break;
     case kSsim: SRED_LAUNCH(kSsim); break;
     case kNrmse: SRED_LAUNCH(kNrmse); break;
+    case kNrmseW: SRED_LAUNCH(kNrmseW); break;
+    case kNrmseD: SRED_LAUNCH(kNrmseD); break;
+    case kNrmseDW: SRED_LAUNCH(kNrmseDW); break;
     case kDebugDot: SRED_LAUNCH(kDebugDot); break;
     default: SRED_LAUNCH(kAbsDiff); break;
   }

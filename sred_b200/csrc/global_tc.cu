@@ -654,7 +654,6 @@ cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int k
   switch (ec.metric) {
     case kPearson: SRED_TC(kPearson); break;
     case kSsim: SRED_TC(kSsim); break;
-    case kNrmse: SRED_TC(kNrmse); break;
     case kDebugDot: SRED_TC(kDebugDot); break;
     default: return cudaErrorInvalidValue;
   }

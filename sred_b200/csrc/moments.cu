@@ -232,8 +232,9 @@ __global__ void k_scatter(const uint8_t* __restrict__ flags, size_t n, const int
 //   sums[0] = sum_q 2^-(a_q)^2           (weight of a pair with a flat block)
 //   sums[1] = sum_q sqrt((K-1)/K) sigma_q (NRMSE against a flat block)
 //   sums[2] = sum_q sigma_q 2^-(a_q)^2     (Abs-diff against a flat block)
-// mode 0: U (fp32, row pitch kp). mode 1: A = [hi|lo|hi], B = [hi|hi|lo]
-// (bf16, row pitch kq). Rows [n, n_pad) are zero-filled by the host.
+// mode 0: U (fp32, row pitch kp). mode 1 / 2: the two- / three-level split
+// BF16 operands A, B (store_split; row pitch kq). Rows [n, n_pad) are
+// zero-filled by the host.
 // ---------------------------------------------------------------------------
 __global__ void k_pack(const float* __restrict__ img, int W, Ellipse e, const int* __restrict__ gram_pix,
                        int n, float wscale, int mode, float* __restrict__ U, int kp,
@@ -264,21 +265,13 @@ __global__ void k_pack(const float* __restrict__ img, int W, Ellipse e, const in
     const double sigma = sqrt(v / (K - 1));
     for (int i = lane; i < K; i += 32) {
       double u = ((double)img[(size_t)(y + e.dy[i]) * W + (x + e.dx[i])] - mu) * inv;
-      if (mode == 0) {
-        U[(size_t)j * kp + i] = (float)u;
-      } else {
-        __nv_bfloat16 hi = __float2bfloat16_rn((float)u);
-        __nv_bfloat16 lo = __float2bfloat16_rn((float)(u - (double)__bfloat162float(hi)));
-        __nv_bfloat16* a = A + (size_t)j * kq;
-        __nv_bfloat16* b = B + (size_t)j * kq;
-        a[i] = hi; a[K + i] = lo; a[2 * K + i] = hi;
-        b[i] = hi; b[K + i] = hi; b[2 * K + i] = lo;
-      }
+      if (mode == 0) U[(size_t)j * kp + i] = (float)u;
+      else store_split(A + (size_t)j * kq, B + (size_t)j * kq, K, i, u, mode + 1);
     }
     if (mode == 0) {
       for (int i = K + lane; i < kp; i += 32) U[(size_t)j * kp + i] = 0.0f;
     } else {
-      for (int i = 3 * K + lane; i < kq; i += 32) {
+      for (int i = (mode == 1 ? 3 : 6) * K + lane; i < kq; i += 32) {
         A[(size_t)j * kq + i] = __float2bfloat16_rn(0.0f);
         B[(size_t)j * kq + i] = __float2bfloat16_rn(0.0f);
       }

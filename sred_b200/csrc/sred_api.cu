@@ -273,10 +273,10 @@ sred_status global_prepare(sred_ctx* c, int metric, const float* d_img, int w, i
   const float npx = given ? given->n_pixels : java_float_count(nmask);
 
   // Operands and per-block parameters of the all-pairs contraction.
-  const int engine = (metric == kAbsDiff) ? SRED_ENGINE_FP32 : c->engine;
+  const int engine = (metric == kAbsDiff || metric == kNrmse) ? SRED_ENGINE_FP32 : c->engine;
   const size_t n_pad = round_up((size_t)std::max(n_g, 1), 256);
   const int kp = (int)round_up(K, 4);
-  const int kq = (int)round_up(3 * K, 32);  // K' of the split-BF16 operands (tail of 0 or 32 columns)
+  const int kq = split_cols(K);  // K' of the split-BF16 operands
   float* d_U = nullptr;
   __nv_bfloat16 *d_A = nullptr, *d_B = nullptr;
   BlockParams* d_params;
@@ -307,8 +307,9 @@ sred_status global_prepare(sred_ctx* c, int metric, const float* d_img, int w, i
   const float wscale = (float)std::sqrt(1.4426950408889634 / (double)hden);
   if (n_g > 0) {
     const int pgrid = grid_for((size_t)n_g * 32, 256, 8 * c->num_sms);
-    k_pack<<<pgrid, 256, 0, st>>>(d_img, w, e, d_gpix, n_g, wscale, engine == SRED_ENGINE_FP32 ? 0 : 1, d_U,
-                                  kp, d_A, d_B, kq, d_params, d_rmax, d_sums);
+    const int mode = engine == SRED_ENGINE_FP32 ? 0 : split_levels(K) - 1;
+    k_pack<<<pgrid, 256, 0, st>>>(d_img, w, e, d_gpix, n_g, wscale, mode, d_U, kp, d_A, d_B, kq, d_params,
+                                  d_rmax, d_sums);
     CK(cudaGetLastError());
   }
   if (engine == SRED_ENGINE_TC) {
@@ -346,6 +347,9 @@ sred_status global_gram(sred_ctx* c, const GState& gs, cudaStream_t st, int rb_b
   if (gs.n_g > 0) {
     EpiConsts ec;
     ec.metric = gs.metric;
+    // NRMSE runs on the FP32 engine in its difference form
+    if (ec.metric == kNrmse) ec.metric = kNrmseD;
+    else if (ec.metric == kNrmseW) ec.metric = kNrmseDW;
     ec.n = gs.n_g;
     ec.nrmse_scale = (float)((double)(gs.K - 1) / (double)gs.K);
     ec.c1 = kC1;
@@ -635,6 +639,162 @@ sred_status block3d_core(sred_ctx* c, int metric, const float* d_vol, int w, int
   return SRED_OK;
 }
 
+// The 3D global repetition map on a device-resident volume
+// (java/GlobalRepetition3D_.java:97-158, java/CLUtils.java:2225-2816): local
+// statistics, the relevance mask of getRelevanceMask3D (the command passes
+// the 2D mask, which fails on its first interior slice), the compacted block
+// lists, the all-pairs contraction on the 2D engines, the 3D host steps.
+sred_status global3d_core(sred_ctx* c, int metric, const float* d_vol, int w, int h, int d, int bw, int bh, int bd,
+                          float relc, int normalize, float* d_out, cudaStream_t st, sred_run_info* info) {
+  c->shard.valid = false;  // shares workspaces with the 2D global map
+  if (fault("launch")) return fail(c, SRED_ERR_LAUNCH, "injected launch failure");
+  CK(cudaEventRecord(c->ev[0], st));
+  Vol3 v;
+  int* d_off;
+  CKS(prepare_volume(c, w, h, d, bw, bh, bd, st, &v, &d_off));
+  if (v.k > kMaxK) return fail(c, SRED_ERR_ARG, "ellipsoid block size above 512 for the global map");
+  const size_t n = (size_t)w * h * d;
+  if (n > (size_t)INT32_MAX / 2) return fail(c, SRED_ERR_ARG, "volume too large");
+  const int K = v.k;
+  float *d_means, *d_stds, *d_mask;
+  CKS(ensure(c, B_MEANS, n, &d_means));
+  CKS(ensure(c, B_STDS, n, &d_stds));
+  CKS(ensure(c, B_MASK, n, &d_mask));
+  const dim3 grid = vol_grid(v), blk(32, 4);
+  k_local_stats3d<<<grid, blk, sizeof(int) * K, st>>>(d_vol, v, d_off, d_means, d_stds);
+  CK(cudaGetLastError());
+  std::vector<float> h_stds(n);
+  CK(cudaMemcpyAsync(h_stds.data(), d_stds, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  const float nv = noise_var_3d(v, h_stds.data());
+  const bool has_interior = w > 2 * v.rw && h > 2 * v.rh && d > 2 * v.rd;
+  if (has_interior && !std::isfinite(nv))
+    return fail(c, SRED_ERR_INVALID_INPUT, "Input contains invalid (NaN or Infinite) values.");
+  const float thr = nv * relc;
+
+  uint8_t* d_flags;
+  int *d_slot, *d_gpix, *d_fpix;
+  int2* d_counts;
+  unsigned long long* d_nmask;
+  const int nseg = (int)((n + kCompactSeg - 1) / kCompactSeg);
+  CKS(ensure(c, B_FLAGS, n, &d_flags));
+  CKS(ensure(c, B_SLOT, n, &d_slot));
+  CKS(ensure(c, B_GPIX, n, &d_gpix));
+  CKS(ensure(c, B_FPIX, n, &d_fpix));
+  CKS(ensure(c, B_COUNTS, nseg + 1, &d_counts));
+  CKS(ensure(c, B_NMASK, 1, &d_nmask));
+  CK(cudaMemsetAsync(d_nmask, 0, sizeof(unsigned long long), st));
+  k_flags3d<<<grid, blk, 0, st>>>(d_stds, v, thr, metric == kAbsDiff ? 0 : 1, d_mask, d_flags, d_nmask);
+  k_count<<<nseg, 256, 0, st>>>(d_flags, n, d_counts);
+  k_scan<<<1, 1024, 0, st>>>(d_counts, nseg);
+  k_scatter<<<nseg, 256, 0, st>>>(d_flags, n, d_counts, d_gpix, d_fpix, d_slot);
+  CK(cudaGetLastError());
+  int2 tot;
+  unsigned long long nmask = 0;
+  CK(cudaMemcpyAsync(&tot, d_counts + nseg, sizeof(int2), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&nmask, d_nmask, sizeof(nmask), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  const int n_g = tot.x, n_flat = tot.y;
+  const float npx = java_float_count(nmask);
+
+  const int engine = (metric == kAbsDiff || metric == kNrmse) ? SRED_ENGINE_FP32 : c->engine;
+  const size_t n_pad = round_up((size_t)std::max(n_g, 1), 256);
+  const int kp = (int)round_up(K, 4);
+  const int kq = split_cols(K);
+  float* d_U = nullptr;
+  __nv_bfloat16 *d_A = nullptr, *d_B = nullptr;
+  BlockParams* d_params;
+  float* d_rmax;
+  double *d_num, *d_den;
+  CKS(ensure(c, B_PARAMS, n_pad, &d_params));
+  CKS(ensure(c, B_RMAX, n_pad / 128, &d_rmax));
+  CKS(ensure(c, B_NUM, n_pad, &d_num));
+  CKS(ensure(c, B_DEN, n_pad, &d_den));
+  if (engine == SRED_ENGINE_FP32) {
+    CKS(ensure(c, B_U, n_pad * kp, &d_U));
+    CK(cudaMemsetAsync(d_U + (size_t)n_g * kp, 0, (n_pad - n_g) * kp * sizeof(float), st));
+  } else {
+    CKS(ensure(c, B_A, n_pad * kq, &d_A));
+    CKS(ensure(c, B_B, n_pad * kq, &d_B));
+    CK(cudaMemsetAsync(d_A + (size_t)n_g * kq, 0, (n_pad - n_g) * kq * sizeof(__nv_bfloat16), st));
+    CK(cudaMemsetAsync(d_B + (size_t)n_g * kq, 0, (n_pad - n_g) * kq * sizeof(__nv_bfloat16), st));
+  }
+  CK(cudaMemsetAsync(d_params + n_g, 0, (n_pad - n_g) * sizeof(BlockParams), st));
+  CK(cudaMemsetAsync(d_rmax, 0, (n_pad / 128) * sizeof(float), st));
+  CK(cudaMemsetAsync(d_num, 0, n_pad * sizeof(double), st));
+  CK(cudaMemsetAsync(d_den, 0, n_pad * sizeof(double), st));
+  // weight = exp(-(s_p - s_q)^2 / (FILTER_PARAM + EPSILON)) = 2^-(a_p - a_q)^2
+  const float hden = nv + kEps;
+  const float wscale = (float)std::sqrt(1.4426950408889634 / (double)hden);
+  if (n_g > 0) {
+    k_pack3d<<<grid_for((size_t)n_g * 32, 256, 8 * c->num_sms), 256, 0, st>>>(
+        d_vol, v, d_off, d_gpix, n_g, wscale, engine == SRED_ENGINE_FP32 ? 0 : split_levels(K) - 1, d_U, kp, d_A,
+        d_B, kq, d_params, d_rmax);
+    CK(cudaGetLastError());
+  }
+  if (engine == SRED_ENGINE_TC) {
+    float* d_colsoa;
+    CKS(ensure(c, B_COLSOA, (n_pad / 256) * kColSoaFloats, &d_colsoa));
+    k_col_soa<<<(int)(n_pad / 256), 256, 0, st>>>(d_params, d_colsoa);
+    CK(cudaGetLastError());
+  }
+  CK(cudaEventRecord(c->ev[1], st));
+  GState gs;
+  gs.metric = metric == kNrmse ? kNrmseW : metric;
+  gs.K = K;
+  gs.n_g = n_g;
+  gs.engine = engine;
+  gs.kp = kp;
+  gs.kq = kq;
+  gs.n_pad = n_pad;
+  CKS(global_gram(c, gs, st, 0, -1));
+  k_finalize3d<<<grid, blk, 0, st>>>(d_slot, v, d_num, d_den, d_params, n_flat, metric,
+                                     std::sqrt((double)(K - 1) / (double)K), (double)npx, d_mask,
+                                     relc > 0.0f ? 1 : 0, d_out);
+  CK(cudaGetLastError());
+  if (normalize) {
+    unsigned* mm;
+    CKS(ensure(c, B_MM, 2, &mm));
+    const unsigned init[2] = {0xffffffffu, 0u};
+    CK(cudaMemcpyAsync(mm, init, sizeof(init), cudaMemcpyHostToDevice, st));
+    k_minmax3d<<<grid, blk, 0, st>>>(d_out, d_mask, v, mm);
+    k_remap3d<<<grid, blk, 0, st>>>(d_out, d_mask, v, mm);
+    CK(cudaGetLastError());
+  }
+  CK(cudaEventRecord(c->ev[3], st));
+  CK(cudaEventSynchronize(c->ev[3]));
+  if (info) {
+    info->n_blocks = (int64_t)std::max(0, w - 2 * v.rw) * std::max(0, h - 2 * v.rh) * std::max(0, d - 2 * v.rd);
+    info->n_relevant = (int64_t)n_g + n_flat;
+    info->n_flat = n_flat;
+    info->pairs = (double)n_g * (double)info->n_relevant;
+    info->noise_var = nv;
+    info->threshold = thr;
+    info->n_pixels = npx;
+    info->k = K;
+    info->engine = engine;
+    float t01 = 0, t12 = 0, t23 = 0, t03 = 0;
+    cudaEventElapsedTime(&t01, c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&t12, c->ev[1], c->ev[2]);
+    cudaEventElapsedTime(&t23, c->ev[2], c->ev[3]);
+    cudaEventElapsedTime(&t03, c->ev[0], c->ev[3]);
+    info->ms_moments = t01;
+    info->ms_gram = t12;
+    info->ms_finalize = t23;
+    info->ms_total = t03;
+    info->launches = 5 + (n_g > 0 ? (engine == SRED_ENGINE_TC ? 3 : 2) : 0) + 1 + (normalize ? 2 : 0);
+  }
+  if (c->log_cb) {
+    float t03 = 0;
+    cudaEventElapsedTime(&t03, c->ev[0], c->ev[3]);
+    char line[256];
+    std::snprintf(line, sizeof(line), "global map %dx%dx%d K=%d: %d reference blocks, %d flat test blocks, %s engine, %.3f ms",
+                  w, h, d, K, n_g, n_flat, engine == SRED_ENGINE_TC ? "tensor-core" : "fp32", t03);
+    log_msg(c, line);
+  }
+  return SRED_OK;
+}
+
 cudaStream_t pick(sred_ctx* c, void* s) { return s ? (cudaStream_t)s : c->stream; }
 
 }  // namespace
@@ -839,7 +999,7 @@ sred_status reserve_global(sred_ctx* c, const sred_job* jobs, int n_jobs) {
     const size_t np = round_up(std::max<size_t>(inter, 1), 256);
     n = std::max(n, (size_t)j.w * j.h);
     n_pad = std::max(n_pad, np);
-    a = std::max(a, np * round_up(3 * K, 32));
+    a = std::max(a, np * (size_t)split_cols(K));
     u = std::max(u, np * round_up(K, 4));
     cols = std::max(cols, (np / 256) * kColSoaFloats);
     if (global_metric(j.metric) == kAbsDiff) fp32 = true;
@@ -1511,6 +1671,37 @@ sred_status sred_block_map_3d_device(sred_ctx* c, const char* metric, const floa
   cudaSetDevice(c->device);
   return block3d_core(c, m, d_vol, w, h, d, ref_pixels, block_size, bw, bh, bd, ref_mean, ref_std, relc, normalize,
                       d_out, pick(c, stream));
+}
+
+sred_status sred_calculate_global_repetition_map_3d(sred_ctx* c, const char* metric, const float* vol, int w,
+                                                    int h, int d, int bw, int bh, int bd, float relc, int normalize,
+                                                    float* out, sred_run_info* info) {
+  if (!c || !vol || !out) return SRED_ERR_ARG;
+  const int m = global_metric(metric);
+  if (m < 0) return fail(c, SRED_ERR_UNKNOWN_METRIC, "unknown global metric");
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (w <= 0 || h <= 0 || d <= 0) return fail(c, SRED_ERR_ARG, "bad dimensions");
+  const size_t n = (size_t)w * h * d;
+  float *d_vol, *d_out;
+  CKS(ensure(c, B_IMG, n, &d_vol));
+  CKS(ensure(c, B_OUT, n, &d_out));
+  CK(cudaMemcpyAsync(d_vol, vol, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  CKS(global3d_core(c, m, d_vol, w, h, d, bw, bh, bd, relc, normalize, d_out, c->stream, info));
+  CK(cudaMemcpyAsync(out, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SRED_OK;
+}
+
+sred_status sred_global_map_3d_device(sred_ctx* c, const char* metric, const float* d_vol, int w, int h, int d,
+                                      int bw, int bh, int bd, float relc, int normalize, float* d_out, void* stream,
+                                      sred_run_info* info) {
+  if (!c || !d_vol || !d_out) return SRED_ERR_ARG;
+  const int m = global_metric(metric);
+  if (m < 0) return fail(c, SRED_ERR_UNKNOWN_METRIC, "unknown global metric");
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  return global3d_core(c, m, d_vol, w, h, d, bw, bh, bd, relc, normalize, d_out, pick(c, stream), info);
 }
 
 }  // extern "C"

@@ -204,6 +204,129 @@ __global__ void k_remap3d(float* __restrict__ a, const float* __restrict__ mask,
   a[p] = (a[p] - mn) / (mx - mn + kEps);
 }
 
+// ---------------------------------------------------------------------------
+// 3D global repetition map: flags, operand packing and finalisation around
+// the 2D pair engines (cl/kernelGetGlobal*3D.cl, java/CLUtils.java:2225-2790).
+// ---------------------------------------------------------------------------
+
+// mask: sigma^2 > threshold on the interior (getRelevanceMask3D).
+// flags: 1 = reference and test block (interior, !(sigma^2 < threshold),
+// sigma^2 != 0: the 3D kernels skip a reference voxel of zero variance);
+// 2 = test block only, sigma == 0 (a flat block still counts as a test block
+// of Pearson, SSIM and NRMSE; flat_columns = 0 drops it, as Abs-diff does).
+// A voxel with sigma != 0 but sigma^2 == 0 (sigma below 1.1e-23) is neither;
+// the reference would still use it as a test block.
+// n_mask counts mask > 0 (the command's nPixels).
+__global__ void k_flags3d(const float* __restrict__ stds, Vol3 v, float thr, int flat_columns,
+                          float* __restrict__ mask, uint8_t* __restrict__ flags,
+                          unsigned long long* __restrict__ n_mask) {
+  int x, y, z;
+  size_t p;
+  unsigned c = 0;
+  if (voxel(v, &x, &y, &z, &p)) {
+    const bool in = interior3(x, y, z, v);
+    const float s = stds[p];
+    const float s2 = s * s;
+    const float m = (in && !(s2 <= thr)) ? 1.0f : 0.0f;
+    mask[p] = m;
+    uint8_t f = 0;
+    if (in && !(s2 < thr)) {
+      if (s2 != 0.0f) f = 1;
+      else if (s == 0.0f && flat_columns) f = 2;
+    }
+    flags[p] = f;
+    c = m > 0.0f ? 1u : 0u;
+  }
+  const unsigned wc = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0 && wc) atomicAdd(n_mask, (unsigned long long)wc);
+}
+
+// One warp per listed block: FP64 moments of its ellipsoid vector, the unit
+// vector (x - mu) / |x - mu| as FP32 (mode 0, row pitch kp) or as the two- /
+// three-level split BF16 operands (mode 1 / 2, store_split, row pitch kq),
+// and the epilogue parameters; the same quantities as the 2D packing, over
+// linear offsets.
+__global__ void k_pack3d(const float* __restrict__ img, Vol3 v, const int* __restrict__ off,
+                         const int* __restrict__ gram_pix, int n, float wscale, int mode, float* __restrict__ U,
+                         int kp, __nv_bfloat16* __restrict__ A, __nv_bfloat16* __restrict__ B, int kq,
+                         BlockParams* __restrict__ params, float* __restrict__ tile_rmax) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int K = v.k;
+  for (int j = gw; j < n; j += nw) {
+    const float* c = img + (size_t)gram_pix[j];
+    double s = 0.0;
+    for (int i = lane; i < K; i += 32) s += (double)c[off[i]];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const double mu = s / K;
+    double var = 0.0;
+    for (int i = lane; i < K; i += 32) {
+      const double d = (double)c[off[i]] - mu;
+      var += d * d;
+    }
+    for (int o = 16; o; o >>= 1) var += __shfl_xor_sync(0xffffffffu, var, o);
+    const double nrm = sqrt(var);
+    const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+    const double sigma = sqrt(var / (K - 1));
+    for (int i = lane; i < K; i += 32) {
+      const double u = ((double)c[off[i]] - mu) * inv;
+      if (mode == 0) U[(size_t)j * kp + i] = (float)u;
+      else store_split(A + (size_t)j * kq, B + (size_t)j * kq, K, i, u, mode + 1);
+    }
+    if (mode == 0) {
+      for (int i = K + lane; i < kp; i += 32) U[(size_t)j * kp + i] = 0.0f;
+    } else {
+      for (int i = (mode == 1 ? 3 : 6) * K + lane; i < kq; i += 32) {
+        A[(size_t)j * kq + i] = __float2bfloat16_rn(0.0f);
+        B[(size_t)j * kq + i] = __float2bfloat16_rn(0.0f);
+      }
+    }
+    if (lane == 0) {
+      BlockParams bp;
+      bp.a = (float)(sigma * (double)wscale);
+      bp.e = sigma > 0.0 ? (float)((double)kEps / sigma) : 0.0f;
+      bp.r = sigma > 0.0 ? (float)(1.0 / sigma) : 0.0f;
+      bp.sigma = (float)sigma;
+      bp.mu = (float)mu;
+      bp.pad0 = bp.pad1 = bp.pad2 = 0.0f;
+      params[j] = bp;
+      atomicMax(reinterpret_cast<int*>(tile_rmax) + (j >> 7), __float_as_int(bp.r));
+    }
+  }
+}
+
+// num / (den nPixels + eps) in FP64 over the interior, with the flat test
+// blocks' closed-form share: n_flat pairs of weight 2^-(a_p^2) each, and for
+// NRMSE a term sqrt((K-1)/K) sigma_p per pair times that weight (the flat
+// block's centred vector is zero). NRMSE and Abs-diff are then inverted where
+// mask > 0 (the FP32 value; 0 -> 1), and the mask applied when apply_mask.
+__global__ void k_finalize3d(const int* __restrict__ slot, Vol3 v, const double* __restrict__ num,
+                             const double* __restrict__ den, const BlockParams* __restrict__ params, int n_flat,
+                             int metric, double sk, double n_pixels, const float* __restrict__ mask, int apply_mask,
+                             float* __restrict__ out) {
+  int x, y, z;
+  size_t p;
+  if (!voxel(v, &x, &y, &z, &p)) return;
+  float o = 0.0f;
+  if (interior3(x, y, z, v)) {
+    const int s = slot[p];
+    double nu = 0.0, de = 0.0;
+    if (s >= 0) {
+      const BlockParams bp = params[s];
+      const double a = (double)bp.a;
+      const double w0 = exp2(-(a * a));
+      nu = num[s];
+      de = den[s] + (double)n_flat * w0;
+      if (metric == kNrmse) nu += (double)n_flat * sk * (double)bp.sigma * w0;
+    }
+    o = (float)(nu / (de * n_pixels + (double)kEps));
+    if ((metric == kNrmse || metric == kAbsDiff) && mask[p] > 0.0f) o = (o == 0.0f) ? 1.0f : 1.0f / o;
+    if (apply_mask) o *= mask[p];
+  }
+  out[p] = o;
+}
+
 int build_ellipsoid(int bw, int bh, int bd, int W, int H, int* off) {
   const int rw = bw / 2, rh = bh / 2, rd = bd / 2;
   int k = 0;

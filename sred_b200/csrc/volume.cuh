@@ -29,4 +29,14 @@ __global__ void k_mask3d(const float* stds, Vol3 v, float thr, float* mask, floa
 __global__ void k_minmax3d(const float* a, const float* mask, Vol3 v, unsigned* mm);
 __global__ void k_remap3d(float* a, const float* mask, Vol3 v, const unsigned* mm);
 
+// 3D global map (the 2D pair engines run on the compacted block lists).
+__global__ void k_flags3d(const float* stds, Vol3 v, float thr, int flat_columns, float* mask, uint8_t* flags,
+                          unsigned long long* n_mask);
+__global__ void k_pack3d(const float* img, Vol3 v, const int* off, const int* gram_pix, int n, float wscale,
+                         int mode, float* U, int kp, __nv_bfloat16* A, __nv_bfloat16* B, int kq,
+                         BlockParams* params, float* tile_rmax);
+__global__ void k_finalize3d(const int* slot, Vol3 v, const double* num, const double* den,
+                             const BlockParams* params, int n_flat, int metric, double sk, double n_pixels,
+                             const float* mask, int apply_mask, float* out);
+
 }  // namespace sred

@@ -23,7 +23,10 @@ Two kinds of fixtures are written:
    3D block-map kernels (``cl/kernelGetLocalStatistics3D.cl``,
    ``cl/kernelGetBlock{Pearson,Ssim,Nrmse,AbsDiffStds}3D.cl``), compiled the
    same way, on small seeded volumes, with the Java host steps of
-   ``getBlock*3D`` applied by the oracle. No reference test covers 3D.
+   ``getBlock*3D`` applied by the oracle; and for three of the volumes the
+   3D global maps of ``cl/kernelGetGlobal*3D.cl`` (with the two repairs listed
+   in ``oracle/refshim/build.py``) with the host steps of ``getGlobal*3D``.
+   No reference test covers 3D.
 
 Usage: ``python tests/golden/make_golden.py [--reference /root/reference] [--only volume ...]``
 """
@@ -229,6 +232,11 @@ VOLUME_CASES = [
 ]
 
 
+# cases whose 3D global maps (the reference's 3D global kernels with their two
+# repairs, see oracle/refshim/build.py) are frozen too
+GLOBAL_VOLUME_CASES = ("spots28x24x12_3x3x3", "spots24x24x16_5x5x5", "flat24x20x10_3x3x3")
+
+
 def flat_volume() -> np.ndarray:
     """Volume with exactly flat regions (the std == 0 special cases)."""
     v = np.zeros((10, 20, 24), np.float32)
@@ -263,6 +271,12 @@ def volume_fixtures() -> dict:
                 r = oracle.block_map3d(metric, vol, px, bw, bh, bd, bm, bs, c, True, use_refshim=True)
                 fx[f"{name}/{metric}/raw"] = r["raw"]  # the kernel's output does not depend on c
                 fx[f"{name}/c{c:g}/{metric}/map"] = r["map"]
+        if name in GLOBAL_VOLUME_CASES:
+            for c in (0.0, 1.0):
+                for metric in oracle.GLOBAL_METRICS:
+                    g = oracle.global_map3d(metric, vol, bw, bh, bd, c, True, use_refshim=True)
+                    fx[f"{name}/global/c{c:g}/{metric}/map"] = g["map"]
+                fx[f"{name}/global/c{c:g}/n_pixels"] = g["n_pixels"]
     return fx
 
 

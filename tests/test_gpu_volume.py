@@ -1,4 +1,4 @@
-"""Parity of the 3D block repetition maps through the C ABI.
+"""Parity of the 3D block and global repetition maps through the C ABI.
 
 References: the reference's 3D kernels compiled for the CPU
 (cl/kernelGetLocalStatistics3D.cl, cl/kernelGetBlock{Pearson,Ssim,Nrmse,
@@ -6,10 +6,11 @@ AbsDiffStds}3D.cl) with the Java host steps of getBlock*3D applied, frozen in
 tests/golden/volume_refshim.npz, and the oracle's restatement of both at
 sizes beyond the fixtures.
 
-Bar: bit-exact. The device code runs the kernels' FP32 operations in their
-order without fused multiply-adds, and the host steps (noise variance as an
-FP32 raster-order sum, relevance mask, normalisation) exactly as the
-reference's Java does.
+Bar for the block maps: bit-exact. The device code runs the kernels' FP32
+operations in their order without fused multiply-adds, and the host steps
+(noise variance as an FP32 raster-order sum, relevance mask, normalisation)
+exactly as the reference's Java does. The global maps sum in FP64 and are
+held to the 2D global map's bars (below).
 """
 import numpy as np
 import pytest
@@ -128,3 +129,79 @@ def test_block_map_3d_edges(ctx):
     bad = utils.ReferenceBlock3D(rb.pixels, 3, 3, 3, 1, 1, 1, rb.size + 1, rb.mean, rb.std)
     with pytest.raises(_lib.SredError):
         clutils.calculate_block_repetition_map_3d("SSIM", vol, bad, 0.0, True, ctx=ctx)
+
+
+# --------------------------------------------------------------------------
+# 3D global maps: against the reference's 3D global kernels (two repairs)
+# frozen in volume_refshim.npz, and against the FP64 judge. Bars as for the
+# 2D global map: within 1e-5 of FP64 (or 1.25 x the reference's own FP32
+# deviation from it) and within 2e-5 + that deviation of the reference.
+# --------------------------------------------------------------------------
+
+GLOBAL_TOL = 1e-5
+REF_TOL = 2e-5
+
+
+def _global3d(ctx, engine, metric, vol, bw, bh, bd, c, normalize=True):
+    ctx.set_engine(engine)
+    out, info = clutils.calculate_global_repetition_map_3d(metric, _inp(vol), bw, bh, bd, c, normalize, ctx=ctx,
+                                                           return_info=True)
+    return out.reshape(vol.shape), info
+
+
+@pytest.mark.parametrize("engine", ["fp32", "tc"])
+@pytest.mark.parametrize("metric", clutils.GLOBAL_METRICS)
+def test_global_map_3d_vs_reference_and_fp64(ctx, volume_fx, engine, metric):
+    n = 0
+    for name, bw, bh, bd in volume_cases(volume_fx):
+        if f"{name}/global/c0/{metric}/map" not in volume_fx:
+            continue
+        vol = volume_fx[f"{name}/volume"]
+        for c in (0.0, 1.0):
+            out, info = _global3d(ctx, engine, metric, vol, bw, bh, bd, c)
+            ref = volume_fx[f"{name}/global/c{c:g}/{metric}/map"]
+            j = oracle.global_map3d(metric, vol, bw, bh, bd, c, precision="f64")
+            assert info["n_pixels"] == volume_fx[f"{name}/global/c{c:g}/n_pixels"]
+            e_ref = float(np.max(np.abs(out - ref)))
+            e64 = float(np.max(np.abs(out - j["map"])))
+            e_ref64 = float(np.max(np.abs(ref - j["map"])))
+            assert e64 <= max(GLOBAL_TOL, 1.25 * e_ref64), (name, c, e64)
+            assert e_ref <= REF_TOL + e_ref64, (name, c, e_ref)
+            n += 1
+    assert n == 6
+
+
+@pytest.mark.parametrize("engine", ["fp32", "tc"])
+def test_global_map_3d_larger_volume(ctx, engine):
+    """Ragged 41x37x19 volume, 3x5x3 block, relevance 0.5, against FP64."""
+    vol = synth.normalize_input(synth.spot_volume(41, 37, 19, 5, 3, seed=12))
+    for metric in clutils.GLOBAL_METRICS:
+        out, info = _global3d(ctx, engine, metric, vol, 3, 5, 3, 0.5)
+        j = oracle.global_map3d(metric, vol, 3, 5, 3, 0.5, precision="f64")
+        assert info["n_relevant"] > 1000
+        assert float(np.max(np.abs(out - j["map"]))) <= GLOBAL_TOL, metric
+
+
+def test_global_map_3d_device_and_edges(ctx):
+    import torch
+    vol = synth.normalize_input(synth.spot_volume(20, 18, 9, 3, 2, seed=4))
+    d, h, w = vol.shape
+    ctx.set_engine("tc")
+    host = clutils.calculate_global_repetition_map_3d("SSIM", _inp(vol), 3, 3, 3, 1.0, True, ctx=ctx)
+    dv = torch.from_numpy(vol).cuda()
+    out = torch.empty_like(dv)
+    clutils.global_map_3d_device("SSIM", dv.data_ptr(), w, h, d, 3, 3, 3, 1.0, True, out.data_ptr(),
+                                 torch.cuda.current_stream().cuda_stream, ctx=ctx)
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy().ravel(), host)
+    # no interior: an all-zero map
+    thin = vol[:2].copy()
+    for metric in clutils.GLOBAL_METRICS:
+        got = clutils.calculate_global_repetition_map_3d(metric, _inp(thin), 3, 3, 3, 0.0, True, ctx=ctx)
+        assert np.array_equal(got, np.zeros(thin.size, np.float32)), metric
+    assert clutils.calculate_global_repetition_map_3d("Cosine", _inp(vol), 3, 3, 3, 0.0, True, ctx=ctx) is None
+    with pytest.raises(_lib.SredError):  # ellipsoid of 515 voxels
+        clutils.calculate_global_repetition_map_3d("SSIM", _inp(np.zeros((12, 12, 12), np.float32)), 11, 11, 11,
+                                                   0.0, True, ctx=ctx)
+    with pytest.raises(_lib.SredError):
+        clutils.calculate_global_repetition_map_3d("SSIM", _inp(vol), 3, 4, 3, 0.0, True, ctx=ctx)

@@ -365,3 +365,45 @@ def test_volume_matches_refshim_live():
             x = oracle.block_map3d(metric, vol, px, bw, bh, bd, bm, bs, 1.0)
             y = oracle.block_map3d(metric, vol, px, bw, bh, bd, bm, bs, 1.0, use_refshim=True)
             assert np.array_equal(x["raw"], y["raw"]) and np.array_equal(x["map"], y["map"]), metric
+
+
+# 3D global maps: the restatement against the reference's 3D global kernels
+# (two repairs, oracle/refshim/build.py), frozen in volume_refshim.npz
+
+def test_global3d_f32_matches_refshim_fixtures(volume_fx):
+    fx = volume_fx
+    n = 0
+    for name, bw, bh, bd in volume_cases(fx):
+        if f"{name}/global/c0/Pearson's R/map" not in fx:
+            continue
+        vol = fx[f"{name}/volume"]
+        for c in (0.0, 1.0):
+            for metric in oracle.GLOBAL_METRICS:
+                g = oracle.global_map3d(metric, vol, bw, bh, bd, c)
+                assert np.array_equal(g["map"], fx[f"{name}/global/c{c:g}/{metric}/map"]), (name, c, metric)
+                n += 1
+            assert g["n_pixels"] == fx[f"{name}/global/c{c:g}/n_pixels"]
+    assert n == 24
+
+
+def test_global3d_f64_judge_close_to_f32(volume_fx):
+    vol = volume_fx["spots28x24x12_3x3x3/volume"]
+    for metric in oracle.GLOBAL_METRICS:
+        for c in (0.0, 1.0):
+            a = oracle.global_map3d(metric, vol, 3, 3, 3, c)["map"]
+            b = oracle.global_map3d(metric, vol, 3, 3, 3, c, precision="f64")["map"]
+            assert float(np.max(np.abs(a - b))) < 2e-5, (metric, c)
+
+
+@pytest.mark.skipif(oracle.refshim() is None, reason="refshim not built")
+def test_global3d_matches_refshim_live():
+    from sred_b200 import synth
+    vol = synth.normalize_input(synth.spot_volume(18, 16, 11, 3, 2, seed=78))
+    for bw, bh, bd in ((3, 5, 3), (7, 3, 5)):
+        means, stds = oracle.local_stats3d(vol, bw, bh, bd)
+        mask, nv = oracle.relevance_mask3d(stds, bw, bh, bd, 0.5)
+        thr = np.float32(nv * np.float32(0.5))
+        for metric in oracle.GLOBAL_METRICS:
+            a = oracle.global3d_sums_f32(metric, vol, bw, bh, bd, means, stds, nv, thr)
+            b = oracle.global3d_sums_f32(metric, vol, bw, bh, bd, means, stds, nv, thr, use_refshim=True)
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), (bw, bh, bd, metric)
