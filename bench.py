@@ -262,7 +262,7 @@ def run_ours(args, rank, local, world):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "bf16x3 split (hi/lo) tensor-core Gram, f32 accumulate, f64 moments" if args.engine == "tc"
+        "dtype": "bf16x3 split (hi/lo) tensor-core Gram, f32 accumulate, f64 moments" if r["info"]["engine"] == 0
                  else "f32 CUDA-core Gram, f64 moments",
         "data": "synthetic (seeded spot image, numpy default_rng; no dataset)",
         "config": {"workload": WORKLOAD, "image": f"{W_IMG}x{H_IMG}", "block": f"{BW}x{BH}", "K": K,
@@ -273,7 +273,7 @@ def run_ours(args, rank, local, world):
         "gpu_launches": r["launches"],
         "clocks": r["clocks"],
     }
-    if args.engine == "tc":
+    if r["info"]["engine"] == 0:  # tensor-core engine
         eff_peak = pk["bf16_tflops_sustained"] / 3.0
         achieved = per_launch_pairs * 2 * K / gram_s / 1e12
         line["roofline"] = {
@@ -298,7 +298,7 @@ def run_ours(args, rank, local, world):
 
 def traffic_from_profile():
     """ncu DRAM bytes per Gram launch, recorded for the default workload only."""
-    if (W_IMG, H_IMG, BW, BH, RELC) != (1024, 1024, 9, 9, 1.0):
+    if (W_IMG, H_IMG, BW, BH, RELC, SIM) != (1024, 1024, 9, 9, 1.0, "Pearson's R"):
         return None
     p = ROOT / "profiles" / "traffic.json"
     if p.exists():
@@ -468,6 +468,103 @@ def run_volume(args, rank, local, world):
     print(json.dumps(line), flush=True)
 
 
+def run_volume_global(args, rank, local, world):
+    """3D global repetition map: a 192x192x64 spot volume (9.4 MB), 5x5x5
+    block (ellipsoid K=33), relevance constant 1.0, Pearson's R, normalised;
+    L2 flushed between steps. Reports block-pairs/s (reference voxels x test
+    voxels per second) over the whole call; the tensor-core Gram kernel is
+    the dominant kernel."""
+    import torch
+    from sred_b200 import _lib, clutils, synth, utils
+    torch.cuda.set_device(local)
+    ctx = _lib.Context(local, args.engine)
+    vol = synth.normalize_input(synth.spot_volume(192, 192, 64, 24, 8, seed=rank))
+    D, H, W = vol.shape
+    b, relc, metric = 5, 1.0, "Pearson's R"
+    d_in = torch.from_numpy(vol).cuda()
+    d_out = torch.empty_like(d_in)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()
+    for _ in range(args.warmup):
+        clutils.global_map_3d_device(metric, d_in.data_ptr(), W, H, D, b, b, b, relc, True, d_out.data_ptr(),
+                                     stream.cuda_stream, ctx=ctx)
+    torch.cuda.synchronize()
+    ms, gram_ms, launches, info = [], [], 0, None
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            info = clutils.global_map_3d_device(metric, d_in.data_ptr(), W, H, D, b, b, b, relc, True,
+                                                d_out.data_ptr(), stream.cuda_stream, ctx=ctx)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            gram_ms.append(info["ms_gram"])
+            launches += info["launches"]
+    total_ms = max_over_ranks(sum(ms), world)
+    pairs = sum_over_ranks(info["pairs"] * args.steps, world)
+    # end to end: host volume in, host map out
+    inp = utils.InputImage3D(vol.ravel(), W, H, D)
+    e2e = []
+    for _ in range(max(2, args.steps // 2)):
+        t0 = time.perf_counter()
+        clutils.calculate_global_repetition_map_3d(metric, inp, b, b, b, relc, True, ctx=ctx)
+        e2e.append(time.perf_counter() - t0)
+    e2e_total = max_over_ranks(sum(e2e), world)
+    e2e_pairs = sum_over_ranks(info["pairs"] * len(e2e), world)
+    if rank != 0:
+        return
+    pk = peaks()
+    K = info["k"]
+    gram_s = statistics.mean(gram_ms) / 1e3
+    line = {"metric": "3D global-map block-pairs/s at 192x192x64/5x5x5", "value": pairs / (total_ms / 1e3),
+            "unit": "block-pairs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16x3 split tensor-core Gram, f32 accumulate, f64 sums" if args.engine == "tc"
+                     else "f32 CUDA-core Gram, f64 sums",
+            "data": "synthetic (seeded spot volume, numpy default_rng; no dataset)",
+            "config": {"workload": "3D global repetition map, 192x192x64 float32 spot volume (24x24x8 lattice), "
+                                   f"5x5x5 block (ellipsoid K={K}), Pearson's R, relevance constant 1.0",
+                       "engine": args.engine, "relevant_blocks": info["n_relevant"],
+                       "pairs_per_step": info["pairs"],
+                       "l2": "flushed between steps (256 MiB write, outside the timed region)"},
+            "gpu_launches": launches, "clocks": clk.summary(),
+            "e2e": {"value": e2e_pairs / e2e_total, "unit": "block-pairs/s", "h2d_bytes_per_step": vol.nbytes,
+                    "d2h_bytes_per_step": vol.nbytes, "ms_per_step": 1e3 * e2e_total / len(e2e)}}
+    if args.engine == "tc":
+        eff_peak = pk["bf16_tflops_sustained"] / 3.0
+        achieved = info["pairs"] * 2 * K / gram_s / 1e12
+        line["roofline"] = {"bound": "tensor", "achieved": achieved, "peak": eff_peak, "unit": "TFLOP/s",
+                            "frac": achieved / eff_peak, "traffic": None,
+                            "note": f"all-pairs Gram kernel; algorithmic FLOPs = pairs x 2K (K={K}); peak = "
+                                    f"{pk['source']} sustained BF16 / 3"}
+    if not args.no_cpu_baseline:
+        import oracle
+        kind = "reference" if oracle.refshim() is not None else "port"
+        cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+        means, stds = oracle.local_stats3d(vol, b, b, b)
+        mask, nv = oracle.relevance_mask3d(stds, b, b, b, relc)
+        thr = np.float32(nv * np.float32(relc))
+        rel = np.flatnonzero(mask.ravel() > 0).astype(np.int32)
+        rng = np.random.default_rng(5)
+        rows = rng.choice(rel, size=min(rel.size, 2 * cores), replace=False).astype(np.int32)
+        t0 = time.perf_counter()
+        oracle.global3d_sums_f32(metric, vol, b, b, b, means, stds, nv, thr, rows, use_refshim=(kind == "reference"))
+        dt = time.perf_counter() - t0
+        n_rows = int(max(cores, min(rel.size, 12.0 / max(dt, 1e-6) * rows.size)))
+        rows = rng.choice(rel, size=n_rows, replace=False).astype(np.int32)
+        t0 = time.perf_counter()
+        oracle.global3d_sums_f32(metric, vol, b, b, b, means, stds, nv, thr, rows, use_refshim=(kind == "reference"))
+        dt = time.perf_counter() - t0
+        test_blocks = int(np.count_nonzero(stds.ravel() ** 2 >= thr) )
+        line["cpu_baseline"] = {"value": rows.size * test_blocks / dt, "unit": "block-pairs/s", "cores": cores,
+                                "kind": kind, "sample": f"{rows.size} reference voxels x all {test_blocks} test "
+                                                        f"voxels ({dt:.1f} s); rate extrapolates per pair"}
+    print(json.dumps(line), flush=True)
+
+
 def run_shard(args, rank, local, world):
     """One global map of the default workload split by rows across the ranks
     (strong scaling): every rank prepares the same image, computes the sums
@@ -603,9 +700,12 @@ def main():
     ap.add_argument("--engine", choices=["tc", "fp32"], default="tc")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP32-engine comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["global", "block", "batch", "volume"], default="global",
+    ap.add_argument("--workload", choices=["global", "block", "batch", "volume", "volume-global"],
+                    default="global",
                     help="global repetition map (default, the headline), the block (local) map, batched "
-                         "global maps of many images, or the 3D block map of a volume")
+                         "global maps of many images, the 3D block map of a volume, or the 3D global map")
+    ap.add_argument("--metric", default="Pearson's R",
+                    help="metric of the global workload (the reference's names; default Pearson's R)")
     ap.add_argument("--mode", choices=["replicas", "shard"], default="replicas",
                     help="global workload on N GPUs: independent replicas (default, weak scaling) or one map "
                          "row-sharded across the GPUs (strong scaling)")
@@ -617,7 +717,11 @@ def main():
     ap.add_argument("--block", type=int, default=9, help="block side of the global workload (default 9)")
     ap.add_argument("--relevance", type=float, default=1.0, help="relevance constant of the global workload")
     args = ap.parse_args()
-    global W_IMG, H_IMG, WORKLOAD, BW, BH, METRIC, RELC
+    global W_IMG, H_IMG, WORKLOAD, BW, BH, METRIC, RELC, SIM
+    if args.metric != SIM:
+        SIM = args.metric
+        WORKLOAD = WORKLOAD.replace("Pearson's R", SIM)
+        METRIC = METRIC.replace("global-map", f"global-map ({SIM})")
     if args.size == 256:
         W_IMG = H_IMG = 256
         WORKLOAD = ("global repetition map, 256x256 float32 spot image (20x20 lattice, 400 spots), "
@@ -651,6 +755,8 @@ def main():
             run_block(args, rank, local, world)
         elif args.workload == "volume":
             run_volume(args, rank, local, world)
+        elif args.workload == "volume-global":
+            run_volume_global(args, rank, local, world)
         elif args.workload == "batch":
             run_batch(args, rank, local, world)
         elif args.mode == "shard":

@@ -32,9 +32,12 @@ typedef enum {
     SRED_ERR_INVALID_INPUT = 8   /* NaN/Inf pixel in a noise tile (java/Utils.java:886-889) */
 } sred_status;
 
-/* Contraction engine of the global map. SRED_ENGINE_TC: split-BF16 (hi/lo)
- * tcgen05 tensor-core Gram with FP32 accumulation; SRED_ENGINE_FP32: plain
- * FP32 CUDA-core Gram. Both share moments, tiling and the fused epilogue. */
+/* Contraction engine of the global map. SRED_ENGINE_TC: split-BF16 tcgen05
+ * tensor-core Gram with FP32 accumulation (u = hi + mid, or hi + mid + lo
+ * when 6K <= 128); SRED_ENGINE_FP32: plain FP32 CUDA-core Gram. Both share
+ * moments, tiling and the fused epilogue. NRMSE and Abs-diff always run on
+ * the FP32 engine (NRMSE accumulates |u_p - u_q|^2 directly: the dot-product
+ * form cancels for near-identical blocks). */
 typedef enum { SRED_ENGINE_TC = 0, SRED_ENGINE_FP32 = 1 } sred_engine;
 
 typedef struct sred_ctx sred_ctx;
