@@ -378,6 +378,42 @@ sred_status sred_global_map_3d_device(sred_ctx *ctx, const char *metric, const f
                                       int bw, int bh, int bd, float relevance_constant, int normalize_output,
                                       float *d_out, void *stream, sred_run_info *info);
 
+/* ---------------------------------------------------------------------
+ * Relevance-mask tools. The image is the one the ImageJ commands compute on:
+ * already variance-stabilised (sred_gat_2d) and min-max normalised (the
+ * commands normalise in FP64, java/RelevanceMask2D_.java). The block is the
+ * ellipse of bw x bh; the commands read the dialog's width and height into
+ * each other's radius (java/RelevanceMask2D_.java, bRW = bH / 2), which for a
+ * non-square block makes their kernel overrun its patch array, so only square
+ * blocks are comparable. Threshold: noise_var * c, or c when the noise
+ * variance is 0. A pixel is relevant (1) iff it is interior and s^2 is
+ * neither below the threshold nor 0.
+ * --------------------------------------------------------------------- */
+
+/* Replaces RelevanceMask2D_.run after its preprocessing: s = the local
+ * standard deviation (cl/kernelGetLocalMeans.cl), noise variance from 8x8 or
+ * 16x16 tiles with FP64 sums (its getMeanAndVarBlock). mask: w*h floats. */
+sred_status sred_relevance_mask_tool_2d(sred_ctx *ctx, const float *img, int w, int h, int bw, int bh,
+                                        float filter_constant, float *mask, float *threshold, float *noise_var);
+
+/* Replaces RelevanceMaskStack2D_.run after its preprocessing: n masks at the
+ * constants lower, lower + step, ... (FP32 accumulation; the command makes
+ * n = ceil((upper - lower) / step) + 1), s = the local variance
+ * (cl/kernelGetRelevanceMask2D.cl; the Java code squares it), noise variance
+ * from tiles with FP32 sums (OptimiseRelevanceMask_.getRelevanceMap).
+ * masks: n*w*h floats, constants: n floats; 1 <= n <= 65535. */
+sred_status sred_relevance_mask_sweep_2d(sred_ctx *ctx, const float *img, int w, int h, int bw, int bh, float lower,
+                                         float step, int n, float *masks, float *constants, float *noise_var);
+
+/* Replaces OptimiseRelevanceMask_.run after its preprocessing: steps the
+ * constant from 0 by `step` (FP32 accumulation) until the mask is all 0 and
+ * returns that constant (all_zeros) and the last one whose interior was all 1
+ * (all_ones, 0 if none); s and the noise variance as for the sweep. A step
+ * that stops increasing the constant is SRED_ERR_ARG (the reference loops
+ * forever). */
+sred_status sred_relevance_constant_range_2d(sred_ctx *ctx, const float *img, int w, int h, int bw, int bh,
+                                             float step, float *all_ones, float *all_zeros, float *noise_var);
+
 #ifdef __cplusplus
 }
 #endif

@@ -106,6 +106,13 @@ def lib() -> C.CDLL:
                                                 C.c_int, C.c_int, _f32p, C.c_float, C.c_float, C.c_int, _f32p]
         L.orc_global3d_finalize_f64.argtypes = [C.c_int, _f64p, _f64p, C.c_int, C.c_int, C.c_int, C.c_int,
                                                 C.c_int, C.c_int, _f32p, C.c_float, C.c_double, C.c_int, _f64p]
+        L.orc_local_var2d.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f32p]
+        L.orc_tool_noise_var.restype = C.c_int
+        L.orc_tool_noise_var.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _fp]
+        L.orc_tool_mask.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, _f32p]
+        L.orc_tool_range.restype = C.c_int
+        L.orc_tool_range.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int,
+                                     _fp, _fp]
         L.orc_gat_objective.restype = C.c_double
         L.orc_gat_objective.argtypes = [_f32p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
         L.orc_patch_hu1_ref.restype = C.c_double
@@ -646,3 +653,64 @@ def global_map3d(metric, vol, bw, bh, bd, relevance_constant, normalize=True, pr
     sh = (D, H, W)
     return {"map": out.reshape(sh), "num": nf.reshape(sh), "den": df.reshape(sh), "means": means,
             "stds": stds, "mask": mask, "threshold": thr, "noise_var": nv, "n_pixels": npx}
+
+
+# --------------------------------------------------------------------------
+# Relevance-mask tools (java/RelevanceMask2D_.java, RelevanceMaskStack2D_.java,
+# OptimiseRelevanceMask_.java)
+# --------------------------------------------------------------------------
+
+def local_var2d(img, bw, bh, take_sqrt, use_refshim=False):
+    """cl/kernelGetRelevanceMask2D.cl (variance) or cl/kernelGetLocalMeans.cl (std)."""
+    a = _f32(img)
+    H, W = a.shape
+    out = np.zeros(W * H, np.float32)
+    if use_refshim:
+        R = refshim()
+        K = block_size(bw, bh)
+        ys, xs = np.mgrid[bh // 2:H - bh // 2, bw // 2:W - bw // 2]
+        pix = np.ascontiguousarray((ys * W + xs).ravel(), np.int32)
+        if take_sqrt:
+            means = np.zeros(W * H, np.float32)
+            rc = R.rs_kernelGetLocalMeans(C.c_int(K), W, H, bw, bh, C.c_float(0), C.c_float(0), C.c_float(EPSILON),
+                                          C.c_float(0), C.c_float(0), pix.ctypes.data_as(C.c_void_p),
+                                          C.c_int(pix.size), a.ctypes.data_as(C.c_void_p),
+                                          means.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p))
+        else:
+            rc = R.rs_kernelGetRelevanceMask2D(C.c_int(K), W, H, bw, bh, C.c_float(0), C.c_float(0),
+                                               C.c_float(EPSILON), C.c_float(0), C.c_float(0),
+                                               pix.ctypes.data_as(C.c_void_p), C.c_int(pix.size),
+                                               a.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p))
+        if rc != 0:
+            raise ValueError(f"refshim has no instantiation for K={K}")
+    else:
+        lib().orc_local_var2d(a.ravel(), W, H, bw, bh, int(take_sqrt), out)
+    return out.reshape(H, W)
+
+
+def tool_noise_var(img, fp64):
+    a = _f32(img)
+    H, W = a.shape
+    v = C.c_float()
+    if lib().orc_tool_noise_var(a.ravel(), W, H, int(fp64), C.byref(v)) != 0:
+        raise ValueError("image smaller than one noise-variance tile")
+    return np.float32(v.value)
+
+
+def tool_mask(stat, bw, bh, nv, c):
+    s = _f32(stat)
+    H, W = s.shape
+    m = np.zeros(W * H, np.float32)
+    lib().orc_tool_mask(s.ravel(), W, H, bw // 2, bh // 2, C.c_float(nv), C.c_float(c), m)
+    return m.reshape(H, W)
+
+
+def tool_range(stat, bw, bh, nv, step, max_iter=100000):
+    s = _f32(stat)
+    H, W = s.shape
+    a, b = C.c_float(), C.c_float()
+    rc = lib().orc_tool_range(s.ravel(), W, H, bw // 2, bh // 2, C.c_float(nv), C.c_float(step), max_iter,
+                              C.byref(a), C.byref(b))
+    if rc != 0:
+        raise ValueError("the step never reaches an all-zero mask")
+    return np.float32(a.value), np.float32(b.value)

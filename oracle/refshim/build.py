@@ -43,6 +43,9 @@ KERNELS = {
     "kernelGetBlockSsim2D": ("b", ["ref", "img", "means", "stds", "map"]),
     "kernelGetBlockNrmse2D": ("b", ["ref", "img", "means", "map"]),
     "kernelGetBlockAbsDiffStds2D": ("b", ["stds", "map"]),
+    # relevance-mask tools: local variance and local std of the ellipse block
+    "kernelGetRelevanceMask2D": ("s", ["img", "stds"]),
+    "kernelGetLocalMeans": ("s", ["img", "means", "stds"]),
 }
 
 PLACEHOLDERS = {
@@ -50,10 +53,10 @@ PLACEHOLDERS = {
     "$BW$": "RS_BW", "$BH$": "RS_BH", "$BRW$": "RS_BRW", "$BRH$": "RS_BRH",
     "$FILTER_PARAM$": "RS_FILTER", "$THRESHOLD$": "RS_THRESHOLD",
     "$EPSILON$": "RS_EPSILON", "$BLOCK_STD$": "RS_BLOCK_STD",
-    "$BLOCK_MEAN$": "RS_BLOCK_MEAN",
+    "$BLOCK_MEAN$": "RS_BLOCK_MEAN", "$PATCH_SIZE$": "RS_KT",
 }
 MACROS = ["image_width", "image_height", "block_size", "bW", "bH", "bRW", "bRH",
-          "filter_param", "threshold", "EPSILON", "w", "h", "ref_std", "ref_mean", "kernel"]
+          "filter_param", "threshold", "EPSILON", "w", "h", "ref_std", "ref_mean", "kernel", "patch_size"]
 
 MAX_BLOCK = 15  # every odd block width/height 3..15 is instantiated
 

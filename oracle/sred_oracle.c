@@ -1530,3 +1530,117 @@ void orc_global3d_finalize_f64(int metric, const double *num, const double *den,
                 if (mask[i] > 0.0f) out[i] = (out[i] - mn) / (mx - mn + (double)ORC_EPS);
             }
 }
+
+/* ------------------------------------------------------------------ */
+/* Relevance-mask tools (java/RelevanceMask2D_.java,                    */
+/* java/RelevanceMaskStack2D_.java, java/OptimiseRelevanceMask_.java)   */
+/* ------------------------------------------------------------------ */
+
+/* cl/kernelGetRelevanceMask2D.cl (take_sqrt = 0: the local variance) and
+ * cl/kernelGetLocalMeans.cl (take_sqrt = 1: its square root) over the ellipse
+ * of a bw x bh block; border pixels 0 (the commands' buffers start at 0). */
+void orc_local_var2d(const float *img, int W, int H, int bw, int bh, int take_sqrt, float *out) {
+    const int rw = bw / 2, rh = bh / 2;
+    int *off = (int *)malloc(sizeof(int) * bw * bh);
+    const int K = ellipse_offsets(bw, bh, W, off);
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            const int p = y * W + x;
+            if (x < rw || x >= W - rw || y < rh || y >= H - rh) { out[p] = 0.0f; continue; }
+            float mean = 0.0f;
+            for (int i = 0; i < K; i++) mean += img[p + off[i]];
+            mean /= (float)K;
+            float var = 0.0f;
+            for (int i = 0; i < K; i++) var += (img[p + off[i]] - mean) * (img[p + off[i]] - mean);
+            var /= (float)(K - 1);
+            out[p] = take_sqrt ? sqrtf(var) : var;
+        }
+    free(off);
+}
+
+/* The tools' noise variance: tile variances with FP32 sums
+ * (OptimiseRelevanceMask_.getMeanAndVarBlock, fp64 = 0) or FP64 sums
+ * (RelevanceMask2D_.getMeanAndVarBlock, fp64 = 1), sorted, the lowest 3%
+ * averaged in FP32, then (1 + 0.001 (v - 40)) v. Returns -1 if the image has
+ * no tile. */
+int orc_tool_noise_var(const float *img, int W, int H, int fp64, float *out) {
+    const int wh = W * H, t = (wh <= 352 * 288) ? 8 : 16;
+    const int nbx = W / t, nby = H / t, nb = nbx * nby;
+    const int nv = (int)(0.03f * (float)nb + 1.0f);
+    if (nv > nb) return -1;
+    float *vars = (float *)malloc(sizeof(float) * (nb > 0 ? nb : 1));
+    for (int by = 0; by < nby; by++)
+        for (int bx = 0; bx < nbx; bx++) {
+            float var;
+            if (fp64) {
+                double mean = 0.0, sq = 0.0;
+                for (int y = by * t; y < (by + 1) * t; y++)
+                    for (int x = bx * t; x < (bx + 1) * t; x++) {
+                        const float v = img[y * W + x];
+                        mean += (double)v;
+                        sq += (double)(v * v);
+                    }
+                mean = mean / (t * t);
+                var = (float)(sq / (t * t) - mean * mean);
+            } else {
+                float mean = 0.0f, sq = 0.0f;
+                for (int y = by * t; y < (by + 1) * t; y++)
+                    for (int x = bx * t; x < (bx + 1) * t; x++) {
+                        const float v = img[y * W + x];
+                        mean += v;
+                        sq += v * v;
+                    }
+                mean = mean / (float)(t * t);
+                var = sq / (float)(t * t) - mean * mean;
+            }
+            vars[by * nbx + bx] = var;
+        }
+    qsort(vars, nb, sizeof(float), cmp_float);
+    float v = 0.0f;
+    for (int i = 0; i < nv; i++) v += vars[i];
+    v = fabsf(v / (float)nv);
+    *out = (1.0f + 0.001f * (v - 40.0f)) * v;
+    free(vars);
+    return 0;
+}
+
+/* OptimiseRelevanceMask_.getRelevanceMap's mask (also RelevanceMask2D_'s): an
+ * interior pixel is 1 unless s^2 < threshold or s^2 == 0; threshold = nv * c,
+ * or c when nv == 0. */
+void orc_tool_mask(const float *stat, int W, int H, int rw, int rh, float nv, float c, float *mask) {
+    const float thr = nv == 0.0f ? c : nv * c;
+    memset(mask, 0, sizeof(float) * (size_t)W * H);
+    for (int y = rh; y < H - rh; y++)
+        for (int x = rw; x < W - rw; x++) {
+            const float v = stat[y * W + x] * stat[y * W + x];
+            mask[y * W + x] = (v < thr || v == 0.0f) ? 0.0f : 1.0f;
+        }
+}
+
+/* OptimiseRelevanceMask_.run's loop, literally: whole masks at c = 0, step,
+ * ... until one is all 0. Returns -1 if the constant stops increasing (the
+ * reference would loop forever) or after max_iter masks. */
+int orc_tool_range(const float *stat, int W, int H, int rw, int rh, float nv, float step, int max_iter,
+                   float *all_ones, float *all_zeros) {
+    float *m = (float *)malloc(sizeof(float) * (size_t)W * H);
+    float fc = 0.0f, ones = 0.0f;
+    int it = 0, rc = -1;
+    for (; it < max_iter; it++) {
+        orc_tool_mask(stat, W, H, rw, rh, nv, fc, m);
+        int all1 = 1, all0 = 1;
+        for (int y = rh; y < H - rh && all1; y++)
+            for (int x = rw; x < W - rw; x++)
+                if (m[y * W + x] != 1.0f) { all1 = 0; break; }
+        for (int i = 0; i < W * H; i++)
+            if (m[i] != 0.0f) { all0 = 0; break; }
+        if (all1) ones = fc;
+        if (all0) { rc = 0; break; }
+        const float next = fc + step;
+        if (!(next > fc)) break;
+        fc = next;
+    }
+    free(m);
+    *all_ones = ones;
+    *all_zeros = fc;
+    return rc;
+}

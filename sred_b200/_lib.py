@@ -29,6 +29,7 @@ EXPORTS = [
     "sred_gat_2d", "sred_gat_objective_2d", "sred_gat_fit_2d", "sred_block_size_3d", "sred_reference_block_3d",
     "sred_local_statistics_3d", "sred_relevance_mask_3d", "sred_calculate_block_repetition_map_3d",
     "sred_block_map_3d_device", "sred_calculate_global_repetition_map_3d", "sred_global_map_3d_device",
+    "sred_relevance_mask_tool_2d", "sred_relevance_mask_sweep_2d", "sred_relevance_constant_range_2d",
 ]
 
 
@@ -118,6 +119,9 @@ def load() -> C.CDLL:
                                                               C.POINTER(RunInfo)]
         L.sred_global_map_3d_device.argtypes = [_vp, C.c_char_p, _vp, s, s, s, s, s, s, f, s, _vp, _vp,
                                                 C.POINTER(RunInfo)]
+        L.sred_relevance_mask_tool_2d.argtypes = [_vp, _f32p, s, s, s, s, f, _f32p, _fp, _fp]
+        L.sred_relevance_mask_sweep_2d.argtypes = [_vp, _f32p, s, s, s, s, f, f, s, _f32p, _f32p, _fp]
+        L.sred_relevance_constant_range_2d.argtypes = [_vp, _f32p, s, s, s, s, f, _fp, _fp, _fp]
         _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
         L.sred_debug_gram_rowdot.argtypes = [_vp, s, _f32p, _f32p, _f32p, s, s, _f64p, _f64p]
         L.sred_block_map_2d_device_noalloc.argtypes = [C.c_char_p, _vp, s, s, s, _f32p, s, s, s, C.c_float,

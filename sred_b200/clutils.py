@@ -396,3 +396,51 @@ def global_map_3d_device(metric: str, d_vol_ptr: int, width: int, height: int, d
                                            int(bool(normalize_output)), C.c_void_p(d_out_ptr),
                                            C.c_void_p(stream_ptr or None), C.byref(info)), "sred_global_map_3d_device")
     return info.as_dict()
+
+
+# ---------------------------------------------------------------------------
+# Relevance-mask tools on a preprocessed image (variance-stabilised and
+# min-max normalised); the commands themselves are in plugins.py.
+# ---------------------------------------------------------------------------
+
+def relevance_mask_tool_2d(image: np.ndarray, block_width: int, block_height: int, filter_constant: float,
+                           ctx=None) -> RelevanceMask:
+    """The mask of java/RelevanceMask2D_.java (local std, FP64 noise tiles)."""
+    c = _ctx(ctx)
+    a = np.ascontiguousarray(image, np.float32)
+    h, w = a.shape
+    mask = np.zeros(w * h, np.float32)
+    thr, nv = C.c_float(), C.c_float()
+    c.check(c._L.sred_relevance_mask_tool_2d(c.h, a.ravel(), w, h, block_width, block_height, float(filter_constant),
+                                             mask, C.byref(thr), C.byref(nv)), "sred_relevance_mask_tool_2d")
+    return RelevanceMask(mask.reshape(h, w), np.float32(filter_constant), np.float32(thr.value), np.float32(nv.value))
+
+
+def relevance_mask_sweep_2d(image: np.ndarray, block_width: int, block_height: int, lower: float, step: float,
+                            n: int, ctx=None) -> tuple:
+    """The n masks of java/RelevanceMaskStack2D_.java: (masks [n, h, w],
+    constants [n], noise variance)."""
+    c = _ctx(ctx)
+    a = np.ascontiguousarray(image, np.float32)
+    h, w = a.shape
+    masks = np.zeros(n * w * h, np.float32)
+    consts = np.zeros(n, np.float32)
+    nv = C.c_float()
+    c.check(c._L.sred_relevance_mask_sweep_2d(c.h, a.ravel(), w, h, block_width, block_height, float(lower),
+                                              float(step), int(n), masks, consts, C.byref(nv)),
+            "sred_relevance_mask_sweep_2d")
+    return masks.reshape(n, h, w), consts, np.float32(nv.value)
+
+
+def relevance_constant_range_2d(image: np.ndarray, block_width: int, block_height: int, step: float,
+                                ctx=None) -> tuple:
+    """java/OptimiseRelevanceMask_.java's result: (last constant with an
+    all-1 interior, first constant with an all-0 mask, noise variance)."""
+    c = _ctx(ctx)
+    a = np.ascontiguousarray(image, np.float32)
+    h, w = a.shape
+    ones, zeros, nv = C.c_float(), C.c_float(), C.c_float()
+    c.check(c._L.sred_relevance_constant_range_2d(c.h, a.ravel(), w, h, block_width, block_height, float(step),
+                                                  C.byref(ones), C.byref(zeros), C.byref(nv)),
+            "sred_relevance_constant_range_2d")
+    return np.float32(ones.value), np.float32(zeros.value), np.float32(nv.value)

@@ -15,6 +15,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "shape.cuh"
+#include "relevance.cuh"
 #include "volume.cuh"
 
 using namespace sred;
@@ -24,7 +25,7 @@ namespace {
 enum BufId {
   B_IMG, B_MEANS, B_STDS, B_MASK, B_MASKIN, B_FLAGS, B_SLOT, B_GPIX, B_FPIX, B_COUNTS, B_U, B_A, B_B,
   B_PARAMS, B_RMAX, B_NUM, B_DEN, B_SUMS, B_OUT, B_VARS, B_MM, B_NMASK, B_BAD, B_STATUS, B_STDS2, B_COLSOA,
-  B_FEAT, B_SIG, B_FR, B_FI, B_GAT, B_OFF3, B_REF3, B_NBUF
+  B_FEAT, B_SIG, B_FR, B_FI, B_GAT, B_OFF3, B_REF3, B_STAT, B_THR, B_NBUF
 };
 
 struct DevBuf {
@@ -795,6 +796,82 @@ sred_status global3d_core(sred_ctx* c, int metric, const float* d_vol, int w, in
   return SRED_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Relevance-mask tools (java/RelevanceMask2D_.java, RelevanceMaskStack2D_.java,
+// OptimiseRelevanceMask_.java)
+// ---------------------------------------------------------------------------
+
+// The tools' noise variance: t x t tile variances (t = 8 up to CIF size, else
+// 16), FP32 sums (OptimiseRelevanceMask_.getMeanAndVarBlock) or FP64 sums
+// (RelevanceMask2D_.getMeanAndVarBlock), sorted, the mean of the lowest 3% in
+// FP32, then (1 + 0.001 (v - 40)) v. No NaN check (the tools have none).
+sred_status tool_noise_var(sred_ctx* c, const float* d_img, int w, int h, bool fp64, cudaStream_t st, float* out) {
+  const int wh = w * h;
+  const int t = (wh <= 352 * 288) ? 8 : 16;
+  const int nbx = w / t, nby = h / t, nb = nbx * nby;
+  const int nv = (int)(0.03f * (float)nb + 1.0f);
+  if (nv > nb) return fail(c, SRED_ERR_ARG, "image smaller than one noise-variance tile");
+  float* d_vars;
+  int* d_bad;
+  CKS(ensure(c, B_VARS, nb, &d_vars));
+  CKS(ensure(c, B_BAD, 1, &d_bad));
+  if (fp64) {
+    k_noise_tiles64<<<grid_for(nb, 128, 1 << 30), 128, 0, st>>>(d_img, w, t, nbx, nb, d_vars);
+  } else {
+    k_noise_tiles<<<grid_for(nb, 128, 1 << 30), 128, 0, st>>>(d_img, w, t, nbx, nb, d_vars, d_bad);
+  }
+  CK(cudaGetLastError());
+  c->hvars.resize(nb);
+  CK(cudaMemcpyAsync(c->hvars.data(), d_vars, sizeof(float) * nb, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  std::sort(c->hvars.begin(), c->hvars.end());
+  float v = 0.0f;
+  for (int i = 0; i < nv; i++) v += c->hvars[i];
+  v = std::fabs(v / (float)nv);
+  *out = (1.0f + 0.001f * (v - 40.0f)) * v;
+  return SRED_OK;
+}
+
+// Uploads the image and computes the tools' block statistic (local std or
+// local variance) into B_STAT.
+sred_status tool_stat(sred_ctx* c, const float* img, int w, int h, int bw, int bh, int take_sqrt, Ellipse* e,
+                      float** d_img_out, float** d_stat_out) {
+  CKS(check_block(c, w, h, bw, bh, e));
+  const size_t n = (size_t)w * h;
+  float *d_img, *d_stat;
+  CKS(ensure(c, B_IMG, n, &d_img));
+  CKS(ensure(c, B_STAT, n, &d_stat));
+  CK(cudaMemcpyAsync(d_img, img, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  k_local_var2d<<<dim3((w + 127) / 128, h), 128, 0, c->stream>>>(d_img, w, h, *e, take_sqrt, d_stat);
+  CK(cudaGetLastError());
+  *d_img_out = d_img;
+  *d_stat_out = d_stat;
+  return SRED_OK;
+}
+
+// Threshold of the tools: noise_var * c, or c itself when the noise variance is 0.
+float tool_threshold(float nv, float c) { return nv == 0.0f ? c : nv * c; }
+
+sred_status tool_masks(sred_ctx* c, const float* d_stat, int w, int h, const Ellipse& e, const float* thr, int n,
+                       float* masks) {
+  float *d_thr, *d_masks;
+  const size_t px = (size_t)w * h;
+  // at most 256 MiB of masks on the device at a time
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)n, ((size_t)64 << 20) / px));
+  CKS(ensure(c, B_THR, n, &d_thr));
+  CKS(ensure(c, B_OUT, px * chunk, &d_masks));
+  CK(cudaMemcpyAsync(d_thr, thr, sizeof(float) * n, cudaMemcpyHostToDevice, c->stream));
+  for (int i0 = 0; i0 < n; i0 += chunk) {
+    const int m = std::min(chunk, n - i0);
+    k_sweep_masks<<<dim3(grid_for(px, 256, 2 * c->num_sms), m), 256, 0, c->stream>>>(d_stat, w, h, e.rw, e.rh,
+                                                                                       d_thr + i0, d_masks);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(masks + px * i0, d_masks, px * m * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  return SRED_OK;
+}
+
 cudaStream_t pick(sred_ctx* c, void* s) { return s ? (cudaStream_t)s : c->stream; }
 
 }  // namespace
@@ -1427,7 +1504,10 @@ sred_status sred_gat_fit_2d(sred_ctx* c, const float* img, int w, int h, int max
   int evals = 0;
   auto eval = [&](const double* p, double* out) -> sred_status {
     evals++;
-    return gat_objective_dev(c, d, w, h, p[0], p[1], p[2], out);
+    const sred_status st = gat_objective_dev(c, d, w, h, p[0], p[1], p[2], out);
+    // gain 0 (the relevance tools start there) gives inf - inf; rank NaN last
+    if (st == SRED_OK && std::isnan(*out)) *out = HUGE_VAL;
+    return st;
   };
   for (int v = 0; v < 4; v++) {
     x[v][0] = *gain;
@@ -1702,6 +1782,97 @@ sred_status sred_global_map_3d_device(sred_ctx* c, const char* metric, const flo
   std::lock_guard<std::recursive_mutex> lk(c->mu);
   cudaSetDevice(c->device);
   return global3d_core(c, m, d_vol, w, h, d, bw, bh, bd, relc, normalize, d_out, pick(c, stream), info);
+}
+
+// ---------------------------------------------------------------------------
+// Relevance-mask tools
+// ---------------------------------------------------------------------------
+
+sred_status sred_relevance_mask_tool_2d(sred_ctx* c, const float* img, int w, int h, int bw, int bh,
+                                        float filter_constant, float* mask, float* threshold, float* noise_var) {
+  if (!c || !img || !mask || !threshold || !noise_var) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->shard.valid = false;
+  Ellipse e;
+  float *d_img, *d_stat;
+  CKS(tool_stat(c, img, w, h, bw, bh, 1, &e, &d_img, &d_stat));
+  float nv;
+  CKS(tool_noise_var(c, d_img, w, h, true, c->stream, &nv));
+  const float thr = tool_threshold(nv, filter_constant);
+  CKS(tool_masks(c, d_stat, w, h, e, &thr, 1, mask));
+  *threshold = thr;
+  *noise_var = nv;
+  return SRED_OK;
+}
+
+sred_status sred_relevance_mask_sweep_2d(sred_ctx* c, const float* img, int w, int h, int bw, int bh, float lower,
+                                         float step, int n, float* masks, float* constants, float* noise_var) {
+  if (!c || !img || !masks || !constants || !noise_var) return SRED_ERR_ARG;
+  if (n < 1 || n > 65535) return fail(c, SRED_ERR_ARG, "the number of masks must be in 1..65535");
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->shard.valid = false;
+  Ellipse e;
+  float *d_img, *d_stat;
+  CKS(tool_stat(c, img, w, h, bw, bh, 0, &e, &d_img, &d_stat));
+  float nv;
+  CKS(tool_noise_var(c, d_img, w, h, false, c->stream, &nv));
+  std::vector<float> thr(n);
+  float fc = lower;
+  for (int i = 0; i < n; i++) {
+    constants[i] = fc;
+    thr[i] = tool_threshold(nv, fc);
+    fc += step;
+  }
+  CKS(tool_masks(c, d_stat, w, h, e, thr.data(), n, masks));
+  *noise_var = nv;
+  return SRED_OK;
+}
+
+sred_status sred_relevance_constant_range_2d(sred_ctx* c, const float* img, int w, int h, int bw, int bh,
+                                             float step, float* all_ones, float* all_zeros, float* noise_var) {
+  if (!c || !img || !all_ones || !all_zeros || !noise_var) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->shard.valid = false;
+  Ellipse e;
+  float *d_img, *d_stat;
+  CKS(tool_stat(c, img, w, h, bw, bh, 0, &e, &d_img, &d_stat));
+  float nv;
+  CKS(tool_noise_var(c, d_img, w, h, false, c->stream, &nv));
+  unsigned* mm;
+  CKS(ensure(c, B_MM, 2, &mm));
+  const unsigned init[2] = {0xffffffffu, 0u};
+  CK(cudaMemcpyAsync(mm, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+  k_stat_sq_minmax<<<grid_for((size_t)w * h, 256, 4 * c->num_sms), 256, 0, c->stream>>>(d_stat, w, h, e.rw, e.rh,
+                                                                                        mm);
+  CK(cudaGetLastError());
+  unsigned hm[2];
+  CK(cudaMemcpyAsync(hm, mm, sizeof(hm), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  // The reference's loop (OptimiseRelevanceMask_.run): c = 0, step, 2 step, ...
+  // (FP32 accumulation) until the mask is all 0, remembering the last c whose
+  // interior is all 1. One pixel is 1 at c iff !(s^2 < thr) and s^2 != 0, so
+  // the interior's smallest and largest s^2 decide every step.
+  const bool any = hm[0] != 0xffffffffu;
+  float mn = 0.0f, mx = 0.0f;
+  std::memcpy(&mn, &hm[0], sizeof(float));
+  std::memcpy(&mx, &hm[1], sizeof(float));
+  float fc = 0.0f, ones = 0.0f;
+  for (;;) {
+    const float thr = tool_threshold(nv, fc);
+    if (!any || (!(mn < thr) && mn != 0.0f)) ones = fc;
+    if (!any || mx < thr || mx == 0.0f) break;
+    const float next = fc + step;
+    if (!(next > fc))
+      return fail(c, SRED_ERR_ARG, "the relevance constant step never reaches an all-zero mask");
+    fc = next;
+  }
+  *all_ones = ones;
+  *all_zeros = fc;
+  *noise_var = nv;
+  return SRED_OK;
 }
 
 }  // extern "C"

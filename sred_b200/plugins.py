@@ -1,11 +1,13 @@
-"""The ImageJ commands of the hot path as functions over arrays.
+"""The ImageJ commands as functions over arrays, with the dialog fields as
+keyword arguments (same defaults) and the windowing left out.
 
 ``global_repetition_2d`` follows GlobalRepetition2D_.run
-(java/GlobalRepetition2D_.java:35-156) and ``block_repetition_2d`` follows
-BlockRepetition2D_.run (java/BlockRepetition2D_.java:32-158), with the dialog
-fields as keyword arguments (same defaults) and the windowing left out.
-Noise-variance stabilisation (GAT) is not part of this path: pass an image
-that is already stabilised, or leave ``stabilise_noise_variance`` False.
+(java/GlobalRepetition2D_.java:35-156), ``block_repetition_2d``
+BlockRepetition2D_.run (java/BlockRepetition2D_.java:32-158), the 3D pair
+GlobalRepetition3D_ / BlockRepetition3D_, and the relevance-mask tools
+RelevanceMask2D_, RelevanceMaskStack2D_ and OptimiseRelevanceMask_. Variance
+stabilisation uses the GPU GAT fit ("Simplex"); the reference's other
+estimation method ("Quad/Octree") is not provided.
 """
 from __future__ import annotations
 
@@ -20,10 +22,8 @@ def global_repetition_2d(image: np.ndarray, block_width: int = 5, block_height: 
                          run_info: dict | None = None):
     if block_width % 2 == 0 or block_height % 2 == 0:
         raise ValueError("Patch dimensions must be odd. Please try again.")
-    if stabilise_noise_variance:
-        raise NotImplementedError("variance stabilisation is outside the accelerated path")
     bs = utils.block_size(block_width, block_height)
-    inp = utils.get_input_image_2d(image, True)
+    inp = utils.get_input_image_2d(image, True, stabilise_noise_variance, ctx=ctx)
     stats = clutils.get_local_statistics_2d(inp, block_width, block_height, ctx)
     mask = utils.get_relevance_mask(inp.image_array, inp.width, inp.height, block_width // 2, block_height // 2,
                                     stats.local_stds, relevance_constant, ctx)
@@ -39,18 +39,86 @@ def global_repetition_2d(image: np.ndarray, block_width: int = 5, block_height: 
 def block_repetition_2d(block: np.ndarray, image: np.ndarray, relevance_constant: float = 0.0,
                         metric: str = "Pearson's R", stabilise_noise_variance: bool = False,
                         normalize_output: bool = True, ctx=None):
-    if stabilise_noise_variance:
-        raise NotImplementedError("variance stabilisation is outside the accelerated path")
     ref = utils.get_reference_block_2d(block)
     if ref is None:
         raise ValueError("Block dimensions must be odd (e.g., 3x3 or 5x5). Please try again.")
     frames = image if image.ndim == 3 else image[None]
     outs = []
     for f in frames:  # time-lapse: each frame normalised on its own (java/BlockRepetition2D_.java:104-130)
-        inp = utils.get_input_image_2d(f, True)
+        inp = utils.get_input_image_2d(f, True, stabilise_noise_variance, ctx=ctx)
         out = clutils.calculate_block_repetition_map_2d(metric, inp, ref, relevance_constant, normalize_output,
                                                         ctx=ctx)
         if out is None:
             return None
         outs.append(out.reshape(inp.height, inp.width))
     return np.stack(outs) if image.ndim == 3 else outs[0]
+
+
+def global_repetition_3d(volume: np.ndarray, block_width: int = 3, block_height: int = 3, block_depth: int = 3,
+                         relevance_constant: float = 0.0, metric: str = "Pearson's R",
+                         normalize_output: bool = True, ctx=None, run_info: dict | None = None):
+    """GlobalRepetition3D_.run (java/GlobalRepetition3D_.java:40-158) on a
+    [depth, height, width] volume; see sred_calculate_global_repetition_map_3d
+    for the repairs that make the reference's path run."""
+    if block_width % 2 == 0 or block_height % 2 == 0 or block_depth % 2 == 0:
+        raise ValueError("Block dimensions must be odd. Please try again.")
+    if block_depth < 3:
+        raise ValueError("Block depth must be at least 3. Please try again.")
+    inp = utils.get_input_image_3d(volume)
+    res = clutils.calculate_global_repetition_map_3d(metric, inp, block_width, block_height, block_depth,
+                                                     relevance_constant, normalize_output, ctx=ctx, return_info=True)
+    if res is None:
+        return None
+    out, info = res
+    if run_info is not None:
+        run_info.update(info)
+    return out.reshape(inp.depth, inp.height, inp.width)
+
+
+def block_repetition_3d(block: np.ndarray, volume: np.ndarray, relevance_constant: float = 0.0,
+                        metric: str = "Pearson's R", normalize_output: bool = True, ctx=None):
+    """BlockRepetition3D_.run (java/BlockRepetition3D_.java:40-115)."""
+    ref = utils.get_reference_block_3d(block)
+    inp = utils.get_input_image_3d(volume)
+    out = clutils.calculate_block_repetition_map_3d(metric, inp, ref, relevance_constant, normalize_output, ctx=ctx)
+    return None if out is None else out.reshape(inp.depth, inp.height, inp.width)
+
+
+def relevance_tools_input(image: np.ndarray, max_iter: int = 5000, ctx=None) -> np.ndarray:
+    """The preprocessing the relevance-mask tools share (e.g.
+    java/RelevanceMask2D_.java, GAT section and normalisation): the GAT
+    parameters fitted from gain 0, sigma 100, offset 0, the transform, then
+    min-max to [0, 1] in FP64 with epsilon, stored as float."""
+    a = np.ascontiguousarray(image, np.float32)
+    g, s, o, _ = utils.fit_gat_2d(a, max_iter, gain=0.0, sigma=100.0, offset=0.0, ctx=ctx)
+    t = utils.get_gat_2d(a, g, s, o, ctx=ctx).astype(np.float64)
+    mn, mx = t.min(), t.max()
+    return ((t - mn) / (mx - mn + float(utils.EPSILON))).astype(np.float32)
+
+
+def relevance_mask_2d(image: np.ndarray, block_width: int = 3, block_height: int = 3, filter_constant: float = 0.0,
+                      ctx=None) -> utils.RelevanceMask:
+    """RelevanceMask2D_.run: the relevance mask of one filter constant."""
+    return clutils.relevance_mask_tool_2d(relevance_tools_input(image, ctx=ctx), block_width, block_height,
+                                          filter_constant, ctx=ctx)
+
+
+def relevance_mask_stack_2d(image: np.ndarray, block_width: int = 3, block_height: int = 3,
+                            lower_limit: float = 0.0, upper_limit: float = 1.0, step: float = 0.1, ctx=None):
+    """RelevanceMaskStack2D_.run: masks at lower, lower + step, ... with
+    ceil((upper - lower) / step) + 1 slices (FP32, as the command computes
+    it); returns (masks [n, h, w], constants, the preprocessed input)."""
+    f = np.float32
+    n = int(np.ceil(np.float64((f(upper_limit) - f(lower_limit)) / f(step)))) + 1
+    inp = relevance_tools_input(image, ctx=ctx)
+    masks, consts, _ = clutils.relevance_mask_sweep_2d(inp, block_width, block_height, lower_limit, step, n, ctx=ctx)
+    return masks, consts, inp
+
+
+def optimise_relevance_mask(image: np.ndarray, block_width: int = 3, block_height: int = 3, step: float = 1.0,
+                            ctx=None) -> tuple:
+    """OptimiseRelevanceMask_.run: the filter-constant range (all-relevant,
+    all-irrelevant) the command logs."""
+    ones, zeros, _ = clutils.relevance_constant_range_2d(relevance_tools_input(image, ctx=ctx), block_width,
+                                                         block_height, step, ctx=ctx)
+    return ones, zeros

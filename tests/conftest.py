@@ -41,3 +41,9 @@ def volume_cases(fx):
     for n in sorted({k.split("/")[0] for k in fx}):
         bw, bh, bd = (int(v) for v in n.rsplit("_", 1)[1].split("x"))
         yield n, bw, bh, bd
+
+
+@pytest.fixture(scope="session")
+def relevance_fx():
+    import numpy as np
+    return dict(np.load(ROOT / "tests" / "golden" / "relevance_refshim.npz"))

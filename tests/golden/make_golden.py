@@ -28,6 +28,10 @@ Two kinds of fixtures are written:
    in ``oracle/refshim/build.py``) with the host steps of ``getGlobal*3D``.
    No reference test covers 3D.
 
+5. ``relevance_refshim.npz``: outputs of the relevance-mask tools' kernels
+   (``cl/kernelGetRelevanceMask2D.cl``, the local variance, and
+   ``cl/kernelGetLocalMeans.cl``, the local std) on small seeded images.
+
 Usage: ``python tests/golden/make_golden.py [--reference /root/reference] [--only volume ...]``
 """
 from __future__ import annotations
@@ -280,20 +284,39 @@ def volume_fixtures() -> dict:
     return fx
 
 
+RELEVANCE_CASES = [
+    # (name, W, H, lattice, seed, block)
+    ("spots60x50_3x3", 60, 50, 5, 41, 3),
+    ("spots72x64_5x5", 72, 64, 6, 42, 5),
+    ("spots48x56_7x7", 48, 56, 4, 43, 7),
+]
+
+
+def relevance_fixtures() -> dict:
+    fx: dict = {}
+    for name, W, H, lat, seed, b in RELEVANCE_CASES:
+        img = synth.normalize_input(synth.spot_image(W, H, lat, seed=seed))
+        fx[f"{name}/image"] = img
+        fx[f"{name}/var"] = oracle.local_var2d(img, b, b, 0, use_refshim=True)
+        fx[f"{name}/std"] = oracle.local_var2d(img, b, b, 1, use_refshim=True)
+    return fx
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", choices=["junit", "global", "shape", "volume"], action="append",
+    ap.add_argument("--only", choices=["junit", "global", "shape", "volume", "relevance"], action="append",
                     help="regenerate only these fixture files (default: all)")
     a = ap.parse_args(argv)
-    only = set(a.only or ["junit", "global", "shape", "volume"])
+    only = set(a.only or ["junit", "global", "shape", "volume", "relevance"])
     if "junit" in only:
         vec = junit_vectors(Path(a.reference))
         (HERE / "reference_junit.json").write_text(json.dumps(vec, indent=1))
         print("wrote", HERE / "reference_junit.json")
     for kind, fname, make in (("global", "global_refshim.npz", refshim_fixtures),
                               ("shape", "shape_refshim.npz", shape_fixtures),
-                              ("volume", "volume_refshim.npz", volume_fixtures)):
+                              ("volume", "volume_refshim.npz", volume_fixtures),
+                              ("relevance", "relevance_refshim.npz", relevance_fixtures)):
         if kind in only:
             fx = make()
             np.savez_compressed(HERE / fname, **fx)

@@ -407,3 +407,37 @@ def test_global3d_matches_refshim_live():
             a = oracle.global3d_sums_f32(metric, vol, bw, bh, bd, means, stds, nv, thr)
             b = oracle.global3d_sums_f32(metric, vol, bw, bh, bd, means, stds, nv, thr, use_refshim=True)
             assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), (bw, bh, bd, metric)
+
+
+# Relevance-mask tools: the local variance / std of cl/kernelGetRelevanceMask2D.cl
+# and cl/kernelGetLocalMeans.cl, frozen in relevance_refshim.npz
+
+def test_tool_statistics_match_refshim_fixtures(relevance_fx):
+    for name in sorted({k.split("/")[0] for k in relevance_fx}):
+        b = int(name.rsplit("x", 1)[1])
+        img = relevance_fx[f"{name}/image"]
+        assert np.array_equal(oracle.local_var2d(img, b, b, 0), relevance_fx[f"{name}/var"]), name
+        assert np.array_equal(oracle.local_var2d(img, b, b, 1), relevance_fx[f"{name}/std"]), name
+
+
+@pytest.mark.skipif(oracle.refshim() is None, reason="refshim not built")
+def test_tool_statistics_match_refshim_live():
+    from sred_b200 import synth
+    img = synth.normalize_input(synth.spot_image(45, 38, 4, seed=99))
+    for b in (3, 5, 9):
+        for ts in (0, 1):
+            assert np.array_equal(oracle.local_var2d(img, b, b, ts), oracle.local_var2d(img, b, b, ts, True))
+
+
+def test_tool_range_matches_mask_definition():
+    """The literal loop of OptimiseRelevanceMask_: at all_zeros the mask is all
+    0 and one step before it is not; at all_ones the interior is all 1."""
+    from sred_b200 import synth
+    img = synth.normalize_input(synth.spot_image(64, 48, 5, seed=7))
+    v = oracle.local_var2d(img, 3, 3, 0)
+    nv = oracle.tool_noise_var(img, 0)
+    for step in (1.0, 0.05):
+        ones, zeros = oracle.tool_range(v, 3, 3, nv, step)
+        assert not oracle.tool_mask(v, 3, 3, nv, zeros).any()
+        assert oracle.tool_mask(v, 3, 3, nv, np.float32(zeros - np.float32(step))).any()
+        assert oracle.tool_mask(v, 3, 3, nv, ones)[1:-1, 1:-1].all()
