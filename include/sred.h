@@ -223,6 +223,21 @@ sred_status sred_gat_objective_2d(sred_ctx *ctx, const float *img, int w, int h,
 sred_status sred_gat_fit_2d(sred_ctx *ctx, const float *img, int w, int h, int max_iter, double *gain,
                             double *sigma, double *offset, double *error);
 
+/* 3D variance stabilisation (java/GATMinimizer3D.java). sred_gat_3d:
+ * getGAT over all w*h*d voxels, in place. sred_gat_objective_3d:
+ * GATMinimizer3D.userFunction: NaN unless gain > 0, sigma >= 0, offset >= 0;
+ * blocks of width/6 x height/6 x depth/6 voxels (halved along an axis with
+ * fewer than 2 blocks), per-block variance of the transformed voxels (FP64
+ * sums), sum over blocks of (variance - 1)^2 / blocks. sred_gat_fit_3d: the
+ * simplex of sred_gat_fit_2d over that objective (an objective of NaN ranks
+ * last); the reference's command starts it at gain 0, sigma 100, offset 0
+ * (java/Utils.java:1222). */
+sred_status sred_gat_3d(sred_ctx *ctx, float *vol, int w, int h, int d, double gain, double sigma, double offset);
+sred_status sred_gat_objective_3d(sred_ctx *ctx, const float *vol, int w, int h, int d, double gain, double sigma,
+                                  double offset, double *error);
+sred_status sred_gat_fit_3d(sred_ctx *ctx, const float *vol, int w, int h, int d, int max_iter, double *gain,
+                            double *sigma, double *offset, double *error);
+
 /* Replaces Utils.normalizeImage2D (java/Utils.java:985-1031) on host memory.
  * mask may be NULL. SRED_ERR_ARG for a non-binary mask. */
 sred_status sred_normalize_image_2d(float *img, int w, int h, int border_w, int border_h,

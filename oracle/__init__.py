@@ -113,6 +113,8 @@ def lib() -> C.CDLL:
         L.orc_tool_range.restype = C.c_int
         L.orc_tool_range.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int,
                                      _fp, _fp]
+        L.orc_gat_objective3d.restype = C.c_double
+        L.orc_gat_objective3d.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
         L.orc_gat_objective.restype = C.c_double
         L.orc_gat_objective.argtypes = [_f32p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
         L.orc_patch_hu1_ref.restype = C.c_double
@@ -714,3 +716,10 @@ def tool_range(stat, bw, bh, nv, step, max_iter=100000):
     if rc != 0:
         raise ValueError("the step never reaches an all-zero mask")
     return np.float32(a.value), np.float32(b.value)
+
+
+def gat_objective3d(vol, gain, sigma, offset) -> float:
+    """GATMinimizer3D.userFunction (java/GATMinimizer3D.java)."""
+    v = _f32(vol)
+    D, H, W = v.shape
+    return float(lib().orc_gat_objective3d(v.ravel(), W, H, D, float(gain), float(sigma), float(offset)))

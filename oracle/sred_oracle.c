@@ -1644,3 +1644,53 @@ int orc_tool_range(const float *stat, int W, int H, int rw, int rh, float nv, fl
     *all_zeros = fc;
     return rc;
 }
+
+/* ------------------------------------------------------------------ */
+/* 3D variance stabilisation objective (java/GATMinimizer3D.java        */
+/* userFunction, java/Utils.java getMeanAndVarBlock3D), sequential FP64 */
+/* ------------------------------------------------------------------ */
+double orc_gat_objective3d(const float *vox, int W, int H, int D, double gain, double sigma, double offset) {
+    if (gain <= 0 || sigma < 0 || offset < 0) return NAN;
+    const long n = (long)W * H * D;
+    float *g = (float *)malloc(sizeof(float) * (size_t)n);
+    const double c = (3.0 / 8.0) * gain * gain + sigma * sigma - gain * offset;
+    for (long i = 0; i < n; i++) {
+        double v = vox[i];
+        v = (v <= -c / gain) ? 0.0 : (2 / gain) * sqrt(gain * v + c);
+        g[i] = (float)v;
+    }
+    int bw = W / 6 > 1 ? W / 6 : 1, bh = H / 6 > 1 ? H / 6 : 1, bd = D / 6 > 1 ? D / 6 : 1;
+    int nx = W / bw, ny = H / bh, nz = D / bd;
+    while (nx < 2 || ny < 2 || nz < 2) {
+        const int a0 = bw, b0 = bh, c0 = bd;
+        if (nx < 2 && bw > 1) bw = bw / 2 > 1 ? bw / 2 : 1;
+        if (ny < 2 && bh > 1) bh = bh / 2 > 1 ? bh / 2 : 1;
+        if (nz < 2 && bd > 1) bd = bd / 2 > 1 ? bd / 2 : 1;
+        nx = W / bw;
+        ny = H / bh;
+        nz = D / bd;
+        if (bw == 1 && bh == 1 && bd == 1) break;
+        if (bw == a0 && bh == b0 && bd == c0) break; /* an axis of 1 voxel: the reference loops forever */
+    }
+    const int nb = nx * ny * nz;
+    double error = 0.0;
+    for (int bz = 0; bz < nz; bz++)
+        for (int by = 0; by < ny; by++)
+            for (int bx = 0; bx < nx; bx++) {
+                double mean = 0.0, sq = 0.0;
+                for (int z = bz * bd; z < (bz + 1) * bd; z++)
+                    for (int y = by * bh; y < (by + 1) * bh; y++)
+                        for (int x = bx * bw; x < (bx + 1) * bw; x++) {
+                            const double v = (double)g[(long)W * H * z + (long)y * W + x];
+                            mean += v;
+                            sq += v * v;
+                        }
+                const int bs = bw * bh * bd;
+                mean = mean / bs;
+                const double var = sq / bs - mean * mean;
+                const double delta = var - 1.0;
+                error += (delta * delta) / (double)nb;
+            }
+    free(g);
+    return error;
+}

@@ -30,6 +30,7 @@ EXPORTS = [
     "sred_local_statistics_3d", "sred_relevance_mask_3d", "sred_calculate_block_repetition_map_3d",
     "sred_block_map_3d_device", "sred_calculate_global_repetition_map_3d", "sred_global_map_3d_device",
     "sred_relevance_mask_tool_2d", "sred_relevance_mask_sweep_2d", "sred_relevance_constant_range_2d",
+    "sred_gat_3d", "sred_gat_objective_3d", "sred_gat_fit_3d",
 ]
 
 
@@ -89,6 +90,9 @@ def load() -> C.CDLL:
         L.sred_gat_2d.argtypes = [_vp, _f32p, s, s, C.c_double, C.c_double, C.c_double]
         L.sred_gat_objective_2d.argtypes = [_vp, _f32p, s, s, C.c_double, C.c_double, C.c_double, _dp]
         L.sred_gat_fit_2d.argtypes = [_vp, _f32p, s, s, s, _dp, _dp, _dp, _dp]
+        L.sred_gat_3d.argtypes = [_vp, _f32p, s, s, s, C.c_double, C.c_double, C.c_double]
+        L.sred_gat_objective_3d.argtypes = [_vp, _f32p, s, s, s, C.c_double, C.c_double, C.c_double, _dp]
+        L.sred_gat_fit_3d.argtypes = [_vp, _f32p, s, s, s, s, _dp, _dp, _dp, _dp]
         L.sred_block_size.argtypes = [s, s]
         L.sred_local_statistics_2d.argtypes = [_vp, _f32p, s, s, s, s, _f32p, _f32p]
         L.sred_mean_noise_var_2d.argtypes = [_vp, _f32p, s, s, _fp]

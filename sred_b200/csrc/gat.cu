@@ -8,6 +8,7 @@
 // blocks. Both are double-precision code in the reference; this file is
 // compiled with -fmad=false so that no multiply-add is fused where Java
 // rounds twice.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -64,6 +65,71 @@ __global__ void __launch_bounds__(256)
     out[2 * b] = s1[0];
     out[2 * b + 1] = s2[0];
   }
+}
+
+// One block of GATMinimizer3D.userFunction's grid: the voxels transformed as
+// applyGAT does (stored as float), then sum v and sum v*v in double (the
+// product of the widened value, as java/Utils.java getMeanAndVarBlock3D
+// computes it). One CTA per block; out[2 b] = sum, out[2 b + 1] = sum of
+// squares.
+__global__ void __launch_bounds__(256)
+    k_gat_block_moments3d(const float* __restrict__ vol, int W, int H, int bw, int bh, int bd, int nbx, int nby,
+                          double gain, double c, double* __restrict__ out) {
+  __shared__ double s1[256], s2[256];
+  const int b = blockIdx.x, bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
+  const size_t x0 = (size_t)bx * bw, y0 = (size_t)by * bh, z0 = (size_t)bz * bd;
+  const double lim = -c / gain, scale = 2.0 / gain;
+  const size_t n = (size_t)bw * bh * bd;
+  double a1 = 0.0, a2 = 0.0;
+  for (size_t t = threadIdx.x; t < n; t += blockDim.x) {
+    const size_t x = x0 + t % bw, y = y0 + (t / bw) % bh, z = z0 + t / ((size_t)bw * bh);
+    double v = (double)vol[(z * H + y) * W + x];
+    v = (v <= lim) ? 0.0 : scale * sqrt(gain * v + c);
+    const double f = (double)(float)v;
+    a1 += f;
+    a2 += f * f;
+  }
+  s1[threadIdx.x] = a1;
+  s2[threadIdx.x] = a2;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      s1[threadIdx.x] += s1[threadIdx.x + s];
+      s2[threadIdx.x] += s2[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[2 * b] = s1[0];
+    out[2 * b + 1] = s2[0];
+  }
+}
+
+// GATMinimizer3D's grid: width/6, height/6, depth/6 (at least 1), halved
+// along the axes with fewer than 2 blocks until all have 2 or the block is a
+// single voxel (or, for an axis of length 1, until nothing changes).
+void gat3d_grid(int w, int h, int d, int* bw, int* bh, int* bd, int* nbx, int* nby, int* nbz) {
+  int a = std::max(w / 6, 1), b = std::max(h / 6, 1), c = std::max(d / 6, 1);
+  int nx = w / a, ny = h / b, nz = d / c;
+  while (nx < 2 || ny < 2 || nz < 2) {
+    const int a0 = a, b0 = b, c0 = c;
+    if (nx < 2 && a > 1) a = std::max(a / 2, 1);
+    if (ny < 2 && b > 1) b = std::max(b / 2, 1);
+    if (nz < 2 && c > 1) c = std::max(c / 2, 1);
+    nx = w / a;
+    ny = h / b;
+    nz = d / c;
+    if (a == 1 && b == 1 && c == 1) break;
+    // An axis of 1 voxel can never have 2 blocks: the reference's loop then
+    // runs forever; stop once nothing changes.
+    if (a == a0 && b == b0 && c == c0) break;
+  }
+  *bw = a;
+  *bh = b;
+  *bd = c;
+  *nbx = nx;
+  *nby = ny;
+  *nbz = nz;
 }
 
 // Block grid of the objective: width / 6 by height / 6 pixels

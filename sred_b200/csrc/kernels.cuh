@@ -50,6 +50,9 @@ __global__ void k_gat_block_moments(const float* img, int W, int bw, int bh, int
                                     double* out);
 bool gat_grid(int w, int h, int* bw, int* bh, int* nbx, int* nby);
 double gat_error(const double* sums, int nblocks, int bw, int bh);
+__global__ void k_gat_block_moments3d(const float* vol, int W, int H, int bw, int bh, int bd, int nbx, int nby,
+                                      double gain, double c, double* out);
+void gat3d_grid(int w, int h, int d, int* bw, int* bh, int* bd, int* nbx, int* nby, int* nbz);
 
 // shape.cu (k_block_phase is declared in shape.cuh, next to PhaseRef)
 __global__ void k_patch_hu(const float* img, int W, int H, Ellipse e, int patch_size, double ref_hu1, float* out,

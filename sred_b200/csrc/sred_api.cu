@@ -1450,6 +1450,33 @@ sred_status gat_objective_dev(sred_ctx* c, const float* d_img, int w, int h, dou
   return SRED_OK;
 }
 
+// GATMinimizer3D.userFunction (java/GATMinimizer3D.java): NaN outside gain > 0,
+// sigma >= 0, offset >= 0; block grid of width/6 x height/6 x depth/6 voxels
+// (at least 1), halved along every axis with fewer than 2 blocks until each
+// has 2 or the block is one voxel; per-block variance with FP64 sums of the
+// transformed voxels (as float, then widened).
+sred_status gat_objective3d_dev(sred_ctx* c, const float* d_vol, int w, int h, int d, double gain, double sigma,
+                                double offset, double* error) {
+  if (gain <= 0 || sigma < 0 || offset < 0) {
+    *error = std::nan("");
+    return SRED_OK;
+  }
+  int bw, bh, bd, nbx, nby, nbz;
+  gat3d_grid(w, h, d, &bw, &bh, &bd, &nbx, &nby, &nbz);
+  const size_t nb = (size_t)nbx * nby * nbz;
+  if (nb == 0) return fail(c, SRED_ERR_ARG, "volume too small for the GAT fit");
+  double* d_sums;
+  CKS(ensure(c, B_GAT, 2 * nb, &d_sums));
+  const double cst = (3.0 / 8.0) * gain * gain + sigma * sigma - gain * offset;
+  k_gat_block_moments3d<<<(unsigned)nb, 256, 0, c->stream>>>(d_vol, w, h, bw, bh, bd, nbx, nby, gain, cst, d_sums);
+  CK(cudaGetLastError());
+  std::vector<double> sums(2 * nb);
+  CK(cudaMemcpyAsync(sums.data(), d_sums, sums.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *error = gat_error(sums.data(), (int)nb, bw * bh * bd, 1);
+  return SRED_OK;
+}
+
 }  // namespace
 
 sred_status sred_gat_2d(sred_ctx* c, float* img, int w, int h, double gain, double sigma, double offset) {
@@ -1484,35 +1511,25 @@ sred_status sred_gat_objective_2d(sred_ctx* c, const float* img, int w, int h, d
 
 // Nelder-Mead downhill simplex (Nelder & Mead, Computer Journal 7:308, 1965;
 // reflection 1, expansion 2, contraction 1/2, shrink 1/2) over (gain, sigma,
-// offset), started from the given values with the initial steps of
-// GATMinimizer2D.run (1, 10, 100). The objective is evaluated on the GPU with
-// the image resident. Stops after max_iter evaluations or when the simplex's
-// objective values agree to 1e-15 of the best.
-sred_status sred_gat_fit_2d(sred_ctx* c, const float* img, int w, int h, int max_iter, double* gain, double* sigma,
-                            double* offset, double* error_out) {
-  if (!c || !img || !gain || !sigma || !offset || w <= 0 || h <= 0 || max_iter < 1) return SRED_ERR_ARG;
-  std::lock_guard<std::recursive_mutex> lk(c->mu);
-  cudaSetDevice(c->device);
-  c->shard.valid = false;
-  const size_t n = (size_t)w * h;
-  float* d;
-  CKS(ensure(c, B_IMG, n, &d));
-  CK(cudaMemcpyAsync(d, img, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+// offset) from x0 with the initial steps of the reference's Minimizer set-up
+// (1, 10, 100; java/GATMinimizer2D.java:42-45). An objective of NaN ranks
+// last. Stops after max_iter evaluations or when the simplex's objective
+// values agree to 1e-15 of the best.
+extern "C++" {
+template <class F>
+sred_status nelder_mead3(F objective, int max_iter, double* x0, double* f_best) {
   double x[4][3];
   double f[4];
   const double step[3] = {1.0, 10.0, 100.0};
   int evals = 0;
   auto eval = [&](const double* p, double* out) -> sred_status {
     evals++;
-    const sred_status st = gat_objective_dev(c, d, w, h, p[0], p[1], p[2], out);
-    // gain 0 (the relevance tools start there) gives inf - inf; rank NaN last
+    const sred_status st = objective(p, out);
     if (st == SRED_OK && std::isnan(*out)) *out = HUGE_VAL;
     return st;
   };
   for (int v = 0; v < 4; v++) {
-    x[v][0] = *gain;
-    x[v][1] = *sigma;
-    x[v][2] = *offset;
+    for (int k = 0; k < 3; k++) x[v][k] = x0[k];
     if (v > 0) x[v][v - 1] += step[v - 1];
     CKS(eval(x[v], &f[v]));
   }
@@ -1563,10 +1580,72 @@ sred_status sred_gat_fit_2d(sred_ctx* c, const float* img, int w, int h, int max
   int best = 0;
   for (int v = 1; v < 4; v++)
     if (f[v] < f[best]) best = v;
-  *gain = x[best][0];
-  *sigma = x[best][1];
-  *offset = x[best][2];
-  if (error_out) *error_out = f[best];
+  for (int k = 0; k < 3; k++) x0[k] = x[best][k];
+  *f_best = f[best];
+  return SRED_OK;
+}
+}  // extern "C++"
+
+// The GAT parameters minimising the objective of java/GATMinimizer2D.java, with
+// the image resident.
+sred_status sred_gat_fit_2d(sred_ctx* c, const float* img, int w, int h, int max_iter, double* gain, double* sigma,
+                            double* offset, double* error_out) {
+  if (!c || !img || !gain || !sigma || !offset || w <= 0 || h <= 0 || max_iter < 1) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->shard.valid = false;
+  const size_t n = (size_t)w * h;
+  float* d;
+  CKS(ensure(c, B_IMG, n, &d));
+  CK(cudaMemcpyAsync(d, img, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  double x[3] = {*gain, *sigma, *offset}, fb;
+  CKS(nelder_mead3([&](const double* p, double* out) { return gat_objective_dev(c, d, w, h, p[0], p[1], p[2], out); },
+                   max_iter, x, &fb));
+  *gain = x[0];
+  *sigma = x[1];
+  *offset = x[2];
+  if (error_out) *error_out = fb;
+  return SRED_OK;
+}
+
+// ---- 3D (java/GATMinimizer3D.java) ----
+
+sred_status sred_gat_3d(sred_ctx* c, float* vol, int w, int h, int d, double gain, double sigma, double offset) {
+  if (!c || !vol || w <= 0 || h <= 0 || d <= 0) return SRED_ERR_ARG;
+  return sred_gat_2d(c, vol, w, h * d, gain, sigma, offset);
+}
+
+sred_status sred_gat_objective_3d(sred_ctx* c, const float* vol, int w, int h, int d, double gain, double sigma,
+                                  double offset, double* error) {
+  if (!c || !vol || !error || w <= 0 || h <= 0 || d <= 0) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->shard.valid = false;
+  const size_t n = (size_t)w * h * d;
+  float* dv;
+  CKS(ensure(c, B_IMG, n, &dv));
+  CK(cudaMemcpyAsync(dv, vol, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  return gat_objective3d_dev(c, dv, w, h, d, gain, sigma, offset, error);
+}
+
+sred_status sred_gat_fit_3d(sred_ctx* c, const float* vol, int w, int h, int d, int max_iter, double* gain,
+                            double* sigma, double* offset, double* error_out) {
+  if (!c || !vol || !gain || !sigma || !offset || w <= 0 || h <= 0 || d <= 0 || max_iter < 1) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->shard.valid = false;
+  const size_t n = (size_t)w * h * d;
+  float* dv;
+  CKS(ensure(c, B_IMG, n, &dv));
+  CK(cudaMemcpyAsync(dv, vol, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  double x[3] = {*gain, *sigma, *offset}, fb;
+  CKS(nelder_mead3(
+      [&](const double* p, double* out) { return gat_objective3d_dev(c, dv, w, h, d, p[0], p[1], p[2], out); },
+      max_iter, x, &fb));
+  *gain = x[0];
+  *sigma = x[1];
+  *offset = x[2];
+  if (error_out) *error_out = fb;
   return SRED_OK;
 }
 

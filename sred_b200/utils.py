@@ -214,15 +214,58 @@ class ReferenceBlock3D:
     std: float
 
 
-def get_input_image_3d(volume: np.ndarray, stabilise_noise_variance: bool = False,
-                       normalize_output: bool = True) -> InputImage3D:
-    """java/Utils.java:1279-1354 for a volume given as an array: float
-    conversion and normalizeArray (min-max over the whole volume with epsilon,
-    FP32). Variance stabilisation of volumes is not provided (ValueError)."""
-    if stabilise_noise_variance:
-        raise ValueError("variance stabilisation of volumes is not provided")
+def get_gat_3d(volume: np.ndarray, gain: float, sigma: float, offset: float, ctx=None) -> np.ndarray:
+    """getGAT over every voxel of a [depth, height, width] volume, on the GPU."""
+    c = _ctx(ctx)
+    a = np.ascontiguousarray(volume, dtype=np.float32).copy()
+    d, h, w = a.shape
+    c.check(c._L.sred_gat_3d(c.h, a, w, h, d, float(gain), float(sigma), float(offset)), "sred_gat_3d")
+    return a
+
+
+def gat_objective_3d(volume: np.ndarray, gain: float, sigma: float, offset: float, ctx=None) -> float:
+    """GATMinimizer3D.userFunction (java/GATMinimizer3D.java) on the GPU."""
+    c = _ctx(ctx)
     a = np.ascontiguousarray(volume, dtype=np.float32)
     d, h, w = a.shape
+    e = C.c_double()
+    c.check(c._L.sred_gat_objective_3d(c.h, a, w, h, d, float(gain), float(sigma), float(offset), C.byref(e)),
+            "sred_gat_objective_3d")
+    return e.value
+
+
+def fit_gat_3d(volume: np.ndarray, max_iter: int = 5000, gain: float = 0.0, sigma: float = 100.0,
+               offset: float = 0.0, ctx=None) -> tuple:
+    """GATMinimizer3D.run from the 3D command's starting point (gain 0, sigma
+    100, offset 0; java/Utils.java:1222): (gain, sigma, offset, objective)."""
+    c = _ctx(ctx)
+    a = np.ascontiguousarray(volume, dtype=np.float32)
+    d, h, w = a.shape
+    g, s, o, e = C.c_double(gain), C.c_double(sigma), C.c_double(offset), C.c_double()
+    c.check(c._L.sred_gat_fit_3d(c.h, a, w, h, d, int(max_iter), C.byref(g), C.byref(s), C.byref(o), C.byref(e)),
+            "sred_gat_fit_3d")
+    return g.value, s.value, o.value, e.value
+
+
+def get_input_image_3d(volume: np.ndarray, stabilise_noise_variance: bool = False,
+                       normalize_output: bool = True, gat_method: str = "Simplex", max_iter: int = 5000,
+                       ctx=None) -> InputImage3D:
+    """java/Utils.java:1167-1277 for a volume given as an array: float
+    conversion, optional variance stabilisation (Simplex: the GAT parameters
+    fitted on the GPU, then the transform) and normalizeArray (min-max over the
+    whole volume with epsilon, FP32). Neither of the reference's two versions
+    returns the transformed volume: the image-ID version transforms copies it
+    then drops (java/Utils.java:1216-1232), the array version normalises an
+    array it never filled (java/Utils.java:1311-1327, a volume of zeros); here
+    the volume is transformed, then normalised. The "Quad/Octree" method is
+    not provided."""
+    a = np.ascontiguousarray(volume, dtype=np.float32)
+    d, h, w = a.shape
+    if stabilise_noise_variance:
+        if gat_method != "Simplex":
+            raise ValueError(f"unsupported GAT method {gat_method!r} (only 'Simplex')")
+        gain, sigma, offset, _ = fit_gat_3d(a, max_iter, ctx=ctx)
+        a = get_gat_3d(a, gain, sigma, offset, ctx=ctx)
     if normalize_output:
         mn, mx = np.float32(a.min()), np.float32(a.max())
         a = ((a - mn) / (mx - mn + EPSILON)).astype(np.float32)

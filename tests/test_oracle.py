@@ -292,7 +292,11 @@ def test_gat_objective_matches_numpy():
 # tests/golden/volume_refshim.npz
 # ---------------------------------------------------------------------------
 
-from conftest import volume_cases  # noqa: E402
+def volume_cases(fx):
+    """(name, bw, bh, bd) of the cases in volume_refshim.npz."""
+    for n in sorted({k.split("/")[0] for k in fx}):
+        bw, bh, bd = (int(v) for v in n.rsplit("_", 1)[1].split("x"))
+        yield n, bw, bh, bd
 
 
 def test_block_size_ellipsoid():
@@ -441,3 +445,29 @@ def test_tool_range_matches_mask_definition():
         assert not oracle.tool_mask(v, 3, 3, nv, zeros).any()
         assert oracle.tool_mask(v, 3, 3, nv, np.float32(zeros - np.float32(step))).any()
         assert oracle.tool_mask(v, 3, 3, nv, ones)[1:-1, 1:-1].all()
+
+
+def _poisson_gaussian3d(w, h, d, gain, sigma, offset, seed):
+    """Poisson-Gaussian noise on an intensity constant over each cell of the
+    3D objective's 6 x 6 x 6 block grid."""
+    rng = np.random.default_rng(seed)
+    cells = rng.uniform(20, 500, (6, 6, 6))
+    lam = np.kron(cells, np.ones((d // 6, h // 6, w // 6)))
+    lam = np.pad(lam, ((0, d - lam.shape[0]), (0, h - lam.shape[1]), (0, w - lam.shape[2])), mode="edge")
+    return (gain * rng.poisson(lam) + offset + rng.normal(0, sigma, (d, h, w))).astype(np.float32)
+
+
+def test_gat_objective3d_matches_numpy():
+    vol = _poisson_gaussian3d(36, 30, 24, 2.0, 5.0, 100.0, 6)
+    for g, s, o in [(2.0, 5.0, 100.0), (1.0, 10.0, 100.0)]:
+        c = 3.0 / 8.0 * g * g + s * s - g * o
+        v = vol.astype(np.float64)
+        t = np.where(v <= -c / g, 0.0, (2 / g) * np.sqrt(np.maximum(g * v + c, 0))).astype(np.float32)
+        blk = t.reshape(6, 4, 6, 5, 6, 6).astype(np.float64)  # bd=4, bh=5, bw=6
+        var = (blk ** 2).mean(axis=(1, 3, 5)) - blk.mean(axis=(1, 3, 5)) ** 2
+        err = float(((var - 1) ** 2).sum() / 216)
+        assert abs(oracle.gat_objective3d(vol, g, s, o) - err) <= 1e-9 * err
+    assert np.isnan(oracle.gat_objective3d(vol, 0.0, 1.0, 1.0))
+    assert np.isnan(oracle.gat_objective3d(vol, 1.0, -1.0, 1.0))
+    assert np.isnan(oracle.gat_objective3d(vol, 1.0, 1.0, -1.0))
+    assert oracle.gat_objective3d(vol, 2.0, 5.0, 100.0) < 0.1 * oracle.gat_objective3d(vol, 1.0, 10.0, 100.0)
