@@ -429,6 +429,22 @@ sred_status sred_relevance_mask_sweep_2d(sred_ctx *ctx, const float *img, int w,
 sred_status sred_relevance_constant_range_2d(sred_ctx *ctx, const float *img, int w, int h, int bw, int bh,
                                              float step, float *all_ones, float *all_zeros, float *noise_var);
 
+/* Replaces ClassifyRedundancy_.run (java/ClassifyRedundancy_.java) on a
+ * repetition map: the pixels inside `border` clustered by value into k classes
+ * with k-means++ and Lloyd iterations, as its clusterer (commons-math3 3.6.1
+ * KMeansPlusPlusClusterer: at most 1000 rounds, an empty cluster refilled with
+ * a random point of the cluster whose distances vary most); with optimal_k the
+ * elbow of getOptimalK picks k in 1..max_k first (the first k whose WCSS does
+ * not fall ends the search). out (w*h floats): the class of each interior
+ * pixel ranked by class size (0 = largest, ties in cluster order), border 0.
+ * Random choices come from java.util.Random seeded with `seed` (the reference
+ * seeds from the clock, a new generator per clustering; one generator serves
+ * every clustering of a call here). k_used and wcss (sum of squared distances
+ * to the class centres) may be NULL. Classes: 1..64. */
+sred_status sred_classify_redundancy_2d(sred_ctx *ctx, const float *map, int w, int h, int border, int k,
+                                        int optimal_k, int max_k, int64_t seed, float *out, int *k_used,
+                                        double *wcss);
+
 #ifdef __cplusplus
 }
 #endif

@@ -115,6 +115,11 @@ def lib() -> C.CDLL:
                                      _fp, _fp]
         L.orc_gat_objective3d.restype = C.c_double
         L.orc_gat_objective3d.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
+        L.orc_classify_redundancy.restype = C.c_int
+        L.orc_classify_redundancy.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                              C.c_int64, _f32p, C.POINTER(C.c_double)]
+        L.orc_java_random_next.argtypes = [C.c_int64, C.c_int, C.c_int, np.ctypeslib.ndpointer(np.int32)]
+        L.orc_java_random_doubles.argtypes = [C.c_int64, C.c_int, _f64p]
         L.orc_gat_objective.restype = C.c_double
         L.orc_gat_objective.argtypes = [_f32p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
         L.orc_patch_hu1_ref.restype = C.c_double
@@ -723,3 +728,26 @@ def gat_objective3d(vol, gain, sigma, offset) -> float:
     v = _f32(vol)
     D, H, W = v.shape
     return float(lib().orc_gat_objective3d(v.ravel(), W, H, D, float(gain), float(sigma), float(offset)))
+
+
+def classify_redundancy(redundancy_map, border=1, k=3, optimal_k=False, max_k=10, seed=0):
+    """ClassifyRedundancy_.run (java/ClassifyRedundancy_.java) restated:
+    (class map, classes used, WCSS)."""
+    m = _f32(redundancy_map)
+    H, W = m.shape
+    out = np.zeros(W * H, np.float32)
+    w = C.c_double()
+    kc = lib().orc_classify_redundancy(m.ravel(), W, H, border, k, int(optimal_k), max_k, seed, out, C.byref(w))
+    return out.reshape(H, W), kc, w.value
+
+
+def java_random_next(seed, bits, n):
+    out = np.zeros(n, np.int32)
+    lib().orc_java_random_next(seed, bits, n, out)
+    return out
+
+
+def java_random_doubles(seed, n):
+    out = np.zeros(n, np.float64)
+    lib().orc_java_random_doubles(seed, n, out)
+    return out

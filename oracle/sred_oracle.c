@@ -1694,3 +1694,213 @@ double orc_gat_objective3d(const float *vox, int W, int H, int D, double gain, d
     free(g);
     return error;
 }
+
+/* ------------------------------------------------------------------ */
+/* Redundancy classification (java/ClassifyRedundancy_.java): k-means++ */
+/* and Lloyd as commons-math3 3.6.1 KMeansPlusPlusClusterer runs them,  */
+/* with java.util.Random, and every sum in the library's fixed block     */
+/* order (blocks of 1024 points; thread t of 256 adds points t, t + 256, */
+/* t + 512, t + 768 of its block; then pairwise t += t + 128 ... t + 1;   */
+/* blocks added in turn).                                                */
+/* ------------------------------------------------------------------ */
+#define KM_T 256
+#define KM_PER 4
+#define KM_SPAN (KM_T * KM_PER)
+
+typedef struct { uint64_t seed; } jrand;
+static void jr_init(jrand *r, int64_t s) { r->seed = ((uint64_t)s ^ 0x5DEECE66DULL) & ((1ULL << 48) - 1); }
+static int jr_next(jrand *r, int bits) {
+    r->seed = (r->seed * 0x5DEECE66DULL + 0xBULL) & ((1ULL << 48) - 1);
+    return (int)(int64_t)(r->seed >> (48 - bits));
+}
+static int jr_int(jrand *r, int bound) {
+    if ((bound & -bound) == bound) return (int)(((int64_t)bound * (int64_t)jr_next(r, 31)) >> 31);
+    int bits, val;
+    do {
+        bits = jr_next(r, 31);
+        val = bits % bound;
+    } while ((int64_t)bits - val + (bound - 1) > INT32_MAX);
+    return val;
+}
+static double jr_double(jrand *r) { return (double)(((int64_t)jr_next(r, 26) << 27) + jr_next(r, 27)) * 0x1.0p-53; }
+
+/* fixed-order sum over block b of v[i] for the points of that block */
+static double km_block_sum(const double *v, size_t n, size_t b) {
+    double s[KM_T];
+    for (int t = 0; t < KM_T; t++) {
+        double a = 0.0;
+        for (int j = 0; j < KM_PER; j++) {
+            size_t i = b * KM_SPAN + (size_t)j * KM_T + t;
+            if (i < n) a += v[i];
+        }
+        s[t] = a;
+    }
+    for (int st = KM_T / 2; st > 0; st >>= 1)
+        for (int t = 0; t < st; t++) s[t] += s[t + st];
+    return s[0];
+}
+
+static int km_taken(const size_t *taken, int nt, size_t i) {
+    for (int q = 0; q < nt; q++)
+        if (taken[q] == i) return 1;
+    return 0;
+}
+
+/* One clustering of x[0..n): returns the number of centres; labels, centres,
+ * counts and the WCSS out. */
+static int km_run(const double *x, size_t n, int k, jrand *rng, int *lab, double *cen, double *cnt, double *wcss) {
+    const size_t nb = (n + KM_SPAN - 1) / KM_SPAN;
+    double *d2 = (double *)malloc(sizeof(double) * n), *tmp = (double *)malloc(sizeof(double) * n);
+    double *part = (double *)malloc(sizeof(double) * nb);
+    size_t taken[64];
+    int nt = 0, have = 1;
+    size_t first = (size_t)jr_int(rng, (int)n);
+    cen[0] = x[first];
+    taken[nt++] = first;
+    while (have < k) {
+        for (size_t i = 0; i < n; i++) {
+            const double d = x[i] - cen[have - 1], e = d * d;
+            d2[i] = have == 1 ? e : fmin(d2[i], e);
+        }
+        double sum = 0.0;
+        for (size_t b = 0; b < nb; b++) { part[b] = km_block_sum(d2, n, b); sum += part[b]; }
+        const double r = jr_double(rng) * sum;
+        size_t pick = SIZE_MAX;
+        double run = 0.0;
+        for (size_t b = 0; b < nb && pick == SIZE_MAX; b++) {
+            if (run + part[b] < r && b + 1 < nb) { run += part[b]; continue; }
+            const size_t i0 = b * KM_SPAN, i1 = (i0 + KM_SPAN < n) ? i0 + KM_SPAN : n;
+            for (size_t i = i0; i < i1; i++) {
+                run += d2[i];
+                if (run >= r && !km_taken(taken, nt, i)) { pick = i; break; }
+            }
+            if (pick == SIZE_MAX && run >= r)
+                for (size_t i = i1; i-- > i0;)
+                    if (!km_taken(taken, nt, i)) { pick = i; break; }
+        }
+        if (pick == SIZE_MAX)
+            for (size_t i = n; i-- > 0;)
+                if (!km_taken(taken, nt, i)) { pick = i; break; }
+        if (pick == SIZE_MAX) break;
+        cen[have++] = x[pick];
+        taken[nt++] = pick;
+    }
+    k = have;
+    double *sums = (double *)malloc(sizeof(double) * k), *next = (double *)malloc(sizeof(double) * k);
+    for (size_t i = 0; i < n; i++) lab[i] = -1;
+    /* assignment; returns changes, fills sums/cnt and the wcss in block order */
+    #define KM_ASSIGN(changes_out)                                                                      \
+        do {                                                                                            \
+            long ch = 0;                                                                                \
+            for (size_t i = 0; i < n; i++) {                                                            \
+                int best = 0;                                                                           \
+                double bd = (x[i] - cen[0]) * (x[i] - cen[0]);                                          \
+                for (int c = 1; c < k; c++) {                                                           \
+                    const double d = (x[i] - cen[c]) * (x[i] - cen[c]);                                 \
+                    if (d < bd) { bd = d; best = c; }                                                   \
+                }                                                                                       \
+                if (lab[i] != best) ch++;                                                               \
+                lab[i] = best;                                                                          \
+                tmp[i] = bd;                                                                            \
+            }                                                                                           \
+            *wcss = 0.0;                                                                                \
+            for (size_t b = 0; b < nb; b++) *wcss += km_block_sum(tmp, n, b);                           \
+            for (int c = 0; c < k; c++) { sums[c] = 0.0; cnt[c] = 0.0; }                                \
+            for (size_t b = 0; b < nb; b++)                                                             \
+                for (int c = 0; c < k; c++) {                                                           \
+                    for (size_t i = b * KM_SPAN; i < n && i < (b + 1) * KM_SPAN; i++)                   \
+                        d2[i] = lab[i] == c ? x[i] : 0.0;                                               \
+                    sums[c] += km_block_sum(d2, n, b);                                                  \
+                    for (size_t i = b * KM_SPAN; i < n && i < (b + 1) * KM_SPAN; i++)                   \
+                        d2[i] = lab[i] == c ? 1.0 : 0.0;                                                \
+                    cnt[c] += km_block_sum(d2, n, b);                                                   \
+                }                                                                                       \
+            changes_out = ch;                                                                           \
+        } while (0)
+    long changes;
+    KM_ASSIGN(changes);
+    for (int it = 0; it < 1000; it++) {
+        int empty = 0;
+        for (int j = 0; j < k; j++) next[j] = cnt[j] > 0.0 ? sums[j] / cnt[j] : 0.0;
+        for (int j = 0; j < k; j++) {
+            if (cnt[j] > 0.0) continue;
+            empty = 1;
+            int sel = -1;
+            double best = -HUGE_VAL;
+            for (int q = 0; q < k; q++) {
+                if (!(cnt[q] > 0.0)) continue;
+                double s1 = 0.0, s2 = 0.0;
+                for (size_t b = 0; b < nb; b++) {
+                    for (size_t i = b * KM_SPAN; i < n && i < (b + 1) * KM_SPAN; i++)
+                        tmp[i] = lab[i] == q ? fabs(x[i] - cen[q]) : 0.0;
+                    s1 += km_block_sum(tmp, n, b);
+                    for (size_t i = b * KM_SPAN; i < n && i < (b + 1) * KM_SPAN; i++)
+                        tmp[i] = lab[i] == q ? fabs(x[i] - cen[q]) * fabs(x[i] - cen[q]) : 0.0;
+                    s2 += km_block_sum(tmp, n, b);
+                }
+                const double var = cnt[q] > 1.0 ? (s2 - s1 * s1 / cnt[q]) / (cnt[q] - 1.0) : 0.0;
+                if (var > best) { best = var; sel = q; }
+            }
+            const int want = jr_int(rng, (int)cnt[sel]);
+            int seen = 0;
+            for (size_t i = 0; i < n; i++)
+                if (lab[i] == sel && seen++ == want) { next[j] = x[i]; cnt[sel] -= 1.0; break; }
+        }
+        for (int j = 0; j < k; j++) cen[j] = next[j];
+        KM_ASSIGN(changes);
+        if (changes == 0 && !empty) break;
+    }
+    #undef KM_ASSIGN
+    free(d2); free(tmp); free(part); free(sums); free(next);
+    return k;
+}
+
+/* ClassifyRedundancy_.run on a map: the interior (border cut) clustered into
+ * k classes (or the elbow's k up to max_k), ranked by size (0 = largest, ties
+ * in cluster order); the border is 0. Returns the number of classes. */
+int orc_classify_redundancy(const float *map, int W, int H, int border, int k, int optimal_k, int max_k, int64_t seed,
+                            float *out, double *wcss_out) {
+    const int iw = W - 2 * border, ih = H - 2 * border;
+    const size_t n = (size_t)iw * ih;
+    double *x = (double *)malloc(sizeof(double) * n);
+    int *lab = (int *)malloc(sizeof(int) * n);
+    for (int y = 0; y < ih; y++)
+        for (int xx = 0; xx < iw; xx++) x[(size_t)y * iw + xx] = (double)map[(y + border) * W + xx + border];
+    jrand rng;
+    jr_init(&rng, seed);
+    double cen[64], cnt[64], wcss = 0.0;
+    int kf = k;
+    if (optimal_k) {
+        double prev = DBL_MAX;
+        kf = 1;
+        for (int kt = 1; kt <= max_k; kt++) {
+            km_run(x, n, kt, &rng, lab, cen, cnt, &wcss);
+            if (wcss < prev) { prev = wcss; kf = kt; } else break;
+        }
+    }
+    const int kc = km_run(x, n, kf, &rng, lab, cen, cnt, &wcss);
+    int order[64], rank[64];
+    for (int j = 0; j < kc; j++) order[j] = j;
+    for (int a = 1; a < kc; a++) /* stable insertion sort, largest count first */
+        for (int b = a; b > 0 && cnt[order[b]] > cnt[order[b - 1]]; b--) { int t = order[b]; order[b] = order[b - 1]; order[b - 1] = t; }
+    for (int j = 0; j < kc; j++) rank[order[j]] = j;
+    memset(out, 0, sizeof(float) * (size_t)W * H);
+    for (int y = 0; y < ih; y++)
+        for (int xx = 0; xx < iw; xx++) out[(y + border) * W + xx + border] = (float)rank[lab[(size_t)y * iw + xx]];
+    *wcss_out = wcss;
+    free(x);
+    free(lab);
+    return kc;
+}
+
+/* java.util.Random outputs for tests: next(bits) and nextDouble(). */
+void orc_java_random_next(int64_t seed, int bits, int n, int32_t *out) {
+    jrand r;
+    jr_init(&r, seed);
+    for (int i = 0; i < n; i++) out[i] = jr_next(&r, bits);
+}
+void orc_java_random_doubles(int64_t seed, int n, double *out) {
+    jrand r;
+    jr_init(&r, seed);
+    for (int i = 0; i < n; i++) out[i] = jr_double(&r);
+}

@@ -2,6 +2,7 @@
 // block repetition maps (the part of java/CLUtils.java and java/Utils.java
 // that runs between the plugin commands and the kernels).
 #include <algorithm>
+#include <cfloat>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -15,6 +16,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "shape.cuh"
+#include "cluster.cuh"
 #include "relevance.cuh"
 #include "volume.cuh"
 
@@ -25,7 +27,7 @@ namespace {
 enum BufId {
   B_IMG, B_MEANS, B_STDS, B_MASK, B_MASKIN, B_FLAGS, B_SLOT, B_GPIX, B_FPIX, B_COUNTS, B_U, B_A, B_B,
   B_PARAMS, B_RMAX, B_NUM, B_DEN, B_SUMS, B_OUT, B_VARS, B_MM, B_NMASK, B_BAD, B_STATUS, B_STDS2, B_COLSOA,
-  B_FEAT, B_SIG, B_FR, B_FI, B_GAT, B_OFF3, B_REF3, B_STAT, B_THR, B_NBUF
+  B_FEAT, B_SIG, B_FR, B_FI, B_GAT, B_OFF3, B_REF3, B_STAT, B_THR, B_KMX, B_KMD2, B_KMLAB, B_KMB, B_NBUF
 };
 
 struct DevBuf {
@@ -869,6 +871,204 @@ sred_status tool_masks(sred_ctx* c, const float* d_stat, int w, int h, const Ell
     CK(cudaMemcpyAsync(masks + px * i0, d_masks, px * m * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
   }
+  return SRED_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Redundancy classification (java/ClassifyRedundancy_.java)
+// ---------------------------------------------------------------------------
+
+// java.util.Random (48-bit linear congruential generator), the generator of
+// the clusterer (commons-math3 JDKRandomGenerator): nextInt(bound) and
+// nextDouble() as the JDK defines them.
+struct JavaRandom {
+  uint64_t seed;
+  explicit JavaRandom(int64_t s) : seed(((uint64_t)s ^ 0x5DEECE66DULL) & ((1ULL << 48) - 1)) {}
+  int next(int bits) {
+    seed = (seed * 0x5DEECE66DULL + 0xBULL) & ((1ULL << 48) - 1);
+    return (int)(int64_t)(seed >> (48 - bits));
+  }
+  int next_int(int bound) {
+    if ((bound & -bound) == bound) return (int)(((int64_t)bound * (int64_t)next(31)) >> 31);
+    int bits, val;
+    do {
+      bits = next(31);
+      val = bits % bound;
+    } while ((int64_t)bits - val + (bound - 1) > INT32_MAX);
+    return val;
+  }
+  double next_double() { return (double)(((int64_t)next(26) << 27) + next(27)) * 0x1.0p-53; }
+};
+
+struct KmState {
+  size_t n = 0;
+  int nblk = 0;
+  double *x = nullptr, *d2 = nullptr, *blk = nullptr;
+  int* lab = nullptr;
+  unsigned long long* changed = nullptr;
+};
+
+// One clustering: k-means++ centres, then Lloyd until no point changes
+// cluster (and no cluster was refilled) or 1000 rounds. Returns the centres,
+// the per-cluster counts and the WCSS; labels stay in st.lab.
+sred_status kmeans_run(sred_ctx* c, KmState& st, int k, JavaRandom& rng, std::vector<double>& centers,
+                       std::vector<double>& counts, double* wcss) {
+  cudaStream_t s = c->stream;
+  const size_t n = st.n;
+  const int nb = st.nblk;
+  std::vector<double> part(nb);
+  std::vector<size_t> taken;
+  centers.assign(k, 0.0);
+  // first centre: a uniformly chosen point
+  size_t first = (size_t)rng.next_int((int)n);
+  double xv;
+  CK(cudaMemcpyAsync(&xv, st.x + first, sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  centers[0] = xv;
+  taken.push_back(first);
+  int have = 1;
+  while (have < k) {
+    k_km_d2<<<nb, kKmThreads, 0, s>>>(st.x, n, centers[have - 1], have == 1, st.d2, st.blk);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(part.data(), st.blk, sizeof(double) * nb, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    double sum = 0.0;
+    for (int b = 0; b < nb; b++) sum += part[b];
+    const double r = rng.next_double() * sum;
+    // the first point whose running sum of d^2 reaches r: whole blocks, then
+    // the points of that block in index order
+    size_t pick = SIZE_MAX;
+    double run = 0.0;
+    for (int b = 0; b < nb && pick == SIZE_MAX; b++) {
+      if (run + part[b] < r && b + 1 < nb) {
+        run += part[b];
+        continue;
+      }
+      const size_t i0 = (size_t)b * kKmSpan, i1 = std::min(n, i0 + kKmSpan);
+      std::vector<double> d(i1 - i0);
+      CK(cudaMemcpyAsync(d.data(), st.d2 + i0, sizeof(double) * d.size(), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      for (size_t i = i0; i < i1; i++) {
+        run += d[i - i0];
+        if (run >= r && std::find(taken.begin(), taken.end(), i) == taken.end()) {
+          pick = i;
+          break;
+        }
+      }
+      if (pick == SIZE_MAX && run >= r) {
+        // rounding left r above this block's running sum: its last untaken point
+        for (size_t i = i1; i-- > i0;)
+          if (std::find(taken.begin(), taken.end(), i) == taken.end()) {
+            pick = i;
+            break;
+          }
+      }
+    }
+    if (pick == SIZE_MAX) {  // every remaining weight is 0: the last untaken point
+      for (size_t i = n; i-- > 0;)
+        if (std::find(taken.begin(), taken.end(), i) == taken.end()) {
+          pick = i;
+          break;
+        }
+    }
+    if (pick == SIZE_MAX) break;
+    CK(cudaMemcpyAsync(&xv, st.x + pick, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    centers[have++] = xv;
+    taken.push_back(pick);
+  }
+  k = have;
+  centers.resize(k);
+  double *d_c, *bsum, *bcnt, *bw;
+  CKS(ensure(c, B_KMB, (size_t)nb * (2 * k + 1) + k, &bsum));
+  bcnt = bsum + (size_t)nb * k;
+  bw = bcnt + (size_t)nb * k;
+  d_c = bw + nb;
+  std::vector<double> hs((size_t)nb * k), hc((size_t)nb * k), hw(nb);
+  CK(cudaMemsetAsync(st.lab, 0xff, n * sizeof(int), s));  // -1: every point counts as changed
+  auto assign = [&](unsigned long long* changes) -> sred_status {
+    CK(cudaMemcpyAsync(d_c, centers.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(st.changed, 0, sizeof(unsigned long long), s));
+    k_km_assign<<<nb, kKmThreads, 0, s>>>(st.x, n, d_c, k, st.lab, st.changed, bsum, bcnt, bw);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(hs.data(), bsum, sizeof(double) * hs.size(), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hc.data(), bcnt, sizeof(double) * hc.size(), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hw.data(), bw, sizeof(double) * nb, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(changes, st.changed, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return SRED_OK;
+  };
+  auto cluster_sums = [&](std::vector<double>& sum, std::vector<double>& cnt) {
+    sum.assign(k, 0.0);
+    cnt.assign(k, 0.0);
+    for (int b = 0; b < nb; b++)
+      for (int j = 0; j < k; j++) {
+        sum[j] += hs[(size_t)b * k + j];
+        cnt[j] += hc[(size_t)b * k + j];
+      }
+  };
+  unsigned long long changes = 0;
+  CKS(assign(&changes));
+  std::vector<double> sum, cnt;
+  for (int it = 0; it < 1000; it++) {
+    cluster_sums(sum, cnt);
+    bool empty = false;
+    std::vector<double> next(k);
+    for (int j = 0; j < k; j++)
+      if (cnt[j] > 0.0) next[j] = sum[j] / cnt[j];
+    for (int j = 0; j < k; j++) {
+      if (cnt[j] > 0.0) continue;
+      // empty: a random point of the cluster whose distances to its centre
+      // vary most (sample variance; 0 for a single point)
+      empty = true;
+      double* d1 = bsum;  // reuse: [nb][k] sums of |d| and of d^2
+      double* d2s = bcnt;
+      CK(cudaMemcpyAsync(d_c, centers.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
+      k_km_distvar<<<nb, kKmThreads, 0, s>>>(st.x, n, d_c, k, st.lab, d1, d2s);
+      CK(cudaGetLastError());
+      std::vector<double> a((size_t)nb * k), b2((size_t)nb * k);
+      CK(cudaMemcpyAsync(a.data(), d1, sizeof(double) * a.size(), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(b2.data(), d2s, sizeof(double) * b2.size(), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      int sel = -1;
+      double best = -HUGE_VAL;
+      for (int q = 0; q < k; q++) {
+        if (!(cnt[q] > 0.0)) continue;
+        double s1 = 0.0, s2 = 0.0;
+        for (int bb = 0; bb < nb; bb++) {
+          s1 += a[(size_t)bb * k + q];
+          s2 += b2[(size_t)bb * k + q];
+        }
+        const double var = cnt[q] > 1.0 ? (s2 - s1 * s1 / cnt[q]) / (cnt[q] - 1.0) : 0.0;
+        if (var > best) {
+          best = var;
+          sel = q;
+        }
+      }
+      if (sel < 0) return fail(c, SRED_ERR_INTERNAL, "k-means: no cluster to refill from");
+      const int want = rng.next_int((int)cnt[sel]);
+      std::vector<int> labs(n);
+      CK(cudaMemcpyAsync(labs.data(), st.lab, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      int seen = 0;
+      for (size_t i = 0; i < n; i++)
+        if (labs[i] == sel && seen++ == want) {
+          CK(cudaMemcpyAsync(&xv, st.x + i, sizeof(double), cudaMemcpyDeviceToHost, s));
+          CK(cudaStreamSynchronize(s));
+          next[j] = xv;
+          cnt[sel] -= 1.0;
+          break;
+        }
+    }
+    centers = next;
+    CKS(assign(&changes));
+    if (changes == 0 && !empty) break;
+  }
+  cluster_sums(sum, cnt);
+  counts = cnt;
+  double w = 0.0;
+  for (int b = 0; b < nb; b++) w += hw[b];
+  *wcss = w;
   return SRED_OK;
 }
 
@@ -1951,6 +2151,76 @@ sred_status sred_relevance_constant_range_2d(sred_ctx* c, const float* img, int 
   *all_ones = ones;
   *all_zeros = fc;
   *noise_var = nv;
+  return SRED_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Redundancy classification
+// ---------------------------------------------------------------------------
+
+sred_status sred_classify_redundancy_2d(sred_ctx* c, const float* map, int w, int h, int border, int k,
+                                        int optimal_k, int max_k, int64_t seed, float* out, int* k_used,
+                                        double* wcss_out) {
+  if (!c || !map || !out) return SRED_ERR_ARG;
+  if (border < 0 || w - 2 * border < 1 || h - 2 * border < 1) return fail(c, SRED_ERR_ARG, "border leaves no pixels");
+  const int kk = optimal_k ? max_k : k;
+  if (kk < 1 || kk > kKmMaxK) return fail(c, SRED_ERR_ARG, "number of classes must be in 1..64");
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->shard.valid = false;
+  cudaStream_t s = c->stream;
+  KmState st;
+  st.n = (size_t)(w - 2 * border) * (h - 2 * border);
+  if (st.n > (size_t)INT32_MAX) return fail(c, SRED_ERR_ARG, "map too large");
+  if ((size_t)kk > st.n) return fail(c, SRED_ERR_ARG, "more classes than pixels");
+  st.nblk = (int)((st.n + kKmSpan - 1) / kKmSpan);
+  float* d_map;
+  CKS(ensure(c, B_IMG, (size_t)w * h, &d_map));
+  CKS(ensure(c, B_KMX, st.n, &st.x));
+  CKS(ensure(c, B_KMD2, st.n, &st.d2));
+  CKS(ensure(c, B_KMLAB, st.n, &st.lab));
+  CKS(ensure(c, B_NMASK, 1, &st.changed));
+  CKS(ensure(c, B_VARS, 2 * (size_t)st.nblk, &st.blk));
+  CK(cudaMemcpyAsync(d_map, map, sizeof(float) * w * h, cudaMemcpyHostToDevice, s));
+  k_km_gather<<<grid_for(st.n, 256, 8 * c->num_sms), 256, 0, s>>>(d_map, w, h, border, st.x);
+  CK(cudaGetLastError());
+  JavaRandom rng(seed);
+  std::vector<double> centers, counts;
+  double wcss = 0.0;
+  int k_final = k;
+  if (optimal_k) {
+    // elbow (ClassifyRedundancy_.getOptimalK): the first k whose WCSS does not
+    // drop below the previous one ends the search at the previous k
+    double prev = DBL_MAX;
+    k_final = 1;
+    for (int kt = 1; kt <= max_k; kt++) {
+      CKS(kmeans_run(c, st, kt, rng, centers, counts, &wcss));
+      if (wcss < prev) {
+        prev = wcss;
+        k_final = kt;
+      } else {
+        break;
+      }
+    }
+  }
+  CKS(kmeans_run(c, st, k_final, rng, centers, counts, &wcss));
+  // ranks: clusters by point count, largest first, ties in cluster order
+  const int kc = (int)centers.size();
+  std::vector<int> order(kc), rank(kc);
+  for (int j = 0; j < kc; j++) order[j] = j;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return counts[a] > counts[b]; });
+  for (int j = 0; j < kc; j++) rank[order[j]] = j;
+  int* d_rank;
+  float* d_out;
+  CKS(ensure(c, B_THR, kc, &d_rank));
+  CKS(ensure(c, B_OUT, (size_t)w * h, &d_out));
+  CK(cudaMemcpyAsync(d_rank, rank.data(), sizeof(int) * kc, cudaMemcpyHostToDevice, s));
+  k_km_scatter<<<grid_for((size_t)w * h, 256, 8 * c->num_sms), 256, 0, s>>>(st.lab, d_rank, w, h, border, d_out);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, d_out, sizeof(float) * w * h, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (k_used) *k_used = kc;
+  if (wcss_out) *wcss_out = wcss;
   return SRED_OK;
 }
 

@@ -122,3 +122,32 @@ def optimise_relevance_mask(image: np.ndarray, block_width: int = 3, block_heigh
     ones, zeros, _ = clutils.relevance_constant_range_2d(relevance_tools_input(image, ctx=ctx), block_width,
                                                          block_height, step, ctx=ctx)
     return ones, zeros
+
+
+def classify_redundancy(redundancy_map: np.ndarray, border: int = 1, k: int = 3, optimal_k: bool = False,
+                        max_k: int = 10, seed: int = 0, ctx=None) -> tuple:
+    """ClassifyRedundancy_.run (java/ClassifyRedundancy_.java): (class map,
+    classes used, WCSS); see sred_classify_redundancy_2d."""
+    import ctypes as C
+    from . import _lib
+    c = ctx if ctx is not None else _lib.default_context()
+    m = np.ascontiguousarray(redundancy_map, np.float32)
+    h, w = m.shape
+    out = np.zeros(w * h, np.float32)
+    kc, wcss = C.c_int(), C.c_double()
+    c.check(c._L.sred_classify_redundancy_2d(c.h, m.ravel(), w, h, border, k, int(bool(optimal_k)), max_k, seed, out,
+                                             C.byref(kc), C.byref(wcss)), "sred_classify_redundancy_2d")
+    return out.reshape(h, w), kc.value, wcss.value
+
+
+def calculate_local_means(image: np.ndarray, block_width: int = 3, block_height: int = 3, ctx=None) -> np.ndarray:
+    """CalculateLocalMeans_.run (java/CalculateLocalMeans_.java): the relevance
+    tools' preprocessing, then the local means and standard deviations as a
+    2-slice stack [2, h, w]. As shipped the command asks its program for a
+    kernel, kernelGetPatchMeans2D, that the program (kernelGetLocalStatistics2D.cl)
+    does not define, and stops there; this returns what it evidently meant to
+    show."""
+    inp = relevance_tools_input(image, ctx=ctx)
+    h, w = inp.shape
+    st = clutils.get_local_statistics_2d(utils.InputImage2D(inp.ravel(), w, h), block_width, block_height, ctx)
+    return np.stack([st.local_means.reshape(h, w), st.local_stds.reshape(h, w)])

@@ -471,3 +471,40 @@ def test_gat_objective3d_matches_numpy():
     assert np.isnan(oracle.gat_objective3d(vol, 1.0, -1.0, 1.0))
     assert np.isnan(oracle.gat_objective3d(vol, 1.0, 1.0, -1.0))
     assert oracle.gat_objective3d(vol, 2.0, 5.0, 100.0) < 0.1 * oracle.gat_objective3d(vol, 1.0, 10.0, 100.0)
+
+
+# Redundancy classification (java/ClassifyRedundancy_.java)
+
+def test_java_random_generator():
+    """The k-means generator is java.util.Random: its 48-bit sequence equals
+    the one pinned by the reference's relevance-mask JUnit vectors (nextFloat =
+    next(24) / 2^24, seed 42), and nextDouble follows the JDK's definition."""
+    f = oracle.java_random_floats(42, 64)
+    n24 = oracle.java_random_next(42, 24, 64)
+    assert np.array_equal(f, (n24.astype(np.float64) / 2 ** 24).astype(np.float32))
+    d = oracle.java_random_doubles(42, 8)
+    # nextDouble draws next(26) then next(27) from consecutive states
+    a26 = oracle.java_random_next(42, 26, 16).astype(np.int64)
+    a27 = oracle.java_random_next(42, 27, 16).astype(np.int64)
+    seq = [float(((int(a26[2 * i]) << 27) + int(a27[2 * i + 1])) * 2.0 ** -53) for i in range(8)]
+    assert np.array_equal(d, np.array(seq))
+    assert d[0] == 0.7275636800328681 and oracle.java_random_doubles(0, 1)[0] == 0.730967787376657
+    assert 0.0 <= d.min() and d.max() < 1.0
+
+
+def test_classify_redundancy_oracle_properties():
+    from sred_b200 import synth
+    m = synth.normalize_input(synth.spot_image(90, 70, 6, seed=3))
+    for k in (1, 2, 4):
+        out, kc, wcss = oracle.classify_redundancy(m, 2, k, seed=5)
+        inner = out[2:-2, 2:-2].astype(int)
+        counts = np.bincount(inner.ravel(), minlength=kc)
+        assert kc == k and np.all(np.diff(counts) <= 0)  # ranked by size
+        assert not out[:2].any() and not out[:, :2].any()
+        # a Lloyd fixed point: each class is a contiguous value range
+        vals = m[2:-2, 2:-2]
+        cls = [vals[inner == j] for j in range(kc)]
+        spans = sorted((c.min(), c.max()) for c in cls)
+        assert all(spans[i][1] <= spans[i + 1][0] for i in range(len(spans) - 1))
+        if k > 1:
+            assert wcss < oracle.classify_redundancy(m, 2, 1, seed=5)[2]
