@@ -565,6 +565,65 @@ def run_volume_global(args, rank, local, world):
     print(json.dumps(line), flush=True)
 
 
+def run_aux(args, rank, local, world):
+    """The widened rows on one 1024x1024 image: variance stabilisation (GAT
+    fit and transform), the relevance-mask sweep (11 constants), the
+    constant-range search, and the redundancy classification (k = 3) of the
+    image's 9x9 global map. Host image in, host result out, timed per call
+    (wall clock around the synchronous C ABI call). Each line item also has
+    the oracle's single-thread CPU restatement timed on the same input (one
+    run), the reference-order baseline for these host-side Java steps."""
+    import torch
+    import oracle
+    from sred_b200 import _lib, clutils, plugins, synth, utils
+    torch.cuda.set_device(local)
+    ctx = _lib.Context(local, "tc")
+    rng = np.random.default_rng(rank)
+    lam = synth.image_1024_spots(seed=rank).clip(0, None) / 4.0
+    raw = (2.0 * rng.poisson(lam) + 100.0 + rng.normal(0, 5.0, lam.shape)).astype(np.float32)
+    inp = synth.normalize_input(raw)
+    gmap, _ = clutils.global_map_host("Pearson's R", inp, 9, 9, 1.0, True, ctx=ctx)
+
+    def timed(fn, reps):
+        fn()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            r = fn()
+        return (time.perf_counter() - t0) / reps, r
+
+    res = {}
+    t, (g, sg, o, _) = timed(lambda: utils.fit_gat_2d(raw, 5000, ctx=ctx), 1)
+    res["gat_fit_2d"] = {"ms": 1e3 * t, "params": [g, sg, o]}
+    t_cpu, _ = timed(lambda: oracle.gat_objective(raw, g, sg, o), 1)
+    res["gat_fit_2d"]["cpu_ms_per_objective"] = 1e3 * t_cpu
+    t, _ = timed(lambda: utils.get_gat_2d(raw, g, sg, o, ctx=ctx), max(3, args.steps))
+    res["gat_transform_2d"] = {"ms": 1e3 * t}
+    t_cpu, _ = timed(lambda: oracle.gat(raw, g, sg, o), 1)
+    res["gat_transform_2d"]["cpu_ms"] = 1e3 * t_cpu
+    t, _ = timed(lambda: clutils.relevance_mask_sweep_2d(inp, 3, 3, 0.0, 0.1, 11, ctx=ctx), max(3, args.steps))
+    var = oracle.local_var2d(inp, 3, 3, 0)
+    nv = oracle.tool_noise_var(inp, 0)
+    t_cpu, _ = timed(lambda: [oracle.tool_mask(var, 3, 3, nv, np.float32(0.1 * i)) for i in range(11)], 1)
+    res["relevance_sweep_11"] = {"ms": 1e3 * t, "cpu_ms_masks_only": 1e3 * t_cpu}
+    t, rr = timed(lambda: clutils.relevance_constant_range_2d(inp, 3, 3, 0.05, ctx=ctx), max(3, args.steps))
+    res["relevance_range"] = {"ms": 1e3 * t, "range": [float(rr[0]), float(rr[1])]}
+    t, (cm, kc, w) = timed(lambda: plugins.classify_redundancy(gmap, 1, 3, seed=1, ctx=ctx), 1)
+    t_cpu, _ = timed(lambda: oracle.classify_redundancy(gmap, 1, 3, seed=1), 1)
+    res["classify_k3"] = {"ms": 1e3 * t, "cpu_ms": 1e3 * t_cpu}
+    if rank != 0:
+        return
+    line = {"metric": "auxiliary steps on 1024x1024 (GAT fit, relevance tools, classification), ms per call",
+            "value": res["gat_fit_2d"]["ms"], "unit": "ms (GAT fit)", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res["gat_fit_2d"]["ms"], "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 objective, f32 masks, f64 k-means",
+            "data": "synthetic (Poisson-Gaussian spot image: gain 2, offset 100, read noise 5)",
+            "config": {"workload": "1024x1024 spot image; GAT fit from (1, 10, 100), relevance sweep 0..1 step "
+                                   "0.1, range search step 0.05, k-means k = 3 on its 9x9 global map"},
+            "per_step": res, "cpu_baseline": {"kind": "port", "cores": 1,
+                                              "sample": "oracle restatements, single thread, one run each"}}
+    print(json.dumps(line), flush=True)
+
+
 def run_shard(args, rank, local, world):
     """One global map of the default workload split by rows across the ranks
     (strong scaling): every rank prepares the same image, computes the sums
@@ -700,7 +759,7 @@ def main():
     ap.add_argument("--engine", choices=["tc", "fp32"], default="tc")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP32-engine comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["global", "block", "batch", "volume", "volume-global"],
+    ap.add_argument("--workload", choices=["global", "block", "batch", "volume", "volume-global", "aux"],
                     default="global",
                     help="global repetition map (default, the headline), the block (local) map, batched "
                          "global maps of many images, the 3D block map of a volume, or the 3D global map")
@@ -757,6 +816,8 @@ def main():
             run_volume(args, rank, local, world)
         elif args.workload == "volume-global":
             run_volume_global(args, rank, local, world)
+        elif args.workload == "aux":
+            run_aux(args, rank, local, world)
         elif args.workload == "batch":
             run_batch(args, rank, local, world)
         elif args.mode == "shard":
