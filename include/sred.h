@@ -445,6 +445,11 @@ sred_status sred_classify_redundancy_2d(sred_ctx *ctx, const float *map, int w, 
                                         int optimal_k, int max_k, int64_t seed, float *out, int *k_used,
                                         double *wcss);
 
+/* Diagnostics (no counterpart in the reference): out[i] = a[i] / b computed
+ * on the device the way the 3D Pearson block kernel divides by a shared
+ * divisor (Markstein's correction of a * RN(1/b)); equal to IEEE division. */
+sred_status sred_debug_divide_fixed(sred_ctx *ctx, const float *a, size_t n, float b, float *out);
+
 #ifdef __cplusplus
 }
 #endif

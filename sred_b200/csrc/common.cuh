@@ -77,6 +77,18 @@ __device__ __forceinline__ void store_split(__nv_bfloat16* a, __nv_bfloat16* b, 
   b[i] = hi; b[K + i] = hi; b[2 * K + i] = hi; b[3 * K + i] = mid; b[4 * K + i] = mid; b[5 * K + i] = lo;
 }
 
+// a / b, correctly rounded, for many a and one b: y = RN(1/b) once, then
+// q = RN(a y), the exact residual r = a - b q (one FMA) and RN(q + r y).
+// Markstein's theorem (P. Markstein, IBM J. Res. Dev. 34(1):111-119, 1990)
+// makes the result the correctly rounded quotient when y is the correctly
+// rounded reciprocal and q is within one ulp, barring underflow; tested
+// against IEEE division (sred_debug_divide_fixed).
+__device__ __forceinline__ float div_fixed(float a, float b, float y) {
+  const float q = __fmul_rn(a, y);
+  const float r = __fmaf_rn(-q, b, a);
+  return __fmaf_rn(r, y, q);
+}
+
 // Epilogue constants shared by all tiles of one map.
 struct EpiConsts {
   int metric;

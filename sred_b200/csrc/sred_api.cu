@@ -620,8 +620,7 @@ sred_status block3d_core(sred_ctx* c, int metric, const float* d_vol, int w, int
   CK(cudaMemcpyAsync(d_ref, ref_pixels, sizeof(float) * v.k, cudaMemcpyHostToDevice, st));
   const dim3 grid = vol_grid(v), blk(32, 4);
   k_local_stats3d<<<grid, blk, sizeof(int) * v.k, st>>>(d_vol, v, d_off, d_means, d_stds);
-  k_block_map3d<<<grid, blk, 2 * sizeof(int) * v.k, st>>>(d_vol, v, d_off, d_ref, ref_mean, ref_std, metric,
-                                                          d_means, d_stds, d_out);
+  CK(launch_block_map3d(d_vol, v, d_off, d_ref, ref_mean, ref_std, metric, d_means, d_stds, d_out, st));
   if (metric == kNrmse || metric == kAbsDiff) k_block3d_post<<<grid, blk, 0, st>>>(d_out, v, metric);
   CK(cudaGetLastError());
   float* d_mask = nullptr;
@@ -2221,6 +2220,22 @@ sred_status sred_classify_redundancy_2d(sred_ctx* c, const float* map, int w, in
   CK(cudaStreamSynchronize(s));
   if (k_used) *k_used = kc;
   if (wcss_out) *wcss_out = wcss;
+  return SRED_OK;
+}
+
+sred_status sred_debug_divide_fixed(sred_ctx* c, const float* a, size_t n, float b, float* out) {
+  if (!c || !a || !out) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->shard.valid = false;
+  float *d_a, *d_o;
+  CKS(ensure(c, B_IMG, n, &d_a));
+  CKS(ensure(c, B_OUT, n, &d_o));
+  CK(cudaMemcpyAsync(d_a, a, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  k_divide_fixed<<<grid_for(n, 256, 8 * c->num_sms), 256, 0, c->stream>>>(d_a, n, b, d_o);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, d_o, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return SRED_OK;
 }
 

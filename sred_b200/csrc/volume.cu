@@ -72,12 +72,14 @@ __global__ void __launch_bounds__(128)
   stds[p] = sqrtf(var / (float)(K - 1));
 }
 
+template <bool CACHE>
 __global__ void __launch_bounds__(128)
-    k_block_map3d(const float* __restrict__ img, Vol3 v, const int* __restrict__ off, const float* __restrict__ ref,
-                  float ref_mean, float ref_std, int metric, const float* __restrict__ means,
-                  const float* __restrict__ stds, float* __restrict__ out) {
+    k_block_map3d_t(const float* __restrict__ img, Vol3 v, const int* __restrict__ off,
+                    const float* __restrict__ ref, float ref_mean, float ref_std, int metric,
+                    const float* __restrict__ means, const float* __restrict__ stds, float* __restrict__ out) {
   extern __shared__ int s_off[];
   float* s_ref = reinterpret_cast<float*>(s_off + v.k);
+  float* s_t = s_ref + v.k;  // CACHE: [K][128] normalised block values of the Pearson chain
   for (int i = threadIdx.y * blockDim.x + threadIdx.x; i < v.k; i += blockDim.x * blockDim.y) {
     s_off[i] = off[i];
     s_ref[i] = ref[i];
@@ -100,25 +102,30 @@ __global__ void __launch_bounds__(128)
   const float tmean = means[p];
   if (metric == kPearson) {
     // cl/kernelGetBlockPearson3D.cl: min-max of the block, minus its mean,
-    // min-max again, then the covariance with the reference.
+    // min-max again, then the covariance with the reference. Every division of
+    // a pass shares its divisor (div_fixed: correctly rounded, as the
+    // kernel's own divisions); with CACHE the first normalisation is kept in
+    // shared memory for the last pass instead of being computed again.
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     float mn = FLT_MAX, mx = -FLT_MAX;
     for (int i = 0; i < K; i++) {
       const float t = c[s_off[i]];
       mn = fminf(mn, t);
       mx = fmaxf(mx, t);
     }
-    const float d1 = mx - mn + kEps;
+    const float d1 = mx - mn + kEps, y1 = __frcp_rn(d1);
     float mn2 = FLT_MAX, mx2 = -FLT_MAX;
     for (int i = 0; i < K; i++) {
-      const float t = (c[s_off[i]] - mn) / d1 - tmean;
+      const float t = div_fixed(c[s_off[i]] - mn, d1, y1) - tmean;
+      if (CACHE) s_t[i * 128 + tid] = t;
       mn2 = fminf(mn2, t);
       mx2 = fmaxf(mx2, t);
     }
-    const float d2 = mx2 - mn2 + kEps;
+    const float d2 = mx2 - mn2 + kEps, y2 = __frcp_rn(d2);
     float cov = 0.0f;
     for (int i = 0; i < K; i++) {
-      const float t = (((c[s_off[i]] - mn) / d1 - tmean) - mn2) / d2;
-      cov += s_ref[i] * t;
+      const float t = CACHE ? s_t[i * 128 + tid] : div_fixed(c[s_off[i]] - mn, d1, y1) - tmean;
+      cov += s_ref[i] * div_fixed(t - mn2, d2, y2);
     }
     cov /= (float)(K - 1);
     if (ref_std == 0.0f && tstd == 0.0f) out[p] = 1.0f;
@@ -149,6 +156,36 @@ __global__ void __launch_bounds__(128)
   }
   mse /= (float)K;
   out[p] = sqrtf(mse);
+}
+
+cudaError_t launch_block_map3d(const float* img, Vol3 v, const int* off, const float* ref, float ref_mean,
+                               float ref_std, int metric, const float* means, const float* stds, float* out,
+                               cudaStream_t st) {
+  const dim3 grid((v.W + 31) / 32, (v.H + 3) / 4, v.D), blk(32, 4);
+  // The Pearson chain caches its first normalisation (K x 128 floats) while
+  // that fits in 96 KB of shared memory; past it, it recomputes.
+  const size_t smem_base = 2 * sizeof(int) * (size_t)v.k;
+  const size_t smem_cache = smem_base + sizeof(float) * 128 * (size_t)v.k;
+  if (metric == kPearson && smem_cache <= 96 * 1024) {
+    if (smem_cache > 48 * 1024) {
+      const cudaError_t e =
+          cudaFuncSetAttribute(k_block_map3d_t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cache);
+      if (e != cudaSuccess) return e;
+    }
+    k_block_map3d_t<true><<<grid, blk, smem_cache, st>>>(img, v, off, ref, ref_mean, ref_std, metric, means, stds,
+                                                         out);
+  } else {
+    k_block_map3d_t<false><<<grid, blk, smem_base, st>>>(img, v, off, ref, ref_mean, ref_std, metric, means, stds,
+                                                          out);
+  }
+  return cudaGetLastError();
+}
+
+// Elementwise a[i] / b by div_fixed (diagnostics: checked against IEEE division).
+__global__ void k_divide_fixed(const float* __restrict__ a, size_t n, float b, float* __restrict__ out) {
+  const float y = __frcp_rn(b);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = div_fixed(a[i], b, y);
 }
 
 // Host steps on the interior (java/CLUtils.java:1459-1471, 1590-1600): NRMSE

@@ -22,8 +22,12 @@ int build_ellipsoid(int bw, int bh, int bd, int W, int H, int* off);
 // One thread per voxel; dynamic shared memory: k ints (stats), k ints + k
 // floats (block map).
 __global__ void k_local_stats3d(const float* img, Vol3 v, const int* off, float* means, float* stds);
-__global__ void k_block_map3d(const float* img, Vol3 v, const int* off, const float* ref, float ref_mean,
-                              float ref_std, int metric, const float* means, const float* stds, float* out);
+// The raw 3D block map (one thread per voxel; the dynamic shared memory it
+// needs is chosen here).
+cudaError_t launch_block_map3d(const float* img, Vol3 v, const int* off, const float* ref, float ref_mean,
+                               float ref_std, int metric, const float* means, const float* stds, float* out,
+                               cudaStream_t st);
+__global__ void k_divide_fixed(const float* a, size_t n, float b, float* out);
 __global__ void k_block3d_post(float* a, Vol3 v, int metric);
 __global__ void k_mask3d(const float* stds, Vol3 v, float thr, float* mask, float* map);
 __global__ void k_minmax3d(const float* a, const float* mask, Vol3 v, unsigned* mm);

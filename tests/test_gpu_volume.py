@@ -205,3 +205,22 @@ def test_global_map_3d_device_and_edges(ctx):
                                                    0.0, True, ctx=ctx)
     with pytest.raises(_lib.SredError):
         clutils.calculate_global_repetition_map_3d("SSIM", _inp(vol), 3, 4, 3, 0.0, True, ctx=ctx)
+
+
+def test_fixed_divisor_division_is_ieee(ctx):
+    """div_fixed (Markstein's correction of a * RN(1/b)) against IEEE float32
+    division on 4M numerators per divisor: uniform in [0, 1], tiny (down to
+    1e-30), powers of two and exact multiples of the divisor, and divisors
+    spanning the normalisation ranges of the Pearson chain."""
+    rng = np.random.default_rng(21)
+    a = np.concatenate([rng.random(1 << 21, dtype=np.float32),
+                        (10.0 ** rng.uniform(-30, 0, 1 << 20)).astype(np.float32),
+                        (2.0 ** rng.integers(-60, 1, 1 << 19)).astype(np.float32),
+                        np.zeros(16, np.float32)])
+    for b in [np.float32(x) for x in (1e-7, 3.1e-4, 0.0123, 0.1, 0.7071068, 0.99999994, 1.0000001, 1.9999999)]:
+        aa = np.concatenate([a, (b * np.arange(1, 1 << 19, dtype=np.float32)).astype(np.float32)])
+        out = np.empty_like(aa)
+        ctx.check(ctx._L.sred_debug_divide_fixed(ctx.h, aa, aa.size, float(b), out), "sred_debug_divide_fixed")
+        exp = aa / b
+        bad = np.flatnonzero(out.view(np.uint32) != exp.view(np.uint32))
+        assert bad.size == 0, (b, aa[bad[:5]], out[bad[:5]], exp[bad[:5]])
