@@ -450,6 +450,32 @@ sred_status sred_classify_redundancy_2d(sred_ctx *ctx, const float *map, int w, 
  * divisor (Markstein's correction of a * RN(1/b)); equal to IEEE division. */
 sred_status sred_debug_divide_fixed(sred_ctx *ctx, const float *a, size_t n, float b, float *out);
 
+/* Variance stabilisation by the quadtree (2D) / octree (3D) method, the
+ * "Quad/Octree" option (java/QuadTree_.java, java/OcTree_.java; the commands'
+ * defaults and java/Utils.java:686-705 use min_size 4, alpha 0.01, max_iter
+ * 50, lts_fraction 0.75). The image is split recursively into quadrants
+ * (octants) while a node is larger than min_size along every axis and the
+ * Fisher test finds its variance different from the variance of its
+ * Laplacian pseudo-residuals (ratio of the smaller to the larger below the
+ * alpha quantile of F(n-1, n-1); n = width*height, in 3D too); every leaf
+ * gives a robust (Gaussian-weighted) mean and a least-trimmed-squares
+ * variance; a least-squares line through the (mean, variance) pairs gives g0
+ * (slope) and eDC (intercept), and every pixel is transformed in place as
+ * applyGATtree does ((g0 v + 3/8 g0^2 + eDC) < 0 -> 0, else (2/g0) sqrt(...)).
+ * Statistics are FP64 sums on the device (the reference: FP32), the F
+ * quantiles host FP64 (the reference: commons-math3 FDistribution). In 3D all
+ * w*h*d voxels are transformed (the reference's Utils call transforms the
+ * first w*h). SRED_ERR_ARG if the regression has no slope. */
+sred_status sred_gat_quadtree_2d(sred_ctx *ctx, float *img, int w, int h, int min_size, float alpha, int max_iter,
+                                 float lts_fraction, double *g0, double *edc, int *n_leaves);
+sred_status sred_gat_octree_3d(sred_ctx *ctx, float *vol, int w, int h, int d, int min_size, float alpha,
+                               int max_iter, float lts_fraction, double *g0, double *edc, int *n_leaves);
+
+/* Quantile at p of the F distribution with (df, df) degrees of freedom, the
+ * threshold of the trees' Fisher test (host only; NaN outside 0 < p < 1,
+ * df > 0). */
+double sred_f_quantile(double p, double df);
+
 #ifdef __cplusplus
 }
 #endif

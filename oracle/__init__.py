@@ -34,6 +34,7 @@ _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _fp = C.POINTER(C.c_float)
+_dp = C.POINTER(C.c_double)
 
 _lib = None
 _ref = None
@@ -120,6 +121,11 @@ def lib() -> C.CDLL:
                                               C.c_int64, _f32p, C.POINTER(C.c_double)]
         L.orc_java_random_next.argtypes = [C.c_int64, C.c_int, C.c_int, np.ctypeslib.ndpointer(np.int32)]
         L.orc_java_random_doubles.argtypes = [C.c_int64, C.c_int, _f64p]
+        L.orc_f_quantile.restype = C.c_double
+        L.orc_f_quantile.argtypes = [C.c_double, C.c_double]
+        L.orc_gat_tree.restype = C.c_int
+        L.orc_gat_tree.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int,
+                                   C.c_float, _dp, _dp, np.ctypeslib.ndpointer(np.int32), _f32p, _f32p, C.c_int]
         L.orc_gat_objective.restype = C.c_double
         L.orc_gat_objective.argtypes = [_f32p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
         L.orc_patch_hu1_ref.restype = C.c_double
@@ -751,3 +757,27 @@ def java_random_doubles(seed, n):
     out = np.zeros(n, np.float64)
     lib().orc_java_random_doubles(seed, n, out)
     return out
+
+
+def f_quantile(p, df):
+    return float(lib().orc_f_quantile(float(p), float(df)))
+
+
+def gat_tree(img, octree=False, min_size=4, alpha=0.01, max_iter=50, frac=0.75, max_leaves=1 << 20):
+    """QuadTree_ / OcTree_ variance stabilisation restated (FP32 reference
+    order): dict with the transformed image, g0, eDC and the leaves."""
+    a = _f32(img).copy()
+    if octree:
+        D, H, W = a.shape
+    else:
+        (H, W), D = a.shape, 1
+    g0, edc = C.c_double(), C.c_double()
+    boxes = np.zeros(6 * max_leaves, np.int32)
+    means = np.zeros(max_leaves, np.float32)
+    var = np.zeros(max_leaves, np.float32)
+    nl = lib().orc_gat_tree(a.ravel(), W, H, D, int(octree), min_size, C.c_float(alpha), max_iter, C.c_float(frac),
+                            C.byref(g0), C.byref(edc), boxes, means, var, max_leaves)
+    if nl < 0:
+        raise ValueError("the regression has no slope")
+    return {"image": a, "g0": g0.value, "edc": edc.value, "boxes": boxes[:6 * nl].reshape(nl, 6),
+            "means": means[:nl], "vars": var[:nl]}

@@ -1904,3 +1904,234 @@ void orc_java_random_doubles(int64_t seed, int n, double *out) {
     jr_init(&r, seed);
     for (int i = 0; i < n; i++) out[i] = jr_double(&r);
 }
+
+/* ------------------------------------------------------------------ */
+/* Quadtree / octree variance stabilisation (java/QuadTree_.java,       */
+/* java/OcTree_.java), literally: recursive build, FP32 sums in raster  */
+/* order, Fisher test with the F quantile (same bisection of the        */
+/* regularised incomplete beta as the library: Numerical Recipes'       */
+/* continued fraction, modified Lentz), robust means, LTS variances by  */
+/* sorting, SimpleRegression's updating sums, applyGATtree.             */
+/* ------------------------------------------------------------------ */
+static double orc_betacf(double a, double b, double x) {
+    const double fpmin = 1e-300, eps = 1e-16;
+    double qab = a + b, qap = a + 1.0, qam = a - 1.0, c = 1.0, d = 1.0 - qab * x / qap;
+    if (fabs(d) < fpmin) d = fpmin;
+    d = 1.0 / d;
+    double h = d;
+    for (int m = 1; m <= 1000000; m++) {
+        int m2 = 2 * m;
+        double aa = m * (b - m) * x / ((qam + m2) * (a + m2));
+        d = 1.0 + aa * d; if (fabs(d) < fpmin) d = fpmin;
+        c = 1.0 + aa / c; if (fabs(c) < fpmin) c = fpmin;
+        d = 1.0 / d; h *= d * c;
+        aa = -(a + m) * (qab + m) * x / ((a + m2) * (qap + m2));
+        d = 1.0 + aa * d; if (fabs(d) < fpmin) d = fpmin;
+        c = 1.0 + aa / c; if (fabs(c) < fpmin) c = fpmin;
+        d = 1.0 / d;
+        double del = d * c;
+        h *= del;
+        if (fabs(del - 1.0) < eps) break;
+    }
+    return h;
+}
+static double orc_ibeta(double a, double b, double x) {
+    if (x <= 0.0) return 0.0;
+    if (x >= 1.0) return 1.0;
+    double front = exp(lgamma(a + b) - lgamma(a) - lgamma(b) + a * log(x) + b * log1p(-x));
+    if (x < (a + 1.0) / (a + b + 2.0)) return front * orc_betacf(a, b, x) / a;
+    return 1.0 - front * orc_betacf(b, a, 1.0 - x) / b;
+}
+double orc_f_quantile(double p, double df) {
+    double a = 0.5 * df, lo = 0.0, hi = 1.0;
+    for (int it = 0; it < 200; it++) {
+        double mid = 0.5 * (lo + hi);
+        if (mid <= lo || mid >= hi) break;
+        if (orc_ibeta(a, a, mid) < p) lo = mid; else hi = mid;
+    }
+    double x = 0.5 * (lo + hi);
+    return x / (1.0 - x);
+}
+
+typedef struct { int x, y, z, w, h, d; } tbox;
+typedef struct {
+    const float *img;
+    int W, H, D, oct, min_size, max_iter;
+    float alpha, frac;
+    tbox *leaves;
+    int n_leaves, cap;
+} tctx;
+
+static float tree_block_var(const tctx *t, tbox b) {
+    /* 2D: Utils.getMeanAndVarBlock2D (FP32); 3D: getMeanAndVarBlock3D (FP64) */
+    const long n = (long)b.w * b.h * b.d;
+    if (!t->oct) {
+        float mean = 0.0f, sq = 0.0f;
+        for (int y = b.y; y < b.y + b.h; y++)
+            for (int x = b.x; x < b.x + b.w; x++) {
+                float v = t->img[(long)y * t->W + x];
+                mean += v;
+                sq += v * v;
+            }
+        mean = mean / (float)n;
+        return sq / (float)n - mean * mean;
+    }
+    double mean = 0.0, sq = 0.0;
+    for (int z = b.z; z < b.z + b.d; z++)
+        for (int y = b.y; y < b.y + b.h; y++)
+            for (int x = b.x; x < b.x + b.w; x++) {
+                double v = (double)t->img[((long)z * t->H + y) * t->W + x];
+                mean += v;
+                sq += v * v;
+            }
+    mean = mean / n;
+    return (float)(sq / n - mean * mean);
+}
+
+static float tree_noise_var(const tctx *t, tbox b) {
+    const int W = t->W, H = t->H, D = t->D;
+    const float l = t->oct ? 7.0f : 5.0f;
+    const float scale = (float)(1.0 / sqrt((double)(l * l + l)));
+    const long n = (long)b.w * b.h * b.d;
+    float *r = (float *)malloc(sizeof(float) * (size_t)n);
+    long k = 0;
+    for (int z = b.z; z < b.z + b.d; z++)
+        for (int y = b.y; y < b.y + b.h; y++)
+            for (int x = b.x; x < b.x + b.w; x++) {
+                const long p = ((long)z * H + y) * W + x;
+                float lap = l * t->img[p];
+                if (x > 0) lap -= t->img[p - 1];
+                if (x < W - 1) lap -= t->img[p + 1];
+                if (y > 0) lap -= t->img[p - W];
+                if (y < H - 1) lap -= t->img[p + W];
+                if (t->oct) {
+                    if (z > 0) lap -= t->img[p - (long)W * H];
+                    if (z < D - 1) lap -= t->img[p + (long)W * H];
+                }
+                r[k++] = lap * scale;
+            }
+    float s = 0.0f;
+    for (long i = 0; i < n; i++) s += r[i];
+    const float m = s / (float)n;
+    float ss = 0.0f;
+    for (long i = 0; i < n; i++) ss += (float)pow((double)r[i] - (double)m, 2.0);
+    free(r);
+    return ss / ((float)n - 1.0f);
+}
+
+static void tree_build(tctx *t, tbox b) {
+    const float vz = tree_block_var(t, b), ve = tree_noise_var(t, b);
+    const float ratio = fminf(vz, ve) / fmaxf(vz, ve);
+    const long df = (long)b.w * b.h - 1;
+    const float thr = df >= 1 ? (float)orc_f_quantile((double)t->alpha, (double)df) : 0.0f;
+    const int divide = ratio < thr;
+    if (b.w <= t->min_size || b.h <= t->min_size || (t->oct && b.d <= t->min_size) || !divide) {
+        if (t->n_leaves == t->cap) {
+            t->cap = t->cap ? 2 * t->cap : 64;
+            t->leaves = (tbox *)realloc(t->leaves, sizeof(tbox) * t->cap);
+        }
+        t->leaves[t->n_leaves++] = b;
+        return;
+    }
+    const int hw = b.w / 2, hh = b.h / 2, hd = t->oct ? b.d / 2 : 1;
+    const int nch = t->oct ? 8 : 4;
+    for (int k = 0; k < nch; k++) {
+        tbox c = {b.x + ((k & 1) ? hw : 0), b.y + ((k & 2) ? hh : 0), b.z + ((k & 4) ? hd : 0), hw, hh, hd};
+        tree_build(t, c);
+    }
+}
+
+static float tree_robust_mean(const tctx *t, tbox b) {
+    float mean = 0.0f, var = 0.0f;
+    long n = 0;
+    for (int z = b.z; z < b.z + b.d; z++)
+        for (int y = b.y; y < b.y + b.h; y++)
+            for (int x = b.x; x < b.x + b.w; x++) {
+                float v = t->img[((long)z * t->H + y) * t->W + x];
+                mean += v;
+                var += (v - mean) * (v - mean);
+                n++;
+            }
+    mean /= (float)n;
+    var /= (float)(n - 1);
+    var = fmaxf(var, ORC_EPS);
+    float prev;
+    int it = 0;
+    do {
+        prev = mean;
+        float ws = 0.0f, wv = 0.0f;
+        for (int z = b.z; z < b.z + b.d; z++)
+            for (int y = b.y; y < b.y + b.h; y++)
+                for (int x = b.x; x < b.x + b.w; x++) {
+                    float v = t->img[((long)z * t->H + y) * t->W + x];
+                    float w = (float)exp(-((double)(v - mean) * (double)(v - mean)) / (2.0 * (double)var));
+                    ws += w;
+                    wv += w * v;
+                }
+        mean = wv / fmaxf(ws, ORC_EPS);
+        it++;
+    } while (fabsf(mean - prev) > 1e-5f && it < t->max_iter);
+    return mean;
+}
+
+static int cmp_f(const void *a, const void *b) {
+    float x = *(const float *)a, y = *(const float *)b;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+static float tree_lts(const tctx *t, tbox b, float m) {
+    const long n = (long)b.w * b.h * b.d;
+    float *r = (float *)malloc(sizeof(float) * (size_t)n);
+    long k = 0;
+    for (int z = b.z; z < b.z + b.d; z++)
+        for (int y = b.y; y < b.y + b.h; y++)
+            for (int x = b.x; x < b.x + b.w; x++) {
+                float v = t->img[((long)z * t->H + y) * t->W + x];
+                r[k++] = (v - m) * (v - m);
+            }
+    qsort(r, (size_t)n, sizeof(float), cmp_f);
+    const int h = (int)floorf(t->frac * (float)n);
+    float s = 0.0f;
+    for (int i = 0; i < h; i++) s += r[i];
+    free(r);
+    return s / ((float)h + ORC_EPS);
+}
+
+/* Returns the number of leaves (or -1 if the regression has no slope);
+ * leaves (x, y, z, w, h, d each), means and variances go to the out arrays
+ * when given (capacity max_leaves). img is transformed in place. */
+int orc_gat_tree(float *img, int W, int H, int D, int oct, int min_size, float alpha, int max_iter, float frac,
+                 double *g0_out, double *edc_out, int *boxes_out, float *means_out, float *vars_out, int max_leaves) {
+    tctx t = {img, W, H, D, oct, min_size, max_iter, alpha, frac, NULL, 0, 0};
+    tbox root = {0, 0, 0, W, H, D};
+    tree_build(&t, root);
+    double sx = 0, sy = 0, sxx = 0, sxy = 0, xbar = 0, ybar = 0;
+    for (int i = 0; i < t.n_leaves; i++) {
+        const float m = tree_robust_mean(&t, t.leaves[i]);
+        const float v = tree_lts(&t, t.leaves[i], m);
+        if (i < max_leaves) {
+            if (boxes_out) memcpy(boxes_out + 6 * i, &t.leaves[i], sizeof(tbox));
+            if (means_out) means_out[i] = m;
+            if (vars_out) vars_out[i] = v;
+        }
+        const double x = m, y = v;
+        if (i == 0) { xbar = x; ybar = y; }
+        else {
+            const double nn = (double)i, f1 = 1.0 + nn, f2 = nn / (1.0 + nn), dx = x - xbar, dy = y - ybar;
+            sxx += dx * dx * f2; sxy += dx * dy * f2; xbar += dx / f1; ybar += dy / f1;
+        }
+        sx += x; sy += y;
+    }
+    const int nl = t.n_leaves;
+    free(t.leaves);
+    if (nl < 2 || fabs(sxx) < 10 * DBL_MIN) return -1;
+    const double g0 = sxy / sxx, edc = (sy - g0 * sx) / nl, c = 0.375 * g0 * g0 + edc;
+    for (long i = 0; i < (long)W * H * D; i++) {
+        double v = (double)img[i];
+        v = (g0 * v + c) < 0.0 ? 0.0 : (2.0 / g0) * sqrt(g0 * v + c);
+        img[i] = (float)v;
+    }
+    *g0_out = g0;
+    *edc_out = edc;
+    return nl;
+}

@@ -18,10 +18,10 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
          "--expt-relaxed-constexpr", "-Xptxas", "-v"]
-SOURCES = ["sred_api.cu", "moments.cu", "block_map.cu", "global_fp32.cu", "global_tc.cu", "noalloc.cu", "shape.cu", "gat.cu", "volume.cu", "relevance.cu", "cluster.cu"]
-# shape.cu, gat.cu, volume.cu and relevance.cu restate the reference's FP32/FP64 evaluation order: no fused multiply-add.
+SOURCES = ["sred_api.cu", "moments.cu", "block_map.cu", "global_fp32.cu", "global_tc.cu", "noalloc.cu", "shape.cu", "gat.cu", "volume.cu", "relevance.cu", "cluster.cu", "gat_tree.cu"]
+# shape.cu, gat.cu, volume.cu, relevance.cu and gat_tree.cu restate the reference's FP32/FP64 evaluation order: no fused multiply-add.
 FILE_FLAGS = {"shape.cu": ["-fmad=false"], "gat.cu": ["-fmad=false"], "volume.cu": ["-fmad=false"],
-              "relevance.cu": ["-fmad=false"]}
+              "relevance.cu": ["-fmad=false"], "gat_tree.cu": ["-fmad=false"]}
 
 
 def _digest() -> str:

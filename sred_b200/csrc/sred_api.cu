@@ -17,6 +17,7 @@
 #include "kernels.cuh"
 #include "shape.cuh"
 #include "cluster.cuh"
+#include "gat_tree.cuh"
 #include "relevance.cuh"
 #include "volume.cuh"
 
@@ -27,7 +28,7 @@ namespace {
 enum BufId {
   B_IMG, B_MEANS, B_STDS, B_MASK, B_MASKIN, B_FLAGS, B_SLOT, B_GPIX, B_FPIX, B_COUNTS, B_U, B_A, B_B,
   B_PARAMS, B_RMAX, B_NUM, B_DEN, B_SUMS, B_OUT, B_VARS, B_MM, B_NMASK, B_BAD, B_STATUS, B_STDS2, B_COLSOA,
-  B_FEAT, B_SIG, B_FR, B_FI, B_GAT, B_OFF3, B_REF3, B_STAT, B_THR, B_KMX, B_KMD2, B_KMLAB, B_KMB, B_NBUF
+  B_FEAT, B_SIG, B_FR, B_FI, B_GAT, B_OFF3, B_REF3, B_STAT, B_THR, B_KMX, B_KMD2, B_KMLAB, B_KMB, B_TBOX, B_TSTAT, B_TMEAN, B_TVAR, B_NBUF
 };
 
 struct DevBuf {
@@ -1068,6 +1069,218 @@ sred_status kmeans_run(sred_ctx* c, KmState& st, int k, JavaRandom& rng, std::ve
   double w = 0.0;
   for (int b = 0; b < nb; b++) w += hw[b];
   *wcss = w;
+  return SRED_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Quadtree / octree variance stabilisation (java/QuadTree_.java, OcTree_.java)
+// ---------------------------------------------------------------------------
+
+// Regularised incomplete beta I_x(a, b) by the continued fraction of
+// Numerical Recipes (Press et al., 3rd ed., section 6.4: the fraction
+// evaluated with the modified Lentz method, Lentz 1976), with the symmetry
+// I_x(a, b) = 1 - I_{1-x}(b, a) where the fraction converges slowly.
+double beta_cf(double a, double b, double x) {
+  const double fpmin = 1e-300, eps = 1e-16;
+  const double qab = a + b, qap = a + 1.0, qam = a - 1.0;
+  double c = 1.0, d = 1.0 - qab * x / qap;
+  if (std::fabs(d) < fpmin) d = fpmin;
+  d = 1.0 / d;
+  double h = d;
+  for (int m = 1; m <= 1000000; m++) {
+    const int m2 = 2 * m;
+    double aa = m * (b - m) * x / ((qam + m2) * (a + m2));
+    d = 1.0 + aa * d;
+    if (std::fabs(d) < fpmin) d = fpmin;
+    c = 1.0 + aa / c;
+    if (std::fabs(c) < fpmin) c = fpmin;
+    d = 1.0 / d;
+    h *= d * c;
+    aa = -(a + m) * (qab + m) * x / ((a + m2) * (qap + m2));
+    d = 1.0 + aa * d;
+    if (std::fabs(d) < fpmin) d = fpmin;
+    c = 1.0 + aa / c;
+    if (std::fabs(c) < fpmin) c = fpmin;
+    d = 1.0 / d;
+    const double del = d * c;
+    h *= del;
+    if (std::fabs(del - 1.0) < eps) break;
+  }
+  return h;
+}
+
+double reg_inc_beta(double a, double b, double x) {
+  if (x <= 0.0) return 0.0;
+  if (x >= 1.0) return 1.0;
+  const double front = std::exp(std::lgamma(a + b) - std::lgamma(a) - std::lgamma(b) + a * std::log(x) +
+                                b * std::log1p(-x));
+  if (x < (a + 1.0) / (a + b + 2.0)) return front * beta_cf(a, b, x) / a;
+  return 1.0 - front * beta_cf(b, a, 1.0 - x) / b;
+}
+
+// Quantile at p of the F distribution with (df, df) degrees of freedom: X ~
+// F(df, df) iff X / (1 + X) ~ Beta(df/2, df/2); the Beta quantile by
+// bisection of I_x(df/2, df/2) to the last bit.
+double f_quantile_equal_df(double p, double df) {
+  const double a = 0.5 * df;
+  double lo = 0.0, hi = 1.0;
+  for (int it = 0; it < 200; it++) {
+    const double mid = 0.5 * (lo + hi);
+    if (mid <= lo || mid >= hi) break;
+    if (reg_inc_beta(a, a, mid) < p) lo = mid;
+    else hi = mid;
+  }
+  const double x = 0.5 * (lo + hi);
+  return x / (1.0 - x);
+}
+
+// The Fisher test of the reference (QuadTree_.performFisherTest): split when
+// min(var)/max(var) < F^-1(alpha; n - 1, n - 1), the quantile as float.
+bool fisher_split(double var_z, double var_e, int64_t region, float alpha, std::vector<std::pair<int64_t, float>>& cache) {
+  const float vz = (float)var_z, ve = (float)var_e;
+  const float ratio = std::min(vz, ve) / std::max(vz, ve);
+  const int64_t df = region - 1;
+  if (df < 1) return false;
+  float thr = 0.0f;
+  bool found = false;
+  for (auto& e : cache)
+    if (e.first == df) {
+      thr = e.second;
+      found = true;
+      break;
+    }
+  if (!found) {
+    thr = (float)f_quantile_equal_df((double)alpha, (double)df);
+    cache.emplace_back(df, thr);
+  }
+  return ratio < thr;
+}
+
+// Least-squares line through (mean, variance) pairs, updated point by point
+// as commons-math3's SimpleRegression does (centred sums with the running
+// means; slope = Sxy / Sxx, intercept = (sum y - slope sum x) / n).
+void simple_regression(const std::vector<double>& xs, const std::vector<double>& ys, double* slope, double* icpt) {
+  double sx = 0, sy = 0, sxx = 0, sxy = 0, xbar = 0, ybar = 0;
+  for (size_t i = 0; i < xs.size(); i++) {
+    const double x = xs[i], y = ys[i];
+    if (i == 0) {
+      xbar = x;
+      ybar = y;
+    } else {
+      const double n = (double)i, f1 = 1.0 + n, f2 = n / (1.0 + n);
+      const double dx = x - xbar, dy = y - ybar;
+      sxx += dx * dx * f2;
+      sxy += dx * dy * f2;
+      xbar += dx / f1;
+      ybar += dy / f1;
+    }
+    sx += x;
+    sy += y;
+  }
+  const double n = (double)xs.size();
+  *slope = (n < 2 || std::fabs(sxx) < 10 * DBL_MIN) ? std::nan("") : sxy / sxx;
+  *icpt = (sy - *slope * sx) / n;
+}
+
+// The tree of QuadTree_ / OcTree_ built level by level (every level's split
+// criteria in one launch), then the robust mean and LTS variance of every
+// leaf (one launch each), the regression of the leaves' variances on their
+// means in the reference's leaf order (depth first, children in the order
+// the reference creates them), and the transform with its slope and
+// intercept. d_img holds the image (w x h x d) on the device.
+sred_status gat_tree_core(sred_ctx* c, float* d_img, int w, int h, int d, bool octree, int min_size, float alpha,
+                          int max_iter, float frac, double* g0_out, double* edc_out, int* n_leaves) {
+  if (min_size < 1 || !(alpha > 0.0f && alpha < 1.0f) || max_iter < 1 || !(frac > 0.0f && frac <= 1.0f))
+    return fail(c, SRED_ERR_ARG, "tree GAT: min_size >= 1, 0 < alpha < 1, max_iter >= 1, 0 < fraction <= 1");
+  cudaStream_t st = c->stream;
+  const float l = octree ? 7.0f : 5.0f;
+  const float scale = (float)(1.0 / std::sqrt((double)(l * l + l)));
+  struct Node {
+    TreeBox b;
+    int first_child;  // -1: leaf
+  };
+  std::vector<Node> nodes{{{0, 0, 0, w, h, d}, -1}};
+  std::vector<int> level{0};
+  std::vector<std::pair<int64_t, float>> fcache;
+  const int nch = octree ? 8 : 4;
+  while (!level.empty()) {
+    // nodes the size test lets split: only their criterion matters
+    std::vector<int> cand;
+    for (int i : level) {
+      const TreeBox& b = nodes[i].b;
+      if (!(b.w <= min_size || b.h <= min_size || (octree && b.d <= min_size))) cand.push_back(i);
+    }
+    std::vector<int> next;
+    if (!cand.empty()) {
+      TreeBox* d_boxes;
+      double* d_stats;
+      CKS(ensure(c, B_TBOX, cand.size(), &d_boxes));
+      CKS(ensure(c, B_TSTAT, 2 * cand.size(), &d_stats));
+      std::vector<TreeBox> hb(cand.size());
+      for (size_t j = 0; j < cand.size(); j++) hb[j] = nodes[cand[j]].b;
+      CK(cudaMemcpyAsync(d_boxes, hb.data(), sizeof(TreeBox) * hb.size(), cudaMemcpyHostToDevice, st));
+      k_tree_node_stats<<<(unsigned)cand.size(), kTreeThreads, 0, st>>>(d_img, w, h, d, d_boxes, octree ? 1 : 0,
+                                                                         scale, d_stats);
+      CK(cudaGetLastError());
+      std::vector<double> hs(2 * cand.size());
+      CK(cudaMemcpyAsync(hs.data(), d_stats, sizeof(double) * hs.size(), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      for (size_t j = 0; j < cand.size(); j++) {
+        const TreeBox b = nodes[cand[j]].b;
+        // the reference's degrees of freedom: width * height - 1, in 3D too
+        if (!fisher_split(hs[2 * j], hs[2 * j + 1], (int64_t)b.w * b.h, alpha, fcache)) continue;
+        const int hw = b.w / 2, hh = b.h / 2, hd = octree ? b.d / 2 : 1;
+        nodes[cand[j]].first_child = (int)nodes.size();
+        for (int k = 0; k < nch; k++) {
+          const int ox = (k & 1) ? hw : 0, oy = (k & 2) ? hh : 0, oz = (k & 4) ? hd : 0;
+          nodes.push_back({{b.x + ox, b.y + oy, b.z + oz, hw, hh, hd}, -1});
+          next.push_back((int)nodes.size() - 1);
+        }
+      }
+    }
+    level.swap(next);
+  }
+  // leaves in the reference's traversal order
+  std::vector<TreeBox> leaves;
+  std::vector<int> stack{0};
+  while (!stack.empty()) {
+    const int i = stack.back();
+    stack.pop_back();
+    if (nodes[i].first_child < 0) {
+      leaves.push_back(nodes[i].b);
+    } else {
+      for (int k = nch - 1; k >= 0; k--) stack.push_back(nodes[i].first_child + k);
+    }
+  }
+  const size_t nl = leaves.size();
+  TreeBox* d_boxes;
+  float *d_means, *d_vars;
+  CKS(ensure(c, B_TBOX, nl, &d_boxes));
+  CKS(ensure(c, B_TMEAN, nl, &d_means));
+  CKS(ensure(c, B_TVAR, nl, &d_vars));
+  CK(cudaMemcpyAsync(d_boxes, leaves.data(), sizeof(TreeBox) * nl, cudaMemcpyHostToDevice, st));
+  k_tree_robust_mean<<<(unsigned)nl, kTreeThreads, 0, st>>>(d_img, w, h, d_boxes, max_iter, d_means);
+  k_tree_lts<<<(unsigned)nl, kTreeThreads, 0, st>>>(d_img, w, h, d_boxes, d_means, frac, d_vars);
+  CK(cudaGetLastError());
+  std::vector<float> hm(nl), hv(nl);
+  CK(cudaMemcpyAsync(hm.data(), d_means, sizeof(float) * nl, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(hv.data(), d_vars, sizeof(float) * nl, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  std::vector<double> xs(nl), ys(nl);
+  for (size_t i = 0; i < nl; i++) {
+    xs[i] = hm[i];
+    ys[i] = hv[i];
+  }
+  double g0, edc;
+  simple_regression(xs, ys, &g0, &edc);
+  if (!std::isfinite(g0) || g0 == 0.0) return fail(c, SRED_ERR_ARG, "tree GAT: the regression has no slope");
+  // applyGATtree: refConstant = 3/8 g0^2 + eDC; (g0 v + c) < 0 -> 0
+  const size_t n = (size_t)w * h * d;
+  k_gat<<<grid_for(n, 256, 8 * c->num_sms), 256, 0, st>>>(d_img, n, g0, 0.375 * g0 * g0 + edc);
+  CK(cudaGetLastError());
+  *g0_out = g0;
+  *edc_out = edc;
+  if (n_leaves) *n_leaves = (int)nl;
   return SRED_OK;
 }
 
@@ -2238,5 +2451,43 @@ sred_status sred_debug_divide_fixed(sred_ctx* c, const float* a, size_t n, float
   CK(cudaStreamSynchronize(c->stream));
   return SRED_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Quadtree / octree variance stabilisation
+// ---------------------------------------------------------------------------
+
+sred_status sred_gat_quadtree_2d(sred_ctx* c, float* img, int w, int h, int min_size, float alpha, int max_iter,
+                                 float lts_fraction, double* g0, double* edc, int* n_leaves) {
+  if (!c || !img || !g0 || !edc || w <= 0 || h <= 0) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->shard.valid = false;
+  const size_t n = (size_t)w * h;
+  float* d;
+  CKS(ensure(c, B_IMG, n, &d));
+  CK(cudaMemcpyAsync(d, img, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  CKS(gat_tree_core(c, d, w, h, 1, false, min_size, alpha, max_iter, lts_fraction, g0, edc, n_leaves));
+  CK(cudaMemcpyAsync(img, d, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SRED_OK;
+}
+
+sred_status sred_gat_octree_3d(sred_ctx* c, float* vol, int w, int h, int d, int min_size, float alpha, int max_iter,
+                               float lts_fraction, double* g0, double* edc, int* n_leaves) {
+  if (!c || !vol || !g0 || !edc || w <= 0 || h <= 0 || d <= 0) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->shard.valid = false;
+  const size_t n = (size_t)w * h * d;
+  float* dv;
+  CKS(ensure(c, B_IMG, n, &dv));
+  CK(cudaMemcpyAsync(dv, vol, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  CKS(gat_tree_core(c, dv, w, h, d, true, min_size, alpha, max_iter, lts_fraction, g0, edc, n_leaves));
+  CK(cudaMemcpyAsync(vol, dv, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SRED_OK;
+}
+
+double sred_f_quantile(double p, double df) { return (p > 0.0 && p < 1.0 && df > 0.0) ? f_quantile_equal_df(p, df) : std::nan(""); }
 
 }  // extern "C"

@@ -5,9 +5,10 @@ keyword arguments (same defaults) and the windowing left out.
 (java/GlobalRepetition2D_.java:35-156), ``block_repetition_2d``
 BlockRepetition2D_.run (java/BlockRepetition2D_.java:32-158), the 3D pair
 GlobalRepetition3D_ / BlockRepetition3D_, and the relevance-mask tools
-RelevanceMask2D_, RelevanceMaskStack2D_ and OptimiseRelevanceMask_. Variance
-stabilisation uses the GPU GAT fit ("Simplex"); the reference's other
-estimation method ("Quad/Octree") is not provided.
+RelevanceMask2D_, RelevanceMaskStack2D_ and OptimiseRelevanceMask_,
+ClassifyRedundancy_, CalculateLocalMeans_, and the variance-stabilisation
+commands QuadTree_ / OcTree_. Variance stabilisation inside the map commands
+uses either GAT method ("Simplex" or "Quad/Octree").
 """
 from __future__ import annotations
 
@@ -151,3 +152,15 @@ def calculate_local_means(image: np.ndarray, block_width: int = 3, block_height:
     h, w = inp.shape
     st = clutils.get_local_statistics_2d(utils.InputImage2D(inp.ravel(), w, h), block_width, block_height, ctx)
     return np.stack([st.local_means.reshape(h, w), st.local_stds.reshape(h, w)])
+
+
+def quadtree_gat_2d(image: np.ndarray, min_size: int = 4, alpha: float = 0.01, max_iterations: int = 50,
+                    lts_fraction: float = 0.75, ctx=None) -> tuple:
+    """QuadTree_.run (java/QuadTree_.java): (variance-stabilised image, g0, eDC, leaves)."""
+    return utils.gat_quadtree_2d(image, min_size, alpha, max_iterations, lts_fraction, ctx=ctx)
+
+
+def octree_gat_3d(volume: np.ndarray, min_size: int = 4, alpha: float = 0.01, max_iterations: int = 50,
+                  lts_fraction: float = 0.75, ctx=None) -> tuple:
+    """OcTree_.run (java/OcTree_.java): (variance-stabilised volume, g0, eDC, leaves)."""
+    return utils.gat_octree_3d(volume, min_size, alpha, max_iterations, lts_fraction, ctx=ctx)

@@ -93,20 +93,49 @@ def fit_gat_2d(image: np.ndarray, max_iter: int = 5000, gain: float = 1.0, sigma
     return g.value, s.value, o.value, e.value
 
 
+def gat_quadtree_2d(image: np.ndarray, min_size: int = 4, alpha: float = 0.01, max_iter: int = 50,
+                    lts_fraction: float = 0.75, ctx=None) -> tuple:
+    """Quadtree variance stabilisation (java/QuadTree_.java) on the GPU:
+    (transformed image, g0, eDC, leaves)."""
+    c = _ctx(ctx)
+    a = np.ascontiguousarray(image, dtype=np.float32).copy()
+    h, w = a.shape
+    g0, edc, nl = C.c_double(), C.c_double(), C.c_int()
+    c.check(c._L.sred_gat_quadtree_2d(c.h, a, w, h, int(min_size), float(alpha), int(max_iter), float(lts_fraction),
+                                      C.byref(g0), C.byref(edc), C.byref(nl)), "sred_gat_quadtree_2d")
+    return a, g0.value, edc.value, nl.value
+
+
+def gat_octree_3d(volume: np.ndarray, min_size: int = 4, alpha: float = 0.01, max_iter: int = 50,
+                  lts_fraction: float = 0.75, ctx=None) -> tuple:
+    """Octree variance stabilisation (java/OcTree_.java) on the GPU:
+    (transformed volume, g0, eDC, leaves)."""
+    c = _ctx(ctx)
+    a = np.ascontiguousarray(volume, dtype=np.float32).copy()
+    d, h, w = a.shape
+    g0, edc, nl = C.c_double(), C.c_double(), C.c_int()
+    c.check(c._L.sred_gat_octree_3d(c.h, a, w, h, d, int(min_size), float(alpha), int(max_iter), float(lts_fraction),
+                                    C.byref(g0), C.byref(edc), C.byref(nl)), "sred_gat_octree_3d")
+    return a, g0.value, edc.value, nl.value
+
+
 def get_input_image_2d(image: np.ndarray, normalize_output: bool = True, stabilise_noise_variance: bool = False,
                        gat_method: str = "Simplex", max_iter: int = 5000, ctx=None) -> InputImage2D:
     """java/Utils.java:653-725 for an image given as an array: float
-    conversion, optional variance stabilisation (the Simplex method: the GAT
-    parameters fitted on the GPU, then the transform), and min-max to [0, 1]
-    with epsilon, in FP32. The reference's other method ("Quad/Octree") is
-    not provided."""
+    conversion, optional variance stabilisation ("Simplex": the GAT
+    parameters fitted on the GPU, then the transform; "Quad/Octree": the
+    quadtree method with the reference's fixed parameters, java/Utils.java:686-705),
+    and min-max to [0, 1] with epsilon, in FP32."""
     a = np.ascontiguousarray(image, dtype=np.float32)
     h, w = a.shape
     if stabilise_noise_variance:
-        if gat_method != "Simplex":
-            raise ValueError(f"unsupported GAT method {gat_method!r} (only 'Simplex')")
-        gain, sigma, offset, _ = fit_gat_2d(a, max_iter, ctx=ctx)
-        a = get_gat_2d(a, np.float32(gain), np.float32(sigma), np.float32(offset), ctx=ctx)
+        if gat_method == "Simplex":
+            gain, sigma, offset, _ = fit_gat_2d(a, max_iter, ctx=ctx)
+            a = get_gat_2d(a, np.float32(gain), np.float32(sigma), np.float32(offset), ctx=ctx)
+        elif gat_method == "Quad/Octree":
+            a = gat_quadtree_2d(a, 4, 0.01, 50, 0.75, ctx=ctx)[0]
+        else:
+            raise ValueError(f"unknown GAT method {gat_method!r}")
     if normalize_output:
         mn, mx = np.float32(a.min()), np.float32(a.max())
         a = ((a - mn) / (mx - mn + EPSILON)).astype(np.float32)
@@ -257,15 +286,19 @@ def get_input_image_3d(volume: np.ndarray, stabilise_noise_variance: bool = Fals
     returns the transformed volume: the image-ID version transforms copies it
     then drops (java/Utils.java:1216-1232), the array version normalises an
     array it never filled (java/Utils.java:1311-1327, a volume of zeros); here
-    the volume is transformed, then normalised. The "Quad/Octree" method is
-    not provided."""
+    the volume is transformed, then normalised. "Quad/Octree": the octree
+    method with the reference's fixed parameters (java/Utils.java:1235-1250),
+    every voxel transformed."""
     a = np.ascontiguousarray(volume, dtype=np.float32)
     d, h, w = a.shape
     if stabilise_noise_variance:
-        if gat_method != "Simplex":
-            raise ValueError(f"unsupported GAT method {gat_method!r} (only 'Simplex')")
-        gain, sigma, offset, _ = fit_gat_3d(a, max_iter, ctx=ctx)
-        a = get_gat_3d(a, gain, sigma, offset, ctx=ctx)
+        if gat_method == "Simplex":
+            gain, sigma, offset, _ = fit_gat_3d(a, max_iter, ctx=ctx)
+            a = get_gat_3d(a, gain, sigma, offset, ctx=ctx)
+        elif gat_method == "Quad/Octree":
+            a = gat_octree_3d(a, 4, 0.01, 50, 0.75, ctx=ctx)[0]
+        else:
+            raise ValueError(f"unknown GAT method {gat_method!r}")
     if normalize_output:
         mn, mx = np.float32(a.min()), np.float32(a.max())
         a = ((a - mn) / (mx - mn + EPSILON)).astype(np.float32)

@@ -75,3 +75,43 @@ def test_gat_3d(ctx):
     assert err <= oracle.gat_objective3d(vol, 2.0, 5.0, 100.0) * (1 + 1e-9), (gain, sigma, offset, err)
     inp = utils.get_input_image_3d(vol, True, True, ctx=ctx)
     assert inp.depth == 48 and 0.0 <= inp.image_array.min() and inp.image_array.max() <= 1.0
+
+
+def _pg_spots(shape, seed):
+    from sred_b200 import synth
+    rng = np.random.default_rng(seed)
+    if len(shape) == 2:
+        lam = synth.spot_image(shape[1], shape[0], 8, seed=seed, read_noise=0.0)
+    else:
+        lam = synth.spot_volume(shape[2], shape[1], shape[0], 4, 2, seed=seed, read_noise=0.0)
+    lam = lam.clip(0, None) / 4
+    return (2.0 * rng.poisson(lam) + 100.0 + rng.normal(0, 5.0, lam.shape)).astype(np.float32)
+
+
+@pytest.mark.parametrize("shape", [(96, 128), (200, 160), (36, 40, 48)])
+def test_gat_tree_matches_restatement(ctx, shape):
+    """QuadTree_ / OcTree_ against the oracle's literal FP32 restatement: the
+    same leaves; g0, eDC and the transformed image within the difference of
+    FP32 (reference) and FP64 (here) sums."""
+    img = _pg_spots(shape, 3 + len(shape))
+    octree = len(shape) == 3
+    r = oracle.gat_tree(img, octree=octree)
+    if octree:
+        out, g0, edc, nl = utils.gat_octree_3d(img, ctx=ctx)
+    else:
+        out, g0, edc, nl = utils.gat_quadtree_2d(img, ctx=ctx)
+    assert nl == len(r["boxes"])
+    assert abs(g0 - r["g0"]) <= 2e-3 * abs(r["g0"]) and abs(edc - r["edc"]) <= 2e-3 * abs(r["edc"]), (g0, edc, r)
+    ref = r["image"]
+    assert float(np.max(np.abs(out - ref) / np.maximum(np.abs(ref), 1.0))) <= 2e-3
+
+
+def test_gat_tree_in_input_images(ctx):
+    img = _pg_spots((96, 128), 9)
+    inp = utils.get_input_image_2d(img, True, True, "Quad/Octree", ctx=ctx)
+    assert inp.image_array.min() == 0.0 and inp.image_array.max() <= 1.0
+    vol = _pg_spots((24, 40, 48), 10)
+    inp3 = utils.get_input_image_3d(vol, True, True, "Quad/Octree", ctx=ctx)
+    assert inp3.depth == 24 and np.isfinite(inp3.image_array).all()
+    with pytest.raises(_lib.SredError):
+        utils.gat_quadtree_2d(img, min_size=0, ctx=ctx)

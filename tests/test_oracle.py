@@ -508,3 +508,29 @@ def test_classify_redundancy_oracle_properties():
         assert all(spans[i][1] <= spans[i + 1][0] for i in range(len(spans) - 1))
         if k > 1:
             assert wcss < oracle.classify_redundancy(m, 2, 1, seed=5)[2]
+
+
+def test_f_quantile_matches_scipy():
+    """The Fisher test's threshold (QuadTree_.performFisherTest): F(df, df)
+    quantiles by bisection of the regularised incomplete beta, in the oracle
+    and in the library (host function), against scipy."""
+    from scipy import stats
+    from sred_b200 import _lib
+    L = _lib.load()
+    for df in [1, 2, 3, 8, 15, 63, 255, 4095, 65535, 1048575]:
+        for p in [0.001, 0.01, 0.05, 0.5, 0.9]:
+            e = stats.f.ppf(p, df, df)
+            a = oracle.f_quantile(p, df)
+            assert abs(a - e) <= 1e-10 * e, (df, p, a, e)
+            assert L.sred_f_quantile(p, df) == a
+
+
+def test_gat_tree_oracle_properties():
+    from sred_b200 import synth
+    rng = np.random.default_rng(1)
+    lam = synth.spot_image(128, 96, 8, seed=2, read_noise=0.0).clip(0, None) / 4
+    img = (2.0 * rng.poisson(lam) + 100 + rng.normal(0, 5.0, lam.shape)).astype(np.float32)
+    r = oracle.gat_tree(img)
+    b = r["boxes"]
+    assert (b[:, 3] * b[:, 4]).sum() <= 128 * 96 and len(b) > 16  # disjoint leaves inside the image
+    assert r["g0"] > 0 and np.isfinite(r["image"]).all()
