@@ -324,12 +324,14 @@ def get_local_statistics_3d(input_image: InputImage3D, block_width: int, block_h
 
 def calculate_block_repetition_map_3d(metric: str, input_image: InputImage3D, reference_block: ReferenceBlock3D,
                                       relevance_constant: float, normalize_output: bool, use_device: bool = False,
-                                      ctx=None):
-    """java/CLUtils.java:1639-1653 (None for an unknown metric)."""
+                                      ctx=None, out: np.ndarray | None = None):
+    """java/CLUtils.java:1639-1653 (None for an unknown metric). ``out``: an
+    optional float32 buffer of the volume's size to write into (pinned host
+    memory makes the copies faster)."""
     if metric not in BLOCK_METRICS_3D:
         return None
     c = _ctx(ctx)
-    out = np.zeros(input_image.size, np.float32)
+    out = np.zeros(input_image.size, np.float32) if out is None else out.reshape(-1)
     rb = reference_block
     c.check(c._L.sred_calculate_block_repetition_map_3d(
         c.h, metric.encode(), np.ascontiguousarray(input_image.image_array, np.float32).ravel(), input_image.width,
@@ -368,7 +370,7 @@ def block_map_3d_device(metric: str, d_vol_ptr: int, width: int, height: int, de
 
 def calculate_global_repetition_map_3d(metric: str, input_image: InputImage3D, block_width: int, block_height: int,
                                        block_depth: int, relevance_constant: float, normalize_output: bool = True,
-                                       ctx=None, return_info: bool = False):
+                                       ctx=None, return_info: bool = False, out: np.ndarray | None = None):
     """java/CLUtils.java:2793-2816 with the preprocessing of
     java/GlobalRepetition3D_.java:97-143 (local statistics, the 3D relevance
     mask, nPixels) done inside libsred. None for an unknown metric; with
@@ -376,7 +378,7 @@ def calculate_global_repetition_map_3d(metric: str, input_image: InputImage3D, b
     if metric not in GLOBAL_METRICS:
         return None
     c = _ctx(ctx)
-    out = np.zeros(input_image.size, np.float32)
+    out = np.zeros(input_image.size, np.float32) if out is None else out.reshape(-1)
     info = _lib.RunInfo()
     c.check(c._L.sred_calculate_global_repetition_map_3d(
         c.h, metric.encode(), np.ascontiguousarray(input_image.image_array, np.float32).ravel(), input_image.width,
