@@ -476,6 +476,17 @@ sred_status sred_gat_octree_3d(sred_ctx *ctx, float *vol, int w, int h, int d, i
  * df > 0). */
 double sred_f_quantile(double p, double df);
 
+/* Row-sharded 3D global map (no counterpart in the reference): the two
+ * phases of sred_global_map_2d_shard_sums / _finish for
+ * sred_global_map_3d_device; the sums layout and the row split are the same
+ * ([num | den] over the relevant non-zero-variance blocks, 128-row blocks of
+ * the compacted list). Either finish function completes either map. */
+sred_status sred_global_map_3d_shard_sums(sred_ctx *ctx, const char *metric, const float *d_vol, int w, int h, int d,
+                                          int bw, int bh, int bd, float relevance_constant, int shard, int n_shards,
+                                          double *d_sums, size_t capacity, void *stream, sred_run_info *info);
+sred_status sred_global_map_3d_shard_finish(sred_ctx *ctx, const double *d_sums, int normalize_output,
+                                            float *d_out, void *stream, sred_run_info *info);
+
 #ifdef __cplusplus
 }
 #endif

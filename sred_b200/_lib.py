@@ -32,6 +32,7 @@ EXPORTS = [
     "sred_relevance_mask_tool_2d", "sred_relevance_mask_sweep_2d", "sred_relevance_constant_range_2d",
     "sred_gat_3d", "sred_gat_objective_3d", "sred_gat_fit_3d", "sred_classify_redundancy_2d",
     "sred_debug_divide_fixed", "sred_gat_quadtree_2d", "sred_gat_octree_3d", "sred_f_quantile",
+    "sred_global_map_3d_shard_sums", "sred_global_map_3d_shard_finish",
 ]
 
 
@@ -131,6 +132,9 @@ def load() -> C.CDLL:
         L.sred_gat_octree_3d.argtypes = [_vp, _f32p, s, s, s, s, f, s, f, _dp, _dp, C.POINTER(C.c_int)]
         L.sred_f_quantile.restype = C.c_double
         L.sred_f_quantile.argtypes = [C.c_double, C.c_double]
+        L.sred_global_map_3d_shard_sums.argtypes = [_vp, C.c_char_p, _vp, s, s, s, s, s, s, f, s, s, _vp, C.c_size_t,
+                                                    _vp, C.POINTER(RunInfo)]
+        L.sred_global_map_3d_shard_finish.argtypes = [_vp, _vp, s, _vp, _vp, C.POINTER(RunInfo)]
         L.sred_relevance_mask_tool_2d.argtypes = [_vp, _f32p, s, s, s, s, f, _f32p, _fp, _fp]
         L.sred_relevance_mask_sweep_2d.argtypes = [_vp, _f32p, s, s, s, s, f, f, s, _f32p, _f32p, _fp]
         L.sred_relevance_constant_range_2d.argtypes = [_vp, _f32p, s, s, s, s, f, _fp, _fp, _fp]

@@ -446,3 +446,34 @@ def relevance_constant_range_2d(image: np.ndarray, block_width: int, block_heigh
                                                   C.byref(ones), C.byref(zeros), C.byref(nv)),
             "sred_relevance_constant_range_2d")
     return np.float32(ones.value), np.float32(zeros.value), np.float32(nv.value)
+
+
+def global_map_3d_device_sharded(metric: str, d_vol_ptr: int, width: int, height: int, depth: int, block_width: int,
+                                 block_height: int, block_depth: int, relevance_constant: float,
+                                 normalize_output: bool, d_out_ptr: int, rank: int, world: int, allreduce=None,
+                                 stream_ptr: int = 0, ctx=None) -> dict:
+    """One 3D global map computed by `world` ranks, as global_map_device_sharded."""
+    import torch
+    c = _ctx(ctx)
+    cap = 2 * max(1, width * height * depth)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    sums = torch.zeros(cap, dtype=torch.float64, device=dev)
+    info1, info2 = _lib.RunInfo(), _lib.RunInfo()
+    if allreduce is None:
+        import torch.distributed as dist
+        allreduce = dist.all_reduce
+
+    def compute():
+        c.check(c._L.sred_global_map_3d_shard_sums(
+            c.h, metric.encode(), C.c_void_p(d_vol_ptr), width, height, depth, block_width, block_height, block_depth,
+            float(relevance_constant), int(rank), int(world), C.c_void_p(sums.data_ptr()), cap,
+            C.c_void_p(stream_ptr or None), C.byref(info1)), "sred_global_map_3d_shard_sums")
+        return sums, int(info1.n_relevant - info1.n_flat)
+
+    def fin(summed):
+        c.check(c._L.sred_global_map_3d_shard_finish(c.h, C.c_void_p(summed.data_ptr()), int(bool(normalize_output)),
+                                                     C.c_void_p(d_out_ptr), C.c_void_p(stream_ptr or None),
+                                                     C.byref(info2)), "sred_global_map_3d_shard_finish")
+        return info2.as_dict()
+
+    return sharded_exchange(compute, fin, allreduce)

@@ -41,6 +41,8 @@ struct DevBuf {
 // between the two phases of the row-sharded entry points.
 struct GState {
   bool valid = false;
+  bool vol = false;  // a 3D map (depth d, z radius rd)
+  int d = 1, rd = 0;
   int metric = 0, w = 0, h = 0, rw = 0, rh = 0, K = 0, n_g = 0, n_flat = 0, engine = 0, kp = 0, kq = 0;
   size_t n = 0, n_pad = 0;
   float nv = 0, thr = 0, npx = 0, relc = 0;
@@ -647,8 +649,9 @@ sred_status block3d_core(sred_ctx* c, int metric, const float* d_vol, int w, int
 // statistics, the relevance mask of getRelevanceMask3D (the command passes
 // the 2D mask, which fails on its first interior slice), the compacted block
 // lists, the all-pairs contraction on the 2D engines, the 3D host steps.
-sred_status global3d_core(sred_ctx* c, int metric, const float* d_vol, int w, int h, int d, int bw, int bh, int bd,
-                          float relc, int normalize, float* d_out, cudaStream_t st, sred_run_info* info) {
+sred_status global3d_prepare(sred_ctx* c, int metric, const float* d_vol, int w, int h, int d, int bw, int bh,
+                             int bd, float relc, cudaStream_t st, GState* gs) {
+  gs->valid = false;
   c->shard.valid = false;  // shares workspaces with the 2D global map
   if (fault("launch")) return fail(c, SRED_ERR_LAUNCH, "injected launch failure");
   CK(cudaEventRecord(c->ev[0], st));
@@ -742,18 +745,43 @@ sred_status global3d_core(sred_ctx* c, int metric, const float* d_vol, int w, in
     CK(cudaGetLastError());
   }
   CK(cudaEventRecord(c->ev[1], st));
-  GState gs;
-  gs.metric = metric == kNrmse ? kNrmseW : metric;
-  gs.K = K;
-  gs.n_g = n_g;
-  gs.engine = engine;
-  gs.kp = kp;
-  gs.kq = kq;
-  gs.n_pad = n_pad;
-  CKS(global_gram(c, gs, st, 0, -1));
-  k_finalize3d<<<grid, blk, 0, st>>>(d_slot, v, d_num, d_den, d_params, n_flat, metric,
-                                     std::sqrt((double)(K - 1) / (double)K), (double)npx, d_mask,
-                                     relc > 0.0f ? 1 : 0, d_out);
+  gs->vol = true;
+  gs->metric = metric == kNrmse ? kNrmseW : metric;
+  gs->w = w;
+  gs->h = h;
+  gs->d = d;
+  gs->rw = v.rw;
+  gs->rh = v.rh;
+  gs->rd = v.rd;
+  gs->K = K;
+  gs->n_g = n_g;
+  gs->n_flat = n_flat;
+  gs->engine = engine;
+  gs->kp = kp;
+  gs->kq = kq;
+  gs->n = n;
+  gs->n_pad = n_pad;
+  gs->nv = nv;
+  gs->thr = thr;
+  gs->npx = npx;
+  gs->relc = relc;
+  gs->valid = true;
+  return SRED_OK;
+}
+
+// Finalisation of a prepared 3D map whose num/den workspaces hold the sums.
+sred_status global3d_finish(sred_ctx* c, const GState& gs, cudaStream_t st, int normalize, float* d_out,
+                            sred_run_info* info) {
+  const int metric = gs.metric == kNrmseW ? kNrmse : gs.metric;
+  const Vol3 v{gs.w, gs.h, gs.d, gs.rw, gs.rh, gs.rd, gs.K};
+  const dim3 grid = vol_grid(v), blk(32, 4);
+  const float* d_mask = static_cast<const float*>(c->buf[B_MASK].p);
+  k_finalize3d<<<grid, blk, 0, st>>>(static_cast<const int*>(c->buf[B_SLOT].p), v,
+                                     static_cast<const double*>(c->buf[B_NUM].p),
+                                     static_cast<const double*>(c->buf[B_DEN].p),
+                                     static_cast<const BlockParams*>(c->buf[B_PARAMS].p), gs.n_flat, metric,
+                                     std::sqrt((double)(gs.K - 1) / (double)gs.K), (double)gs.npx, d_mask,
+                                     gs.relc > 0.0f ? 1 : 0, d_out);
   CK(cudaGetLastError());
   if (normalize) {
     unsigned* mm;
@@ -767,15 +795,16 @@ sred_status global3d_core(sred_ctx* c, int metric, const float* d_vol, int w, in
   CK(cudaEventRecord(c->ev[3], st));
   CK(cudaEventSynchronize(c->ev[3]));
   if (info) {
-    info->n_blocks = (int64_t)std::max(0, w - 2 * v.rw) * std::max(0, h - 2 * v.rh) * std::max(0, d - 2 * v.rd);
-    info->n_relevant = (int64_t)n_g + n_flat;
-    info->n_flat = n_flat;
-    info->pairs = (double)n_g * (double)info->n_relevant;
-    info->noise_var = nv;
-    info->threshold = thr;
-    info->n_pixels = npx;
-    info->k = K;
-    info->engine = engine;
+    info->n_blocks = (int64_t)std::max(0, gs.w - 2 * gs.rw) * std::max(0, gs.h - 2 * gs.rh) *
+                     std::max(0, gs.d - 2 * gs.rd);
+    info->n_relevant = (int64_t)gs.n_g + gs.n_flat;
+    info->n_flat = gs.n_flat;
+    info->pairs = (double)gs.n_g * (double)info->n_relevant;
+    info->noise_var = gs.nv;
+    info->threshold = gs.thr;
+    info->n_pixels = gs.npx;
+    info->k = gs.K;
+    info->engine = gs.engine;
     float t01 = 0, t12 = 0, t23 = 0, t03 = 0;
     cudaEventElapsedTime(&t01, c->ev[0], c->ev[1]);
     cudaEventElapsedTime(&t12, c->ev[1], c->ev[2]);
@@ -785,17 +814,26 @@ sred_status global3d_core(sred_ctx* c, int metric, const float* d_vol, int w, in
     info->ms_gram = t12;
     info->ms_finalize = t23;
     info->ms_total = t03;
-    info->launches = 5 + (n_g > 0 ? (engine == SRED_ENGINE_TC ? 3 : 2) : 0) + 1 + (normalize ? 2 : 0);
+    info->launches = 5 + (gs.n_g > 0 ? (gs.engine == SRED_ENGINE_TC ? 3 : 2) : 0) + 1 + (normalize ? 2 : 0);
   }
   if (c->log_cb) {
     float t03 = 0;
     cudaEventElapsedTime(&t03, c->ev[0], c->ev[3]);
     char line[256];
-    std::snprintf(line, sizeof(line), "global map %dx%dx%d K=%d: %d reference blocks, %d flat test blocks, %s engine, %.3f ms",
-                  w, h, d, K, n_g, n_flat, engine == SRED_ENGINE_TC ? "tensor-core" : "fp32", t03);
+    std::snprintf(line, sizeof(line),
+                  "global map %dx%dx%d K=%d: %d reference blocks, %d flat test blocks, %s engine, %.3f ms", gs.w,
+                  gs.h, gs.d, gs.K, gs.n_g, gs.n_flat, gs.engine == SRED_ENGINE_TC ? "tensor-core" : "fp32", t03);
     log_msg(c, line);
   }
   return SRED_OK;
+}
+
+sred_status global3d_core(sred_ctx* c, int metric, const float* d_vol, int w, int h, int d, int bw, int bh, int bd,
+                          float relc, int normalize, float* d_out, cudaStream_t st, sred_run_info* info) {
+  GState gs;
+  CKS(global3d_prepare(c, metric, d_vol, w, h, d, bw, bh, bd, relc, st, &gs));
+  CKS(global_gram(c, gs, st, 0, -1));
+  return global3d_finish(c, gs, st, normalize, d_out, info);
 }
 
 // ---------------------------------------------------------------------------
@@ -1606,7 +1644,7 @@ sred_status sred_global_map_2d_shard_finish(sred_ctx* c, const double* d_sums, i
   if (!c || !d_sums || !d_out) return SRED_ERR_ARG;
   std::lock_guard<std::recursive_mutex> lk(c->mu);
   cudaSetDevice(c->device);
-  if (!c->shard.valid) return fail(c, SRED_ERR_ARG, "no map prepared by sred_global_map_2d_shard_sums on this context");
+  if (!c->shard.valid) return fail(c, SRED_ERR_ARG, "no map prepared by a shard_sums call on this context");
   cudaStream_t st = pick(c, stream);
   const GState gs = c->shard;
   c->shard.valid = false;
@@ -1617,7 +1655,48 @@ sred_status sred_global_map_2d_shard_finish(sred_ctx* c, const double* d_sums, i
   CK(cudaEventRecord(c->ev[0], st));
   CK(cudaEventRecord(c->ev[1], st));
   CK(cudaEventRecord(c->ev[2], st));
-  return global_finish(c, gs, st, normalize, d_out, info);
+  return gs.vol ? global3d_finish(c, gs, st, normalize, d_out, info) : global_finish(c, gs, st, normalize, d_out, info);
+}
+
+sred_status sred_global_map_3d_shard_sums(sred_ctx* c, const char* metric, const float* d_vol, int w, int h, int d,
+                                          int bw, int bh, int bd, float relc, int shard, int n_shards, double* d_sums,
+                                          size_t capacity, void* stream, sred_run_info* info) {
+  if (!c || !d_vol || !d_sums || n_shards < 1 || shard < 0 || shard >= n_shards) return SRED_ERR_ARG;
+  const int m = global_metric(metric);
+  if (m < 0) return fail(c, SRED_ERR_UNKNOWN_METRIC, "unknown global metric");
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  cudaStream_t st = pick(c, stream);
+  GState gs;
+  CKS(global3d_prepare(c, m, d_vol, w, h, d, bw, bh, bd, relc, st, &gs));
+  if (capacity < 2 * (size_t)gs.n_g) return fail(c, SRED_ERR_ARG, "sums buffer smaller than 2 x relevant blocks");
+  int rb0, rb1;
+  shard_row_blocks(gs.n_g, shard, n_shards, &rb0, &rb1);
+  if (rb0 < rb1) CKS(global_gram(c, gs, st, rb0, rb1));
+  if (gs.n_g > 0) {
+    CK(cudaMemcpyAsync(d_sums, c->buf[B_NUM].p, gs.n_g * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(d_sums + gs.n_g, c->buf[B_DEN].p, gs.n_g * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  if (info) {
+    std::memset(info, 0, sizeof(*info));
+    info->n_blocks = (int64_t)std::max(0, w - 2 * gs.rw) * std::max(0, h - 2 * gs.rh) * std::max(0, d - 2 * gs.rd);
+    info->n_relevant = (int64_t)gs.n_g + gs.n_flat;
+    info->n_flat = gs.n_flat;
+    info->pairs = (double)gs.n_g * (double)info->n_relevant;
+    info->noise_var = gs.nv;
+    info->threshold = gs.thr;
+    info->n_pixels = gs.npx;
+    info->k = gs.K;
+    info->engine = gs.engine;
+  }
+  c->shard = gs;
+  return SRED_OK;
+}
+
+sred_status sred_global_map_3d_shard_finish(sred_ctx* c, const double* d_sums, int normalize, float* d_out,
+                                            void* stream, sred_run_info* info) {
+  return sred_global_map_2d_shard_finish(c, d_sums, normalize, d_out, stream, info);
 }
 
 sred_status sred_global_map_2d_device(sred_ctx* c, const char* metric, const float* d_img, int w, int h, int bw,

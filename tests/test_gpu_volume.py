@@ -224,3 +224,39 @@ def test_fixed_divisor_division_is_ieee(ctx):
         exp = aa / b
         bad = np.flatnonzero(out.view(np.uint32) != exp.view(np.uint32))
         assert bad.size == 0, (b, aa[bad[:5]], out[bad[:5]], exp[bad[:5]])
+
+
+def test_sharded_3d_map_equals_full_map(ctx):
+    """The row-sharded 3D entry points, every shard run in turn on one GPU and
+    their sums added (what the all-reduce does across GPUs), give the map of
+    sred_global_map_3d_device."""
+    import ctypes as C
+
+    import torch
+    vol = synth.normalize_input(synth.spot_volume(40, 36, 20, 4, 2, seed=9))
+    d, h, w = vol.shape
+    d_in = torch.from_numpy(vol).cuda()
+    for engine in ("tc", "fp32"):
+        ctx.set_engine(engine)
+        for metric in clutils.GLOBAL_METRICS:
+            full = torch.empty_like(d_in)
+            clutils.global_map_3d_device(metric, d_in.data_ptr(), w, h, d, 3, 3, 3, 1.0, True, full.data_ptr(),
+                                         ctx=ctx)
+            torch.cuda.synchronize()
+            for world in (2, 3):
+                cap = 2 * vol.size
+                acc = torch.zeros(cap, dtype=torch.float64, device="cuda")
+                for s in range(world):
+                    part = torch.zeros(cap, dtype=torch.float64, device="cuda")
+                    info = _lib.RunInfo()
+                    ctx.check(ctx._L.sred_global_map_3d_shard_sums(
+                        ctx.h, metric.encode(), C.c_void_p(d_in.data_ptr()), w, h, d, 3, 3, 3, 1.0, s, world,
+                        C.c_void_p(part.data_ptr()), cap, None, C.byref(info)), "shard_sums")
+                    acc += part
+                out = torch.empty_like(d_in)
+                ctx.check(ctx._L.sred_global_map_3d_shard_finish(ctx.h, C.c_void_p(acc.data_ptr()), 1,
+                                                                 C.c_void_p(out.data_ptr()), None, None),
+                          "shard_finish")
+                torch.cuda.synchronize()
+                np.testing.assert_allclose(out.cpu().numpy(), full.cpu().numpy(), rtol=0, atol=1e-6)
+    ctx.set_engine("fp32")
