@@ -636,7 +636,7 @@ sred_status block3d_core(sred_ctx* c, int metric, const float* d_vol, int w, int
     CKS(ensure(c, B_MM, 2, &mm));
     const unsigned init[2] = {0xffffffffu, 0u};
     CK(cudaMemcpyAsync(mm, init, sizeof(init), cudaMemcpyHostToDevice, st));
-    k_minmax3d<<<grid, blk, 0, st>>>(d_out, d_mask, v, mm);
+    k_minmax3d<<<grid_for((size_t)v.W * v.H * v.D, 256, 4 * c->num_sms), 256, 0, st>>>(d_out, d_mask, v, mm);
     k_remap3d<<<grid, blk, 0, st>>>(d_out, d_mask, v, mm);
     CK(cudaGetLastError());
   }
@@ -690,7 +690,8 @@ sred_status global3d_prepare(sred_ctx* c, int metric, const float* d_vol, int w,
   CKS(ensure(c, B_COUNTS, nseg + 1, &d_counts));
   CKS(ensure(c, B_NMASK, 1, &d_nmask));
   CK(cudaMemsetAsync(d_nmask, 0, sizeof(unsigned long long), st));
-  k_flags3d<<<grid, blk, 0, st>>>(d_stds, v, thr, metric == kAbsDiff ? 0 : 1, d_mask, d_flags, d_nmask);
+  k_flags3d<<<grid_for(n, 256, 4 * c->num_sms), 256, 0, st>>>(d_stds, v, thr, metric == kAbsDiff ? 0 : 1, d_mask,
+                                                                d_flags, d_nmask);
   k_count<<<nseg, 256, 0, st>>>(d_flags, n, d_counts);
   k_scan<<<1, 1024, 0, st>>>(d_counts, nseg);
   k_scatter<<<nseg, 256, 0, st>>>(d_flags, n, d_counts, d_gpix, d_fpix, d_slot);
@@ -788,7 +789,7 @@ sred_status global3d_finish(sred_ctx* c, const GState& gs, cudaStream_t st, int 
     CKS(ensure(c, B_MM, 2, &mm));
     const unsigned init[2] = {0xffffffffu, 0u};
     CK(cudaMemcpyAsync(mm, init, sizeof(init), cudaMemcpyHostToDevice, st));
-    k_minmax3d<<<grid, blk, 0, st>>>(d_out, d_mask, v, mm);
+    k_minmax3d<<<grid_for((size_t)v.W * v.H * v.D, 256, 4 * c->num_sms), 256, 0, st>>>(d_out, d_mask, v, mm);
     k_remap3d<<<grid, blk, 0, st>>>(d_out, d_mask, v, mm);
     CK(cudaGetLastError());
   }

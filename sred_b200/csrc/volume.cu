@@ -212,14 +212,20 @@ __global__ void k_mask3d(const float* __restrict__ stds, Vol3 v, float thr, floa
 }
 
 // java/Utils.java:1572-1630 (normalizeImage3D): min and max over the interior
-// (where mask > 0 when a mask is given); mm = {min key, max key}.
+// (where mask > 0 when a mask is given); mm = {min key, max key}. Grid-stride
+// over the volume (a grid of a few CTAs per SM) so that each warp issues one
+// pair of atomics for many voxels.
 __global__ void k_minmax3d(const float* __restrict__ a, const float* __restrict__ mask, Vol3 v,
                            unsigned* __restrict__ mm) {
-  int x, y, z;
-  size_t p;
+  const size_t n = (size_t)v.W * v.H * v.D, plane = (size_t)v.W * v.H;
   unsigned lo = 0xffffffffu, hi = 0u;
-  if (voxel(v, &x, &y, &z, &p) && interior3(x, y, z, v) && (!mask || mask[p] > 0.0f)) {
-    lo = hi = f2key(a[p]);
+  for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+    const int z = (int)(p / plane), y = (int)((p % plane) / v.W), x = (int)(p % v.W);
+    if (interior3(x, y, z, v) && (!mask || mask[p] > 0.0f)) {
+      const unsigned k = f2key(a[p]);
+      lo = min(lo, k);
+      hi = max(hi, k);
+    }
   }
   for (int o = 16; o; o >>= 1) {
     lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
@@ -257,10 +263,10 @@ __global__ void k_remap3d(float* __restrict__ a, const float* __restrict__ mask,
 __global__ void k_flags3d(const float* __restrict__ stds, Vol3 v, float thr, int flat_columns,
                           float* __restrict__ mask, uint8_t* __restrict__ flags,
                           unsigned long long* __restrict__ n_mask) {
-  int x, y, z;
-  size_t p;
+  const size_t n = (size_t)v.W * v.H * v.D, plane = (size_t)v.W * v.H;
   unsigned c = 0;
-  if (voxel(v, &x, &y, &z, &p)) {
+  for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+    const int z = (int)(p / plane), y = (int)((p % plane) / v.W), x = (int)(p % v.W);
     const bool in = interior3(x, y, z, v);
     const float s = stds[p];
     const float s2 = s * s;
@@ -272,7 +278,7 @@ __global__ void k_flags3d(const float* __restrict__ stds, Vol3 v, float thr, int
       else if (s == 0.0f && flat_columns) f = 2;
     }
     flags[p] = f;
-    c = m > 0.0f ? 1u : 0u;
+    c += m > 0.0f ? 1u : 0u;
   }
   const unsigned wc = __reduce_add_sync(0xffffffffu, c);
   if ((threadIdx.x & 31) == 0 && wc) atomicAdd(n_mask, (unsigned long long)wc);
