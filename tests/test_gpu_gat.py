@@ -81,10 +81,11 @@ def _pg_spots(shape, seed):
     from sred_b200 import synth
     rng = np.random.default_rng(seed)
     if len(shape) == 2:
-        lam = synth.spot_image(shape[1], shape[0], 8, seed=seed, read_noise=0.0)
+        lam = synth.spot_image(shape[1], shape[0], 8, seed=seed, read_noise=0.0).clip(0, None) / 4
     else:
-        lam = synth.spot_volume(shape[2], shape[1], shape[0], 4, 2, seed=seed, read_noise=0.0)
-    lam = lam.clip(0, None) / 4
+        # dense, bright spots: the octree's Fisher test (width*height - 1
+        # degrees of freedom for a whole block of voxels) splits the root
+        lam = synth.spot_volume(shape[2], shape[1], shape[0], 6, 4, seed=seed, read_noise=0.0).clip(0, None)
     return (2.0 * rng.poisson(lam) + 100.0 + rng.normal(0, 5.0, lam.shape)).astype(np.float32)
 
 
@@ -115,3 +116,9 @@ def test_gat_tree_in_input_images(ctx):
     assert inp3.depth == 24 and np.isfinite(inp3.image_array).all()
     with pytest.raises(_lib.SredError):
         utils.gat_quadtree_2d(img, min_size=0, ctx=ctx)
+    # every leaf with the same mean: no regression line (the reference goes on with NaN)
+    flat = np.full((16, 24, 24), 100.0, np.float32)
+    with pytest.raises(ValueError):
+        oracle.gat_tree(flat, octree=True)
+    with pytest.raises(_lib.SredError):
+        utils.gat_octree_3d(flat, ctx=ctx)
