@@ -19,16 +19,25 @@ constexpr int kTileX = 32, kTileY = 8;
 __global__ void __launch_bounds__(kTileX* kTileY)
     k_block_map(const float* __restrict__ img_all, int W, int H, int frames, Ellipse e, RefBlock rb,
                 int metric, float* __restrict__ out_all, float* __restrict__ stds_out) {
-  extern __shared__ float tile[];  // (kTileY + 2rh) x (kTileX + 2rw)
+  // shared: the image tile (kTileY + 2rh) x (kTileX + 2rw), then the ellipse
+  // as linear tile offsets (K ints) and the reference block (K floats), so
+  // each element of a pass costs two broadcast shared loads
+  extern __shared__ float tile[];
   const int f = blockIdx.z;
   const float* img = img_all + (size_t)f * W * H;
   float* out = out_all + (size_t)f * W * H;
   const int tw = kTileX + 2 * e.rw, th = kTileY + 2 * e.rh;
+  int* s_off = reinterpret_cast<int*>(tile + tw * th);
+  float* s_ref = reinterpret_cast<float*>(s_off + e.k);
   const int x0 = blockIdx.x * kTileX - e.rw, y0 = blockIdx.y * kTileY - e.rh;
   for (int i = threadIdx.y * kTileX + threadIdx.x; i < tw * th; i += kTileX * kTileY) {
     const int ty = i / tw, tx = i - ty * tw;
     const int gx = x0 + tx, gy = y0 + ty;
     tile[i] = (gx >= 0 && gx < W && gy >= 0 && gy < H) ? img[(size_t)gy * W + gx] : 0.0f;
+  }
+  for (int i = threadIdx.y * kTileX + threadIdx.x; i < e.k; i += kTileX * kTileY) {
+    s_off[i] = e.dy[i] * tw + e.dx[i];
+    s_ref[i] = rb.px[i];
   }
   __syncthreads();
   const int x = blockIdx.x * kTileX + threadIdx.x, y = blockIdx.y * kTileY + threadIdx.y;
@@ -42,14 +51,14 @@ __global__ void __launch_bounds__(kTileX* kTileY)
   const float* c = tile + (threadIdx.y + e.rh) * tw + (threadIdx.x + e.rw);
   const int K = e.k;
   float s = 0.0f;
-  for (int i = 0; i < K; i++) s = __fadd_rn(s, c[e.dy[i] * tw + e.dx[i]]);
+  for (int i = 0; i < K; i++) s = __fadd_rn(s, c[s_off[i]]);
   const float mean = __fdiv_rn(s, (float)K);
   float v = 0.0f, acc = 0.0f, rr = 0.0f, xx = 0.0f;
   for (int i = 0; i < K; i++) {
-    const float px = c[e.dy[i] * tw + e.dx[i]];
+    const float px = c[s_off[i]];
     const float d = __fsub_rn(px, mean);
     v = __fadd_rn(v, __fmul_rn(d, d));
-    const float ref = rb.px[i];
+    const float ref = s_ref[i];
     if (metric == kNrmse) {
       const float t = __fsub_rn(ref, d);
       acc = __fadd_rn(acc, __fmul_rn(t, t));

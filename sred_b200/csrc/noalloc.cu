@@ -91,7 +91,9 @@ extern "C" sred_status sred_block_map_2d_device_noalloc(const char* metric, cons
   // Sizes beyond the fixed scratch are refused, not truncated.
   if (frames > kNoAllocMaxFrames) return SRED_ERR_ARG;
   if (m == kNrmse && n > kNoAllocMaskFloats) return SRED_ERR_ARG;
-  const size_t tile_smem = sizeof(float) * (32 + 2 * e.rw) * (8 + 2 * e.rh);
+  // image tile, then the ellipse offsets and reference block k_block_map stages
+  const size_t tile_smem =
+      sizeof(float) * (32 + 2 * e.rw) * (8 + 2 * e.rh) + (sizeof(int) + sizeof(float)) * (size_t)e.k;
   if (tile_smem > 48 * 1024) return SRED_ERR_ARG;
 
   int dev = 0;
