@@ -39,6 +39,9 @@ __global__ void k_remap(float* a, const float* mask, int W, int H, int bw_, int 
 // block_map.cu
 __global__ void k_block_map(const float* img, int W, int H, int frames, Ellipse e, RefBlock rb, int metric,
                             float* out, float* stds_out);
+// Dynamic shared memory and launch shape of k_block_map.
+size_t block_map_smem(const Ellipse& e);
+void block_map_launch_shape(int w, int h, int frames, dim3* grid, dim3* block);
 __global__ void k_block_absdiff_post(float* a, int W, int H, int rw, int rh, size_t plane, const unsigned* mm);
 __global__ void k_interior_mask(float* mask, int W, int H, int rw, int rh, size_t plane);
 __global__ void k_apply_mask(float* a, const float* mask, size_t n);

@@ -91,9 +91,7 @@ extern "C" sred_status sred_block_map_2d_device_noalloc(const char* metric, cons
   // Sizes beyond the fixed scratch are refused, not truncated.
   if (frames > kNoAllocMaxFrames) return SRED_ERR_ARG;
   if (m == kNrmse && n > kNoAllocMaskFloats) return SRED_ERR_ARG;
-  // image tile, then the ellipse offsets and reference block k_block_map stages
-  const size_t tile_smem =
-      sizeof(float) * (32 + 2 * e.rw) * (8 + 2 * e.rh) + (sizeof(int) + sizeof(float)) * (size_t)e.k;
+  const size_t tile_smem = block_map_smem(e);
   if (tile_smem > 48 * 1024) return SRED_ERR_ARG;
 
   int dev = 0;
@@ -126,7 +124,8 @@ extern "C" sred_status sred_block_map_2d_device_noalloc(const char* metric, cons
     k_block_phase<<<dim3((unsigned)((plane + 127) / 128), frames), 128, 0, s>>>(d_img, w, h, e, bw, bh, pr,
                                                                                   d_out, nullptr);
   } else {
-    dim3 grid((w + 31) / 32, (h + 7) / 8, frames), blk(32, 8);
+    dim3 grid, blk;
+    block_map_launch_shape(w, h, frames, &grid, &blk);
     k_block_map<<<grid, blk, tile_smem, s>>>(d_img, w, h, frames, e, rb, m, d_out, nullptr);
   }
   const dim3 pg(grid_of(plane, 256, 4 * sms), frames);

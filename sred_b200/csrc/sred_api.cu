@@ -490,8 +490,9 @@ sred_status block_core(sred_ctx* c, int metric, const float* d_img, int w, int h
   if (metric == kHu || metric == kPhase) {
     CKS(block_shape_launch(c, metric, d_img, w, h, frames, e, ref_pixels, bw, bh, ref_std, d_out, d_stds, st));
   } else {
-    dim3 grid((w + 31) / 32, (h + 7) / 8, frames), blk(32, 8);
-    size_t smem = sizeof(float) * (32 + 2 * rw) * (8 + 2 * rh) + (sizeof(int) + sizeof(float)) * (size_t)e.k;
+    dim3 grid, blk;
+    block_map_launch_shape(w, h, frames, &grid, &blk);
+    const size_t smem = block_map_smem(e);
     if (smem > 200 * 1024) return fail(c, SRED_ERR_ARG, "block too large for the streaming tile");
     if (smem > 48 * 1024)
       CK(cudaFuncSetAttribute(k_block_map, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
