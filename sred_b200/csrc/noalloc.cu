@@ -121,8 +121,7 @@ extern "C" sred_status sred_block_map_2d_device_noalloc(const char* metric, cons
     if (bw > kPhaseMaxDim || bh > kPhaseMaxDim) return SRED_ERR_ARG;
     PhaseRef pr;
     phase_reference_dft(ref_pixels, ref_std, bw, bh, &pr);
-    k_block_phase<<<dim3((unsigned)((plane + 127) / 128), frames), 128, 0, s>>>(d_img, w, h, e, bw, bh, pr,
-                                                                                  d_out, nullptr);
+    launch_block_phase(d_img, w, h, frames, e, bw, bh, pr, d_out, nullptr, s);
   } else {
     dim3 grid, blk;
     block_map_launch_shape(w, h, frames, &grid, &blk);

@@ -230,41 +230,228 @@ __global__ void __launch_bounds__(128)
   }
 }
 
-// Block-map form: the reference block's DFT against each block's, one thread
-// per pixel. Blocks are normalised with their FP32 local statistics (computed
-// here, and written to stds_out when it is given) and restricted to the
-// ellipse (0 elsewhere on the bw x bh grid).
+// Block-map form: the reference block's DFT against each block's. Blocks are
+// normalised with their FP32 local statistics (computed here, and written to
+// stds_out when it is given) and restricted to the ellipse (0 elsewhere on
+// the bw x bh grid).
+//
+// A group of G lanes (G = 16, 8 or 4 as D = max(bw, bh) allows) evaluates one
+// pixel at a time; the 128 threads of a CTA are 128 / G groups, each taking G
+// consecutive pixels in turn. The separable transforms run one line per lane:
+// the lane holds its line (a patch row, a half-transformed column, ...) in
+// registers and walks the outputs, so the twiddles are the only operands it
+// loads, and every lane of the warp loads the same one (a broadcast). Between
+// stages the lines go through the group's two shared buffers (real,
+// imaginary), each stage reading its lines before any lane overwrites them.
+// Every output is the same sequential sum as in phase_dft / phase_peak, and
+// the peak search keeps their rule (largest value above 0, lowest raster
+// index on ties), so the map equals the one-thread-per-pixel evaluation.
+// Pixels outside the interior (and past the plane) run on a zero patch and
+// are written as 0, so the warp stays converged for its shuffles.
+template <int D>
 __global__ void __launch_bounds__(128)
     k_block_phase(const float* __restrict__ img_all, int W, int H, Ellipse e, int bw, int bh, PhaseRef ref,
                   float* __restrict__ out_all, float* __restrict__ stds_out) {
-  __shared__ double tw[4 * kPhaseMaxN];
+  constexpr int G = D <= 3 ? 4 : D <= 7 ? 8 : 16;
+  constexpr int NG = 128 / G;
+  __shared__ double tw[4 * D * D];
+  __shared__ double rre[D * D], rim[D * D];
+  __shared__ double buf[NG][2 * D * D];
+  __shared__ int s_img[D * D], s_grid[D * D];  // ellipse: image offset, patch position
   double *cw = tw, *sw = tw + bw * bw, *ch = sw + bw * bw, *sh = ch + bh * bh;
   phase_twiddles_smem(bw, bh, cw, sw, ch, sh);
+  const int nn = bw * bh;
+  for (int k = threadIdx.x; k < nn; k += blockDim.x) {
+    rre[k] = ref.re[k];
+    rim[k] = ref.im[k];
+  }
+  for (int k = threadIdx.x; k < e.k; k += blockDim.x) {
+    s_img[k] = e.dy[k] * W + e.dx[k];
+    s_grid[k] = (e.dy[k] + e.rh) * bw + e.dx[k] + e.rw;
+  }
   __syncthreads();
+  const unsigned full = 0xffffffffu;
+  const int g = threadIdx.x / G, t = threadIdx.x % G, leader = (threadIdx.x & 31) & ~(G - 1);
+  double* re = buf[g];
+  double* im = re + D * D;
   const size_t plane = (size_t)W * H;
-  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= plane) return;
   const size_t off = (size_t)blockIdx.y * plane;
   const float* img = img_all + off;
   float* out = out_all + off;
-  const int x = (int)(idx % W), y = (int)(idx / W), rw = e.rw, rh = e.rh, nn = bw * bh;
-  if (x < rw || x >= W - rw || y < rh || y >= H - rh) {
-    out[idx] = 0.0f;
-    if (stds_out) stds_out[off + idx] = 0.0f;
-    return;
+  const int rw = e.rw, rh = e.rh;
+  const double sn = sqrt((double)(bw * bh));
+  const size_t first = (size_t)blockIdx.x * 128 + (size_t)g * G;
+  // local statistics of the group's G pixels, lane t for pixel first + t
+  float own_m = 0.0f, own_s = 0.0f;
+  {
+    const size_t idx = first + t;
+    const int x = (int)(idx % W), y = (int)(idx / W);
+    if (idx < plane && x >= rw && x < W - rw && y >= rh && y < H - rh) {
+      // block_stats_f32's sequence over the offsets in shared memory
+      const float* c = img + idx;
+      float sum = 0.0f;
+      for (int i = 0; i < e.k; i++) sum = __fadd_rn(sum, c[s_img[i]]);
+      own_m = __fdiv_rn(sum, (float)e.k);
+      float v = 0.0f;
+      for (int i = 0; i < e.k; i++) {
+        const float d = __fsub_rn(c[s_img[i]], own_m);
+        v = __fadd_rn(v, __fmul_rn(d, d));
+      }
+      own_s = __fsqrt_rn(__fdiv_rn(v, (float)(e.k - 1)));
+    }
+    if (stds_out && idx < plane) stds_out[off + idx] = own_s;
   }
-  float mf, sf;
-  block_stats_f32(img + idx, W, e, &mf, &sf);
-  if (stds_out) stds_out[off + idx] = sf;
-  const double m = (double)mf, s = (double)sf + (double)kEps;
-  double work[3 * kPhaseMaxN + kPhaseTmp];  // [patch | spectrum re | spectrum im | temporaries]
-  double *xg = work, *cr = work + kPhaseMaxN, *ci = work + 2 * kPhaseMaxN, *tmp = work + 3 * kPhaseMaxN;
-  for (int k = 0; k < nn; k++) xg[k] = 0.0;
-  for (int k = 0; k < e.k; k++)
-    xg[(e.dy[k] + rh) * bw + e.dx[k] + rw] = ((double)img[(size_t)(y + e.dy[k]) * W + x + e.dx[k]] - m) / s;
-  phase_dft(xg, bw, bh, cw, sw, ch, sh, cr, ci, tmp);
-  for (int k = 0; k < nn; k++) phase_cross(ref.re[k], ref.im[k], cr[k], ci[k], &cr[k], &ci[k]);
-  out[idx] = phase_peak(cr, ci, bw, bh, cw, sw, ch, sh, tmp);
+  for (int n = 0; n < G; n++) {
+    const size_t idx = first + n;
+    const int x = (int)(idx % W), y = (int)(idx / W);
+    const bool act = idx < plane && x >= rw && x < W - rw && y >= rh && y < H - rh;
+    const float mf = __shfl_sync(full, own_m, leader + n);
+    const float sf = __shfl_sync(full, own_s, leader + n);
+    const double m = (double)mf, sd = (double)sf + (double)kEps;
+    // the patch, in the real buffer
+    for (int k = t; k < nn; k += G) re[k] = 0.0;
+    __syncwarp();
+    if (act) {
+      const float* c = img + (size_t)y * W + x;
+      for (int k = t; k < e.k; k += G) re[s_grid[k]] = ((double)c[s_img[k]] - m) / sd;
+    }
+    __syncwarp();
+    double lr[D], li[D];
+    // forward, rows: lane jj holds patch row jj; T(i, jj) = sum_ii x[jj][ii] e^{-i a(i, ii)}
+    if (t < bh) {
+#pragma unroll
+      for (int ii = 0; ii < D; ii++) lr[ii] = ii < bw ? re[t * bw + ii] : 0.0;
+    }
+    __syncwarp();
+    if (t < bh) {
+      for (int i = 0; i < bw; i++) {
+        double ar = 0.0, ai = 0.0;
+#pragma unroll
+        for (int ii = 0; ii < D; ii++) {
+          if (ii < bw) {
+            const double v = lr[ii];
+            ar += v * cw[i * bw + ii];
+            ai -= v * sw[i * bw + ii];
+          }
+        }
+        re[i * bh + t] = ar;
+        im[i * bh + t] = ai;
+      }
+    }
+    __syncwarp();
+    // forward, columns: lane i holds T(i, :); then the normalised cross-power
+    // spectrum with the reference, X(j, i), over the same buffers
+    if (t < bw) {
+#pragma unroll
+      for (int jj = 0; jj < D; jj++) {
+        lr[jj] = jj < bh ? re[t * bh + jj] : 0.0;
+        li[jj] = jj < bh ? im[t * bh + jj] : 0.0;
+      }
+    }
+    __syncwarp();
+    if (t < bw) {
+      for (int j = 0; j < bh; j++) {
+        double br = 0.0, bi = 0.0;
+#pragma unroll
+        for (int jj = 0; jj < D; jj++) {
+          if (jj < bh) {
+            const double c = ch[j * bh + jj], s = sh[j * bh + jj];
+            br += lr[jj] * c + li[jj] * s;
+            bi += li[jj] * c - lr[jj] * s;
+          }
+        }
+        const int k = j * bw + t;
+        phase_cross(rre[k], rim[k], br / sn, bi / sn, &re[k], &im[k]);
+      }
+    }
+    __syncwarp();
+    // inverse, rows: lane jj holds X(jj, :); S(i, jj) = sum_ii X[jj][ii] e^{+i a(i, ii)}
+    if (t < bh) {
+#pragma unroll
+      for (int ii = 0; ii < D; ii++) {
+        lr[ii] = ii < bw ? re[t * bw + ii] : 0.0;
+        li[ii] = ii < bw ? im[t * bw + ii] : 0.0;
+      }
+    }
+    __syncwarp();
+    if (t < bh) {
+      for (int i = 0; i < bw; i++) {
+        double sr = 0.0, si = 0.0;
+#pragma unroll
+        for (int ii = 0; ii < D; ii++) {
+          if (ii < bw) {
+            const double c = cw[i * bw + ii], s = sw[i * bw + ii];
+            sr += lr[ii] * c - li[ii] * s;
+            si += lr[ii] * s + li[ii] * c;
+          }
+        }
+        re[i * bh + t] = sr;
+        im[i * bh + t] = si;
+      }
+    }
+    __syncwarp();
+    // inverse, columns (real part): lane i holds S(i, :) and scans its column
+    double best = 0.0;
+    int bidx = -1;
+    if (t < bw) {
+#pragma unroll
+      for (int jj = 0; jj < D; jj++) {
+        lr[jj] = jj < bh ? re[t * bh + jj] : 0.0;
+        li[jj] = jj < bh ? im[t * bh + jj] : 0.0;
+      }
+      for (int j = 0; j < bh; j++) {
+        double v = 0.0;
+#pragma unroll
+        for (int jj = 0; jj < D; jj++)
+          if (jj < bh) v += lr[jj] * ch[j * bh + jj] - li[jj] * sh[j * bh + jj];
+        v /= sn;
+        const int k = j * bw + t;
+        if (v > best || (bidx >= 0 && v == best && k < bidx)) {
+          best = v;
+          bidx = k;
+        }
+      }
+    }
+    // the group's peak: largest value above 0, lowest raster index on ties
+#pragma unroll
+    for (int o = G / 2; o; o >>= 1) {
+      const double ob = __shfl_xor_sync(full, best, o);
+      const int oi = __shfl_xor_sync(full, bidx, o);
+      if (oi >= 0 && (bidx < 0 || ob > best || (ob == best && oi < bidx))) {
+        best = ob;
+        bidx = oi;
+      }
+    }
+    if (t == 0 && idx < plane) {
+      float r = 0.0f;
+      if (act && bidx >= 0) {
+        const double px = (double)(bidx % bw + 1), py = (double)(bidx / bw + 1);
+        r = (float)sqrt((px * px) + (py * py));
+      }
+      out[idx] = r;
+    }
+    __syncwarp();
+  }
+}
+
+void launch_block_phase(const float* img, int W, int H, int frames, const Ellipse& e, int bw, int bh,
+                        const PhaseRef& ref, float* out, float* stds_out, cudaStream_t st) {
+  const dim3 grid((unsigned)(((size_t)W * H + 127) / 128), (unsigned)frames);
+  const int d = bw > bh ? bw : bh;
+  if (d <= 3)
+    k_block_phase<3><<<grid, 128, 0, st>>>(img, W, H, e, bw, bh, ref, out, stds_out);
+  else if (d <= 5)
+    k_block_phase<5><<<grid, 128, 0, st>>>(img, W, H, e, bw, bh, ref, out, stds_out);
+  else if (d <= 7)
+    k_block_phase<7><<<grid, 128, 0, st>>>(img, W, H, e, bw, bh, ref, out, stds_out);
+  else if (d <= 9)
+    k_block_phase<9><<<grid, 128, 0, st>>>(img, W, H, e, bw, bh, ref, out, stds_out);
+  else if (d <= 11)
+    k_block_phase<11><<<grid, 128, 0, st>>>(img, W, H, e, bw, bh, ref, out, stds_out);
+  else if (d <= 13)
+    k_block_phase<13><<<grid, 128, 0, st>>>(img, W, H, e, bw, bh, ref, out, stds_out);
+  else
+    k_block_phase<15><<<grid, 128, 0, st>>>(img, W, H, e, bw, bh, ref, out, stds_out);
 }
 
 // Values of `a` at the interior pixels, in interior raster order.

@@ -13,11 +13,12 @@
 // third with those three defects repaired (no unique-coordinate pre-filter,
 // real-valued phases, block-width indexing).
 //
-// Per-thread work arrays of the phase kernels live in ONE local array per
-// thread, carved into sections by offset. With separate local arrays,
-// k_block_phase built by nvcc 12.9 for sm_100a computed DFTs whose first row
-// read overwritten inputs, as if phase_dft's column temporaries shared the
-// input patch's stack slots; with one array per thread the results are exact.
+// Per-thread work arrays of the all-pairs phase kernels live in ONE local
+// array per thread, carved into sections by offset. With separate local
+// arrays, a one-thread-per-pixel block-map phase kernel built by nvcc 12.9 for
+// sm_100a computed DFTs whose first row read overwritten inputs, as if
+// phase_dft's column temporaries shared the input patch's stack slots; with
+// one array per thread the results were exact.
 #pragma once
 #include <math.h>
 
@@ -160,9 +161,11 @@ __device__ __forceinline__ void block_stats_f32(const float* c, int W, const Ell
   *std_out = __fsqrt_rn(__fdiv_rn(v, (float)(e.k - 1)));
 }
 
-// Block-map phase correlation against the reference block's DFT (shape.cu).
-__global__ void k_block_phase(const float* img, int W, int H, Ellipse e, int bw, int bh, PhaseRef ref, float* out,
-                              float* stds_out);
+// Block-map phase correlation against the reference block's DFT (shape.cu):
+// the frames x W x H raw map (and the FP32 local stds when stds_out is given)
+// on stream st; bw, bh <= kPhaseMaxDim.
+void launch_block_phase(const float* img, int W, int H, int frames, const Ellipse& e, int bw, int bh,
+                        const PhaseRef& ref, float* out, float* stds_out, cudaStream_t st);
 
 // Host side (shape.cu).
 // Block-map Hu metric: the bw x bh reference patch (ellipse pixels of the

@@ -462,7 +462,7 @@ sred_status block_shape_launch(sred_ctx* c, int metric, const float* d_img, int 
       return fail(c, SRED_ERR_ARG, "phase correlation supports blocks up to 15x15");
     PhaseRef pr;
     phase_reference_dft(ref_pixels, ref_std, bw, bh, &pr);
-    k_block_phase<<<grid, 128, 0, st>>>(d_img, w, h, e, bw, bh, pr, d_out, d_stds);
+    launch_block_phase(d_img, w, h, frames, e, bw, bh, pr, d_out, d_stds, st);
   }
   CK(cudaGetLastError());
   return SRED_OK;

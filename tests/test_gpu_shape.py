@@ -112,6 +112,21 @@ def test_block_shape_metrics(ctx, shape_fx, metric):
             np.testing.assert_allclose(got, a, atol=1e-6, rtol=0, err_msg=f"{name} c={c}")
 
 
+@pytest.mark.parametrize("bw,bh", [(7, 7), (11, 9), (13, 13), (15, 15), (15, 7), (3, 15), (5, 11)])
+def test_block_phase_every_block_size(ctx, bw, bh):
+    """The block-map phase kernel is instantiated per max(bw, bh) (3 ... 15),
+    with 4, 8 or 16 lanes per pixel; every size equals the FP64 oracle. The
+    45 x 37 plane is not a multiple of the 128 pixels of a CTA."""
+    from sred_b200 import synth
+    img = synth.normalize_input(synth.spot_image(45, 37, 6, seed=bw * 31 + bh))
+    cy, cx = 18, 22
+    rb = utils.get_reference_block_2d(img[cy - bh // 2:cy + bh // 2 + 1, cx - bw // 2:cx + bw // 2 + 1])
+    raw = clutils.calculate_block_repetition_map_2d(clutils.PHASE, _inp(img), rb, 0.0, False, ctx=ctx)
+    exp = oracle.block_phase_raw(img, rb.pixels, bw, bh, rb.std).astype(np.float32)
+    assert np.count_nonzero(exp) > 0
+    np.testing.assert_array_equal(raw, exp.ravel(), err_msg=f"{bw}x{bh}")
+
+
 @pytest.mark.parametrize("metric", [clutils.HU, clutils.PHASE])
 def test_block_shape_frames_and_noalloc(ctx, shape_fx, metric):
     """A stack of frames on the device equals the frames one by one; the
