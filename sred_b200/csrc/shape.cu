@@ -235,28 +235,34 @@ __global__ void __launch_bounds__(128)
 // stds_out when it is given) and restricted to the ellipse (0 elsewhere on
 // the bw x bh grid).
 //
-// A group of G lanes (G = 16, 8 or 4 as D = max(bw, bh) allows) evaluates one
-// pixel at a time; the 128 threads of a CTA are 128 / G groups, each taking G
-// consecutive pixels in turn. The separable transforms run one line per lane:
-// the lane holds its line (a patch row, a half-transformed column, ...) in
-// registers and walks the outputs, so the twiddles are the only operands it
-// loads, and every lane of the warp loads the same one (a broadcast). Between
-// stages the lines go through the group's two shared buffers (real,
-// imaginary), each stage reading its lines before any lane overwrites them.
+// A group of D = max(bw, bh) lanes evaluates one pixel at a time: a warp
+// holds P = 32 / D groups, a CTA 4P, and each group takes D consecutive
+// pixels in turn (lane t computes the local statistics of the group's pixel t
+// up front). The separable transforms run one line per lane: the lane holds
+// its line (a patch row, a half-transformed column, ...) in registers and
+// walks the outputs, so the twiddles are the only operands it loads, and
+// every lane of the warp loads the same one (a broadcast). Between stages the
+// lines go through the group's two shared buffers (real, imaginary).
 // Every output is the same sequential sum as in phase_dft / phase_peak, and
 // the peak search keeps their rule (largest value above 0, lowest raster
 // index on ties), so the map equals the one-thread-per-pixel evaluation.
 // Pixels outside the interior (and past the plane) run on a zero patch and
 // are written as 0, so the warp stays converged for its shuffles.
 template <int D>
+struct PhaseShape {
+  static constexpr int P = 32 / D;       // groups per warp
+  static constexpr int NG = 4 * P;       // groups per CTA
+  static constexpr int PIX = NG * D;     // pixels per CTA
+};
+
+template <int D>
 __global__ void __launch_bounds__(128)
     k_block_phase(const float* __restrict__ img_all, int W, int H, Ellipse e, int bw, int bh, PhaseRef ref,
                   float* __restrict__ out_all, float* __restrict__ stds_out) {
-  constexpr int G = D <= 3 ? 4 : D <= 7 ? 8 : 16;
-  constexpr int NG = 128 / G;
+  using S = PhaseShape<D>;
   __shared__ double tw[4 * D * D];
   __shared__ double rre[D * D], rim[D * D];
-  __shared__ double buf[NG][2 * D * D];
+  __shared__ double buf[S::NG][2 * D * D];
   __shared__ int s_img[D * D], s_grid[D * D];  // ellipse: image offset, patch position
   double *cw = tw, *sw = tw + bw * bw, *ch = sw + bw * bw, *sh = ch + bh * bh;
   phase_twiddles_smem(bw, bh, cw, sw, ch, sh);
@@ -271,8 +277,13 @@ __global__ void __launch_bounds__(128)
   }
   __syncthreads();
   const unsigned full = 0xffffffffu;
-  const int g = threadIdx.x / G, t = threadIdx.x % G, leader = (threadIdx.x & 31) & ~(G - 1);
-  double* re = buf[g];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // lanes past the warp's last group take no line (t = D) and no buffer
+  const bool live = lane < S::P * D;
+  const int gw = live ? lane / D : 0;
+  const int t = live ? lane - gw * D : D;
+  const int base = gw * D;  // the group's first lane
+  double* re = buf[warp * S::P + gw];
   double* im = re + D * D;
   const size_t plane = (size_t)W * H;
   const size_t off = (size_t)blockIdx.y * plane;
@@ -280,10 +291,10 @@ __global__ void __launch_bounds__(128)
   float* out = out_all + off;
   const int rw = e.rw, rh = e.rh;
   const double sn = sqrt((double)(bw * bh));
-  const size_t first = (size_t)blockIdx.x * 128 + (size_t)g * G;
-  // local statistics of the group's G pixels, lane t for pixel first + t
+  const size_t first = (size_t)blockIdx.x * S::PIX + (size_t)(warp * S::P + gw) * D;
+  // local statistics of the group's D pixels, lane t for pixel first + t
   float own_m = 0.0f, own_s = 0.0f;
-  {
+  if (live) {
     const size_t idx = first + t;
     const int x = (int)(idx % W), y = (int)(idx / W);
     if (idx < plane && x >= rw && x < W - rw && y >= rh && y < H - rh) {
@@ -301,23 +312,27 @@ __global__ void __launch_bounds__(128)
     }
     if (stds_out && idx < plane) stds_out[off + idx] = own_s;
   }
-  for (int n = 0; n < G; n++) {
+  for (int n = 0; n < D; n++) {
     const size_t idx = first + n;
     const int x = (int)(idx % W), y = (int)(idx / W);
     const bool act = idx < plane && x >= rw && x < W - rw && y >= rh && y < H - rh;
-    const float mf = __shfl_sync(full, own_m, leader + n);
-    const float sf = __shfl_sync(full, own_s, leader + n);
+    const float mf = __shfl_sync(full, own_m, base + n);
+    const float sf = __shfl_sync(full, own_s, base + n);
     const double m = (double)mf, sd = (double)sf + (double)kEps;
     // the patch, in the real buffer
-    for (int k = t; k < nn; k += G) re[k] = 0.0;
+    if (live)
+      for (int k = t; k < nn; k += D) re[k] = 0.0;
     __syncwarp();
-    if (act) {
+    if (live && act) {
       const float* c = img + (size_t)y * W + x;
-      for (int k = t; k < e.k; k += G) re[s_grid[k]] = ((double)c[s_img[k]] - m) / sd;
+      for (int k = t; k < e.k; k += D) re[s_grid[k]] = ((double)c[s_img[k]] - m) / sd;
     }
     __syncwarp();
+    // Each stage: the lane holds its line in registers and walks the
+    // outputs it owns, each one sequential sum; the lines are overwritten
+    // only after every lane of the warp has read its own.
     double lr[D], li[D];
-    // forward, rows: lane jj holds patch row jj; T(i, jj) = sum_ii x[jj][ii] e^{-i a(i, ii)}
+    // forward, rows: lane jj, T(i, jj) = sum_ii x[jj][ii] e^{-i a(i, ii)}
     if (t < bh) {
 #pragma unroll
       for (int ii = 0; ii < D; ii++) lr[ii] = ii < bw ? re[t * bw + ii] : 0.0;
@@ -339,8 +354,8 @@ __global__ void __launch_bounds__(128)
       }
     }
     __syncwarp();
-    // forward, columns: lane i holds T(i, :); then the normalised cross-power
-    // spectrum with the reference, X(j, i), over the same buffers
+    // forward, columns: lane i holds T(i, :); F(j, i) = sum_jj T(i, jj) e^{-i b(j, jj)},
+    // then the normalised cross-power spectrum with the reference, X(j, i)
     if (t < bw) {
 #pragma unroll
       for (int jj = 0; jj < D; jj++) {
@@ -390,7 +405,8 @@ __global__ void __launch_bounds__(128)
       }
     }
     __syncwarp();
-    // inverse, columns (real part): lane i holds S(i, :) and scans its column
+    // inverse, columns (real part): lane i holds S(i, :);
+    // v(j, i) = sum_jj Re(S(i, jj) e^{+i b(j, jj)}) / sn, and the lane's peak
     double best = 0.0;
     int bidx = -1;
     if (t < bw) {
@@ -412,12 +428,13 @@ __global__ void __launch_bounds__(128)
         }
       }
     }
-    // the group's peak: largest value above 0, lowest raster index on ties
+    // the group's peak (lane t gathers lanes t .. t + 2o - 1 of the group):
+    // largest value above 0, lowest raster index on ties
 #pragma unroll
-    for (int o = G / 2; o; o >>= 1) {
-      const double ob = __shfl_xor_sync(full, best, o);
-      const int oi = __shfl_xor_sync(full, bidx, o);
-      if (oi >= 0 && (bidx < 0 || ob > best || (ob == best && oi < bidx))) {
+    for (int o = 1; o < D; o <<= 1) {
+      const double ob = __shfl_down_sync(full, best, o);
+      const int oi = __shfl_down_sync(full, bidx, o);
+      if (t + o < D && oi >= 0 && (bidx < 0 || ob > best || (ob == best && oi < bidx))) {
         best = ob;
         bidx = oi;
       }
@@ -434,24 +451,30 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+template <int D>
+void launch_block_phase_t(const float* img, int W, int H, int frames, const Ellipse& e, int bw, int bh,
+                          const PhaseRef& ref, float* out, float* stds_out, cudaStream_t st) {
+  const dim3 grid((unsigned)(((size_t)W * H + PhaseShape<D>::PIX - 1) / PhaseShape<D>::PIX), (unsigned)frames);
+  k_block_phase<D><<<grid, 128, 0, st>>>(img, W, H, e, bw, bh, ref, out, stds_out);
+}
+
 void launch_block_phase(const float* img, int W, int H, int frames, const Ellipse& e, int bw, int bh,
                         const PhaseRef& ref, float* out, float* stds_out, cudaStream_t st) {
-  const dim3 grid((unsigned)(((size_t)W * H + 127) / 128), (unsigned)frames);
   const int d = bw > bh ? bw : bh;
   if (d <= 3)
-    k_block_phase<3><<<grid, 128, 0, st>>>(img, W, H, e, bw, bh, ref, out, stds_out);
+    launch_block_phase_t<3>(img, W, H, frames, e, bw, bh, ref, out, stds_out, st);
   else if (d <= 5)
-    k_block_phase<5><<<grid, 128, 0, st>>>(img, W, H, e, bw, bh, ref, out, stds_out);
+    launch_block_phase_t<5>(img, W, H, frames, e, bw, bh, ref, out, stds_out, st);
   else if (d <= 7)
-    k_block_phase<7><<<grid, 128, 0, st>>>(img, W, H, e, bw, bh, ref, out, stds_out);
+    launch_block_phase_t<7>(img, W, H, frames, e, bw, bh, ref, out, stds_out, st);
   else if (d <= 9)
-    k_block_phase<9><<<grid, 128, 0, st>>>(img, W, H, e, bw, bh, ref, out, stds_out);
+    launch_block_phase_t<9>(img, W, H, frames, e, bw, bh, ref, out, stds_out, st);
   else if (d <= 11)
-    k_block_phase<11><<<grid, 128, 0, st>>>(img, W, H, e, bw, bh, ref, out, stds_out);
+    launch_block_phase_t<11>(img, W, H, frames, e, bw, bh, ref, out, stds_out, st);
   else if (d <= 13)
-    k_block_phase<13><<<grid, 128, 0, st>>>(img, W, H, e, bw, bh, ref, out, stds_out);
+    launch_block_phase_t<13>(img, W, H, frames, e, bw, bh, ref, out, stds_out, st);
   else
-    k_block_phase<15><<<grid, 128, 0, st>>>(img, W, H, e, bw, bh, ref, out, stds_out);
+    launch_block_phase_t<15>(img, W, H, frames, e, bw, bh, ref, out, stds_out, st);
 }
 
 // Values of `a` at the interior pixels, in interior raster order.
