@@ -255,8 +255,10 @@ struct PhaseShape {
   static constexpr int PIX = NG * D;     // pixels per CTA
 };
 
+// (five CTAs per SM for the two largest sizes: 9.5 instead of 10.1 ms per
+// 1024 x 1024 frame at 15 x 15; the smaller sizes run best unconstrained)
 template <int D>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, D >= 13 ? 5 : 0)
     k_block_phase(const float* __restrict__ img_all, int W, int H, Ellipse e, int bw, int bh, PhaseRef ref,
                   float* __restrict__ out_all, float* __restrict__ stds_out) {
   using S = PhaseShape<D>;
