@@ -353,6 +353,20 @@ def run_block(args, rank, local, world):
         px = 1024 * 1024 * nf * world
         res[metric] = {"frames": nf, "ms_per_step": ms, "ms_per_frame": ms / nf, "pixels_per_s": px / (ms / 1e3),
                        "gbs_8B_per_pixel": 8 * px / (ms / 1e3) / 1e9}
+    # end to end: host stack in, host maps out, through the public call (page-locked host buffers, as a
+    # caller streaming time-lapses would hold); pipelined in chunks, and as one chunk (copies not overlapped)
+    h_in = torch.from_numpy(stack).pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    e2e = {}
+    for name, chunk in (("pipelined", 0), ("one_chunk", frames)):
+        for _ in range(args.warmup):
+            clutils.block_map_stack("Pearson's R", h_in.numpy(), ref, 0.0, True, chunk_frames=chunk,
+                                    out=h_out.numpy(), ctx=ctx)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            clutils.block_map_stack("Pearson's R", h_in.numpy(), ref, 0.0, True, chunk_frames=chunk,
+                                    out=h_out.numpy(), ctx=ctx)
+        e2e[name] = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps, world)
     if rank != 0:
         return
     pk = peaks()
@@ -365,6 +379,10 @@ def run_block(args, rank, local, world):
                                    f"15x15 reference block (K=149), relevance 0, normalised per frame",
                        "frames": frames, "l2": f"stack of {4 * frames} MB > L2"},
             "per_metric": res,
+            "e2e": {"value": 1024 * 1024 * frames * world / (e2e["pipelined"] / 1e3), "unit": "pixels/s",
+                    "h2d_bytes_per_step": int(stack.nbytes), "d2h_bytes_per_step": int(stack.nbytes),
+                    "ms_per_step": e2e["pipelined"], "ms_per_step_one_chunk": e2e["one_chunk"],
+                    "call": "clutils.block_map_stack (sred_block_map_2d_stack), Pearson's R, page-locked buffers"},
             "roofline": {"bound": "hbm", "achieved": p["gbs_8B_per_pixel"], "peak": pk["hbm_gbs"], "unit": "GB/s",
                          "frac": p["gbs_8B_per_pixel"] / pk["hbm_gbs"], "traffic": None,
                          "note": "8 algorithmic bytes per pixel over the whole call (map kernel plus per-frame "
@@ -460,8 +478,8 @@ def run_volume(args, rank, local, world):
             "e2e": {"value": vol.size * world / (e2e_ms / 1e3), "unit": "voxels/s",
                     "h2d_bytes_per_step": vol.nbytes, "d2h_bytes_per_step": vol.nbytes},
             "clocks": clocks.summary(),
-            # per Pearson call: local statistics, map, min-max, remap
-            "gpu_launches": 4 * args.steps,
+            # per Pearson call: local statistics, map, min-max initialisation, min-max, remap
+            "gpu_launches": 5 * args.steps,
             "roofline": {"bound": "hbm", "achieved": p["gbs_8B_per_voxel"], "peak": pk["hbm_gbs"], "unit": "GB/s",
                          "frac": p["gbs_8B_per_voxel"] / pk["hbm_gbs"], "traffic": None,
                          "note": "8 algorithmic bytes per voxel over the whole call; the kernels evaluate "

@@ -192,6 +192,20 @@ sred_status sred_block_map_2d_device(sred_ctx *ctx, const char *metric, const fl
                                      int bh, float ref_mean, float ref_std, float relevance_constant,
                                      int normalize_output, float *d_out, void *stream);
 
+/* Host-buffer variant over a stack of `frames` images (the same time-lapse
+ * loop): img and out are frames*w*h floats in host memory, each frame mapped
+ * and normalised on its own, exactly as sred_block_map_2d_device maps them.
+ * The stack moves in chunks of chunk_frames frames (0: about 32 MiB per
+ * chunk) through two device slots, so the upload of one chunk, the map of the
+ * previous one and the download of the one before run at the same time; with
+ * page-locked host buffers the copies run concurrently with the kernels.
+ * Returns when out is complete (or, on an error, when no copy touches img or
+ * out any more). */
+sred_status sred_block_map_2d_stack(sred_ctx *ctx, const char *metric, const float *img, int w, int h,
+                                    int frames, const float *ref_pixels, int block_size, int bw, int bh,
+                                    float ref_mean, float ref_std, float relevance_constant,
+                                    int normalize_output, int chunk_frames, float *out);
+
 /* Replaces Utils.getReferenceBlock2D (java/Utils.java:557-639) for a block
  * image already converted to float: ellipse-flatten, min-max, mean-subtract,
  * std. pixels must hold sred_block_size(bw, bh) floats. */

@@ -22,7 +22,8 @@ EXPORTS = [
     "sred_create", "sred_destroy", "sred_set_engine", "sred_status_string", "sred_last_error",
     "sred_block_size", "sred_local_statistics_2d", "sred_mean_noise_var_2d", "sred_relevance_mask_2d",
     "sred_calculate_global_repetition_map_2d", "sred_global_map_2d", "sred_global_map_2d_device",
-    "sred_calculate_block_repetition_map_2d", "sred_block_map_2d_device", "sred_reference_block_2d",
+    "sred_calculate_block_repetition_map_2d", "sred_block_map_2d_device", "sred_block_map_2d_stack",
+    "sred_reference_block_2d",
     "sred_normalize_image_2d", "sred_debug_gram_rowdot", "sred_block_map_2d_device_noalloc",
     "sred_patch_hu_map_2d", "sred_hu_map_2d", "sred_phase_correlation_map_2d", "sred_global_map_2d_batch",
     "sred_global_map_2d_shard_sums", "sred_global_map_2d_shard_finish", "sred_set_log_callback",
@@ -110,6 +111,8 @@ def load() -> C.CDLL:
             _vp, C.c_char_p, _f32p, s, s, _f32p, s, s, s, C.c_float, C.c_float, C.c_float, s, _f32p]
         L.sred_block_map_2d_device.argtypes = [_vp, C.c_char_p, _vp, s, s, s, _f32p, s, s, s, C.c_float,
                                                C.c_float, C.c_float, s, _vp, _vp]
+        L.sred_block_map_2d_stack.argtypes = [_vp, C.c_char_p, _f32p, s, s, s, _f32p, s, s, s, C.c_float,
+                                              C.c_float, C.c_float, s, s, _f32p]
         L.sred_reference_block_2d.argtypes = [_f32p, s, s, _f32p, C.POINTER(C.c_int), _fp, _fp]
         L.sred_normalize_image_2d.argtypes = [_f32p, s, s, s, s, _vp]
         f = C.c_float

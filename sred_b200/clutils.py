@@ -305,6 +305,33 @@ def block_map_device(metric: str, d_img_ptr: int, width: int, height: int, frame
         C.c_void_p(stream_ptr or None)), "sred_block_map_2d_device")
 
 
+def block_map_stack(metric: str, stack: np.ndarray, reference_block: ReferenceBlock2D, relevance_constant: float,
+                    normalize_output: bool, chunk_frames: int = 0, out: np.ndarray | None = None,
+                    ctx=None) -> np.ndarray:
+    """Block maps of a host stack of frames [frames, h, w] (the time-lapse loop
+    of java/BlockRepetition2D_.java:95-130), each frame mapped and normalised
+    on its own. The stack streams through the GPU in chunks whose uploads,
+    maps and downloads overlap; pass page-locked arrays (e.g. a pinned torch
+    tensor's .numpy()) for stack and out to let the copies run concurrently."""
+    if metric not in BLOCK_METRICS and metric not in EXTRA_BLOCK_METRICS:
+        return None
+    c = _ctx(ctx)
+    a = np.ascontiguousarray(stack, np.float32)
+    if a.ndim == 2:
+        a = a[None]
+    frames, h, w = a.shape
+    if out is None:
+        out = np.empty_like(a)
+    res = out.reshape(frames, h, w)
+    st = c._L.sred_block_map_2d_stack(
+        c.h, metric.encode(), a.reshape(-1), w, h, frames,
+        np.ascontiguousarray(reference_block.pixels, np.float32).ravel(), int(reference_block.size),
+        reference_block.width, reference_block.height, float(reference_block.mean), float(reference_block.std),
+        float(relevance_constant), int(bool(normalize_output)), int(chunk_frames), res.reshape(-1))
+    c.check(st, "sred_block_map_2d_stack")
+    return res
+
+
 # ---------------------------------------------------------------------------
 # Volumes (java/CLUtils.java:1030-1653)
 # ---------------------------------------------------------------------------

@@ -138,6 +138,13 @@ void block_map_launch_shape(int w, int h, int frames, dim3* grid, dim3* block) {
   *block = dim3(kTileX, kThreadsY);
 }
 
+__global__ void k_init_minmax(unsigned* mm, int planes) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < planes; i += gridDim.x * blockDim.x) {
+    mm[2 * i] = 0xffffffffu;
+    mm[2 * i + 1] = 0u;
+  }
+}
+
 __device__ __forceinline__ float ord_to_float(unsigned u) {
   return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
 }

@@ -35,6 +35,10 @@ __global__ void k_minmax(const float* a, const float* mask, int W, int H, int bw
                          unsigned* mm);
 __global__ void k_remap(float* a, const float* mask, int W, int H, int bw_, int bh_, size_t plane,
                         const unsigned* mm);
+// Per-plane min/max words before k_minmax: {ordered +inf, ordered -inf} per plane
+// (a kernel rather than a copy from pageable host memory, which would wait
+// for the stream to drain).
+__global__ void k_init_minmax(unsigned* mm, int planes);
 
 // block_map.cu
 __global__ void k_block_map(const float* img, int W, int H, int frames, Ellipse e, RefBlock rb, int metric,

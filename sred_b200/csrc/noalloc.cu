@@ -48,13 +48,6 @@ sred_status scratch_address(int dev, unsigned char** out) {
   return SRED_OK;
 }
 
-__global__ void k_init_minmax(unsigned* mm, int planes) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < planes; i += gridDim.x * blockDim.x) {
-    mm[2 * i] = 0xffffffffu;
-    mm[2 * i + 1] = 0u;
-  }
-}
-
 int grid_of(size_t n, int threads, int cap) {
   size_t g = (n + threads - 1) / threads;
   if (g < 1) g = 1;

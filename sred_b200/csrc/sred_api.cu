@@ -28,7 +28,8 @@ namespace {
 enum BufId {
   B_IMG, B_MEANS, B_STDS, B_MASK, B_MASKIN, B_FLAGS, B_SLOT, B_GPIX, B_FPIX, B_COUNTS, B_U, B_A, B_B,
   B_PARAMS, B_RMAX, B_NUM, B_DEN, B_SUMS, B_OUT, B_VARS, B_MM, B_NMASK, B_BAD, B_STATUS, B_STDS2, B_COLSOA,
-  B_FEAT, B_SIG, B_FR, B_FI, B_GAT, B_OFF3, B_REF3, B_STAT, B_THR, B_KMX, B_KMD2, B_KMLAB, B_KMB, B_TBOX, B_TSTAT, B_TMEAN, B_TVAR, B_NBUF
+  B_FEAT, B_SIG, B_FR, B_FI, B_GAT, B_OFF3, B_REF3, B_STAT, B_THR, B_KMX, B_KMD2, B_KMLAB, B_KMB, B_TBOX, B_TSTAT, B_TMEAN, B_TVAR, B_STKIN, B_STKOUT,
+  B_NBUF
 };
 
 struct DevBuf {
@@ -56,6 +57,7 @@ struct sred_ctx {
   int num_sms = 148;
   int engine = SRED_ENGINE_FP32;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;  // sred_block_map_2d_stack's copy streams (lazily)
   cudaEvent_t ev[6] = {};
   DevBuf buf[B_NBUF];
   std::vector<float> hvars;
@@ -199,9 +201,7 @@ sred_status normalize_dev(sred_ctx* c, float* d_a, const float* d_mask, int w, i
                           cudaStream_t st) {
   unsigned* mm;
   CKS(ensure(c, B_MM, 2 * planes, &mm));
-  std::vector<unsigned> init(2 * planes);
-  for (int i = 0; i < planes; i++) { init[2 * i] = 0xffffffffu; init[2 * i + 1] = 0u; }
-  CK(cudaMemcpyAsync(mm, init.data(), sizeof(unsigned) * 2 * planes, cudaMemcpyHostToDevice, st));
+  k_init_minmax<<<grid_for((size_t)planes, 256, 64), 256, 0, st>>>(mm, planes);
   dim3 g(grid_for((size_t)w * h, 256, 4 * c->num_sms), planes);
   k_minmax<<<g, 256, 0, st>>>(d_a, d_mask, w, h, rw, rh, (size_t)w * h, mm);
   k_remap<<<g, 256, 0, st>>>(d_a, d_mask, w, h, rw, rh, (size_t)w * h, mm);
@@ -420,7 +420,7 @@ sred_status global_finish(sred_ctx* c, const GState& gs, cudaStream_t st, int no
     info->ms_finalize = t23;
     info->ms_total = t03;
     info->launches = (gs.given ? 0 : 2) + 4 + (gs.n_g > 0 ? (gs.engine == SRED_ENGINE_TC ? 3 : 2) : 0) + 1 +
-                     (normalize ? 2 : 0);
+                     (normalize ? 3 : 0);
   }
   if (c->log_cb) {
     float t03 = 0;
@@ -535,9 +535,7 @@ sred_status block_core(sred_ctx* c, int metric, const float* d_img, int w, int h
     if (metric == kAbsDiff) {
       unsigned* mm;
       CKS(ensure(c, B_MM, 2 * frames, &mm));
-      std::vector<unsigned> init(2 * frames);
-      for (int i = 0; i < frames; i++) { init[2 * i] = 0xffffffffu; init[2 * i + 1] = 0u; }
-      CK(cudaMemcpyAsync(mm, init.data(), sizeof(unsigned) * 2 * frames, cudaMemcpyHostToDevice, st));
+      k_init_minmax<<<grid_for((size_t)frames, 256, 64), 256, 0, st>>>(mm, frames);
       k_minmax<<<pg, 256, 0, st>>>(d_out, nullptr, w, h, rw, rh, plane, mm);
       k_block_absdiff_post<<<pg, 256, 0, st>>>(d_out, w, h, rw, rh, plane, mm);
     }
@@ -548,8 +546,7 @@ sred_status block_core(sred_ctx* c, int metric, const float* d_img, int w, int h
     if (normalize) CKS(normalize_dev(c, d_out, d_mask, w, h, rw, rh, frames, st));
   }
   CK(cudaGetLastError());
-  CK(cudaStreamSynchronize(st));
-  return SRED_OK;
+  return SRED_OK;  // enqueued on st; the callers decide when to wait
 }
 
 // ---------------------------------------------------------------------------
@@ -635,8 +632,7 @@ sred_status block3d_core(sred_ctx* c, int metric, const float* d_vol, int w, int
   if (normalize) {
     unsigned* mm;
     CKS(ensure(c, B_MM, 2, &mm));
-    const unsigned init[2] = {0xffffffffu, 0u};
-    CK(cudaMemcpyAsync(mm, init, sizeof(init), cudaMemcpyHostToDevice, st));
+    k_init_minmax<<<1, 32, 0, st>>>(mm, 1);
     k_minmax3d<<<grid_for((size_t)v.W * v.H * v.D, 256, 4 * c->num_sms), 256, 0, st>>>(d_out, d_mask, v, mm);
     k_remap3d<<<grid, blk, 0, st>>>(d_out, d_mask, v, mm);
     CK(cudaGetLastError());
@@ -788,8 +784,7 @@ sred_status global3d_finish(sred_ctx* c, const GState& gs, cudaStream_t st, int 
   if (normalize) {
     unsigned* mm;
     CKS(ensure(c, B_MM, 2, &mm));
-    const unsigned init[2] = {0xffffffffu, 0u};
-    CK(cudaMemcpyAsync(mm, init, sizeof(init), cudaMemcpyHostToDevice, st));
+    k_init_minmax<<<1, 32, 0, st>>>(mm, 1);
     k_minmax3d<<<grid_for((size_t)v.W * v.H * v.D, 256, 4 * c->num_sms), 256, 0, st>>>(d_out, d_mask, v, mm);
     k_remap3d<<<grid, blk, 0, st>>>(d_out, d_mask, v, mm);
     CK(cudaGetLastError());
@@ -816,7 +811,7 @@ sred_status global3d_finish(sred_ctx* c, const GState& gs, cudaStream_t st, int 
     info->ms_gram = t12;
     info->ms_finalize = t23;
     info->ms_total = t03;
-    info->launches = 5 + (gs.n_g > 0 ? (gs.engine == SRED_ENGINE_TC ? 3 : 2) : 0) + 1 + (normalize ? 2 : 0);
+    info->launches = 5 + (gs.n_g > 0 ? (gs.engine == SRED_ENGINE_TC ? 3 : 2) : 0) + 1 + (normalize ? 3 : 0);
   }
   if (c->log_cb) {
     float t03 = 0;
@@ -1384,6 +1379,8 @@ sred_status sred_destroy(sred_ctx* c) {
   for (auto& b : c->buf)
     if (b.p) cudaFree(b.p);
   for (auto& e : c->ev) cudaEventDestroy(e);
+  if (c->copy_in) cudaStreamDestroy(c->copy_in);
+  if (c->copy_out) cudaStreamDestroy(c->copy_out);
   cudaStreamDestroy(c->stream);
   delete c;
   return SRED_OK;
@@ -1734,6 +1731,89 @@ sred_status sred_calculate_block_repetition_map_2d(sred_ctx* c, const char* metr
   return SRED_OK;
 }
 
+sred_status sred_block_map_2d_stack(sred_ctx* c, const char* metric, const float* img, int w, int h, int frames,
+                                    const float* ref_pixels, int block_size, int bw, int bh, float ref_mean,
+                                    float ref_std, float relc, int normalize, int chunk_frames, float* out) {
+  if (!c || !img || !ref_pixels || !out) return SRED_ERR_ARG;
+  const int m = block_metric(metric);
+  if (m < 0) return fail(c, SRED_ERR_UNKNOWN_METRIC, "unknown block metric");
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (w <= 0 || h <= 0) return fail(c, SRED_ERR_ARG, "bad dimensions");
+  if (frames < 1 || chunk_frames < 0) return fail(c, SRED_ERR_ARG, "frames must be >= 1 and chunk_frames >= 0");
+  const size_t plane = (size_t)w * h;
+  // default chunk: about 32 MiB of frames, so a chunk's copy is long enough
+  // to hide the kernels of the neighbouring chunks and short enough to start
+  // the pipeline quickly
+  size_t chunk = chunk_frames > 0 ? (size_t)chunk_frames : ((size_t)32 << 20) / (plane * sizeof(float));
+  chunk = std::max<size_t>(1, std::min<size_t>(chunk, std::min(frames, 65535)));
+  const int nchunks = (int)((frames + chunk - 1) / chunk);
+  const size_t slot = chunk * plane;
+  float *d_in, *d_out;
+  CKS(ensure(c, B_STKIN, 2 * slot, &d_in));
+  CKS(ensure(c, B_STKOUT, 2 * slot, &d_out));
+  if (!c->copy_in) CK(cudaStreamCreateWithFlags(&c->copy_in, cudaStreamNonBlocking));
+  if (!c->copy_out) CK(cudaStreamCreateWithFlags(&c->copy_out, cudaStreamNonBlocking));
+  // events: [0] start, then per slot s: in_ready, computed, out_done
+  cudaEvent_t ev[7] = {};
+  for (auto& e : ev) {
+    const cudaError_t r = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    if (r != cudaSuccess) {
+      for (auto& x : ev)
+        if (x) cudaEventDestroy(x);
+      return cuda_fail(c, r, "sred_block_map_2d_stack: events");
+    }
+  }
+  cudaEvent_t *in_ready = ev + 1, *computed = ev + 3, *out_done = ev + 5;
+  auto drain = [&](sred_status st) {
+    // no copy may still read or write the caller's buffers when this returns
+    cudaStreamSynchronize(c->copy_in);
+    cudaStreamSynchronize(c->stream);
+    cudaStreamSynchronize(c->copy_out);
+    for (auto& x : ev) cudaEventDestroy(x);
+    if (st != SRED_OK) cudaGetLastError();
+    return st;
+  };
+  // the slots may still be in use by earlier work on the context's stream
+  {
+    cudaError_t e = cudaEventRecord(ev[0], c->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->copy_in, ev[0], 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->copy_out, ev[0], 0);
+    if (e != cudaSuccess) return drain(cuda_fail(c, e, "sred_block_map_2d_stack"));
+  }
+  // Chunk i uses slot i % 2: its upload waits until the map of chunk i - 2
+  // has read the slot, its map until its upload has landed and the download
+  // of chunk i - 2 has left the output slot, its download until its map is
+  // done. Uploads, maps and downloads of neighbouring chunks overlap.
+  for (int i = 0; i < nchunks; i++) {
+    const int s = i & 1;
+    const size_t f0 = (size_t)i * chunk;
+    const int nf = (int)std::min<size_t>(chunk, frames - f0);
+    float* di = d_in + s * slot;
+    float* dout = d_out + s * slot;
+    cudaError_t e = cudaSuccess;
+    if (i >= 2) e = cudaStreamWaitEvent(c->copy_in, computed[s], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(di, img + f0 * plane, nf * plane * sizeof(float), cudaMemcpyHostToDevice, c->copy_in);
+    if (e == cudaSuccess) e = cudaEventRecord(in_ready[s], c->copy_in);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, in_ready[s], 0);
+    if (e == cudaSuccess && i >= 2) e = cudaStreamWaitEvent(c->stream, out_done[s], 0);
+    if (e != cudaSuccess) return drain(cuda_fail(c, e, "sred_block_map_2d_stack: upload"));
+    sred_status st = block_core(c, m, di, w, h, nf, ref_pixels, block_size, bw, bh, ref_mean, ref_std, relc,
+                                normalize, dout, c->stream);
+    if (st != SRED_OK) return drain(st);
+    e = cudaEventRecord(computed[s], c->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->copy_out, computed[s], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(out + f0 * plane, dout, nf * plane * sizeof(float), cudaMemcpyDeviceToHost, c->copy_out);
+    if (e == cudaSuccess) e = cudaEventRecord(out_done[s], c->copy_out);
+    if (e != cudaSuccess) return drain(cuda_fail(c, e, "sred_block_map_2d_stack: download"));
+  }
+  cudaError_t e = cudaStreamSynchronize(c->copy_out);
+  if (e != cudaSuccess) return drain(cuda_fail(c, e, "sred_block_map_2d_stack"));
+  return drain(SRED_OK);
+}
+
 sred_status sred_block_map_2d_device(sred_ctx* c, const char* metric, const float* d_img, int w, int h,
                                      int frames, const float* ref_pixels, int block_size, int bw, int bh,
                                      float ref_mean, float ref_std, float relc, int normalize, float* d_out,
@@ -1743,8 +1823,11 @@ sred_status sred_block_map_2d_device(sred_ctx* c, const char* metric, const floa
   if (m < 0) return fail(c, SRED_ERR_UNKNOWN_METRIC, "unknown block metric");
   std::lock_guard<std::recursive_mutex> lk(c->mu);
   cudaSetDevice(c->device);
-  return block_core(c, m, d_img, w, h, frames, ref_pixels, block_size, bw, bh, ref_mean, ref_std, relc, normalize,
-                    d_out, pick(c, stream));
+  const cudaStream_t st = pick(c, stream);
+  CKS(block_core(c, m, d_img, w, h, frames, ref_pixels, block_size, bw, bh, ref_mean, ref_std, relc, normalize,
+                 d_out, st));
+  CK(cudaStreamSynchronize(st));
+  return SRED_OK;
 }
 
 sred_status sred_debug_gram_rowdot(sred_ctx* c, int engine, const float* u, const float* w1, const float* w2, int n,

@@ -43,16 +43,17 @@ def block_repetition_2d(block: np.ndarray, image: np.ndarray, relevance_constant
     ref = utils.get_reference_block_2d(block)
     if ref is None:
         raise ValueError("Block dimensions must be odd (e.g., 3x3 or 5x5). Please try again.")
-    frames = image if image.ndim == 3 else image[None]
-    outs = []
-    for f in frames:  # time-lapse: each frame normalised on its own (java/BlockRepetition2D_.java:104-130)
-        inp = utils.get_input_image_2d(f, True, stabilise_noise_variance, ctx=ctx)
+    if image.ndim == 2:
+        inp = utils.get_input_image_2d(image, True, stabilise_noise_variance, ctx=ctx)
         out = clutils.calculate_block_repetition_map_2d(metric, inp, ref, relevance_constant, normalize_output,
                                                         ctx=ctx)
-        if out is None:
-            return None
-        outs.append(out.reshape(inp.height, inp.width))
-    return np.stack(outs) if image.ndim == 3 else outs[0]
+        return None if out is None else out.reshape(inp.height, inp.width)
+    # time-lapse: each frame prepared on its own (java/BlockRepetition2D_.java:104-130), then the whole
+    # stack streams through the GPU with its copies overlapping the maps
+    h, w = image.shape[1:]
+    stack = np.stack([utils.get_input_image_2d(f, True, stabilise_noise_variance, ctx=ctx).image_array.reshape(h, w)
+                      for f in image])
+    return clutils.block_map_stack(metric, stack, ref, relevance_constant, normalize_output, ctx=ctx)
 
 
 def global_repetition_3d(volume: np.ndarray, block_width: int = 3, block_height: int = 3, block_depth: int = 3,
