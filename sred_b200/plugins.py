@@ -7,8 +7,9 @@ BlockRepetition2D_.run (java/BlockRepetition2D_.java:32-158), the 3D pair
 GlobalRepetition3D_ / BlockRepetition3D_, and the relevance-mask tools
 RelevanceMask2D_, RelevanceMaskStack2D_ and OptimiseRelevanceMask_,
 ClassifyRedundancy_, CalculateLocalMeans_, and the variance-stabilisation
-commands QuadTree_ / OcTree_. Variance stabilisation inside the map commands
-uses either GAT method ("Simplex" or "Quad/Octree").
+commands VarianceStabilisingTransform2D_ / 3D_ (Simplex) and QuadTree_ /
+OcTree_. Variance stabilisation inside the map commands uses either GAT method
+("Simplex" or "Quad/Octree").
 """
 from __future__ import annotations
 
@@ -165,3 +166,48 @@ def octree_gat_3d(volume: np.ndarray, min_size: int = 4, alpha: float = 0.01, ma
                   lts_fraction: float = 0.75, ctx=None) -> tuple:
     """OcTree_.run (java/OcTree_.java): (variance-stabilised volume, g0, eDC, leaves)."""
     return utils.gat_octree_3d(volume, min_size, alpha, max_iterations, lts_fraction, ctx=ctx)
+
+
+def roi_offset_and_sigma(image: np.ndarray, roi: tuple) -> tuple:
+    """The ROI estimate of VarianceStabilisingTransform2D_ (meanAndStdDev,
+    java/VarianceStabilisingTransform2D_.java:116-133): over the rectangle
+    roi = (x, y, width, height), row by row, the one-pass FP64 mean and
+    sqrt(sum(v^2)/n - mean^2), summed in raster order (NaN if rounding makes
+    the variance negative, as Math.sqrt does)."""
+    x, y, w, h = (int(v) for v in roi)
+    v = np.asarray(image, np.float64)[y:y + h, x:x + w].ravel()
+    if v.size == 0:
+        return 0.0, 0.0
+    s = float(np.cumsum(v)[-1])           # sequential, as the Java loop
+    sq = float(np.cumsum(v * v)[-1])
+    mean = s / v.size
+    with np.errstate(invalid="ignore"):
+        return mean, float(np.sqrt(np.float64(sq / v.size - mean * mean)))
+
+
+def variance_stabilising_transform_2d(image: np.ndarray, gain: float = 1.0, offset: float = 10.0,
+                                      sigma: float = 100.0, roi: tuple | None = None, max_iterations: int = 5000,
+                                      ctx=None) -> tuple:
+    """VarianceStabilisingTransform2D_.run (java/VarianceStabilisingTransform2D_.java:17-113): the
+    GATMinimizer2D Simplex fit from the dialog's starting guesses (or with the offset and noise std
+    estimated from a rectangular ROI), then getGAT with the fitted parameters. Returns
+    (variance-stabilised image, gain, sigma, offset)."""
+    a = np.ascontiguousarray(image, np.float32)
+    if a.ndim != 2:
+        raise ValueError("expected a 2D image")
+    if roi is not None:
+        offset, sigma = roi_offset_and_sigma(a, roi)
+    g, s, o, _ = utils.fit_gat_2d(a, max_iterations, gain, sigma, offset, ctx=ctx)
+    return utils.get_gat_2d(a, g, s, o, ctx=ctx), g, s, o
+
+
+def variance_stabilising_transform_3d(volume: np.ndarray, gain: float = 1.0, offset: float = 10.0,
+                                      sigma: float = 100.0, max_iterations: int = 5000, ctx=None) -> tuple:
+    """VarianceStabilisingTransform3D_.run (java/VarianceStabilisingTransform3D_.java): the
+    GATMinimizer3D Simplex fit from the dialog's starting guesses, then getGAT over every voxel.
+    Returns (variance-stabilised volume, gain, sigma, offset)."""
+    a = np.ascontiguousarray(volume, np.float32)
+    if a.ndim != 3 or a.shape[0] < 2:
+        raise ValueError("Image is not 3D. Please open a 3D image and try again.")
+    g, s, o, _ = utils.fit_gat_3d(a, max_iterations, gain, sigma, offset, ctx=ctx)
+    return utils.get_gat_3d(a, g, s, o, ctx=ctx), g, s, o

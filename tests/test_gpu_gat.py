@@ -122,3 +122,27 @@ def test_gat_tree_in_input_images(ctx):
         oracle.gat_tree(flat, octree=True)
     with pytest.raises(_lib.SredError):
         utils.gat_octree_3d(flat, ctx=ctx)
+
+
+def test_variance_stabilising_commands(ctx):
+    """VarianceStabilisingTransform2D_ / 3D_: the Simplex fit from the dialog's
+    guesses (gain 1, offset 10, noise std 100) or from a ROI estimate, then
+    getGAT with the fitted parameters; the 3D command refuses single slices."""
+    from sred_b200 import plugins
+    from tests.test_oracle import _poisson_gaussian3d
+    img = _poisson_gaussian(200, 150, 2.0, 5.0, 100.0, 9)
+    out, g, s, o = plugins.variance_stabilising_transform_2d(img, max_iterations=3000, ctx=ctx)
+    assert (g, s, o) == utils.fit_gat_2d(img, 3000, 1.0, 100.0, 10.0, ctx=ctx)[:3]
+    np.testing.assert_array_equal(out, oracle.gat(img, g, s, o))
+    assert oracle.gat_objective(img, g, s, o) < oracle.gat_objective(img, 1.0, 100.0, 10.0) / 10
+    roi = (10, 20, 30, 25)
+    off, sd = plugins.roi_offset_and_sigma(img, roi)
+    out2, g2, s2, o2 = plugins.variance_stabilising_transform_2d(img, roi=roi, max_iterations=3000, ctx=ctx)
+    assert (g2, s2, o2) == utils.fit_gat_2d(img, 3000, 1.0, sd, off, ctx=ctx)[:3]
+    np.testing.assert_array_equal(out2, oracle.gat(img, g2, s2, o2))
+    vol = _poisson_gaussian3d(40, 36, 12, 2.0, 5.0, 100.0, 10)
+    v3, g3, s3, o3 = plugins.variance_stabilising_transform_3d(vol, max_iterations=2000, ctx=ctx)
+    assert (g3, s3, o3) == utils.fit_gat_3d(vol, 2000, 1.0, 100.0, 10.0, ctx=ctx)[:3]
+    np.testing.assert_array_equal(v3, utils.get_gat_3d(vol, g3, s3, o3, ctx=ctx))
+    with pytest.raises(ValueError):
+        plugins.variance_stabilising_transform_3d(vol[:1], ctx=ctx)
