@@ -463,6 +463,8 @@ sred_status sred_classify_redundancy_2d(sred_ctx *ctx, const float *map, int w, 
  * on the device the way the 3D Pearson block kernel divides by a shared
  * divisor (Markstein's correction of a * RN(1/b)); equal to IEEE division. */
 sred_status sred_debug_divide_fixed(sred_ctx *ctx, const float *a, size_t n, float b, float *out);
+/* The same in FP64 (the block-map Hu kernel's divisor: one per block). */
+sred_status sred_debug_divide_fixed64(sred_ctx *ctx, const double *a, size_t n, double b, double *out);
 
 /* Variance stabilisation by the quadtree (2D) / octree (3D) method, the
  * "Quad/Octree" option (java/QuadTree_.java, java/OcTree_.java; the commands'

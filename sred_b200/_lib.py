@@ -32,7 +32,7 @@ EXPORTS = [
     "sred_block_map_3d_device", "sred_calculate_global_repetition_map_3d", "sred_global_map_3d_device",
     "sred_relevance_mask_tool_2d", "sred_relevance_mask_sweep_2d", "sred_relevance_constant_range_2d",
     "sred_gat_3d", "sred_gat_objective_3d", "sred_gat_fit_3d", "sred_classify_redundancy_2d",
-    "sred_debug_divide_fixed", "sred_gat_quadtree_2d", "sred_gat_octree_3d", "sred_f_quantile",
+    "sred_debug_divide_fixed", "sred_debug_divide_fixed64", "sred_gat_quadtree_2d", "sred_gat_octree_3d", "sred_f_quantile",
     "sred_global_map_3d_shard_sums", "sred_global_map_3d_shard_finish",
 ]
 
@@ -131,6 +131,8 @@ def load() -> C.CDLL:
         L.sred_classify_redundancy_2d.argtypes = [_vp, _f32p, s, s, s, s, s, s, C.c_int64, _f32p,
                                                   C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L.sred_debug_divide_fixed.argtypes = [_vp, _f32p, C.c_size_t, f, _f32p]
+        _f64p = np.ctypeslib.ndpointer(np.float64, flags="C")
+        L.sred_debug_divide_fixed64.argtypes = [_vp, _f64p, C.c_size_t, C.c_double, _f64p]
         L.sred_gat_quadtree_2d.argtypes = [_vp, _f32p, s, s, s, f, s, f, _dp, _dp, C.POINTER(C.c_int)]
         L.sred_gat_octree_3d.argtypes = [_vp, _f32p, s, s, s, s, f, s, f, _dp, _dp, C.POINTER(C.c_int)]
         L.sred_f_quantile.restype = C.c_double

@@ -88,6 +88,13 @@ __device__ __forceinline__ float div_fixed(float a, float b, float y) {
   const float r = __fmaf_rn(-q, b, a);
   return __fmaf_rn(r, y, q);
 }
+// The same in FP64 (y = RN(1/b) from __drcp_rn); tested against IEEE
+// division (sred_debug_divide_fixed64).
+__device__ __forceinline__ double div_fixed(double a, double b, double y) {
+  const double q = __dmul_rn(a, y);
+  const double r = __fma_rn(-q, b, a);
+  return __fma_rn(r, y, q);
+}
 
 // Epilogue constants shared by all tiles of one map.
 struct EpiConsts {

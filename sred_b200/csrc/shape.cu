@@ -39,12 +39,14 @@ __global__ void __launch_bounds__(128)
   // :129-140: the gather's ellipse test divides integers, which keeps every
   // position of the square except its four corners; the sum is divided by
   // patch_size all the same.
+  // (i / rw and j / rh are 0 inside and +-1 on the square's edges, so the
+  // test fails exactly where both are +-1; tested that way, in the same order)
   double mean = 0.0;
-  for (int j = -rh; j <= rh; j++)
-    for (int i = -rw; i <= rw; i++) {
-      const float dx = (float)(i / rw), dy = (float)(j / rh);
-      if (dx * dx + dy * dy <= 1.0f) mean += (double)img[(size_t)(y + j) * W + x + i];
-    }
+  for (int j = -rh; j <= rh; j++) {
+    const bool edge_y = j == -rh || j == rh;
+    for (int i = -rw; i <= rw; i++)
+      if (!(edge_y && (i == -rw || i == rw))) mean += (double)img[(size_t)(y + j) * W + x + i];
+  }
   mean /= (double)patch_size;
   // :143-171: mean-subtract and min/max over the ellipse (raster order).
   double mn = DBL_MAX, mx = -DBL_MAX;
@@ -54,10 +56,14 @@ __global__ void __launch_bounds__(128)
     mx = mx < p ? p : mx;
   }
   const double den = mx - mn + (double)kEps;
+  // every element is divided by the block's one divisor: its correctly
+  // rounded reciprocal once, then Markstein's correction per element (the
+  // IEEE quotient, for three FP64 operations instead of a division)
+  const double rden = __drcp_rn(den);
   // :174-205: remap to [0, 1] and raw moments (1-based coordinates).
   double m00 = 0.0, m10 = 0.0, m01 = 0.0;
   for (int k = 0; k < e.k; k++) {
-    const double r = (((double)img[(size_t)(y + e.dy[k]) * W + x + e.dx[k]] - mean) - mn) / den;
+    const double r = div_fixed(((double)img[(size_t)(y + e.dy[k]) * W + x + e.dx[k]] - mean) - mn, den, rden);
     m00 += r;
     m10 += (double)(e.dx[k] + rw + 1) * r;
     m01 += (double)(e.dy[k] + rh + 1) * r;
@@ -66,7 +72,7 @@ __global__ void __launch_bounds__(128)
   const double cx = m10 / (m00 + (double)kEps), cy = m01 / (m00 + (double)kEps);
   double mu20 = 0.0, mu02 = 0.0;
   for (int k = 0; k < e.k; k++) {
-    const double r = (((double)img[(size_t)(y + e.dy[k]) * W + x + e.dx[k]] - mean) - mn) / den;
+    const double r = div_fixed(((double)img[(size_t)(y + e.dy[k]) * W + x + e.dx[k]] - mean) - mn, den, rden);
     const double ax = (double)(e.dx[k] + rw) - cx, ay = (double)(e.dy[k] + rh) - cy;
     mu20 += (ax * ax) * r;
     mu02 += (ay * ay) * r;

@@ -2600,6 +2600,22 @@ sred_status sred_classify_redundancy_2d(sred_ctx* c, const float* map, int w, in
   return SRED_OK;
 }
 
+sred_status sred_debug_divide_fixed64(sred_ctx* c, const double* a, size_t n, double b, double* out) {
+  if (!c || !a || !out) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  c->shard.valid = false;
+  double *d_a, *d_o;
+  CKS(ensure(c, B_IMG, n, &d_a));
+  CKS(ensure(c, B_OUT, n, &d_o));
+  CK(cudaMemcpyAsync(d_a, a, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  k_divide_fixed64<<<grid_for(n, 256, 8 * c->num_sms), 256, 0, c->stream>>>(d_a, n, b, d_o);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, d_o, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SRED_OK;
+}
+
 sred_status sred_debug_divide_fixed(sred_ctx* c, const float* a, size_t n, float b, float* out) {
   if (!c || !a || !out) return SRED_ERR_ARG;
   std::lock_guard<std::recursive_mutex> lk(c->mu);

@@ -188,6 +188,13 @@ __global__ void k_divide_fixed(const float* __restrict__ a, size_t n, float b, f
     out[i] = div_fixed(a[i], b, y);
 }
 
+// Elementwise a[i] / b by the FP64 div_fixed (diagnostics: checked against IEEE division).
+__global__ void k_divide_fixed64(const double* __restrict__ a, size_t n, double b, double* __restrict__ out) {
+  const double y = __drcp_rn(b);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = div_fixed(a[i], b, y);
+}
+
 // Host steps on the interior (java/CLUtils.java:1459-1471, 1590-1600): NRMSE
 // inverted (0 -> 1), Abs-diff turned into 1 - x.
 __global__ void k_block3d_post(float* __restrict__ a, Vol3 v, int metric) {

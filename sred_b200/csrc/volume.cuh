@@ -28,6 +28,7 @@ cudaError_t launch_block_map3d(const float* img, Vol3 v, const int* off, const f
                                float ref_std, int metric, const float* means, const float* stds, float* out,
                                cudaStream_t st);
 __global__ void k_divide_fixed(const float* a, size_t n, float b, float* out);
+__global__ void k_divide_fixed64(const double* a, size_t n, double b, double* out);
 __global__ void k_block3d_post(float* a, Vol3 v, int metric);
 __global__ void k_mask3d(const float* stds, Vol3 v, float thr, float* mask, float* map);
 __global__ void k_minmax3d(const float* a, const float* mask, Vol3 v, unsigned* mm);

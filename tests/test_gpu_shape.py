@@ -171,3 +171,23 @@ def test_hu_map_constant_image(ctx):
     img = np.full((20, 24), 0.25, np.float32)
     got = clutils.get_hu_map_2d(_inp(img), _stats(img, 3, 3), 3, 3, ctx=ctx)
     assert not np.any(got)
+
+
+def test_fixed_divisor_division_fp64_is_ieee(ctx):
+    """The FP64 div_fixed (Markstein's correction of a * RN(1/b)) that the
+    block-map Hu kernel divides each block by, against IEEE float64 division
+    on 4M numerators per divisor: uniform in [0, b] (the kernel's range),
+    uniform in [0, 1], tiny (down to 1e-200), powers of two and exact
+    multiples of the divisor; divisors like max - min + eps of normalised
+    blocks and awkward significands."""
+    rng = np.random.default_rng(22)
+    base = np.concatenate([rng.random(1 << 21), 10.0 ** rng.uniform(-200, 0, 1 << 20),
+                           2.0 ** rng.integers(-600, 1, 1 << 19).astype(np.float64), np.zeros(16)])
+    for b in (1.0 + 1e-9, 0.37, 3.0e-3, 1.0e-6 + 1e-9, 0.9999999999999999, 1.0000000000000002,
+              1.9999999999999998, 1.4142135623730951):
+        aa = np.concatenate([base, base[: 1 << 21] * b, b * np.arange(1, 1 << 19, dtype=np.float64)])
+        out = np.empty_like(aa)
+        ctx.check(ctx._L.sred_debug_divide_fixed64(ctx.h, aa, aa.size, float(b), out), "sred_debug_divide_fixed64")
+        exp = aa / b
+        bad = np.flatnonzero(out.view(np.uint64) != exp.view(np.uint64))
+        assert bad.size == 0, (b, aa[bad[:5]], out[bad[:5]], exp[bad[:5]])
