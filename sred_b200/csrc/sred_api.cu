@@ -603,9 +603,13 @@ sred_status mask_3d(sred_ctx* c, const Vol3& v, const float* d_stds, float relc,
   return SRED_OK;
 }
 
+// With h_vol, d_vol is filled from host memory here, in slabs of slices on
+// the context's upload stream, and each slab's local statistics and map run
+// as soon as the slices they read have landed, so the upload overlaps the
+// kernels; the slabs' maps equal one launch over the volume.
 sred_status block3d_core(sred_ctx* c, int metric, const float* d_vol, int w, int h, int d, const float* ref_pixels,
                          int block_size, int bw, int bh, int bd, float ref_mean, float ref_std, float relc,
-                         int normalize, float* d_out, cudaStream_t st) {
+                         int normalize, float* d_out, cudaStream_t st, const float* h_vol = nullptr) {
   c->shard.valid = false;  // shares workspaces with the global map
   if (metric < kPearson || metric > kAbsDiff) return fail(c, SRED_ERR_UNKNOWN_METRIC, "unknown 3D block metric");
   if (fault("launch")) return fail(c, SRED_ERR_LAUNCH, "injected launch failure");
@@ -620,10 +624,53 @@ sred_status block3d_core(sred_ctx* c, int metric, const float* d_vol, int w, int
   CKS(ensure(c, B_STDS, n, &d_stds));
   CK(cudaMemcpyAsync(d_ref, ref_pixels, sizeof(float) * v.k, cudaMemcpyHostToDevice, st));
   const dim3 grid = vol_grid(v), blk(32, 4);
-  k_local_stats3d<<<grid, blk, sizeof(int) * v.k, st>>>(d_vol, v, d_off, d_means, d_stds);
-  CK(launch_block_map3d(d_vol, v, d_off, d_ref, ref_mean, ref_std, metric, d_means, d_stds, d_out, st));
-  if (metric == kNrmse || metric == kAbsDiff) k_block3d_post<<<grid, blk, 0, st>>>(d_out, v, metric);
-  CK(cudaGetLastError());
+  // slices [z0, z1): local statistics, map, metric transform
+  auto slab = [&](int z0, int z1) -> sred_status {
+    if (z1 <= z0) return SRED_OK;
+    Vol3 vs = v;
+    vs.z0 = z0;
+    const dim3 gs(grid.x, grid.y, z1 - z0);
+    k_local_stats3d<<<gs, blk, sizeof(int) * v.k, st>>>(d_vol, vs, d_off, d_means, d_stds);
+    CK(launch_block_map3d(d_vol, vs, d_off, d_ref, ref_mean, ref_std, metric, d_means, d_stds, d_out, st, z1));
+    if (metric == kNrmse || metric == kAbsDiff) k_block3d_post<<<gs, blk, 0, st>>>(d_out, vs, metric);
+    CK(cudaGetLastError());
+    return SRED_OK;
+  };
+  if (!h_vol) {
+    CKS(slab(0, d));
+  } else {
+    // slabs of about 16 MiB (at most 64): the map of slices [z0, z1) reads
+    // slices [z0 - rd, z1 + rd), so after slab i has landed the slices up to
+    // its end minus rd are computed
+    const size_t plane = (size_t)w * h;
+    int ds = (int)std::max<size_t>(1, ((size_t)16 << 20) / (plane * sizeof(float)));
+    ds = std::max(ds, (d + 63) / 64);
+    const int ns = (d + ds - 1) / ds;
+    if (!c->copy_in) CK(cudaStreamCreateWithFlags(&c->copy_in, cudaStreamNonBlocking));
+    std::vector<cudaEvent_t> up(ns, nullptr);
+    sred_status res = SRED_OK;
+    cudaError_t e = cudaEventRecord(c->ev[5], st);  // the volume buffer may still be read by earlier work
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->copy_in, c->ev[5], 0);
+    int done = 0;  // slices computed so far
+    for (int i = 0; i < ns && e == cudaSuccess && res == SRED_OK; i++) {
+      const int z_lo = i * ds, z_hi = std::min(d, z_lo + ds);
+      e = cudaEventCreateWithFlags(&up[i], cudaEventDisableTiming);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(const_cast<float*>(d_vol) + (size_t)z_lo * plane, h_vol + (size_t)z_lo * plane,
+                            (size_t)(z_hi - z_lo) * plane * sizeof(float), cudaMemcpyHostToDevice, c->copy_in);
+      if (e == cudaSuccess) e = cudaEventRecord(up[i], c->copy_in);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(st, up[i], 0);
+      if (e != cudaSuccess) break;
+      const int z_end = i == ns - 1 ? d : std::max(done, z_hi - v.rd);
+      res = slab(done, z_end);
+      done = z_end;
+    }
+    cudaStreamSynchronize(c->copy_in);  // the host volume is no longer read
+    for (cudaEvent_t x : up)
+      if (x) cudaEventDestroy(x);
+    if (e != cudaSuccess) return cuda_fail(c, e, "block3d_core: slab upload");
+    CKS(res);
+  }
   float* d_mask = nullptr;
   if (relc > 0.0f) {
     CKS(ensure(c, B_MASK, n, &d_mask));
@@ -2388,9 +2435,8 @@ sred_status sred_calculate_block_repetition_map_3d(sred_ctx* c, const char* metr
   float *d_vol, *d_out;
   CKS(ensure(c, B_IMG, n, &d_vol));
   CKS(ensure(c, B_OUT, n, &d_out));
-  CK(cudaMemcpyAsync(d_vol, vol, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
   CKS(block3d_core(c, m, d_vol, w, h, d, ref_pixels, block_size, bw, bh, bd, ref_mean, ref_std, relc, normalize,
-                   d_out, c->stream));
+                   d_out, c->stream, vol));
   CK(cudaMemcpyAsync(out, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return SRED_OK;

@@ -22,11 +22,12 @@ __device__ __forceinline__ bool interior3(int x, int y, int z, const Vol3& v) {
   return x >= v.rw && x < v.W - v.rw && y >= v.rh && y < v.H - v.rh && z >= v.rd && z < v.D - v.rd;
 }
 
-// Voxel of this thread for the (32, 4) block and ((W+31)/32, (H+3)/4, D) grid.
+// Voxel of this thread for the (32, 4) block and ((W+31)/32, (H+3)/4, D) grid
+// (or a grid of fewer slices starting at slice v.z0).
 __device__ __forceinline__ bool voxel(const Vol3& v, int* x, int* y, int* z, size_t* p) {
   *x = blockIdx.x * blockDim.x + threadIdx.x;
   *y = blockIdx.y * blockDim.y + threadIdx.y;
-  *z = blockIdx.z;
+  *z = blockIdx.z + v.z0;
   if (*x >= v.W || *y >= v.H) return false;
   *p = ((size_t)*z * v.H + *y) * v.W + *x;
   return true;
@@ -160,8 +161,8 @@ __global__ void __launch_bounds__(128)
 
 cudaError_t launch_block_map3d(const float* img, Vol3 v, const int* off, const float* ref, float ref_mean,
                                float ref_std, int metric, const float* means, const float* stds, float* out,
-                               cudaStream_t st) {
-  const dim3 grid((v.W + 31) / 32, (v.H + 3) / 4, v.D), blk(32, 4);
+                               cudaStream_t st, int z1) {
+  const dim3 grid((v.W + 31) / 32, (v.H + 3) / 4, (z1 < 0 ? v.D : z1) - v.z0), blk(32, 4);
   // The Pearson chain caches its first normalisation (K x 128 floats) while
   // that fits in 96 KB of shared memory; past it, it recomputes.
   const size_t smem_base = 2 * sizeof(int) * (size_t)v.k;

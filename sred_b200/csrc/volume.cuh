@@ -12,6 +12,7 @@ struct Vol3 {
   int W, H, D;
   int rw, rh, rd;
   int k;
+  int z0 = 0;  // first slice of a launch over slices [z0, z0 + gridDim.z) of the per-voxel kernels
 };
 
 // Host: linear offsets (z W H + y W + x) of the voxels of the ellipsoid
@@ -23,10 +24,10 @@ int build_ellipsoid(int bw, int bh, int bd, int W, int H, int* off);
 // floats (block map).
 __global__ void k_local_stats3d(const float* img, Vol3 v, const int* off, float* means, float* stds);
 // The raw 3D block map (one thread per voxel; the dynamic shared memory it
-// needs is chosen here).
+// needs is chosen here) over slices [v.z0, z1) (z1 < 0: to the last slice).
 cudaError_t launch_block_map3d(const float* img, Vol3 v, const int* off, const float* ref, float ref_mean,
                                float ref_std, int metric, const float* means, const float* stds, float* out,
-                               cudaStream_t st);
+                               cudaStream_t st, int z1 = -1);
 __global__ void k_divide_fixed(const float* a, size_t n, float b, float* out);
 __global__ void k_divide_fixed64(const double* a, size_t n, double b, double* out);
 __global__ void k_block3d_post(float* a, Vol3 v, int metric);

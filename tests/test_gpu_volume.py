@@ -207,6 +207,29 @@ def test_global_map_3d_device_and_edges(ctx):
         clutils.calculate_global_repetition_map_3d("SSIM", _inp(vol), 3, 4, 3, 0.0, True, ctx=ctx)
 
 
+def test_host_volume_streams_in_slabs(ctx):
+    """The host-buffer 3D block map uploads the volume in slabs of 16 MiB
+    (16 slices of 512 x 512 here) and maps each slab once the slices it reads
+    have landed; the maps equal the device entry point's one launch over the
+    volume, for every metric, relevance 0 and 1, and depth radii 1 and 2
+    (slab edges fall inside blocks)."""
+    import torch
+    vol = synth.normalize_input(synth.spot_volume(512, 512, 37, 40, 6, seed=12))
+    d, h, w = vol.shape
+    d_in = torch.from_numpy(vol).cuda()
+    d_out = torch.empty_like(d_in)
+    for bw, bd in ((3, 3), (5, 5)):
+        rb = utils.get_reference_block_3d(_block(vol, bw, bw, bd))
+        for metric in clutils.BLOCK_METRICS_3D:
+            for relc in (0.0, 1.0):
+                got = clutils.calculate_block_repetition_map_3d(metric, _inp(vol), rb, relc, True, ctx=ctx)
+                clutils.block_map_3d_device(metric, d_in.data_ptr(), w, h, d, rb, relc, True, d_out.data_ptr(),
+                                            ctx=ctx)
+                torch.cuda.synchronize()
+                np.testing.assert_array_equal(got.ravel(), d_out.cpu().numpy().ravel(),
+                                              err_msg=f"{metric} {bw}x{bw}x{bd} c={relc}")
+
+
 def test_fixed_divisor_division_is_ieee(ctx):
     """div_fixed (Markstein's correction of a * RN(1/b)) against IEEE float32
     division on 4M numerators per divisor: uniform in [0, 1], tiny (down to
