@@ -332,6 +332,53 @@ def block_map_stack(metric: str, stack: np.ndarray, reference_block: ReferenceBl
     return res
 
 
+def shard_frames(frames: int, rank: int, world: int) -> tuple[int, int]:
+    """Frames [f0, f1) of a time-lapse that rank `rank` of `world` maps:
+    contiguous, sizes differing by at most one."""
+    return frames * rank // world, frames * (rank + 1) // world
+
+
+def block_map_stack_sharded(metric: str, stack: np.ndarray, reference_block: ReferenceBlock2D,
+                            relevance_constant: float, normalize_output: bool, rank: int, world: int,
+                            gather: bool = True, all_gather=None, compute=None, ctx=None):
+    """A time-lapse block map across `world` ranks (one GPU each): frames are
+    independent, so rank r maps frames shard_frames(F, r, world) with
+    block_map_stack and no data moves between ranks while mapping. With
+    gather, one all-gather (default torch.distributed.all_gather, padded to
+    the largest shard) gives every rank the whole [F, h, w] result; without
+    it, the rank's own (f0, f1, maps) is returned. `compute(sub_stack)`
+    replaces the per-rank mapping (tests)."""
+    a = np.ascontiguousarray(stack, np.float32)
+    frames, h, w = a.shape
+    f0, f1 = shard_frames(frames, rank, world)
+    if compute is None:
+        def compute(sub):
+            if sub.shape[0] == 0:
+                return np.zeros_like(sub)
+            return block_map_stack(metric, sub, reference_block, relevance_constant, normalize_output, ctx=ctx)
+    mine = compute(a[f0:f1])
+    if mine is None:
+        return None
+    if not gather:
+        return f0, f1, mine
+    import torch
+    import torch.distributed as dist
+    if all_gather is None:
+        all_gather = dist.all_gather
+    span = max(shard_frames(frames, r, world)[1] - shard_frames(frames, r, world)[0] for r in range(world))
+    on_gpu = dist.is_initialized() and dist.get_backend() == "nccl"
+    dev = torch.device("cuda", torch.cuda.current_device()) if on_gpu else torch.device("cpu")
+    buf = torch.zeros((span, h, w), dtype=torch.float32, device=dev)
+    buf[:f1 - f0] = torch.from_numpy(np.ascontiguousarray(mine, np.float32)).to(dev)
+    parts = [torch.empty_like(buf) for _ in range(world)]
+    all_gather(parts, buf)
+    out = np.empty((frames, h, w), np.float32)
+    for r in range(world):
+        g0, g1 = shard_frames(frames, r, world)
+        out[g0:g1] = parts[r][:g1 - g0].cpu().numpy()
+    return out
+
+
 # ---------------------------------------------------------------------------
 # Volumes (java/CLUtils.java:1030-1653)
 # ---------------------------------------------------------------------------

@@ -75,3 +75,16 @@ def test_stack_errors(ctx):
         one = clutils.calculate_block_repetition_map_2d("Pearson's R", utils.InputImage2D(small[f].ravel(), 4, 4), rb,
                                                         0.0, True, ctx=ctx)
         np.testing.assert_array_equal(got[f].ravel(), one)
+
+
+def test_frame_sharded_stack_on_one_gpu(ctx):
+    """Each of three ranks' frame shards, mapped in turn on one GPU
+    (block_map_stack_sharded without the gather), put together equals the
+    whole stack mapped at once."""
+    st = _stack(7)
+    rb = utils.get_reference_block_2d(st[0, 10:15, 20:25])
+    whole = clutils.block_map_stack("SSIM", st, rb, 1.0, True, ctx=ctx)
+    parts = [clutils.block_map_stack_sharded("SSIM", st, rb, 1.0, True, r, 3, gather=False, ctx=ctx)
+             for r in range(3)]
+    assert [(f0, f1) for f0, f1, _ in parts] == [(0, 2), (2, 4), (4, 7)]
+    np.testing.assert_array_equal(np.concatenate([m for _, _, m in parts]), whole)

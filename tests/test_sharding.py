@@ -101,3 +101,56 @@ def test_sharded_exchange_gloo_two_ranks(metric):
     res = sorted(q.get(timeout=5) for _ in range(2))
     assert [r for r, _ in res] == [0, 1]
     assert all(err < 1e-12 for _, err in res), res
+
+
+@pytest.mark.parametrize("frames,world", [(0, 2), (1, 2), (7, 2), (8, 3), (5, 8)])
+def test_shard_frames_partition(frames, world):
+    spans = [clutils.shard_frames(frames, r, world) for r in range(world)]
+    assert spans[0][0] == 0 and spans[-1][1] == frames
+    assert all(a1 == b0 for (_, a1), (b0, _) in zip(spans, spans[1:]))
+    sizes = [b - a for a, b in spans]
+    assert max(sizes) - min(sizes) <= 1
+
+
+def _stack_rank(rank, world, port, out_q):
+    import torch.distributed as dist
+
+    import oracle
+    from sred_b200 import synth, utils
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        stack = np.stack([synth.normalize_input(synth.spot_image(36, 30, 4, seed=s)) for s in range(5)])
+        rb = utils.ReferenceBlock2D(stack[0, 10:13, 10:13].ravel()[[1, 3, 4, 5, 7]].copy(), 3, 3, 1, 1, 5,
+                                    np.float32(0.5), np.float32(0.2))
+        seen = []
+
+        def compute(sub):  # the oracle maps this rank's frames (no GPU here)
+            seen.append(sub.shape[0])
+            return np.stack([oracle.block_map("Pearson's R", f, rb.pixels, 3, 3, rb.mean, rb.std)["map"]
+                             for f in sub]) if sub.shape[0] else np.zeros_like(sub)
+
+        got = clutils.block_map_stack_sharded("Pearson's R", stack, rb, 0.0, True, rank, world, compute=compute)
+        exp = np.stack([oracle.block_map("Pearson's R", f, rb.pixels, 3, 3, rb.mean, rb.std)["map"] for f in stack])
+        f0, f1 = clutils.shard_frames(5, rank, world)
+        out_q.put((rank, seen == [f1 - f0], bool(np.array_equal(got.reshape(exp.shape), exp))))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_time_lapse_gloo_two_ranks():
+    """Frames split across two gloo ranks, each mapping its own (the oracle
+    standing in for the GPU), one all-gather: every rank holds the whole
+    stack's maps, equal to mapping all frames in one place."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_stack_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    res = sorted(q.get(timeout=5) for _ in range(2))
+    assert res == [(0, True, True), (1, True, True)], res
