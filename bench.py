@@ -388,7 +388,27 @@ def run_block(args, rank, local, world):
                          "note": "8 algorithmic bytes per pixel over the whole call (map kernel plus per-frame "
                                  "normalisation passes); the map kernel evaluates 149-element sums in the "
                                  "reference's sequential FP32 order, so it is issue-bound, not HBM-bound"}}
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = block_cpu_baseline(stack, ref)
     print(json.dumps(line), flush=True)
+
+
+def block_cpu_baseline(frames: np.ndarray, ref, budget_s: float = 10.0) -> dict:
+    """The reference's 2D block kernel (oracle/_ref, compiled for the CPU; the
+    oracle's FP32 port if not built) with the Java host steps, Pearson's R,
+    15x15, on whole 1024x1024 frames until about budget_s, on all host cores."""
+    import oracle
+    kind = "reference" if oracle.refshim() is not None else "port"
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    n, t0 = 0, time.perf_counter()
+    while n < frames.shape[0] and (n == 0 or time.perf_counter() - t0 < budget_s):
+        oracle.block_map("Pearson's R", frames[n], ref.pixels, ref.width, ref.height, ref.mean, ref.std, 0.0, True,
+                         use_refshim=(kind == "reference"))
+        n += 1
+    dt = time.perf_counter() - t0
+    px = n * frames.shape[1] * frames.shape[2]
+    return {"value": px / dt, "unit": "pixels/s", "cores": cores, "kind": kind,
+            "sample": f"Pearson's R on {n} whole 1024x1024 frame(s) ({dt:.1f} s): kernel and host steps"}
 
 
 def volume_cpu_baseline(vol: np.ndarray, ref, bw: int, budget_s: float = 12.0) -> dict:
