@@ -70,7 +70,8 @@ __global__ void k_hu_pairs(const float* feat, const float* sig, int n, int W, in
 __global__ void k_phase_dft(const float* img, const float* means, const float* stds, int W, int bw, int bh, int nx,
                             int n, double* fr, double* fi);
 __global__ void k_gather_interior(const float* a, int W, int rw, int rh, int nx, int n, float* out);
-__global__ void k_phase_pairs(const double* fr, const double* fi, const float* sig, int n, int bw, int bh, int W,
-                              int nx, float* out);
+// The all-pairs phase map (shape.cu): one CTA per reference block, on stream st.
+void launch_phase_pairs(const double* fr, const double* fi, const float* sig, int n, int bw, int bh, int W, int nx,
+                        float* out, cudaStream_t st);
 
 }  // namespace sred

@@ -196,46 +196,6 @@ __global__ void __launch_bounds__(128)
   phase_dft(xg, bw, bh, cw, sw, ch, sh, fr + (size_t)q * nn, fi + (size_t)q * nn, work + kPhaseMaxN);
 }
 
-// :73-163: one CTA per reference block p, threads over comparison blocks q;
-// phase_map[p] = sum_q |peak_pq| * weight(sigma_p, sigma_q), summed in FP64 in
-// a fixed order.
-__global__ void __launch_bounds__(128)
-    k_phase_pairs(const double* __restrict__ fr, const double* __restrict__ fi, const float* __restrict__ sig,
-                  int n, int bw, int bh, int W, int nx, float* __restrict__ out) {
-  __shared__ double tw[4 * kPhaseMaxN];
-  __shared__ double pr[kPhaseMaxN], pi[kPhaseMaxN];
-  __shared__ double red[128];
-  double *cw = tw, *sw = tw + bw * bw, *ch = sw + bw * bw, *sh = ch + bh * bh;
-  const int p = blockIdx.x, nn = bw * bh;
-  phase_twiddles_smem(bw, bh, cw, sw, ch, sh);
-  for (int k = threadIdx.x; k < nn; k += blockDim.x) {
-    pr[k] = fr[(size_t)p * nn + k];
-    pi[k] = fi[(size_t)p * nn + k];
-  }
-  __syncthreads();
-  const float sp = sig[p];
-  double acc = 0.0;
-  double work[2 * kPhaseMaxN + kPhaseTmp];  // [cross re | cross im | temporaries]
-  double *cr = work, *ci = work + kPhaseMaxN;
-  for (int q = threadIdx.x; q < n; q += blockDim.x) {
-    const double* qr = fr + (size_t)q * nn;
-    const double* qi = fi + (size_t)q * nn;
-    for (int k = 0; k < nn; k++) phase_cross(pr[k], pi[k], qr[k], qi[k], &cr[k], &ci[k]);
-    const float d = phase_peak(cr, ci, bw, bh, cw, sw, ch, sh, work + 2 * kPhaseMaxN);
-    acc += (double)d * (double)phase_weight(sp, sig[q]);
-  }
-  red[threadIdx.x] = acc;
-  __syncthreads();
-  for (int s = 64; s > 0; s >>= 1) {
-    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    const int rw = bw / 2, rh = bh / 2;
-    out[(size_t)(rh + p / nx) * W + rw + p % nx] = (float)red[0];
-  }
-}
-
 // Block-map form: the reference block's DFT against each block's. Blocks are
 // normalised with their FP32 local statistics (computed here, and written to
 // stds_out when it is given) and restricted to the ellipse (0 elsewhere on
@@ -260,6 +220,80 @@ struct PhaseShape {
   static constexpr int NG = 4 * P;       // groups per CTA
   static constexpr int PIX = NG * D;     // pixels per CTA
 };
+
+// Inverse DFT (real part) of the cross-power spectrum X held in a group's
+// buffers (X(j, i) at j * bw + i; overwritten) and its peak: each lane of the
+// group (t < D; t = D takes no line) holds one line in registers, as in the
+// forward transform, and every output keeps the sequential sum of
+// phase_peak. Returns, in the group's lane t = 0, the raster index of the
+// largest value above 0 (lowest index on ties), -1 if none. All 32 lanes of
+// the warp call it together; lr and li are the caller's line registers.
+template <int D>
+__device__ __forceinline__ int phase_group_peak(double* re, double* im, const double* cw, const double* sw,
+                                                const double* ch, const double* sh, int bw, int bh, double sn,
+                                                int t, double (&lr)[D], double (&li)[D]) {
+  const unsigned full = 0xffffffffu;
+  // inverse, rows: lane jj holds X(jj, :); S(i, jj) = sum_ii X[jj][ii] e^{+i a(i, ii)}
+  if (t < bh) {
+#pragma unroll
+    for (int ii = 0; ii < D; ii++) {
+      lr[ii] = ii < bw ? re[t * bw + ii] : 0.0;
+      li[ii] = ii < bw ? im[t * bw + ii] : 0.0;
+    }
+  }
+  __syncwarp();
+  if (t < bh) {
+    for (int i = 0; i < bw; i++) {
+      double sr = 0.0, si = 0.0;
+#pragma unroll
+      for (int ii = 0; ii < D; ii++) {
+        if (ii < bw) {
+          const double c = cw[i * bw + ii], s = sw[i * bw + ii];
+          sr += lr[ii] * c - li[ii] * s;
+          si += lr[ii] * s + li[ii] * c;
+        }
+      }
+      re[i * bh + t] = sr;
+      im[i * bh + t] = si;
+    }
+  }
+  __syncwarp();
+  // inverse, columns (real part): lane i holds S(i, :);
+  // v(j, i) = sum_jj Re(S(i, jj) e^{+i b(j, jj)}) / sn, and the lane's peak
+  double best = 0.0;
+  int bidx = -1;
+  if (t < bw) {
+#pragma unroll
+    for (int jj = 0; jj < D; jj++) {
+      lr[jj] = jj < bh ? re[t * bh + jj] : 0.0;
+      li[jj] = jj < bh ? im[t * bh + jj] : 0.0;
+    }
+    for (int j = 0; j < bh; j++) {
+      double v = 0.0;
+#pragma unroll
+      for (int jj = 0; jj < D; jj++)
+        if (jj < bh) v += lr[jj] * ch[j * bh + jj] - li[jj] * sh[j * bh + jj];
+      v /= sn;
+      const int k = j * bw + t;
+      if (v > best || (bidx >= 0 && v == best && k < bidx)) {
+        best = v;
+        bidx = k;
+      }
+    }
+  }
+  // the group's peak (lane t gathers lanes t .. t + 2o - 1 of the group):
+  // largest value above 0, lowest raster index on ties
+#pragma unroll
+  for (int o = 1; o < D; o <<= 1) {
+    const double ob = __shfl_down_sync(full, best, o);
+    const int oi = __shfl_down_sync(full, bidx, o);
+    if (t + o < D && oi >= 0 && (bidx < 0 || ob > best || (ob == best && oi < bidx))) {
+      best = ob;
+      bidx = oi;
+    }
+  }
+  return bidx;
+}
 
 // (five CTAs per SM for the two largest sizes: 9.5 instead of 10.1 ms per
 // 1024 x 1024 frame at 15 x 15; the smaller sizes run best unconstrained)
@@ -388,65 +422,7 @@ __global__ void __launch_bounds__(128, D >= 13 ? 5 : 0)
       }
     }
     __syncwarp();
-    // inverse, rows: lane jj holds X(jj, :); S(i, jj) = sum_ii X[jj][ii] e^{+i a(i, ii)}
-    if (t < bh) {
-#pragma unroll
-      for (int ii = 0; ii < D; ii++) {
-        lr[ii] = ii < bw ? re[t * bw + ii] : 0.0;
-        li[ii] = ii < bw ? im[t * bw + ii] : 0.0;
-      }
-    }
-    __syncwarp();
-    if (t < bh) {
-      for (int i = 0; i < bw; i++) {
-        double sr = 0.0, si = 0.0;
-#pragma unroll
-        for (int ii = 0; ii < D; ii++) {
-          if (ii < bw) {
-            const double c = cw[i * bw + ii], s = sw[i * bw + ii];
-            sr += lr[ii] * c - li[ii] * s;
-            si += lr[ii] * s + li[ii] * c;
-          }
-        }
-        re[i * bh + t] = sr;
-        im[i * bh + t] = si;
-      }
-    }
-    __syncwarp();
-    // inverse, columns (real part): lane i holds S(i, :);
-    // v(j, i) = sum_jj Re(S(i, jj) e^{+i b(j, jj)}) / sn, and the lane's peak
-    double best = 0.0;
-    int bidx = -1;
-    if (t < bw) {
-#pragma unroll
-      for (int jj = 0; jj < D; jj++) {
-        lr[jj] = jj < bh ? re[t * bh + jj] : 0.0;
-        li[jj] = jj < bh ? im[t * bh + jj] : 0.0;
-      }
-      for (int j = 0; j < bh; j++) {
-        double v = 0.0;
-#pragma unroll
-        for (int jj = 0; jj < D; jj++)
-          if (jj < bh) v += lr[jj] * ch[j * bh + jj] - li[jj] * sh[j * bh + jj];
-        v /= sn;
-        const int k = j * bw + t;
-        if (v > best || (bidx >= 0 && v == best && k < bidx)) {
-          best = v;
-          bidx = k;
-        }
-      }
-    }
-    // the group's peak (lane t gathers lanes t .. t + 2o - 1 of the group):
-    // largest value above 0, lowest raster index on ties
-#pragma unroll
-    for (int o = 1; o < D; o <<= 1) {
-      const double ob = __shfl_down_sync(full, best, o);
-      const int oi = __shfl_down_sync(full, bidx, o);
-      if (t + o < D && oi >= 0 && (bidx < 0 || ob > best || (ob == best && oi < bidx))) {
-        best = ob;
-        bidx = oi;
-      }
-    }
+    const int bidx = phase_group_peak<D>(re, im, cw, sw, ch, sh, bw, bh, sn, t, lr, li);
     if (t == 0 && idx < plane) {
       float r = 0.0f;
       if (act && bidx >= 0) {
@@ -483,6 +459,96 @@ void launch_block_phase(const float* img, int W, int H, int frames, const Ellips
     launch_block_phase_t<13>(img, W, H, frames, e, bw, bh, ref, out, stds_out, st);
   else
     launch_block_phase_t<15>(img, W, H, frames, e, bw, bh, ref, out, stds_out, st);
+}
+
+// :73-163: one CTA per reference block p; phase_map[p] = sum_q |peak_pq| *
+// weight(sigma_p, sigma_q). The CTA's groups of D lanes (PhaseShape) take the
+// comparison blocks q in turn: the cross-power spectrum of the two stored DFTs
+// spread over the group's lanes, then phase_group_peak. Each group sums its
+// pairs in FP64 in q order, and the CTA adds the groups' sums in group order.
+template <int D>
+__global__ void __launch_bounds__(128)
+    k_phase_pairs(const double* __restrict__ fr, const double* __restrict__ fi, const float* __restrict__ sig,
+                  int n, int bw, int bh, int W, int nx, float* __restrict__ out) {
+  using S = PhaseShape<D>;
+  __shared__ double tw[4 * D * D];
+  __shared__ double pr[D * D], pi[D * D];
+  __shared__ double buf[S::NG][2 * D * D];
+  __shared__ double red[S::NG];
+  double *cw = tw, *sw = tw + bw * bw, *ch = sw + bw * bw, *sh = ch + bh * bh;
+  const int p = blockIdx.x, nn = bw * bh;
+  phase_twiddles_smem(bw, bh, cw, sw, ch, sh);
+  for (int k = threadIdx.x; k < nn; k += blockDim.x) {
+    pr[k] = fr[(size_t)p * nn + k];
+    pi[k] = fi[(size_t)p * nn + k];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool live = lane < S::P * D;  // lanes past the warp's last group take no line
+  const int gw = live ? lane / D : 0;
+  const int t = live ? lane - gw * D : D;
+  const int g = warp * S::P + gw;
+  double* re = buf[g];
+  double* im = re + D * D;
+  const float sp = sig[p];
+  const double sn = sqrt((double)(bw * bh));
+  double acc = 0.0;  // the group's sum, in its lane t = 0
+  // every group of a warp runs the same rounds, so the warp stays converged
+  const int rounds = (n + S::NG - 1) / S::NG;
+  for (int r = 0; r < rounds; r++) {
+    const int q = r * S::NG + g;
+    const bool act = live && q < n;
+    if (act) {
+      const double* qr = fr + (size_t)q * nn;
+      const double* qi = fi + (size_t)q * nn;
+      for (int k = t; k < nn; k += D) phase_cross(pr[k], pi[k], qr[k], qi[k], &re[k], &im[k]);
+    }
+    __syncwarp();
+    double lr[D], li[D];
+    const int bidx = phase_group_peak<D>(re, im, cw, sw, ch, sh, bw, bh, sn, act ? t : D, lr, li);
+    if (act && t == 0) {
+      float d = 0.0f;
+      if (bidx >= 0) {
+        const double px = (double)(bidx % bw + 1), py = (double)(bidx / bw + 1);
+        d = (float)sqrt((px * px) + (py * py));
+      }
+      acc += (double)d * (double)phase_weight(sp, sig[q]);
+    }
+    __syncwarp();
+  }
+  if (live && t == 0) red[g] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sum = 0.0;
+    for (int i = 0; i < S::NG; i++) sum += red[i];
+    const int rw = bw / 2, rh = bh / 2;
+    out[(size_t)(rh + p / nx) * W + rw + p % nx] = (float)sum;
+  }
+}
+
+template <int D>
+void launch_phase_pairs_t(const double* fr, const double* fi, const float* sig, int n, int bw, int bh, int W, int nx,
+                          float* out, cudaStream_t st) {
+  k_phase_pairs<D><<<n, 128, 0, st>>>(fr, fi, sig, n, bw, bh, W, nx, out);
+}
+
+void launch_phase_pairs(const double* fr, const double* fi, const float* sig, int n, int bw, int bh, int W, int nx,
+                        float* out, cudaStream_t st) {
+  const int d = bw > bh ? bw : bh;
+  if (d <= 3)
+    launch_phase_pairs_t<3>(fr, fi, sig, n, bw, bh, W, nx, out, st);
+  else if (d <= 5)
+    launch_phase_pairs_t<5>(fr, fi, sig, n, bw, bh, W, nx, out, st);
+  else if (d <= 7)
+    launch_phase_pairs_t<7>(fr, fi, sig, n, bw, bh, W, nx, out, st);
+  else if (d <= 9)
+    launch_phase_pairs_t<9>(fr, fi, sig, n, bw, bh, W, nx, out, st);
+  else if (d <= 11)
+    launch_phase_pairs_t<11>(fr, fi, sig, n, bw, bh, W, nx, out, st);
+  else if (d <= 13)
+    launch_phase_pairs_t<13>(fr, fi, sig, n, bw, bh, W, nx, out, st);
+  else
+    launch_phase_pairs_t<15>(fr, fi, sig, n, bw, bh, W, nx, out, st);
 }
 
 // Values of `a` at the interior pixels, in interior raster order.

@@ -2041,7 +2041,7 @@ sred_status sred_phase_correlation_map_2d(sred_ctx* c, const float* img, const f
   CKS(ensure(c, B_FI, (size_t)ni * nn, &d_fi));
   k_phase_dft<<<(ni + 127) / 128, 128, 0, st>>>(d_img, d_m, d_s, w, bw, bh, nx, ni, d_fr, d_fi);
   k_gather_interior<<<(ni + 255) / 256, 256, 0, st>>>(d_s, w, e.rw, e.rh, nx, ni, d_sig);
-  k_phase_pairs<<<ni, 128, 0, st>>>(d_fr, d_fi, d_sig, ni, bw, bh, w, nx, d_out);
+  launch_phase_pairs(d_fr, d_fi, d_sig, ni, bw, bh, w, nx, d_out, st);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
