@@ -194,6 +194,42 @@ __device__ __forceinline__ void pearson_pair2(F2 G, F2 aq, F2 rq, const PearsonR
   sd = add2(sd, w);
 }
 
+// Row constants of the packed SSIM path, both halves equal.
+struct SsimRow2 {
+  F2 a, mu2x2, sig2x, mumu, s2, c1, c2;
+};
+
+__device__ __forceinline__ SsimRow2 make_ssim_row2(const RowState& rs, const EpiConsts& ec) {
+  SsimRow2 r;
+  r.a = f2(rs.a, rs.a);
+  r.mu2x2 = f2(rs.mu2x2, rs.mu2x2);
+  r.sig2x = f2(rs.sig2x, rs.sig2x);
+  r.mumu = f2(rs.mumu, rs.mumu);
+  r.s2 = f2(rs.s2, rs.s2);
+  r.c1 = f2(ec.c1, ec.c1);
+  r.c2 = f2(ec.c2, ec.c2);
+  return r;
+}
+
+// Two SSIM pairs (columns q0, q1 of one row): pair_terms' kSsim arithmetic,
+// operation for operation, on f32x2 pairs (the quotient and the weight per
+// half), accumulated into packed sums.
+__device__ __forceinline__ void ssim_pair2(F2 G, F2 aq, F2 sq, F2 mq, const SsimRow2& r, F2& sn, F2& sd) {
+  const F2 d = sub2(r.a, aq);
+  float m0, m1;
+  f2_split(mul2(d, d), m0, m1);
+  const F2 w = f2(ex2_approx(-m0), ex2_approx(-m1));
+  const F2 num = mul2(fma2(r.mu2x2, mq, r.c1), fma2(mul2(r.sig2x, sq), G, r.c2));
+  const F2 den = mul2(fma2(r.mumu, mul2(mq, mq), r.c1), fma2(sq, sq, r.s2));
+  float n0, n1, d0, d1;
+  f2_split(num, n0, n1);
+  f2_split(den, d0, d1);
+  float t0, t1;
+  f2_split(mul2(f2(__fdividef(n0, d0), __fdividef(n1, d1)), w), t0, t1);
+  sn = add2(sn, f2(fmaxf(t0, 0.0f), fmaxf(t1, 0.0f)));
+  sd = add2(sd, w);
+}
+
 // Column sums of 16 columns over the 32 lanes of a warp (lane l holds row l's
 // terms x[0..15]): four butterfly exchanges halve the columns each lane keeps,
 // a fifth adds the lane pairs. Afterwards lanes 2c and 2c+1 both hold the sum

@@ -251,6 +251,44 @@ __device__ __forceinline__ void epi_chunk_pearson2(const uint32_t (&v)[16], cons
   }
 }
 
+// Packed SSIM path (full, off-diagonal tiles): 16 pairs as eight f32x2 pairs.
+__device__ __forceinline__ void epi_chunk_ssim2(const uint32_t (&v)[16], const float* __restrict__ soa, int c0,
+                                                const SsimRow2& r2, F2& sn, F2& sd) {
+#pragma unroll
+  for (int j = 0; j < 16; j += 4) {
+    const float4 a4 = *reinterpret_cast<const float4*>(soa + c0 + j);
+    const float4 s4 = *reinterpret_cast<const float4*>(soa + 2 * kBN + c0 + j);
+    const float4 m4 = *reinterpret_cast<const float4*>(soa + 3 * kBN + c0 + j);
+    ssim_pair2(f2(__uint_as_float(v[j]), __uint_as_float(v[j + 1])), f2(a4.x, a4.y), f2(s4.x, s4.y),
+               f2(m4.x, m4.y), r2, sn, sd);
+    ssim_pair2(f2(__uint_as_float(v[j + 2]), __uint_as_float(v[j + 3])), f2(a4.z, a4.w), f2(s4.z, s4.w),
+               f2(m4.z, m4.w), r2, sn, sd);
+  }
+}
+
+__device__ __forceinline__ void epi_tile_ssim2(uint32_t taddr, const float* __restrict__ soa, int cbase,
+                                               const SsimRow2& r2, float& sn_out, float& sd_out) {
+  uint32_t v0[16], v1[16];
+  F2 sn = f2(0.0f, 0.0f), sd = sn;
+  tmem_ld16(taddr, v0);
+  tmem_wait(v0);
+  tmem_ld16(taddr + 16, v1);
+  epi_chunk_ssim2(v0, soa, cbase, r2, sn, sd);
+  tmem_wait(v1);
+  tmem_ld16(taddr + 32, v0);
+  epi_chunk_ssim2(v1, soa, cbase + 16, r2, sn, sd);
+  tmem_wait(v0);
+  tmem_ld16(taddr + 48, v1);
+  epi_chunk_ssim2(v0, soa, cbase + 32, r2, sn, sd);
+  tmem_wait(v1);
+  epi_chunk_ssim2(v1, soa, cbase + 48, r2, sn, sd);
+  float a, b;
+  f2_split(sn, a, b);
+  sn_out += a + b;
+  f2_split(sd, a, b);
+  sd_out += a + b;
+}
+
 template <int CMODE>
 __device__ __forceinline__ void epi_tile_pearson2(uint32_t taddr, const float* __restrict__ soa, int cbase,
                                                   const PearsonRow2& r2, float& sn_out, float& sd_out) {
@@ -502,6 +540,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int row = rb * kBM + quarter * 32 + lane;
       const RowState rs = make_row(g.params[row], g.ec);
       const PearsonRow2 r2 = make_pearson_row2(rs);
+      const SsimRow2 s2 = make_ssim_row2(rs, g.ec);
       const float rmax_r = g.tile_rmax[rb];
       double acc_n = 0.0, acc_d = 0.0;
       for (int ct = ct0; ok && ct < ct1; ct++, tile++) {
@@ -524,6 +563,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           epi_tile_pearson2<kCFirst>(taddr, soa, cbase, r2, sn, sd);
         else if (METRIC == kPearson && full && !diag && cm == kCSecond)
           epi_tile_pearson2<kCSecond>(taddr, soa, cbase, r2, sn, sd);
+        else if (METRIC == kSsim && full && !diag)
+          epi_tile_ssim2(taddr, soa, cbase, s2, sn, sd);
         else if (full && !diag && cm == kCFirst)
           epi_tile<METRIC, kCFirst, true, false>(taddr, soa, cbase, col0, row, rs, g.ec, sn, sd);
         else if (full && !diag && cm == kCSecond)
