@@ -322,6 +322,8 @@ def block_map_stack(metric: str, stack: np.ndarray, reference_block: ReferenceBl
     frames, h, w = a.shape
     if out is None:
         out = np.empty_like(a)
+    elif out.dtype != np.float32 or not out.flags.c_contiguous or out.size != a.size:
+        raise ValueError("out must be a C-contiguous float32 array of frames * h * w elements")
     res = out.reshape(frames, h, w)
     st = c._L.sred_block_map_2d_stack(
         c.h, metric.encode(), a.reshape(-1), w, h, frames,
