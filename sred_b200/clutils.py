@@ -201,6 +201,13 @@ def global_map_device(metric: str, d_img_ptr: int, width: int, height: int, bloc
     return info.as_dict()
 
 
+def _out_buffer(out, n: int, what: str) -> np.ndarray:
+    """A caller's output buffer, flat, if the library can write it in place."""
+    if out.dtype != np.float32 or not out.flags.c_contiguous or out.size != n:
+        raise ValueError(f"out must be a C-contiguous float32 array of {what}")
+    return out.reshape(-1)
+
+
 def global_map_host(metric: str, img: np.ndarray, block_width: int, block_height: int, relevance_constant: float,
                     normalize_output: bool = True, out: np.ndarray | None = None, ctx=None) -> tuple:
     """The whole global-map command on host buffers (sred_global_map_2d):
@@ -210,6 +217,8 @@ def global_map_host(metric: str, img: np.ndarray, block_width: int, block_height
     h, w = a.shape
     if out is None:
         out = np.empty((h, w), np.float32)
+    else:
+        _out_buffer(out, h * w, "h * w elements")
     info = _lib.RunInfo()
     c.check(c._L.sred_global_map_2d(c.h, metric.encode(), C.c_void_p(a.ctypes.data), w, h, block_width,
                                     block_height, float(relevance_constant), int(bool(normalize_output)),
@@ -322,9 +331,7 @@ def block_map_stack(metric: str, stack: np.ndarray, reference_block: ReferenceBl
     frames, h, w = a.shape
     if out is None:
         out = np.empty_like(a)
-    elif out.dtype != np.float32 or not out.flags.c_contiguous or out.size != a.size:
-        raise ValueError("out must be a C-contiguous float32 array of frames * h * w elements")
-    res = out.reshape(frames, h, w)
+    res = _out_buffer(out, a.size, "frames * h * w elements").reshape(frames, h, w)
     st = c._L.sred_block_map_2d_stack(
         c.h, metric.encode(), a.reshape(-1), w, h, frames,
         np.ascontiguousarray(reference_block.pixels, np.float32).ravel(), int(reference_block.size),
@@ -407,7 +414,8 @@ def calculate_block_repetition_map_3d(metric: str, input_image: InputImage3D, re
     if metric not in BLOCK_METRICS_3D:
         return None
     c = _ctx(ctx)
-    out = np.zeros(input_image.size, np.float32) if out is None else out.reshape(-1)
+    out = np.zeros(input_image.size, np.float32) if out is None else _out_buffer(out, input_image.size,
+                                                                                  "the volume's size")
     rb = reference_block
     c.check(c._L.sred_calculate_block_repetition_map_3d(
         c.h, metric.encode(), np.ascontiguousarray(input_image.image_array, np.float32).ravel(), input_image.width,
@@ -454,7 +462,8 @@ def calculate_global_repetition_map_3d(metric: str, input_image: InputImage3D, b
     if metric not in GLOBAL_METRICS:
         return None
     c = _ctx(ctx)
-    out = np.zeros(input_image.size, np.float32) if out is None else out.reshape(-1)
+    out = np.zeros(input_image.size, np.float32) if out is None else _out_buffer(out, input_image.size,
+                                                                                  "the volume's size")
     info = _lib.RunInfo()
     c.check(c._L.sred_calculate_global_repetition_map_3d(
         c.h, metric.encode(), np.ascontiguousarray(input_image.image_array, np.float32).ravel(), input_image.width,

@@ -36,3 +36,15 @@ def test_roi_offset_and_sigma_matches_the_java_loop():
     flat = np.full((8, 8), 0.1, np.float32)
     got, exp = plugins.roi_offset_and_sigma(flat, (0, 0, 8, 8)), _java_mean_std(flat, 0, 0, 8, 8)
     assert got[0] == exp[0] and (got[1] == exp[1] or (math.isnan(got[1]) and math.isnan(exp[1])))
+
+
+def test_output_buffers_are_checked_before_any_call():
+    """The host-buffer entry points refuse an `out` they could not fill in
+    place (wrong dtype, strided, wrong size) before touching the library."""
+    import pytest
+    from sred_b200 import clutils
+    good = np.zeros((4, 5), np.float32)
+    assert clutils._out_buffer(good, 20, "x").base is good
+    for bad in (np.zeros((4, 5), np.float64), np.zeros((4, 10), np.float32)[:, ::2], np.zeros(21, np.float32)):
+        with pytest.raises(ValueError):
+            clutils._out_buffer(bad, 20, "x")
