@@ -209,9 +209,11 @@ __global__ void __launch_bounds__(128)
 // walks the outputs, so the twiddles are the only operands it loads, and
 // every lane of the warp loads the same one (a broadcast). Between stages the
 // lines go through the group's two shared buffers (real, imaginary).
-// Every output is the same sequential sum as in phase_dft / phase_peak, and
-// the peak search keeps their rule (largest value above 0, lowest raster
-// index on ties), so the map equals the one-thread-per-pixel evaluation.
+// Every output is the same sequential sum as in phase_dft (forward) and in the
+// kernel's inverse DFT (:132-142: rows over ii, then columns over jj), and the
+// peak search keeps the kernel's rule (:144-157: the largest value above 0,
+// the lowest raster index on ties), so the map equals the one-thread-per-pixel
+// evaluation of the oracle.
 // Pixels outside the interior (and past the plane) run on a zero patch and
 // are written as 0, so the warp stays converged for its shuffles.
 template <int D>
@@ -224,8 +226,9 @@ struct PhaseShape {
 // Inverse DFT (real part) of the cross-power spectrum X held in a group's
 // buffers (X(j, i) at j * bw + i; overwritten) and its peak: each lane of the
 // group (t < D; t = D takes no line) holds one line in registers, as in the
-// forward transform, and every output keeps the sequential sum of
-// phase_peak. Returns, in the group's lane t = 0, the raster index of the
+// forward transform, and every output keeps the kernel's sequential sums
+// (:132-142: S(i, jj) over ii, then v(j, i) over jj, divided by sqrt(bw bh)).
+// Returns, in the group's lane t = 0, the raster index of the
 // largest value above 0 (lowest index on ties), -1 if none. All 32 lanes of
 // the warp call it together; lr and li are the caller's line registers.
 template <int D>

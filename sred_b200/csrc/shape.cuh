@@ -13,12 +13,13 @@
 // third with those three defects repaired (no unique-coordinate pre-filter,
 // real-valued phases, block-width indexing).
 //
-// Per-thread work arrays of the all-pairs phase kernels live in ONE local
-// array per thread, carved into sections by offset. With separate local
-// arrays, a one-thread-per-pixel block-map phase kernel built by nvcc 12.9 for
-// sm_100a computed DFTs whose first row read overwritten inputs, as if
-// phase_dft's column temporaries shared the input patch's stack slots; with
-// one array per thread the results were exact.
+// The per-thread work arrays of k_phase_dft live in ONE local array per
+// thread, carved into sections by offset. With separate local arrays, a
+// one-thread-per-pixel block-map phase kernel built by nvcc 12.9 for sm_100a
+// computed DFTs whose first row read overwritten inputs, as if phase_dft's
+// column temporaries shared the input patch's stack slots; with one array per
+// thread the results were exact. (The block-map and all-pairs kernels now
+// keep their lines in registers and shared memory.)
 #pragma once
 #include <math.h>
 
@@ -28,7 +29,7 @@ namespace sred {
 
 constexpr int kPhaseMaxDim = 15;                    // phase correlation: bw, bh <= 15
 constexpr int kPhaseMaxN = kPhaseMaxDim * kPhaseMaxDim;
-constexpr int kPhaseTmp = 2 * kPhaseMaxDim;         // temporaries of phase_dft / phase_peak
+constexpr int kPhaseTmp = 2 * kPhaseMaxDim;         // temporaries of phase_dft
 // The kernel's pi is a float literal widened to double (:44).
 constexpr double kPhasePi = (double)3.14159265358979323846f;
 constexpr float kLog2Hundred = 6.64385618977472469574f;  // log2(100)
@@ -95,47 +96,6 @@ __host__ __device__ inline void phase_cross(double rr, double ri, double qr, dou
   const double ar = fabs(mr), ai = fabs(mi);
   *xr = ((mr * ar) + (mi * ai)) / ((ar * ar) + (ai * ai) + (double)kEps);
   *xi = ((mi * ar) - (mr * ai)) / ((ar * ar) + (ai * ai) + (double)kEps);
-}
-
-// Inverse DFT (real part, :132-142) of the cross-power spectrum and peak
-// search (:144-157): the first strict maximum above 0 in raster order, at
-// 1-based coordinates (x, y); returns (float)sqrt(x^2 + y^2), 0 when no value
-// is positive. Evaluated separably one output column at a time; ties keep
-// the lowest raster index, which is what the raster scan keeps.
-// tmp: kPhaseTmp doubles, disjoint from cr and ci.
-__host__ __device__ inline float phase_peak(const double* cr, const double* ci, int bw, int bh, const double* cw,
-                                            const double* sw, const double* ch, const double* sh, double* tmp) {
-  const double sn = sqrt((double)(bw * bh));
-  double* sr = tmp;
-  double* si = tmp + kPhaseMaxDim;
-  double best = 0.0;
-  int bidx = -1;
-  for (int i = 0; i < bw; i++) {
-    for (int jj = 0; jj < bh; jj++) {
-      double ar = 0.0, ai = 0.0;
-      for (int ii = 0; ii < bw; ii++) {
-        const double c = cw[i * bw + ii], s = sw[i * bw + ii];
-        const double xr = cr[jj * bw + ii], xi = ci[jj * bw + ii];
-        ar += xr * c - xi * s;
-        ai += xr * s + xi * c;
-      }
-      sr[jj] = ar;
-      si[jj] = ai;
-    }
-    for (int j = 0; j < bh; j++) {
-      double v = 0.0;
-      for (int jj = 0; jj < bh; jj++) v += sr[jj] * ch[j * bh + jj] - si[jj] * sh[j * bh + jj];
-      v /= sn;
-      const int idx = j * bw + i;
-      if (v > best || (bidx >= 0 && v == best && idx < bidx)) {
-        best = v;
-        bidx = idx;
-      }
-    }
-  }
-  if (bidx < 0) return 0.0f;
-  const double x = (double)(bidx % bw + 1), y = (double)(bidx / bw + 1);
-  return (float)sqrt((x * x) + (y * y));
 }
 
 // getExpDecayWeight of kernelGetPhaseCorrelationMap.cl:167-179.
