@@ -336,6 +336,8 @@ def run_block(args, rank, local, world):
     d_out = torch.empty_like(d_in)
     stream = torch.cuda.Stream()
     res = {}
+    clocks = Clocks(local)
+    clocks.__enter__()
     for metric in BLOCK_METRICS:
         nf = min(frames, SHAPE_FRAMES) if metric in ("Hu moments", "Phase correlation") else frames
         for _ in range(args.warmup):
@@ -353,6 +355,7 @@ def run_block(args, rank, local, world):
         px = 1024 * 1024 * nf * world
         res[metric] = {"frames": nf, "ms_per_step": ms, "ms_per_frame": ms / nf, "pixels_per_s": px / (ms / 1e3),
                        "gbs_8B_per_pixel": 8 * px / (ms / 1e3) / 1e9}
+    clocks.__exit__(None, None, None)
     # end to end: host stack in, host maps out, through the public call (page-locked host buffers, as a
     # caller streaming time-lapses would hold); pipelined in chunks, and as one chunk (copies not overlapped)
     h_in = torch.from_numpy(stack).pin_memory()
@@ -383,6 +386,9 @@ def run_block(args, rank, local, world):
                     "h2d_bytes_per_step": int(stack.nbytes), "d2h_bytes_per_step": int(stack.nbytes),
                     "ms_per_step": e2e["pipelined"], "ms_per_step_one_chunk": e2e["one_chunk"],
                     "call": "clutils.block_map_stack (sred_block_map_2d_stack), Pearson's R, page-locked buffers"},
+            "clocks": clocks.summary(),
+            # per Pearson call: map, min-max initialisation, min-max, remap
+            "gpu_launches": 4 * args.steps,
             "roofline": {"bound": "hbm", "achieved": p["gbs_8B_per_pixel"], "peak": pk["hbm_gbs"], "unit": "GB/s",
                          "frac": p["gbs_8B_per_pixel"] / pk["hbm_gbs"], "traffic": None,
                          "note": "8 algorithmic bytes per pixel over the whole call (map kernel plus per-frame "
