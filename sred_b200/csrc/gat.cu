@@ -34,7 +34,9 @@ __global__ void k_gat(float* __restrict__ img, size_t n, double gain, double c) 
 // One block of the objective (GATMinimizer2D.userFunction): the pixels
 // transformed as applyGAT does (v <= -c / gain -> 0), stored as float, then
 // sum v and sum v*v (the product in float, as Java multiplies two floats) in
-// double. One CTA per block; out[2 b] = sum, out[2 b + 1] = sum of squares.
+// double. Block b's pixels are split into gridDim.y equal runs, one CTA per
+// run (so a grid of few blocks still fills the GPU); out[2 (b S + s)] = the
+// run's sum, out[2 (b S + s) + 1] = its sum of squares, S = gridDim.y.
 __global__ void __launch_bounds__(256)
     k_gat_block_moments(const float* __restrict__ img, int W, int bw, int bh, int nbx, double gain, double c,
                         double* __restrict__ out) {
@@ -42,8 +44,10 @@ __global__ void __launch_bounds__(256)
   const int b = blockIdx.x, bx = b % nbx, by = b / nbx;
   const int x0 = bx * bw, y0 = by * bh;
   const double lim = -c / gain, scale = 2.0 / gain;
+  const int n = bw * bh, run = (n + gridDim.y - 1) / gridDim.y;
+  const int t0 = blockIdx.y * run, t1 = min(n, t0 + run);
   double a1 = 0.0, a2 = 0.0;
-  for (int t = threadIdx.x; t < bw * bh; t += blockDim.x) {
+  for (int t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
     const int x = x0 + t % bw, y = y0 + t / bw;
     double v = (double)img[(size_t)y * W + x];
     v = (v <= lim) ? 0.0 : scale * sqrt(gain * v + c);
@@ -62,16 +66,17 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    out[2 * b] = s1[0];
-    out[2 * b + 1] = s2[0];
+    const size_t o = 2 * ((size_t)b * gridDim.y + blockIdx.y);
+    out[o] = s1[0];
+    out[o + 1] = s2[0];
   }
 }
 
 // One block of GATMinimizer3D.userFunction's grid: the voxels transformed as
 // applyGAT does (stored as float), then sum v and sum v*v in double (the
 // product of the widened value, as java/Utils.java getMeanAndVarBlock3D
-// computes it). One CTA per block; out[2 b] = sum, out[2 b + 1] = sum of
-// squares.
+// computes it). Runs of a block per CTA and the output layout as in
+// k_gat_block_moments.
 __global__ void __launch_bounds__(256)
     k_gat_block_moments3d(const float* __restrict__ vol, int W, int H, int bw, int bh, int bd, int nbx, int nby,
                           double gain, double c, double* __restrict__ out) {
@@ -79,9 +84,10 @@ __global__ void __launch_bounds__(256)
   const int b = blockIdx.x, bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
   const size_t x0 = (size_t)bx * bw, y0 = (size_t)by * bh, z0 = (size_t)bz * bd;
   const double lim = -c / gain, scale = 2.0 / gain;
-  const size_t n = (size_t)bw * bh * bd;
+  const size_t n = (size_t)bw * bh * bd, run = (n + gridDim.y - 1) / gridDim.y;
+  const size_t t0 = blockIdx.y * run, t1 = n < t0 + run ? n : t0 + run;
   double a1 = 0.0, a2 = 0.0;
-  for (size_t t = threadIdx.x; t < n; t += blockDim.x) {
+  for (size_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
     const size_t x = x0 + t % bw, y = y0 + (t / bw) % bh, z = z0 + t / ((size_t)bw * bh);
     double v = (double)vol[(z * H + y) * W + x];
     v = (v <= lim) ? 0.0 : scale * sqrt(gain * v + c);
@@ -100,8 +106,9 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    out[2 * b] = s1[0];
-    out[2 * b + 1] = s2[0];
+    const size_t o = 2 * ((size_t)b * gridDim.y + blockIdx.y);
+    out[o] = s1[0];
+    out[o + 1] = s2[0];
   }
 }
 

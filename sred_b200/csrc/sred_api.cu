@@ -2056,19 +2056,42 @@ namespace {
 
 // The objective of GATMinimizer2D for one parameter set, the image already on
 // the device.
+// Runs per block of the objective's moments kernels: enough CTAs for about
+// four per SM, each run at least 1,024 elements, at most 64 runs.
+int gat_runs(const sred_ctx* c, size_t nb, size_t per_block) {
+  size_t r = (4 * (size_t)c->num_sms + nb - 1) / std::max<size_t>(nb, 1);
+  r = std::min<size_t>(r, std::max<size_t>(1, per_block / 1024));
+  return (int)std::max<size_t>(1, std::min<size_t>(r, 64));
+}
+
+// The per-block [sum, sum of squares] from the runs' partial sums, added in
+// run order in FP64 on the host.
+sred_status gat_block_sums(sred_ctx* c, const double* d_part, size_t nb, int runs, std::vector<double>* sums) {
+  std::vector<double> part(2 * nb * runs);
+  CK(cudaMemcpyAsync(part.data(), d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  sums->assign(2 * nb, 0.0);
+  for (size_t b = 0; b < nb; b++)
+    for (int s = 0; s < runs; s++) {
+      (*sums)[2 * b] += part[2 * (b * runs + s)];
+      (*sums)[2 * b + 1] += part[2 * (b * runs + s) + 1];
+    }
+  return SRED_OK;
+}
+
 sred_status gat_objective_dev(sred_ctx* c, const float* d_img, int w, int h, double gain, double sigma,
                               double offset, double* error) {
   int bw, bh, nbx, nby;
   if (!gat_grid(w, h, &bw, &bh, &nbx, &nby)) return fail(c, SRED_ERR_ARG, "image too small for the GAT fit (width and height >= 12)");
   const int nb = nbx * nby;
+  const int runs = gat_runs(c, (size_t)nb, (size_t)bw * bh);
   double* d_sums;
-  CKS(ensure(c, B_GAT, 2 * (size_t)nb, &d_sums));
+  CKS(ensure(c, B_GAT, 2 * (size_t)nb * runs, &d_sums));
   const double cst = (3.0 / 8.0) * gain * gain + sigma * sigma - gain * offset;
-  k_gat_block_moments<<<nb, 256, 0, c->stream>>>(d_img, w, bw, bh, nbx, gain, cst, d_sums);
+  k_gat_block_moments<<<dim3(nb, runs), 256, 0, c->stream>>>(d_img, w, bw, bh, nbx, gain, cst, d_sums);
   CK(cudaGetLastError());
-  std::vector<double> sums(2 * (size_t)nb);
-  CK(cudaMemcpyAsync(sums.data(), d_sums, sums.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  std::vector<double> sums;
+  CKS(gat_block_sums(c, d_sums, (size_t)nb, runs, &sums));
   *error = gat_error(sums.data(), nb, bw, bh);
   return SRED_OK;
 }
@@ -2088,14 +2111,15 @@ sred_status gat_objective3d_dev(sred_ctx* c, const float* d_vol, int w, int h, i
   gat3d_grid(w, h, d, &bw, &bh, &bd, &nbx, &nby, &nbz);
   const size_t nb = (size_t)nbx * nby * nbz;
   if (nb == 0) return fail(c, SRED_ERR_ARG, "volume too small for the GAT fit");
+  const int runs = gat_runs(c, nb, (size_t)bw * bh * bd);
   double* d_sums;
-  CKS(ensure(c, B_GAT, 2 * nb, &d_sums));
+  CKS(ensure(c, B_GAT, 2 * nb * runs, &d_sums));
   const double cst = (3.0 / 8.0) * gain * gain + sigma * sigma - gain * offset;
-  k_gat_block_moments3d<<<(unsigned)nb, 256, 0, c->stream>>>(d_vol, w, h, bw, bh, bd, nbx, nby, gain, cst, d_sums);
+  k_gat_block_moments3d<<<dim3((unsigned)nb, runs), 256, 0, c->stream>>>(d_vol, w, h, bw, bh, bd, nbx, nby, gain,
+                                                                         cst, d_sums);
   CK(cudaGetLastError());
-  std::vector<double> sums(2 * nb);
-  CK(cudaMemcpyAsync(sums.data(), d_sums, sums.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  std::vector<double> sums;
+  CKS(gat_block_sums(c, d_sums, nb, runs, &sums));
   *error = gat_error(sums.data(), (int)nb, bw * bh * bd, 1);
   return SRED_OK;
 }
