@@ -35,12 +35,14 @@ __global__ void k_gat(float* __restrict__ img, size_t n, double gain, double c) 
 // transformed as applyGAT does (v <= -c / gain -> 0), stored as float, then
 // sum v and sum v*v (the product in float, as Java multiplies two floats) in
 // double. Block b's pixels are split into gridDim.y equal runs, one CTA per
-// run (so a grid of few blocks still fills the GPU); out[2 (b S + s)] = the
-// run's sum, out[2 (b S + s) + 1] = its sum of squares, S = gridDim.y.
+// run (so a grid of few blocks still fills the GPU), for each of gridDim.z
+// parameter points; out[2 ((p B + b) S + s)] = the run's sum, + 1 its sum of
+// squares (B = gridDim.x blocks, S = gridDim.y runs).
 __global__ void __launch_bounds__(256)
-    k_gat_block_moments(const float* __restrict__ img, int W, int bw, int bh, int nbx, double gain, double c,
+    k_gat_block_moments(const float* __restrict__ img, int W, int bw, int bh, int nbx, GatPoints pts,
                         double* __restrict__ out) {
   __shared__ double s1[256], s2[256];
+  const double gain = pts.gain[blockIdx.z], c = pts.c[blockIdx.z];
   const int b = blockIdx.x, bx = b % nbx, by = b / nbx;
   const int x0 = bx * bw, y0 = by * bh;
   const double lim = -c / gain, scale = 2.0 / gain;
@@ -66,7 +68,7 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    const size_t o = 2 * ((size_t)b * gridDim.y + blockIdx.y);
+    const size_t o = 2 * (((size_t)blockIdx.z * gridDim.x + b) * gridDim.y + blockIdx.y);
     out[o] = s1[0];
     out[o + 1] = s2[0];
   }
@@ -79,8 +81,9 @@ __global__ void __launch_bounds__(256)
 // k_gat_block_moments.
 __global__ void __launch_bounds__(256)
     k_gat_block_moments3d(const float* __restrict__ vol, int W, int H, int bw, int bh, int bd, int nbx, int nby,
-                          double gain, double c, double* __restrict__ out) {
+                          GatPoints pts, double* __restrict__ out) {
   __shared__ double s1[256], s2[256];
+  const double gain = pts.gain[blockIdx.z], c = pts.c[blockIdx.z];
   const int b = blockIdx.x, bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
   const size_t x0 = (size_t)bx * bw, y0 = (size_t)by * bh, z0 = (size_t)bz * bd;
   const double lim = -c / gain, scale = 2.0 / gain;
@@ -106,7 +109,7 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    const size_t o = 2 * ((size_t)b * gridDim.y + blockIdx.y);
+    const size_t o = 2 * (((size_t)blockIdx.z * gridDim.x + b) * gridDim.y + blockIdx.y);
     out[o] = s1[0];
     out[o + 1] = s2[0];
   }

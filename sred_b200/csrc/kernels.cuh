@@ -53,12 +53,17 @@ __global__ void k_invert_masked(float* a, const float* mask, int W, int H, int r
 
 // gat.cu
 __global__ void k_gat(float* img, size_t n, double gain, double c);
-__global__ void k_gat_block_moments(const float* img, int W, int bw, int bh, int nbx, double gain, double c,
-                                    double* out);
+// Parameter points of one launch of the GAT objective's moments kernels
+// (gain and c = 3/8 gain^2 + sigma^2 - gain offset per point).
+constexpr int kGatMaxPoints = 4;
+struct GatPoints {
+  double gain[kGatMaxPoints], c[kGatMaxPoints];
+};
+__global__ void k_gat_block_moments(const float* img, int W, int bw, int bh, int nbx, GatPoints pts, double* out);
 bool gat_grid(int w, int h, int* bw, int* bh, int* nbx, int* nby);
 double gat_error(const double* sums, int nblocks, int bw, int bh);
 __global__ void k_gat_block_moments3d(const float* vol, int W, int H, int bw, int bh, int bd, int nbx, int nby,
-                                      double gain, double c, double* out);
+                                      GatPoints pts, double* out);
 void gat3d_grid(int w, int h, int d, int* bw, int* bh, int* bd, int* nbx, int* nby, int* nbz);
 
 // shape.cu (k_block_phase is declared in shape.cuh, next to PhaseRef)

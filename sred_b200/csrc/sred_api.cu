@@ -2064,35 +2064,42 @@ int gat_runs(const sred_ctx* c, size_t nb, size_t per_block) {
   return (int)std::max<size_t>(1, std::min<size_t>(r, 64));
 }
 
-// The per-block [sum, sum of squares] from the runs' partial sums, added in
-// run order in FP64 on the host.
-sred_status gat_block_sums(sred_ctx* c, const double* d_part, size_t nb, int runs, std::vector<double>* sums) {
-  std::vector<double> part(2 * nb * runs);
+// The per-block [sum, sum of squares] of each of np points from the runs'
+// partial sums, added in run order in FP64 on the host.
+sred_status gat_block_sums(sred_ctx* c, const double* d_part, int np, size_t nb, int runs,
+                           std::vector<double>* sums) {
+  std::vector<double> part(2 * (size_t)np * nb * runs);
   CK(cudaMemcpyAsync(part.data(), d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  sums->assign(2 * nb, 0.0);
-  for (size_t b = 0; b < nb; b++)
+  sums->assign(2 * (size_t)np * nb, 0.0);
+  for (size_t pb = 0; pb < (size_t)np * nb; pb++)
     for (int s = 0; s < runs; s++) {
-      (*sums)[2 * b] += part[2 * (b * runs + s)];
-      (*sums)[2 * b + 1] += part[2 * (b * runs + s) + 1];
+      (*sums)[2 * pb] += part[2 * (pb * runs + s)];
+      (*sums)[2 * pb + 1] += part[2 * (pb * runs + s) + 1];
     }
   return SRED_OK;
 }
 
-sred_status gat_objective_dev(sred_ctx* c, const float* d_img, int w, int h, double gain, double sigma,
-                              double offset, double* error) {
+// GATMinimizer2D.userFunction at np <= kGatMaxPoints points p[i] = (gain,
+// sigma, offset), one launch for all of them.
+sred_status gat_objective_dev(sred_ctx* c, const float* d_img, int w, int h, const double (*p)[3], int np,
+                              double* error) {
   int bw, bh, nbx, nby;
   if (!gat_grid(w, h, &bw, &bh, &nbx, &nby)) return fail(c, SRED_ERR_ARG, "image too small for the GAT fit (width and height >= 12)");
   const int nb = nbx * nby;
   const int runs = gat_runs(c, (size_t)nb, (size_t)bw * bh);
   double* d_sums;
-  CKS(ensure(c, B_GAT, 2 * (size_t)nb * runs, &d_sums));
-  const double cst = (3.0 / 8.0) * gain * gain + sigma * sigma - gain * offset;
-  k_gat_block_moments<<<dim3(nb, runs), 256, 0, c->stream>>>(d_img, w, bw, bh, nbx, gain, cst, d_sums);
+  CKS(ensure(c, B_GAT, 2 * (size_t)kGatMaxPoints * nb * runs, &d_sums));
+  GatPoints pts;
+  for (int i = 0; i < np; i++) {
+    pts.gain[i] = p[i][0];
+    pts.c[i] = (3.0 / 8.0) * p[i][0] * p[i][0] + p[i][1] * p[i][1] - p[i][0] * p[i][2];
+  }
+  k_gat_block_moments<<<dim3(nb, runs, np), 256, 0, c->stream>>>(d_img, w, bw, bh, nbx, pts, d_sums);
   CK(cudaGetLastError());
   std::vector<double> sums;
-  CKS(gat_block_sums(c, d_sums, (size_t)nb, runs, &sums));
-  *error = gat_error(sums.data(), nb, bw, bh);
+  CKS(gat_block_sums(c, d_sums, np, (size_t)nb, runs, &sums));
+  for (int i = 0; i < np; i++) error[i] = gat_error(sums.data() + 2 * (size_t)i * nb, nb, bw, bh);
   return SRED_OK;
 }
 
@@ -2100,27 +2107,37 @@ sred_status gat_objective_dev(sred_ctx* c, const float* d_img, int w, int h, dou
 // sigma >= 0, offset >= 0; block grid of width/6 x height/6 x depth/6 voxels
 // (at least 1), halved along every axis with fewer than 2 blocks until each
 // has 2 or the block is one voxel; per-block variance with FP64 sums of the
-// transformed voxels (as float, then widened).
-sred_status gat_objective3d_dev(sred_ctx* c, const float* d_vol, int w, int h, int d, double gain, double sigma,
-                                double offset, double* error) {
-  if (gain <= 0 || sigma < 0 || offset < 0) {
-    *error = std::nan("");
-    return SRED_OK;
+// transformed voxels (as float, then widened). np <= kGatMaxPoints points,
+// the ones inside the domain in one launch.
+sred_status gat_objective3d_dev(sred_ctx* c, const float* d_vol, int w, int h, int d, const double (*p)[3], int np,
+                                double* error) {
+  int in[kGatMaxPoints], nin = 0;
+  for (int i = 0; i < np; i++) {
+    if (p[i][0] <= 0 || p[i][1] < 0 || p[i][2] < 0)
+      error[i] = std::nan("");
+    else
+      in[nin++] = i;
   }
+  if (nin == 0) return SRED_OK;
   int bw, bh, bd, nbx, nby, nbz;
   gat3d_grid(w, h, d, &bw, &bh, &bd, &nbx, &nby, &nbz);
   const size_t nb = (size_t)nbx * nby * nbz;
   if (nb == 0) return fail(c, SRED_ERR_ARG, "volume too small for the GAT fit");
   const int runs = gat_runs(c, nb, (size_t)bw * bh * bd);
   double* d_sums;
-  CKS(ensure(c, B_GAT, 2 * nb * runs, &d_sums));
-  const double cst = (3.0 / 8.0) * gain * gain + sigma * sigma - gain * offset;
-  k_gat_block_moments3d<<<dim3((unsigned)nb, runs), 256, 0, c->stream>>>(d_vol, w, h, bw, bh, bd, nbx, nby, gain,
-                                                                         cst, d_sums);
+  CKS(ensure(c, B_GAT, 2 * (size_t)kGatMaxPoints * nb * runs, &d_sums));
+  GatPoints pts;
+  for (int k = 0; k < nin; k++) {
+    const double* q = p[in[k]];
+    pts.gain[k] = q[0];
+    pts.c[k] = (3.0 / 8.0) * q[0] * q[0] + q[1] * q[1] - q[0] * q[2];
+  }
+  k_gat_block_moments3d<<<dim3((unsigned)nb, runs, nin), 256, 0, c->stream>>>(d_vol, w, h, bw, bh, bd, nbx, nby,
+                                                                               pts, d_sums);
   CK(cudaGetLastError());
   std::vector<double> sums;
-  CKS(gat_block_sums(c, d_sums, nb, runs, &sums));
-  *error = gat_error(sums.data(), (int)nb, bw * bh * bd, 1);
+  CKS(gat_block_sums(c, d_sums, nin, nb, runs, &sums));
+  for (int k = 0; k < nin; k++) error[in[k]] = gat_error(sums.data() + 2 * (size_t)k * nb, (int)nb, bw * bh * bd, 1);
   return SRED_OK;
 }
 
@@ -2153,7 +2170,8 @@ sred_status sred_gat_objective_2d(sred_ctx* c, const float* img, int w, int h, d
   float* d;
   CKS(ensure(c, B_IMG, n, &d));
   CK(cudaMemcpyAsync(d, img, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-  return gat_objective_dev(c, d, w, h, gain, sigma, offset, error);
+  const double p[1][3] = {{gain, sigma, offset}};
+  return gat_objective_dev(c, d, w, h, p, 1, error);
 }
 
 // Nelder-Mead downhill simplex (Nelder & Mead, Computer Journal 7:308, 1965;
@@ -2162,24 +2180,31 @@ sred_status sred_gat_objective_2d(sred_ctx* c, const float* img, int w, int h, d
 // (1, 10, 100; java/GATMinimizer2D.java:42-45). An objective of NaN ranks
 // last. Stops after max_iter evaluations or when the simplex's objective
 // values agree to 1e-15 of the best.
+// objective(p, np, out) evaluates np <= 4 points in one go. Each iteration
+// evaluates the reflection, the expansion and both contractions together and
+// then takes the same decisions as evaluating them one at a time, so the
+// simplex path is the sequential one; `evals` counts only the evaluations
+// the sequential method makes.
 extern "C++" {
 template <class F>
 sred_status nelder_mead3(F objective, int max_iter, double* x0, double* f_best) {
   double x[4][3];
   double f[4];
   const double step[3] = {1.0, 10.0, 100.0};
-  int evals = 0;
-  auto eval = [&](const double* p, double* out) -> sred_status {
-    evals++;
-    const sred_status st = objective(p, out);
-    if (st == SRED_OK && std::isnan(*out)) *out = HUGE_VAL;
-    return st;
+  auto batch = [&](const double (*p)[3], int np, double* out) -> sred_status {
+    const sred_status st = objective(p, np, out);
+    if (st != SRED_OK) return st;
+    for (int i = 0; i < np; i++)
+      if (std::isnan(out[i])) out[i] = HUGE_VAL;
+    return SRED_OK;
   };
   for (int v = 0; v < 4; v++) {
     for (int k = 0; k < 3; k++) x[v][k] = x0[k];
     if (v > 0) x[v][v - 1] += step[v - 1];
-    CKS(eval(x[v], &f[v]));
   }
+  sred_status st = batch(x, 4, f);
+  if (st != SRED_OK) return st;
+  int evals = 4;
   while (evals < max_iter) {
     int order[4] = {0, 1, 2, 3};
     std::sort(order, order + 4, [&](int a, int b) { return f[a] < f[b]; });
@@ -2189,38 +2214,50 @@ sred_status nelder_mead3(F objective, int max_iter, double* x0, double* f_best) 
     for (int v = 0; v < 4; v++)
       if (v != worst)
         for (int k = 0; k < 3; k++) cen[k] += x[v][k] / 3.0;
-    double xr[3], fr;
-    for (int k = 0; k < 3; k++) xr[k] = cen[k] + (cen[k] - x[worst][k]);
-    CKS(eval(xr, &fr));
+    // candidates: reflection, expansion, outside and inside contraction
+    double cand[4][3], fc4[4];
+    for (int k = 0; k < 3; k++) {
+      cand[0][k] = cen[k] + (cen[k] - x[worst][k]);
+      cand[1][k] = cen[k] + 2.0 * (cen[k] - x[worst][k]);
+      cand[2][k] = cen[k] + 0.5 * (cand[0][k] - cen[k]);
+      cand[3][k] = cen[k] + 0.5 * (x[worst][k] - cen[k]);
+    }
+    st = batch(cand, 4, fc4);
+    if (st != SRED_OK) return st;
+    const double fr = fc4[0];
+    evals++;
     if (fr < f[best]) {
-      double xe[3], fe;
-      for (int k = 0; k < 3; k++) xe[k] = cen[k] + 2.0 * (cen[k] - x[worst][k]);
-      CKS(eval(xe, &fe));
-      if (fe < fr) {
-        std::copy(xe, xe + 3, x[worst]);
-        f[worst] = fe;
-      } else {
-        std::copy(xr, xr + 3, x[worst]);
-        f[worst] = fr;
-      }
+      const double fe = fc4[1];
+      evals++;
+      const int pick = fe < fr ? 1 : 0;
+      std::copy(cand[pick], cand[pick] + 3, x[worst]);
+      f[worst] = fc4[pick];
     } else if (fr < f[second]) {
-      std::copy(xr, xr + 3, x[worst]);
+      std::copy(cand[0], cand[0] + 3, x[worst]);
       f[worst] = fr;
     } else {
-      double xc[3], fc;
       const bool outside = fr < f[worst];
-      for (int k = 0; k < 3; k++)
-        xc[k] = outside ? cen[k] + 0.5 * (xr[k] - cen[k]) : cen[k] + 0.5 * (x[worst][k] - cen[k]);
-      CKS(eval(xc, &fc));
+      const int ic = outside ? 2 : 3;
+      const double fc = fc4[ic];
+      evals++;
       if (fc < (outside ? fr : f[worst])) {
-        std::copy(xc, xc + 3, x[worst]);
+        std::copy(cand[ic], cand[ic] + 3, x[worst]);
         f[worst] = fc;
       } else {
+        double sx[3][3], sf[3];
+        int idx[3], ns = 0;
         for (int v = 0; v < 4; v++)
           if (v != best) {
-            for (int k = 0; k < 3; k++) x[v][k] = x[best][k] + 0.5 * (x[v][k] - x[best][k]);
-            CKS(eval(x[v], &f[v]));
+            for (int k = 0; k < 3; k++) sx[ns][k] = x[best][k] + 0.5 * (x[v][k] - x[best][k]);
+            idx[ns++] = v;
           }
+        st = batch(sx, 3, sf);
+        if (st != SRED_OK) return st;
+        for (int q = 0; q < 3; q++) {
+          std::copy(sx[q], sx[q] + 3, x[idx[q]]);
+          f[idx[q]] = sf[q];
+        }
+        evals += 3;
       }
     }
   }
@@ -2246,7 +2283,7 @@ sred_status sred_gat_fit_2d(sred_ctx* c, const float* img, int w, int h, int max
   CKS(ensure(c, B_IMG, n, &d));
   CK(cudaMemcpyAsync(d, img, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
   double x[3] = {*gain, *sigma, *offset}, fb;
-  CKS(nelder_mead3([&](const double* p, double* out) { return gat_objective_dev(c, d, w, h, p[0], p[1], p[2], out); },
+  CKS(nelder_mead3([&](const double (*p)[3], int np, double* out) { return gat_objective_dev(c, d, w, h, p, np, out); },
                    max_iter, x, &fb));
   *gain = x[0];
   *sigma = x[1];
@@ -2272,7 +2309,8 @@ sred_status sred_gat_objective_3d(sred_ctx* c, const float* vol, int w, int h, i
   float* dv;
   CKS(ensure(c, B_IMG, n, &dv));
   CK(cudaMemcpyAsync(dv, vol, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-  return gat_objective3d_dev(c, dv, w, h, d, gain, sigma, offset, error);
+  const double p[1][3] = {{gain, sigma, offset}};
+  return gat_objective3d_dev(c, dv, w, h, d, p, 1, error);
 }
 
 sred_status sred_gat_fit_3d(sred_ctx* c, const float* vol, int w, int h, int d, int max_iter, double* gain,
@@ -2287,7 +2325,7 @@ sred_status sred_gat_fit_3d(sred_ctx* c, const float* vol, int w, int h, int d, 
   CK(cudaMemcpyAsync(dv, vol, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
   double x[3] = {*gain, *sigma, *offset}, fb;
   CKS(nelder_mead3(
-      [&](const double* p, double* out) { return gat_objective3d_dev(c, dv, w, h, d, p[0], p[1], p[2], out); },
+      [&](const double (*p)[3], int np, double* out) { return gat_objective3d_dev(c, dv, w, h, d, p, np, out); },
       max_iter, x, &fb));
   *gain = x[0];
   *sigma = x[1];
