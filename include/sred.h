@@ -34,10 +34,12 @@ typedef enum {
 
 /* Contraction engine of the global map. SRED_ENGINE_TC: split-BF16 tcgen05
  * tensor-core Gram with FP32 accumulation (u = hi + mid, or hi + mid + lo
- * when 6K <= 128); SRED_ENGINE_FP32: plain FP32 CUDA-core Gram. Both share
- * moments, tiling and the fused epilogue. NRMSE and Abs-diff always run on
- * the FP32 engine (NRMSE accumulates |u_p - u_q|^2 directly: the dot-product
- * form cancels for near-identical blocks). */
+ * when 6K <= 128 and for NRMSE); SRED_ENGINE_FP32: plain FP32 CUDA-core Gram.
+ * Both share moments, the symmetric schedule (each unordered block pair
+ * evaluated once) and the fused epilogue. Abs-diff needs no contraction and
+ * runs on the FP32 engine's kernel; a map whose operands do not fit the
+ * tensor-core kernel's shared memory (K' above 576) falls back to the FP32
+ * engine, where NRMSE accumulates |u_p - u_q|^2 directly. */
 typedef enum { SRED_ENGINE_TC = 0, SRED_ENGINE_FP32 = 1 } sred_engine;
 
 typedef struct sred_ctx sred_ctx;
@@ -318,6 +320,16 @@ sred_status sred_block_map_2d_device_noalloc(const char *metric, const float *d_
  * bf16 hi/lo without normalising it). */
 sred_status sred_debug_gram_rowdot(sred_ctx *ctx, int engine, const float *u, const float *w1,
                                    const float *w2, int n, int k, double *num, double *den);
+
+/* Test hook of the tensor-core engine's bounded waits (no counterpart in the
+ * reference; the reference's host raises a RuntimeException when its OpenCL
+ * set-up fails, java/CLUtils.java:175-180): every pipeline wait of later
+ * global maps on this context gives up after timeout_ns (0: the default 4 s),
+ * and withhold_tile >= 0 makes the copy producer stop before that tile's
+ * operands, so the waits run out with no copy in flight and the call returns
+ * SRED_ERR_TIMEOUT with the context still usable. withhold_tile = -1 restores
+ * normal operation. */
+sred_status sred_debug_set_tc_wait(sred_ctx *ctx, unsigned long long timeout_ns, long long withhold_tile);
 
 /* ---------------------------------------------------------------------
  * 3D block repetition maps. Volumes are w x h x d floats, x fastest then y

@@ -33,7 +33,7 @@ EXPORTS = [
     "sred_relevance_mask_tool_2d", "sred_relevance_mask_sweep_2d", "sred_relevance_constant_range_2d",
     "sred_gat_3d", "sred_gat_objective_3d", "sred_gat_fit_3d", "sred_classify_redundancy_2d",
     "sred_debug_divide_fixed", "sred_debug_divide_fixed64", "sred_gat_quadtree_2d", "sred_gat_octree_3d", "sred_f_quantile",
-    "sred_global_map_3d_shard_sums", "sred_global_map_3d_shard_finish",
+    "sred_global_map_3d_shard_sums", "sred_global_map_3d_shard_finish", "sred_debug_set_tc_wait",
 ]
 
 
@@ -145,6 +145,7 @@ def load() -> C.CDLL:
         L.sred_relevance_constant_range_2d.argtypes = [_vp, _f32p, s, s, s, s, f, _fp, _fp, _fp]
         _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
         L.sred_debug_gram_rowdot.argtypes = [_vp, s, _f32p, _f32p, _f32p, s, s, _f64p, _f64p]
+        L.sred_debug_set_tc_wait.argtypes = [_vp, C.c_ulonglong, C.c_longlong]
         L.sred_block_map_2d_device_noalloc.argtypes = [C.c_char_p, _vp, s, s, s, _f32p, s, s, s, C.c_float,
                                                        C.c_float, s, _vp, _vp]
         L.sred_global_map_2d_batch.argtypes = [_vp, C.POINTER(SredJob), s, s]

@@ -252,17 +252,52 @@ def global_map_batch(jobs: list[dict], n_workers: int = 4, ctx=None) -> list[tup
 # Row-sharded global map (one map across several processes / GPUs)
 # ---------------------------------------------------------------------------
 
-def shard_row_blocks(n_gram: int, shard: int, n_shards: int) -> tuple[int, int]:
-    """Row blocks [rb0, rb1) (128 rows of the compacted block list each) that
-    shard `shard` of `n_shards` computes; the rule libsred applies."""
+def _items_before(ct: int, h: int) -> int:
+    """Work items of column tiles [0, ct): sum over c < ct of ceil((c + 1) / h)."""
+    q, r = divmod(ct, h)
+    return h * q * (q + 1) // 2 + r * (q + 1)
+
+
+def gram_items(n_gram: int, bn: int = 256, num_sms: int = 148) -> tuple[int, int]:
+    """(items, L) of the tensor-core engine's symmetric schedule for n_gram
+    blocks and bn-column tiles: the upper triangle of 128-row x bn-column
+    tiles in runs of up to L row blocks per column tile, L the largest of
+    16, 8, 4, 2 that leaves at least 4 items per SM (the rule libsred applies,
+    global_tc.cu: gram_tc_items)."""
+    m = bn // 128
+    n_ct = (n_gram + bn - 1) // bn
+    L = 16
+    while L > 2 and _items_before(n_ct, L // m) < 4 * num_sms:
+        L //= 2
+    L = max(L, m)
+    return _items_before(n_ct, L // m), L
+
+
+def shard_items(n_gram: int, shard: int, n_shards: int, bn: int = 256, num_sms: int = 148):
+    """Tiles of shard `shard` of `n_shards`: the work items [I s / S, I (s + 1) / S)
+    of the symmetric schedule, each as (column tile, first row block, end row
+    block); empty runs (rows past n_gram) are left out. Every pair (p <= q) of
+    the n_gram blocks lies in exactly one tile of exactly one shard."""
+    items, L = gram_items(n_gram, bn, num_sms)
+    m, h = bn // 128, L // (bn // 128)
     n_rb = (n_gram + 127) // 128
-    return n_rb * shard // n_shards, n_rb * (shard + 1) // n_shards
+    i0, i1 = items * shard // n_shards, items * (shard + 1) // n_shards
+    out = []
+    ct = 0
+    for it in range(i0, i1):
+        while _items_before(ct + 1, h) <= it:
+            ct += 1
+        rb0 = (it - _items_before(ct, h)) * L
+        rb1 = min(rb0 + L, (ct + 1) * m, n_rb)
+        if rb0 < rb1:
+            out.append((ct, rb0, rb1))
+    return out
 
 
 def sharded_exchange(compute_sums, finish, allreduce):
-    """The row-sharded global map's one exchange step: this rank's per-row
-    sums (zero outside its rows) -> summed over all ranks in place (the only
-    collective) -> the map finished from the summed sums."""
+    """The sharded global map's one exchange step: this rank's per-block
+    sums over its tiles of block pairs -> summed over all ranks in place (the
+    only collective) -> the map finished from the summed sums."""
     sums, n_gram = compute_sums()
     allreduce(sums[:2 * n_gram])
     return finish(sums)

@@ -58,9 +58,15 @@ struct BlockParams {
 //   three levels: A = [hi|mid|lo|hi|mid|hi], B = [hi|hi|hi|mid|mid|lo] (6K
 //                 columns); every product down to 2^-18 relative, an FP32-level
 //                 dot product. Used while 6K fits in 128 columns, where the
-//                 tiles are bound by the epilogue and the deeper MMA is free.
+//                 tiles are bound by the epilogue and the deeper MMA is free,
+//                 and always for NRMSE, whose 1 - G term needs it.
 inline int split_levels(int K) { return 6 * K <= 128 ? 3 : 2; }
 inline int split_cols(int K) { return split_levels(K) == 3 ? (6 * K + 31) / 32 * 32 : (3 * K + 31) / 32 * 32; }
+inline bool nrmse_metric(int m) { return m == 2 /* kNrmse */ || m == 8 /* kNrmseW */; }
+inline int split_levels_for(int metric, int K) { return nrmse_metric(metric) ? 3 : split_levels(K); }
+inline int split_cols_for(int metric, int K) {
+  return split_levels_for(metric, K) == 3 ? (6 * K + 31) / 32 * 32 : (3 * K + 31) / 32 * 32;
+}
 
 __device__ __forceinline__ void store_split(__nv_bfloat16* a, __nv_bfloat16* b, int K, int i, double u,
                                             int levels) {
@@ -102,27 +108,77 @@ struct EpiConsts {
   int n;            // valid blocks (rows == cols)
   float nrmse_scale;  // (K-1)/K
   float c1, c2;
+  // NRMSE on the tensor cores: pairs with G above nrmse_near get the term of
+  // the exact squared difference of their FP32 unit vectors U (row pitch kp,
+  // K values), the form the FP32 engine evaluates for every pair.
+  const float* U = nullptr;
+  int kp = 0, K = 0;
+  float nrmse_near = 1.0f;
 };
 
-// Launch the FP32 CUDA-core all-pairs kernel (global_fp32.cu).
-// U: n_pad x kp floats (unit vectors), params: n_pad entries, num/den: n doubles (zeroed).
-// Rows are processed in 128-row blocks; [rb_begin, rb_end) restricts the launch
-// to those row blocks (rb_end < 0: all), the unit of row sharding.
+// Near-identical pairs (G > 1 - 2^-7) of tensor-core NRMSE take the exact
+// difference form: there 1 - G is within an order of magnitude of the FP32
+// accumulation error of G, which the square root of the term amplifies.
+constexpr float kNrmseNear = 1.0f - 1.0f / 128.0f;
+
+// Launch the FP32 CUDA-core all-pairs kernel (global_fp32.cu), on the same
+// symmetric schedule as the tensor-core engine with 128 x 128 tiles.
+// U: n_pad x kp floats (unit vectors), params: n_pad entries, num/den: n
+// doubles (zeroed). The work items are split into n_shards equal ranges; this
+// launch runs range `shard`.
 cudaError_t launch_gram_fp32(const float* U, int kp, const BlockParams* params, const float* tile_rmax,
                              EpiConsts ec, double* num, double* den, int num_sms, cudaStream_t st,
-                             int rb_begin = 0, int rb_end = -1);
+                             int shard = 0, int n_shards = 1);
 
-// Column parameters of one 256-column tile, structure of arrays, as the
-// tensor-core engine copies them into shared memory:
-//   [a x256 | r x256 | sigma x256 | mu x256 | max r of the tile | 3 x pad]
-constexpr int kColSoaFloats = 4 * 256 + 4;
+// Column parameters of one BN-column tile as the tensor-core engine copies
+// them into shared memory: [a x BN | r x BN | sigma x BN | mu x BN | max r of
+// the tile | 3 x pad], each array permuted within every 16-column group so that
+// an epilogue thread's four columns of the group (2j, 2j + 1, 8 + 2j, 9 + 2j for
+// j = t % 4) are one float4.
+__host__ __device__ constexpr int col_soa_floats(int bn) { return 4 * bn + 4; }
+__host__ __device__ constexpr int col_soa_pos(int i) {
+  return (i & ~15) + 4 * ((i & 7) >> 1) + 2 * ((i >> 3) & 1) + (i & 1);
+}
+// Row parameters of one 128-row block, natural order: [a | r | sigma | mu] x 128,
+// max r, 3 x pad.
+constexpr int kRowSoaFloats = 4 * 128 + 4;
+
+// Launch shape of the tensor-core engine for a K': column tile width (256 or
+// 128), whole-tile A buffers or a ring of 64-column chunks, dynamic shared
+// memory. False if the B tile does not fit in shared memory.
+struct TcPlan {
+  int bn;
+  bool tr;
+  int stages;
+  size_t smem;
+};
+bool plan_gram_tc(int kq, TcPlan* plan);
+
+// Test hooks of the tensor-core engine: a wait limit (0: 4 s) and a tile whose
+// operand copies the producer never issues (-1: none), so that the pipeline
+// waits run out with nothing in flight.
+struct TcDebug {
+  unsigned long long timeout_ns;
+  long long withhold_tile;
+};
+
+// Floats of the parameter workspace launch_gram_tc fills (column tiles and
+// row blocks) for n_pad blocks.
+size_t gram_tc_soa_floats(int n_pad);
+
+// Work items of the symmetric schedule for n blocks and tile width bn (the
+// upper triangle of 128-row x bn-column tiles in runs of L row blocks).
+long long gram_tc_items(int n, int bn, int* L, int num_sms);
 
 // Launch the split-BF16 tcgen05 all-pairs kernel (global_tc.cu).
-// A, B: n_pad x kq bf16 ([hi|lo|hi] and [hi|hi|lo]); colsoa: n_pad/256 tiles
-// of kColSoaFloats (k_col_soa).
+// A, B: n_pad x kq bf16 (store_split); params: n_pad entries (rows past n
+// zero); soa_ws: gram_tc_soa_floats(n_pad) floats of workspace; num/den: n
+// doubles (zeroed), to which every pair's terms are added for both blocks.
+// The upper-triangle work items are split into n_shards equal ranges; this
+// launch runs range `shard` (the shards' num/den add up to the whole map).
 cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int kq, int n_pad,
-                           const BlockParams* params, const float* colsoa, const float* tile_rmax, EpiConsts ec,
-                           double* num, double* den, int num_sms, int* status, cudaStream_t st,
-                           int rb_begin = 0, int rb_end = -1);
+                           const BlockParams* params, float* soa_ws, EpiConsts ec, double* num, double* den,
+                           int num_sms, int* status, cudaStream_t st, int shard = 0, int n_shards = 1,
+                           const TcDebug* dbg = nullptr);
 
 }  // namespace sred

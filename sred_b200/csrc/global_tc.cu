@@ -1,34 +1,41 @@
 // Split-BF16 tcgen05 engine of the global repetition map (sm_100a).
 //
 // G = A' B'^T on the 5th-generation tensor cores, where each block's FP64 unit
-// vector u is split into bf16 hi = bf16(u), lo = bf16(u - hi), and
-//   A' = [hi | lo | hi],  B' = [hi | hi | lo]   (K' = round_up(3K, 16))
-// so one BF16 MMA chain with FP32 accumulation yields hi.hi + lo.hi + hi.lo,
-// an FP32-accurate <u_p, u_q> (the dropped lo.lo term is below 2^-16).
+// vector u is split into bf16 parts (common.cuh: store_split), so one BF16
+// MMA chain with FP32 accumulation yields an FP32-accurate <u_p, u_q>.
 //
-// CTA = 1 per SM, persistent over work items (128-row block, range of
-// 256-column tiles). Warp roles:
-//   warp 16     TMA producer: the item's A tile (resident, all K' chunks), a
-//               ring of B stages (one 256 x 64 bf16 chunk each, SWIZZLE_128B)
-//               and a ring of four column-parameter slots (4 KB per tile)
-//   warp 17     MMA issuer (one thread): on claiming one of two TMEM
-//               accumulators (2 x 256 columns) it issues tcgen05.mma
-//               M=128 N=256 K=16 and tcgen05.commit to release B stages and
-//               to publish the finished accumulator. It shares an SM
-//               sub-partition with four busy epilogue warps, so its loop is
-//               kept to a few instructions per MMA: no divisions, operand
-//               descriptors advanced by adds, K steps unrolled.
-//   warps 0-15  epilogue: tcgen05.ld of the accumulator (warp w reads TMEM
-//               lanes 32(w%4).. and columns 64(w/4)..), the fused per-pair
-//               metric (epilogue.cuh), row sums in registers; FP64 atomics
-//               per row per item. The N x N matrix is never stored. Epilogue
-//               warps synchronise only through mbarriers, so they drift and
-//               overlap each other's TMEM-load latency.
-// Every mbarrier wait is bounded by wall time; on expiry the kernel records a
-// status code, stops issuing work, waits (bounded) for its own copies in
-// flight, frees TMEM and returns. No TMA multicast is used.
+// Symmetric schedule. Every per-pair term of the global map (weight, Pearson,
+// global SSIM, NRMSE, Abs-diff; epilogue.cuh) is symmetric in (p, q), so each
+// unordered pair is evaluated once: only tiles of the upper triangle are
+// scheduled (a 128-row block rb against a BN-column tile ct with
+// 128 rb <= BN ct + BN - 1), pairs below the diagonal are masked in the
+// diagonal tiles, and each pair's numerator and denominator terms are added to
+// the sums of both blocks (the self pair once).
+//
+// Work item = (column tile ct, a run of up to L row blocks). The item's B tile
+// (BN x K') and column parameters stay in shared memory for the whole item;
+// the A tiles of its row blocks stream through (two whole tiles when they fit,
+// else a ring of 64-column chunks). CTA = 1 per SM, persistent. Warp roles:
+//   warp 16     TMA producer (one thread)
+//   warp 17     MMA issuer (one thread): tcgen05.mma M=128 N=BN K=16 into one
+//               of two TMEM accumulators, tcgen05.commit to publish it
+//   warps 0-15  epilogue: warp w reads TMEM lanes 32(w%4).. and BN/4 columns
+//               from BN/4 (w/4) with tcgen05.ld.16x256b, which gives each
+//               thread 4 rows x (BN/16) columns of the warp's slab. The fused
+//               per-pair metric runs on f32x2 pairs of neighbouring columns.
+//               Column sums of the item accumulate in registers (BN/8 values
+//               per thread and sum) and leave once per item after a butterfly
+//               over the 8 lanes that share columns; row sums of a tile leave
+//               once per tile after a butterfly over the 4 lanes that share
+//               rows and a combine of the 4 column-group warps in shared
+//               memory: one FP64 atomic add per row per tile.
+// Every mbarrier wait is bounded by wall time (a host-set limit); on expiry the
+// kernel records a status code, stops issuing work, waits (bounded) for its own
+// copies in flight, frees TMEM and returns. No TMA multicast is used.
 #include <cuda.h>
 #include <cudaTypedefs.h>
+
+#include <algorithm>
 
 #include "common.cuh"
 #include "epilogue.cuh"
@@ -37,34 +44,46 @@ namespace sred {
 
 namespace {
 
-constexpr int kBM = 128;          // rows per tile (TMEM lanes)
-constexpr int kBN = 256;          // columns per tile
-constexpr int kChunk = 64;        // bf16 elements per K chunk (128 B, one SWIZZLE_128B atom row)
-constexpr int kAChunkBytes = kBM * kChunk * 2;   // 16 KB
-constexpr int kBStageBytes = kBN * kChunk * 2;   // 32 KB
+constexpr int kBM = 128;                          // rows per tile (TMEM lanes)
+constexpr int kChunk = 64;                        // bf16 per K chunk (128 B: one SWIZZLE_128B atom row)
+constexpr int kAChunkBytes = kBM * kChunk * 2;    // 16 KB
 constexpr int kMaxStages = 16;
-constexpr int kEpiWarps = 16;                       // 4 per SM sub-partition
-constexpr int kColsPerWarp = kBN / (kEpiWarps / 4);  // 64: each warp reads 32 lanes x 64 columns
+constexpr int kEpiWarps = 16;                     // 4 per SM sub-partition
 constexpr int kThreads = (kEpiWarps + 2) * 32;
-constexpr int kSoaBytes = kColSoaFloats * 4;         // one tile's column parameters
-constexpr int kParSlots = 4;                         // column-parameter ring depth
-constexpr unsigned long long kTimeoutNs = 4000000000ull;  // 4 s per wait
+constexpr int kEpiThreads = kEpiWarps * 32;
+constexpr int kRSlots = 4;                        // row-parameter ring depth
+constexpr int kRowFloats = kRowSoaFloats;         // one 128-row block's parameters
+constexpr int kRowPartBytes = 2 * 4 * kBM * 8;    // [2 buffers][4 column groups][128 rows] float2
+constexpr int kBarBytes = 512;
+constexpr size_t kSmemBudget = 227 * 1024;
 
 enum { ST_OK = 0, ST_TIMEOUT_PRODUCER = 1, ST_TIMEOUT_MMA = 2, ST_TIMEOUT_EPI = 3, ST_TIMEOUT_DRAIN = 4 };
 
+template <int BN>
+struct Cfg {
+  static constexpr int kColW = BN / 4;              // columns per epilogue warp
+  static constexpr int kCH = kColW / 16;            // 16-column chunks per warp and tile
+  static constexpr int kM = BN / kBM;               // row blocks per column tile
+  static constexpr int kCSoa = col_soa_floats(BN);  // floats per column tile's parameters
+  static constexpr int kBChunkBytes = BN * kChunk * 2;
+  static constexpr int kColAccBytes = kEpiThreads * 8 * kCH * 4;  // per thread: 2 sums x 4 columns x chunks
+};
+
 struct TcArgs {
-  int kq, nkc, stages;
-  int nfull, tail;              // tile-ring mode: 64-column chunks and a 32-column tail (0 or 1)
-  uint32_t a_bytes, b_bytes;    // tile-ring mode: A tile and one B tile in shared memory
-  int rb0;                      // first 128-row block of this launch
-  int n_rb, n_ct, ct_per_item, n_items;
-  const BlockParams* params;
-  const float* colsoa;
-  const float* tile_rmax;
+  int kq, nkc, stages;          // K', K chunks per tile (nfull + tail), chunk-ring depth
+  int nfull, tail;              // whole-tile mode: 64-column chunks and a 32-column tail (0 or 1)
+  uint32_t a_bytes, b_bytes;    // whole A tile and whole B tile (64-column chunks + 32-column tail)
+  int n_rb, n_ct;               // row blocks holding valid rows, column tiles
+  int L, h;                     // row blocks per item, L / (BN / 128)
+  long long item0, item1;       // items of this launch
+  const float* colsoa;          // per column tile, permuted (col_soa_pos)
+  const float* rowsoa;          // per 128-row block, natural order
   EpiConsts ec;
   double* num;
   double* den;
   int* status;
+  unsigned long long timeout_ns;
+  long long withhold;           // test hook: the producer never issues this tile's loads (-1: none)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -102,20 +121,20 @@ __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
 }
 
 // Bounded wait for the phase with the given parity. Returns false (and
-// records `code`) if the wait exceeded kTimeoutNs or another role of any CTA
+// records `code`) if the wait exceeded the limit or another role of any CTA
 // already gave up. Drain waits (for copies or MMAs this CTA issued) pass
 // abort = false: they keep waiting, within the same bound, after another
 // role has given up.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* status, int code,
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const TcArgs& g, int code,
                                           bool abort = true) {
   if (mbar_test(bar, parity)) return true;
   const unsigned long long t0 = globaltimer();
   for (uint32_t i = 1;; i++) {
     if (mbar_test(bar, parity)) return true;
     if ((i & 255u) == 0) {
-      if (abort && *reinterpret_cast<volatile int*>(status) != ST_OK) return false;
-      if (globaltimer() - t0 > kTimeoutNs) {
-        atomicCAS(status, ST_OK, code);
+      if (abort && *reinterpret_cast<volatile int*>(g.status) != ST_OK) return false;
+      if (globaltimer() - t0 > g.timeout_ns) {
+        atomicCAS(g.status, ST_OK, code);
         return false;
       }
     }
@@ -150,7 +169,7 @@ __device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
 }
 
 // Same for SWIZZLE_64B (64-byte rows, 8-row groups 512 B apart): the 32-column
-// tail of K' in the tile-ring mode.
+// tail of K' in the whole-tile mode.
 __device__ __forceinline__ uint64_t desc_sw64(uint32_t saddr) {
   uint64_t d = 0;
   d |= static_cast<uint64_t>((saddr & 0x3FFFFu) >> 4);
@@ -161,16 +180,20 @@ __device__ __forceinline__ uint64_t desc_sw64(uint32_t saddr) {
   return d;
 }
 
-// Instruction descriptor, kind::f16: D = F32, A = B = BF16, both K-major, M = 128, N = 256.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(kBN >> 3) << 17) |
-                            (static_cast<uint32_t>(kBM >> 4) << 24);
+// Instruction descriptor, kind::f16: D = F32, A = B = BF16, both K-major, M = 128, N = BN.
+template <int BN>
+constexpr uint32_t idesc() {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(BN >> 3) << 17) |
+         (static_cast<uint32_t>(kBM >> 4) << 24);
+}
 
+template <int BN>
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate)
+      "l"(da), "l"(db), "r"(idesc<BN>()), "r"(accumulate)
       : "memory");
 }
 
@@ -182,209 +205,429 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// Issue a load of 32 lanes x 16 columns of 32-bit accumulator (no wait).
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15}, [%16];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-      : "r"(taddr)
-      : "memory");
+// Issue a load of 16 lanes x 16 columns of 32-bit accumulator (no wait).
+// Thread t receives lanes t/4 and t/4 + 8, columns 2(t%4), 2(t%4) + 1 of
+// each 8-column half: v[0..1] (lane t/4, cols 0-7), v[2..3] (lane t/4 + 8),
+// v[4..5] and v[6..7] the same for columns 8-15.
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.16x256b.x2.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr)
+               : "memory");
 }
 
 // Wait for every TMEM load this thread issued; the register operands tie
 // later uses of v to the wait, so none is scheduled before it.
-__device__ __forceinline__ void tmem_wait(uint32_t (&v)[16]) {
+__device__ __forceinline__ void tmem_wait8(uint32_t (&v)[8]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;"
-               : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
-                 "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]),
-                 "+r"(v[15])
+               : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7])
                :
                : "memory");
 }
 
-// 16 pairs: accumulator columns c0..c0+15 of this thread's row against the
-// columns' parameters in the shared-memory slot (structure of arrays).
-template <int METRIC, int CMODE, bool FULL, bool DIAG>
-__device__ __forceinline__ void epi_chunk(const uint32_t (&v)[16], const float* __restrict__ soa, int c0, int col0,
-                                          int row, const RowState& rs, const EpiConsts& ec, float& sn, float& sd) {
-#pragma unroll
-  for (int j = 0; j < 16; j += 4) {
-    const int q = c0 + j;
-    const float4 a4 = *reinterpret_cast<const float4*>(soa + q);
-    const float4 r4 = *reinterpret_cast<const float4*>(soa + kBN + q);
-    float4 s4 = make_float4(0.f, 0.f, 0.f, 0.f), m4 = s4;
-    if (METRIC != kPearson && METRIC != kDebugDot) s4 = *reinterpret_cast<const float4*>(soa + 2 * kBN + q);
-    if (METRIC == kSsim) m4 = *reinterpret_cast<const float4*>(soa + 3 * kBN + q);
-    const float av[4] = {a4.x, a4.y, a4.z, a4.w};
-    const float rv[4] = {r4.x, r4.y, r4.z, r4.w};
-    const float sv[4] = {s4.x, s4.y, s4.z, s4.w};
-    const float mv[4] = {m4.x, m4.y, m4.z, m4.w};
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-      BlockParams cq;
-      cq.a = av[u];
-      cq.r = rv[u];
-      cq.sigma = sv[u];
-      cq.mu = mv[u];
-      float G = __uint_as_float(v[j + u]);
-      if (DIAG && col0 + q + u == row && rs.r > 0.0f) G = 1.0f;
-      if (FULL || col0 + q + u < ec.n) epi_pair<METRIC, CMODE>(G, rs, cq, ec, sn, sd);
+// ---------------------------------------------------------------------------
+// Epilogue arithmetic on f32x2 pairs (two neighbouring columns of one row).
+// ---------------------------------------------------------------------------
+
+// Row constants, both halves equal (only the fields a metric uses survive).
+struct RowC {
+  F2 a, ne, r;                 // weight argument, -eps/sigma, 1/sigma (diagnostic terms)
+  F2 mu2, sg2, mumu, s2, sg;   // 2 mu, 2 sigma, mu^2, sigma^2 + c2, sigma
+};
+
+template <int METRIC>
+__device__ __forceinline__ RowC make_rowc(const float* __restrict__ rs, int row, const EpiConsts& ec) {
+  RowC c;
+  const float a = rs[row], r = rs[kBM + row];
+  c.a = f2(a, a);
+  if (METRIC == kPearson) {
+    const float ne = -kEps * r;
+    c.ne = f2(ne, ne);
+  }
+  if (METRIC == kDebugDot) c.r = f2(r, r);
+  if (METRIC == kSsim || METRIC == kNrmse || METRIC == kNrmseW) {
+    const float s = rs[2 * kBM + row];
+    c.sg2 = f2(2.0f * s, 2.0f * s);
+    c.sg = f2(s, s);
+    if (METRIC == kSsim) {
+      const float m = rs[3 * kBM + row];
+      c.mu2 = f2(2.0f * m, 2.0f * m);
+      c.mumu = f2(m * m, m * m);
+      const float s2 = s * s + ec.c2;
+      c.s2 = f2(s2, s2);
     }
   }
+  return c;
 }
 
-// Packed Pearson fast path (full, off-diagonal tiles, CMODE kCFirst or
-// kCSecond): 16 pairs as eight f32x2 pairs.
-template <int CMODE>
-__device__ __forceinline__ void epi_chunk_pearson2(const uint32_t (&v)[16], const float* __restrict__ soa, int c0,
-                                                   const PearsonRow2& r2, F2& sn, F2& sd) {
-#pragma unroll
-  for (int j = 0; j < 16; j += 4) {
-    const float4 a4 = *reinterpret_cast<const float4*>(soa + c0 + j);
-    const float4 r4 = *reinterpret_cast<const float4*>(soa + kBN + c0 + j);
-    pearson_pair2<CMODE>(f2(__uint_as_float(v[j]), __uint_as_float(v[j + 1])), f2(a4.x, a4.y), f2(r4.x, r4.y), r2,
-                         sn, sd);
-    pearson_pair2<CMODE>(f2(__uint_as_float(v[j + 2]), __uint_as_float(v[j + 3])), f2(a4.z, a4.w),
-                         f2(r4.z, r4.w), r2, sn, sd);
+// Numerator factor x and weight w of two pairs; the numerator term is x w for
+// the weighted metrics and x for unweighted NRMSE (2D) and the diagnostic dot
+// product (whose "weight" is r_p + r_q). Same arithmetic as pair_terms.
+template <int METRIC, int CMODE>
+__device__ __forceinline__ void terms2(F2 G, const RowC& rc, F2 qa, F2 qr, F2 qs, F2 qm, const EpiConsts& ec,
+                                       F2& x, F2& w) {
+  const F2 one = f2(1.0f, 1.0f);
+  if (METRIC == kDebugDot) {
+    x = mul2(G, mul2(rc.a, qa));
+    w = add2(rc.r, qr);
+    return;
+  }
+  const F2 d = sub2(rc.a, qa);
+  float m0, m1;
+  f2_split(mul2(d, d), m0, m1);
+  w = f2(ex2_approx(-m0), ex2_approx(-m1));
+  float x0, x1;
+  if (METRIC == kPearson) {
+    F2 gc;
+    if (CMODE == kCFirst) {
+      gc = fma2(mul2(G, rc.ne), qr, G);  // G (1 - t)
+    } else if (CMODE == kCSecond) {
+      const F2 nt = mul2(rc.ne, qr);     // -t
+      gc = mul2(G, fma2(nt, add2(nt, one), one));  // G (1 - t + t^2)
+    } else {
+      float d0, d1, g0, g1;
+      f2_split(sub2(one, mul2(rc.ne, qr)), d0, d1);  // 1 + t
+      f2_split(G, g0, g1);
+      gc = f2(g0 * __frcp_rn(d0), g1 * __frcp_rn(d1));
+    }
+    f2_split(gc, x0, x1);
+    x = f2(fmaxf(x0, 0.0f), fmaxf(x1, 0.0f));
+  } else if (METRIC == kSsim) {
+    const F2 c1 = f2(ec.c1, ec.c1), c2 = f2(ec.c2, ec.c2);
+    const F2 num = mul2(fma2(rc.mu2, qm, c1), fma2(mul2(rc.sg2, qs), G, c2));
+    const F2 den = mul2(fma2(rc.mumu, mul2(qm, qm), c1), fma2(qs, qs, rc.s2));
+    float n0, n1, e0, e1;
+    f2_split(num, n0, n1);
+    f2_split(den, e0, e1);
+    x = f2(fmaxf(__fdividef(n0, e0), 0.0f), fmaxf(__fdividef(n1, e1), 0.0f));
+  } else {  // kNrmse, kNrmseW: ((K-1)/K)((s_p - s_q)^2 + 2 s_p s_q (1 - G))
+    const F2 sc = f2(ec.nrmse_scale, ec.nrmse_scale);
+    const F2 ds = sub2(rc.sg, qs);
+    f2_split(mul2(sc, fma2(ds, ds, mul2(mul2(rc.sg2, qs), sub2(one, G)))), x0, x1);
+    x = f2(sqrtf(fmaxf(x0, 0.0f)), sqrtf(fmaxf(x1, 0.0f)));
   }
 }
 
-// Packed SSIM path (full, off-diagonal tiles): 16 pairs as eight f32x2 pairs.
-__device__ __forceinline__ void epi_chunk_ssim2(const uint32_t (&v)[16], const float* __restrict__ soa, int c0,
-                                                const SsimRow2& r2, F2& sn, F2& sd) {
+template <int METRIC>
+constexpr bool weighted_num() {
+  return METRIC == kPearson || METRIC == kSsim || METRIC == kNrmseW;
+}
+
+// Exact squared distance of two FP32 unit vectors (NRMSE near-identical pairs).
+__device__ __noinline__ float exact_diff2(const float* __restrict__ up, const float* __restrict__ uq, int K) {
+  float acc = 0.0f;
+  for (int i = 0; i < K; i++) {
+    const float d = up[i] - uq[i];
+    acc = fmaf(d, d, acc);
+  }
+  return acc;
+}
+
+__device__ __forceinline__ void f2_add_half(F2& v, int half, float x) {
+  float lo, hi;
+  f2_split(v, lo, hi);
+  if (half) hi += x;
+  else lo += x;
+  v = f2(lo, hi);
+}
+
+template <int METRIC>
+constexpr bool nrmse_tc() {
+  return METRIC == kNrmse || METRIC == kNrmseW;
+}
+
+// One 32-row x BN/4-column slab of a tile for this warp: BN/64 chunks of 16
+// columns, each read for both 16-lane halves of the warp's 32 TMEM lanes.
+// rs: the tile's row parameters; cs: this warp's column parameters (permuted);
+// cacc: this thread's column accumulators in shared memory, float4 j at
+// cacc[j * kEpiThreads] for j = 2c + {0: num, 1: den}, each holding the
+// thread's four columns of chunk c (2(t%4) + {0, 1}, 8 + 2(t%4) + {0, 1});
+// p0: block index of tile row 0; q0: block index of the slab's first column.
+// The tile's row sums are returned in rsum[2k + {0: num, 1: den}] for rows
+// 32(w%4) + t/4 + 8k.
+template <int METRIC, int BN, int CMODE, bool MASKED>
+__device__ __forceinline__ void sym_tile(uint32_t taddr, const float* __restrict__ rs, const float* __restrict__ cs,
+                                         float4* __restrict__ cacc, int p0, int q0, const EpiConsts& ec,
+                                         float (&rsum)[8]) {
+  constexpr int CH = Cfg<BN>::kCH;
+  const int lane = threadIdx.x & 31, rsub = lane >> 2, csub = lane & 3;
+  const int quarter = (threadIdx.x >> 5) & 3;
+  RowC rc[4];
+  F2 rn[4], rd[4];
+  int prow[4];
+  bool force[4];
 #pragma unroll
-  for (int j = 0; j < 16; j += 4) {
-    const float4 a4 = *reinterpret_cast<const float4*>(soa + c0 + j);
-    const float4 s4 = *reinterpret_cast<const float4*>(soa + 2 * kBN + c0 + j);
-    const float4 m4 = *reinterpret_cast<const float4*>(soa + 3 * kBN + c0 + j);
-    ssim_pair2(f2(__uint_as_float(v[j]), __uint_as_float(v[j + 1])), f2(a4.x, a4.y), f2(s4.x, s4.y),
-               f2(m4.x, m4.y), r2, sn, sd);
-    ssim_pair2(f2(__uint_as_float(v[j + 2]), __uint_as_float(v[j + 3])), f2(a4.z, a4.w), f2(s4.z, s4.w),
-               f2(m4.z, m4.w), r2, sn, sd);
+  for (int k = 0; k < 4; k++) {
+    const int row = quarter * 32 + rsub + 8 * k;
+    rc[k] = make_rowc<METRIC>(rs, row, ec);
+    rn[k] = rd[k] = f2(0.0f, 0.0f);
+    prow[k] = p0 + row;
+    force[k] = MASKED && rs[kBM + row] > 0.0f;
+  }
+#pragma unroll
+  for (int c = 0; c < CH; c++) {
+    const float4 cnv = cacc[(2 * c) * kEpiThreads], cdv = cacc[(2 * c + 1) * kEpiThreads];
+    F2 cn[2] = {f2(cnv.x, cnv.y), f2(cnv.z, cnv.w)};
+    F2 cd[2] = {f2(cdv.x, cdv.y), f2(cdv.z, cdv.w)};
+    const int cb = 16 * c + 4 * csub;
+    const float4 a4 = *reinterpret_cast<const float4*>(cs + cb);
+    float4 r4 = make_float4(0.f, 0.f, 0.f, 0.f), s4 = r4, m4 = r4;
+    if (METRIC == kPearson || METRIC == kDebugDot) r4 = *reinterpret_cast<const float4*>(cs + BN + cb);
+    if (METRIC == kSsim || METRIC == kNrmse || METRIC == kNrmseW)
+      s4 = *reinterpret_cast<const float4*>(cs + 2 * BN + cb);
+    if (METRIC == kSsim) m4 = *reinterpret_cast<const float4*>(cs + 3 * BN + cb);
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+      uint32_t cur[8];
+      tmem_ld8(taddr + ((uint32_t)(16 * half) << 16) + 16 * c, cur);
+      tmem_wait8(cur);
+      uint32_t near = 0;  // NRMSE: sign bits of (1 - delta) - G, any set = a near-identical pair
+#pragma unroll
+      for (int rep = 0; rep < 2; rep++) {
+        const F2 qa = rep ? f2(a4.z, a4.w) : f2(a4.x, a4.y);
+        const F2 qr = rep ? f2(r4.z, r4.w) : f2(r4.x, r4.y);
+        const F2 qs = rep ? f2(s4.z, s4.w) : f2(s4.x, s4.y);
+        const F2 qm = rep ? f2(m4.z, m4.w) : f2(m4.x, m4.y);
+        const int qlo = q0 + 16 * c + 8 * rep + 2 * csub;
+#pragma unroll
+        for (int kk = 0; kk < 2; kk++) {
+          const int k = 2 * half + kk;
+          float g0 = __uint_as_float(cur[4 * rep + 2 * kk]), g1 = __uint_as_float(cur[4 * rep + 2 * kk + 1]);
+          const int p = prow[k];
+          if (MASKED) {
+            if (force[k] && qlo == p) g0 = 1.0f;
+            if (force[k] && qlo + 1 == p) g1 = 1.0f;
+          }
+          F2 x, w;
+          terms2<METRIC, CMODE>(f2(g0, g1), rc[k], qa, qr, qs, qm, ec, x, w);
+          if (nrmse_tc<METRIC>()) {
+            float t0, t1;
+            f2_split(sub2(f2(ec.nrmse_near, ec.nrmse_near), f2(g0, g1)), t0, t1);
+            asm("lop3.b32 %0, %0, %1, %2, 0xFE;" : "+r"(near) : "r"(__float_as_uint(t0)), "r"(__float_as_uint(t1)));
+          }
+          if (!MASKED) {
+            if (weighted_num<METRIC>()) {
+              rn[k] = fma2(x, w, rn[k]);
+              cn[rep] = fma2(x, w, cn[rep]);
+            } else {
+              rn[k] = add2(rn[k], x);
+              cn[rep] = add2(cn[rep], x);
+            }
+            rd[k] = add2(rd[k], w);
+            cd[rep] = add2(cd[rep], w);
+          } else {
+            float x0, x1, w0, w1;
+            f2_split(weighted_num<METRIC>() ? mul2(x, w) : x, x0, x1);
+            f2_split(w, w0, w1);
+            const bool pv = p < ec.n;
+            const bool r0 = pv && qlo >= p && qlo < ec.n, r1 = pv && qlo + 1 >= p && qlo + 1 < ec.n;
+            const bool c0 = r0 && qlo != p, c1 = r1 && qlo + 1 != p;
+            rn[k] = add2(rn[k], f2(r0 ? x0 : 0.0f, r1 ? x1 : 0.0f));
+            rd[k] = add2(rd[k], f2(r0 ? w0 : 0.0f, r1 ? w1 : 0.0f));
+            cn[rep] = add2(cn[rep], f2(c0 ? x0 : 0.0f, c1 ? x1 : 0.0f));
+            cd[rep] = add2(cd[rep], f2(c0 ? w0 : 0.0f, c1 ? w1 : 0.0f));
+          }
+        }
+      }
+      if (nrmse_tc<METRIC>() && (int)near < 0) {
+        // Near-identical pairs: replace the accumulated term by the one of the
+        // exact squared difference (the same arithmetic as terms2 recomputes
+        // the term to remove).
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          const int rep = j >> 2, kk = (j >> 1) & 1, lh = j & 1;
+          const float g = __uint_as_float(cur[4 * rep + 2 * kk + lh]);
+          const int k = 2 * half + kk, row = quarter * 32 + rsub + 8 * k;
+          const int p = prow[k], q = q0 + 16 * c + 8 * rep + 2 * csub + lh;
+          const bool rv = !MASKED || (p < ec.n && q >= p && q < ec.n);
+          const bool cv = !MASKED || (rv && q != p);
+          float ge = g;
+          if (MASKED && force[k] && q == p) ge = 1.0f;
+          if (!(ge > ec.nrmse_near) || !rv) continue;
+          const float sp = rs[2 * kBM + row];
+          const int ci = 16 * c + 4 * csub + 2 * rep + lh;  // permuted column slot
+          const float sq = cs[2 * BN + ci];
+          const float ds = __fsub_rn(sp, sq);
+          const float approx = sqrtf(fmaxf(
+              __fmul_rn(ec.nrmse_scale, __fmaf_rn(ds, ds, __fmul_rn(__fmul_rn(2.0f * sp, sq), __fsub_rn(1.0f, ge)))),
+              0.0f));
+          const float D = (q == p) ? 0.0f : exact_diff2(ec.U + (size_t)p * ec.kp, ec.U + (size_t)q * ec.kp, ec.K);
+          const float exact = sqrtf(__fmul_rn(ec.nrmse_scale, __fmaf_rn(ds, ds, __fmul_rn(__fmul_rn(sp, sq), D))));
+          float corr = exact - approx;
+          if (METRIC == kNrmseW) {
+            const float d = __fsub_rn(rs[row], cs[ci]);
+            corr *= ex2_approx(-__fmul_rn(d, d));
+          }
+          f2_add_half(rn[k], lh, corr);
+          if (cv) f2_add_half(cn[rep], lh, corr);
+        }
+      }
+    }
+    float4 o;
+    f2_split(cn[0], o.x, o.y);
+    f2_split(cn[1], o.z, o.w);
+    cacc[(2 * c) * kEpiThreads] = o;
+    f2_split(cd[0], o.x, o.y);
+    f2_split(cd[1], o.z, o.w);
+    cacc[(2 * c + 1) * kEpiThreads] = o;
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    float lo, hi;
+    f2_split(rn[k], lo, hi);
+    rsum[2 * k] = lo + hi;
+    f2_split(rd[k], lo, hi);
+    rsum[2 * k + 1] = lo + hi;
   }
 }
 
-__device__ __forceinline__ void epi_tile_ssim2(uint32_t taddr, const float* __restrict__ soa, int cbase,
-                                               const SsimRow2& r2, float& sn_out, float& sd_out) {
-  uint32_t v0[16], v1[16];
-  F2 sn = f2(0.0f, 0.0f), sd = sn;
-  tmem_ld16(taddr, v0);
-  tmem_wait(v0);
-  tmem_ld16(taddr + 16, v1);
-  epi_chunk_ssim2(v0, soa, cbase, r2, sn, sd);
-  tmem_wait(v1);
-  tmem_ld16(taddr + 32, v0);
-  epi_chunk_ssim2(v1, soa, cbase + 16, r2, sn, sd);
-  tmem_wait(v0);
-  tmem_ld16(taddr + 48, v1);
-  epi_chunk_ssim2(v0, soa, cbase + 32, r2, sn, sd);
-  tmem_wait(v1);
-  epi_chunk_ssim2(v1, soa, cbase + 48, r2, sn, sd);
-  float a, b;
-  f2_split(sn, a, b);
-  sn_out += a + b;
-  f2_split(sd, a, b);
-  sd_out += a + b;
+// Row sums of the 4 lanes that share rows (lanes 4i..4i+3): x[2k + s] holds
+// row k's sum s; lane t ends with (num, den) of row k = 2 (t & 1) + ((t >> 1) & 1).
+__device__ __forceinline__ float2 reduce_rows4(const float (&x)[8]) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const bool b0 = lane & 1, b1 = lane & 2;
+  float y[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const float keep = b0 ? x[4 + i] : x[i], send = b0 ? x[i] : x[4 + i];
+    y[i] = keep + __shfl_xor_sync(full, send, 1);
+  }
+  float z[2];
+#pragma unroll
+  for (int i = 0; i < 2; i++) {
+    const float keep = b1 ? y[2 + i] : y[i], send = b1 ? y[i] : y[2 + i];
+    z[i] = keep + __shfl_xor_sync(full, send, 2);
+  }
+  return make_float2(z[0], z[1]);
 }
 
-template <int CMODE>
-__device__ __forceinline__ void epi_tile_pearson2(uint32_t taddr, const float* __restrict__ soa, int cbase,
-                                                  const PearsonRow2& r2, float& sn_out, float& sd_out) {
-  uint32_t v0[16], v1[16];
-  F2 sn = f2(0.0f, 0.0f), sd = sn;
-  tmem_ld16(taddr, v0);
-  tmem_wait(v0);
-  tmem_ld16(taddr + 16, v1);
-  epi_chunk_pearson2<CMODE>(v0, soa, cbase, r2, sn, sd);
-  tmem_wait(v1);
-  tmem_ld16(taddr + 32, v0);
-  epi_chunk_pearson2<CMODE>(v1, soa, cbase + 16, r2, sn, sd);
-  tmem_wait(v0);
-  tmem_ld16(taddr + 48, v1);
-  epi_chunk_pearson2<CMODE>(v0, soa, cbase + 32, r2, sn, sd);
-  tmem_wait(v1);
-  epi_chunk_pearson2<CMODE>(v1, soa, cbase + 48, r2, sn, sd);
-  float a, b;
-  f2_split(sn, a, b);
-  sn_out += a + b;
-  f2_split(sd, a, b);
-  sd_out += a + b;
+// Column sums of the 8 lanes that share columns (lanes with equal t % 4),
+// then one FP64 atomic add per column and sum. x index:
+// ((c * 2 + rep) * 2 + lohi) * 2 + sum, column 16c + 8rep + 2(t % 4) + lohi.
+template <int NV>
+__device__ __forceinline__ void flush_columns(const float (&x)[NV], int q0, const EpiConsts& ec, double* num,
+                                              double* den) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, csub = lane & 3;
+  const int b1 = (lane >> 2) & 1, b2 = (lane >> 3) & 1, b3 = (lane >> 4) & 1;
+  float y[NV / 2], z[NV / 4], u[NV / 8];
+#pragma unroll
+  for (int i = 0; i < NV / 2; i++) {
+    const float keep = b1 ? x[NV / 2 + i] : x[i], send = b1 ? x[i] : x[NV / 2 + i];
+    y[i] = keep + __shfl_xor_sync(full, send, 4);
+  }
+#pragma unroll
+  for (int i = 0; i < NV / 4; i++) {
+    const float keep = b2 ? y[NV / 4 + i] : y[i], send = b2 ? y[i] : y[NV / 4 + i];
+    z[i] = keep + __shfl_xor_sync(full, send, 8);
+  }
+#pragma unroll
+  for (int i = 0; i < NV / 8; i++) {
+    const float keep = b3 ? z[NV / 8 + i] : z[i], send = b3 ? z[i] : z[NV / 8 + i];
+    u[i] = keep + __shfl_xor_sync(full, send, 16);
+  }
+#pragma unroll
+  for (int j = 0; j < NV / 8; j++) {
+    const int i = b1 * (NV / 2) + b2 * (NV / 4) + b3 * (NV / 8) + j;
+    const int c = i >> 3, rep = (i >> 2) & 1, lohi = (i >> 1) & 1, s = i & 1;
+    const int q = q0 + 16 * c + 8 * rep + 2 * csub + lohi;
+    if (q < ec.n) atomicAdd((s ? den : num) + q, (double)u[j]);
+  }
 }
 
-// One warp's 64 columns of a tile in four 16-column chunks: each chunk's TMEM
-// load is in flight while the previous chunk is evaluated.
-template <int METRIC, int CMODE, bool FULL, bool DIAG>
-__device__ __forceinline__ void epi_tile(uint32_t taddr, const float* __restrict__ soa, int cbase, int col0, int row,
-                                         const RowState& rs, const EpiConsts& ec, float& sn, float& sd) {
-  uint32_t v0[16], v1[16];
-  tmem_ld16(taddr, v0);
-  tmem_wait(v0);
-  tmem_ld16(taddr + 16, v1);
-  epi_chunk<METRIC, CMODE, FULL, DIAG>(v0, soa, cbase, col0, row, rs, ec, sn, sd);
-  tmem_wait(v1);
-  tmem_ld16(taddr + 32, v0);
-  epi_chunk<METRIC, CMODE, FULL, DIAG>(v1, soa, cbase + 16, col0, row, rs, ec, sn, sd);
-  tmem_wait(v0);
-  tmem_ld16(taddr + 48, v1);
-  epi_chunk<METRIC, CMODE, FULL, DIAG>(v0, soa, cbase + 32, col0, row, rs, ec, sn, sd);
-  tmem_wait(v1);
-  epi_chunk<METRIC, CMODE, FULL, DIAG>(v1, soa, cbase + 48, col0, row, rs, ec, sn, sd);
+__host__ __device__ inline long long items_before(long long ct, int h) {
+  // sum over column tiles c < ct of ceil((c + 1) / h)
+  const long long Q = ct / h, R = ct - Q * h;
+  return (long long)h * Q * (Q + 1) / 2 + R * (Q + 1);
 }
 
-// TR (tile ring, K' <= 160): the B operand moves one whole 256-column tile at
-// a time through two buffers, and the single tcgen05.commit per tile both
-// publishes the accumulator and frees the tile's B buffer (the producer waits
-// on the accumulator barrier). Each mbarrier operation that follows a commit
-// stalls the MMA stream for ~100 cycles, so one commit-then-wait per tile
-// instead of one per K chunk is worth ~30% of MMA throughput. K' = 64 c + 32 t:
+// Item -> (column tile, row-block run); false for an empty run (rows past n).
+__device__ __forceinline__ bool decode_item(long long it, const TcArgs& g, int m, int& ct, int& rb0, int& rb1) {
+  int lo = 0, hi = g.n_ct - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (items_before(mid, g.h) <= it) lo = mid;
+    else hi = mid - 1;
+  }
+  ct = lo;
+  rb0 = (int)(it - items_before(lo, g.h)) * g.L;
+  rb1 = min(rb0 + g.L, min((lo + 1) * m, g.n_rb));
+  return rb0 < rb1;
+}
+
+// End of a role: all warps meet, then the MMA warp frees TMEM. Each role
+// calls it from its own code, so no code after the register split is shared
+// by warps of different register budgets.
+__device__ __forceinline__ void role_exit(uint32_t tmem, int tmem_cols, bool owner) {
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (owner) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols) : "memory");
+}
+
+// TR (whole-tile mode, when two A tiles and the B tile fit): A moves one
+// whole 128-row tile at a time through two buffers, and the single
+// tcgen05.commit per tile both publishes the accumulator and frees the tile's
+// A buffer (the producer waits on the accumulator barrier). K' = 64 c + 32 t:
 // c SWIZZLE_128B chunks and an optional SWIZZLE_64B tail.
-// !TR (chunk ring): B moves in 64-column chunks through S stages, one commit
-// per chunk; used when two whole tiles do not fit in shared memory.
-template <int METRIC, bool TR>
+// !TR (chunk ring): A moves in 64-column chunks through S stages, one commit
+// per chunk.
+template <int METRIC, int BN, bool TR>
 __global__ void __launch_bounds__(kThreads, 1)
     k_gram_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               const __grid_constant__ CUtensorMap tmA64, const __grid_constant__ CUtensorMap tmB64, TcArgs g) {
+  using C = Cfg<BN>;
+  constexpr int CH = C::kCH;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   uint8_t* sbase = smem_raw + (base - raw);
   const int S = g.stages, nkc = g.nkc;
-  const uint32_t sA = base;  // TR: a_bytes; else nkc x 16 KB
-  const uint32_t sB = sA + (TR ? g.a_bytes : nkc * kAChunkBytes);   // TR: 2 x b_bytes; else S x 32 KB
-  const uint32_t sP = sB + (TR ? 2 * g.b_bytes : S * kBStageBytes);  // kParSlots column-parameter slots
-  const float* slots = reinterpret_cast<const float*>(sbase + (sP - base));
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sbase + (sP - base) + kParSlots * kSoaBytes);
-  // barrier layout: full[S], empty[S], acc_full[2], acc_empty[2], par_full[4], par_empty[4],
-  //                 a_full, a_empty, done
-  const uint32_t b_full = smem_u32(bars), b_empty = b_full + 8 * S, b_accf = b_empty + 8 * S,
-                 b_acce = b_accf + 16, b_parf = b_acce + 16, b_pare = b_parf + 8 * kParSlots,
-                 b_afull = b_pare + 8 * kParSlots, b_aempty = b_afull + 8, b_done = b_aempty + 8;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 4 + 2 * kParSlots + 3);
+  const uint32_t sB = base;                                            // resident B tile
+  const uint32_t sA = sB + g.b_bytes;                                  // TR: 2 x a_bytes; else S x 16 KB
+  const uint32_t sC = sA + (TR ? 2 * g.a_bytes : S * kAChunkBytes);    // 2 column-parameter slots
+  const uint32_t sR = sC + 2 * C::kCSoa * 4;                           // kRSlots row-parameter slots
+  const uint32_t sP = sR + kRSlots * kRowFloats * 4;                   // row partials
+  const uint32_t sQ = sP + kRowPartBytes;                              // column accumulators
+  const uint32_t sBar = sQ + C::kColAccBytes;
+  const float* cslots = reinterpret_cast<const float*>(sbase + (sC - base));
+  const float* rslots = reinterpret_cast<const float*>(sbase + (sR - base));
+  float2* rowpart = reinterpret_cast<float2*>(sbase + (sP - base));
+  float4* colacc = reinterpret_cast<float4*>(sbase + (sQ - base));
+  // barriers: a_full[16], a_empty[16], b_full, b_empty, acc_full[2], acc_empty[2],
+  //           c_full[2], c_empty[2], r_full[4], r_empty[4], p_full[2][4], done
+  const uint32_t b_afull = sBar, b_aempty = b_afull + 8 * kMaxStages, b_bfull = b_aempty + 8 * kMaxStages,
+                 b_bempty = b_bfull + 8, b_accf = b_bempty + 8, b_acce = b_accf + 16, b_cfull = b_acce + 16,
+                 b_cempty = b_cfull + 16, b_rfull = b_cempty + 16, b_rempty = b_rfull + 8 * kRSlots,
+                 b_pfull = b_rempty + 8 * kRSlots, b_done = b_pfull + 64;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sbase + (b_done + 8 - base));
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < S; s++) {
-      mbar_init(b_full + 8 * s, 1);
-      mbar_init(b_empty + 8 * s, 1);
+    for (int s = 0; s < kMaxStages; s++) {
+      mbar_init(b_afull + 8 * s, 1);
+      mbar_init(b_aempty + 8 * s, 1);
     }
+    mbar_init(b_bfull, 1);
+    mbar_init(b_bempty, 1);
     for (int b = 0; b < 2; b++) {
       mbar_init(b_accf + 8 * b, 1);
       mbar_init(b_acce + 8 * b, kEpiWarps);
+      mbar_init(b_cfull + 8 * b, 1);
+      mbar_init(b_cempty + 8 * b, kEpiWarps);
     }
-    for (int p = 0; p < kParSlots; p++) {
-      mbar_init(b_parf + 8 * p, 1);
-      mbar_init(b_pare + 8 * p, kEpiWarps);
+    for (int r = 0; r < kRSlots; r++) {
+      mbar_init(b_rfull + 8 * r, 1);
+      mbar_init(b_rempty + 8 * r, kEpiWarps);
     }
-    mbar_init(b_afull, 1);
-    mbar_init(b_aempty, 1);
+    for (int i = 0; i < 8; i++) mbar_init(b_pfull + 8 * i, 4);
     mbar_init(b_done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == kEpiWarps + 1) {  // MMA warp owns the TMEM allocation
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(2 * kBN)
+                 "r"(2 * BN)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -396,51 +639,55 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == kEpiWarps) {
     // ---------------------------------------------------------------- TMA
     if (lane == 0) {
-      uint32_t it = 0, item_i = 0, ptile = 0;
-      uint32_t s = 0, eph = 0;  // B ring: stage, parity of the round being refilled
-      bool ok = true, a_issued = false;
-      for (int item = blockIdx.x; ok && item < g.n_items; item += gridDim.x, item_i++) {
-        const int rb = g.rb0 + item % g.n_rb, seg = item / g.n_rb;
-        const int ct0 = seg * g.ct_per_item, ct1 = min(ct0 + g.ct_per_item, g.n_ct);
-        if (!mbar_wait(b_aempty, (item_i & 1) ^ 1, g.status, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
-        if (TR) {
-          mbar_expect_tx(b_afull, g.a_bytes);
-          for (int c = 0; c < g.nfull; c++) tma_load_2d(sA + c * kAChunkBytes, &tmA, b_afull, c * kChunk, rb * kBM);
-          if (g.tail) tma_load_2d(sA + g.nfull * kAChunkBytes, &tmA64, b_afull, g.nfull * kChunk, rb * kBM);
-        } else {
-          mbar_expect_tx(b_afull, nkc * kAChunkBytes);
-          for (int kc = 0; kc < nkc; kc++) tma_load_2d(sA + kc * kAChunkBytes, &tmA, b_afull, kc * kChunk, rb * kBM);
-        }
-        a_issued = true;
-        for (int ct = ct0; ok && ct < ct1; ct++, ptile++) {
-          // the tile's column parameters, into the slot the epilogue released four tiles ago
-          const uint32_t ps = ptile & (kParSlots - 1);
-          if (!mbar_wait(b_pare + 8 * ps, ((ptile / kParSlots) & 1) ^ 1, g.status, ST_TIMEOUT_PRODUCER)) {
+      long long tile = 0;
+      uint32_t item_i = 0, n_r = 0, n_a = 0;  // items, row-parameter loads, A loads (tiles or chunks) issued
+      uint32_t s = 0, eph = 0;                // chunk ring: stage, parity of the round being refilled
+      bool ok = true;
+      for (long long it = g.item0 + blockIdx.x; ok && it < g.item1; it += gridDim.x) {
+        int ct, rb0, rb1;
+        if (!decode_item(it, g, C::kM, ct, rb0, rb1)) continue;
+        const uint32_t cs = item_i & 1;
+        // the column-parameter slot the epilogue released two items ago, and the
+        // B buffer once the MMAs of the previous item are complete
+        if (!mbar_wait(b_cempty + 8 * cs, ((item_i >> 1) & 1) ^ 1, g, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
+        if (item_i > 0 && !mbar_wait(b_bempty, (item_i - 1) & 1, g, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
+        mbar_expect_tx(b_cfull + 8 * cs, C::kCSoa * 4);
+        bulk_load(sC + cs * C::kCSoa * 4, g.colsoa + (size_t)ct * C::kCSoa, C::kCSoa * 4, b_cfull + 8 * cs);
+        mbar_expect_tx(b_bfull, g.b_bytes);
+        for (int c = 0; c < g.nfull; c++) tma_load_2d(sB + c * C::kBChunkBytes, &tmB, b_bfull, c * kChunk, ct * BN);
+        if (g.tail) tma_load_2d(sB + g.nfull * C::kBChunkBytes, &tmB64, b_bfull, g.nfull * kChunk, ct * BN);
+        item_i++;
+        for (int rb = rb0; ok && rb < rb1; rb++, tile++) {
+          if (tile == g.withhold) { ok = false; break; }
+          const uint32_t rsl = (uint32_t)(tile & (kRSlots - 1));
+          if (!mbar_wait(b_rempty + 8 * rsl, ((tile / kRSlots) & 1) ^ 1, g, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
+          // TR: A buffer tile & 1 is free once the accumulator of tile - 2 is published
+          if (TR && tile >= 2 && !mbar_wait(b_accf + 8 * (tile & 1), ((tile - 2) >> 1) & 1, g, ST_TIMEOUT_PRODUCER)) {
             ok = false;
             break;
           }
-          // TR: B buffer ptile & 1 is free once the accumulator of tile ptile - 2
-          // is published. Both waits come before any copy of this tile is issued.
-          if (TR && !mbar_wait(b_accf + 8 * (ptile & 1), ((ptile >> 1) & 1) ^ 1, g.status, ST_TIMEOUT_PRODUCER)) {
-            ok = false;
-            break;
-          }
-          mbar_expect_tx(b_parf + 8 * ps, kSoaBytes);
-          bulk_load(sP + ps * kSoaBytes, g.colsoa + (size_t)ct * kColSoaFloats, kSoaBytes, b_parf + 8 * ps);
+          mbar_expect_tx(b_rfull + 8 * rsl, kRowFloats * 4);
+          bulk_load(sR + rsl * kRowFloats * 4, g.rowsoa + (size_t)rb * kRowFloats, kRowFloats * 4, b_rfull + 8 * rsl);
+          n_r++;
           if (TR) {
-            const uint32_t b = ptile & 1;
-            const uint32_t dst = sB + b * g.b_bytes;
-            mbar_expect_tx(b_full + 8 * b, g.b_bytes);
-            for (int c = 0; c < g.nfull; c++)
-              tma_load_2d(dst + c * kBStageBytes, &tmB, b_full + 8 * b, c * kChunk, ct * kBN);
-            if (g.tail) tma_load_2d(dst + g.nfull * kBStageBytes, &tmB64, b_full + 8 * b, g.nfull * kChunk, ct * kBN);
-            it++;
+            const uint32_t ab = (uint32_t)(tile & 1);
+            const uint32_t dst = sA + ab * g.a_bytes;
+            mbar_expect_tx(b_afull + 8 * ab, g.a_bytes);
+            for (int c = 0; c < g.nfull; c++) tma_load_2d(dst + c * kAChunkBytes, &tmA, b_afull + 8 * ab, c * kChunk, rb * kBM);
+            if (g.tail) tma_load_2d(dst + g.nfull * kAChunkBytes, &tmA64, b_afull + 8 * ab, g.nfull * kChunk, rb * kBM);
+            n_a++;
             continue;
           }
-          for (int kc = 0; kc < nkc; kc++, it++) {
-            if (!mbar_wait(b_empty + 8 * s, eph ^ 1, g.status, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
-            mbar_expect_tx(b_full + 8 * s, kBStageBytes);
-            tma_load_2d(sB + s * kBStageBytes, &tmB, b_full + 8 * s, kc * kChunk, ct * kBN);
+          for (int kc = 0; kc < nkc; kc++) {
+            if (!mbar_wait(b_aempty + 8 * s, eph ^ 1, g, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
+            if (kc < g.nfull) {
+              mbar_expect_tx(b_afull + 8 * s, kAChunkBytes);
+              tma_load_2d(sA + s * kAChunkBytes, &tmA, b_afull + 8 * s, kc * kChunk, rb * kBM);
+            } else {  // the 32-column tail
+              mbar_expect_tx(b_afull + 8 * s, kAChunkBytes / 2);
+              tma_load_2d(sA + s * kAChunkBytes, &tmA64, b_afull + 8 * s, kc * kChunk, rb * kBM);
+            }
+            n_a++;
             if (++s == (uint32_t)S) {
               s = 0;
               eph ^= 1;
@@ -448,71 +695,76 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
         }
       }
-      // Drain: every issued copy has landed before the CTA may exit (TR: `it`
-      // counts whole-tile loads through S = 2 buffers).
-      for (uint32_t k = (it > (uint32_t)S ? it - S : 0); k < it; k++)
-        mbar_wait(b_full + 8 * (k % S), (k / S) & 1, g.status, ST_TIMEOUT_DRAIN, false);
-      for (uint32_t k = (ptile > (uint32_t)kParSlots ? ptile - kParSlots : 0); k < ptile; k++)
-        mbar_wait(b_parf + 8 * (k % kParSlots), (k / kParSlots) & 1, g.status, ST_TIMEOUT_DRAIN, false);
-      // item_i - 1 is the last item whose A tile was issued (a failed wait
-      // leaves item_i at the item it was waiting for)
-      if (a_issued) mbar_wait(b_afull, (item_i - 1) & 1, g.status, ST_TIMEOUT_DRAIN, false);
+      // Drain: every issued copy has landed before the CTA may exit.
+      if (item_i > 0) {
+        mbar_wait(b_bfull, (item_i - 1) & 1, g, ST_TIMEOUT_DRAIN, false);
+        for (uint32_t k = (item_i > 2 ? item_i - 2 : 0); k < item_i; k++)
+          mbar_wait(b_cfull + 8 * (k & 1), (k >> 1) & 1, g, ST_TIMEOUT_DRAIN, false);
+      }
+      for (uint32_t k = (n_r > (uint32_t)kRSlots ? n_r - kRSlots : 0); k < n_r; k++)
+        mbar_wait(b_rfull + 8 * (k % kRSlots), (k / kRSlots) & 1, g, ST_TIMEOUT_DRAIN, false);
+      const uint32_t ring = TR ? 2u : (uint32_t)S;
+      for (uint32_t k = (n_a > ring ? n_a - ring : 0); k < n_a; k++)
+        mbar_wait(b_afull + 8 * (k % ring), (k / ring) & 1, g, ST_TIMEOUT_DRAIN, false);
     }
     __syncwarp();
+    role_exit(tmem, 2 * BN, false);
+    return;
   } else if (warp == kEpiWarps + 1) {
     // ---------------------------------------------------------------- MMA
     if (lane == 0) {
-      uint32_t tile = 0, item_i = 0;
-      uint32_t s = 0, fph = 0;  // B ring: stage, parity of the round being consumed
+      long long tile = 0;
+      uint32_t item_i = 0;
+      uint32_t s = 0, fph = 0;  // chunk ring: stage, parity of the round being consumed
       // Operand descriptors: the start-address field counts 16-byte units, so
       // a K step of 16 bf16 (32 B) adds 2 and a chunk or stage adds its size / 16.
       const uint64_t a_desc0 = desc_sw128(sA), b_desc0 = desc_sw128(sB);
-      const int last_nks = (g.kq - (nkc - 1) * kChunk) / 16;
       bool ok = true;
-      for (int item = blockIdx.x; ok && item < g.n_items; item += gridDim.x, item_i++) {
-        const int seg = item / g.n_rb;
-        const int ct0 = seg * g.ct_per_item, ct1 = min(ct0 + g.ct_per_item, g.n_ct);
-        if (!mbar_wait(b_afull, item_i & 1, g.status, ST_TIMEOUT_MMA)) { ok = false; break; }
+      for (long long it = g.item0 + blockIdx.x; ok && it < g.item1; it += gridDim.x) {
+        int ct, rb0, rb1;
+        if (!decode_item(it, g, C::kM, ct, rb0, rb1)) continue;
+        if (!mbar_wait(b_bfull, item_i & 1, g, ST_TIMEOUT_MMA)) { ok = false; break; }
         tc_fence_after();
-        for (int ct = ct0; ok && ct < ct1; ct++, tile++) {
-          const uint32_t b = tile & 1;
-          if (!mbar_wait(b_acce + 8 * b, ((tile >> 1) & 1) ^ 1, g.status, ST_TIMEOUT_MMA)) { ok = false; break; }
+        item_i++;
+        for (int rb = rb0; ok && rb < rb1; rb++, tile++) {
+          const uint32_t b = (uint32_t)(tile & 1);
+          if (!mbar_wait(b_acce + 8 * b, ((tile >> 1) & 1) ^ 1, g, ST_TIMEOUT_MMA)) { ok = false; break; }
           tc_fence_after();
-          const uint32_t d = tmem + b * kBN;
+          const uint32_t d = tmem + b * BN;
           if (TR) {
-            if (!mbar_wait(b_full + 8 * b, (tile >> 1) & 1, g.status, ST_TIMEOUT_MMA)) { ok = false; break; }
+            if (!mbar_wait(b_afull + 8 * b, (tile >> 1) & 1, g, ST_TIMEOUT_MMA)) { ok = false; break; }
             tc_fence_after();
-            const uint64_t db0 = b_desc0 + (uint64_t)((b * g.b_bytes) >> 4);
+            const uint64_t da0 = a_desc0 + (uint64_t)((b * g.a_bytes) >> 4);
             for (int c = 0; c < g.nfull; c++) {
 #pragma unroll
               for (int ks = 0; ks < kChunk / 16; ks++)
-                mma_bf16(d, a_desc0 + (uint64_t)(c * (kAChunkBytes >> 4) + 2 * ks),
-                         db0 + (uint64_t)(c * (kBStageBytes >> 4) + 2 * ks), (c | ks) != 0);
+                mma_bf16<BN>(d, da0 + (uint64_t)(c * (kAChunkBytes >> 4) + 2 * ks),
+                             b_desc0 + (uint64_t)(c * (C::kBChunkBytes >> 4) + 2 * ks), (c | ks) != 0);
             }
             if (g.tail) {
-              const uint64_t da = desc_sw64(sA + g.nfull * kAChunkBytes);
-              const uint64_t db = desc_sw64(sB + b * g.b_bytes + g.nfull * kBStageBytes);
-              mma_bf16(d, da, db, g.nfull != 0);
-              mma_bf16(d, da + 2, db + 2, 1);
+              const uint64_t da = desc_sw64(sA + b * g.a_bytes + g.nfull * kAChunkBytes);
+              const uint64_t db = desc_sw64(sB + g.nfull * C::kBChunkBytes);
+              mma_bf16<BN>(d, da, db, g.nfull != 0);
+              mma_bf16<BN>(d, da + 2, db + 2, 1);
             }
             mma_commit(b_accf + 8 * b);
             continue;
           }
-          uint64_t da = a_desc0;
           for (int kc = 0; kc < nkc; kc++) {
-            if (!mbar_wait(b_full + 8 * s, fph, g.status, ST_TIMEOUT_MMA)) { ok = false; break; }
+            if (!mbar_wait(b_afull + 8 * s, fph, g, ST_TIMEOUT_MMA)) { ok = false; break; }
             tc_fence_after();
-            const uint64_t db = b_desc0 + (uint64_t)(s * (kBStageBytes >> 4));
-            if (kc + 1 < nkc) {
+            if (kc < g.nfull) {
+              const uint64_t da = a_desc0 + (uint64_t)(s * (kAChunkBytes >> 4));
+              const uint64_t db = b_desc0 + (uint64_t)(kc * (C::kBChunkBytes >> 4));
 #pragma unroll
-              for (int ks = 0; ks < kChunk / 16; ks++) mma_bf16(d, da + 2 * ks, db + 2 * ks, (kc | ks) != 0);
+              for (int ks = 0; ks < kChunk / 16; ks++) mma_bf16<BN>(d, da + 2 * ks, db + 2 * ks, (kc | ks) != 0);
             } else {
-#pragma unroll
-              for (int ks = 0; ks < kChunk / 16; ks++)
-                if (ks < last_nks) mma_bf16(d, da + 2 * ks, db + 2 * ks, (kc | ks) != 0);
+              const uint64_t da = desc_sw64(sA + s * kAChunkBytes);
+              const uint64_t db = desc_sw64(sB + g.nfull * C::kBChunkBytes);
+              mma_bf16<BN>(d, da, db, kc != 0);
+              mma_bf16<BN>(d, da + 2, db + 2, 1);
             }
-            mma_commit(b_empty + 8 * s);
-            da += kAChunkBytes >> 4;
+            mma_commit(b_aempty + 8 * s);
             if (++s == (uint32_t)S) {
               s = 0;
               fph ^= 1;
@@ -520,81 +772,148 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           if (ok) mma_commit(b_accf + 8 * b);
         }
-        if (ok) mma_commit(b_aempty);
+        if (ok) mma_commit(b_bempty);  // the item's B tile is free once these MMAs complete
       }
       // All MMAs this thread issued are complete before TMEM is released and
       // the CTA exits.
       mma_commit(b_done);
-      mbar_wait(b_done, 0, g.status, ST_TIMEOUT_DRAIN, false);
+      mbar_wait(b_done, 0, g, ST_TIMEOUT_DRAIN, false);
     }
     __syncwarp();
+    role_exit(tmem, 2 * BN, true);
+    return;
   } else {
     // ---------------------------------------------------------------- epilogue
     const int quarter = warp & 3, group = warp >> 2;
-    const int cbase = group * kColsPerWarp;
-    uint32_t tile = 0;
+    long long tile = 0;
+    uint32_t item_i = 0;
     bool ok = true;
-    for (int item = blockIdx.x; ok && item < g.n_items; item += gridDim.x) {
-      const int rb = g.rb0 + item % g.n_rb, seg = item / g.n_rb;
-      const int ct0 = seg * g.ct_per_item, ct1 = min(ct0 + g.ct_per_item, g.n_ct);
-      const int row = rb * kBM + quarter * 32 + lane;
-      const RowState rs = make_row(g.params[row], g.ec);
-      const PearsonRow2 r2 = make_pearson_row2(rs);
-      const SsimRow2 s2 = make_ssim_row2(rs, g.ec);
-      const float rmax_r = g.tile_rmax[rb];
-      double acc_n = 0.0, acc_d = 0.0;
-      for (int ct = ct0; ok && ct < ct1; ct++, tile++) {
-        const uint32_t b = tile & 1, par = (tile >> 1) & 1;
-        const uint32_t ps = tile & (kParSlots - 1), pph = (tile / kParSlots) & 1;
-        if (!mbar_wait(b_parf + 8 * ps, pph, g.status, ST_TIMEOUT_EPI) ||
-            !mbar_wait(b_accf + 8 * b, par, g.status, ST_TIMEOUT_EPI)) {
+    for (long long it = g.item0 + blockIdx.x; ok && it < g.item1; it += gridDim.x) {
+      int ct, rb0, rb1;
+      if (!decode_item(it, g, C::kM, ct, rb0, rb1)) continue;
+      const uint32_t cs = item_i & 1;
+      if (!mbar_wait(b_cfull + 8 * cs, (item_i >> 1) & 1, g, ST_TIMEOUT_EPI)) { ok = false; break; }
+      item_i++;
+      const float* csl = cslots + cs * C::kCSoa;
+      const float rmax_c = csl[4 * BN];
+      const int q0 = ct * BN + group * C::kColW;
+      const bool full = ct * BN + BN <= g.ec.n;
+      float4* cacc = colacc + threadIdx.x;
+#pragma unroll
+      for (int j = 0; j < 2 * CH; j++) cacc[j * kEpiThreads] = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int rb = rb0; ok && rb < rb1; rb++, tile++) {
+        const uint32_t b = (uint32_t)(tile & 1);
+        const uint32_t rsl = (uint32_t)(tile & (kRSlots - 1));
+        if (!mbar_wait(b_rfull + 8 * rsl, (tile / kRSlots) & 1, g, ST_TIMEOUT_EPI) ||
+            !mbar_wait(b_accf + 8 * b, (tile >> 1) & 1, g, ST_TIMEOUT_EPI)) {
           ok = false;
           break;
         }
         tc_fence_after();
-        const float* soa = slots + ps * kColSoaFloats;
-        const int col0 = ct * kBN;
-        const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + b * kBN + cbase;
-        const int cm = METRIC == kPearson ? c_mode(kEps * rmax_r * soa[4 * kBN]) : kCFirst;
-        const bool full = col0 + kBN <= g.ec.n;
-        const bool diag = (ct == (rb >> 1));
-        float sn = 0.0f, sd = 0.0f;
-        if (METRIC == kPearson && full && !diag && cm == kCFirst)
-          epi_tile_pearson2<kCFirst>(taddr, soa, cbase, r2, sn, sd);
-        else if (METRIC == kPearson && full && !diag && cm == kCSecond)
-          epi_tile_pearson2<kCSecond>(taddr, soa, cbase, r2, sn, sd);
-        else if (METRIC == kSsim && full && !diag)
-          epi_tile_ssim2(taddr, soa, cbase, s2, sn, sd);
-        else if (full && !diag && cm == kCFirst)
-          epi_tile<METRIC, kCFirst, true, false>(taddr, soa, cbase, col0, row, rs, g.ec, sn, sd);
-        else if (full && !diag && cm == kCSecond)
-          epi_tile<METRIC, kCSecond, true, false>(taddr, soa, cbase, col0, row, rs, g.ec, sn, sd);
+        const float* rsp = rslots + rsl * kRowFloats;
+        const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + b * BN + group * C::kColW;
+        const int p0 = rb * kBM;
+        const bool masked = !full || ct * BN <= p0 + kBM - 1;
+        const int cm = METRIC == kPearson ? c_mode(kEps * rsp[4 * kBM] * rmax_c) : kCFirst;
+        const float* csw = csl + group * C::kColW;
+        float rsum[8];
+        if (masked)
+          sym_tile<METRIC, BN, kCExact, true>(taddr, rsp, csw, cacc, p0, q0, g.ec, rsum);
         else if (cm == kCFirst)
-          epi_tile<METRIC, kCFirst, false, true>(taddr, soa, cbase, col0, row, rs, g.ec, sn, sd);
-        else if (cm == kCSecond)
-          epi_tile<METRIC, kCSecond, false, true>(taddr, soa, cbase, col0, row, rs, g.ec, sn, sd);
+          sym_tile<METRIC, BN, kCFirst, false>(taddr, rsp, csw, cacc, p0, q0, g.ec, rsum);
+        else if (METRIC == kPearson && cm == kCSecond)
+          sym_tile<METRIC, BN, kCSecond, false>(taddr, rsp, csw, cacc, p0, q0, g.ec, rsum);
         else
-          epi_tile<METRIC, kCExact, false, true>(taddr, soa, cbase, col0, row, rs, g.ec, sn, sd);
+          sym_tile<METRIC, BN, kCExact, false>(taddr, rsp, csw, cacc, p0, q0, g.ec, rsum);
         tc_fence_before();
         __syncwarp();
         if (lane == 0) {
           mbar_arrive(b_acce + 8 * b);
-          mbar_arrive(b_pare + 8 * ps);
+          mbar_arrive(b_rempty + 8 * rsl);
         }
-        acc_n += (double)sn;
-        acc_d += (double)sd;
+        // Row sums: 4 lanes per row, then the 4 column-group warps of this
+        // quarter through shared memory (fixed order), one atomic per row.
+        const float2 z = reduce_rows4(rsum);
+        const int krow = 2 * (lane & 1) + ((lane >> 1) & 1);
+        float2* rp = rowpart + b * (4 * kBM);
+        rp[group * kBM + quarter * 32 + (lane >> 2) + 8 * krow] = z;
+        __syncwarp();
+        const uint32_t pbar = b_pfull + 8 * (b * 4 + quarter);
+        if (lane == 0) mbar_arrive(pbar);
+        if (!mbar_wait(pbar, (tile >> 1) & 1, g, ST_TIMEOUT_EPI)) {
+          ok = false;
+          break;
+        }
+        if (lane < 16) {
+          const int row = quarter * 32 + group * 8 + (lane & 7);
+          const int sidx = lane >> 3;
+          float s = 0.0f;
+#pragma unroll
+          for (int gg = 0; gg < 4; gg++) {
+            const float2 v = rp[gg * kBM + row];
+            s += sidx ? v.y : v.x;
+          }
+          const int p = p0 + row;
+          if (p < g.ec.n) atomicAdd((sidx ? g.den : g.num) + p, (double)s);
+        }
       }
-      if (ok && row < g.ec.n) {
-        atomicAdd(g.num + row, acc_n);
-        atomicAdd(g.den + row, acc_d);
+      if (!ok) break;
+      // Column sums of the item.
+      float x[8 * CH];
+#pragma unroll
+      for (int c = 0; c < CH; c++) {
+        const float4 nv = cacc[(2 * c) * kEpiThreads], dv = cacc[(2 * c + 1) * kEpiThreads];
+        const float ns[4] = {nv.x, nv.y, nv.z, nv.w}, ds[4] = {dv.x, dv.y, dv.z, dv.w};
+#pragma unroll
+        for (int r = 0; r < 2; r++)
+#pragma unroll
+          for (int lh = 0; lh < 2; lh++) {
+            const int i = ((c * 2 + r) * 2 + lh) * 2;
+            x[i] = ns[2 * r + lh];
+            x[i + 1] = ds[2 * r + lh];
+          }
       }
+      flush_columns<8 * CH>(x, q0, g.ec, g.num, g.den);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(b_cempty + 8 * cs);
     }
+    role_exit(tmem, 2 * BN, false);
   }
-  tc_fence_before();
+}
+
+// Column parameters of each BN-column tile, permuted so that thread t of an
+// epilogue warp finds its four columns of a 16-column chunk (2(t%4) + {0, 1}
+// and 8 + 2(t%4) + {0, 1}) in one float4 (col_soa_pos), with the tile's
+// largest 1/sigma; and the row parameters of each 128-row block in natural
+// order with the block's largest 1/sigma. Blocks [0, n_ctp): column tiles;
+// [n_ctp, n_ctp + n_rbp): row blocks.
+template <int BN>
+__global__ void k_sym_soa(const BlockParams* __restrict__ params, int n_ctp, float* __restrict__ colsoa,
+                          float* __restrict__ rowsoa) {
+  const int i = threadIdx.x;
+  __shared__ float wm[8];
+  const bool col = blockIdx.x < n_ctp;
+  const int width = col ? BN : kBM;
+  const int tile = col ? blockIdx.x : blockIdx.x - n_ctp;
+  float* o = col ? colsoa + (size_t)tile * col_soa_floats(BN) : rowsoa + (size_t)tile * kRowSoaFloats;
+  float r = 0.0f;
+  if (i < width) {
+    const BlockParams p = params[(size_t)tile * width + i];
+    const int pos = col ? col_soa_pos(i) : i;
+    o[pos] = p.a;
+    o[width + pos] = p.r;
+    o[2 * width + pos] = p.sigma;
+    o[3 * width + pos] = p.mu;
+    r = p.r;
+  }
+  for (int s = 16; s; s >>= 1) r = fmaxf(r, __shfl_xor_sync(0xffffffffu, r, s));
+  if ((i & 31) == 0) wm[i >> 5] = r;
   __syncthreads();
-  tc_fence_after();
-  if (warp == kEpiWarps + 1) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kBN) : "memory");
+  if (i < 4) {
+    float m = 0.0f;
+    if (i == 0)
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = fmaxf(m, wm[w]);
+    o[4 * width + i] = m;
   }
 }
 
@@ -625,80 +944,118 @@ bool make_map(CUtensorMap* m, const __nv_bfloat16* ptr, int kq, int rows, int bo
   return r == CUDA_SUCCESS;
 }
 
+size_t fixed_smem(int bn) {
+  return 1024 + 2 * (size_t)col_soa_floats(bn) * 4 + kRSlots * kRowFloats * 4 + kRowPartBytes +
+         (size_t)kEpiThreads * 8 * (bn / 64) * 4 + kBarBytes;
+}
+
 }  // namespace
 
+bool plan_gram_tc(int kq, TcPlan* p) {
+  if (kq <= 0 || kq % 32 != 0) return false;
+  for (int bn : {256, 128}) {
+    const size_t fixed = fixed_smem(bn);
+    const size_t a_bytes = (size_t)kBM * kq * 2, b_bytes = (size_t)bn * kq * 2;
+    // whole-tile mode: two A tiles beside the B tile
+    if (fixed + 2 * a_bytes + b_bytes <= kSmemBudget) {
+      *p = TcPlan{bn, true, 2, fixed + 2 * a_bytes + b_bytes};
+      return true;
+    }
+    // chunk ring: at least three 16 KB A stages beside the B tile
+    if (fixed + b_bytes + 3 * kAChunkBytes <= kSmemBudget) {
+      const int st = (int)std::min<size_t>(kMaxStages, (kSmemBudget - fixed - b_bytes) / kAChunkBytes);
+      *p = TcPlan{bn, false, st, fixed + b_bytes + (size_t)st * kAChunkBytes};
+      return true;
+    }
+  }
+  return false;
+}
+
+size_t gram_tc_soa_floats(int n_pad) {
+  // column tiles of 128 or 256 blocks plus one row-parameter block per 128 rows
+  return (size_t)(n_pad / 128) * col_soa_floats(128) + (size_t)(n_pad / 128) * kRowSoaFloats;
+}
+
+long long gram_tc_items(int n, int bn, int* L_out, int num_sms) {
+  const int m = bn / kBM;
+  const int n_ct = (n + bn - 1) / bn;
+  int L = 16;
+  while (L > 2 && items_before(n_ct, L / m) < 4LL * num_sms) L >>= 1;
+  if (L < m) L = m;
+  if (L_out) *L_out = L;
+  return items_before(n_ct, L / m);
+}
+
 cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int kq, int n_pad,
-                           const BlockParams* params, const float* colsoa, const float* tile_rmax, EpiConsts ec,
-                           double* num, double* den, int num_sms, int* status, cudaStream_t st, int rb_begin,
-                           int rb_end) {
-  if (kq % 16 != 0 || n_pad % kBN != 0) return cudaErrorInvalidValue;
+                           const BlockParams* params, float* soa_ws, EpiConsts ec, double* num, double* den,
+                           int num_sms, int* status, cudaStream_t st, int shard, int n_shards,
+                           const TcDebug* dbg) {
+  TcPlan plan;
+  if (!plan_gram_tc(kq, &plan) || n_pad % 256 != 0 || n_shards < 1 || shard < 0 || shard >= n_shards)
+    return cudaErrorInvalidValue;
+  if (ec.n <= 0) return cudaSuccess;
+  const int bn = plan.bn;
   TcArgs g;
   g.kq = kq;
-  g.nkc = (kq + kChunk - 1) / kChunk;
-  g.n_ct = (ec.n + kBN - 1) / kBN;
-  const size_t budget = 227 * 1024;
+  g.nkc = (kq + kChunk - 1) / kChunk;  // nfull + tail
+  g.stages = plan.stages;
   g.nfull = kq / kChunk;
   g.tail = (kq % kChunk) ? 1 : 0;
   g.a_bytes = (uint32_t)kBM * kq * 2;
-  g.b_bytes = (uint32_t)kBN * kq * 2;
-  const size_t tr_smem = 1024 + (size_t)g.a_bytes + 2 * (size_t)g.b_bytes + kParSlots * kSoaBytes + 8 * 64;
-  const bool tr = (kq % (kChunk / 2) == 0) && tr_smem <= budget;
-  size_t smem;
-  if (tr) {
-    g.stages = 2;
-    smem = tr_smem;
-  } else {
-    const size_t fixed = 1024 + (size_t)g.nkc * kAChunkBytes + kParSlots * kSoaBytes + 8 * 64;
-    if (fixed + 2 * kBStageBytes > budget) return cudaErrorInvalidValue;
-    g.stages = (int)std::min<size_t>(kMaxStages, (budget - fixed) / kBStageBytes);
-    smem = fixed + (size_t)g.stages * kBStageBytes;
-  }
-  // Only row blocks that hold valid rows are work; split the column range so
-  // that every SM gets several items.
-  int n_rb_valid = (ec.n + kBM - 1) / kBM;
-  if (rb_end < 0) rb_end = n_rb_valid;
-  rb_end = std::min(rb_end, n_rb_valid);
-  if (rb_begin < 0 || rb_begin >= rb_end) return cudaSuccess;  // no rows in this range
-  g.rb0 = rb_begin;
-  n_rb_valid = rb_end - rb_begin;
-  int segs = (4 * num_sms + n_rb_valid - 1) / n_rb_valid;
-  segs = std::max(1, std::min(segs, g.n_ct));
-  g.ct_per_item = (g.n_ct + segs - 1) / segs;
-  segs = (g.n_ct + g.ct_per_item - 1) / g.ct_per_item;
-  g.n_rb = n_rb_valid;
-  g.n_items = g.n_rb * segs;
-  g.params = params;
+  g.b_bytes = (uint32_t)bn * kq * 2;
+  g.n_rb = (ec.n + kBM - 1) / kBM;
+  g.n_ct = (ec.n + bn - 1) / bn;
+  int L;
+  const long long items = gram_tc_items(ec.n, bn, &L, num_sms);
+  g.L = L;
+  g.h = L / (bn / kBM);
+  g.item0 = items * shard / n_shards;
+  g.item1 = items * (shard + 1) / n_shards;
+  const int n_ctp = n_pad / bn, n_rbp = n_pad / kBM;
+  float* colsoa = soa_ws;
+  float* rowsoa = soa_ws + (size_t)n_ctp * col_soa_floats(bn);
   g.colsoa = colsoa;
-  g.tile_rmax = tile_rmax;
+  g.rowsoa = rowsoa;
   g.ec = ec;
   g.num = num;
   g.den = den;
   g.status = status;
+  g.timeout_ns = dbg && dbg->timeout_ns ? dbg->timeout_ns : 4000000000ull;
+  g.withhold = dbg ? dbg->withhold_tile : -1;
+  if (bn == 256) k_sym_soa<256><<<n_ctp + n_rbp, 256, 0, st>>>(params, n_ctp, colsoa, rowsoa);
+  else k_sym_soa<128><<<n_ctp + n_rbp, 256, 0, st>>>(params, n_ctp, colsoa, rowsoa);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (g.item0 >= g.item1) return cudaSuccess;
   CUtensorMap mA, mB, mA64, mB64;
-  if (!make_map(&mA, A, kq, n_pad, kBM) || !make_map(&mB, B, kq, n_pad, kBN)) return cudaErrorInvalidValue;
+  if (!make_map(&mA, A, kq, n_pad, kBM) || !make_map(&mB, B, kq, n_pad, bn)) return cudaErrorInvalidValue;
   mA64 = mA;
   mB64 = mB;
-  if (tr && g.tail && (!make_map(&mA64, A, kq, n_pad, kBM, kChunk / 2) || !make_map(&mB64, B, kq, n_pad, kBN, kChunk / 2)))
+  if (g.tail && (!make_map(&mA64, A, kq, n_pad, kBM, kChunk / 2) || !make_map(&mB64, B, kq, n_pad, bn, kChunk / 2)))
     return cudaErrorInvalidValue;
-  const int grid = std::min(g.n_items, num_sms);
-  cudaError_t e;
-#define SRED_TC(M)                                                                                         \
-  if (tr) {                                                                                                \
-    e = cudaFuncSetAttribute(k_gram_tc<M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);   \
-    if (e != cudaSuccess) return e;                                                                        \
-    k_gram_tc<M, true><<<grid, kThreads, smem, st>>>(mA, mB, mA64, mB64, g);                               \
-  } else {                                                                                                 \
-    e = cudaFuncSetAttribute(k_gram_tc<M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
-    if (e != cudaSuccess) return e;                                                                        \
-    k_gram_tc<M, false><<<grid, kThreads, smem, st>>>(mA, mB, mA64, mB64, g);                              \
-  }
+  const int grid = (int)std::min<long long>(g.item1 - g.item0, num_sms);
+  const int smem = (int)plan.smem;
+#define SRED_TC3(M, BNV, TRV)                                                                            \
+  do {                                                                                                   \
+    e = cudaFuncSetAttribute(k_gram_tc<M, BNV, TRV>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); \
+    if (e != cudaSuccess) return e;                                                                      \
+    k_gram_tc<M, BNV, TRV><<<grid, kThreads, smem, st>>>(mA, mB, mA64, mB64, g);                         \
+  } while (0)
+#define SRED_TC(M)                                   \
+  if (bn == 256 && plan.tr) SRED_TC3(M, 256, true);       \
+  else if (bn == 256) SRED_TC3(M, 256, false);       \
+  else if (plan.tr) SRED_TC3(M, 128, true);          \
+  else SRED_TC3(M, 128, false);
   switch (ec.metric) {
     case kPearson: SRED_TC(kPearson); break;
     case kSsim: SRED_TC(kSsim); break;
+    case kNrmse: SRED_TC(kNrmse); break;
+    case kNrmseW: SRED_TC(kNrmseW); break;
     case kDebugDot: SRED_TC(kDebugDot); break;
     default: return cudaErrorInvalidValue;
   }
 #undef SRED_TC
+#undef SRED_TC3
   return cudaGetLastError();
 }
 

@@ -28,7 +28,6 @@ __global__ void k_pack(const float* img, int W, Ellipse e, const int* gram_pix, 
 __global__ void k_finalize(const int* slot, int W, int H, int rw, int rh, const double* num, const double* den,
                            const BlockParams* params, const double* sums, int n_flat, int metric, double sk,
                            double n_pixels, const float* mask, int apply_mask, float* out);
-__global__ void k_col_soa(const BlockParams* params, float* colsoa);
 __global__ void k_pack_vectors(const float* u, int n, int K, int mode, float* U, int kp, __nv_bfloat16* A,
                                __nv_bfloat16* B, int kq);
 __global__ void k_minmax(const float* a, const float* mask, int W, int H, int bw_, int bh_, size_t plane,

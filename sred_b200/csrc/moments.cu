@@ -232,9 +232,9 @@ __global__ void k_scatter(const uint8_t* __restrict__ flags, size_t n, const int
 //   sums[0] = sum_q 2^-(a_q)^2           (weight of a pair with a flat block)
 //   sums[1] = sum_q sqrt((K-1)/K) sigma_q (NRMSE against a flat block)
 //   sums[2] = sum_q sigma_q 2^-(a_q)^2     (Abs-diff against a flat block)
-// mode 0: U (fp32, row pitch kp). mode 1 / 2: the two- / three-level split
-// BF16 operands A, B (store_split; row pitch kq). Rows [n, n_pad) are
-// zero-filled by the host.
+// mode 0: U only (fp32, row pitch kp). mode 1 / 2: the two- / three-level
+// split BF16 operands A, B (store_split; row pitch kq), and U as well when U
+// is given (tensor-core NRMSE). Rows [n, n_pad) are zero-filled by the host.
 // ---------------------------------------------------------------------------
 __global__ void k_pack(const float* __restrict__ img, int W, Ellipse e, const int* __restrict__ gram_pix,
                        int n, float wscale, int mode, float* __restrict__ U, int kp,
@@ -265,12 +265,12 @@ __global__ void k_pack(const float* __restrict__ img, int W, Ellipse e, const in
     const double sigma = sqrt(v / (K - 1));
     for (int i = lane; i < K; i += 32) {
       double u = ((double)img[(size_t)(y + e.dy[i]) * W + (x + e.dx[i])] - mu) * inv;
-      if (mode == 0) U[(size_t)j * kp + i] = (float)u;
-      else store_split(A + (size_t)j * kq, B + (size_t)j * kq, K, i, u, mode + 1);
+      if (U) U[(size_t)j * kp + i] = (float)u;
+      if (mode != 0) store_split(A + (size_t)j * kq, B + (size_t)j * kq, K, i, u, mode + 1);
     }
-    if (mode == 0) {
+    if (U)
       for (int i = K + lane; i < kp; i += 32) U[(size_t)j * kp + i] = 0.0f;
-    } else {
+    if (mode != 0) {
       for (int i = (mode == 1 ? 3 : 6) * K + lane; i < kq; i += 32) {
         A[(size_t)j * kq + i] = __float2bfloat16_rn(0.0f);
         B[(size_t)j * kq + i] = __float2bfloat16_rn(0.0f);
@@ -302,30 +302,6 @@ __global__ void k_pack(const float* __restrict__ img, int W, Ellipse e, const in
     double t = 0.0;
     for (int i = 0; i < (int)(blockDim.x >> 5); i++) t += red[threadIdx.x][i];
     atomicAdd(sums + threadIdx.x, t);
-  }
-}
-
-// Tile-major structure-of-arrays copy of the column parameters (one CTA of
-// 256 threads per 256-column tile), with each tile's largest 1/sigma.
-__global__ void k_col_soa(const BlockParams* __restrict__ params, float* __restrict__ colsoa) {
-  const int t = blockIdx.x, i = threadIdx.x;
-  const BlockParams p = params[(size_t)t * 256 + i];
-  float* o = colsoa + (size_t)t * kColSoaFloats;
-  o[i] = p.a;
-  o[256 + i] = p.r;
-  o[512 + i] = p.sigma;
-  o[768 + i] = p.mu;
-  float m = p.r;
-  for (int s = 16; s; s >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, s));
-  __shared__ float wm[8];
-  if ((i & 31) == 0) wm[i >> 5] = m;
-  __syncthreads();
-  if (i < 4) o[1024 + i] = 0.0f;
-  __syncthreads();
-  if (i == 0) {
-    float mm = wm[0];
-    for (int w = 1; w < 8; w++) mm = fmaxf(mm, wm[w]);
-    o[1024] = mm;
   }
 }
 

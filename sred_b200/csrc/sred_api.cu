@@ -65,6 +65,7 @@ struct sred_ctx {
   std::recursive_mutex mu;
   std::vector<sred_ctx*> workers;  // extra contexts of sred_global_map_2d_batch (own streams and workspaces)
   GState shard;                    // the map prepared by sred_global_map_2d_shard_sums
+  TcDebug tc_debug{0, -1};         // tensor-core wait limit and withheld tile (sred_debug_set_tc_wait)
   void (*log_cb)(const char*, void*) = nullptr;
   void* log_user = nullptr;
 };
@@ -76,6 +77,17 @@ namespace {
 bool fault(const char* what) {
   const char* f = std::getenv("SRED_FAULT");
   return f && std::strcmp(f, what) == 0;
+}
+
+// Contraction engine and K' of a global map: Abs-diff needs no contraction
+// (the FP32 engine's kernel without a Gram); the other metrics run on the
+// context's engine, the tensor cores while the operands' B tile fits in
+// shared memory (NRMSE with the three-level split), else the FP32 engine.
+int pick_engine(const sred_ctx* c, int metric, int K, int* kq) {
+  *kq = split_cols_for(metric, K);
+  if (metric == kAbsDiff || c->engine != SRED_ENGINE_TC) return SRED_ENGINE_FP32;
+  TcPlan plan;
+  return plan_gram_tc(*kq, &plan) ? SRED_ENGINE_TC : SRED_ENGINE_FP32;
 }
 
 void log_msg(sred_ctx* c, const std::string& msg) {
@@ -279,10 +291,10 @@ sred_status global_prepare(sred_ctx* c, int metric, const float* d_img, int w, i
   const float npx = given ? given->n_pixels : java_float_count(nmask);
 
   // Operands and per-block parameters of the all-pairs contraction.
-  const int engine = (metric == kAbsDiff || metric == kNrmse) ? SRED_ENGINE_FP32 : c->engine;
+  int kq;  // K' of the split-BF16 operands
+  const int engine = pick_engine(c, metric, K, &kq);
   const size_t n_pad = round_up((size_t)std::max(n_g, 1), 256);
   const int kp = (int)round_up(K, 4);
-  const int kq = split_cols(K);  // K' of the split-BF16 operands
   float* d_U = nullptr;
   __nv_bfloat16 *d_A = nullptr, *d_B = nullptr;
   BlockParams* d_params;
@@ -293,10 +305,11 @@ sred_status global_prepare(sred_ctx* c, int metric, const float* d_img, int w, i
   CKS(ensure(c, B_NUM, n_pad, &d_num));
   CKS(ensure(c, B_DEN, n_pad, &d_den));
   CKS(ensure(c, B_SUMS, 4, &d_sums));
-  if (engine == SRED_ENGINE_FP32) {
+  if (engine == SRED_ENGINE_FP32 || metric == kNrmse) {  // tensor-core NRMSE reads U for near-identical pairs
     CKS(ensure(c, B_U, n_pad * kp, &d_U));
     CK(cudaMemsetAsync(d_U + (size_t)n_g * kp, 0, (n_pad - n_g) * kp * sizeof(float), st));
-  } else {
+  }
+  if (engine == SRED_ENGINE_TC) {
     CKS(ensure(c, B_A, n_pad * kq, &d_A));
     CKS(ensure(c, B_B, n_pad * kq, &d_B));
     CK(cudaMemsetAsync(d_A + (size_t)n_g * kq, 0, (n_pad - n_g) * kq * sizeof(__nv_bfloat16), st));
@@ -313,16 +326,14 @@ sred_status global_prepare(sred_ctx* c, int metric, const float* d_img, int w, i
   const float wscale = (float)std::sqrt(1.4426950408889634 / (double)hden);
   if (n_g > 0) {
     const int pgrid = grid_for((size_t)n_g * 32, 256, 8 * c->num_sms);
-    const int mode = engine == SRED_ENGINE_FP32 ? 0 : split_levels(K) - 1;
+    const int mode = engine == SRED_ENGINE_FP32 ? 0 : split_levels_for(metric, K) - 1;
     k_pack<<<pgrid, 256, 0, st>>>(d_img, w, e, d_gpix, n_g, wscale, mode, d_U, kp, d_A, d_B, kq, d_params,
                                   d_rmax, d_sums);
     CK(cudaGetLastError());
   }
   if (engine == SRED_ENGINE_TC) {
-    float* d_colsoa;
-    CKS(ensure(c, B_COLSOA, (n_pad / 256) * kColSoaFloats, &d_colsoa));
-    k_col_soa<<<(int)(n_pad / 256), 256, 0, st>>>(d_params, d_colsoa);
-    CK(cudaGetLastError());
+    float* d_soa;
+    CKS(ensure(c, B_COLSOA, gram_tc_soa_floats((int)n_pad), &d_soa));
   }
   CK(cudaEventRecord(c->ev[1], st));
   gs->metric = metric;
@@ -347,34 +358,40 @@ sred_status global_prepare(sred_ctx* c, int metric, const float* d_img, int w, i
   return SRED_OK;
 }
 
-// Phase 2: the all-pairs contraction for the row blocks [rb_begin, rb_end)
-// (128 rows each; rb_end < 0: all rows) into the num/den workspaces.
-sred_status global_gram(sred_ctx* c, const GState& gs, cudaStream_t st, int rb_begin, int rb_end) {
+// Phase 2: the all-pairs contraction (work-item range `shard` of n_shards of
+// the upper triangle) into the num/den workspaces.
+sred_status global_gram(sred_ctx* c, const GState& gs, cudaStream_t st, int shard, int n_shards) {
   if (gs.n_g > 0) {
     EpiConsts ec;
     ec.metric = gs.metric;
-    // NRMSE runs on the FP32 engine in its difference form
-    if (ec.metric == kNrmse) ec.metric = kNrmseD;
-    else if (ec.metric == kNrmseW) ec.metric = kNrmseDW;
+    // NRMSE on the FP32 engine accumulates |u_p - u_q|^2 (difference form)
+    if (gs.engine == SRED_ENGINE_FP32 && ec.metric == kNrmse) ec.metric = kNrmseD;
+    else if (gs.engine == SRED_ENGINE_FP32 && ec.metric == kNrmseW) ec.metric = kNrmseDW;
     ec.n = gs.n_g;
     ec.nrmse_scale = (float)((double)(gs.K - 1) / (double)gs.K);
     ec.c1 = kC1;
     ec.c2 = kC2;
+    if (gs.engine == SRED_ENGINE_TC && nrmse_metric(ec.metric)) {
+      ec.U = static_cast<const float*>(c->buf[B_U].p);
+      ec.kp = gs.kp;
+      ec.K = gs.K;
+      ec.nrmse_near = kNrmseNear;
+    }
     double* d_num = static_cast<double*>(c->buf[B_NUM].p);
     double* d_den = static_cast<double*>(c->buf[B_DEN].p);
     const BlockParams* d_params = static_cast<const BlockParams*>(c->buf[B_PARAMS].p);
     const float* d_rmax = static_cast<const float*>(c->buf[B_RMAX].p);
     if (gs.engine == SRED_ENGINE_FP32) {
       CK(launch_gram_fp32(static_cast<const float*>(c->buf[B_U].p), gs.kp, d_params, d_rmax, ec, d_num, d_den,
-                          c->num_sms, st, rb_begin, rb_end));
+                          c->num_sms, st, shard, n_shards));
     } else {
       int* d_status;
       CKS(ensure(c, B_STATUS, 4, &d_status));
       CK(cudaMemsetAsync(d_status, 0, 4 * sizeof(int), st));
       CK(launch_gram_tc(static_cast<const __nv_bfloat16*>(c->buf[B_A].p),
                         static_cast<const __nv_bfloat16*>(c->buf[B_B].p), gs.kq, (int)gs.n_pad, d_params,
-                        static_cast<const float*>(c->buf[B_COLSOA].p), d_rmax, ec, d_num, d_den, c->num_sms,
-                        d_status, st, rb_begin, rb_end));
+                        static_cast<float*>(c->buf[B_COLSOA].p), ec, d_num, d_den, c->num_sms, d_status, st, shard,
+                        n_shards, &c->tc_debug));
       int status = 0;
       CK(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
@@ -440,7 +457,7 @@ sred_status global_core(sred_ctx* c, int metric, const float* d_img, int w, int 
                         const GivenStats* given) {
   GState gs;
   CKS(global_prepare(c, metric, d_img, w, h, bw, bh, relc, st, given, &gs));
-  CKS(global_gram(c, gs, st, 0, -1));
+  CKS(global_gram(c, gs, st, 0, 1));
   return global_finish(c, gs, st, normalize, d_out, info);
 }
 
@@ -748,10 +765,10 @@ sred_status global3d_prepare(sred_ctx* c, int metric, const float* d_vol, int w,
   const int n_g = tot.x, n_flat = tot.y;
   const float npx = java_float_count(nmask);
 
-  const int engine = (metric == kAbsDiff || metric == kNrmse) ? SRED_ENGINE_FP32 : c->engine;
+  int kq;
+  const int engine = pick_engine(c, metric, K, &kq);
   const size_t n_pad = round_up((size_t)std::max(n_g, 1), 256);
   const int kp = (int)round_up(K, 4);
-  const int kq = split_cols(K);
   float* d_U = nullptr;
   __nv_bfloat16 *d_A = nullptr, *d_B = nullptr;
   BlockParams* d_params;
@@ -761,10 +778,11 @@ sred_status global3d_prepare(sred_ctx* c, int metric, const float* d_vol, int w,
   CKS(ensure(c, B_RMAX, n_pad / 128, &d_rmax));
   CKS(ensure(c, B_NUM, n_pad, &d_num));
   CKS(ensure(c, B_DEN, n_pad, &d_den));
-  if (engine == SRED_ENGINE_FP32) {
+  if (engine == SRED_ENGINE_FP32 || metric == kNrmse) {  // tensor-core NRMSE reads U for near-identical pairs
     CKS(ensure(c, B_U, n_pad * kp, &d_U));
     CK(cudaMemsetAsync(d_U + (size_t)n_g * kp, 0, (n_pad - n_g) * kp * sizeof(float), st));
-  } else {
+  }
+  if (engine == SRED_ENGINE_TC) {
     CKS(ensure(c, B_A, n_pad * kq, &d_A));
     CKS(ensure(c, B_B, n_pad * kq, &d_B));
     CK(cudaMemsetAsync(d_A + (size_t)n_g * kq, 0, (n_pad - n_g) * kq * sizeof(__nv_bfloat16), st));
@@ -779,15 +797,13 @@ sred_status global3d_prepare(sred_ctx* c, int metric, const float* d_vol, int w,
   const float wscale = (float)std::sqrt(1.4426950408889634 / (double)hden);
   if (n_g > 0) {
     k_pack3d<<<grid_for((size_t)n_g * 32, 256, 8 * c->num_sms), 256, 0, st>>>(
-        d_vol, v, d_off, d_gpix, n_g, wscale, engine == SRED_ENGINE_FP32 ? 0 : split_levels(K) - 1, d_U, kp, d_A,
+        d_vol, v, d_off, d_gpix, n_g, wscale, engine == SRED_ENGINE_FP32 ? 0 : split_levels_for(metric, K) - 1, d_U, kp, d_A,
         d_B, kq, d_params, d_rmax);
     CK(cudaGetLastError());
   }
   if (engine == SRED_ENGINE_TC) {
-    float* d_colsoa;
-    CKS(ensure(c, B_COLSOA, (n_pad / 256) * kColSoaFloats, &d_colsoa));
-    k_col_soa<<<(int)(n_pad / 256), 256, 0, st>>>(d_params, d_colsoa);
-    CK(cudaGetLastError());
+    float* d_soa;
+    CKS(ensure(c, B_COLSOA, gram_tc_soa_floats((int)n_pad), &d_soa));
   }
   CK(cudaEventRecord(c->ev[1], st));
   gs->vol = true;
@@ -876,7 +892,7 @@ sred_status global3d_core(sred_ctx* c, int metric, const float* d_vol, int w, in
                           float relc, int normalize, float* d_out, cudaStream_t st, sred_run_info* info) {
   GState gs;
   CKS(global3d_prepare(c, metric, d_vol, w, h, d, bw, bh, bd, relc, st, &gs));
-  CKS(global_gram(c, gs, st, 0, -1));
+  CKS(global_gram(c, gs, st, 0, 1));
   return global3d_finish(c, gs, st, normalize, d_out, info);
 }
 
@@ -1572,9 +1588,12 @@ sred_status reserve_global(sred_ctx* c, const sred_job* jobs, int n_jobs) {
     const size_t np = round_up(std::max<size_t>(inter, 1), 256);
     n = std::max(n, (size_t)j.w * j.h);
     n_pad = std::max(n_pad, np);
-    a = std::max(a, np * (size_t)split_cols(K));
+    a = std::max(a, np * (size_t)split_cols_for(global_metric(j.metric), K));
     u = std::max(u, np * round_up(K, 4));
-    cols = std::max(cols, (np / 256) * kColSoaFloats);
+    cols = std::max(cols, gram_tc_soa_floats((int)np));
+    int kq;
+    if (tc && pick_engine(c, global_metric(j.metric), K, &kq) == SRED_ENGINE_FP32) fp32 = true;
+    if (global_metric(j.metric) == kNrmse) fp32 = true;  // U for the near-identical pairs
     if (global_metric(j.metric) == kAbsDiff) fp32 = true;
   }
   float* f;
@@ -1642,13 +1661,6 @@ sred_status sred_global_map_2d_batch(sred_ctx* c, sred_job* jobs, int n_jobs, in
   return SRED_OK;
 }
 
-// Row blocks (128 rows of the compacted block list) of shard `shard`.
-void shard_row_blocks(int n_g, int shard, int n_shards, int* rb0, int* rb1) {
-  const int64_t n_rb = (n_g + 127) / 128;
-  *rb0 = (int)(n_rb * shard / n_shards);
-  *rb1 = (int)(n_rb * (shard + 1) / n_shards);
-}
-
 sred_status sred_global_map_2d_shard_sums(sred_ctx* c, const char* metric, const float* d_img, int w, int h,
                                           int bw, int bh, float relc, int shard, int n_shards, double* d_sums,
                                           size_t capacity, void* stream, sred_run_info* info) {
@@ -1661,9 +1673,7 @@ sred_status sred_global_map_2d_shard_sums(sred_ctx* c, const char* metric, const
   GState gs;
   CKS(global_prepare(c, m, d_img, w, h, bw, bh, relc, st, nullptr, &gs));
   if (capacity < 2 * (size_t)gs.n_g) return fail(c, SRED_ERR_ARG, "sums buffer smaller than 2 x relevant blocks");
-  int rb0, rb1;
-  shard_row_blocks(gs.n_g, shard, n_shards, &rb0, &rb1);
-  if (rb0 < rb1) CKS(global_gram(c, gs, st, rb0, rb1));
+  CKS(global_gram(c, gs, st, shard, n_shards));
   if (gs.n_g > 0) {
     CK(cudaMemcpyAsync(d_sums, c->buf[B_NUM].p, gs.n_g * sizeof(double), cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(d_sums + gs.n_g, c->buf[B_DEN].p, gs.n_g * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -1716,9 +1726,7 @@ sred_status sred_global_map_3d_shard_sums(sred_ctx* c, const char* metric, const
   GState gs;
   CKS(global3d_prepare(c, m, d_vol, w, h, d, bw, bh, bd, relc, st, &gs));
   if (capacity < 2 * (size_t)gs.n_g) return fail(c, SRED_ERR_ARG, "sums buffer smaller than 2 x relevant blocks");
-  int rb0, rb1;
-  shard_row_blocks(gs.n_g, shard, n_shards, &rb0, &rb1);
-  if (rb0 < rb1) CKS(global_gram(c, gs, st, rb0, rb1));
+  CKS(global_gram(c, gs, st, shard, n_shards));
   if (gs.n_g > 0) {
     CK(cudaMemcpyAsync(d_sums, c->buf[B_NUM].p, gs.n_g * sizeof(double), cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(d_sums + gs.n_g, c->buf[B_DEN].p, gs.n_g * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -1877,6 +1885,14 @@ sred_status sred_block_map_2d_device(sred_ctx* c, const char* metric, const floa
   return SRED_OK;
 }
 
+sred_status sred_debug_set_tc_wait(sred_ctx* c, unsigned long long timeout_ns, long long withhold_tile) {
+  if (!c || withhold_tile < -1) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  c->tc_debug.timeout_ns = timeout_ns;
+  c->tc_debug.withhold_tile = withhold_tile;
+  return SRED_OK;
+}
+
 sred_status sred_debug_gram_rowdot(sred_ctx* c, int engine, const float* u, const float* w1, const float* w2, int n,
                                    int k, double* num, double* den) {
   if (!c || !u || !w1 || !w2 || !num || !den || n <= 0 || k <= 0 || k > kMaxK) return SRED_ERR_ARG;
@@ -1923,11 +1939,12 @@ sred_status sred_debug_gram_rowdot(sred_ctx* c, int engine, const float* u, cons
     int* d_status;
     CKS(ensure(c, B_STATUS, 4, &d_status));
     CK(cudaMemsetAsync(d_status, 0, 4 * sizeof(int), st));
-    float* d_colsoa;
-    CKS(ensure(c, B_COLSOA, (n_pad / 256) * kColSoaFloats, &d_colsoa));
-    k_col_soa<<<(int)(n_pad / 256), 256, 0, st>>>(d_params, d_colsoa);
-    CK(launch_gram_tc(d_A, d_B, kq, (int)n_pad, d_params, d_colsoa, d_rmax, ec, d_num, d_den, c->num_sms, d_status,
-                      st));
+    float* d_soa;
+    CKS(ensure(c, B_COLSOA, gram_tc_soa_floats((int)n_pad), &d_soa));
+    TcPlan plan;
+    if (!plan_gram_tc(kq, &plan)) return fail(c, SRED_ERR_ARG, "K too large for the tensor-core engine");
+    CK(launch_gram_tc(d_A, d_B, kq, (int)n_pad, d_params, d_soa, ec, d_num, d_den, c->num_sms, d_status, st, 0, 1,
+                      &c->tc_debug));
     int status = 0;
     CK(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));

@@ -322,12 +322,12 @@ __global__ void k_pack3d(const float* __restrict__ img, Vol3 v, const int* __res
     const double sigma = sqrt(var / (K - 1));
     for (int i = lane; i < K; i += 32) {
       const double u = ((double)c[off[i]] - mu) * inv;
-      if (mode == 0) U[(size_t)j * kp + i] = (float)u;
-      else store_split(A + (size_t)j * kq, B + (size_t)j * kq, K, i, u, mode + 1);
+      if (U) U[(size_t)j * kp + i] = (float)u;
+      if (mode != 0) store_split(A + (size_t)j * kq, B + (size_t)j * kq, K, i, u, mode + 1);
     }
-    if (mode == 0) {
+    if (U)
       for (int i = K + lane; i < kp; i += 32) U[(size_t)j * kp + i] = 0.0f;
-    } else {
+    if (mode != 0) {
       for (int i = (mode == 1 ? 3 : 6) * K + lane; i < kq; i += 32) {
         A[(size_t)j * kq + i] = __float2bfloat16_rn(0.0f);
         B[(size_t)j * kq + i] = __float2bfloat16_rn(0.0f);

@@ -1,10 +1,13 @@
-"""Row sharding of one global map across ranks (host logic, CPU only).
+"""Sharding of one global map across ranks (host logic, CPU only).
 
-The exchange is checked with two gloo ranks on the CPU: each rank computes
-the FP64 oracle's per-row sums of its own row blocks (zero elsewhere), the
-ranks sum them with one all-reduce, and every rank finishes the map; the
-result must equal the unsharded map. The partition rule is the one libsred
-applies (clutils.shard_row_blocks).
+libsred evaluates each unordered block pair once: the work is the upper
+triangle of 128-row x 256-column tiles, cut into work items, and shard s of
+S takes the items [I s / S, I (s + 1) / S) (clutils.shard_items mirrors the
+rule). The partition test checks that every pair lies in exactly one tile of
+one shard. The exchange is checked with two gloo ranks on the CPU: each rank
+adds the FP64 pair terms of its tiles to both blocks of each pair (the self
+pair once), the ranks sum their per-block sums with one all-reduce, and every
+rank finishes the map; the result must equal the oracle's unsharded FP64 map.
 """
 import datetime
 import multiprocessing as mp
@@ -17,16 +20,29 @@ import pytest
 from sred_b200 import clutils
 
 
-@pytest.mark.parametrize("n_gram", [0, 1, 127, 128, 129, 1000, 754587])
+@pytest.mark.parametrize("n_gram", [0, 1, 127, 128, 129, 255, 256, 257, 1000, 4097])
 @pytest.mark.parametrize("world", [1, 2, 3, 8])
-def test_shard_row_blocks_partition(n_gram, world):
+@pytest.mark.parametrize("bn,sms", [(256, 148), (128, 148), (256, 4)])
+def test_shard_items_cover_each_pair_once(n_gram, world, bn, sms):
     n_rb = (n_gram + 127) // 128
-    spans = [clutils.shard_row_blocks(n_gram, s, world) for s in range(world)]
-    assert spans[0][0] == 0 and spans[-1][1] == n_rb
-    for (a0, a1), (b0, b1) in zip(spans, spans[1:]):
-        assert a1 == b0 and a0 <= a1
-    sizes = [b - a for a, b in spans]
-    assert max(sizes) - min(sizes) <= 1
+    n_ct = (n_gram + bn - 1) // bn
+    seen = {}
+    for s in range(world):
+        for ct, rb0, rb1 in clutils.shard_items(n_gram, s, world, bn, sms):
+            for rb in range(rb0, rb1):
+                assert (rb, ct) not in seen, (rb, ct)
+                seen[(rb, ct)] = s
+    # exactly the tiles holding a pair p <= q with both below n_gram
+    want = {(rb, ct) for ct in range(n_ct) for rb in range(n_rb) if rb * 128 <= ct * bn + bn - 1}
+    assert set(seen) == want
+
+
+@pytest.mark.parametrize("world", [1, 2, 8])
+def test_shard_items_balanced(world):
+    n = 754587  # relevant blocks of the 1024^2 / 9x9 benchmark map
+    items, _ = clutils.gram_items(n)
+    sizes = [items * (s + 1) // world - items * s // world for s in range(world)]
+    assert sum(sizes) == items and max(sizes) - min(sizes) <= 1
 
 
 def _free_port():
@@ -35,6 +51,40 @@ def _free_port():
     p = s.getsockname()[1]
     s.close()
     return p
+
+
+def _pair_terms_f64(metric, img, bw, bh, listed, nv):
+    """FP64 numerator and denominator terms of every pair of the listed
+    blocks, as the oracle's FP64 judge evaluates them (orc_global_f64): FP64
+    block moments, weight exp(-(s_p - s_q)^2 / (nv + eps)), Pearson
+    max(0, cov / (s_p s_q + eps)) (flat pairs: 1 if both flat, else 0), NRMSE
+    sqrt(mse / K) unweighted."""
+    import oracle
+    H, W = img.shape
+    rw, rh = bw // 2, bh // 2
+    off = [(dy, dx) for dy in range(-rh, rh + 1) for dx in range(-rw, rw + 1)
+           if (dx * dx) / float(rw * rw) + (dy * dy) / float(rh * rh) <= 1.0]
+    K = oracle.block_size(bw, bh)
+    assert len(off) == K
+    x = img.astype(np.float64)
+    ys, xs = np.divmod(listed, W)
+    V = np.stack([x[ys + dy, xs + dx] for dy, dx in off], axis=1)
+    mu = V.mean(axis=1, keepdims=True)
+    C = V - mu
+    sig = np.sqrt((C * C).sum(axis=1) / (K - 1))
+    h = float(np.float32(nv)) + float(np.float32(oracle.EPSILON))
+    w = np.exp(-((sig[:, None] - sig[None, :]) ** 2) / h)
+    if metric == "NRMSE":
+        d2 = (C * C).sum(1)[:, None] + (C * C).sum(1)[None, :] - 2.0 * (C @ C.T)
+        tn = np.sqrt(np.maximum(d2, 0.0) / K)
+        np.fill_diagonal(tn, 0.0)
+        return tn, w
+    cov = (C @ C.T) / (K - 1)
+    r = cov / (sig[:, None] * sig[None, :] + float(np.float32(oracle.EPSILON)))
+    flat = sig == 0.0
+    tn = np.maximum(r, 0.0) * w
+    tn = np.where(flat[:, None] & flat[None, :], w, np.where(flat[:, None] | flat[None, :], 0.0, tn))
+    return tn, w
 
 
 def _rank(rank, world, port, metric, out_q):
@@ -58,15 +108,27 @@ def _rank(rank, world, port, metric, out_q):
         s = stds.ravel()[pix]
         listed = pix[s * s >= thr].astype(np.int32)  # the compacted list, raster order
         n = listed.size
-        rb0, rb1 = clutils.shard_row_blocks(n, rank, world)
+        terms_n, terms_d = _pair_terms_f64(metric, img, bw, bh, listed, nv)
 
         def compute():
-            rows = listed[rb0 * 128:rb1 * 128]
             sums = torch.zeros(2 * n, dtype=torch.float64)
-            if rows.size:
-                num, den = oracle.global_sums_f64(metric, img, bw, bh, stds, nv, thr, rows)
-                sums[rb0 * 128:rb0 * 128 + rows.size] = torch.from_numpy(num)
-                sums[n + rb0 * 128:n + rb0 * 128 + rows.size] = torch.from_numpy(den)
+            num = np.zeros(n)
+            den = np.zeros(n)
+            for ct, rb0, rb1 in clutils.shard_items(n, rank, world):
+                q0, q1 = ct * 256, min(ct * 256 + 256, n)
+                for rb in range(rb0, rb1):
+                    p0, p1 = rb * 128, min(rb * 128 + 128, n)
+                    P, Q = np.meshgrid(np.arange(p0, p1), np.arange(q0, q1), indexing="ij")
+                    keep = Q >= P
+                    tn = np.where(keep, terms_n[p0:p1, q0:q1], 0.0)
+                    td = np.where(keep, terms_d[p0:p1, q0:q1], 0.0)
+                    num[p0:p1] += tn.sum(axis=1)
+                    den[p0:p1] += td.sum(axis=1)
+                    off = Q > P  # the pair's second block (the self pair once)
+                    num[q0:q1] += np.where(off, tn, 0.0).sum(axis=0)
+                    den[q0:q1] += np.where(off, td, 0.0).sum(axis=0)
+            sums[:n] = torch.from_numpy(num)
+            sums[n:] = torch.from_numpy(den)
             return sums, n
 
         def finish(summed):
