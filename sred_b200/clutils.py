@@ -252,42 +252,46 @@ def global_map_batch(jobs: list[dict], n_workers: int = 4, ctx=None) -> list[tup
 # Row-sharded global map (one map across several processes / GPUs)
 # ---------------------------------------------------------------------------
 
-def _items_before(ct: int, h: int) -> int:
-    """Work items of column tiles [0, ct): sum over c < ct of ceil((c + 1) / h)."""
-    q, r = divmod(ct, h)
-    return h * q * (q + 1) // 2 + r * (q + 1)
+def _items_before_run(j: int, n_ct: int, h: int) -> int:
+    """Work items of runs [0, j): run j' has the column tiles j' h .. n_ct - 1."""
+    return j * n_ct - h * j * (j - 1) // 2
 
 
 def gram_items(n_gram: int, bn: int = 256, num_sms: int = 148) -> tuple[int, int]:
     """(items, L) of the tensor-core engine's symmetric schedule for n_gram
     blocks and bn-column tiles: the upper triangle of 128-row x bn-column
-    tiles in runs of up to L row blocks per column tile, L the largest of
-    16, 8, 4, 2 that leaves at least 4 items per SM (the rule libsred applies,
-    global_tc.cu: gram_tc_items)."""
+    tiles, run-major (runs of L row blocks, each run against every column tile
+    that reaches it), L the largest of 16, 8, 4, 2 that leaves at least 4 items
+    per SM (the rule libsred applies, global_tc.cu: gram_tc_items)."""
     m = bn // 128
-    n_ct = (n_gram + bn - 1) // bn
+    n_rb, n_ct = (n_gram + 127) // 128, (n_gram + bn - 1) // bn
+
+    def items(L):
+        return _items_before_run((n_rb + L - 1) // L, n_ct, L // m)
+
     L = 16
-    while L > 2 and _items_before(n_ct, L // m) < 4 * num_sms:
+    while L > 2 and items(L) < 4 * num_sms:
         L //= 2
     L = max(L, m)
-    return _items_before(n_ct, L // m), L
+    return items(L), L
 
 
 def shard_items(n_gram: int, shard: int, n_shards: int, bn: int = 256, num_sms: int = 148):
     """Tiles of shard `shard` of `n_shards`: the work items [I s / S, I (s + 1) / S)
     of the symmetric schedule, each as (column tile, first row block, end row
-    block); empty runs (rows past n_gram) are left out. Every pair (p <= q) of
-    the n_gram blocks lies in exactly one tile of exactly one shard."""
+    block). Every pair (p <= q) of the n_gram blocks lies in exactly one tile
+    of exactly one shard."""
     items, L = gram_items(n_gram, bn, num_sms)
     m, h = bn // 128, L // (bn // 128)
-    n_rb = (n_gram + 127) // 128
+    n_rb, n_ct = (n_gram + 127) // 128, (n_gram + bn - 1) // bn
     i0, i1 = items * shard // n_shards, items * (shard + 1) // n_shards
     out = []
-    ct = 0
+    j = 0
     for it in range(i0, i1):
-        while _items_before(ct + 1, h) <= it:
-            ct += 1
-        rb0 = (it - _items_before(ct, h)) * L
+        while _items_before_run(j + 1, n_ct, h) <= it:
+            j += 1
+        ct = j * h + (it - _items_before_run(j, n_ct, h))
+        rb0 = j * L
         rb1 = min(rb0 + L, (ct + 1) * m, n_rb)
         if rb0 < rb1:
             out.append((ct, rb0, rb1))

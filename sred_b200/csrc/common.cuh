@@ -139,9 +139,10 @@ __host__ __device__ constexpr int col_soa_floats(int bn) { return 4 * bn + 4; }
 __host__ __device__ constexpr int col_soa_pos(int i) {
   return (i & ~15) + 4 * ((i & 7) >> 1) + 2 * ((i >> 3) & 1) + (i & 1);
 }
-// Row parameters of one 128-row block, natural order: [a | r | sigma | mu] x 128,
-// max r, 3 x pad.
-constexpr int kRowSoaFloats = 4 * 128 + 4;
+// Row parameters of one 128-row block: per row the pairs (a, a, -eps r, -eps r,
+// sigma, sigma, mu, mu) as the epilogue's f32x2 operands, then r x 128, then
+// max r and 3 x pad.
+constexpr int kRowSoaFloats = 8 * 128 + 128 + 4;
 
 // Launch shape of the tensor-core engine for a K': column tile width (256 or
 // 128), whole-tile A buffers or a ring of 64-column chunks, dynamic shared

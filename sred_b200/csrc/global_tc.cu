@@ -51,7 +51,9 @@ constexpr int kMaxStages = 16;
 constexpr int kEpiWarps = 16;                     // 4 per SM sub-partition
 constexpr int kThreads = (kEpiWarps + 2) * 32;
 constexpr int kEpiThreads = kEpiWarps * 32;
-constexpr int kRSlots = 4;                        // row-parameter ring depth
+constexpr int kRSlots = 2;                        // row-parameter ring depth
+constexpr int kRowR = 8 * kBM;                    // offset of r in a row-parameter slot
+constexpr int kRowMax = kRowR + kBM;              // offset of max r
 constexpr int kRowFloats = kRowSoaFloats;         // one 128-row block's parameters
 constexpr int kRowPartBytes = 2 * 4 * kBM * 8;    // [2 buffers][4 column groups][128 rows] float2
 constexpr int kBarBytes = 512;
@@ -74,7 +76,8 @@ struct TcArgs {
   int nfull, tail;              // whole-tile mode: 64-column chunks and a 32-column tail (0 or 1)
   uint32_t a_bytes, b_bytes;    // whole A tile and whole B tile (64-column chunks + 32-column tail)
   int n_rb, n_ct;               // row blocks holding valid rows, column tiles
-  int L, h;                     // row blocks per item, L / (BN / 128)
+  int L, h;                     // row blocks per item (a run), L / (BN / 128)
+  int n_runs;                   // runs of L row blocks
   long long item0, item1;       // items of this launch
   const float* colsoa;          // per column tile, permuted (col_soa_pos)
   const float* rowsoa;          // per 128-row block, natural order
@@ -124,14 +127,22 @@ __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
 // records `code`) if the wait exceeded the limit or another role of any CTA
 // already gave up. Drain waits (for copies or MMAs this CTA issued) pass
 // abort = false: they keep waiting, within the same bound, after another
-// role has given up.
+// role has given up. The single-thread roles (producer, MMA issuer) wait
+// mostly for the epilogue; they back off with nanosleep (up to 0.5 us) so
+// that their polling does not take issue slots from the epilogue warps of
+// their SM sub-partition.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const TcArgs& g, int code,
-                                          bool abort = true) {
+                                          bool abort = true, bool backoff = false) {
   if (mbar_test(bar, parity)) return true;
   const unsigned long long t0 = globaltimer();
+  uint32_t ns = 32;
   for (uint32_t i = 1;; i++) {
+    if (backoff) {
+      __nanosleep(ns);
+      ns = ns < 512 ? 2 * ns : 512;
+    }
     if (mbar_test(bar, parity)) return true;
-    if ((i & 255u) == 0) {
+    if ((i & (backoff ? 7u : 255u)) == 0) {
       if (abort && *reinterpret_cast<volatile int*>(g.status) != ST_OK) return false;
       if (globaltimer() - t0 > g.timeout_ns) {
         atomicCAS(g.status, ST_OK, code);
@@ -147,6 +158,13 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
           "r"(dst),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
       : "memory");
+}
+
+// L2 prefetch of one tensor-map box (no shared memory, no completion).
+__device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* map, int x, int y) {
+  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(reinterpret_cast<uint64_t>(map)),
+               "r"(x), "r"(y)
+               : "memory");
 }
 
 // Plain bulk copy (no tensor map): 16-byte aligned addresses, size a multiple of 16.
@@ -218,6 +236,13 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
 
 // Wait for every TMEM load this thread issued; the register operands tie
 // later uses of v to the wait, so none is scheduled before it.
+__device__ __forceinline__ void tmem_wait16(uint32_t (&v)[8], uint32_t (&u)[8]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
+                 "+r"(u[0]), "+r"(u[1]), "+r"(u[2]), "+r"(u[3]), "+r"(u[4]), "+r"(u[5]), "+r"(u[6]), "+r"(u[7])
+               :
+               : "memory");
+}
 __device__ __forceinline__ void tmem_wait8(uint32_t (&v)[8]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;"
                : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7])
@@ -238,23 +263,22 @@ struct RowC {
 template <int METRIC>
 __device__ __forceinline__ RowC make_rowc(const float* __restrict__ rs, int row, const EpiConsts& ec) {
   RowC c;
-  const float a = rs[row], r = rs[kBM + row];
-  c.a = f2(a, a);
-  if (METRIC == kPearson) {
-    const float ne = -kEps * r;
-    c.ne = f2(ne, ne);
+  const float4 lo = *reinterpret_cast<const float4*>(rs + 8 * row);  // a, a, -eps r, -eps r
+  c.a = f2(lo.x, lo.y);
+  if (METRIC == kPearson) c.ne = f2(lo.z, lo.w);
+  if (METRIC == kDebugDot) {
+    const float r = rs[kRowR + row];
+    c.r = f2(r, r);
   }
-  if (METRIC == kDebugDot) c.r = f2(r, r);
   if (METRIC == kSsim || METRIC == kNrmse || METRIC == kNrmseW) {
-    const float s = rs[2 * kBM + row];
-    c.sg2 = f2(2.0f * s, 2.0f * s);
-    c.sg = f2(s, s);
+    const float4 hi = *reinterpret_cast<const float4*>(rs + 8 * row + 4);  // sigma, sigma, mu, mu
+    c.sg = f2(hi.x, hi.y);
+    c.sg2 = add2(c.sg, c.sg);
     if (METRIC == kSsim) {
-      const float m = rs[3 * kBM + row];
-      c.mu2 = f2(2.0f * m, 2.0f * m);
-      c.mumu = f2(m * m, m * m);
-      const float s2 = s * s + ec.c2;
-      c.s2 = f2(s2, s2);
+      const F2 m = f2(hi.z, hi.w);
+      c.mu2 = add2(m, m);
+      c.mumu = mul2(m, m);
+      c.s2 = fma2(c.sg, c.sg, f2(ec.c2, ec.c2));
     }
   }
   return c;
@@ -345,139 +369,171 @@ constexpr bool nrmse_tc() {
 // p0: block index of tile row 0; q0: block index of the slab's first column.
 // The tile's row sums are returned in rsum[2k + {0: num, 1: den}] for rows
 // 32(w%4) + t/4 + 8k.
+// Row passes of the epilogue: the metrics with many row constants (SSIM,
+// NRMSE) take the 4 rows in two passes of 2 so that their constants fit in
+// registers; the column accumulators are then read and written once per pass.
+template <int METRIC>
+constexpr int row_passes() {
+  return (METRIC == kSsim || METRIC == kNrmse || METRIC == kNrmseW) ? 2 : 1;
+}
+
 template <int METRIC, int BN, int CMODE, bool MASKED>
 __device__ __forceinline__ void sym_tile(uint32_t taddr, const float* __restrict__ rs, const float* __restrict__ cs,
                                          float4* __restrict__ cacc, int p0, int q0, const EpiConsts& ec,
                                          float (&rsum)[8]) {
   constexpr int CH = Cfg<BN>::kCH;
+  constexpr int NP = row_passes<METRIC>(), R = 4 / NP;  // passes, rows per pass
+  constexpr int HP = R / 2;                              // 16-lane halves per pass
   const int lane = threadIdx.x & 31, rsub = lane >> 2, csub = lane & 3;
   const int quarter = (threadIdx.x >> 5) & 3;
-  RowC rc[4];
-  F2 rn[4], rd[4];
-  int prow[4];
-  bool force[4];
+#pragma unroll 1
+  for (int pass = 0; pass < NP; pass++) {
+    RowC rc[R];
+    F2 rn[R], rd[R];
+    int prow[R];
+    bool force[R];
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
-    const int row = quarter * 32 + rsub + 8 * k;
-    rc[k] = make_rowc<METRIC>(rs, row, ec);
-    rn[k] = rd[k] = f2(0.0f, 0.0f);
-    prow[k] = p0 + row;
-    force[k] = MASKED && rs[kBM + row] > 0.0f;
-  }
+    for (int kr = 0; kr < R; kr++) {
+      const int row = quarter * 32 + rsub + 8 * (pass * R + kr);
+      rc[kr] = make_rowc<METRIC>(rs, row, ec);
+      rn[kr] = rd[kr] = f2(0.0f, 0.0f);
+      prow[kr] = p0 + row;
+      force[kr] = MASKED && rs[kRowR + row] > 0.0f;
+    }
+    // TMEM reads, one (chunk, half) step at a time; the next step's load is
+    // issued before the current step is evaluated.
+    const uint32_t tp = taddr + ((uint32_t)(16 * pass * HP) << 16);
+    uint32_t buf[2][8];
+    tmem_ld8(tp, buf[0]);
+    tmem_wait8(buf[0]);
 #pragma unroll
-  for (int c = 0; c < CH; c++) {
-    const float4 cnv = cacc[(2 * c) * kEpiThreads], cdv = cacc[(2 * c + 1) * kEpiThreads];
-    F2 cn[2] = {f2(cnv.x, cnv.y), f2(cnv.z, cnv.w)};
-    F2 cd[2] = {f2(cdv.x, cdv.y), f2(cdv.z, cdv.w)};
-    const int cb = 16 * c + 4 * csub;
-    const float4 a4 = *reinterpret_cast<const float4*>(cs + cb);
-    float4 r4 = make_float4(0.f, 0.f, 0.f, 0.f), s4 = r4, m4 = r4;
-    if (METRIC == kPearson || METRIC == kDebugDot) r4 = *reinterpret_cast<const float4*>(cs + BN + cb);
-    if (METRIC == kSsim || METRIC == kNrmse || METRIC == kNrmseW)
-      s4 = *reinterpret_cast<const float4*>(cs + 2 * BN + cb);
-    if (METRIC == kSsim) m4 = *reinterpret_cast<const float4*>(cs + 3 * BN + cb);
+    for (int c = 0; c < CH; c++) {
+      const float4 cnv = cacc[(2 * c) * kEpiThreads], cdv = cacc[(2 * c + 1) * kEpiThreads];
+      F2 cn[2] = {f2(cnv.x, cnv.y), f2(cnv.z, cnv.w)};
+      F2 cd[2] = {f2(cdv.x, cdv.y), f2(cdv.z, cdv.w)};
+      const int cb = 16 * c + 4 * csub;
+      const float4 a4 = *reinterpret_cast<const float4*>(cs + cb);
+      float4 r4 = make_float4(0.f, 0.f, 0.f, 0.f), s4 = r4, m4 = r4;
+      if (METRIC == kPearson || METRIC == kDebugDot) r4 = *reinterpret_cast<const float4*>(cs + BN + cb);
+      if (METRIC == kSsim || METRIC == kNrmse || METRIC == kNrmseW)
+        s4 = *reinterpret_cast<const float4*>(cs + 2 * BN + cb);
+      if (METRIC == kSsim) m4 = *reinterpret_cast<const float4*>(cs + 3 * BN + cb);
 #pragma unroll
-    for (int half = 0; half < 2; half++) {
-      uint32_t cur[8];
-      tmem_ld8(taddr + ((uint32_t)(16 * half) << 16) + 16 * c, cur);
-      tmem_wait8(cur);
-      uint32_t near = 0;  // NRMSE: sign bits of (1 - delta) - G, any set = a near-identical pair
+      for (int hh = 0; hh < HP; hh++) {
+        const int step = c * HP + hh;
+        uint32_t(&cur)[8] = buf[step & 1];
+        uint32_t(&nxt)[8] = buf[(step + 1) & 1];
+        if (step + 1 < CH * HP) {
+          const int nc = (step + 1) / HP, nh = (step + 1) % HP;
+          tmem_ld8(tp + ((uint32_t)(16 * nh) << 16) + 16 * nc, nxt);
+        }
+        uint32_t near = 0;  // NRMSE: sign bits of (1 - delta) - G, any set = a near-identical pair
 #pragma unroll
-      for (int rep = 0; rep < 2; rep++) {
-        const F2 qa = rep ? f2(a4.z, a4.w) : f2(a4.x, a4.y);
-        const F2 qr = rep ? f2(r4.z, r4.w) : f2(r4.x, r4.y);
-        const F2 qs = rep ? f2(s4.z, s4.w) : f2(s4.x, s4.y);
-        const F2 qm = rep ? f2(m4.z, m4.w) : f2(m4.x, m4.y);
-        const int qlo = q0 + 16 * c + 8 * rep + 2 * csub;
+        for (int rep = 0; rep < 2; rep++) {
+          const F2 qa = rep ? f2(a4.z, a4.w) : f2(a4.x, a4.y);
+          const F2 qr = rep ? f2(r4.z, r4.w) : f2(r4.x, r4.y);
+          const F2 qs = rep ? f2(s4.z, s4.w) : f2(s4.x, s4.y);
+          const F2 qm = rep ? f2(m4.z, m4.w) : f2(m4.x, m4.y);
+          const int qlo = q0 + 16 * c + 8 * rep + 2 * csub;
 #pragma unroll
-        for (int kk = 0; kk < 2; kk++) {
-          const int k = 2 * half + kk;
-          float g0 = __uint_as_float(cur[4 * rep + 2 * kk]), g1 = __uint_as_float(cur[4 * rep + 2 * kk + 1]);
-          const int p = prow[k];
-          if (MASKED) {
-            if (force[k] && qlo == p) g0 = 1.0f;
-            if (force[k] && qlo + 1 == p) g1 = 1.0f;
-          }
-          F2 x, w;
-          terms2<METRIC, CMODE>(f2(g0, g1), rc[k], qa, qr, qs, qm, ec, x, w);
-          if (nrmse_tc<METRIC>()) {
-            float t0, t1;
-            f2_split(sub2(f2(ec.nrmse_near, ec.nrmse_near), f2(g0, g1)), t0, t1);
-            asm("lop3.b32 %0, %0, %1, %2, 0xFE;" : "+r"(near) : "r"(__float_as_uint(t0)), "r"(__float_as_uint(t1)));
-          }
-          if (!MASKED) {
-            if (weighted_num<METRIC>()) {
-              rn[k] = fma2(x, w, rn[k]);
-              cn[rep] = fma2(x, w, cn[rep]);
-            } else {
-              rn[k] = add2(rn[k], x);
-              cn[rep] = add2(cn[rep], x);
+          for (int kk = 0; kk < 2; kk++) {
+            const int kr = 2 * hh + kk;
+            float g0 = __uint_as_float(cur[4 * rep + 2 * kk]), g1 = __uint_as_float(cur[4 * rep + 2 * kk + 1]);
+            const int p = prow[kr];
+            if (MASKED) {
+              if (force[kr] && qlo == p) g0 = 1.0f;
+              if (force[kr] && qlo + 1 == p) g1 = 1.0f;
             }
-            rd[k] = add2(rd[k], w);
-            cd[rep] = add2(cd[rep], w);
-          } else {
-            float x0, x1, w0, w1;
-            f2_split(weighted_num<METRIC>() ? mul2(x, w) : x, x0, x1);
-            f2_split(w, w0, w1);
-            const bool pv = p < ec.n;
-            const bool r0 = pv && qlo >= p && qlo < ec.n, r1 = pv && qlo + 1 >= p && qlo + 1 < ec.n;
-            const bool c0 = r0 && qlo != p, c1 = r1 && qlo + 1 != p;
-            rn[k] = add2(rn[k], f2(r0 ? x0 : 0.0f, r1 ? x1 : 0.0f));
-            rd[k] = add2(rd[k], f2(r0 ? w0 : 0.0f, r1 ? w1 : 0.0f));
-            cn[rep] = add2(cn[rep], f2(c0 ? x0 : 0.0f, c1 ? x1 : 0.0f));
-            cd[rep] = add2(cd[rep], f2(c0 ? w0 : 0.0f, c1 ? w1 : 0.0f));
+            F2 x, w;
+            terms2<METRIC, CMODE>(f2(g0, g1), rc[kr], qa, qr, qs, qm, ec, x, w);
+            if (nrmse_tc<METRIC>()) {
+              float t0, t1;
+              f2_split(sub2(f2(ec.nrmse_near, ec.nrmse_near), f2(g0, g1)), t0, t1);
+              asm("lop3.b32 %0, %0, %1, %2, 0xFE;" : "+r"(near) : "r"(__float_as_uint(t0)), "r"(__float_as_uint(t1)));
+            }
+            if (!MASKED) {
+              if (weighted_num<METRIC>()) {
+                rn[kr] = fma2(x, w, rn[kr]);
+                cn[rep] = fma2(x, w, cn[rep]);
+              } else {
+                rn[kr] = add2(rn[kr], x);
+                cn[rep] = add2(cn[rep], x);
+              }
+              rd[kr] = add2(rd[kr], w);
+              cd[rep] = add2(cd[rep], w);
+            } else {
+              float x0, x1, w0, w1;
+              f2_split(weighted_num<METRIC>() ? mul2(x, w) : x, x0, x1);
+              f2_split(w, w0, w1);
+              const bool pv = p < ec.n;
+              const bool r0 = pv && qlo >= p && qlo < ec.n, r1 = pv && qlo + 1 >= p && qlo + 1 < ec.n;
+              const bool c0 = r0 && qlo != p, c1 = r1 && qlo + 1 != p;
+              rn[kr] = add2(rn[kr], f2(r0 ? x0 : 0.0f, r1 ? x1 : 0.0f));
+              rd[kr] = add2(rd[kr], f2(r0 ? w0 : 0.0f, r1 ? w1 : 0.0f));
+              cn[rep] = add2(cn[rep], f2(c0 ? x0 : 0.0f, c1 ? x1 : 0.0f));
+              cd[rep] = add2(cd[rep], f2(c0 ? w0 : 0.0f, c1 ? w1 : 0.0f));
+            }
           }
         }
-      }
-      if (nrmse_tc<METRIC>() && (int)near < 0) {
-        // Near-identical pairs: replace the accumulated term by the one of the
-        // exact squared difference (the same arithmetic as terms2 recomputes
-        // the term to remove).
+        if (nrmse_tc<METRIC>() && (int)near < 0) {
+          // Near-identical pairs: replace the accumulated term by the one of the
+          // exact squared difference (the same arithmetic as terms2 recomputes
+          // the term to remove).
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-          const int rep = j >> 2, kk = (j >> 1) & 1, lh = j & 1;
-          const float g = __uint_as_float(cur[4 * rep + 2 * kk + lh]);
-          const int k = 2 * half + kk, row = quarter * 32 + rsub + 8 * k;
-          const int p = prow[k], q = q0 + 16 * c + 8 * rep + 2 * csub + lh;
-          const bool rv = !MASKED || (p < ec.n && q >= p && q < ec.n);
-          const bool cv = !MASKED || (rv && q != p);
-          float ge = g;
-          if (MASKED && force[k] && q == p) ge = 1.0f;
-          if (!(ge > ec.nrmse_near) || !rv) continue;
-          const float sp = rs[2 * kBM + row];
-          const int ci = 16 * c + 4 * csub + 2 * rep + lh;  // permuted column slot
-          const float sq = cs[2 * BN + ci];
-          const float ds = __fsub_rn(sp, sq);
-          const float approx = sqrtf(fmaxf(
-              __fmul_rn(ec.nrmse_scale, __fmaf_rn(ds, ds, __fmul_rn(__fmul_rn(2.0f * sp, sq), __fsub_rn(1.0f, ge)))),
-              0.0f));
-          const float D = (q == p) ? 0.0f : exact_diff2(ec.U + (size_t)p * ec.kp, ec.U + (size_t)q * ec.kp, ec.K);
-          const float exact = sqrtf(__fmul_rn(ec.nrmse_scale, __fmaf_rn(ds, ds, __fmul_rn(__fmul_rn(sp, sq), D))));
-          float corr = exact - approx;
-          if (METRIC == kNrmseW) {
-            const float d = __fsub_rn(rs[row], cs[ci]);
-            corr *= ex2_approx(-__fmul_rn(d, d));
+          for (int j = 0; j < 8; j++) {
+            const int rep = j >> 2, kk = (j >> 1) & 1, lh = j & 1;
+            const int kr = 2 * hh + kk;
+            const float g = __uint_as_float(cur[4 * rep + 2 * kk + lh]);
+            const int row = quarter * 32 + rsub + 8 * (pass * R + kr);
+            const int p = prow[kr], q = q0 + 16 * c + 8 * rep + 2 * csub + lh;
+            const bool rv = !MASKED || (p < ec.n && q >= p && q < ec.n);
+            const bool cv = !MASKED || (rv && q != p);
+            float ge = g;
+            if (MASKED && force[kr] && q == p) ge = 1.0f;
+            if (!(ge > ec.nrmse_near) || !rv) continue;
+            const float sp = rs[8 * row + 4];
+            const int ci = 16 * c + 4 * csub + 2 * rep + lh;  // permuted column slot
+            const float sq = cs[2 * BN + ci];
+            const float ds = __fsub_rn(sp, sq);
+            const float approx = sqrtf(fmaxf(
+                __fmul_rn(ec.nrmse_scale, __fmaf_rn(ds, ds, __fmul_rn(__fmul_rn(__fadd_rn(sp, sp), sq), __fsub_rn(1.0f, ge)))),
+                0.0f));
+            const float D = (q == p) ? 0.0f : exact_diff2(ec.U + (size_t)p * ec.kp, ec.U + (size_t)q * ec.kp, ec.K);
+            const float exact = sqrtf(__fmul_rn(ec.nrmse_scale, __fmaf_rn(ds, ds, __fmul_rn(__fmul_rn(sp, sq), D))));
+            float corr = exact - approx;
+            if (METRIC == kNrmseW) {
+              const float d = __fsub_rn(rs[8 * row], cs[ci]);
+              corr *= ex2_approx(-__fmul_rn(d, d));
+            }
+            f2_add_half(rn[kr], lh, corr);
+            if (cv) f2_add_half(cn[rep], lh, corr);
           }
-          f2_add_half(rn[k], lh, corr);
-          if (cv) f2_add_half(cn[rep], lh, corr);
         }
+        if (step + 1 < CH * HP) tmem_wait8(nxt);
+      }
+      float4 o;
+      f2_split(cn[0], o.x, o.y);
+      f2_split(cn[1], o.z, o.w);
+      cacc[(2 * c) * kEpiThreads] = o;
+      f2_split(cd[0], o.x, o.y);
+      f2_split(cd[1], o.z, o.w);
+      cacc[(2 * c + 1) * kEpiThreads] = o;
+    }
+#pragma unroll
+    for (int kr = 0; kr < R; kr++) {
+      float lo, hi, n, d;
+      f2_split(rn[kr], lo, hi);
+      n = lo + hi;
+      f2_split(rd[kr], lo, hi);
+      d = lo + hi;
+      if (pass == 0) {  // compile-time indices into rsum (the pass loop is not unrolled)
+        rsum[2 * kr] = n;
+        rsum[2 * kr + 1] = d;
+      } else {
+        rsum[2 * (R + kr)] = n;
+        rsum[2 * (R + kr) + 1] = d;
       }
     }
-    float4 o;
-    f2_split(cn[0], o.x, o.y);
-    f2_split(cn[1], o.z, o.w);
-    cacc[(2 * c) * kEpiThreads] = o;
-    f2_split(cd[0], o.x, o.y);
-    f2_split(cd[1], o.z, o.w);
-    cacc[(2 * c + 1) * kEpiThreads] = o;
-  }
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    float lo, hi;
-    f2_split(rn[k], lo, hi);
-    rsum[2 * k] = lo + hi;
-    f2_split(rd[k], lo, hi);
-    rsum[2 * k + 1] = lo + hi;
   }
 }
 
@@ -536,29 +592,31 @@ __device__ __forceinline__ void flush_columns(const float (&x)[NV], int q0, cons
   }
 }
 
-__host__ __device__ inline long long items_before(long long ct, int h) {
-  // sum over column tiles c < ct of ceil((c + 1) / h)
-  const long long Q = ct / h, R = ct - Q * h;
-  return (long long)h * Q * (Q + 1) / 2 + R * (Q + 1);
+// Work items, run-major: run j holds row blocks [jL, jL + L); its items are
+// the column tiles ct = j h .. n_ct - 1 (h = L / (BN / 128): the first column
+// tile that reaches the run's rows), each clipped to the triangle. All CTAs
+// then work on the same row blocks at once, so the A tiles they stream are
+// shared in L2; each item loads its own B tile once.
+__host__ __device__ inline long long items_before_run(long long j, int n_ct, int h) {
+  // sum over runs j' < j of (n_ct - j' h)
+  return j * n_ct - (long long)h * j * (j - 1) / 2;
 }
 
-// Item -> (column tile, row-block run); false for an empty run (rows past n).
+// Item -> (column tile, row-block range); false for an empty range.
 __device__ __forceinline__ bool decode_item(long long it, const TcArgs& g, int m, int& ct, int& rb0, int& rb1) {
-  int lo = 0, hi = g.n_ct - 1;
+  int lo = 0, hi = g.n_runs - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (items_before(mid, g.h) <= it) lo = mid;
+    if (items_before_run(mid, g.n_ct, g.h) <= it) lo = mid;
     else hi = mid - 1;
   }
-  ct = lo;
-  rb0 = (int)(it - items_before(lo, g.h)) * g.L;
-  rb1 = min(rb0 + g.L, min((lo + 1) * m, g.n_rb));
+  ct = lo * g.h + (int)(it - items_before_run(lo, g.n_ct, g.h));
+  rb0 = lo * g.L;
+  rb1 = min(rb0 + g.L, min((ct + 1) * m, g.n_rb));
   return rb0 < rb1;
 }
 
-// End of a role: all warps meet, then the MMA warp frees TMEM. Each role
-// calls it from its own code, so no code after the register split is shared
-// by warps of different register budgets.
+// End of a role: all warps meet, then the MMA warp frees TMEM.
 __device__ __forceinline__ void role_exit(uint32_t tmem, int tmem_cols, bool owner) {
   tc_fence_before();
   __syncthreads();
@@ -596,12 +654,16 @@ __global__ void __launch_bounds__(kThreads, 1)
   float2* rowpart = reinterpret_cast<float2*>(sbase + (sP - base));
   float4* colacc = reinterpret_cast<float4*>(sbase + (sQ - base));
   // barriers: a_full[16], a_empty[16], b_full, b_empty, acc_full[2], acc_empty[2],
-  //           c_full[2], c_empty[2], r_full[4], r_empty[4], p_full[2][4], done
+  //           c_full[2], c_empty[2], r_full[2], r_empty[2], done; then the TMEM
+  //           address and 8 row-partial counters
   const uint32_t b_afull = sBar, b_aempty = b_afull + 8 * kMaxStages, b_bfull = b_aempty + 8 * kMaxStages,
                  b_bempty = b_bfull + 8, b_accf = b_bempty + 8, b_acce = b_accf + 16, b_cfull = b_acce + 16,
                  b_cempty = b_cfull + 16, b_rfull = b_cempty + 16, b_rempty = b_rfull + 8 * kRSlots,
-                 b_pfull = b_rempty + 8 * kRSlots, b_done = b_pfull + 64;
+                 b_done = b_rempty + 8 * kRSlots;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sbase + (b_done + 8 - base));
+  // per (accumulator buffer, quarter): column-group warps that have written
+  // their row partials of the current tile (the fourth combines them)
+  unsigned* rowcnt = tmem_slot + 1;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -621,7 +683,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(b_rfull + 8 * r, 1);
       mbar_init(b_rempty + 8 * r, kEpiWarps);
     }
-    for (int i = 0; i < 8; i++) mbar_init(b_pfull + 8 * i, 4);
+    for (int i = 0; i < 8; i++) rowcnt[i] = 0;
     mbar_init(b_done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -649,50 +711,66 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t cs = item_i & 1;
         // the column-parameter slot the epilogue released two items ago, and the
         // B buffer once the MMAs of the previous item are complete
-        if (!mbar_wait(b_cempty + 8 * cs, ((item_i >> 1) & 1) ^ 1, g, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
-        if (item_i > 0 && !mbar_wait(b_bempty, (item_i - 1) & 1, g, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
+        if (!mbar_wait(b_cempty + 8 * cs, ((item_i >> 1) & 1) ^ 1, g, ST_TIMEOUT_PRODUCER, true, true)) { ok = false; break; }
+        if (item_i > 0 && !mbar_wait(b_bempty, (item_i - 1) & 1, g, ST_TIMEOUT_PRODUCER, true, true)) { ok = false; break; }
         mbar_expect_tx(b_cfull + 8 * cs, C::kCSoa * 4);
         bulk_load(sC + cs * C::kCSoa * 4, g.colsoa + (size_t)ct * C::kCSoa, C::kCSoa * 4, b_cfull + 8 * cs);
         mbar_expect_tx(b_bfull, g.b_bytes);
         for (int c = 0; c < g.nfull; c++) tma_load_2d(sB + c * C::kBChunkBytes, &tmB, b_bfull, c * kChunk, ct * BN);
         if (g.tail) tma_load_2d(sB + g.nfull * C::kBChunkBytes, &tmB64, b_bfull, g.nfull * kChunk, ct * BN);
         item_i++;
+        {  // the B tile of this CTA's next item into L2
+          int nct, nrb0, nrb1;
+          const long long nit = it + gridDim.x;
+          if (nit < g.item1 && decode_item(nit, g, C::kM, nct, nrb0, nrb1) && nct != ct) {
+            for (int c = 0; c < g.nfull; c++) tma_prefetch_2d(&tmB, c * kChunk, nct * BN);
+            if (g.tail) tma_prefetch_2d(&tmB64, g.nfull * kChunk, nct * BN);
+          }
+        }
         for (int rb = rb0; ok && rb < rb1; rb++, tile++) {
           if (tile == g.withhold) { ok = false; break; }
-          const uint32_t rsl = (uint32_t)(tile & (kRSlots - 1));
-          if (!mbar_wait(b_rempty + 8 * rsl, ((tile / kRSlots) & 1) ^ 1, g, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
-          // TR: A buffer tile & 1 is free once the accumulator of tile - 2 is published
-          if (TR && tile >= 2 && !mbar_wait(b_accf + 8 * (tile & 1), ((tile - 2) >> 1) & 1, g, ST_TIMEOUT_PRODUCER)) {
-            ok = false;
-            break;
+          // A two row blocks ahead into L2, so that the copies below hit L2
+          if (rb + 2 < rb1) {
+            for (int c = 0; c < g.nfull; c++) tma_prefetch_2d(&tmA, c * kChunk, (rb + 2) * kBM);
+            if (g.tail) tma_prefetch_2d(&tmA64, g.nfull * kChunk, (rb + 2) * kBM);
           }
-          mbar_expect_tx(b_rfull + 8 * rsl, kRowFloats * 4);
-          bulk_load(sR + rsl * kRowFloats * 4, g.rowsoa + (size_t)rb * kRowFloats, kRowFloats * 4, b_rfull + 8 * rsl);
-          n_r++;
+          // The A operand first (the MMA waits for it), then the row parameters
+          // (the epilogue needs them only once the accumulator is ready).
           if (TR) {
+            // A buffer tile & 1 is free once the accumulator of tile - 2 is published
+            if (tile >= 2 && !mbar_wait(b_accf + 8 * (tile & 1), ((tile - 2) >> 1) & 1, g, ST_TIMEOUT_PRODUCER, true, true)) {
+              ok = false;
+              break;
+            }
             const uint32_t ab = (uint32_t)(tile & 1);
             const uint32_t dst = sA + ab * g.a_bytes;
             mbar_expect_tx(b_afull + 8 * ab, g.a_bytes);
             for (int c = 0; c < g.nfull; c++) tma_load_2d(dst + c * kAChunkBytes, &tmA, b_afull + 8 * ab, c * kChunk, rb * kBM);
             if (g.tail) tma_load_2d(dst + g.nfull * kAChunkBytes, &tmA64, b_afull + 8 * ab, g.nfull * kChunk, rb * kBM);
             n_a++;
-            continue;
-          }
-          for (int kc = 0; kc < nkc; kc++) {
-            if (!mbar_wait(b_aempty + 8 * s, eph ^ 1, g, ST_TIMEOUT_PRODUCER)) { ok = false; break; }
-            if (kc < g.nfull) {
-              mbar_expect_tx(b_afull + 8 * s, kAChunkBytes);
-              tma_load_2d(sA + s * kAChunkBytes, &tmA, b_afull + 8 * s, kc * kChunk, rb * kBM);
-            } else {  // the 32-column tail
-              mbar_expect_tx(b_afull + 8 * s, kAChunkBytes / 2);
-              tma_load_2d(sA + s * kAChunkBytes, &tmA64, b_afull + 8 * s, kc * kChunk, rb * kBM);
+          } else {
+            for (int kc = 0; kc < nkc; kc++) {
+              if (!mbar_wait(b_aempty + 8 * s, eph ^ 1, g, ST_TIMEOUT_PRODUCER, true, true)) { ok = false; break; }
+              if (kc < g.nfull) {
+                mbar_expect_tx(b_afull + 8 * s, kAChunkBytes);
+                tma_load_2d(sA + s * kAChunkBytes, &tmA, b_afull + 8 * s, kc * kChunk, rb * kBM);
+              } else {  // the 32-column tail
+                mbar_expect_tx(b_afull + 8 * s, kAChunkBytes / 2);
+                tma_load_2d(sA + s * kAChunkBytes, &tmA64, b_afull + 8 * s, kc * kChunk, rb * kBM);
+              }
+              n_a++;
+              if (++s == (uint32_t)S) {
+                s = 0;
+                eph ^= 1;
+              }
             }
-            n_a++;
-            if (++s == (uint32_t)S) {
-              s = 0;
-              eph ^= 1;
-            }
+            if (!ok) break;
           }
+          const uint32_t rsl = (uint32_t)(tile & (kRSlots - 1));
+          if (!mbar_wait(b_rempty + 8 * rsl, ((tile / kRSlots) & 1) ^ 1, g, ST_TIMEOUT_PRODUCER, true, true)) { ok = false; break; }
+          mbar_expect_tx(b_rfull + 8 * rsl, kRowFloats * 4);
+          bulk_load(sR + rsl * kRowFloats * 4, g.rowsoa + (size_t)rb * kRowFloats, kRowFloats * 4, b_rfull + 8 * rsl);
+          n_r++;
         }
       }
       // Drain: every issued copy has landed before the CTA may exit.
@@ -723,16 +801,16 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (long long it = g.item0 + blockIdx.x; ok && it < g.item1; it += gridDim.x) {
         int ct, rb0, rb1;
         if (!decode_item(it, g, C::kM, ct, rb0, rb1)) continue;
-        if (!mbar_wait(b_bfull, item_i & 1, g, ST_TIMEOUT_MMA)) { ok = false; break; }
+        if (!mbar_wait(b_bfull, item_i & 1, g, ST_TIMEOUT_MMA, true, true)) { ok = false; break; }
         tc_fence_after();
         item_i++;
         for (int rb = rb0; ok && rb < rb1; rb++, tile++) {
           const uint32_t b = (uint32_t)(tile & 1);
-          if (!mbar_wait(b_acce + 8 * b, ((tile >> 1) & 1) ^ 1, g, ST_TIMEOUT_MMA)) { ok = false; break; }
+          if (!mbar_wait(b_acce + 8 * b, ((tile >> 1) & 1) ^ 1, g, ST_TIMEOUT_MMA, true, true)) { ok = false; break; }
           tc_fence_after();
           const uint32_t d = tmem + b * BN;
           if (TR) {
-            if (!mbar_wait(b_afull + 8 * b, (tile >> 1) & 1, g, ST_TIMEOUT_MMA)) { ok = false; break; }
+            if (!mbar_wait(b_afull + 8 * b, (tile >> 1) & 1, g, ST_TIMEOUT_MMA, true, true)) { ok = false; break; }
             tc_fence_after();
             const uint64_t da0 = a_desc0 + (uint64_t)((b * g.a_bytes) >> 4);
             for (int c = 0; c < g.nfull; c++) {
@@ -751,7 +829,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             continue;
           }
           for (int kc = 0; kc < nkc; kc++) {
-            if (!mbar_wait(b_afull + 8 * s, fph, g, ST_TIMEOUT_MMA)) { ok = false; break; }
+            if (!mbar_wait(b_afull + 8 * s, fph, g, ST_TIMEOUT_MMA, true, true)) { ok = false; break; }
             tc_fence_after();
             if (kc < g.nfull) {
               const uint64_t da = a_desc0 + (uint64_t)(s * (kAChunkBytes >> 4));
@@ -814,7 +892,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + b * BN + group * C::kColW;
         const int p0 = rb * kBM;
         const bool masked = !full || ct * BN <= p0 + kBM - 1;
-        const int cm = METRIC == kPearson ? c_mode(kEps * rsp[4 * kBM] * rmax_c) : kCFirst;
+        const int cm = METRIC == kPearson ? c_mode(kEps * rsp[kRowMax] * rmax_c) : kCFirst;
         const float* csw = csl + group * C::kColW;
         float rsum[8];
         if (masked)
@@ -826,35 +904,42 @@ __global__ void __launch_bounds__(kThreads, 1)
         else
           sym_tile<METRIC, BN, kCExact, false>(taddr, rsp, csw, cacc, p0, q0, g.ec, rsum);
         tc_fence_before();
-        __syncwarp();
-        if (lane == 0) {
-          mbar_arrive(b_acce + 8 * b);
-          mbar_arrive(b_rempty + 8 * rsl);
-        }
         // Row sums: 4 lanes per row, then the 4 column-group warps of this
-        // quarter through shared memory (fixed order), one atomic per row.
+        // quarter through shared memory: the last of them to write its
+        // partials adds the four (fixed order) and issues one atomic per row
+        // and sum. It releases the accumulator only after reading, so no warp
+        // overwrites these partials (two tiles later) before they are read.
         const float2 z = reduce_rows4(rsum);
         const int krow = 2 * (lane & 1) + ((lane >> 1) & 1);
         float2* rp = rowpart + b * (4 * kBM);
         rp[group * kBM + quarter * 32 + (lane >> 2) + 8 * krow] = z;
         __syncwarp();
-        const uint32_t pbar = b_pfull + 8 * (b * 4 + quarter);
-        if (lane == 0) mbar_arrive(pbar);
-        if (!mbar_wait(pbar, (tile >> 1) & 1, g, ST_TIMEOUT_EPI)) {
-          ok = false;
-          break;
+        unsigned last = 0;
+        if (lane == 0) {
+          asm volatile("fence.acq_rel.cta;" ::: "memory");
+          last = (atomicAdd(rowcnt + b * 4 + quarter, 1u) & 3u) == 3u;
+          asm volatile("fence.acq_rel.cta;" ::: "memory");
         }
-        if (lane < 16) {
-          const int row = quarter * 32 + group * 8 + (lane & 7);
-          const int sidx = lane >> 3;
-          float s = 0.0f;
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (last) {
+          const int row = quarter * 32 + lane;
+          float sn = 0.0f, sd = 0.0f;
 #pragma unroll
           for (int gg = 0; gg < 4; gg++) {
             const float2 v = rp[gg * kBM + row];
-            s += sidx ? v.y : v.x;
+            sn += v.x;
+            sd += v.y;
           }
           const int p = p0 + row;
-          if (p < g.ec.n) atomicAdd((sidx ? g.den : g.num) + p, (double)s);
+          if (p < g.ec.n) {
+            atomicAdd(g.num + p, (double)sn);
+            atomicAdd(g.den + p, (double)sd);
+          }
+        }
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(b_acce + 8 * b);
+          mbar_arrive(b_rempty + 8 * rsl);
         }
       }
       if (!ok) break;
@@ -884,9 +969,9 @@ __global__ void __launch_bounds__(kThreads, 1)
 // Column parameters of each BN-column tile, permuted so that thread t of an
 // epilogue warp finds its four columns of a 16-column chunk (2(t%4) + {0, 1}
 // and 8 + 2(t%4) + {0, 1}) in one float4 (col_soa_pos), with the tile's
-// largest 1/sigma; and the row parameters of each 128-row block in natural
-// order with the block's largest 1/sigma. Blocks [0, n_ctp): column tiles;
-// [n_ctp, n_ctp + n_rbp): row blocks.
+// largest 1/sigma; and the row parameters of each 128-row block as the
+// epilogue's f32x2 pairs (kRowSoaFloats) with the block's largest 1/sigma.
+// Blocks [0, n_ctp): column tiles; [n_ctp, n_ctp + n_rbp): row blocks.
 template <int BN>
 __global__ void k_sym_soa(const BlockParams* __restrict__ params, int n_ctp, float* __restrict__ colsoa,
                           float* __restrict__ rowsoa) {
@@ -899,11 +984,18 @@ __global__ void k_sym_soa(const BlockParams* __restrict__ params, int n_ctp, flo
   float r = 0.0f;
   if (i < width) {
     const BlockParams p = params[(size_t)tile * width + i];
-    const int pos = col ? col_soa_pos(i) : i;
-    o[pos] = p.a;
-    o[width + pos] = p.r;
-    o[2 * width + pos] = p.sigma;
-    o[3 * width + pos] = p.mu;
+    if (col) {
+      const int pos = col_soa_pos(i);
+      o[pos] = p.a;
+      o[width + pos] = p.r;
+      o[2 * width + pos] = p.sigma;
+      o[3 * width + pos] = p.mu;
+    } else {
+      const float ne = -kEps * p.r;
+      reinterpret_cast<float4*>(o + 8 * i)[0] = make_float4(p.a, p.a, ne, ne);
+      reinterpret_cast<float4*>(o + 8 * i)[1] = make_float4(p.sigma, p.sigma, p.mu, p.mu);
+      o[kRowR + i] = p.r;
+    }
     r = p.r;
   }
   for (int s = 16; s; s >>= 1) r = fmaxf(r, __shfl_xor_sync(0xffffffffu, r, s));
@@ -913,7 +1005,7 @@ __global__ void k_sym_soa(const BlockParams* __restrict__ params, int n_ctp, flo
     float m = 0.0f;
     if (i == 0)
       for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = fmaxf(m, wm[w]);
-    o[4 * width + i] = m;
+    o[(col ? 4 * width : kRowMax) + i] = m;
   }
 }
 
@@ -978,12 +1070,16 @@ size_t gram_tc_soa_floats(int n_pad) {
 
 long long gram_tc_items(int n, int bn, int* L_out, int num_sms) {
   const int m = bn / kBM;
-  const int n_ct = (n + bn - 1) / bn;
+  const int n_rb = (n + kBM - 1) / kBM, n_ct = (n + bn - 1) / bn;
+  auto items = [&](int L) {
+    const int runs = (n_rb + L - 1) / L;
+    return items_before_run(runs, n_ct, L / m);
+  };
   int L = 16;
-  while (L > 2 && items_before(n_ct, L / m) < 4LL * num_sms) L >>= 1;
+  while (L > 2 && items(L) < 4LL * num_sms) L >>= 1;
   if (L < m) L = m;
   if (L_out) *L_out = L;
-  return items_before(n_ct, L / m);
+  return items(L);
 }
 
 cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int kq, int n_pad,
@@ -1009,6 +1105,7 @@ cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int k
   const long long items = gram_tc_items(ec.n, bn, &L, num_sms);
   g.L = L;
   g.h = L / (bn / kBM);
+  g.n_runs = (g.n_rb + L - 1) / L;
   g.item0 = items * shard / n_shards;
   g.item1 = items * (shard + 1) / n_shards;
   const int n_ctp = n_pad / bn, n_rbp = n_pad / kBM;
