@@ -46,7 +46,7 @@ def _build() -> None:
     mod = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mod)
     mod.build_oracle()
-    mod.build_refshim(Path("/root/reference"))
+    mod.build_refshim(mod.reference_root())
 
 
 def lib() -> C.CDLL:

@@ -383,9 +383,15 @@ def build_refshim(ref: Path, force: bool = False) -> Path | None:
     return out
 
 
+def reference_root() -> Path:
+    """The SReD checkout the recipe reads: $SRED_REFERENCE, else the default
+    location of this build's reference checkout."""
+    return Path(os.environ.get("SRED_REFERENCE", "/root/reference"))
+
+
 def main(argv: list[str] | None = None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("SRED_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=str(reference_root()))
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args(argv)
     print("oracle:", build_oracle(a.force))

@@ -32,7 +32,8 @@ Two kinds of fixtures are written:
    (``cl/kernelGetRelevanceMask2D.cl``, the local variance, and
    ``cl/kernelGetLocalMeans.cl``, the local std) on small seeded images.
 
-Usage: ``python tests/golden/make_golden.py [--reference /root/reference] [--only volume ...]``
+Usage: ``python tests/golden/make_golden.py [--reference <SReD checkout>] [--only volume ...]``
+(default: $SRED_REFERENCE, as ``oracle/refshim/build.py``)
 """
 from __future__ import annotations
 
@@ -79,6 +80,19 @@ def _scalar(body: str, pattern: str) -> float:
     if not m:
         raise ValueError(pattern)
     return float(m.group(1).rstrip("f"))
+
+
+def _class(src: str, name: str) -> str:
+    """Body of the (nested) class `name`."""
+    i = src.index(f"class {name}")
+    j = src.index("{", i)
+    depth = 0
+    for k in range(j, len(src)):
+        depth += src[k] == "{"
+        depth -= src[k] == "}"
+        if depth == 0:
+            return src[j:k + 1]
+    raise ValueError(name)
 
 
 def junit_vectors(ref: Path) -> dict:
@@ -130,6 +144,26 @@ def junit_vectors(ref: Path) -> dict:
     out["normalize_image_2d_invalid"] = {
         "cite": "src/test/java/UtilsTest.java testNormalizeImageWithInvalidMask",
         "width": 4, "height": 4, "image": _array(b, "imageArray"), "mask": _array(b, "invalidMask"),
+    }
+    c = _class(ut, "GetReferenceBlock2DTest")
+    valid = _method(c, "testGetReferenceBlock2DValidBlock")
+    out["reference_block_2d"] = {
+        "cite": "src/test/java/UtilsTest.java GetReferenceBlock2DTest",
+        "width": 5, "height": 5, "pixels": _array(_method(c, "setup"), "pixels"),
+        "expected_mean": _scalar(valid, r"assertEquals\((" + FLOAT + r"),\s*block\.getMean\(\)"),
+        "expected_std": _scalar(valid, r"assertEquals\((" + FLOAT + r"),\s*block\.getStd\(\)"),
+        "expected_radius": [2, 2], "tolerance": 1e-6,
+        "even_pixels": _array(_method(c, "testGetReferenceBlock2DEvenDimensions"), "evenPixels"),
+        "even_width": 4, "even_height": 4,
+    }
+    c = _class(ut, "GetInputImage2DTestOverloaded")
+    nn = _method(c, "testGetInputImage2D_NoStabilization_NoNormalization")
+    wn = _method(c, "testGetInputImage2D_WithNormalization")
+    out["input_image_2d"] = {
+        "cite": "src/test/java/UtilsTest.java GetInputImage2DTest, GetInputImage2DTestOverloaded",
+        "plain": {"width": 3, "height": 3, "pixels": _array(nn, "pixels")},
+        "normalized": {"width": 2, "height": 2, "pixels": _array(wn, "pixels"),
+                       "expected": _array(wn, "normalizedPixels"), "tolerance": 1e-4},
     }
     b = _method(ut, "testApplyMask2D")
     out["apply_mask_2d"] = {
@@ -304,7 +338,9 @@ def relevance_fixtures() -> dict:
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    sys.path.insert(0, str(HERE.parent.parent / "oracle" / "refshim"))
+    from build import reference_root  # noqa: E402
+    ap.add_argument("--reference", default=str(reference_root()))
     ap.add_argument("--only", choices=["junit", "global", "shape", "volume", "relevance"], action="append",
                     help="regenerate only these fixture files (default: all)")
     a = ap.parse_args(argv)
