@@ -315,7 +315,7 @@ def traffic_from_profile():
 
 
 BLOCK_METRICS = ["Pearson's R", "SSIM", "NRMSE (inverted)", "Abs. Diff. of StdDevs.", "Cosine", "Hu moments",
-                 "Phase correlation"]
+                 "Phase correlation", "Hu distance"]
 # FP64 shape metrics run on the first frames of the stack only (they are compute-bound: ~1 ms and ~21 ms per
 # 1024x1024 frame at 15x15), so the block workload still ends within a few minutes.
 SHAPE_FRAMES = 8
@@ -344,7 +344,7 @@ def run_block(args, rank, local, world):
     clocks = Clocks(local)
     clocks.__enter__()
     for metric in BLOCK_METRICS:
-        nf = min(frames, SHAPE_FRAMES) if metric in ("Hu moments", "Phase correlation") else frames
+        nf = min(frames, SHAPE_FRAMES) if metric in ("Hu moments", "Phase correlation", "Hu distance") else frames
         for _ in range(args.warmup):
             clutils.block_map_device(metric, d_in.data_ptr(), 1024, 1024, nf, ref, 0.0, True, d_out.data_ptr(),
                                      stream.cuda_stream, ctx=ctx)

@@ -296,17 +296,19 @@ sred_status sred_phase_correlation_map_2d(sred_ctx *ctx, const float *img, const
                                           const float *local_stds, int w, int h, int bw, int bh, float *out);
 
 /* Block map that allocates nothing (no counterpart in the reference): for
- * callers that cannot call cudaMalloc, such as code inside a CUDA graph being
- * captured, hosts whose runtime owns the device allocator, or loops that must
- * not touch the allocator once started. Same result as
- * sred_block_map_2d_device with relevance_constant 0; needs no context.
- * Runs on the current device and on `stream` (NULL = the default stream) and
- * returns when the map is complete. Scratch is a fixed device array of about
- * 4 MiB that every GPU loading this library holds until exit; the limits are
- * frames <= 4096 and, for NRMSE, frames * w * h <= 1,048,576
- * (SRED_ERR_ARG beyond them). The first call on a device looks the array's
- * device address up (make that first call before any stream capture). Every
- * call shares the array, so calls that overlap on the GPU race. */
+ * callers that cannot call cudaMalloc, such as hosts whose runtime owns the
+ * device allocator, or loops that must not touch the allocator once started.
+ * Same result as sred_block_map_2d_device with relevance_constant 0; needs no
+ * context. Runs on the current device and on `stream` (NULL = the default
+ * stream) and synchronises that stream before it returns, so the map is
+ * complete then. Scratch is a fixed device array of about 4 MiB that every
+ * GPU loading this library holds until exit; the limits are frames <= 4096,
+ * for NRMSE frames * w * h <= 1,048,576, and a block whose image tile with
+ * halo fits in 48 KB of shared memory (every block up to 25 x 25; a 3 x 401
+ * block does not) (SRED_ERR_ARG beyond them). The first call on a device
+ * looks the array's device address up (make that first call before any
+ * stream capture). Every call shares the array, so calls that overlap on the
+ * GPU race. */
 sred_status sred_block_map_2d_device_noalloc(const char *metric, const float *d_img, int w, int h,
                                              int frames, const float *ref_pixels, int block_size, int bw,
                                              int bh, float ref_mean, float ref_std, int normalize_output,

@@ -136,6 +136,9 @@ def lib() -> C.CDLL:
         L.orc_hu_feature.argtypes = [_f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
         L.orc_hu_map.argtypes = [_f32p, _f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f64p]
         L.orc_phase_map.argtypes = [_f32p, _f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _f64p]
+        L.orc_block_hu7.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, _f32p,
+                                    np.ctypeslib.ndpointer(np.float64, flags="C"),
+                                    np.ctypeslib.ndpointer(np.float64, flags="C")]
         L.orc_block_phase.argtypes = [_f32p, _f32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, _f32p,
                                       C.c_float, _f64p]
         _lib = L
@@ -475,6 +478,18 @@ def block_phase_raw(img, ref_pixels, bw, bh, ref_std, means=None, stds=None):
                              C.c_float(ref_std), out):
         raise ValueError("phase correlation supports blocks up to 15x15")
     return out.reshape(H, W)
+
+
+def block_hu7_raw(img, ref_pixels, bw, bh):
+    """Block-map Hu distance before post-processing (FP64): the L2 distance of
+    each block's seven Hu invariants to the reference block's; returns (map,
+    reference 7-vector)."""
+    img = _f32(img)
+    H, W = img.shape
+    out = np.zeros(W * H, np.float64)
+    ref_h = np.zeros(7, np.float64)
+    lib().orc_block_hu7(img, W, H, bw, bh, _f32(ref_pixels), ref_h, out)
+    return out.reshape(H, W), ref_h
 
 
 # --------------------------------------------------------------------------

@@ -2135,3 +2135,85 @@ int orc_gat_tree(float *img, int W, int H, int D, int oct, int min_size, float a
     *edc_out = edc;
     return nl;
 }
+
+/* ------------------------------------------------------------------ */
+/* Block-map Hu distance (this library's north-star Hu metric; the     */
+/* reference outputs only Hu1, cl/kernelGetPatchHu2D.cl:267): the L2    */
+/* distance between the seven Hu invariants (Hu 1962) of each block and */
+/* of the reference block, FP64. Intensities are min-max normalised     */
+/* over the ellipse (all invariants 0 for a flat block); eta_pq =       */
+/* mu_pq / m00^(1 + (p + q) / 2) from the central moments about the     */
+/* intensity centroid, the offsets taken relative to the block centre.  */
+/* ------------------------------------------------------------------ */
+static void orc_hu7_vec(const double *x, const int *dx, const int *dy, int K, double *h) {
+    double mn = x[0], mx = x[0];
+    for (int k = 1; k < K; k++) {
+        if (x[k] < mn) mn = x[k];
+        if (x[k] > mx) mx = x[k];
+    }
+    for (int i = 0; i < 7; i++) h[i] = 0.0;
+    double span = mx - mn;
+    if (!(span > 0.0)) return;
+    double m00 = 0.0, m10 = 0.0, m01 = 0.0;
+    for (int k = 0; k < K; k++) {
+        double v = (x[k] - mn) / span;
+        m00 += v;
+        m10 += (double)dx[k] * v;
+        m01 += (double)dy[k] * v;
+    }
+    double cx = m10 / m00, cy = m01 / m00;
+    double u20 = 0, u11 = 0, u02 = 0, u30 = 0, u21 = 0, u12 = 0, u03 = 0;
+    for (int k = 0; k < K; k++) {
+        double v = (x[k] - mn) / span;
+        double a = (double)dx[k] - cx, b = (double)dy[k] - cy;
+        double a2 = a * a, b2 = b * b;
+        u20 += a2 * v;
+        u11 += (a * b) * v;
+        u02 += b2 * v;
+        u30 += (a2 * a) * v;
+        u21 += (a2 * b) * v;
+        u12 += (a * b2) * v;
+        u03 += (b2 * b) * v;
+    }
+    double s2 = m00 * m00, s3 = s2 * sqrt(m00);
+    double n20 = u20 / s2, n11 = u11 / s2, n02 = u02 / s2;
+    double n30 = u30 / s3, n21 = u21 / s3, n12 = u12 / s3, n03 = u03 / s3;
+    double p = n30 + n12, q = n21 + n03, r = n30 - 3.0 * n12, s = 3.0 * n21 - n03, d = n20 - n02;
+    h[0] = n20 + n02;
+    h[1] = d * d + 4.0 * (n11 * n11);
+    h[2] = r * r + s * s;
+    h[3] = p * p + q * q;
+    h[4] = r * p * (p * p - 3.0 * (q * q)) + s * q * (3.0 * (p * p) - q * q);
+    h[5] = d * (p * p - q * q) + 4.0 * n11 * p * q;
+    h[6] = s * p * (p * p - 3.0 * (q * q)) - r * q * (3.0 * (p * p) - q * q);
+}
+
+/* Raw map (interior pixels; border 0) and the reference 7-vector. */
+void orc_block_hu7(const float *img, int W, int H, int bw, int bh, const float *ref_pixels, double *ref_h,
+                   double *out) {
+    int rw = bw / 2, rh = bh / 2;
+    int *dx = (int *)malloc(sizeof(int) * bw * bh), *dy = (int *)malloc(sizeof(int) * bw * bh);
+    int K = 0;
+    for (int y = -rh; y <= rh; y++)
+        for (int x = -rw; x <= rw; x++)
+            if (in_ellipse(x, y, rw, rh)) { dx[K] = x; dy[K] = y; K++; }
+    double *rv = (double *)malloc(sizeof(double) * K);
+    for (int k = 0; k < K; k++) rv[k] = (double)ref_pixels[k];
+    orc_hu7_vec(rv, dx, dy, K, ref_h);
+    #pragma omp parallel for schedule(static)
+    for (int gy = 0; gy < H; gy++) {
+        double v[1024], h[7];
+        for (int gx = 0; gx < W; gx++) {
+            out[gy * W + gx] = 0.0;
+            if (gx < rw || gx >= W - rw || gy < rh || gy >= H - rh) continue;
+            for (int k = 0; k < K; k++) v[k] = (double)img[(gy + dy[k]) * W + gx + dx[k]];
+            orc_hu7_vec(v, dx, dy, K, h);
+            double s2 = 0.0;
+            for (int i = 0; i < 7; i++) { double t = h[i] - ref_h[i]; s2 += t * t; }
+            out[gy * W + gx] = sqrt(s2);
+        }
+    }
+    free(rv);
+    free(dx);
+    free(dy);
+}

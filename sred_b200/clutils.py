@@ -24,7 +24,8 @@ COSINE = "Cosine"  # raw-vector cosine similarity; no reference counterpart
 # Block-map forms of the reference's shape-metric kernels (no dialog entry in the reference).
 HU = "Hu moments"  # cl/kernelGetPatchHu2D.cl
 PHASE = "Phase correlation"  # cl/kernelGetPhaseCorrelationMap.cl (repaired)
-EXTRA_BLOCK_METRICS = [COSINE, HU, PHASE]
+HU7 = "Hu distance"  # L2 distance of the seven Hu invariants; no reference counterpart (it outputs Hu1 only)
+EXTRA_BLOCK_METRICS = [COSINE, HU, PHASE, HU7]
 BLOCK_METRICS_3D = ["Pearson's R", "SSIM", "NRMSE (inverted)", "Abs. Diff. of StdDevs."]  # java/BlockRepetition3D_.java:19-24
 
 

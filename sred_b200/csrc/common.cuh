@@ -19,7 +19,8 @@ enum Metric { kPearson = 0, kSsim = 1, kNrmse = 2, kAbsDiff = 3, kCosine = 4,
               kNrmseW = 8 /* NRMSE with each term weighted (the 3D global kernel) */,
               // NRMSE from the accumulated squared difference of the unit
               // vectors (FP32 engine): unweighted (2D) and weighted (3D)
-              kNrmseD = 9, kNrmseDW = 10 };
+              kNrmseD = 9, kNrmseDW = 10,
+              kHu7 = 11 /* block map: distance of the seven Hu invariants */ };
 
 // The FP32 engine's accumulator holds sum_i (u_p,i - u_q,i)^2 instead of the
 // dot product for these metrics.

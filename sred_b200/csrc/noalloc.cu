@@ -1,17 +1,22 @@
 // Allocation-free block repetition map.
 //
-// Some callers cannot call cudaMalloc at all: code running inside a CUDA
-// graph that is being captured, host runtimes that own the device allocator
-// and forbid foreign allocations, and real-time loops that must not touch the
-// allocator once started. For them this entry point computes the same block
-// map as sred_block_map_2d_device without allocating anything: the little
-// device scratch it needs (the per-frame min/max words of the normalisation
-// and, for NRMSE, the interior mask) lives in one file-scope __device__ array
-// of fixed size that every GPU loading this library holds until exit.
+// Some callers cannot call cudaMalloc at all: host runtimes that own the
+// device allocator and forbid foreign allocations, and real-time loops that
+// must not touch the allocator once started. For them this entry point
+// computes the same block map as sred_block_map_2d_device without allocating
+// anything: the little device scratch it needs (the per-frame min/max words
+// of the normalisation and, for NRMSE, the interior mask) lives in one
+// file-scope __device__ array of fixed size that every GPU loading this
+// library holds until exit. The call synchronises its stream before it
+// returns; the caller's buffers are complete then.
 //
 // Host code must not use the array's name as a device address (there it is
 // a host-side stand-in); the device address is obtained once per device with
-// cudaGetSymbolAddress, on the first call made while that device is current.
+// cudaGetSymbolAddress, on the first call made while that device is current
+// (make that first call before any stream capture). Limits: at most 4096
+// frames, for NRMSE frames * w * h <= 1,048,576, and an image tile with halo
+// of at most 48 KB of shared memory (blocks whose ellipse needs more, such as
+// 3 x 401, are refused); SRED_ERR_ARG beyond any of them.
 #include <cstring>
 #include <mutex>
 

@@ -83,6 +83,46 @@ __global__ void __launch_bounds__(128)
 }
 
 // ---------------------------------------------------------------------------
+// Block-map Hu distance: the seven Hu invariants of each block against the
+// reference block's, one thread per pixel (FP64; hu7_invariants).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128)
+    k_block_hu7(const float* __restrict__ img_all, int W, int H, Ellipse e, Hu7Ref ref, float* __restrict__ out_all,
+                float* __restrict__ stds_out) {
+  const size_t plane = (size_t)W * H;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= plane) return;
+  const size_t off = (size_t)blockIdx.y * plane;
+  const float* img = img_all + off;
+  const int x = (int)(idx % W), y = (int)(idx / W);
+  if (x < e.rw || x >= W - e.rw || y < e.rh || y >= H - e.rh) {
+    out_all[off + idx] = 0.0f;
+    if (stds_out) stds_out[off + idx] = 0.0f;
+    return;
+  }
+  const float* c = img + idx;
+  if (stds_out) {
+    float m, sd;
+    block_stats_f32(c, W, e, &m, &sd);
+    stds_out[off + idx] = sd;
+  }
+  double h[7];
+  hu7_invariants([&](int k) { return (double)__ldg(c + e.dy[k] * W + e.dx[k]); }, e, h);
+  out_all[off + idx] = (float)hu7_distance(h, ref.h);
+}
+
+void launch_block_hu7(const float* img, int W, int H, int frames, const Ellipse& e, const Hu7Ref& ref, float* out,
+                      float* stds_out, cudaStream_t st) {
+  const size_t plane = (size_t)W * H;
+  k_block_hu7<<<dim3((unsigned)((plane + 127) / 128), (unsigned)frames), 128, 0, st>>>(img, W, H, e, ref, out,
+                                                                                        stds_out);
+}
+
+void hu7_reference(const float* ref_pixels, const Ellipse& e, Hu7Ref* out) {
+  hu7_invariants([&](int k) { return (double)ref_pixels[k]; }, e, out->h);
+}
+
+// ---------------------------------------------------------------------------
 // Hu map, kernelGetHuMap.cl (FP32): per-block feature, then all pairs.
 // ---------------------------------------------------------------------------
 

@@ -121,6 +121,81 @@ __device__ __forceinline__ void block_stats_f32(const float* c, int W, const Ell
   *std_out = __fsqrt_rn(__fdiv_rn(v, (float)(e.k - 1)));
 }
 
+// Hu's seven moment invariants (M.-K. Hu, "Visual pattern recognition by
+// moment invariants", IRE Trans. Inf. Theory 8(2):179-187, 1962) of one
+// block's intensities v_k at the ellipse offsets (dx_k, dy_k), in FP64:
+// v = (x - min) / (max - min) over the block (every invariant 0 for a flat
+// block), centroid from the raw moments, central moments mu_pq for
+// p + q = 2, 3, normalised eta_pq = mu_pq / m00^(1 + (p + q) / 2). `get(k)`
+// returns x_k as a double; the same function serves the device (image
+// blocks) and the host (the reference block), so both sides round alike.
+template <class Get>
+__host__ __device__ inline void hu7_invariants(Get get, const Ellipse& e, double* h) {
+  double mn = get(0), mx = mn;
+  for (int k = 1; k < e.k; k++) {
+    const double x = get(k);
+    mn = x < mn ? x : mn;
+    mx = x > mx ? x : mx;
+  }
+  for (int i = 0; i < 7; i++) h[i] = 0.0;
+  const double span = mx - mn;
+  if (!(span > 0.0)) return;
+  double m00 = 0.0, m10 = 0.0, m01 = 0.0;
+  for (int k = 0; k < e.k; k++) {
+    const double v = (get(k) - mn) / span;
+    m00 += v;
+    m10 += (double)e.dx[k] * v;
+    m01 += (double)e.dy[k] * v;
+  }
+  const double cx = m10 / m00, cy = m01 / m00;
+  double u20 = 0.0, u11 = 0.0, u02 = 0.0, u30 = 0.0, u21 = 0.0, u12 = 0.0, u03 = 0.0;
+  for (int k = 0; k < e.k; k++) {
+    const double v = (get(k) - mn) / span;
+    const double a = (double)e.dx[k] - cx, b = (double)e.dy[k] - cy;
+    const double a2 = a * a, b2 = b * b;
+    u20 += a2 * v;
+    u11 += (a * b) * v;
+    u02 += b2 * v;
+    u30 += (a2 * a) * v;
+    u21 += (a2 * b) * v;
+    u12 += (a * b2) * v;
+    u03 += (b2 * b) * v;
+  }
+  const double s2 = m00 * m00, s3 = s2 * sqrt(m00);
+  const double n20 = u20 / s2, n11 = u11 / s2, n02 = u02 / s2;
+  const double n30 = u30 / s3, n21 = u21 / s3, n12 = u12 / s3, n03 = u03 / s3;
+  const double p = n30 + n12, q = n21 + n03, r = n30 - 3.0 * n12, s = 3.0 * n21 - n03;
+  const double d = n20 - n02;
+  h[0] = n20 + n02;
+  h[1] = d * d + 4.0 * (n11 * n11);
+  h[2] = r * r + s * s;
+  h[3] = p * p + q * q;
+  h[4] = r * p * (p * p - 3.0 * (q * q)) + s * q * (3.0 * (p * p) - q * q);
+  h[5] = d * (p * p - q * q) + 4.0 * n11 * p * q;
+  h[6] = s * p * (p * p - 3.0 * (q * q)) - r * q * (3.0 * (p * p) - q * q);
+}
+
+// L2 distance of two Hu 7-vectors.
+__host__ __device__ inline double hu7_distance(const double* a, const double* b) {
+  double s = 0.0;
+  for (int i = 0; i < 7; i++) {
+    const double t = a[i] - b[i];
+    s += t * t;
+  }
+  return sqrt(s);
+}
+
+struct Hu7Ref {
+  double h[7];
+};
+
+// Block-map Hu distance (shape.cu): the frames x W x H raw map (and the FP32
+// local stds when stds_out is given) on stream st.
+void launch_block_hu7(const float* img, int W, int H, int frames, const Ellipse& e, const Hu7Ref& ref, float* out,
+                      float* stds_out, cudaStream_t st);
+// The reference block's 7-vector from its ellipse pixels (ReferenceBlock2D).
+void hu7_reference(const float* ref_pixels, const Ellipse& e, Hu7Ref* out);
+
 // Block-map phase correlation against the reference block's DFT (shape.cu):
 // the frames x W x H raw map (and the FP32 local stds when stds_out is given)
 // on stream st; bw, bh <= kPhaseMaxDim.

@@ -155,6 +155,7 @@ int block_metric(const char* m) {
   if (!std::strcmp(m, "Cosine")) return kCosine;
   if (!std::strcmp(m, "Hu moments")) return kHu;
   if (!std::strcmp(m, "Phase correlation")) return kPhase;
+  if (!std::strcmp(m, "Hu distance")) return kHu7;
   return -1;
 }
 
@@ -474,6 +475,10 @@ sred_status block_shape_launch(sred_ctx* c, int metric, const float* d_img, int 
     std::vector<float> patch((size_t)bw * bh);
     hu_prepare_patch(ref_pixels, bw, bh, patch.data());
     k_patch_hu<<<grid, 128, 0, st>>>(d_img, w, h, e, e.k, patch_hu1(patch.data(), bw, bh), d_out, d_stds);
+  } else if (metric == kHu7) {
+    Hu7Ref r;
+    hu7_reference(ref_pixels, e, &r);
+    launch_block_hu7(d_img, w, h, frames, e, r, d_out, d_stds, st);
   } else {
     if (bw > kPhaseMaxDim || bh > kPhaseMaxDim)
       return fail(c, SRED_ERR_ARG, "phase correlation supports blocks up to 15x15");
@@ -504,7 +509,7 @@ sred_status block_core(sred_ctx* c, int metric, const float* d_img, int w, int h
   const bool need_mask = (metric == kNrmse) || relc > 0.0f;
   float* d_stds = nullptr;
   if (need_mask) CKS(ensure(c, B_STDS2, n, &d_stds));
-  if (metric == kHu || metric == kPhase) {
+  if (metric == kHu || metric == kHu7 || metric == kPhase) {
     CKS(block_shape_launch(c, metric, d_img, w, h, frames, e, ref_pixels, bw, bh, ref_std, d_out, d_stds, st));
   } else {
     dim3 grid, blk;

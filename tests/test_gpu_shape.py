@@ -112,6 +112,45 @@ def test_block_shape_metrics(ctx, shape_fx, metric):
             np.testing.assert_allclose(got, a, atol=1e-6, rtol=0, err_msg=f"{name} c={c}")
 
 
+def test_block_hu_distance(ctx, shape_fx):
+    """Block-map Hu distance (the L2 distance of the seven Hu invariants to the
+    reference block's; this library's metric, the reference outputs Hu1 only):
+    the raw map within 1e-6 of the FP64 oracle on every shape fixture (relative
+    to the map's largest distance), about 0 at the reference block's own
+    position, frame stacks equal to single frames, and the post-processing of
+    the other block metrics (relevance mask, min-max normalisation)."""
+    from sred_b200 import synth
+    for name, bw, bh in _cases(shape_fx):
+        img = shape_fx[f"{name}/image"]
+        H, W = img.shape
+        rb = _block(shape_fx, name, bw, bh)
+        raw = clutils.calculate_block_repetition_map_2d(clutils.HU7, _inp(img), rb, 0.0, False, ctx=ctx)
+        exp, _ = oracle.block_hu7_raw(img, rb.pixels[:rb.size], bw, bh)
+        scale = float(np.max(exp))
+        assert scale > 0 and float(np.max(np.abs(raw - exp.ravel()))) <= 1e-6 * scale, name
+        _, stds = oracle.local_stats(img, bw, bh)
+        for c in (0.0, 1.0):
+            got = clutils.calculate_block_repetition_map_2d(clutils.HU7, _inp(img), rb, c, True, ctx=ctx)
+            a = np.ascontiguousarray(exp, np.float32).ravel().copy()
+            rc = oracle.lib().orc_block_postprocess_f32(0, a, np.ascontiguousarray(img, np.float32), W, H,
+                                                        bw // 2, bh // 2, stds, np.float32(c), 1)
+            assert rc == 0
+            np.testing.assert_allclose(got, a, atol=2e-6, rtol=0, err_msg=f"{name} c={c}")
+    img = synth.normalize_input(synth.spot_image(45, 37, 6, seed=77))
+    rb = utils.get_reference_block_2d(img[15:24, 18:27])  # 9 x 9 centred at (19, 22)
+    raw = clutils.calculate_block_repetition_map_2d(clutils.HU7, _inp(img), rb, 0.0, False, ctx=ctx).reshape(37, 45)
+    assert raw[19, 22] <= 1e-6 * float(raw.max())
+    torch = pytest.importorskip("torch")
+    stack = np.stack([img, img[::-1].copy()])
+    d_in = torch.from_numpy(stack).cuda()
+    d_out = torch.empty_like(d_in)
+    clutils.block_map_device(clutils.HU7, d_in.data_ptr(), 45, 37, 2, rb, 0.0, False, d_out.data_ptr(), ctx=ctx)
+    torch.cuda.synchronize()
+    for f in range(2):
+        single = clutils.calculate_block_repetition_map_2d(clutils.HU7, _inp(stack[f]), rb, 0.0, False, ctx=ctx)
+        assert np.array_equal(d_out[f].cpu().numpy().ravel(), single), f
+
+
 @pytest.mark.parametrize("bw,bh", [(7, 7), (11, 9), (13, 13), (15, 15), (15, 7), (3, 15), (5, 11)])
 def test_block_phase_every_block_size(ctx, bw, bh):
     """The block-map phase kernel is instantiated per max(bw, bh) (3 ... 15),

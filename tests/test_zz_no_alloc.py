@@ -1,8 +1,8 @@
 """The allocation-free block map entry point, through the C ABI.
 
 sred_block_map_2d_device_noalloc serves callers that cannot call cudaMalloc
-(a CUDA graph under capture, a host runtime that owns the device allocator,
-a real-time loop that must not allocate). It keeps its scratch in a fixed
+(a host runtime that owns the device allocator, a real-time loop that must
+not allocate). It keeps its scratch in a fixed
 device array shared by all calls, so this test checks two calls in a row on
 different inputs (nothing left over from the first call may leak into the
 second) against the regular entry point, sred_block_map_2d_device, with the
@@ -64,3 +64,8 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     d = torch.zeros(1025 * 1025, device="cuda")
     assert _noalloc("NRMSE (inverted)", d, 1025, 1025, 1, ref, True, d, torch) == _lib.ERR_ARG
     assert _noalloc("nope", d, 1025, 1025, 1, ref, True, d, torch) == _lib.ERR_UNKNOWN_METRIC
+    # a block whose image tile with halo needs more than 48 KB of shared memory
+    L = _lib.load()
+    k = L.sred_block_size(3, 401)
+    tall = utils.ReferenceBlock2D(np.zeros(k, np.float32), 3, 401, 1, 200, k, 0.0, 1.0)
+    assert _noalloc("Pearson's R", d, 1025, 1025, 1, tall, True, d, torch) == _lib.ERR_ARG
