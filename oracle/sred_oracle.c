@@ -955,25 +955,66 @@ int orc_phase_map(const float *img, const float *means, const float *stds, int W
  * reference has only the all-pairs kernel): the reference block
  * (ReferenceBlock2D pixels / (std + eps)) and each interior block
  * ((x - mean) / (std + eps) with the block's FP32 local statistics), both on
- * the ellipse and 0 elsewhere on the bw x bh grid, go through the kernel's
- * DFT, cross-power, inverse DFT and peak search; out = peak distance. */
+ * the ellipse and 0 elsewhere on the bw x bh grid, go through the exact DFT
+ * (twiddles cos / sin(2 pi m / L), m = (a b) mod L; direct sums, rows then
+ * columns), the kernel's normalised cross-power spectrum (:108-130), the real
+ * part of the exact inverse DFT (rows, then columns) divided by
+ * sqrt(bw bh), and the kernel's peak search (:144-157: first strict maximum
+ * above 0 in raster order, 1-based coordinates); out = peak distance. */
+static void orc_exact_tables(int L, double *c, double *s) {
+    const double two_pi = 6.283185307179586476925286766559;
+    for (int m = 0; m < L; m++) {
+        c[m] = cos(two_pi * m / L);
+        s[m] = sin(two_pi * m / L);
+    }
+}
+
+static void orc_exact_dft(const double *x, int bw, int bh, const double *cw, const double *sw, const double *ch,
+                          const double *sh, double *re, double *im) {
+    double tr[225], ti[225];
+    for (int jj = 0; jj < bh; jj++)
+        for (int i = 0; i < bw; i++) {
+            double sr = 0.0, si = 0.0;
+            for (int ii = 0; ii < bw; ii++) {
+                const int m = (i * ii) % bw;
+                sr += x[jj * bw + ii] * cw[m];
+                si -= x[jj * bw + ii] * sw[m];
+            }
+            tr[jj * bw + i] = sr;
+            ti[jj * bw + i] = si;
+        }
+    for (int j = 0; j < bh; j++)
+        for (int i = 0; i < bw; i++) {
+            double sr = 0.0, si = 0.0;
+            for (int jj = 0; jj < bh; jj++) {
+                const int m = (j * jj) % bh;
+                sr += tr[jj * bw + i] * ch[m] + ti[jj * bw + i] * sh[m];
+                si += ti[jj * bw + i] * ch[m] - tr[jj * bw + i] * sh[m];
+            }
+            re[j * bw + i] = sr;
+            im[j * bw + i] = si;
+        }
+}
+
 int orc_block_phase(const float *img, const float *means, const float *stds, int W, int H, int bw, int bh,
                     const float *ref_pixels, float ref_std, double *out) {
     const int rw = bw / 2, rh = bh / 2, n = bw * bh;
-    if (n > 225) return -1;
-    double *tc = (double *)malloc(sizeof(double) * n * n), *ts = (double *)malloc(sizeof(double) * n * n);
-    orc_phase_tables(bw, bh, tc, ts);
+    if (bw > 15 || bh > 15) return -1;
+    double cw[15], sw[15], ch[15], sh[15];
+    orc_exact_tables(bw, cw, sw);
+    orc_exact_tables(bh, ch, sh);
     double x[225], rr[225], ri[225];
     int k = 0;
     for (int j = 0; j < bh; j++)
         for (int i = 0; i < bw; i++)
             x[j * bw + i] = in_ellipse(i - rw, j - rh, rw, rh)
                                 ? (double)ref_pixels[k++] / ((double)ref_std + ORC_EPS) : 0.0;
-    orc_phase_dft(x, n, tc, ts, rr, ri);
+    orc_exact_dft(x, bw, bh, cw, sw, ch, sh, rr, ri);
+    const double sn = sqrt((double)n);
     #pragma omp parallel for schedule(dynamic, 4)
     for (int y = 0; y < H; y++)
         for (int xq = 0; xq < W; xq++) {
-            double x[225], cr[225], ci[225], xr[225], xi[225];
+            double xv[225], cr[225], ci[225], xr[225], xi[225], sr_[225], si_[225];
             if (xq < rw || xq >= W - rw || y < rh || y >= H - rh) {
                 out[y * W + xq] = 0.0;
                 continue;
@@ -981,12 +1022,47 @@ int orc_block_phase(const float *img, const float *means, const float *stds, int
             const double m = (double)means[y * W + xq], s = (double)stds[y * W + xq] + ORC_EPS;
             for (int j = 0; j < bh; j++)
                 for (int i = 0; i < bw; i++)
-                    x[j * bw + i] = in_ellipse(i - rw, j - rh, rw, rh)
-                                        ? ((double)img[(y + j - rh) * W + xq + i - rw] - m) / s : 0.0;
-            orc_phase_dft(x, n, tc, ts, cr, ci);
-            out[y * W + xq] = (double)orc_phase_peak(rr, ri, cr, ci, bw, bh, tc, ts, xr, xi);
+                    xv[j * bw + i] = in_ellipse(i - rw, j - rh, rw, rh)
+                                         ? ((double)img[(y + j - rh) * W + xq + i - rw] - m) / s : 0.0;
+            orc_exact_dft(xv, bw, bh, cw, sw, ch, sh, cr, ci);
+            for (int i = 0; i < n; i++) {
+                double conj = (-1) * (ci[i] / sn), q = cr[i] / sn;
+                double multReal = rr[i] * q - ri[i] * conj;
+                double multImag = rr[i] * conj + ri[i] * q;
+                double ar = fabs(multReal), ai = fabs(multImag);
+                xr[i] = ((multReal * ar) + (multImag * ai)) / ((ar * ar) + (ai * ai) + ORC_EPS);
+                xi[i] = ((multImag * ar) - (multReal * ai)) / ((ar * ar) + (ai * ai) + ORC_EPS);
+            }
+            /* inverse: rows, then the real part over columns */
+            for (int jj = 0; jj < bh; jj++)
+                for (int i = 0; i < bw; i++) {
+                    double a = 0.0, b = 0.0;
+                    for (int ii = 0; ii < bw; ii++) {
+                        const int mm = (i * ii) % bw;
+                        a += xr[jj * bw + ii] * cw[mm] - xi[jj * bw + ii] * sw[mm];
+                        b += xr[jj * bw + ii] * sw[mm] + xi[jj * bw + ii] * cw[mm];
+                    }
+                    sr_[jj * bw + i] = a;
+                    si_[jj * bw + i] = b;
+                }
+            double max_value = 0.0;
+            int xc = 0, yc = 0;
+            for (int j = 0; j < bh; j++)
+                for (int i = 0; i < bw; i++) {
+                    double v = 0.0;
+                    for (int jj = 0; jj < bh; jj++) {
+                        const int mm = (j * jj) % bh;
+                        v += sr_[jj * bw + i] * ch[mm] - si_[jj * bw + i] * sh[mm];
+                    }
+                    v /= sn;
+                    if (v > max_value) {
+                        max_value = v;
+                        xc = i + 1;
+                        yc = j + 1;
+                    }
+                }
+            out[y * W + xq] = (double)(float)sqrt(((double)xc * (double)xc) + ((double)yc * (double)yc));
         }
-    free(tc); free(ts);
     return 0;
 }
 

@@ -5,6 +5,8 @@
 // multiply-add would round differently.
 #include <float.h>
 
+#include <cmath>
+
 #include "common.cuh"
 #include "kernels.cuh"
 #include "shape.cuh"
@@ -338,19 +340,58 @@ __device__ __forceinline__ int phase_group_peak(double* re, double* im, const do
   return bidx;
 }
 
-// (five CTAs per SM for the two largest sizes: 9.5 instead of 10.1 ms per
-// 1024 x 1024 frame at 15 x 15; the smaller sizes run best unconstrained)
+// Block-map form (this library's definition; the reference wires phase
+// correlation into no block map): the exact DFT, twiddles e^{-2 pi i m / L}
+// (PhaseRef), of each block normalised as (x - mean) / (std + eps) with its FP32
+// local statistics and restricted to the ellipse, the kernel's normalised
+// cross-power spectrum with the reference block's DFT, the real part of the
+// inverse DFT and the kernel's peak rule (largest value above 0, lowest raster
+// index on ties; 1-based coordinates). With exact roots of unity a length-L
+// line transform pairs x_n with x_{L-n}: a_n = x_n + x_{L-n} and
+// b_n = x_n - x_{L-n} share the cosine and sine of each output pair (k, L - k),
+// (L - 1)^2 real multiply-adds per complex line instead of 4 L^2, and the
+// forward transform of the real patch is Hermitian, so it needs half its rows'
+// outputs and (bw + 1) / 2 column lines. Lines are read from the group's
+// shared buffers already paired, so every register index is a compile-time
+// constant.
+//
+// A group of D = max(bw, bh) lanes evaluates one pixel at a time as in the
+// all-pairs kernel (PhaseShape): lane t holds line t of each stage.
+// phase_cross with x / sn given as x and 1/sn, and the two quotients by the
+// shared denominator as one correctly rounded reciprocal and Markstein's
+// correction (div_fixed): every quotient is the IEEE one, as in phase_cross.
+__device__ __forceinline__ void phase_cross_fixed(double rr, double ri, double fr, double fi, double sn, double rsn,
+                                                  double* xr, double* xi) {
+  const double qr = div_fixed(fr, sn, rsn), qi = div_fixed(fi, sn, rsn);
+  const double conj = (-1) * qi;
+  const double mr = rr * qr - ri * conj;
+  const double mi = rr * conj + ri * qr;
+  const double ar = fabs(mr), ai = fabs(mi);
+  const double den = (ar * ar) + (ai * ai) + (double)kEps;
+  const double rden = __drcp_rn(den);
+  *xr = div_fixed((mr * ar) + (mi * ai), den, rden);
+  *xi = div_fixed((mi * ar) - (mr * ai), den, rden);
+}
+
 template <int D>
-__global__ void __launch_bounds__(128, D >= 13 ? 5 : 0)
+__global__ void __launch_bounds__(128)
     k_block_phase(const float* __restrict__ img_all, int W, int H, Ellipse e, int bw, int bh, PhaseRef ref,
                   float* __restrict__ out_all, float* __restrict__ stds_out) {
   using S = PhaseShape<D>;
-  __shared__ double tw[4 * D * D];
+  constexpr int HD = (D - 1) / 2;
+  __shared__ double tcw[HD * HD + 1], tsw[HD * HD + 1], tch[HD * HD + 1], tsh[HD * HD + 1];
   __shared__ double rre[D * D], rim[D * D];
   __shared__ double buf[S::NG][2 * D * D];
   __shared__ int s_img[D * D], s_grid[D * D];  // ellipse: image offset, patch position
-  double *cw = tw, *sw = tw + bw * bw, *ch = sw + bw * bw, *sh = ch + bh * bh;
-  phase_twiddles_smem(bw, bh, cw, sw, ch, sh);
+  const int hw = (bw - 1) / 2, hh = (bh - 1) / 2;
+  // c(n, k) = cos(2 pi (n k mod L) / L) at (n - 1) HD + k - 1, n, k = 1 .. (L - 1) / 2
+  for (int k = threadIdx.x; k < HD * HD; k += blockDim.x) {
+    const int n = k / HD + 1, m = k % HD + 1;
+    tcw[k] = n <= hw && m <= hw ? ref.cw[(n * m) % bw] : 0.0;
+    tsw[k] = n <= hw && m <= hw ? ref.sw[(n * m) % bw] : 0.0;
+    tch[k] = n <= hh && m <= hh ? ref.ch[(n * m) % bh] : 0.0;
+    tsh[k] = n <= hh && m <= hh ? ref.sh[(n * m) % bh] : 0.0;
+  }
   const int nn = bw * bh;
   for (int k = threadIdx.x; k < nn; k += blockDim.x) {
     rre[k] = ref.re[k];
@@ -375,7 +416,7 @@ __global__ void __launch_bounds__(128, D >= 13 ? 5 : 0)
   const float* img = img_all + off;
   float* out = out_all + off;
   const int rw = e.rw, rh = e.rh;
-  const double sn = sqrt((double)(bw * bh));
+  const double sn = sqrt((double)(bw * bh)), rsn = __drcp_rn(sn);
   const size_t first = (size_t)blockIdx.x * S::PIX + (size_t)(warp * S::P + gw) * D;
   // local statistics of the group's D pixels, lane t for pixel first + t
   float own_m = 0.0f, own_s = 0.0f;
@@ -403,69 +444,192 @@ __global__ void __launch_bounds__(128, D >= 13 ? 5 : 0)
     const bool act = idx < plane && x >= rw && x < W - rw && y >= rh && y < H - rh;
     const float mf = __shfl_sync(full, own_m, base + n);
     const float sf = __shfl_sync(full, own_s, base + n);
-    const double m = (double)mf, sd = (double)sf + (double)kEps;
+    const double m = (double)mf, sd = (double)sf + (double)kEps, rsd = __drcp_rn(sd);
     // the patch, in the real buffer
     if (live)
       for (int k = t; k < nn; k += D) re[k] = 0.0;
     __syncwarp();
     if (live && act) {
       const float* c = img + (size_t)y * W + x;
-      for (int k = t; k < e.k; k += D) re[s_grid[k]] = ((double)c[s_img[k]] - m) / sd;
+      for (int k = t; k < e.k; k += D) re[s_grid[k]] = div_fixed((double)c[s_img[k]] - m, sd, rsd);
     }
     __syncwarp();
-    // Each stage: the lane holds its line in registers and walks the
-    // outputs it owns, each one sequential sum; the lines are overwritten
-    // only after every lane of the warp has read its own.
-    double lr[D], li[D];
-    // forward, rows: lane jj, T(i, jj) = sum_ii x[jj][ii] e^{-i a(i, ii)}
+    // paired line registers: x0, a_n, b_n (n = 1 .. HD), real and imaginary
+    double x0r = 0.0, x0i = 0.0, ar[HD], ai[HD], br[HD], bi[HD];
+    // forward, rows (real): lane jj, T(i, jj) for i = 0 .. hw
     if (t < bh) {
+      const double* row = re + t * bw;
+      x0r = row[0];
 #pragma unroll
-      for (int ii = 0; ii < D; ii++) lr[ii] = ii < bw ? re[t * bw + ii] : 0.0;
-    }
-    __syncwarp();
-    if (t < bh) {
-      for (int i = 0; i < bw; i++) {
-        double ar = 0.0, ai = 0.0;
-#pragma unroll
-        for (int ii = 0; ii < D; ii++) {
-          if (ii < bw) {
-            const double v = lr[ii];
-            ar += v * cw[i * bw + ii];
-            ai -= v * sw[i * bw + ii];
-          }
-        }
-        re[i * bh + t] = ar;
-        im[i * bh + t] = ai;
+      for (int q = 1; q <= HD; q++) {
+        const double u = q <= hw ? row[q] : 0.0, v = q <= hw ? row[bw - q] : 0.0;
+        ar[q - 1] = u + v;
+        br[q - 1] = u - v;
       }
     }
     __syncwarp();
-    // forward, columns: lane i holds T(i, :); F(j, i) = sum_jj T(i, jj) e^{-i b(j, jj)},
-    // then the normalised cross-power spectrum with the reference, X(j, i)
-    if (t < bw) {
+    if (t < bh) {
+      double s0 = x0r;
 #pragma unroll
-      for (int jj = 0; jj < D; jj++) {
-        lr[jj] = jj < bh ? re[t * bh + jj] : 0.0;
-        li[jj] = jj < bh ? im[t * bh + jj] : 0.0;
+      for (int q = 0; q < HD; q++) s0 += ar[q];
+      re[t] = s0;  // T(0, jj) at 0 * bh + jj
+      im[t] = 0.0;
+      for (int k = 1; k <= hw; k++) {
+        double pr = x0r, qi = 0.0;
+#pragma unroll
+        for (int q = 0; q < HD; q++) {
+          pr = __fma_rn(ar[q], tcw[q * HD + k - 1], pr);
+          qi = __fma_rn(br[q], tsw[q * HD + k - 1], qi);
+        }
+        re[k * bh + t] = pr;  // e^{-i}: X_k = P - i Q
+        im[k * bh + t] = -qi;
       }
     }
     __syncwarp();
-    if (t < bw) {
-      for (int j = 0; j < bh; j++) {
-        double br = 0.0, bi = 0.0;
+    // forward, columns i = 0 .. hw (complex): F(j, i); the mirrored columns
+    // bw - i are F(bh - j, bw - i) = conj(F(j, i)). Each output leaves as the
+    // normalised cross-power spectrum X with the reference.
+    if (t <= hw) {
+      const double* cr = re + t * bh;
+      const double* ci = im + t * bh;
+      x0r = cr[0];
+      x0i = ci[0];
 #pragma unroll
-        for (int jj = 0; jj < D; jj++) {
-          if (jj < bh) {
-            const double c = ch[j * bh + jj], s = sh[j * bh + jj];
-            br += lr[jj] * c + li[jj] * s;
-            bi += li[jj] * c - lr[jj] * s;
-          }
-        }
+      for (int q = 1; q <= HD; q++) {
+        const bool in = q <= hh;
+        const double ur = in ? cr[q] : 0.0, ui = in ? ci[q] : 0.0;
+        const double vr = in ? cr[bh - q] : 0.0, vi = in ? ci[bh - q] : 0.0;
+        ar[q - 1] = ur + vr;
+        ai[q - 1] = ui + vi;
+        br[q - 1] = ur - vr;
+        bi[q - 1] = ui - vi;
+      }
+    }
+    __syncwarp();
+    if (t <= hw) {
+      auto emit = [&](int j, double fr, double fi) {
         const int k = j * bw + t;
-        phase_cross(rre[k], rim[k], br / sn, bi / sn, &re[k], &im[k]);
+        phase_cross_fixed(rre[k], rim[k], fr, fi, sn, rsn, &re[k], &im[k]);
+        if (t > 0) {  // the mirrored column: conj(F(j, t)) at (bh - j) mod bh, bw - t
+          const int k2 = ((bh - j) % bh) * bw + bw - t;
+          phase_cross_fixed(rre[k2], rim[k2], fr, -fi, sn, rsn, &re[k2], &im[k2]);
+        }
+      };
+      double s0r = x0r, s0i = x0i;
+#pragma unroll
+      for (int q = 0; q < HD; q++) {
+        s0r += ar[q];
+        s0i += ai[q];
+      }
+      emit(0, s0r, s0i);
+      for (int k = 1; k <= hh; k++) {
+        double prr = x0r, pri = x0i, qr = 0.0, qi = 0.0;
+#pragma unroll
+        for (int q = 0; q < HD; q++) {
+          const double c = tch[q * HD + k - 1], s = tsh[q * HD + k - 1];
+          prr = __fma_rn(ar[q], c, prr);
+          pri = __fma_rn(ai[q], c, pri);
+          qr = __fma_rn(br[q], s, qr);
+          qi = __fma_rn(bi[q], s, qi);
+        }
+        emit(k, prr + qi, pri - qr);       // P - i Q
+        emit(bh - k, prr - qi, pri + qr);  // P + i Q
       }
     }
     __syncwarp();
-    const int bidx = phase_group_peak<D>(re, im, cw, sw, ch, sh, bw, bh, sn, t, lr, li);
+    // inverse, rows (complex): lane jj holds X(jj, :); S(i, jj) = sum_ii X(jj, ii) e^{+i a(i, ii)}
+    if (t < bh) {
+      const double* xr = re + t * bw;
+      const double* xi = im + t * bw;
+      x0r = xr[0];
+      x0i = xi[0];
+#pragma unroll
+      for (int q = 1; q <= HD; q++) {
+        const bool in = q <= hw;
+        const double ur = in ? xr[q] : 0.0, ui = in ? xi[q] : 0.0;
+        const double vr = in ? xr[bw - q] : 0.0, vi = in ? xi[bw - q] : 0.0;
+        ar[q - 1] = ur + vr;
+        ai[q - 1] = ui + vi;
+        br[q - 1] = ur - vr;
+        bi[q - 1] = ui - vi;
+      }
+    }
+    __syncwarp();
+    if (t < bh) {
+      double s0r = x0r, s0i = x0i;
+#pragma unroll
+      for (int q = 0; q < HD; q++) {
+        s0r += ar[q];
+        s0i += ai[q];
+      }
+      re[t] = s0r;
+      im[t] = s0i;
+      for (int k = 1; k <= hw; k++) {
+        double prr = x0r, pri = x0i, qr = 0.0, qi = 0.0;
+#pragma unroll
+        for (int q = 0; q < HD; q++) {
+          const double c = tcw[q * HD + k - 1], s = tsw[q * HD + k - 1];
+          prr = __fma_rn(ar[q], c, prr);
+          pri = __fma_rn(ai[q], c, pri);
+          qr = __fma_rn(br[q], s, qr);
+          qi = __fma_rn(bi[q], s, qi);
+        }
+        re[k * bh + t] = prr - qi;  // P + i Q
+        im[k * bh + t] = pri + qr;
+        re[(bw - k) * bh + t] = prr + qi;  // P - i Q
+        im[(bw - k) * bh + t] = pri - qr;
+      }
+    }
+    __syncwarp();
+    // inverse, columns (real part): lane i holds S(i, :); v(j, i) = Re sum_jj S(i, jj) e^{+i b(j, jj)} / sn
+    double best = 0.0;
+    int bidx = -1;
+    if (t < bw) {
+      const double* cr = re + t * bh;
+      const double* ci = im + t * bh;
+      x0r = cr[0];
+#pragma unroll
+      for (int q = 1; q <= HD; q++) {
+        const bool in = q <= hh;
+        const double ur = in ? cr[q] : 0.0, ui = in ? ci[q] : 0.0;
+        const double vr = in ? cr[bh - q] : 0.0, vi = in ? ci[bh - q] : 0.0;
+        ar[q - 1] = ur + vr;  // real parts of a_n
+        bi[q - 1] = ui - vi;  // imaginary parts of b_n
+      }
+      auto cand = [&](int j, double v) {
+        v = div_fixed(v, sn, rsn);
+        const int k = j * bw + t;
+        if (v > best || (bidx >= 0 && v == best && k < bidx)) {
+          best = v;
+          bidx = k;
+        }
+      };
+      double s0 = x0r;
+#pragma unroll
+      for (int q = 0; q < HD; q++) s0 += ar[q];
+      cand(0, s0);
+      for (int k = 1; k <= hh; k++) {
+        double pr = x0r, qi = 0.0;
+#pragma unroll
+        for (int q = 0; q < HD; q++) {
+          pr = __fma_rn(ar[q], tch[q * HD + k - 1], pr);
+          qi = __fma_rn(bi[q], tsh[q * HD + k - 1], qi);
+        }
+        cand(k, pr - qi);       // Re(P + i Q)
+        cand(bh - k, pr + qi);  // Re(P - i Q)
+      }
+    }
+    // the group's peak (lane t gathers lanes t .. t + 2o - 1 of the group):
+    // largest value above 0, lowest raster index on ties
+#pragma unroll
+    for (int o = 1; o < D; o <<= 1) {
+      const double ob = __shfl_down_sync(full, best, o);
+      const int oi = __shfl_down_sync(full, bidx, o);
+      if (t + o < D && oi >= 0 && (bidx < 0 || ob > best || (ob == best && oi < bidx))) {
+        best = ob;
+        bidx = oi;
+      }
+    }
     if (t == 0 && idx < plane) {
       float r = 0.0f;
       if (act && bidx >= 0) {
@@ -659,13 +823,42 @@ double patch_hu1(const float* patch, int bw, int bh) {
 void phase_reference_dft(const float* ref_pixels, float ref_std, int bw, int bh, PhaseRef* out) {
   Ellipse e;
   const int K = build_ellipse(bw, bh, &e);
-  double xg[kPhaseMaxN], tmp[kPhaseTmp], cw[kPhaseMaxN], sw[kPhaseMaxN], ch[kPhaseMaxN], sh[kPhaseMaxN];
+  const double two_pi = 6.283185307179586476925286766559;
+  for (int m = 0; m < bw; m++) {
+    out->cw[m] = std::cos(two_pi * m / bw);
+    out->sw[m] = std::sin(two_pi * m / bw);
+  }
+  for (int m = 0; m < bh; m++) {
+    out->ch[m] = std::cos(two_pi * m / bh);
+    out->sh[m] = std::sin(two_pi * m / bh);
+  }
+  double xg[kPhaseMaxN], tr[kPhaseMaxN], ti[kPhaseMaxN];
   for (int k = 0; k < bw * bh; k++) xg[k] = 0.0;
   for (int k = 0; k < K; k++)
     xg[(e.dy[k] + e.rh) * bw + e.dx[k] + e.rw] = (double)ref_pixels[k] / ((double)ref_std + (double)kEps);
-  phase_twiddles(bw, cw, sw);
-  phase_twiddles(bh, ch, sh);
-  phase_dft(xg, bw, bh, cw, sw, ch, sh, out->re, out->im, tmp);
+  // exact DFT, direct sums: rows, then columns
+  for (int jj = 0; jj < bh; jj++)
+    for (int i = 0; i < bw; i++) {
+      double sr = 0.0, si = 0.0;
+      for (int ii = 0; ii < bw; ii++) {
+        const int m = (i * ii) % bw;
+        sr += xg[jj * bw + ii] * out->cw[m];
+        si -= xg[jj * bw + ii] * out->sw[m];
+      }
+      tr[jj * bw + i] = sr;
+      ti[jj * bw + i] = si;
+    }
+  for (int j = 0; j < bh; j++)
+    for (int i = 0; i < bw; i++) {
+      double sr = 0.0, si = 0.0;
+      for (int jj = 0; jj < bh; jj++) {
+        const int m = (j * jj) % bh;
+        sr += tr[jj * bw + i] * out->ch[m] + ti[jj * bw + i] * out->sh[m];
+        si += ti[jj * bw + i] * out->ch[m] - tr[jj * bw + i] * out->sh[m];
+      }
+      out->re[j * bw + i] = sr;
+      out->im[j * bw + i] = si;
+    }
 }
 
 }  // namespace sred

@@ -34,10 +34,13 @@ constexpr int kPhaseTmp = 2 * kPhaseMaxDim;         // temporaries of phase_dft
 constexpr double kPhasePi = (double)3.14159265358979323846f;
 constexpr float kLog2Hundred = 6.64385618977472469574f;  // log2(100)
 
-// DFT of the reference block of the block-map form, computed on the host.
+// Block-map form of phase correlation (exact DFT): the reference block's
+// spectrum and the twiddles cos / sin(2 pi m / L) of both axes, m < L,
+// computed on the host.
 struct PhaseRef {
   double re[kPhaseMaxN];
   double im[kPhaseMaxN];
+  double cw[kPhaseMaxDim], sw[kPhaseMaxDim], ch[kPhaseMaxDim], sh[kPhaseMaxDim];
 };
 
 // Twiddle tables of one axis: c[a*len+b] = cos(2*PI*(1.0*a*b/len)), s = sin.

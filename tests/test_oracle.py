@@ -240,6 +240,46 @@ def test_block_phase_self_peak():
     assert abs(out[y, x] - np.sqrt(2.0)) < 1e-6
 
 
+def test_block_phase_matches_numpy_fft():
+    """The block-map phase correlation (exact DFT) against numpy's FFT: the
+    kernel's normalised cross-power spectrum of the two spectra (each / sqrt(n)),
+    the real part of the inverse transform and the first strict maximum above 0
+    in raster order, for every interior pixel and several block shapes."""
+    from sred_b200 import synth
+    eps = float(np.float32(1e-7))
+    for bw, bh in [(5, 5), (9, 9), (15, 15), (7, 11), (13, 3)]:
+        img = synth.normalize_input(synth.spot_image(34, 30, 4, seed=bw * 7 + bh))
+        means, stds = oracle.local_stats(img, bw, bh)
+        rw, rh = bw // 2, bh // 2
+        f = np.float32
+        ell = np.array([[(f(i - rw) ** 2) / f(rw * rw) + (f(j - rh) ** 2) / f(rh * rh) <= f(1) for i in range(bw)]
+                        for j in range(bh)])
+        y0, x0 = 15, 16
+        ref_px = (img[y0 - rh:y0 + rh + 1, x0 - rw:x0 + rw + 1][ell] - means[y0, x0]).astype(np.float32)
+        got = oracle.block_phase_raw(img, ref_px, bw, bh, stds[y0, x0], means, stds)
+        R = np.zeros((bh, bw))
+        R[ell] = ref_px.astype(np.float64) / (float(stds[y0, x0]) + eps)
+        R = np.fft.fft2(R)
+        sn = np.sqrt(bw * bh)
+        for y in range(rh, img.shape[0] - rh):
+            for x in range(rw, img.shape[1] - rw):
+                P = np.zeros((bh, bw))
+                blk = img[y - rh:y + rh + 1, x - rw:x + rw + 1].astype(np.float64)
+                P[ell] = (blk[ell] - float(means[y, x])) / (float(stds[y, x]) + eps)
+                F = np.fft.fft2(P) / sn
+                m = R * np.conj(F)
+                a, b = np.abs(m.real), np.abs(m.imag)
+                X = (m.real * a + m.imag * b + 1j * (m.imag * a - m.real * b)) / (a * a + b * b + eps)
+                v = np.real(np.fft.ifft2(X)) * (bw * bh) / sn
+                pos = np.flatnonzero(v.ravel() > 0)
+                if pos.size == 0:
+                    exp = 0.0
+                else:
+                    k = pos[np.argmax(v.ravel()[pos])]
+                    exp = float(np.float32(np.hypot(k % bw + 1, k // bw + 1)))
+                assert got[y, x] == exp, (bw, bh, y, x)
+
+
 # ---------------------------------------------------------------------------
 # Variance stabilisation: the restatement against an independent numpy
 # evaluation of java/VarianceStabilisingTransform2D_.java:136-151 and
