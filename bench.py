@@ -748,7 +748,14 @@ def run_batch(args, rank, local, world):
     13x13 and 15x15 blocks (K = 5, 13, 49, 113, 149) and with Pearson's R and
     SSIM at relevance 1.0: 10 maps per image through sred_global_map_2d_batch
     with host buffers. Reports the sum over maps of relevant^2 block pairs per
-    second of wall time (transfers included) and maps per second."""
+    second of wall time (transfers included) and maps per second.
+
+    Before the warm-up, unless --no-tune, a tuning pass (one worker, untimed)
+    maps one image per (block, metric, block-count class) with
+    sred_set_gram_tuning on, so the tensor-core engine times its launch shapes
+    for each key the process table lacks; the table is saved next to the
+    library and its entries go into the line. Tuning is off in the timed
+    run."""
     import torch
     from sred_b200 import _lib, clutils, synth
     torch.cuda.set_device(local)
@@ -762,6 +769,24 @@ def run_batch(args, rank, local, world):
             for metric in ("Pearson's R", "SSIM"):
                 jobs.append({"metric": metric, "img": img, "block_width": b, "block_height": b,
                              "relevance_constant": 1.0})
+    tuning = []
+    if args.tune:
+        groups = {}
+        for j in jobs:
+            hh, ww = j["img"].shape
+            nb = (ww - j["block_width"] + 1) * (hh - j["block_height"] + 1)
+            key = (j["block_width"], j["metric"], 0 if nb < 1 << 16 else 1 if nb < 1 << 18 else 2)
+            groups.setdefault(key, []).append(j)
+        pick = [sorted(g, key=lambda j: j["img"].size)[len(g) // 2] for g in groups.values()]
+        ctx.set_gram_tuning(True)
+        clutils.global_map_batch(pick, n_workers=1, ctx=ctx)
+        ctx.set_gram_tuning(False)
+        torch.cuda.synchronize()
+        if rank == 0:
+            _lib.gram_tuning_save(device=torch.cuda.get_device_name(local))
+        tuning = [f"K'={t['kq']} {t['metric_name']} class {t['size_class']}: {t['bn']} cols, "
+                  f"{'A resident' if t['a_resident'] else 'A chunk ring'}, L<={t['max_l']} ({t['ms']:.3f} ms)"
+                  for t in _lib.gram_tuning_entries()]
     # warm-up: the largest image's ten maps, W times (this also sizes every
     # worker's workspaces)
     big = max(range(args.images), key=lambda i: jobs[10 * i]["img"].size)
@@ -784,7 +809,8 @@ def run_batch(args, rank, local, world):
             "config": {"workload": f"{args.images} images x 5 block sizes x 2 metrics = {len(jobs)} global maps, "
                                    "sides 256-1024, relevance 1.0; warm-up: the largest image's 10 maps",
                        "images": args.images, "maps": len(jobs),
-                       "workers": args.workers, "pairs": pairs},
+                       "workers": args.workers, "pairs": pairs,
+                       "launch_shapes": tuning if args.tune else "default (tuning off)"},
             "maps_per_s": len(jobs) * world / dt}
     print(json.dumps(line), flush=True)
 
@@ -833,6 +859,8 @@ def main():
                          "row-sharded across the GPUs (strong scaling)")
     ap.add_argument("--images", type=int, default=8, help="images of the batch workload (10 maps each)")
     ap.add_argument("--workers", type=int, default=4, help="host workers of the batch workload")
+    ap.add_argument("--no-tune", dest="tune", action="store_false",
+                    help="batch workload: skip the launch-shape tuning pass (default shapes)")
     ap.add_argument("--frames", type=int, default=64, help="frames of the block-map workload")
     ap.add_argument("--size", type=int, default=1024,
                     help="image side (default 1024, the benchmark workload; smaller sides for profiling)")

@@ -107,25 +107,35 @@ sred_status sred_calculate_global_repetition_map_2d(
 
 /* The whole command after preprocessing, as GlobalRepetition2D_.run does it
  * (java/GlobalRepetition2D_.java:97-145): K, local statistics, relevance
- * mask, nPixels and the map, all on the device. */
+ * mask, nPixels and the map, all on the device.
+ *
+ * Run-to-run determinism of every global map: each block's pair sums are
+ * FP32 partial sums (per tile row or column) added into FP64 totals with
+ * atomic adds, in an order that varies between runs. The FP64 totals can
+ * differ in their last bits (relative 1e-16, against the 2^-24 rounding of
+ * the FP32 map), so a map repeats bit for bit except where a total lies
+ * within that distance of an FP32 rounding boundary. */
 sred_status sred_global_map_2d(sred_ctx *ctx, const char *metric, const float *img, int w, int h,
                                int bw, int bh, float relevance_constant, int normalize_output,
                                float *out, sred_run_info *info);
 
-/* Row-sharded global map (no counterpart in the reference): the map of
+/* Sharded global map (no counterpart in the reference): the map of
  * sred_global_map_2d_device split across n_shards processes, usually one
- * per GPU. Phase 1, on every shard: the moment pass, relevance mask and
- * compaction (all of them, on every shard), then the all-pairs sums of this
- * shard's rows only; they are written to d_sums (device memory, capacity in
- * doubles >= 2 x relevant blocks; the interior pixel count always suffices)
- * as [num | den] over the relevant non-flat blocks, zero for other shards'
- * rows, and info->n_relevant - info->n_flat is their count. The caller then
- * sums d_sums over the shards (one all-reduce, e.g. NCCL) and calls phase 2
- * on every shard that needs the map, with the summed buffer: finalisation and
- * normalisation into d_out. Rows are split in 128-row blocks of the compacted
- * block list, shard s taking blocks [n s / S, n (s + 1) / S). No other call
- * may use the context between the two phases (phase 2 then fails with
- * SRED_ERR_ARG). */
+ * per GPU. The all-pairs contraction evaluates each unordered pair of
+ * relevant blocks once, as tiles of the upper triangle of the pair matrix
+ * grouped into work items (a tile adds its pair terms to both blocks' sums);
+ * shard s of S takes work items [I s / S, I (s + 1) / S) of the I items of
+ * the engine's default launch shape. Phase 1, on every shard: the moment
+ * pass, relevance mask and compaction (all of them, on every shard), then
+ * the pair terms of this shard's tiles, added into d_sums (device memory,
+ * capacity in doubles >= 2 x relevant blocks; the interior pixel count
+ * always suffices) laid out as [num | den] over the relevant non-flat
+ * blocks; info->n_relevant - info->n_flat is their count. Every shard's
+ * sums cover part of every block's pairs. The caller then sums d_sums over
+ * the shards (one all-reduce, e.g. NCCL) and calls phase 2 on every shard
+ * that needs the map, with the summed buffer: finalisation and normalisation
+ * into d_out. No other call may use the context between the two phases
+ * (phase 2 then fails with SRED_ERR_ARG). */
 sred_status sred_global_map_2d_shard_sums(sred_ctx *ctx, const char *metric, const float *d_img, int w, int h,
                                           int bw, int bh, float relevance_constant, int shard, int n_shards,
                                           double *d_sums, size_t capacity, void *stream, sred_run_info *info);
@@ -149,7 +159,8 @@ typedef struct {
  * command computes one map per invocation): jobs run on `n_workers` (1..8)
  * host threads, each with its own CUDA stream and workspaces, so that one
  * map's host steps and transfers overlap another map's kernels. Each map is
- * identical to what sred_global_map_2d returns for it. Returns SRED_OK if
+ * what sred_global_map_2d returns for it (up to the FP64 sum order described
+ * there). Returns SRED_OK if
  * every job succeeded, else the first failing job's status. */
 sred_status sred_global_map_2d_batch(sred_ctx *ctx, sred_job *jobs, int n_jobs, int n_workers);
 
@@ -166,20 +177,27 @@ sred_status sred_global_map_2d_device(sred_ctx *ctx, const char *metric, const f
  * block_size, bw, bh, ref_mean and ref_std are the ReferenceBlock2D fields
  * (java/Utils.java:108-216), passed through unchanged. metric:
  * "Pearson's R", "SSIM", "NRMSE (inverted)", "Abs. Diff. of StdDevs." (the
- * reference's four), or one of three without a dialog entry in the
+ * reference's four), or one of four without a dialog entry in the
  * reference, all post-processed like Pearson:
  *   "Cosine"            raw-vector cosine similarity;
  *   "Hu moments"        cl/kernelGetPatchHu2D.cl (sqrt(hu1_ref * hu1_block))
  *                       with the reference block's ellipse pixels normalised
  *                       the way that kernel normalises each block
  *                       (mean-subtract, min-max to [0, 1], FP64);
- *   "Phase correlation" the peak distance of
- *                       cl/kernelGetPhaseCorrelationMap.cl's normalised
- *                       cross-power spectrum (repaired as for
- *                       sred_phase_correlation_map_2d) between the reference
- *                       block / (ref_std + eps) and each block, normalised
- *                       with its FP32 local mean and std, both restricted to
- *                       the ellipse; bw, bh <= 15. */
+ *   "Phase correlation" the peak distance of the normalised cross-power
+ *                       spectrum of cl/kernelGetPhaseCorrelationMap.cl
+ *                       (repaired as for sred_phase_correlation_map_2d)
+ *                       between the reference block / (ref_std + eps) and
+ *                       each block, normalised with its FP32 local mean and
+ *                       std, both restricted to the ellipse, through the
+ *                       exact DFT of the block (twiddle angles 2 pi jk / n
+ *                       reduced modulo n, where the kernel takes pi as a
+ *                       float and does not reduce); bw, bh <= 15;
+ *   "Hu distance"       the L2 distance between the seven Hu moment
+ *                       invariants (Hu 1962) of each block's ellipse pixels
+ *                       and those of the reference block, both min-max
+ *                       normalised to [0, 1] first, FP64 (the reference's
+ *                       Hu kernels output the first invariant only). */
 sred_status sred_calculate_block_repetition_map_2d(sred_ctx *ctx, const char *metric, const float *img,
                                                    int w, int h, const float *ref_pixels, int block_size,
                                                    int bw, int bh, float ref_mean, float ref_std,
@@ -332,6 +350,38 @@ sred_status sred_debug_gram_rowdot(sred_ctx *ctx, int engine, const float *u, co
  * SRED_ERR_TIMEOUT with the context still usable. withhold_tile = -1 restores
  * normal operation. */
 sred_status sred_debug_set_tc_wait(sred_ctx *ctx, unsigned long long timeout_ns, long long withhold_tile);
+
+/* Launch-shape tuner of the tensor-core engine (no counterpart in the
+ * reference, whose OpenCL kernels run one fixed work-group size,
+ * java/CLUtils.java:432-433). A global map's contraction can run as
+ * 128 x 256 or 128 x 128 tiles, with each tile's A operand resident or
+ * streamed through a ring of 16 KB chunks, and with 16, 8 or 4 row blocks per
+ * run of work items. The process keeps one table, shared by every context:
+ * key (K' = padded contraction length, metric code, size class of the
+ * contracted block count n: 0 below 65,536, 1 below 262,144, else 2) ->
+ * shape. A map whose key is in the table runs that shape; other maps run the
+ * default shape (128 x 256, A resident when it fits, 16 row blocks).
+ *
+ * sred_set_gram_tuning(ctx, 1) makes later unsharded maps on ctx (and its
+ * batch workers) whose key is missing time every shape on their own
+ * operands, each from zeroed sums, store the fastest, then compute the map
+ * with it: the map equals the one the stored shape gives. Maps running at
+ * the same time on other streams perturb the timings; tune on one context at
+ * a time. Sharded maps always run the default shape. */
+sred_status sred_set_gram_tuning(sred_ctx *ctx, int on);
+
+/* Copies at most `cap` table entries: entries[6 i .. 6 i + 5] = K', metric
+ * code, size class, tile columns (256 or 128), A resident (1) or chunk ring
+ * (0), row blocks per run; ms[i] = that shape's timed contraction in ms.
+ * Returns the number of entries in the table (call with cap 0 to size). */
+int sred_gram_tuning_entries(int *entries, float *ms, int cap);
+
+/* Stores one entry (a shape read back from a saved table); SRED_ERR_ARG when
+ * the shape does not fit K' or the size class is not 0, 1 or 2. */
+sred_status sred_gram_tuning_set(int kq, int metric, int size_class, int bn, int tr, int max_l, float ms);
+
+/* Empties the table. */
+sred_status sred_gram_tuning_clear(void);
 
 /* ---------------------------------------------------------------------
  * 3D block repetition maps. Volumes are w x h x d floats, x fastest then y
@@ -506,11 +556,11 @@ sred_status sred_gat_octree_3d(sred_ctx *ctx, float *vol, int w, int h, int d, i
  * df > 0). */
 double sred_f_quantile(double p, double df);
 
-/* Row-sharded 3D global map (no counterpart in the reference): the two
- * phases of sred_global_map_2d_shard_sums / _finish for
- * sred_global_map_3d_device; the sums layout and the row split are the same
- * ([num | den] over the relevant non-zero-variance blocks, 128-row blocks of
- * the compacted list). Either finish function completes either map. */
+/* Sharded 3D global map (no counterpart in the reference): the two phases
+ * of sred_global_map_2d_shard_sums / _finish for sred_global_map_3d_device;
+ * the sums layout and the work-item split are the same ([num | den] over the
+ * relevant non-zero-variance blocks). Either finish function completes
+ * either map. */
 sred_status sred_global_map_3d_shard_sums(sred_ctx *ctx, const char *metric, const float *d_vol, int w, int h, int d,
                                           int bw, int bh, int bd, float relevance_constant, int shard, int n_shards,
                                           double *d_sums, size_t capacity, void *stream, sred_run_info *info);

@@ -6,6 +6,8 @@ present, calls raise instead of falling back to anything else.
 from __future__ import annotations
 
 import ctypes as C
+import json
+import os
 import threading
 from pathlib import Path
 
@@ -34,6 +36,7 @@ EXPORTS = [
     "sred_gat_3d", "sred_gat_objective_3d", "sred_gat_fit_3d", "sred_classify_redundancy_2d",
     "sred_debug_divide_fixed", "sred_debug_divide_fixed64", "sred_gat_quadtree_2d", "sred_gat_octree_3d", "sred_f_quantile",
     "sred_global_map_3d_shard_sums", "sred_global_map_3d_shard_finish", "sred_debug_set_tc_wait",
+    "sred_set_gram_tuning", "sred_gram_tuning_entries", "sred_gram_tuning_set", "sred_gram_tuning_clear",
 ]
 
 
@@ -146,6 +149,11 @@ def load() -> C.CDLL:
         _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
         L.sred_debug_gram_rowdot.argtypes = [_vp, s, _f32p, _f32p, _f32p, s, s, _f64p, _f64p]
         L.sred_debug_set_tc_wait.argtypes = [_vp, C.c_ulonglong, C.c_longlong]
+        L.sred_set_gram_tuning.argtypes = [_vp, s]
+        L.sred_gram_tuning_entries.argtypes = [_vp, _vp, s]
+        L.sred_gram_tuning_set.argtypes = [s, s, s, s, s, s, C.c_float]
+        L.sred_gram_tuning_clear.argtypes = []
+        L.sred_gram_tuning_entries.restype = s
         L.sred_block_map_2d_device_noalloc.argtypes = [C.c_char_p, _vp, s, s, s, _f32p, s, s, s, C.c_float,
                                                        C.c_float, s, _vp, _vp]
         L.sred_global_map_2d_batch.argtypes = [_vp, C.POINTER(SredJob), s, s]
@@ -156,6 +164,9 @@ def load() -> C.CDLL:
         L.sred_hu_map_2d.argtypes = [_vp, _f32p, _f32p, _f32p, s, s, s, s, _f32p]
         L.sred_phase_correlation_map_2d.argtypes = [_vp, _f32p, _f32p, _f32p, s, s, s, s, _f32p]
         _lib = L
+    path = tuning_path()
+    if path is not None and path.exists():
+        gram_tuning_load(path)
     return _lib
 
 
@@ -180,6 +191,11 @@ class Context:
         self.check(self._L.sred_set_engine(self.h, e), "sred_set_engine")
         self.engine = engine
 
+    def set_gram_tuning(self, on: bool) -> None:
+        """Time the tensor-core launch shapes of maps whose key the process
+        table lacks (sred_set_gram_tuning)."""
+        self.check(self._L.sred_set_gram_tuning(self.h, int(bool(on))), "sred_set_gram_tuning")
+
     def set_log_callback(self, fn) -> None:
         """fn(message: str) receives the context's messages; None turns logging off."""
         self._log_cb = LOG_CB(lambda msg, user: fn(msg.decode())) if fn else LOG_CB()
@@ -200,6 +216,81 @@ class Context:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# Launch-shape table of the tensor-core engine (sred_set_gram_tuning)
+# ---------------------------------------------------------------------------
+
+# Metric codes of the table's keys.
+TUNING_METRICS = {0: "Pearson's R", 1: "SSIM", 2: "NRMSE", 8: "NRMSE (3D, weighted terms)"}
+
+
+def tuning_path() -> Path | None:
+    """The table file next to the library, or the path in SRED_GRAM_TUNING
+    ("off" or "0": none). load() reads it when it exists."""
+    v = os.environ.get("SRED_GRAM_TUNING")
+    if v in ("off", "0"):
+        return None
+    return Path(v) if v else PKG / "gram_tuning.json"
+
+
+def gram_tuning_entries() -> list[dict]:
+    """The process's table: one dict per (K', metric, size class) key."""
+    L = load()
+    n = L.sred_gram_tuning_entries(None, None, 0)
+    e = np.zeros(6 * max(n, 1), np.int32)
+    ms = np.zeros(max(n, 1), np.float32)
+    n = min(n, L.sred_gram_tuning_entries(e.ctypes.data, ms.ctypes.data, n))
+    out = []
+    for i in range(n):
+        kq, metric, ncls, bn, tr, ml = (int(v) for v in e[6 * i:6 * i + 6])
+        out.append({"kq": kq, "metric": metric, "metric_name": TUNING_METRICS.get(metric, str(metric)),
+                    "size_class": ncls, "bn": bn, "a_resident": bool(tr), "max_l": ml, "ms": float(ms[i])})
+    return out
+
+
+def gram_tuning_set(entries: list[dict]) -> int:
+    """Stores entries (as gram_tuning_entries returns them); returns how many
+    the library accepted (shapes that do not fit their K' are skipped)."""
+    L = load()
+    ok = 0
+    for t in entries:
+        st = L.sred_gram_tuning_set(int(t["kq"]), int(t["metric"]), int(t["size_class"]), int(t["bn"]),
+                                    int(bool(t["a_resident"])), int(t["max_l"]), float(t.get("ms", 0.0)))
+        ok += st == OK
+    return ok
+
+
+def gram_tuning_load(path: Path | str) -> int:
+    """Reads a table file written by gram_tuning_save into the process table."""
+    with open(path) as f:
+        data = json.load(f)
+    return gram_tuning_set(data.get("entries", []))
+
+
+def gram_tuning_save(path: Path | str | None = None, device: str = "") -> Path:
+    """Writes the process table (merged over the file's existing entries) as
+    JSON; `device` names the GPU the shapes were timed on."""
+    path = Path(path) if path is not None else (tuning_path() or PKG / "gram_tuning.json")
+    entries = {}
+    if path.exists():
+        with open(path) as f:
+            for t in json.load(f).get("entries", []):
+                entries[(t["kq"], t["metric"], t["size_class"])] = t
+    for t in gram_tuning_entries():
+        entries[(t["kq"], t["metric"], t["size_class"])] = t
+    tmp = path.with_suffix(".tmp")
+    with open(tmp, "w") as f:
+        json.dump({"device": device, "entries": sorted(entries.values(), key=lambda t: (t["kq"], t["metric"],
+                                                                                       t["size_class"]))},
+                  f, indent=1)
+    os.replace(tmp, path)
+    return path
+
+
+def gram_tuning_clear() -> None:
+    load().sred_gram_tuning_clear()
 
 
 _default: Context | None = None

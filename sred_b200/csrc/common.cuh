@@ -164,13 +164,22 @@ struct TcDebug {
   long long withhold_tile;
 };
 
+// A launch shape of the tensor-core engine (bn 0: the default plan): column
+// tile width, whole-tile A buffers (tr 1) or the chunk ring (tr 0), and the
+// largest run of row blocks per work item (L; the item-count rule may lower it).
+struct TcChoice {
+  int bn = 0, tr = 0, L = 0;
+};
+// The launch shapes that fit in shared memory for a K' (at most cap).
+int gram_tc_candidates(int kq, TcChoice* out, int cap);
+
 // Floats of the parameter workspace launch_gram_tc fills (column tiles and
 // row blocks) for n_pad blocks.
 size_t gram_tc_soa_floats(int n_pad);
 
 // Work items of the symmetric schedule for n blocks and tile width bn (the
 // upper triangle of 128-row x bn-column tiles in runs of L row blocks).
-long long gram_tc_items(int n, int bn, int* L, int num_sms);
+long long gram_tc_items(int n, int bn, int* L, int num_sms, int max_L = 0);
 
 // Launch the split-BF16 tcgen05 all-pairs kernel (global_tc.cu).
 // A, B: n_pad x kq bf16 (store_split); params: n_pad entries (rows past n
@@ -181,6 +190,6 @@ long long gram_tc_items(int n, int bn, int* L, int num_sms);
 cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int kq, int n_pad,
                            const BlockParams* params, float* soa_ws, EpiConsts ec, double* num, double* den,
                            int num_sms, int* status, cudaStream_t st, int shard = 0, int n_shards = 1,
-                           const TcDebug* dbg = nullptr);
+                           const TcDebug* dbg = nullptr, const TcChoice* choice = nullptr);
 
 }  // namespace sred

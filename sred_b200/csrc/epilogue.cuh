@@ -110,19 +110,9 @@ __device__ __forceinline__ void pair_terms(float G, const RowState& rp, const Bl
   }
 }
 
-// One pair accumulated into the row sums.
-template <int METRIC, int CMODE>
-__device__ __forceinline__ void epi_pair(float G, const RowState& rp, const BlockParams& cq,
-                                         const EpiConsts& ec, float& sn, float& sd) {
-  float tn, td;
-  pair_terms<METRIC, CMODE>(G, rp, cq, ec, tn, td);
-  sn += tn;
-  sd += td;
-}
-
 // ---------------------------------------------------------------------------
 // Packed FP32 pairs (sm_100 f32x2 arithmetic): two columns' terms per
-// instruction. Used by the tensor-core engine's Pearson fast path.
+// instruction. Used by the tensor-core engine's epilogue.
 // ---------------------------------------------------------------------------
 struct F2 {
   unsigned long long v;
@@ -155,108 +145,6 @@ __device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {  // a * b + c
   F2 r;
   asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
   return r;
-}
-
-// Row constants of the packed Pearson path, both halves equal.
-struct PearsonRow2 {
-  F2 a, e, ne, m1, one;
-};
-
-__device__ __forceinline__ PearsonRow2 make_pearson_row2(const RowState& rs) {
-  PearsonRow2 r;
-  r.a = f2(rs.a, rs.a);
-  r.e = f2(rs.e, rs.e);
-  r.ne = f2(-rs.e, -rs.e);
-  r.m1 = f2(-1.0f, -1.0f);
-  r.one = f2(1.0f, 1.0f);
-  return r;
-}
-
-// Two Pearson pairs (columns q0, q1 of one row), the terms of pair_terms for
-// CMODE kCFirst / kCSecond, accumulated into packed sums (numerator with one
-// fused multiply-add).
-template <int CMODE>
-__device__ __forceinline__ void pearson_pair2(F2 G, F2 aq, F2 rq, const PearsonRow2& r, F2& sn, F2& sd) {
-  const F2 d = sub2(r.a, aq);
-  float m0, m1;
-  f2_split(mul2(d, d), m0, m1);
-  const F2 w = f2(ex2_approx(-m0), ex2_approx(-m1));
-  F2 gc;
-  if (CMODE == kCFirst) {
-    gc = fma2(mul2(G, r.ne), rq, G);  // G - G e_p r_q
-  } else {
-    const F2 t = mul2(r.e, rq);
-    gc = mul2(G, fma2(t, add2(t, r.m1), r.one));  // G (1 - t + t^2)
-  }
-  float g0, g1;
-  f2_split(gc, g0, g1);
-  sn = fma2(f2(fmaxf(g0, 0.0f), fmaxf(g1, 0.0f)), w, sn);
-  sd = add2(sd, w);
-}
-
-// Row constants of the packed SSIM path, both halves equal.
-struct SsimRow2 {
-  F2 a, mu2x2, sig2x, mumu, s2, c1, c2;
-};
-
-__device__ __forceinline__ SsimRow2 make_ssim_row2(const RowState& rs, const EpiConsts& ec) {
-  SsimRow2 r;
-  r.a = f2(rs.a, rs.a);
-  r.mu2x2 = f2(rs.mu2x2, rs.mu2x2);
-  r.sig2x = f2(rs.sig2x, rs.sig2x);
-  r.mumu = f2(rs.mumu, rs.mumu);
-  r.s2 = f2(rs.s2, rs.s2);
-  r.c1 = f2(ec.c1, ec.c1);
-  r.c2 = f2(ec.c2, ec.c2);
-  return r;
-}
-
-// Two SSIM pairs (columns q0, q1 of one row): pair_terms' kSsim arithmetic,
-// operation for operation, on f32x2 pairs (the quotient and the weight per
-// half), accumulated into packed sums.
-__device__ __forceinline__ void ssim_pair2(F2 G, F2 aq, F2 sq, F2 mq, const SsimRow2& r, F2& sn, F2& sd) {
-  const F2 d = sub2(r.a, aq);
-  float m0, m1;
-  f2_split(mul2(d, d), m0, m1);
-  const F2 w = f2(ex2_approx(-m0), ex2_approx(-m1));
-  const F2 num = mul2(fma2(r.mu2x2, mq, r.c1), fma2(mul2(r.sig2x, sq), G, r.c2));
-  const F2 den = mul2(fma2(r.mumu, mul2(mq, mq), r.c1), fma2(sq, sq, r.s2));
-  float n0, n1, d0, d1;
-  f2_split(num, n0, n1);
-  f2_split(den, d0, d1);
-  float t0, t1;
-  f2_split(mul2(f2(__fdividef(n0, d0), __fdividef(n1, d1)), w), t0, t1);
-  sn = add2(sn, f2(fmaxf(t0, 0.0f), fmaxf(t1, 0.0f)));
-  sd = add2(sd, w);
-}
-
-// Column sums of 16 columns over the 32 lanes of a warp (lane l holds row l's
-// terms x[0..15]): four butterfly exchanges halve the columns each lane keeps,
-// a fifth adds the lane pairs. Afterwards lanes 2c and 2c+1 both hold the sum
-// of column c over all 32 rows.
-__device__ __forceinline__ float lane_column_sums16(const float (&x)[16]) {
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  float y8[8], y4[4], y2[2];
-  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
-    const float send = b4 ? x[i] : x[i + 8], keep = b4 ? x[i + 8] : x[i];
-    y8[i] = keep + __shfl_xor_sync(full, send, 16);
-  }
-#pragma unroll
-  for (int i = 0; i < 4; i++) {
-    const float send = b3 ? y8[i] : y8[i + 4], keep = b3 ? y8[i + 4] : y8[i];
-    y4[i] = keep + __shfl_xor_sync(full, send, 8);
-  }
-#pragma unroll
-  for (int i = 0; i < 2; i++) {
-    const float send = b2 ? y4[i] : y4[i + 2], keep = b2 ? y4[i + 2] : y4[i];
-    y2[i] = keep + __shfl_xor_sync(full, send, 4);
-  }
-  const float send = b1 ? y2[0] : y2[1], keep = b1 ? y2[1] : y2[0];
-  float y = keep + __shfl_xor_sync(full, send, 2);
-  return y + __shfl_xor_sync(full, y, 1);
 }
 
 }  // namespace sred

@@ -15,7 +15,12 @@
 // Work item = (column tile ct, a run of up to L row blocks). The item's B tile
 // (BN x K') and column parameters stay in shared memory for the whole item;
 // the A tiles of its row blocks stream through (two whole tiles when they fit,
-// else a ring of 64-column chunks). CTA = 1 per SM, persistent. Warp roles:
+// else a ring of 64-column chunks). Items are ordered run-major, so all CTAs
+// work on the same row blocks at a time and share their A tiles in L2; the
+// producer prefetches A two row blocks ahead and the next item's B into L2.
+// The launch shape (BN = 256 or 128, whole-tile or chunk-ring A, L) is the
+// default of plan_gram_tc or a tuned TcChoice. CTA = 1 per SM, persistent.
+// Warp roles:
 //   warp 16     TMA producer (one thread)
 //   warp 17     MMA issuer (one thread): tcgen05.mma M=128 N=BN K=16 into one
 //               of two TMEM accumulators, tcgen05.commit to publish it
@@ -23,9 +28,11 @@
 //               from BN/4 (w/4) with tcgen05.ld.16x256b, which gives each
 //               thread 4 rows x (BN/16) columns of the warp's slab. The fused
 //               per-pair metric runs on f32x2 pairs of neighbouring columns.
-//               Column sums of the item accumulate in registers (BN/8 values
-//               per thread and sum) and leave once per item after a butterfly
-//               over the 8 lanes that share columns; row sums of a tile leave
+//               Column sums of the item accumulate in per-thread shared
+//               memory slots (BN/16 values per thread and sum, read and
+//               written once per 16-column chunk of each tile) and leave once
+//               per item after a butterfly over the 8 lanes that share
+//               columns; row sums of a tile leave
 //               once per tile after a butterfly over the 4 lanes that share
 //               rows and a combine of the 4 column-group warps in shared
 //               memory: one FP64 atomic add per row per tile.
@@ -1043,24 +1050,38 @@ size_t fixed_smem(int bn) {
 
 }  // namespace
 
-bool plan_gram_tc(int kq, TcPlan* p) {
-  if (kq <= 0 || kq % 32 != 0) return false;
-  for (int bn : {256, 128}) {
-    const size_t fixed = fixed_smem(bn);
-    const size_t a_bytes = (size_t)kBM * kq * 2, b_bytes = (size_t)bn * kq * 2;
-    // whole-tile mode: two A tiles beside the B tile
-    if (fixed + 2 * a_bytes + b_bytes <= kSmemBudget) {
-      *p = TcPlan{bn, true, 2, fixed + 2 * a_bytes + b_bytes};
-      return true;
-    }
-    // chunk ring: at least three 16 KB A stages beside the B tile
-    if (fixed + b_bytes + 3 * kAChunkBytes <= kSmemBudget) {
-      const int st = (int)std::min<size_t>(kMaxStages, (kSmemBudget - fixed - b_bytes) / kAChunkBytes);
-      *p = TcPlan{bn, false, st, fixed + b_bytes + (size_t)st * kAChunkBytes};
-      return true;
-    }
+// Launch shape for a column tile width and A mode, if it fits: the whole-tile
+// mode needs two A tiles beside the B tile, the chunk ring at least three 16 KB
+// A stages (as many as fit, up to kMaxStages).
+bool plan_shape(int kq, int bn, bool tr, TcPlan* p) {
+  if (kq <= 0 || kq % 32 != 0 || (bn != 256 && bn != 128)) return false;
+  const size_t fixed = fixed_smem(bn);
+  const size_t a_bytes = (size_t)kBM * kq * 2, b_bytes = (size_t)bn * kq * 2;
+  if (tr) {
+    if (fixed + 2 * a_bytes + b_bytes > kSmemBudget) return false;
+    *p = TcPlan{bn, true, 2, fixed + 2 * a_bytes + b_bytes};
+    return true;
   }
-  return false;
+  if (fixed + b_bytes + 3 * kAChunkBytes > kSmemBudget) return false;
+  const int st = (int)std::min<size_t>(kMaxStages, (kSmemBudget - fixed - b_bytes) / kAChunkBytes);
+  *p = TcPlan{bn, false, st, fixed + b_bytes + (size_t)st * kAChunkBytes};
+  return true;
+}
+
+bool plan_gram_tc(int kq, TcPlan* p) {
+  // default: 256-column tiles (whole-tile A when it fits), else 128 (chunk ring)
+  return plan_shape(kq, 256, true, p) || plan_shape(kq, 256, false, p) || plan_shape(kq, 128, false, p);
+}
+
+int gram_tc_candidates(int kq, TcChoice* out, int cap) {
+  int n = 0;
+  TcPlan p;
+  for (int bn : {256, 128})
+    for (int tr : {1, 0})
+      if (plan_shape(kq, bn, tr != 0, &p))
+        for (int L : {16, 8, 4})
+          if (n < cap) out[n++] = TcChoice{bn, tr, L};
+  return n;
 }
 
 size_t gram_tc_soa_floats(int n_pad) {
@@ -1068,14 +1089,14 @@ size_t gram_tc_soa_floats(int n_pad) {
   return (size_t)(n_pad / 128) * col_soa_floats(128) + (size_t)(n_pad / 128) * kRowSoaFloats;
 }
 
-long long gram_tc_items(int n, int bn, int* L_out, int num_sms) {
+long long gram_tc_items(int n, int bn, int* L_out, int num_sms, int max_L) {
   const int m = bn / kBM;
   const int n_rb = (n + kBM - 1) / kBM, n_ct = (n + bn - 1) / bn;
   auto items = [&](int L) {
     const int runs = (n_rb + L - 1) / L;
     return items_before_run(runs, n_ct, L / m);
   };
-  int L = 16;
+  int L = max_L > 0 && max_L < 16 ? max_L : 16;
   while (L > 2 && items(L) < 4LL * num_sms) L >>= 1;
   if (L < m) L = m;
   if (L_out) *L_out = L;
@@ -1085,10 +1106,11 @@ long long gram_tc_items(int n, int bn, int* L_out, int num_sms) {
 cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int kq, int n_pad,
                            const BlockParams* params, float* soa_ws, EpiConsts ec, double* num, double* den,
                            int num_sms, int* status, cudaStream_t st, int shard, int n_shards,
-                           const TcDebug* dbg) {
+                           const TcDebug* dbg, const TcChoice* choice) {
   TcPlan plan;
-  if (!plan_gram_tc(kq, &plan) || n_pad % 256 != 0 || n_shards < 1 || shard < 0 || shard >= n_shards)
-    return cudaErrorInvalidValue;
+  const bool planned = choice && choice->bn ? plan_shape(kq, choice->bn, choice->tr != 0, &plan)
+                                            : plan_gram_tc(kq, &plan);
+  if (!planned || n_pad % 256 != 0 || n_shards < 1 || shard < 0 || shard >= n_shards) return cudaErrorInvalidValue;
   if (ec.n <= 0) return cudaSuccess;
   const int bn = plan.bn;
   TcArgs g;
@@ -1102,7 +1124,7 @@ cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int k
   g.n_rb = (ec.n + kBM - 1) / kBM;
   g.n_ct = (ec.n + bn - 1) / bn;
   int L;
-  const long long items = gram_tc_items(ec.n, bn, &L, num_sms);
+  const long long items = gram_tc_items(ec.n, bn, &L, num_sms, choice ? choice->L : 0);
   g.L = L;
   g.h = L / (bn / kBM);
   g.n_runs = (g.n_rb + L - 1) / L;

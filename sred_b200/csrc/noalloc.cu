@@ -69,6 +69,7 @@ int block_metric_id(const char* m) {
   if (!std::strcmp(m, "Cosine")) return sred::kCosine;
   if (!std::strcmp(m, "Hu moments")) return sred::kHu;
   if (!std::strcmp(m, "Phase correlation")) return sred::kPhase;
+  if (!std::strcmp(m, "Hu distance")) return sred::kHu7;
   return -1;
 }
 
@@ -115,6 +116,10 @@ extern "C" sred_status sred_block_map_2d_device_noalloc(const char* metric, cons
     hu_prepare_patch(ref_pixels, bw, bh, patch);
     k_patch_hu<<<dim3((unsigned)((plane + 127) / 128), frames), 128, 0, s>>>(
         d_img, w, h, e, block_size, patch_hu1(patch, bw, bh), d_out, nullptr);
+  } else if (m == kHu7) {
+    Hu7Ref hr;
+    hu7_reference(ref_pixels, e, &hr);
+    launch_block_hu7(d_img, w, h, frames, e, hr, d_out, nullptr, s);
   } else if (m == kPhase) {
     if (bw > kPhaseMaxDim || bh > kPhaseMaxDim) return SRED_ERR_ARG;
     PhaseRef pr;

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -66,6 +67,7 @@ struct sred_ctx {
   std::vector<sred_ctx*> workers;  // extra contexts of sred_global_map_2d_batch (own streams and workspaces)
   GState shard;                    // the map prepared by sred_global_map_2d_shard_sums
   TcDebug tc_debug{0, -1};         // tensor-core wait limit and withheld tile (sred_debug_set_tc_wait)
+  bool tune = false;               // time the launch shapes of an untuned (K', metric, size class)
   void (*log_cb)(const char*, void*) = nullptr;
   void* log_user = nullptr;
 };
@@ -78,6 +80,25 @@ bool fault(const char* what) {
   const char* f = std::getenv("SRED_FAULT");
   return f && std::strcmp(f, what) == 0;
 }
+
+// Launch-shape tuner of the tensor-core engine, shared by every context of
+// the process: (K', metric, size class of the contracted block count) ->
+// the fastest shape timed on a map of that key (TcChoice) and its time.
+struct TuneKey {
+  int kq, metric, nclass;
+  bool operator<(const TuneKey& o) const {
+    return kq != o.kq ? kq < o.kq : metric != o.metric ? metric < o.metric : nclass < o.nclass;
+  }
+};
+struct TuneEntry {
+  TcChoice choice;
+  float ms;
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneEntry> g_tune;
+
+// Size classes: up to 64 Ki blocks, up to 256 Ki, larger.
+int tune_nclass(int n) { return n < (1 << 16) ? 0 : n < (1 << 18) ? 1 : 2; }
 
 // Contraction engine and K' of a global map: Abs-diff needs no contraction
 // (the FP32 engine's kernel without a Gram); the other metrics run on the
@@ -388,11 +409,59 @@ sred_status global_gram(sred_ctx* c, const GState& gs, cudaStream_t st, int shar
     } else {
       int* d_status;
       CKS(ensure(c, B_STATUS, 4, &d_status));
-      CK(cudaMemsetAsync(d_status, 0, 4 * sizeof(int), st));
-      CK(launch_gram_tc(static_cast<const __nv_bfloat16*>(c->buf[B_A].p),
-                        static_cast<const __nv_bfloat16*>(c->buf[B_B].p), gs.kq, (int)gs.n_pad, d_params,
-                        static_cast<float*>(c->buf[B_COLSOA].p), ec, d_num, d_den, c->num_sms, d_status, st, shard,
-                        n_shards, &c->tc_debug));
+      auto run = [&](const TcChoice* ch) -> sred_status {
+        CK(cudaMemsetAsync(d_status, 0, 4 * sizeof(int), st));
+        CK(launch_gram_tc(static_cast<const __nv_bfloat16*>(c->buf[B_A].p),
+                          static_cast<const __nv_bfloat16*>(c->buf[B_B].p), gs.kq, (int)gs.n_pad, d_params,
+                          static_cast<float*>(c->buf[B_COLSOA].p), ec, d_num, d_den, c->num_sms, d_status, st, shard,
+                          n_shards, &c->tc_debug, ch));
+        return SRED_OK;
+      };
+      // The tuned shape of this key (sharded maps keep the default shape, so
+      // that every shard partitions the work alike).
+      TcChoice chosen;
+      bool have = false;
+      const TuneKey key{gs.kq, ec.metric, tune_nclass(gs.n_g)};
+      if (n_shards == 1) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto f = g_tune.find(key);
+        if (f != g_tune.end()) {
+          chosen = f->second.choice;
+          have = true;
+        }
+      }
+      if (!have && c->tune && n_shards == 1) {
+        // time every shape that fits on this map's operands (each from zeroed
+        // sums), keep the fastest, then compute the map with it. Maps running
+        // on other streams at the same time perturb these timings, so a
+        // tuning pass is best run on one context at a time.
+        TcChoice cand[16];
+        const int nc = gram_tc_candidates(gs.kq, cand, 16);
+        float best = 3.4e38f;
+        for (int i = 0; i < nc; i++) {
+          CK(cudaMemsetAsync(d_num, 0, gs.n_pad * sizeof(double), st));
+          CK(cudaMemsetAsync(d_den, 0, gs.n_pad * sizeof(double), st));
+          CK(cudaEventRecord(c->ev[4], st));
+          CKS(run(&cand[i]));
+          CK(cudaEventRecord(c->ev[5], st));
+          CK(cudaEventSynchronize(c->ev[5]));
+          float ms = 0.0f;
+          CK(cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]));
+          if (ms < best) {
+            best = ms;
+            chosen = cand[i];
+          }
+        }
+        if (nc > 0) {
+          have = true;
+          std::lock_guard<std::mutex> lk(g_tune_mu);
+          g_tune[key] = TuneEntry{chosen, best};
+        }
+        CK(cudaMemsetAsync(d_num, 0, gs.n_pad * sizeof(double), st));
+        CK(cudaMemsetAsync(d_den, 0, gs.n_pad * sizeof(double), st));
+        CK(cudaEventRecord(c->ev[1], st));  // ms_gram times the map's own contraction, not the tuning
+      }
+      CKS(run(have ? &chosen : nullptr));
       int status = 0;
       CK(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
@@ -1641,7 +1710,10 @@ sred_status sred_global_map_2d_batch(sred_ctx* c, sred_job* jobs, int n_jobs, in
     if (s != SRED_OK) return fail(c, s, "could not create a batch worker context");
     c->workers.push_back(w);
   }
-  for (sred_ctx* w : c->workers) w->engine = c->engine;
+  for (sred_ctx* w : c->workers) {
+    w->engine = c->engine;
+    w->tune = c->tune;
+  }
   CKS(reserve_global(c, jobs, n_jobs));
   for (int k = 0; k < n_workers - 1; k++) {
     const sred_status s = reserve_global(c->workers[k], jobs, n_jobs);
@@ -1887,6 +1959,50 @@ sred_status sred_block_map_2d_device(sred_ctx* c, const char* metric, const floa
   CKS(block_core(c, m, d_img, w, h, frames, ref_pixels, block_size, bw, bh, ref_mean, ref_std, relc, normalize,
                  d_out, st));
   CK(cudaStreamSynchronize(st));
+  return SRED_OK;
+}
+
+sred_status sred_set_gram_tuning(sred_ctx* c, int on) {
+  if (!c) return SRED_ERR_ARG;
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  c->tune = on != 0;
+  return SRED_OK;
+}
+
+int sred_gram_tuning_entries(int* entries, float* ms, int cap) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  int n = 0;
+  for (const auto& kv : g_tune) {
+    if (entries && ms && n < cap) {
+      int* e = entries + 6 * n;
+      e[0] = kv.first.kq;
+      e[1] = kv.first.metric;
+      e[2] = kv.first.nclass;
+      e[3] = kv.second.choice.bn;
+      e[4] = kv.second.choice.tr;
+      e[5] = kv.second.choice.L;
+      ms[n] = kv.second.ms;
+    }
+    n++;
+  }
+  return n;
+}
+
+sred_status sred_gram_tuning_set(int kq, int metric, int size_class, int bn, int tr, int max_l, float ms) {
+  TcPlan p;
+  TcChoice cand[16];
+  const int nc = gram_tc_candidates(kq, cand, 16);
+  bool ok = false;
+  for (int i = 0; i < nc; i++) ok |= cand[i].bn == bn && cand[i].tr == tr && cand[i].L == max_l;
+  if (!ok || size_class < 0 || size_class > 2 || !plan_gram_tc(kq, &p)) return SRED_ERR_ARG;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[TuneKey{kq, metric, size_class}] = TuneEntry{TcChoice{bn, tr, max_l}, ms};
+  return SRED_OK;
+}
+
+sred_status sred_gram_tuning_clear(void) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune.clear();
   return SRED_OK;
 }
 

@@ -146,3 +146,57 @@ def test_log_callback(ctx):
     n = len(got)
     clutils.global_map_host("Pearson's R", img, 5, 5, 1.0, ctx=ctx)
     assert len(got) == n
+
+
+@pytest.fixture
+def clean_tuning():
+    _lib.gram_tuning_clear()
+    yield
+    _lib.gram_tuning_clear()
+
+
+@pytest.mark.parametrize("metric,b", [("Pearson's R", 9), ("SSIM", 5), ("NRMSE", 15), ("SSIM", 15)])
+def test_gram_tuning_shapes_give_the_same_map(ctx, clean_tuning, metric, b):
+    """The tuner times every launch shape and stores the fastest; the map it
+    returns, and the map of every other shape stored by hand, equal the
+    default shape's map (the pair terms are the same; only the FP64 sum order
+    differs)."""
+    from sred_b200 import clutils, synth
+    img = synth.normalize_input(synth.spot_image(300, 260, 6, seed=17))
+    ctx.set_engine("tc")
+    base, _ = clutils.global_map_host(metric, img, b, b, 1.0, ctx=ctx)
+    ctx.set_gram_tuning(True)
+    tuned, info = clutils.global_map_host(metric, img, b, b, 1.0, ctx=ctx)
+    ctx.set_gram_tuning(False)
+    ent = _lib.gram_tuning_entries()
+    n_g = info["n_relevant"] - info["n_flat"]
+    ncls = 0 if n_g < 1 << 16 else 1 if n_g < 1 << 18 else 2
+    assert len(ent) == 1 and ent[0]["size_class"] == ncls and ent[0]["ms"] > 0, (ent, n_g)
+    np.testing.assert_allclose(tuned, base, rtol=0, atol=2e-6)
+    key = {k: ent[0][k] for k in ("kq", "metric", "size_class")}
+    tried = 0
+    for bn in (256, 128):
+        for tr in (True, False):
+            for ml in (16, 8, 4):
+                if _lib.gram_tuning_set([dict(key, bn=bn, a_resident=tr, max_l=ml)]) != 1:
+                    continue
+                tried += 1
+                out, _ = clutils.global_map_host(metric, img, b, b, 1.0, ctx=ctx)
+                np.testing.assert_allclose(out, base, rtol=0, atol=2e-6, err_msg=f"{bn} {tr} {ml}")
+    assert tried >= 6
+    # a shape the K' does not admit is refused
+    assert _lib.gram_tuning_set([dict(key, bn=192, a_resident=False, max_l=16)]) == 0
+    ctx.set_engine("fp32")
+
+
+def test_gram_tuning_table_round_trip(tmp_path, clean_tuning):
+    """gram_tuning_save / gram_tuning_load restore the table."""
+    n = _lib.gram_tuning_set([{"kq": 160, "metric": 0, "size_class": 2, "bn": 128, "a_resident": False,
+                               "max_l": 8, "ms": 1.5}])
+    assert n == 1
+    p = _lib.gram_tuning_save(tmp_path / "t.json", device="test")
+    _lib.gram_tuning_clear()
+    assert _lib.gram_tuning_entries() == []
+    assert _lib.gram_tuning_load(p) == 1
+    e = _lib.gram_tuning_entries()
+    assert e[0]["bn"] == 128 and not e[0]["a_resident"] and e[0]["max_l"] == 8

@@ -166,7 +166,7 @@ def test_block_phase_every_block_size(ctx, bw, bh):
     np.testing.assert_array_equal(raw, exp.ravel(), err_msg=f"{bw}x{bh}")
 
 
-@pytest.mark.parametrize("metric", [clutils.HU, clutils.PHASE])
+@pytest.mark.parametrize("metric", [clutils.HU, clutils.PHASE, clutils.HU7])
 def test_block_shape_frames_and_noalloc(ctx, shape_fx, metric):
     """A stack of frames on the device equals the frames one by one; the
     allocation-free entry point gives the same maps."""

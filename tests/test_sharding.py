@@ -165,6 +165,52 @@ def test_sharded_exchange_gloo_two_ranks(metric):
     assert all(err < 1e-12 for _, err in res), res
 
 
+def _failing_rank(rank, world, port, out_q):
+    """Rank 1's shard fails before the exchange (as a failed
+    sred_global_map_2d_shard_sums raises SredError) and leaves; rank 0 is
+    already in the all-reduce and must get an error, not wait for good."""
+    import time
+
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    n = 64
+
+    def compute():
+        if rank == 1:
+            raise RuntimeError("injected shard failure")
+        return torch.ones(2 * n, dtype=torch.float64), n
+
+    t0 = time.monotonic()
+    try:
+        clutils.sharded_exchange(compute, lambda s: s, dist.all_reduce)
+        out_q.put((rank, "completed", time.monotonic() - t0))
+    except Exception as e:  # noqa: BLE001 - the test reports any failure kind
+        out_q.put((rank, type(e).__name__ + ": " + str(e)[:80], time.monotonic() - t0))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_exchange_rank_failure_ends_the_collective():
+    """A rank that fails between steps leaves without joining the all-reduce;
+    the other rank's collective ends with an error within the process
+    group's timeout instead of hanging."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_failing_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    assert all(p.exitcode is not None for p in procs), "a rank did not end"
+    res = dict((r, (msg, t)) for r, msg, t in (q.get(timeout=5) for _ in range(2)))
+    assert res[1][0].startswith("RuntimeError: injected shard failure"), res
+    assert res[0][0] != "completed" and res[0][1] < 60.0, res
+
+
 @pytest.mark.parametrize("frames,world", [(0, 2), (1, 2), (7, 2), (8, 3), (5, 8)])
 def test_shard_frames_partition(frames, world):
     spans = [clutils.shard_frames(frames, r, world) for r in range(world)]
