@@ -811,7 +811,11 @@ def run_batch(args, rank, local, world):
                        "images": args.images, "maps": len(jobs),
                        "workers": args.workers, "pairs": pairs,
                        "launch_shapes": tuning if args.tune else "default (tuning off)"},
-            "maps_per_s": len(jobs) * world / dt}
+            "maps_per_s": len(jobs) * world / dt,
+            # per-map CUDA-event times on the workers' streams, summed (with
+            # several workers a map's events also span other maps' kernels)
+            "sum_ms_gram": sum(info["ms_gram"] for _, info in res),
+            "sum_ms_total": sum(info["ms_total"] for _, info in res)}
     print(json.dumps(line), flush=True)
 
 

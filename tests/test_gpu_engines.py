@@ -155,7 +155,8 @@ def clean_tuning():
     _lib.gram_tuning_clear()
 
 
-@pytest.mark.parametrize("metric,b", [("Pearson's R", 9), ("SSIM", 5), ("NRMSE", 15), ("SSIM", 15)])
+# (NRMSE takes three split levels, so 15x15 (K' = 6 x 149 > 576) runs on the FP32 engine and is not tuned.)
+@pytest.mark.parametrize("metric,b", [("Pearson's R", 9), ("SSIM", 5), ("NRMSE", 9), ("SSIM", 15)])
 def test_gram_tuning_shapes_give_the_same_map(ctx, clean_tuning, metric, b):
     """The tuner times every launch shape and stores the fastest; the map it
     returns, and the map of every other shape stored by hand, equal the
@@ -183,7 +184,9 @@ def test_gram_tuning_shapes_give_the_same_map(ctx, clean_tuning, metric, b):
                 tried += 1
                 out, _ = clutils.global_map_host(metric, img, b, b, 1.0, ctx=ctx)
                 np.testing.assert_allclose(out, base, rtol=0, atol=2e-6, err_msg=f"{bn} {tr} {ml}")
-    assert tried >= 6
+    # every K' admits at least one tile width with 16 / 8 / 4 row blocks per run
+    # (NRMSE 9x9, K' = 320, fits only 128-column tiles with the chunk ring)
+    assert tried >= 3
     # a shape the K' does not admit is refused
     assert _lib.gram_tuning_set([dict(key, bn=192, a_resident=False, max_l=16)]) == 0
     ctx.set_engine("fp32")
