@@ -32,6 +32,18 @@ __device__ __forceinline__ float ex2_approx(float x) {
   return y;
 }
 
+// Approximate reciprocal (PTX rcp.approx, documented to about one ulp; the
+// parity tests bound its effect on the maps). The tensor-core epilogue's
+// quotients use it: their divisors are
+// bounded away from 0 and overflow (1 + t >= 1; the SSIM denominator >= c1 c2),
+// and a correctly rounded reciprocal costs a multi-instruction sequence whose
+// registers made the epilogue loop spill.
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 struct RowState {
   float a, e, r, sigma, mu;
   float mu2x2;   // 2 mu_p

@@ -316,10 +316,9 @@ __device__ __forceinline__ void terms2(F2 G, const RowC& rc, F2 qa, F2 qr, F2 qs
       const F2 nt = mul2(rc.ne, qr);     // -t
       gc = mul2(G, fma2(nt, add2(nt, one), one));  // G (1 - t + t^2)
     } else {
-      float d0, d1, g0, g1;
+      float d0, d1;
       f2_split(sub2(one, mul2(rc.ne, qr)), d0, d1);  // 1 + t
-      f2_split(G, g0, g1);
-      gc = f2(g0 * __frcp_rn(d0), g1 * __frcp_rn(d1));
+      gc = mul2(G, f2(rcp_approx(d0), rcp_approx(d1)));
     }
     f2_split(gc, x0, x1);
     x = f2(fmaxf(x0, 0.0f), fmaxf(x1, 0.0f));
@@ -327,10 +326,10 @@ __device__ __forceinline__ void terms2(F2 G, const RowC& rc, F2 qa, F2 qr, F2 qs
     const F2 c1 = f2(ec.c1, ec.c1), c2 = f2(ec.c2, ec.c2);
     const F2 num = mul2(fma2(rc.mu2, qm, c1), fma2(mul2(rc.sg2, qs), G, c2));
     const F2 den = mul2(fma2(rc.mumu, mul2(qm, qm), c1), fma2(qs, qs, rc.s2));
-    float n0, n1, e0, e1;
-    f2_split(num, n0, n1);
+    float e0, e1, q0, q1;
     f2_split(den, e0, e1);
-    x = f2(fmaxf(__fdividef(n0, e0), 0.0f), fmaxf(__fdividef(n1, e1), 0.0f));
+    f2_split(mul2(num, f2(rcp_approx(e0), rcp_approx(e1))), q0, q1);
+    x = f2(fmaxf(q0, 0.0f), fmaxf(q1, 0.0f));
   } else {  // kNrmse, kNrmseW: ((K-1)/K)((s_p - s_q)^2 + 2 s_p s_q (1 - G))
     const F2 sc = f2(ec.nrmse_scale, ec.nrmse_scale);
     const F2 ds = sub2(rc.sg, qs);
