@@ -355,12 +355,12 @@ sred_status sred_debug_set_tc_wait(sred_ctx *ctx, unsigned long long timeout_ns,
  * reference, whose OpenCL kernels run one fixed work-group size,
  * java/CLUtils.java:432-433). A global map's contraction can run as
  * 128 x 256 or 128 x 128 tiles, with each tile's A operand resident or
- * streamed through a ring of 16 KB chunks, and with 16, 8 or 4 row blocks per
- * run of work items. The process keeps one table, shared by every context:
+ * streamed through a ring of 16 KB chunks, and with 32, 16, 8 or 4 row blocks
+ * per run of work items. The process keeps one table, shared by every context:
  * key (K' = padded contraction length, metric code, size class of the
  * contracted block count n: 0 below 65,536, 1 below 262,144, else 2) ->
  * shape. A map whose key is in the table runs that shape; other maps run the
- * default shape (128 x 256, A resident when it fits, 16 row blocks).
+ * default shape (128 x 256, A resident when it fits, 32 row blocks).
  *
  * sred_set_gram_tuning(ctx, 1) makes later unsharded maps on ctx (and its
  * batch workers) whose key is missing time every shape on their own

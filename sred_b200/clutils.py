@@ -262,7 +262,7 @@ def gram_items(n_gram: int, bn: int = 256, num_sms: int = 148) -> tuple[int, int
     """(items, L) of the tensor-core engine's symmetric schedule for n_gram
     blocks and bn-column tiles: the upper triangle of 128-row x bn-column
     tiles, run-major (runs of L row blocks, each run against every column tile
-    that reaches it), L the largest of 16, 8, 4, 2 that leaves at least 4 items
+    that reaches it), L the largest of 32, 16, 8, 4, 2 that leaves at least 4 items
     per SM (the rule libsred applies, global_tc.cu: gram_tc_items)."""
     m = bn // 128
     n_rb, n_ct = (n_gram + 127) // 128, (n_gram + bn - 1) // bn
@@ -270,7 +270,7 @@ def gram_items(n_gram: int, bn: int = 256, num_sms: int = 148) -> tuple[int, int
     def items(L):
         return _items_before_run((n_rb + L - 1) // L, n_ct, L // m)
 
-    L = 16
+    L = 32
     while L > 2 and items(L) < 4 * num_sms:
         L //= 2
     L = max(L, m)

@@ -63,6 +63,7 @@ constexpr int kRowR = 8 * kBM;                    // offset of r in a row-parame
 constexpr int kRowMax = kRowR + kBM;              // offset of max r
 constexpr int kRowFloats = kRowSoaFloats;         // one 128-row block's parameters
 constexpr int kRowPartBytes = 2 * 4 * kBM * 8;    // [2 buffers][4 column groups][128 rows] float2
+constexpr int kMaxRun = 32;                       // row blocks per run (work item), at most
 constexpr int kBarBytes = 512;
 constexpr size_t kSmemBudget = 227 * 1024;
 
@@ -243,13 +244,6 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
 
 // Wait for every TMEM load this thread issued; the register operands tie
 // later uses of v to the wait, so none is scheduled before it.
-__device__ __forceinline__ void tmem_wait16(uint32_t (&v)[8], uint32_t (&u)[8]) {
-  asm volatile("tcgen05.wait::ld.sync.aligned;"
-               : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]),
-                 "+r"(u[0]), "+r"(u[1]), "+r"(u[2]), "+r"(u[3]), "+r"(u[4]), "+r"(u[5]), "+r"(u[6]), "+r"(u[7])
-               :
-               : "memory");
-}
 __device__ __forceinline__ void tmem_wait8(uint32_t (&v)[8]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;"
                : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7])
@@ -922,12 +916,18 @@ __global__ void __launch_bounds__(kThreads, 1)
         __syncwarp();
         unsigned last = 0;
         if (lane == 0) {
-          asm volatile("fence.acq_rel.cta;" ::: "memory");
-          last = (atomicAdd(rowcnt + b * 4 + quarter, 1u) & 3u) == 3u;
-          asm volatile("fence.acq_rel.cta;" ::: "memory");
+          // acquire-release at CTA scope: publishes this warp's partials and,
+          // for the fourth warp, makes the other three warps' partials visible
+          unsigned prev;
+          asm volatile("atom.acq_rel.cta.shared::cta.add.u32 %0, [%1], 1;"
+                       : "=r"(prev)
+                       : "r"(smem_u32(rowcnt + b * 4 + quarter))
+                       : "memory");
+          last = (prev & 3u) == 3u;
         }
         last = __shfl_sync(0xffffffffu, last, 0);
         if (last) {
+          __syncwarp();
           const int row = quarter * 32 + lane;
           float sn = 0.0f, sd = 0.0f;
 #pragma unroll
@@ -1078,7 +1078,7 @@ int gram_tc_candidates(int kq, TcChoice* out, int cap) {
   for (int bn : {256, 128})
     for (int tr : {1, 0})
       if (plan_shape(kq, bn, tr != 0, &p))
-        for (int L : {16, 8, 4})
+        for (int L : {32, 16, 8, 4})
           if (n < cap) out[n++] = TcChoice{bn, tr, L};
   return n;
 }
@@ -1095,7 +1095,7 @@ long long gram_tc_items(int n, int bn, int* L_out, int num_sms, int max_L) {
     const int runs = (n_rb + L - 1) / L;
     return items_before_run(runs, n_ct, L / m);
   };
-  int L = max_L > 0 && max_L < 16 ? max_L : 16;
+  int L = max_L > 0 && max_L < kMaxRun ? max_L : kMaxRun;
   while (L > 2 && items(L) < 4LL * num_sms) L >>= 1;
   if (L < m) L = m;
   if (L_out) *L_out = L;

@@ -178,13 +178,13 @@ def test_gram_tuning_shapes_give_the_same_map(ctx, clean_tuning, metric, b):
     tried = 0
     for bn in (256, 128):
         for tr in (True, False):
-            for ml in (16, 8, 4):
+            for ml in (32, 16, 8, 4):
                 if _lib.gram_tuning_set([dict(key, bn=bn, a_resident=tr, max_l=ml)]) != 1:
                     continue
                 tried += 1
                 out, _ = clutils.global_map_host(metric, img, b, b, 1.0, ctx=ctx)
                 np.testing.assert_allclose(out, base, rtol=0, atol=2e-6, err_msg=f"{bn} {tr} {ml}")
-    # every K' admits at least one tile width with 16 / 8 / 4 row blocks per run
+    # every K' admits at least one tile width with 32 / 16 / 8 / 4 row blocks per run
     # (NRMSE 9x9, K' = 320, fits only 128-column tiles with the chunk ring)
     assert tried >= 3
     # a shape the K' does not admit is refused
