@@ -226,73 +226,104 @@ __global__ void k_scatter(const uint8_t* __restrict__ flags, size_t n, const int
 }
 
 // ---------------------------------------------------------------------------
-// Operand packing: one warp per gram block. FP64 moments of the ellipse
-// vector, unit vector u = (x - mu) / |x - mu|, per-block epilogue params,
-// and the closed-form sums the flat blocks need:
+// Operand packing: each warp takes 32 consecutive gram blocks at a time (their
+// pixels overlap, so the passes hit L1). FP64 moments of the ellipse vector,
+// unit vector u = (x - mu) / |x - mu|, per-block epilogue params, and the
+// closed-form sums the flat blocks need:
 //   sums[0] = sum_q 2^-(a_q)^2           (weight of a pair with a flat block)
 //   sums[1] = sum_q sqrt((K-1)/K) sigma_q (NRMSE against a flat block)
 //   sums[2] = sum_q sigma_q 2^-(a_q)^2     (Abs-diff against a flat block)
-// mode 0: U only (fp32, row pitch kp). mode 1 / 2: the two- / three-level
-// split BF16 operands A, B (store_split; row pitch kq), and U as well when U
-// is given (tensor-core NRMSE). Rows [n, n_pad) are zero-filled by the host.
+// The block sums are warp-wide reductions, one block after another; the
+// per-block scalar work (square roots, quotients, exp2, params) then runs on
+// lane k for block k of the 32, instead of on one lane per block while the
+// other 31 wait. mode 0: U only (fp32, row pitch kp). mode 1 / 2: the two- /
+// three-level split BF16 operands A, B (store_split; row pitch kq), and U as
+// well when U is given (tensor-core NRMSE). Rows [n, n_pad) are zero-filled by
+// the host.
 // ---------------------------------------------------------------------------
 __global__ void k_pack(const float* __restrict__ img, int W, Ellipse e, const int* __restrict__ gram_pix,
                        int n, float wscale, int mode, float* __restrict__ U, int kp,
                        __nv_bfloat16* __restrict__ A, __nv_bfloat16* __restrict__ B, int kq,
                        BlockParams* __restrict__ params, float* __restrict__ tile_rmax,
                        double* __restrict__ sums) {
+  const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   const int K = e.k;
   const double sk = sqrt((double)(K - 1) / (double)K);
+  const double rK = __drcp_rn((double)K);  // s / K as div_fixed: the correctly rounded quotient
   double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-  for (int j = gw; j < n; j += nw) {
-    const int p = gram_pix[j];
-    const int x = p % W, y = p / W;
-    double s = 0.0;
-    for (int i = lane; i < K; i += 32) s += (double)img[(size_t)(y + e.dy[i]) * W + (x + e.dx[i])];
-    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    const double mu = s / K;
-    double v = 0.0;
-    for (int i = lane; i < K; i += 32) {
-      double d = (double)img[(size_t)(y + e.dy[i]) * W + (x + e.dx[i])] - mu;
-      v += d * d;
-    }
-    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    const double nrm = sqrt(v);
-    const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
-    const double sigma = sqrt(v / (K - 1));
-    for (int i = lane; i < K; i += 32) {
-      double u = ((double)img[(size_t)(y + e.dy[i]) * W + (x + e.dx[i])] - mu) * inv;
-      if (U) U[(size_t)j * kp + i] = (float)u;
-      if (mode != 0) store_split(A + (size_t)j * kq, B + (size_t)j * kq, K, i, u, mode + 1);
-    }
-    if (U)
-      for (int i = K + lane; i < kp; i += 32) U[(size_t)j * kp + i] = 0.0f;
-    if (mode != 0) {
-      for (int i = (mode == 1 ? 3 : 6) * K + lane; i < kq; i += 32) {
-        A[(size_t)j * kq + i] = __float2bfloat16_rn(0.0f);
-        B[(size_t)j * kq + i] = __float2bfloat16_rn(0.0f);
+  for (long long j0 = 32LL * gw; j0 < n; j0 += 32LL * nw) {
+    const int nb = (int)min(32LL, (long long)n - j0);
+    // The sum and centred sum of squares of each block; lane k keeps block k's.
+    double my_s = 0.0, my_v = 0.0;
+    for (int k = 0; k < nb; k++) {
+      const int p = gram_pix[j0 + k];
+      const int x = p % W, y = p / W;
+      double s = 0.0;
+      for (int i = lane; i < K; i += 32) s += (double)img[(size_t)(y + e.dy[i]) * W + (x + e.dx[i])];
+      for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(full, s, o);
+      const double mu = div_fixed(s, (double)K, rK);
+      double v = 0.0;
+      for (int i = lane; i < K; i += 32) {
+        const double d = (double)img[(size_t)(y + e.dy[i]) * W + (x + e.dx[i])] - mu;
+        v += d * d;
+      }
+      for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(full, v, o);
+      if (lane == k) {
+        my_s = s;
+        my_v = v;
       }
     }
-    if (lane == 0) {
+    // Block j0 + lane's scalars.
+    double mu = 0.0, inv = 0.0;
+    if (lane < nb) {
+      const long long j = j0 + lane;
+      mu = div_fixed(my_s, (double)K, rK);
+      const double nrm = sqrt(my_v);
+      inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+      const double sigma = sqrt(my_v / (K - 1));
       BlockParams bp;
-      float sg = (float)sigma;
       bp.a = (float)(sigma * (double)wscale);
       bp.e = sigma > 0.0 ? (float)((double)kEps / sigma) : 0.0f;
       bp.r = sigma > 0.0 ? (float)(1.0 / sigma) : 0.0f;
-      bp.sigma = sg;
+      bp.sigma = (float)sigma;
       bp.mu = (float)mu;
       bp.pad0 = bp.pad1 = bp.pad2 = 0.0f;
       params[j] = bp;
       atomicMax(reinterpret_cast<int*>(tile_rmax) + (j >> 7), __float_as_int(bp.r));
-      double a = sigma * (double)wscale;
-      double w0 = exp2(-(a * a));
+      const double a = sigma * (double)wscale;
+      const double w0 = exp2(-(a * a));
       acc0 += w0;
       acc1 += sk * sigma;
       acc2 += sigma * w0;
     }
+    // Unit vectors and operands, block by block.
+    for (int k = 0; k < nb; k++) {
+      const long long j = j0 + k;
+      const double mu_k = __shfl_sync(full, mu, k), inv_k = __shfl_sync(full, inv, k);
+      const int p = gram_pix[j];
+      const int x = p % W, y = p / W;
+      for (int i = lane; i < K; i += 32) {
+        const double u = ((double)img[(size_t)(y + e.dy[i]) * W + (x + e.dx[i])] - mu_k) * inv_k;
+        if (U) U[(size_t)j * kp + i] = (float)u;
+        if (mode != 0) store_split(A + (size_t)j * kq, B + (size_t)j * kq, K, i, u, mode + 1);
+      }
+      if (U)
+        for (int i = K + lane; i < kp; i += 32) U[(size_t)j * kp + i] = 0.0f;
+      if (mode != 0) {
+        for (int i = (mode == 1 ? 3 : 6) * K + lane; i < kq; i += 32) {
+          A[(size_t)j * kq + i] = __float2bfloat16_rn(0.0f);
+          B[(size_t)j * kq + i] = __float2bfloat16_rn(0.0f);
+        }
+      }
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    acc0 += __shfl_xor_sync(full, acc0, o);
+    acc1 += __shfl_xor_sync(full, acc1, o);
+    acc2 += __shfl_xor_sync(full, acc2, o);
   }
   __shared__ double red[3][32];
   const int wi = threadIdx.x >> 5;

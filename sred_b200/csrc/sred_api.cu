@@ -347,7 +347,8 @@ sred_status global_prepare(sred_ctx* c, int metric, const float* d_img, int w, i
   const float hden = nv + kEps;
   const float wscale = (float)std::sqrt(1.4426950408889634 / (double)hden);
   if (n_g > 0) {
-    const int pgrid = grid_for((size_t)n_g * 32, 256, 8 * c->num_sms);
+    // one warp per group of 32 blocks
+    const int pgrid = grid_for(((size_t)n_g + 31) / 32 * 32, 256, 8 * c->num_sms);
     const int mode = engine == SRED_ENGINE_FP32 ? 0 : split_levels_for(metric, K) - 1;
     k_pack<<<pgrid, 256, 0, st>>>(d_img, w, e, d_gpix, n_g, wscale, mode, d_U, kp, d_A, d_B, kq, d_params,
                                   d_rmax, d_sums);
