@@ -258,11 +258,27 @@ def _items_before_run(j: int, n_ct: int, h: int) -> int:
     return j * n_ct - h * j * (j - 1) // 2
 
 
+def _panel_items_before_run(j: int, c0: int, c1: int, h: int) -> int:
+    """Items of runs [0, j) in the panel of column tiles [c0, c1): each run j'
+    takes the tiles max(c0, j' h) .. c1 - 1 (global_tc.cu: panel_items_before_run)."""
+    a = min(j, c0 // h + 1)
+    s = a * (c1 - c0)
+    if j > a:
+        s += (j - a) * c1 - h * (j * (j - 1) // 2 - a * (a - 1) // 2)
+    return s
+
+
+def gram_panel(bn: int, kq: int) -> int:
+    """Column tiles per panel: as many bn-column B tiles of K' = kq bf16 as fit
+    in 48 MB (the rule libsred applies, global_tc.cu: launch_gram_tc)."""
+    return max(1, (48 << 20) // (bn * kq * 2))
+
+
 def gram_items(n_gram: int, bn: int = 256, num_sms: int = 148) -> tuple[int, int]:
     """(items, L) of the tensor-core engine's symmetric schedule for n_gram
     blocks and bn-column tiles: the upper triangle of 128-row x bn-column
-    tiles, run-major (runs of L row blocks, each run against every column tile
-    that reaches it), L the largest of 32, 16, 8, 4, 2 that leaves at least 4 items
+    tiles, cut into items (a run of L row blocks against one column tile that
+    reaches it), L the largest of 32, 16, 8, 4, 2 that leaves at least 4 items
     per SM (the rule libsred applies, global_tc.cu: gram_tc_items)."""
     m = bn // 128
     n_rb, n_ct = (n_gram + 127) // 128, (n_gram + bn - 1) // bn
@@ -277,26 +293,55 @@ def gram_items(n_gram: int, bn: int = 256, num_sms: int = 148) -> tuple[int, int
     return items(L), L
 
 
-def shard_items(n_gram: int, shard: int, n_shards: int, bn: int = 256, num_sms: int = 148):
-    """Tiles of shard `shard` of `n_shards`: the work items [I s / S, I (s + 1) / S)
-    of the symmetric schedule, each as (column tile, first row block, end row
-    block). Every pair (p <= q) of the n_gram blocks lies in exactly one tile
-    of exactly one shard."""
-    items, L = gram_items(n_gram, bn, num_sms)
+def decode_items(n_gram: int, i0: int, i1: int, bn: int = 256, num_sms: int = 148, panel: int | None = None):
+    """Items [i0, i1) of the schedule in libsred's order (panels of `panel`
+    column tiles, within a panel run by run, within a run by column tile; None:
+    one panel), each as (column tile, first row block, end row block), empty
+    items left out (global_tc.cu: decode_item)."""
+    _, L = gram_items(n_gram, bn, num_sms)
     m, h = bn // 128, L // (bn // 128)
     n_rb, n_ct = (n_gram + 127) // 128, (n_gram + bn - 1) // bn
-    i0, i1 = items * shard // n_shards, items * (shard + 1) // n_shards
+    n_runs = (n_rb + L - 1) // L
+    if n_ct == 0 or i1 <= i0:
+        return []
+    P = n_ct if not panel else panel
+    spans = []  # (first item, c0, c1, runs)
+    base = 0
+    for c0 in range(0, n_ct, P):
+        c1 = min(c0 + P, n_ct)
+        J = min((c1 - 1) // h + 1, n_runs)
+        spans.append((base, c0, c1, J))
+        base += _panel_items_before_run(J, c0, c1, h)
     out = []
-    j = 0
+    k = 0
     for it in range(i0, i1):
-        while _items_before_run(j + 1, n_ct, h) <= it:
-            j += 1
-        ct = j * h + (it - _items_before_run(j, n_ct, h))
-        rb0 = j * L
+        while k + 1 < len(spans) and spans[k + 1][0] <= it:
+            k += 1
+        b0, c0, c1, J = spans[k]
+        r = it - b0
+        lo, hi = 0, J - 1
+        while lo < hi:
+            mid = (lo + hi + 1) // 2
+            if _panel_items_before_run(mid, c0, c1, h) <= r:
+                lo = mid
+            else:
+                hi = mid - 1
+        ct = max(c0, lo * h) + (r - _panel_items_before_run(lo, c0, c1, h))
+        rb0 = lo * L
         rb1 = min(rb0 + L, (ct + 1) * m, n_rb)
         if rb0 < rb1:
             out.append((ct, rb0, rb1))
     return out
+
+
+def shard_items(n_gram: int, shard: int, n_shards: int, bn: int = 256, num_sms: int = 148,
+                panel: int | None = None):
+    """Tiles of shard `shard` of `n_shards`: the work items [I s / S, I (s + 1) / S)
+    of the symmetric schedule, each as (column tile, first row block, end row
+    block). Every pair (p <= q) of the n_gram blocks lies in exactly one tile
+    of exactly one shard."""
+    items, _ = gram_items(n_gram, bn, num_sms)
+    return decode_items(n_gram, items * shard // n_shards, items * (shard + 1) // n_shards, bn, num_sms, panel)
 
 
 def sharded_exchange(compute_sums, finish, allreduce):

@@ -91,6 +91,7 @@ struct TcArgs {
   int n_rb, n_ct;               // row blocks holding valid rows, column tiles
   int L, h;                     // row blocks per item (a run), L / (BN / 128)
   int n_runs;                   // runs of L row blocks
+  int panel, n_panels;          // column tiles per panel (panel-major item order), panels
   long long item0, item1;       // items of this launch
   const float* colsoa;          // per column tile, permuted (col_soa_pos)
   const float* rowsoa;          // per 128-row block, natural order
@@ -597,44 +598,128 @@ __device__ __forceinline__ void flush_columns(const float (&x)[NV], int q0, cons
   }
 }
 
-// Work items, run-major: run j holds row blocks [jL, jL + L); its items are
-// the column tiles ct = j h .. n_ct - 1 (h = L / (BN / 128): the first column
-// tile that reaches the run's rows), each clipped to the triangle. All CTAs
-// then work on the same row blocks at once, so the A tiles they stream are
-// shared in L2; each item loads its own B tile once.
+// Work items. Run j holds row blocks [jL, jL + L); it meets the column tiles
+// ct >= j h (h = L / (BN / 128): the first column tile that reaches the run's
+// rows), each (run, column tile) an item, clipped to the triangle. The column
+// tiles are grouped into panels of g.panel tiles whose B operand fits in L2;
+// items go panel by panel, within a panel run by run, within a run by column
+// tile. All CTAs then work on the same row blocks at once (their A tiles are
+// read from DRAM once per panel and shared in L2), and a panel's B tiles stay
+// in L2 while every run passes over them (B is read from DRAM about once).
+// With one panel this is the plain run-major order.
+//
+// Items of runs [0, j) in the panel of column tiles [c0, c1): sum over
+// j' < j of c1 - max(c0, j' h).
+__host__ __device__ inline long long panel_items_before_run(long long j, int c0, int c1, int h) {
+  const long long a = min(j, (long long)(c0 / h) + 1);  // runs with j' h <= c0 take the whole panel
+  long long s = a * (c1 - c0);
+  if (j > a) s += (j - a) * (long long)c1 - (long long)h * (j * (j - 1) / 2 - a * (a - 1) / 2);
+  return s;
+}
+
+// Items of runs [0, j) over all column tiles (one panel).
 __host__ __device__ inline long long items_before_run(long long j, int n_ct, int h) {
-  // sum over runs j' < j of (n_ct - j' h)
   return j * n_ct - (long long)h * j * (j - 1) / 2;
 }
 
+// Runs that reach the panel [c0, c1) (j h <= c1 - 1), at most n_runs.
+__host__ __device__ inline int panel_runs(int c1, int h, int n_runs) { return min((c1 - 1) / h + 1, n_runs); }
+
 // Item -> (column tile, row-block range); false for an empty range.
-__device__ __forceinline__ bool decode_item(long long it, const TcArgs& g, int m, int& ct, int& rb0, int& rb1) {
-  int lo = 0, hi = g.n_runs - 1;
+__host__ __device__ inline bool decode_item(long long it, const TcArgs& g, int m, int& ct, int& rb0, int& rb1) {
+  long long base = 0;
+  int c0 = 0, c1 = 0, J = 0;
+  for (int k = 0; k < g.n_panels; k++) {
+    c0 = k * g.panel;
+    c1 = min(c0 + g.panel, g.n_ct);
+    J = panel_runs(c1, g.h, g.n_runs);
+    const long long cnt = panel_items_before_run(J, c0, c1, g.h);
+    if (it < base + cnt || k == g.n_panels - 1) break;
+    base += cnt;
+  }
+  const long long r = it - base;
+  int lo = 0, hi = J - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
-    if (items_before_run(mid, g.n_ct, g.h) <= it) lo = mid;
+    if (panel_items_before_run(mid, c0, c1, g.h) <= r) lo = mid;
     else hi = mid - 1;
   }
-  ct = lo * g.h + (int)(it - items_before_run(lo, g.n_ct, g.h));
+  ct = max(c0, lo * g.h) + (int)(r - panel_items_before_run(lo, c0, c1, g.h));
   rb0 = lo * g.L;
   rb1 = min(rb0 + g.L, min((ct + 1) * m, g.n_rb));
-  return rb0 < rb1;
+  return rb0 < rb1 && ct < c1;
 }
 
-// The tiles of item `it` that pass `phase` takes: pass 0 the full tiles, pass
-// 1 the masked ones (tiles that reach the diagonal, rb >= ct m, and every tile
-// of a ragged last column tile). Every role walks pass 0 over all of the
-// CTA's items, then pass 1, so the masked epilogue runs in a loop of its own.
-// False for an empty range.
-__device__ __forceinline__ bool item_part(long long it, int phase, const TcArgs& g, int m, int bn, int& ct, int& lo,
-                                          int& hi) {
-  int rb0, rb1;
-  if (!decode_item(it, g, m, ct, rb0, rb1)) return false;
-  const bool full = (long long)(ct + 1) * bn <= g.ec.n;
-  const int rbm = full ? min(max(rb0, ct * m), rb1) : rb0;
-  lo = phase == 0 ? rb0 : rbm;
-  hi = phase == 0 ? rbm : rb1;
-  return lo < hi;
+// A CTA's walk over its items it = start, start + stride, ...: the first is
+// decoded with decode_item's search, each later one by stepping forward run by
+// run (a few operations per step instead of a search per item, which matters
+// for small maps whose items hold few tiles).
+struct ItemCursor {
+  long long it;  // current item
+  long long r;   // its offset among the items of run j in panel k
+  int k, c0, c1, J, j;
+
+  __host__ __device__ __forceinline__ void set_panel(const TcArgs& g, int kk) {
+    k = kk;
+    c0 = kk * g.panel;
+    c1 = min(c0 + g.panel, g.n_ct);
+    J = panel_runs(c1, g.h, g.n_runs);
+  }
+  __host__ __device__ __forceinline__ void init(const TcArgs& g, long long start) {
+    it = start;
+    long long base = 0;
+    set_panel(g, 0);
+    while (k < g.n_panels - 1) {
+      const long long cnt = panel_items_before_run(J, c0, c1, g.h);
+      if (start < base + cnt) break;
+      base += cnt;
+      set_panel(g, k + 1);
+    }
+    const long long rr = start - base;
+    int lo = 0, hi = J - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (panel_items_before_run(mid, c0, c1, g.h) <= rr) lo = mid;
+      else hi = mid - 1;
+    }
+    j = lo;
+    r = rr - panel_items_before_run(lo, c0, c1, g.h);
+  }
+  __host__ __device__ __forceinline__ void advance(const TcArgs& g, long long d) {
+    it += d;
+    r += d;
+    for (;;) {
+      const int cnt = c1 - max(c0, j * g.h);  // >= 1 for every run below J
+      if (r < cnt) break;
+      r -= cnt;
+      if (++j >= J) {
+        if (k + 1 >= g.n_panels) break;  // past the last item; the caller stops on it
+        set_panel(g, k + 1);
+        j = 0;
+      }
+    }
+  }
+  // The tiles of the current item that pass `phase` takes: pass 0 the full
+  // tiles, pass 1 the masked ones (tiles that reach the diagonal, rb >= ct m,
+  // and every tile of a ragged last column tile). Every role walks pass 0 over
+  // all of the CTA's items, then pass 1, so the masked epilogue runs in a loop
+  // of its own. False for an empty range.
+  __host__ __device__ __forceinline__ bool part(const TcArgs& g, int m, int bn, int phase, int& ct, int& lo,
+                                                int& hi) const {
+    ct = max(c0, j * g.h) + (int)r;
+    const int rb0 = j * g.L, rb1 = min(rb0 + g.L, min((ct + 1) * m, g.n_rb));
+    const bool full = (long long)(ct + 1) * bn <= g.ec.n;
+    const int rbm = full ? min(max(rb0, ct * m), rb1) : rb0;
+    lo = phase == 0 ? rb0 : rbm;
+    hi = phase == 0 ? rbm : rb1;
+    return lo < hi;
+  }
+};
+
+__device__ __forceinline__ ItemCursor first_item(const TcArgs& g) {
+  ItemCursor c;
+  c.init(g, g.item0 + blockIdx.x);
+  return c;
 }
 
 // End of a role: all warps meet, then the MMA warp frees TMEM.
@@ -727,9 +812,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint32_t s = 0, eph = 0;                // chunk ring: stage, parity of the round being refilled
       bool ok = true;
       for (int phase = 0; ok && phase < 2; phase++)
-      for (long long it = g.item0 + blockIdx.x; ok && it < g.item1; it += gridDim.x) {
+      for (ItemCursor cur = first_item(g); ok && cur.it < g.item1; cur.advance(g, gridDim.x)) {
         int ct, rb0, rb1;
-        if (!item_part(it, phase, g, C::kM, BN, ct, rb0, rb1)) continue;
+        if (!cur.part(g, C::kM, BN, phase, ct, rb0, rb1)) continue;
         const uint32_t cs = item_i & 1;
         // the column-parameter slot the epilogue released two items ago, and the
         // B buffer once the MMAs of the previous item are complete
@@ -743,8 +828,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         item_i++;
         {  // the B tile of this CTA's next item into L2
           int nct, nrb0, nrb1;
-          const long long nit = it + gridDim.x;
-          if (nit < g.item1 && item_part(nit, phase, g, C::kM, BN, nct, nrb0, nrb1) && nct != ct) {
+          ItemCursor nx = cur;
+          nx.advance(g, gridDim.x);
+          if (nx.it < g.item1 && nx.part(g, C::kM, BN, phase, nct, nrb0, nrb1) && nct != ct) {
             for (int c = 0; c < g.nfull; c++) tma_prefetch_2d(&tmB, c * kChunk, nct * BN);
             if (g.tail) tma_prefetch_2d(&tmB64, g.nfull * kChunk, nct * BN);
           }
@@ -821,9 +907,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       const uint64_t a_desc0 = desc_sw128(sA), b_desc0 = desc_sw128(sB);
       bool ok = true;
       for (int phase = 0; ok && phase < 2; phase++)
-      for (long long it = g.item0 + blockIdx.x; ok && it < g.item1; it += gridDim.x) {
+      for (ItemCursor cur = first_item(g); ok && cur.it < g.item1; cur.advance(g, gridDim.x)) {
         int ct, rb0, rb1;
-        if (!item_part(it, phase, g, C::kM, BN, ct, rb0, rb1)) continue;
+        if (!cur.part(g, C::kM, BN, phase, ct, rb0, rb1)) continue;
         if (!mbar_wait(b_bfull, item_i & 1, g, ST_TIMEOUT_MMA, true, true)) { ok = false; break; }
         tc_fence_after();
         item_i++;
@@ -889,13 +975,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     long long tile = 0;
     uint32_t item_i = 0;
     bool ok = true;
-    // One pass over the CTA's items per phase (item_part): the full tiles with
+    // One pass over the CTA's items per phase (ItemCursor::part): the full tiles with
     // the unmasked forms, then the masked tiles, each in a loop of its own.
     auto pass = [&](auto phase_tag) {
     constexpr int kPhase = decltype(phase_tag)::value;
-    for (long long it = g.item0 + blockIdx.x; ok && it < g.item1; it += gridDim.x) {
+    for (ItemCursor cur = first_item(g); ok && cur.it < g.item1; cur.advance(g, gridDim.x)) {
       int ct, rb0, rb1;
-      if (!item_part(it, kPhase, g, C::kM, BN, ct, rb0, rb1)) continue;
+      if (!cur.part(g, C::kM, BN, kPhase, ct, rb0, rb1)) continue;
       const uint32_t cs = item_i & 1;
       if (!mbar_wait(b_cfull + 8 * cs, (item_i >> 1) & 1, g, ST_TIMEOUT_EPI)) { ok = false; break; }
       item_i++;
@@ -1157,6 +1243,9 @@ cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int k
   g.L = L;
   g.h = L / (bn / kBM);
   g.n_runs = (g.n_rb + L - 1) / L;
+  // panels of column tiles whose B tiles (bn x K' bf16 each) fill at most 48 MB of L2
+  g.panel = std::max(1, (int)(((size_t)48 << 20) / g.b_bytes));
+  g.n_panels = (g.n_ct + g.panel - 1) / g.panel;
   g.item0 = items * shard / n_shards;
   g.item1 = items * (shard + 1) / n_shards;
   const int n_ctp = n_pad / bn, n_rbp = n_pad / kBM;

@@ -20,21 +20,47 @@ import pytest
 from sred_b200 import clutils
 
 
-@pytest.mark.parametrize("n_gram", [0, 1, 127, 128, 129, 255, 256, 257, 1000, 4097])
+@pytest.mark.parametrize("n_gram", [0, 1, 127, 128, 129, 255, 256, 257, 1000, 4097, 30001])
 @pytest.mark.parametrize("world", [1, 2, 3, 8])
-@pytest.mark.parametrize("bn,sms", [(256, 148), (128, 148), (256, 4)])
-def test_shard_items_cover_each_pair_once(n_gram, world, bn, sms):
+@pytest.mark.parametrize("bn,sms,panel", [(256, 148, None), (128, 148, None), (256, 4, None), (256, 4, 3),
+                                          (128, 2, 5), (256, 148, 7)])
+def test_shard_items_cover_each_pair_once(n_gram, world, bn, sms, panel):
     n_rb = (n_gram + 127) // 128
     n_ct = (n_gram + bn - 1) // bn
     seen = {}
     for s in range(world):
-        for ct, rb0, rb1 in clutils.shard_items(n_gram, s, world, bn, sms):
+        for ct, rb0, rb1 in clutils.shard_items(n_gram, s, world, bn, sms, panel):
             for rb in range(rb0, rb1):
                 assert (rb, ct) not in seen, (rb, ct)
                 seen[(rb, ct)] = s
     # exactly the tiles holding a pair p <= q with both below n_gram
     want = {(rb, ct) for ct in range(n_ct) for rb in range(n_rb) if rb * 128 <= ct * bn + bn - 1}
     assert set(seen) == want
+
+
+@pytest.mark.parametrize("n_gram,bn,panel", [(5000, 256, 4), (30001, 128, 13), (9000, 256, None)])
+def test_item_order_is_panel_major(n_gram, bn, panel):
+    """Items go panel by panel (column tiles [kP, (k+1)P)), within a panel run by
+    run, within a run by column tile: the decoded list equals that enumeration."""
+    _, L = clutils.gram_items(n_gram, bn)
+    m, h = bn // 128, L // (bn // 128)
+    n_rb, n_ct = (n_gram + 127) // 128, (n_gram + bn - 1) // bn
+    P = panel or n_ct
+    want = []
+    for c0 in range(0, n_ct, P):
+        for j in range((n_rb + L - 1) // L):
+            for ct in range(max(c0, j * h), min(c0 + P, n_ct)):
+                rb0, rb1 = j * L, min(j * L + L, (ct + 1) * m, n_rb)
+                if rb0 < rb1:
+                    want.append((ct, rb0, rb1))
+    items, _ = clutils.gram_items(n_gram, bn)
+    assert clutils.decode_items(n_gram, 0, items, bn, panel=panel) == want
+
+
+def test_gram_panel_fits_48_mb():
+    assert clutils.gram_panel(256, 160) == (48 << 20) // (256 * 160 * 2)
+    assert clutils.gram_panel(256, 160) * 256 * 160 * 2 <= 48 << 20
+    assert clutils.gram_panel(128, 1 << 20) == 1
 
 
 @pytest.mark.parametrize("world", [1, 2, 8])
