@@ -15,8 +15,9 @@
 // Work item = (column tile ct, a run of up to L row blocks). The item's B tile
 // (BN x K') and column parameters stay in shared memory for the whole item;
 // the A tiles of its row blocks stream through (two whole tiles when they fit,
-// else a ring of 64-column chunks). Items are ordered run-major, so all CTAs
-// work on the same row blocks at a time and share their A tiles in L2; the
+// else a ring of 64-column chunks). Items are ordered panel-major (decode_item):
+// all CTAs work on the same row blocks at a time and share their A tiles in
+// L2, and a panel's B tiles stay in L2 while the runs pass over them; the
 // producer prefetches A two row blocks ahead and the next item's B into L2.
 // Each CTA walks its items twice: first their full tiles, then their masked
 // ones (diagonal and ragged tiles, about 0.2% of all), so that the masked
