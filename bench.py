@@ -785,8 +785,7 @@ def run_batch(args, rank, local, world):
         if rank == 0:
             _lib.gram_tuning_save(device=torch.cuda.get_device_name(local))
         tuning = [f"K'={t['kq']} {t['metric_name']} class {t['size_class']}: {t['bn']} cols, "
-                  f"{'A resident' if t['a_resident'] else 'A ring of %d-chunk stages' % t['chunks_per_stage']}, "
-                  f"L<={t['max_l']} ({t['ms']:.3f} ms)"
+                  f"{'A resident' if t['a_resident'] else 'A chunk ring'}, L<={t['max_l']} ({t['ms']:.3f} ms)"
                   for t in _lib.gram_tuning_entries()]
     # warm-up: the largest image's ten maps, W times (this also sizes every
     # worker's workspaces)

@@ -355,15 +355,12 @@ sred_status sred_debug_set_tc_wait(sred_ctx *ctx, unsigned long long timeout_ns,
  * reference, whose OpenCL kernels run one fixed work-group size,
  * java/CLUtils.java:432-433). A global map's contraction can run as
  * 128 x 256 or 128 x 128 tiles, with each tile's A operand resident or
- * streamed through a ring of stages of one or two 16 KB chunks (one MMA
- * commit releases a stage), and with 32, 16, 8 or 4 row blocks per run of
- * work items. The process keeps one table, shared by every context:
+ * streamed through a ring of 16 KB chunks, and with 32, 16, 8 or 4 row blocks
+ * per run of work items. The process keeps one table, shared by every context:
  * key (K' = padded contraction length, metric code, size class of the
  * contracted block count n: 0 below 65,536, 1 below 262,144, else 2) ->
  * shape. A map whose key is in the table runs that shape; other maps run the
- * default shape (128 x 256, A resident when it fits, else a ring of one-chunk
- * stages; 128 x 128 with two-chunk stages when 256 columns do not fit; 32 row
- * blocks).
+ * default shape (128 x 256, A resident when it fits, 32 row blocks).
  *
  * sred_set_gram_tuning(ctx, 1) makes later unsharded maps on ctx (and its
  * batch workers) whose key is missing time every shape on their own
@@ -373,17 +370,15 @@ sred_status sred_debug_set_tc_wait(sred_ctx *ctx, unsigned long long timeout_ns,
  * a time. Sharded maps always run the default shape. */
 sred_status sred_set_gram_tuning(sred_ctx *ctx, int on);
 
-/* Copies at most `cap` table entries: entries[7 i .. 7 i + 6] = K', metric
+/* Copies at most `cap` table entries: entries[6 i .. 6 i + 5] = K', metric
  * code, size class, tile columns (256 or 128), A resident (1) or chunk ring
- * (0), row blocks per run, chunks per ring stage (1 or 2; 1 when A is
- * resident); ms[i] = that shape's timed contraction in ms. Returns the number
- * of entries in the table (call with cap 0 to size). */
+ * (0), row blocks per run; ms[i] = that shape's timed contraction in ms.
+ * Returns the number of entries in the table (call with cap 0 to size). */
 int sred_gram_tuning_entries(int *entries, float *ms, int cap);
 
 /* Stores one entry (a shape read back from a saved table); SRED_ERR_ARG when
  * the shape does not fit K' or the size class is not 0, 1 or 2. */
-sred_status sred_gram_tuning_set(int kq, int metric, int size_class, int bn, int tr, int max_l, int cps,
-                                 float ms);
+sred_status sred_gram_tuning_set(int kq, int metric, int size_class, int bn, int tr, int max_l, float ms);
 
 /* Empties the table. */
 sred_status sred_gram_tuning_clear(void);

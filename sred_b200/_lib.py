@@ -151,7 +151,7 @@ def load() -> C.CDLL:
         L.sred_debug_set_tc_wait.argtypes = [_vp, C.c_ulonglong, C.c_longlong]
         L.sred_set_gram_tuning.argtypes = [_vp, s]
         L.sred_gram_tuning_entries.argtypes = [_vp, _vp, s]
-        L.sred_gram_tuning_set.argtypes = [s, s, s, s, s, s, s, C.c_float]
+        L.sred_gram_tuning_set.argtypes = [s, s, s, s, s, s, C.c_float]
         L.sred_gram_tuning_clear.argtypes = []
         L.sred_gram_tuning_entries.restype = s
         L.sred_block_map_2d_device_noalloc.argtypes = [C.c_char_p, _vp, s, s, s, _f32p, s, s, s, C.c_float,
@@ -239,15 +239,14 @@ def gram_tuning_entries() -> list[dict]:
     """The process's table: one dict per (K', metric, size class) key."""
     L = load()
     n = L.sred_gram_tuning_entries(None, None, 0)
-    e = np.zeros(7 * max(n, 1), np.int32)
+    e = np.zeros(6 * max(n, 1), np.int32)
     ms = np.zeros(max(n, 1), np.float32)
     n = min(n, L.sred_gram_tuning_entries(e.ctypes.data, ms.ctypes.data, n))
     out = []
     for i in range(n):
-        kq, metric, ncls, bn, tr, ml, cps = (int(v) for v in e[7 * i:7 * i + 7])
+        kq, metric, ncls, bn, tr, ml = (int(v) for v in e[6 * i:6 * i + 6])
         out.append({"kq": kq, "metric": metric, "metric_name": TUNING_METRICS.get(metric, str(metric)),
-                    "size_class": ncls, "bn": bn, "a_resident": bool(tr), "max_l": ml, "chunks_per_stage": cps,
-                    "ms": float(ms[i])})
+                    "size_class": ncls, "bn": bn, "a_resident": bool(tr), "max_l": ml, "ms": float(ms[i])})
     return out
 
 
@@ -258,8 +257,7 @@ def gram_tuning_set(entries: list[dict]) -> int:
     ok = 0
     for t in entries:
         st = L.sred_gram_tuning_set(int(t["kq"]), int(t["metric"]), int(t["size_class"]), int(t["bn"]),
-                                    int(bool(t["a_resident"])), int(t["max_l"]), int(t.get("chunks_per_stage", 1)),
-                                    float(t.get("ms", 0.0)))
+                                    int(bool(t["a_resident"])), int(t["max_l"]), float(t.get("ms", 0.0)))
         ok += st == OK
     return ok
 

@@ -140,9 +140,10 @@ __host__ __device__ constexpr int col_soa_floats(int bn) { return 4 * bn + 4; }
 __host__ __device__ constexpr int col_soa_pos(int i) {
   return (i & ~15) + 4 * ((i & 7) >> 1) + 2 * ((i >> 3) & 1) + (i & 1);
 }
-// Row parameters of one 128-row block: per row (a, -eps r, sigma, mu), one
-// float4 the epilogue reads at once, then r x 128, then max r and 3 x pad.
-constexpr int kRowSoaFloats = 4 * 128 + 128 + 4;
+// Row parameters of one 128-row block: per row the pairs (a, a, -eps r, -eps r,
+// sigma, sigma, mu, mu) as the epilogue's f32x2 operands, then r x 128, then
+// max r and 3 x pad.
+constexpr int kRowSoaFloats = 8 * 128 + 128 + 4;
 
 // Launch shape of the tensor-core engine for a K': column tile width (256 or
 // 128), whole-tile A buffers or a ring of 64-column chunks, dynamic shared
@@ -152,7 +153,6 @@ struct TcPlan {
   bool tr;
   int stages;
   size_t smem;
-  int cps = 1;  // chunk ring: 64-column A chunks per stage (one MMA commit per stage)
 };
 bool plan_gram_tc(int kq, TcPlan* plan);
 
@@ -168,7 +168,7 @@ struct TcDebug {
 // tile width, whole-tile A buffers (tr 1) or the chunk ring (tr 0), and the
 // largest run of row blocks per work item (L; the item-count rule may lower it).
 struct TcChoice {
-  int bn = 0, tr = 0, L = 0, cps = 1;
+  int bn = 0, tr = 0, L = 0;
 };
 // The launch shapes that fit in shared memory for a K' (at most cap).
 int gram_tc_candidates(int kq, TcChoice* out, int cap);

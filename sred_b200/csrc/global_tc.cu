@@ -65,7 +65,7 @@ constexpr int kEpiWarps = 16;                     // 4 per SM sub-partition
 constexpr int kThreads = (kEpiWarps + 2) * 32;
 constexpr int kEpiThreads = kEpiWarps * 32;
 constexpr int kRSlots = 2;                        // row-parameter ring depth
-constexpr int kRowR = 4 * kBM;                    // offset of r in a row-parameter slot
+constexpr int kRowR = 8 * kBM;                    // offset of r in a row-parameter slot
 constexpr int kRowMax = kRowR + kBM;              // offset of max r
 constexpr int kRowFloats = kRowSoaFloats;         // one 128-row block's parameters
 constexpr int kRowPartBytes = 2 * 4 * kBM * 8;    // [2 buffers][4 column groups][128 rows] float2
@@ -87,7 +87,6 @@ struct Cfg {
 
 struct TcArgs {
   int kq, nkc, stages;          // K', K chunks per tile (nfull + tail), chunk-ring depth
-  int cps;                      // chunk ring: chunks per stage
   int nfull, tail;              // whole-tile mode: 64-column chunks and a 32-column tail (0 or 1)
   uint32_t a_bytes, b_bytes;    // whole A tile and whole B tile (64-column chunks + 32-column tail)
   int n_rb, n_ct;               // row blocks holding valid rows, column tiles
@@ -272,18 +271,19 @@ struct RowC {
 template <int METRIC>
 __device__ __forceinline__ RowC make_rowc(const float* __restrict__ rs, int row, const EpiConsts& ec) {
   RowC c;
-  const float4 v = *reinterpret_cast<const float4*>(rs + 4 * row);  // a, -eps r, sigma, mu
-  c.a = f2(v.x, v.x);
-  if (METRIC == kPearson) c.ne = f2(v.y, v.y);
+  const float4 lo = *reinterpret_cast<const float4*>(rs + 8 * row);  // a, a, -eps r, -eps r
+  c.a = f2(lo.x, lo.y);
+  if (METRIC == kPearson) c.ne = f2(lo.z, lo.w);
   if (METRIC == kDebugDot) {
     const float r = rs[kRowR + row];
     c.r = f2(r, r);
   }
   if (METRIC == kSsim || METRIC == kNrmse || METRIC == kNrmseW) {
-    c.sg = f2(v.z, v.z);
+    const float4 hi = *reinterpret_cast<const float4*>(rs + 8 * row + 4);  // sigma, sigma, mu, mu
+    c.sg = f2(hi.x, hi.y);
     c.sg2 = add2(c.sg, c.sg);
     if (METRIC == kSsim) {
-      const F2 m = f2(v.w, v.w);
+      const F2 m = f2(hi.z, hi.w);
       c.mu2 = add2(m, m);
       c.mumu = mul2(m, m);
       c.s2 = fma2(c.sg, c.sg, f2(ec.c2, ec.c2));
@@ -498,7 +498,7 @@ __device__ __forceinline__ void sym_tile(uint32_t taddr, const float* __restrict
             float ge = g;
             if (MASKED && force[kr] && q == p) ge = 1.0f;
             if (!(ge > ec.nrmse_near) || !rv) continue;
-            const float sp = rs[4 * row + 2];
+            const float sp = rs[8 * row + 4];
             const int ci = 16 * c + 4 * csub + 2 * rep + lh;  // permuted column slot
             const float sq = cs[2 * BN + ci];
             const float ds = __fsub_rn(sp, sq);
@@ -509,7 +509,7 @@ __device__ __forceinline__ void sym_tile(uint32_t taddr, const float* __restrict
             const float exact = sqrtf(__fmul_rn(ec.nrmse_scale, __fmaf_rn(ds, ds, __fmul_rn(__fmul_rn(sp, sq), D))));
             float corr = exact - approx;
             if (METRIC == kNrmseW) {
-              const float d = __fsub_rn(rs[4 * row], cs[ci]);
+              const float d = __fsub_rn(rs[8 * row], cs[ci]);
               corr *= ex2_approx(-__fmul_rn(d, d));
             }
             f2_add_half(rn[kr], lh, corr);
@@ -751,7 +751,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int S = g.stages, nkc = g.nkc;
   const uint32_t sB = base;                                            // resident B tile
   const uint32_t sA = sB + g.b_bytes;                                  // TR: 2 x a_bytes; else S x 16 KB
-  const uint32_t sC = sA + (TR ? 2 * g.a_bytes : S * g.cps * kAChunkBytes);  // 2 column-parameter slots
+  const uint32_t sC = sA + (TR ? 2 * g.a_bytes : S * kAChunkBytes);    // 2 column-parameter slots
   const uint32_t sR = sC + 2 * C::kCSoa * 4;                           // kRSlots row-parameter slots
   const uint32_t sP = sR + kRSlots * kRowFloats * 4;                   // row partials
   const uint32_t sQ = sP + kRowPartBytes;                              // column accumulators
@@ -858,19 +858,14 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (g.tail) tma_load_2d(dst + g.nfull * kAChunkBytes, &tmA64, b_afull + 8 * ab, g.nfull * kChunk, rb * kBM);
             n_a++;
           } else {
-            // stages of cps chunks: chunks kg .. kg + cps - 1 (the last stage of a
-            // tile may hold fewer; a 32-column tail chunk takes half a chunk)
-            for (int kg = 0; kg < nkc; kg += g.cps) {
+            for (int kc = 0; kc < nkc; kc++) {
               if (!mbar_wait(b_aempty + 8 * s, eph ^ 1, g, ST_TIMEOUT_PRODUCER, true, true)) { ok = false; break; }
-              const int kend = min(kg + g.cps, nkc);
-              const uint32_t tx = (uint32_t)(min(kend, g.nfull) - min(kg, g.nfull)) * kAChunkBytes +
-                                  (kend > g.nfull && g.tail ? kAChunkBytes / 2 : 0);
-              mbar_expect_tx(b_afull + 8 * s, tx);
-              const uint32_t base_s = sA + s * g.cps * kAChunkBytes;
-              for (int kc = kg; kc < kend; kc++) {
-                const uint32_t dst = base_s + (kc - kg) * kAChunkBytes;
-                if (kc < g.nfull) tma_load_2d(dst, &tmA, b_afull + 8 * s, kc * kChunk, rb * kBM);
-                else tma_load_2d(dst, &tmA64, b_afull + 8 * s, kc * kChunk, rb * kBM);  // the 32-column tail
+              if (kc < g.nfull) {
+                mbar_expect_tx(b_afull + 8 * s, kAChunkBytes);
+                tma_load_2d(sA + s * kAChunkBytes, &tmA, b_afull + 8 * s, kc * kChunk, rb * kBM);
+              } else {  // the 32-column tail
+                mbar_expect_tx(b_afull + 8 * s, kAChunkBytes / 2);
+                tma_load_2d(sA + s * kAChunkBytes, &tmA64, b_afull + 8 * s, kc * kChunk, rb * kBM);
               }
               n_a++;
               if (++s == (uint32_t)S) {
@@ -943,23 +938,19 @@ __global__ void __launch_bounds__(kThreads, 1)
             mma_commit(b_accf + 8 * b);
             continue;
           }
-          for (int kg = 0; kg < nkc; kg += g.cps) {
+          for (int kc = 0; kc < nkc; kc++) {
             if (!mbar_wait(b_afull + 8 * s, fph, g, ST_TIMEOUT_MMA, true, true)) { ok = false; break; }
             tc_fence_after();
-            const int kend = min(kg + g.cps, nkc);
-            for (int kc = kg; kc < kend; kc++) {
-              const uint32_t a_off = (s * g.cps + (kc - kg)) * kAChunkBytes;
-              if (kc < g.nfull) {
-                const uint64_t da = a_desc0 + (uint64_t)(a_off >> 4);
-                const uint64_t db = b_desc0 + (uint64_t)(kc * (C::kBChunkBytes >> 4));
+            if (kc < g.nfull) {
+              const uint64_t da = a_desc0 + (uint64_t)(s * (kAChunkBytes >> 4));
+              const uint64_t db = b_desc0 + (uint64_t)(kc * (C::kBChunkBytes >> 4));
 #pragma unroll
-                for (int ks = 0; ks < kChunk / 16; ks++) mma_bf16<BN>(d, da + 2 * ks, db + 2 * ks, (kc | ks) != 0);
-              } else {
-                const uint64_t da = desc_sw64(sA + a_off);
-                const uint64_t db = desc_sw64(sB + g.nfull * C::kBChunkBytes);
-                mma_bf16<BN>(d, da, db, kc != 0);
-                mma_bf16<BN>(d, da + 2, db + 2, 1);
-              }
+              for (int ks = 0; ks < kChunk / 16; ks++) mma_bf16<BN>(d, da + 2 * ks, db + 2 * ks, (kc | ks) != 0);
+            } else {
+              const uint64_t da = desc_sw64(sA + s * kAChunkBytes);
+              const uint64_t db = desc_sw64(sB + g.nfull * C::kBChunkBytes);
+              mma_bf16<BN>(d, da, db, kc != 0);
+              mma_bf16<BN>(d, da + 2, db + 2, 1);
             }
             mma_commit(b_aempty + 8 * s);
             if (++s == (uint32_t)S) {
@@ -1101,8 +1092,8 @@ __global__ void __launch_bounds__(kThreads, 1)
 // Column parameters of each BN-column tile, permuted so that thread t of an
 // epilogue warp finds its four columns of a 16-column chunk (2(t%4) + {0, 1}
 // and 8 + 2(t%4) + {0, 1}) in one float4 (col_soa_pos), with the tile's
-// largest 1/sigma; and the row parameters of each 128-row block, one float4
-// per row (kRowSoaFloats), with the block's largest 1/sigma.
+// largest 1/sigma; and the row parameters of each 128-row block as the
+// epilogue's f32x2 pairs (kRowSoaFloats) with the block's largest 1/sigma.
 // Blocks [0, n_ctp): column tiles; [n_ctp, n_ctp + n_rbp): row blocks.
 template <int BN>
 __global__ void k_sym_soa(const BlockParams* __restrict__ params, int n_ctp, float* __restrict__ colsoa,
@@ -1124,7 +1115,8 @@ __global__ void k_sym_soa(const BlockParams* __restrict__ params, int n_ctp, flo
       o[3 * width + pos] = p.mu;
     } else {
       const float ne = -kEps * p.r;
-      reinterpret_cast<float4*>(o + 4 * i)[0] = make_float4(p.a, ne, p.sigma, p.mu);
+      reinterpret_cast<float4*>(o + 8 * i)[0] = make_float4(p.a, p.a, ne, ne);
+      reinterpret_cast<float4*>(o + 8 * i)[1] = make_float4(p.sigma, p.sigma, p.mu, p.mu);
       o[kRowR + i] = p.r;
     }
     r = p.r;
@@ -1177,42 +1169,34 @@ size_t fixed_smem(int bn) {
 // Launch shape for a column tile width and A mode, if it fits: the whole-tile
 // mode needs two A tiles beside the B tile, the chunk ring at least three 16 KB
 // A stages (as many as fit, up to kMaxStages).
-bool plan_shape(int kq, int bn, bool tr, TcPlan* p, int cps = 1) {
-  if (kq <= 0 || kq % 32 != 0 || (bn != 256 && bn != 128) || cps < 1 || cps > 2) return false;
+bool plan_shape(int kq, int bn, bool tr, TcPlan* p) {
+  if (kq <= 0 || kq % 32 != 0 || (bn != 256 && bn != 128)) return false;
   const size_t fixed = fixed_smem(bn);
   const size_t a_bytes = (size_t)kBM * kq * 2, b_bytes = (size_t)bn * kq * 2;
   if (tr) {
-    if (cps != 1 || fixed + 2 * a_bytes + b_bytes > kSmemBudget) return false;
-    *p = TcPlan{bn, true, 2, fixed + 2 * a_bytes + b_bytes, 1};
+    if (fixed + 2 * a_bytes + b_bytes > kSmemBudget) return false;
+    *p = TcPlan{bn, true, 2, fixed + 2 * a_bytes + b_bytes};
     return true;
   }
-  // a stage holds cps 64-column chunks and is released by one MMA commit; at
-  // least three one-chunk or two two-chunk stages, and two-chunk stages only
-  // when a tile has at least two chunks
-  const size_t stage = (size_t)cps * kAChunkBytes;
-  const int nkc = (kq + kChunk - 1) / kChunk;
-  if ((cps > 1 && nkc < 2) || fixed + b_bytes + (cps == 1 ? 3 : 2) * stage > kSmemBudget) return false;
-  const int st = (int)std::min<size_t>(kMaxStages, (kSmemBudget - fixed - b_bytes) / stage);
-  *p = TcPlan{bn, false, st, fixed + b_bytes + (size_t)st * stage, cps};
+  if (fixed + b_bytes + 3 * kAChunkBytes > kSmemBudget) return false;
+  const int st = (int)std::min<size_t>(kMaxStages, (kSmemBudget - fixed - b_bytes) / kAChunkBytes);
+  *p = TcPlan{bn, false, st, fixed + b_bytes + (size_t)st * kAChunkBytes};
   return true;
 }
 
 bool plan_gram_tc(int kq, TcPlan* p) {
-  // default: 256-column tiles (whole-tile A when it fits, else a ring of
-  // one-chunk stages), else 128 (a ring of two-chunk stages when two fit: one
-  // commit per two chunks made 13x13 and 15x15 maps 4-7% faster)
-  return plan_shape(kq, 256, true, p) || plan_shape(kq, 256, false, p) || plan_shape(kq, 128, false, p, 2) ||
-         plan_shape(kq, 128, false, p, 1);
+  // default: 256-column tiles (whole-tile A when it fits), else 128 (chunk ring)
+  return plan_shape(kq, 256, true, p) || plan_shape(kq, 256, false, p) || plan_shape(kq, 128, false, p);
 }
 
 int gram_tc_candidates(int kq, TcChoice* out, int cap) {
   int n = 0;
   TcPlan p;
   for (int bn : {256, 128})
-    for (int mode : {0, 1, 2})  // A resident; chunk ring of 1 or 2 chunks per stage
-      if (plan_shape(kq, bn, mode == 0, &p, mode == 0 ? 1 : mode))
+    for (int tr : {1, 0})
+      if (plan_shape(kq, bn, tr != 0, &p))
         for (int L : {32, 16, 8, 4})
-          if (n < cap) out[n++] = TcChoice{bn, mode == 0 ? 1 : 0, L, mode == 0 ? 1 : mode};
+          if (n < cap) out[n++] = TcChoice{bn, tr, L};
   return n;
 }
 
@@ -1240,7 +1224,7 @@ cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int k
                            int num_sms, int* status, cudaStream_t st, int shard, int n_shards,
                            const TcDebug* dbg, const TcChoice* choice) {
   TcPlan plan;
-  const bool planned = choice && choice->bn ? plan_shape(kq, choice->bn, choice->tr != 0, &plan, choice->cps)
+  const bool planned = choice && choice->bn ? plan_shape(kq, choice->bn, choice->tr != 0, &plan)
                                             : plan_gram_tc(kq, &plan);
   if (!planned || n_pad % 256 != 0 || n_shards < 1 || shard < 0 || shard >= n_shards) return cudaErrorInvalidValue;
   if (ec.n <= 0) return cudaSuccess;
@@ -1249,7 +1233,6 @@ cudaError_t launch_gram_tc(const __nv_bfloat16* A, const __nv_bfloat16* B, int k
   g.kq = kq;
   g.nkc = (kq + kChunk - 1) / kChunk;  // nfull + tail
   g.stages = plan.stages;
-  g.cps = plan.cps;
   g.nfull = kq / kChunk;
   g.tail = (kq % kChunk) ? 1 : 0;
   g.a_bytes = (uint32_t)kBM * kq * 2;

@@ -436,8 +436,8 @@ sred_status global_gram(sred_ctx* c, const GState& gs, cudaStream_t st, int shar
         // sums), keep the fastest, then compute the map with it. Maps running
         // on other streams at the same time perturb these timings, so a
         // tuning pass is best run on one context at a time.
-        TcChoice cand[32];
-        const int nc = gram_tc_candidates(gs.kq, cand, 32);
+        TcChoice cand[16];
+        const int nc = gram_tc_candidates(gs.kq, cand, 16);
         float best = 3.4e38f;
         for (int i = 0; i < nc; i++) {
           CK(cudaMemsetAsync(d_num, 0, gs.n_pad * sizeof(double), st));
@@ -1975,14 +1975,13 @@ int sred_gram_tuning_entries(int* entries, float* ms, int cap) {
   int n = 0;
   for (const auto& kv : g_tune) {
     if (entries && ms && n < cap) {
-      int* e = entries + 7 * n;
+      int* e = entries + 6 * n;
       e[0] = kv.first.kq;
       e[1] = kv.first.metric;
       e[2] = kv.first.nclass;
       e[3] = kv.second.choice.bn;
       e[4] = kv.second.choice.tr;
       e[5] = kv.second.choice.L;
-      e[6] = kv.second.choice.cps;
       ms[n] = kv.second.ms;
     }
     n++;
@@ -1990,17 +1989,15 @@ int sred_gram_tuning_entries(int* entries, float* ms, int cap) {
   return n;
 }
 
-sred_status sred_gram_tuning_set(int kq, int metric, int size_class, int bn, int tr, int max_l, int cps,
-                                 float ms) {
+sred_status sred_gram_tuning_set(int kq, int metric, int size_class, int bn, int tr, int max_l, float ms) {
   TcPlan p;
-  TcChoice cand[32];
-  const int nc = gram_tc_candidates(kq, cand, 32);
+  TcChoice cand[16];
+  const int nc = gram_tc_candidates(kq, cand, 16);
   bool ok = false;
-  for (int i = 0; i < nc; i++)
-    ok |= cand[i].bn == bn && cand[i].tr == tr && cand[i].L == max_l && cand[i].cps == cps;
+  for (int i = 0; i < nc; i++) ok |= cand[i].bn == bn && cand[i].tr == tr && cand[i].L == max_l;
   if (!ok || size_class < 0 || size_class > 2 || !plan_gram_tc(kq, &p)) return SRED_ERR_ARG;
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune[TuneKey{kq, metric, size_class}] = TuneEntry{TcChoice{bn, tr, max_l, cps}, ms};
+  g_tune[TuneKey{kq, metric, size_class}] = TuneEntry{TcChoice{bn, tr, max_l}, ms};
   return SRED_OK;
 }
 

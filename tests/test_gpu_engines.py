@@ -177,13 +177,13 @@ def test_gram_tuning_shapes_give_the_same_map(ctx, clean_tuning, metric, b):
     key = {k: ent[0][k] for k in ("kq", "metric", "size_class")}
     tried = 0
     for bn in (256, 128):
-        for tr, cps in ((True, 1), (False, 1), (False, 2)):
+        for tr in (True, False):
             for ml in (32, 16, 8, 4):
-                if _lib.gram_tuning_set([dict(key, bn=bn, a_resident=tr, max_l=ml, chunks_per_stage=cps)]) != 1:
+                if _lib.gram_tuning_set([dict(key, bn=bn, a_resident=tr, max_l=ml)]) != 1:
                     continue
                 tried += 1
                 out, _ = clutils.global_map_host(metric, img, b, b, 1.0, ctx=ctx)
-                np.testing.assert_allclose(out, base, rtol=0, atol=2e-6, err_msg=f"{bn} {tr} {cps} {ml}")
+                np.testing.assert_allclose(out, base, rtol=0, atol=2e-6, err_msg=f"{bn} {tr} {ml}")
     # every K' admits at least one tile width with 32 / 16 / 8 / 4 row blocks per run
     # (NRMSE 9x9, K' = 320, fits only 128-column tiles with the chunk ring)
     assert tried >= 3
@@ -195,11 +195,11 @@ def test_gram_tuning_shapes_give_the_same_map(ctx, clean_tuning, metric, b):
 def test_gram_tuning_table_round_trip(tmp_path, clean_tuning):
     """gram_tuning_save / gram_tuning_load restore the table."""
     n = _lib.gram_tuning_set([{"kq": 160, "metric": 0, "size_class": 2, "bn": 128, "a_resident": False,
-                               "max_l": 8, "chunks_per_stage": 2, "ms": 1.5}])
+                               "max_l": 8, "ms": 1.5}])
     assert n == 1
     p = _lib.gram_tuning_save(tmp_path / "t.json", device="test")
     _lib.gram_tuning_clear()
     assert _lib.gram_tuning_entries() == []
     assert _lib.gram_tuning_load(p) == 1
     e = _lib.gram_tuning_entries()
-    assert e[0]["bn"] == 128 and not e[0]["a_resident"] and e[0]["max_l"] == 8 and e[0]["chunks_per_stage"] == 2
+    assert e[0]["bn"] == 128 and not e[0]["a_resident"] and e[0]["max_l"] == 8
