@@ -726,13 +726,13 @@ def run_shard(args, rank, local, world):
     if rank != 0:
         return
     pairs = float(info["pairs"])
-    line = {"metric": METRIC.replace("split-BF16 vs FP32 speedup @≤1e-5 err", "one map row-sharded across GPUs"),
+    line = {"metric": METRIC.replace("split-BF16 vs FP32 speedup @≤1e-5 err", "one map sharded across GPUs by work items"),
             "value": pairs / (ms / 1e3), "unit": "block-pairs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "bf16x3 split (hi/lo) tensor-core Gram, f32 accumulate, f64 moments",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "image": f"{W_IMG}x{H_IMG}", "block": f"{BW}x{BH}",
-                       "pairs_per_step": pairs, "parallelism": f"rows sharded over {world} GPU(s), one all-reduce "
+                       "pairs_per_step": pairs, "parallelism": f"work items of the pair triangle sharded over {world} GPU(s), one all-reduce "
                                                                "of per-row sums"}}
     print(json.dumps(line), flush=True)
 
@@ -860,7 +860,7 @@ def main():
                     help="metric of the global workload (the reference's names; default Pearson's R)")
     ap.add_argument("--mode", choices=["replicas", "shard"], default="replicas",
                     help="global workload on N GPUs: independent replicas (default, weak scaling) or one map "
-                         "row-sharded across the GPUs (strong scaling)")
+                         "sharded across the GPUs by work items (strong scaling)")
     ap.add_argument("--images", type=int, default=8, help="images of the batch workload (10 maps each)")
     ap.add_argument("--workers", type=int, default=4, help="host workers of the batch workload")
     ap.add_argument("--no-tune", dest="tune", action="store_false",

@@ -250,7 +250,7 @@ def global_map_batch(jobs: list[dict], n_workers: int = 4, ctx=None) -> list[tup
 
 
 # ---------------------------------------------------------------------------
-# Row-sharded global map (one map across several processes / GPUs)
+# Sharded global map (one map across several processes / GPUs, split by work items)
 # ---------------------------------------------------------------------------
 
 def _items_before_run(j: int, n_ct: int, h: int) -> int:

@@ -92,7 +92,7 @@ def test_global_map_batch_equals_single_maps(ctx):
 
 
 def test_sharded_map_equals_full_map(ctx):
-    """The row-sharded entry points, every shard run in turn on one GPU and
+    """The sharded entry points, every shard run in turn on one GPU and
     their sums added (what the all-reduce does across GPUs), give the map of
     sred_global_map_2d_device."""
     import ctypes as C

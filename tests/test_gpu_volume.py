@@ -250,7 +250,7 @@ def test_fixed_divisor_division_is_ieee(ctx):
 
 
 def test_sharded_3d_map_equals_full_map(ctx):
-    """The row-sharded 3D entry points, every shard run in turn on one GPU and
+    """The sharded 3D entry points, every shard run in turn on one GPU and
     their sums added (what the all-reduce does across GPUs), give the map of
     sred_global_map_3d_device."""
     import ctypes as C
