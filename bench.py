@@ -732,8 +732,9 @@ def run_shard(args, rank, local, world):
             "vs_baseline": None, "dtype": "bf16x3 split (hi/lo) tensor-core Gram, f32 accumulate, f64 moments",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "image": f"{W_IMG}x{H_IMG}", "block": f"{BW}x{BH}",
-                       "pairs_per_step": pairs, "parallelism": f"work items of the pair triangle sharded over {world} GPU(s), one all-reduce "
-                                                               "of per-row sums"}}
+                       "pairs_per_step": pairs,
+                       "parallelism": f"work items of the pair triangle sharded over {world} GPU(s), one all-reduce "
+                                      "of the per-block sums"}}
     print(json.dumps(line), flush=True)
 
 
